@@ -1,0 +1,132 @@
+"""Loader of the in-tree CUDA library ``libalien_b200.so``.
+
+There is no fallback: if the library is missing or no CUDA device is present,
+the facade raises instead of computing anything on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from .params import PhysicsParams
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libalien_b200.so")
+
+ERRORS = {
+    1: "invalid argument",
+    2: "out of memory",
+    3: "CUDA error",
+    4: "device error flag",
+    5: "unsupported",
+    6: "capacity",
+    7: "no CUDA device",
+}
+
+
+class AlienError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, 'error')} ({code}): {message}")
+        self.code = code
+
+
+class Int2(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_int32), ("y", ctypes.c_int32)]
+
+
+class GeneralSettings(ctypes.Structure):
+    _fields_ = [("worldSizeX", ctypes.c_int32), ("worldSizeY", ctypes.c_int32)]
+
+
+class ArraySizes(ctypes.Structure):
+    _fields_ = [("cellArraySize", ctypes.c_uint64), ("particleArraySize", ctypes.c_uint64),
+                ("auxiliaryDataSize", ctypes.c_uint64)]
+
+
+class RawStatistics(ctypes.Structure):
+    _fields_ = [
+        ("timestep", ctypes.c_uint64),
+        ("numCells", ctypes.c_uint64),
+        ("numParticles", ctypes.c_uint64),
+        ("numConnections", ctypes.c_uint64),
+        ("numCellsByColor", ctypes.c_uint64 * 7),
+        ("totalCellEnergy", ctypes.c_double),
+        ("totalParticleEnergy", ctypes.c_double),
+    ]
+
+
+# every symbol declared in include/alien_b200.h and include/alien_b200_batch.h
+EXPORTED_SYMBOLS = [
+    "alien_b200_version", "alien_b200_default_parameters", "alien_b200_last_error", "alien_b200_create",
+    "alien_b200_destroy", "alien_b200_calc_timesteps", "alien_b200_set_data", "alien_b200_get_data",
+    "alien_b200_set_parameters", "alien_b200_get_parameters", "alien_b200_get_array_sizes",
+    "alien_b200_resize_arrays_if_necessary", "alien_b200_get_current_timestep", "alien_b200_set_current_timestep",
+    "alien_b200_clear", "alien_b200_get_raw_statistics", "alien_b200_enqueue_timesteps", "alien_b200_stream",
+    "alien_b200_kernel_launch_count",
+    "alien_b200_batch_create", "alien_b200_batch_destroy", "alien_b200_batch_num_worlds",
+    "alien_b200_batch_calc_timesteps", "alien_b200_batch_enqueue_timesteps", "alien_b200_batch_get_data",
+    "alien_b200_batch_get_array_sizes", "alien_b200_batch_get_raw_statistics", "alien_b200_batch_stream",
+    "alien_b200_batch_kernel_launch_count", "alien_b200_batch_kernels_per_step",
+]
+
+_lib: ctypes.CDLL | None = None
+
+
+def load() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m alien_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, u64, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
+    P = ctypes.POINTER
+    lib.alien_b200_version.restype = i32
+    lib.alien_b200_default_parameters.argtypes = [P(PhysicsParams)]
+    lib.alien_b200_default_parameters.restype = None
+    lib.alien_b200_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+    lib.alien_b200_create.argtypes = [P(GeneralSettings), P(PhysicsParams), u64, P(vp)]
+    lib.alien_b200_destroy.argtypes = [vp]
+    lib.alien_b200_calc_timesteps.argtypes = [vp, u64]
+    lib.alien_b200_enqueue_timesteps.argtypes = [vp, u64]
+    lib.alien_b200_set_data.argtypes = [vp, vp]
+    lib.alien_b200_get_data.argtypes = [vp, Int2, Int2, vp]
+    lib.alien_b200_set_parameters.argtypes = [vp, P(PhysicsParams)]
+    lib.alien_b200_get_parameters.argtypes = [vp, P(PhysicsParams)]
+    lib.alien_b200_get_array_sizes.argtypes = [vp, P(ArraySizes)]
+    lib.alien_b200_resize_arrays_if_necessary.argtypes = [vp, P(ArraySizes)]
+    lib.alien_b200_get_current_timestep.argtypes = [vp, P(u64)]
+    lib.alien_b200_set_current_timestep.argtypes = [vp, u64]
+    lib.alien_b200_clear.argtypes = [vp]
+    lib.alien_b200_get_raw_statistics.argtypes = [vp, P(RawStatistics)]
+    lib.alien_b200_stream.argtypes = [vp]
+    lib.alien_b200_stream.restype = vp
+    lib.alien_b200_kernel_launch_count.argtypes = [vp]
+    lib.alien_b200_kernel_launch_count.restype = u64
+    lib.alien_b200_batch_create.argtypes = [i32, P(GeneralSettings), P(PhysicsParams), vp, u64, P(vp)]
+    lib.alien_b200_batch_destroy.argtypes = [vp]
+    lib.alien_b200_batch_num_worlds.argtypes = [vp]
+    lib.alien_b200_batch_calc_timesteps.argtypes = [vp, u64]
+    lib.alien_b200_batch_enqueue_timesteps.argtypes = [vp, u64]
+    lib.alien_b200_batch_get_data.argtypes = [vp, i32, vp]
+    lib.alien_b200_batch_get_array_sizes.argtypes = [vp, i32, P(ArraySizes)]
+    lib.alien_b200_batch_get_raw_statistics.argtypes = [vp, i32, P(RawStatistics)]
+    lib.alien_b200_batch_stream.argtypes = [vp]
+    lib.alien_b200_batch_stream.restype = vp
+    lib.alien_b200_batch_kernel_launch_count.argtypes = [vp]
+    lib.alien_b200_batch_kernel_launch_count.restype = u64
+    lib.alien_b200_batch_kernels_per_step.argtypes = [vp]
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    lib = load()
+    buf = ctypes.create_string_buffer(1024)
+    lib.alien_b200_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(code: int) -> None:
+    if code != 0:
+        raise AlienError(code, last_error())

@@ -1,0 +1,1064 @@
+// engine.cu - host side of the B200 engine: the arena of worlds, the step
+// launch sequence, data transfer and the C ABI declared in
+// include/alien_b200.h.
+//
+// Arena  : one set of SoA device arrays for N independent worlds; one step
+//          of all worlds is one launch per phase (kernels.cuh), replayed from
+//          a CUDA graph.
+// Facade : alien_b200_simulation = an arena of one world, the counterpart of
+//          _SimulationCudaFacade (source/EngineGpuKernels/SimulationCudaFacade.cuh:27-139).
+// Batch  : alien_b200_batch = an arena of many worlds stepped together.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/alien_b200.h"
+#include "../../include/alien_b200_batch.h"
+#include "device_common.cuh"
+#include "io_kernels.cuh"
+#include "kernels.cuh"
+
+namespace ab {
+
+thread_local std::string g_lastError;
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define AB_CK(x)                                                                                           \
+    do {                                                                                                   \
+        cudaError_t e_ = (x);                                                                              \
+        if (e_ != cudaSuccess) {                                                                           \
+            throw Error(e_ == cudaErrorMemoryAllocation ? ALIEN_B200_ERR_OUT_OF_MEMORY : ALIEN_B200_ERR_CUDA, \
+                        std::string(#x) + ": " + cudaGetErrorString(e_));                                  \
+        }                                                                                                  \
+    } while (0)
+
+static inline long long roundUp(long long v, long long m) { return (v + m - 1) / m * m; }
+static inline int divUp(long long v, long long m) { return static_cast<int>((v + m - 1) / m); }
+
+class DeviceMemory {
+public:
+    ~DeviceMemory() { freeAll(); }
+    template <class T>
+    T* alloc(size_t n)
+    {
+        void* p = nullptr;
+        size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(ALIEN_B200_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+        }
+        ptrs_.push_back(p);
+        bytes_ += bytes;
+        return static_cast<T*>(p);
+    }
+    void freeAll()
+    {
+        for (void* p : ptrs_) cudaFree(p);
+        ptrs_.clear();
+        bytes_ = 0;
+    }
+    size_t bytes() const { return bytes_; }
+
+private:
+    std::vector<void*> ptrs_;
+    size_t bytes_ = 0;
+};
+
+// parameters the physics stage cannot honour are rejected, not ignored
+static void validateParams(const AlienPhysicsParams& p, int W, int H)
+{
+    if (p.numZones != 0) throw Error(ALIEN_B200_ERR_UNSUPPORTED, "zones (numZones > 0) are outside the physics stage");
+    if (p.numRadiationSources != 0) throw Error(ALIEN_B200_ERR_UNSUPPORTED, "radiation sources are not supported");
+    if (p.particleTransformationAllowed)
+        throw Error(ALIEN_B200_ERR_UNSUPPORTED, "particle-to-cell transformation is outside the physics stage");
+    if (p.cellAgeLimiter || p.cellColorTransitionRules || p.advancedAbsorptionControl || p.externalEnergyControl)
+        throw Error(ALIEN_B200_ERR_UNSUPPORTED, "feature flags of cell functions / energy control must be off");
+    if (p.rigidity != 0.0f) throw Error(ALIEN_B200_ERR_UNSUPPORTED, "rigidity clusters (rigidity != 0) are not supported");
+    if (p.motionType != ALIEN_B200_MOTION_FLUID && p.motionType != ALIEN_B200_MOTION_COLLISION)
+        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "motionType must be 0 (fluid) or 1 (collision)");
+    if (!(p.smoothingLength > 0.0f) || !(p.cellMaxCollisionDistance > 0.0f))
+        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "interaction radii must be positive");
+    const int r = p.motionType == ALIEN_B200_MOTION_FLUID ? static_cast<int>(ceilf(p.smoothingLength * 2.0f))
+                                                          : static_cast<int>(ceilf(p.cellMaxCollisionDistance));
+    if (r > kMaxRadius) throw Error(ALIEN_B200_ERR_UNSUPPORTED, "interaction radius above 15 slots");
+    if (W < 2 * r + 1 || H < 2 * r + 1) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "world smaller than the interaction window");
+}
+
+static int scanRadius(const AlienPhysicsParams& p)
+{
+    return std::max(1, p.motionType == ALIEN_B200_MOTION_FLUID ? static_cast<int>(ceilf(p.smoothingLength * 2.0f))
+                                                               : static_cast<int>(ceilf(p.cellMaxCollisionDistance)));
+}
+
+struct WorldSetup {
+    int W = 0, H = 0;
+    AlienPhysicsParams params{};
+    uint64_t timestep = 0;
+    const AlienCellTO* cells = nullptr;
+    uint64_t numCells = 0;
+    const AlienParticleTO* particles = nullptr;
+    uint64_t numParticles = 0;
+    const uint8_t* aux = nullptr;
+    uint64_t numAux = 0;
+    uint64_t extraParticles = 0;  // capacity beyond the default
+};
+
+struct HostWorld {
+    WorldInfo info;
+    AlienPhysicsParams params;
+    std::vector<uint8_t> aux;  // opaque auxiliary bytes, returned unchanged
+};
+
+class Arena {
+public:
+    explicit Arena(cudaStream_t stream) : stream_(stream) {}
+    ~Arena() { releaseGraph(); }
+
+    void build(const std::vector<WorldSetup>& setups);
+    void enqueueStep();
+    void enqueueSteps(uint64_t n);
+    void calcTimesteps(uint64_t n);
+    void sync();
+    void setParams(int w, const AlienPhysicsParams& p);
+    std::vector<WorldCounters> readCounters();
+    void getData(int w, bool useRect, AlienInt2 ul, AlienInt2 lr, const AlienDataTO* out);
+    void countData(int w, uint64_t* cells, uint64_t* particles);
+    AlienRawStatistics statistics(int w);
+    void setTimestep(int w, uint64_t t);
+    void compactParticles(int w);
+    void ensureParticleCapacity();
+
+    int numWorlds() const { return static_cast<int>(worlds_.size()); }
+    const HostWorld& world(int w) const { return worlds_[w]; }
+    uint64_t launches() const { return launches_; }
+    size_t deviceBytes() const { return mem_.bytes(); }
+    int kernelsPerStep() const { return kernelsPerStep_; }
+    cudaStream_t stream() const { return stream_; }
+
+private:
+    template <class K, class... A>
+    void launch(K kernel, int grid, int block, A... args)
+    {
+        if (grid <= 0) return;
+        kernel<<<grid, block, 0, stream_>>>(args...);
+        ++launches_;
+        AB_CK(cudaGetLastError());
+    }
+    void scan(const uint32_t* in, long long n, uint32_t* out);
+    void releaseGraph()
+    {
+        if (graphExec_) cudaGraphExecDestroy(graphExec_);
+        graphExec_ = nullptr;
+    }
+    void rebuildFromHost(const std::vector<std::vector<AlienCellTO>>& cells, const std::vector<std::vector<AlienParticleTO>>& parts,
+                         const std::vector<uint64_t>& extra);
+
+    cudaStream_t stream_;
+    DeviceMemory mem_;
+    std::vector<HostWorld> worlds_;
+    DevState s_{};
+    StatsAcc* stats_ = nullptr;
+    AlienCellTO* cold_ = nullptr;
+    int* rankCells_ = nullptr;
+    int* rankParts_ = nullptr;
+    uint32_t* blockCount_ = nullptr;
+    AlienCellTO* egressCells_ = nullptr;
+    AlienParticleTO* egressParts_ = nullptr;
+    long long maxWorldCells_ = 0, maxWorldParts_ = 0;
+    uint64_t launches_ = 0;
+    int kernelsPerStep_ = 0;
+    cudaGraphExec_t graphExec_ = nullptr;
+    uint64_t stepsSinceCheck_ = 0;
+};
+
+// ------------------------------------------------------------- build -----
+void Arena::build(const std::vector<WorldSetup>& setups)
+{
+    releaseGraph();
+    AB_CK(cudaStreamSynchronize(stream_));
+    mem_.freeAll();
+    worlds_.clear();
+    const int n = static_cast<int>(setups.size());
+    long long cellSlots = 0, partSlots = 0, tiles = 0, pmapSlots = 0, coldTotal = 0;
+    int cellBlocks = 0, partBlocks = 0;
+    maxWorldCells_ = maxWorldParts_ = 0;
+    for (int w = 0; w < n; ++w) {
+        const WorldSetup& ws = setups[w];
+        if (ws.W <= 0 || ws.H <= 0) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "world size must be positive");
+        validateParams(ws.params, ws.W, ws.H);
+        if (ws.numCells > (1ull << 30) || ws.numParticles > (1ull << 30))
+            throw Error(ALIEN_B200_ERR_CAPACITY, "more than 2^30 objects in one world");
+        HostWorld hw;
+        hw.params = ws.params;
+        WorldInfo& wi = hw.info;
+        wi.W = ws.W;
+        wi.H = ws.H;
+        wi.radiusInt = scanRadius(ws.params);
+        wi.T = wi.radiusInt;
+        wi.nTX = divUp(ws.W, wi.T);
+        wi.nTY = divUp(ws.H, wi.T);
+        wi.motionType = ws.params.motionType;
+        wi.paramIndex = w;
+        wi.tileBase = tiles;
+        tiles += static_cast<long long>(wi.nTX) * wi.nTY;
+        wi.cellCap = roundUp(std::max<long long>(static_cast<long long>(ws.numCells), 1), kBlock);
+        const long long np = static_cast<long long>(ws.numParticles), nc = static_cast<long long>(ws.numCells);
+        wi.partCap = roundUp(np + nc + std::max<long long>(4096, (np + nc) / 2) + static_cast<long long>(ws.extraParticles), kBlock);
+        wi.cellBase = cellSlots;
+        wi.partBase = partSlots;
+        wi.firstCellBlock = cellBlocks;
+        wi.numCellBlocks = static_cast<int>(wi.cellCap / kBlock);
+        wi.firstPartBlock = partBlocks;
+        wi.numPartBlocks = static_cast<int>(wi.partCap / kBlock);
+        wi.pmapBase = pmapSlots;
+        pmapSlots += static_cast<long long>(ws.W) * ws.H;
+        cellSlots += wi.cellCap;
+        partSlots += wi.partCap;
+        cellBlocks += wi.numCellBlocks;
+        partBlocks += wi.numPartBlocks;
+        coldTotal += nc;
+        maxWorldCells_ = std::max(maxWorldCells_, wi.cellCap);
+        maxWorldParts_ = std::max(maxWorldParts_, wi.partCap);
+        if (ws.numAux) hw.aux.assign(ws.aux, ws.aux + ws.numAux);
+        worlds_.push_back(std::move(hw));
+    }
+    if (cellSlots >= (1ll << 31) || partSlots >= (1ll << 31) || tiles >= (1ll << 32) - 2)
+        throw Error(ALIEN_B200_ERR_CAPACITY, "arena exceeds 2^31 slots");
+
+    DevState& s = s_;
+    s = DevState{};
+    s.numWorlds = n;
+    s.numCellBlocks = cellBlocks;
+    s.numPartBlocks = partBlocks;
+    s.cellSlots = cellSlots;
+    s.partSlots = partSlots;
+    s.numTiles = tiles;
+    const size_t C = static_cast<size_t>(cellSlots), P = static_cast<size_t>(partSlots);
+
+    auto* worldsDev = mem_.alloc<WorldInfo>(n);
+    s.worlds = worldsDev;
+    s.counters = mem_.alloc<WorldCounters>(n);
+    auto* paramsDev = mem_.alloc<AlienPhysicsParams>(n);
+    s.params = paramsDev;
+    auto* cbw = mem_.alloc<int>(cellBlocks);
+    auto* pbw = mem_.alloc<int>(partBlocks);
+    s.cellBlockWorld = cbw;
+    s.partBlockWorld = pbw;
+    s.errorFlags = mem_.alloc<uint32_t>(1);
+
+    s.id = mem_.alloc<unsigned long long>(C);
+    s.posA = mem_.alloc<float2>(C);
+    s.posB = mem_.alloc<float2>(C);
+    s.velA = mem_.alloc<float2>(C);
+    s.velB = mem_.alloc<float2>(C);
+    s.energy = mem_.alloc<float>(C);
+    s.stiffness = mem_.alloc<float>(C);
+    s.density = mem_.alloc<float>(C);
+    s.densNew = mem_.alloc<float>(C);
+    s.color = mem_.alloc<uint8_t>(C);
+    s.maxConn = mem_.alloc<uint8_t>(C);
+    s.numConn = mem_.alloc<uint8_t>(C);
+    s.barrier = mem_.alloc<uint8_t>(C);
+    s.alive = mem_.alloc<uint8_t>(C);
+    s.livingState = mem_.alloc<uint8_t>(C);
+    s.nextState = mem_.alloc<uint8_t>(C);
+    s.flags = mem_.alloc<uint32_t>(C);
+    s.age = mem_.alloc<uint32_t>(C);
+    s.activationTime = mem_.alloc<uint32_t>(C);
+    s.creatureId = mem_.alloc<uint32_t>(C);
+    s.coldIdx = mem_.alloc<uint32_t>(C);
+    s.bond = mem_.alloc<int>(C * kMaxBonds);
+    s.bondDist = mem_.alloc<float>(C * kMaxBonds);
+    s.bondAngle = mem_.alloc<float>(C * kMaxBonds);
+    s.force = mem_.alloc<float2>(C);
+    s.force1 = mem_.alloc<float2>(C);
+    s.angleAcc = mem_.alloc<long long>(C * 4);
+    s.energyAcc = mem_.alloc<long long>(C);
+    s.best = mem_.alloc<int>(C);
+    s.newPartner = mem_.alloc<int>(C);
+    s.addNum = mem_.alloc<uint8_t>(C);
+    s.addBond = mem_.alloc<int>(C * kMaxBonds);
+    s.addDist = mem_.alloc<float>(C * kMaxBonds);
+    s.addAngle = mem_.alloc<float>(C * kMaxBonds);
+    s.radPos = mem_.alloc<float2>(C);
+    s.radVel = mem_.alloc<float2>(C);
+    s.radEnergy = mem_.alloc<float>(C);
+    s.tileOf = mem_.alloc<uint32_t>(C);
+    s.tileOff = mem_.alloc<uint32_t>(C);
+    s.sorted = mem_.alloc<uint32_t>(C);
+    s.stagedPV = mem_.alloc<float4>(C);
+    s.stagedMeta = mem_.alloc<int4>(C);
+    s.tileCount = mem_.alloc<uint32_t>(static_cast<size_t>(tiles));
+    s.tileStart = mem_.alloc<uint32_t>(static_cast<size_t>(tiles) + 1);
+    s.scanPartials = mem_.alloc<uint32_t>(static_cast<size_t>(divUp(tiles, kScanTile)) + 2);
+
+    s.pid = mem_.alloc<unsigned long long>(P);
+    s.ppos = mem_.alloc<float2>(P);
+    s.pvel = mem_.alloc<float2>(P);
+    s.penergy = mem_.alloc<float>(P);
+    s.pcolor = mem_.alloc<uint8_t>(P);
+    s.palive = mem_.alloc<uint8_t>(P);
+    s.pselected = mem_.alloc<uint8_t>(P);
+    s.pflag = mem_.alloc<uint32_t>(P);
+    s.plast = mem_.alloc<unsigned long long>(P);
+    s.ptarget = mem_.alloc<int>(P);
+    s.pslot = mem_.alloc<int>(P);
+    s.pmerge = mem_.alloc<long long>(P * 3);
+    s.splitPos = mem_.alloc<float2>(P);
+    s.splitVel = mem_.alloc<float2>(P);
+    s.splitEnergy = mem_.alloc<float>(P);
+    s.pmap = mem_.alloc<int>(static_cast<size_t>(pmapSlots));
+    s.blockRad = mem_.alloc<uint32_t>(cellBlocks);
+    s.blockDel = mem_.alloc<uint32_t>(cellBlocks);
+    s.blockSplit = mem_.alloc<uint32_t>(partBlocks);
+
+    stats_ = mem_.alloc<StatsAcc>(n);
+    cold_ = mem_.alloc<AlienCellTO>(static_cast<size_t>(coldTotal));
+    rankCells_ = mem_.alloc<int>(C);
+    rankParts_ = mem_.alloc<int>(P);
+    blockCount_ = mem_.alloc<uint32_t>(static_cast<size_t>(std::max(cellBlocks, partBlocks)) + 2);
+    egressCells_ = nullptr;
+    egressParts_ = nullptr;
+
+    // host-side tables
+    std::vector<WorldInfo> infos(n);
+    std::vector<AlienPhysicsParams> params(n);
+    std::vector<int> cbwHost(cellBlocks), pbwHost(partBlocks);
+    std::vector<WorldCounters> counters(n);
+    for (int w = 0; w < n; ++w) {
+        infos[w] = worlds_[w].info;
+        params[w] = worlds_[w].params;
+        for (int b = 0; b < infos[w].numCellBlocks; ++b) cbwHost[infos[w].firstCellBlock + b] = w;
+        for (int b = 0; b < infos[w].numPartBlocks; ++b) pbwHost[infos[w].firstPartBlock + b] = w;
+        WorldCounters& wc = counters[w];
+        std::memset(&wc, 0, sizeof(wc));
+        wc.timestep = setups[w].timestep;
+        wc.nextId = 1;
+        wc.numCells = static_cast<unsigned int>(setups[w].numCells);
+        wc.numParticles = static_cast<unsigned int>(setups[w].numParticles);
+    }
+    AB_CK(cudaMemcpyAsync(worldsDev, infos.data(), sizeof(WorldInfo) * n, cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemcpyAsync(paramsDev, params.data(), sizeof(AlienPhysicsParams) * n, cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemcpyAsync(s.counters, counters.data(), sizeof(WorldCounters) * n, cudaMemcpyHostToDevice, stream_));
+    if (cellBlocks) AB_CK(cudaMemcpyAsync(cbw, cbwHost.data(), sizeof(int) * cellBlocks, cudaMemcpyHostToDevice, stream_));
+    if (partBlocks) AB_CK(cudaMemcpyAsync(pbw, pbwHost.data(), sizeof(int) * partBlocks, cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemsetAsync(s.errorFlags, 0, sizeof(uint32_t), stream_));
+    AB_CK(cudaMemsetAsync(s.alive, 0, C, stream_));
+    AB_CK(cudaMemsetAsync(s.palive, 0, P, stream_));
+    AB_CK(cudaMemsetAsync(s.pflag, 0, P * sizeof(uint32_t), stream_));
+    AB_CK(cudaMemsetAsync(s.pmap, 0xff, static_cast<size_t>(pmapSlots) * sizeof(int), stream_));
+    AB_CK(cudaMemsetAsync(s.flags, 0, C * sizeof(uint32_t), stream_));
+
+    // ingest: host TOs -> device staging -> SoA (cudaCreateDataFromTO)
+    long long coldBase = 0;
+    for (int w = 0; w < n; ++w) {
+        const WorldSetup& ws = setups[w];
+        const long long nc = static_cast<long long>(ws.numCells), np = static_cast<long long>(ws.numParticles);
+        AlienCellTO* dCells = nullptr;
+        AlienParticleTO* dParts = nullptr;
+        if (nc) {
+            AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&dCells), sizeof(AlienCellTO) * nc, stream_));
+            AB_CK(cudaMemcpyAsync(dCells, ws.cells, sizeof(AlienCellTO) * nc, cudaMemcpyHostToDevice, stream_));
+        }
+        if (np) {
+            AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&dParts), sizeof(AlienParticleTO) * np, stream_));
+            AB_CK(cudaMemcpyAsync(dParts, ws.particles, sizeof(AlienParticleTO) * np, cudaMemcpyHostToDevice, stream_));
+        }
+        launch(kIngestCells, divUp(nc, kBlock), kBlock, s, w, static_cast<const AlienCellTO*>(dCells), nc, cold_, coldBase);
+        launch(kIngestParticles, divUp(np, kBlock), kBlock, s, w, static_cast<const AlienParticleTO*>(dParts), np);
+        launch(kMaxId, divUp(std::max(nc, np), kBlock), kBlock, s, w, static_cast<const AlienCellTO*>(dCells), nc,
+               static_cast<const AlienParticleTO*>(dParts), np);
+        if (dCells) AB_CK(cudaFreeAsync(dCells, stream_));
+        if (dParts) AB_CK(cudaFreeAsync(dParts, stream_));
+        coldBase += nc;
+    }
+    sync();
+}
+
+// -------------------------------------------------------------- scan -----
+void Arena::scan(const uint32_t* in, long long n, uint32_t* out)
+{
+    const int blocks = divUp(n, kScanTile);
+    launch(kScanReduce, blocks, kBlock, in, n, s_.scanPartials);
+    launch(kScanPartials, 1, kBlock, s_.scanPartials, blocks);
+    launch(kScanDown, blocks, kBlock, in, n, static_cast<const uint32_t*>(s_.scanPartials), out);
+}
+
+// -------------------------------------------------------------- step -----
+// the launch sequence of one timestep for every world of the arena
+void Arena::enqueueStep()
+{
+    const DevState& s = s_;
+    const int cells = s.numCellBlocks, both = s.numCellBlocks + s.numPartBlocks;
+    const uint64_t before = launches_;
+    AB_CK(cudaMemsetAsync(s.tileCount, 0, sizeof(uint32_t) * static_cast<size_t>(s.numTiles), stream_));
+    launch(kBin, both, kBlock, s);
+    scan(s.tileCount, s.numTiles, s.tileStart);
+    launch(kScatter, cells, kBlock, s);
+    launch(kStage, cells, kBlock, s);
+    launch(kPairs, cells, kBlock, s);
+    launch(kApplyBond1, both, kBlock, s);
+    launch(kVerletPos, both, kBlock, s);
+    launch(kBond2, both, kBlock, s);
+    launch(kVerletVel, both, kBlock, s);
+    launch(kTransition, both, kBlock, s);
+    launch(kDecay, cells, kBlock, s);
+    launch(kResolve, cells, kBlock, s);
+    launch(kCommit, cells, kBlock, s);
+    launch(kEventCount, both, kBlock, s);
+    launch(kEventWorld, divUp(static_cast<long long>(s.numWorlds) * 32, kBlock), kBlock, s);
+    launch(kEventEmit, both, kBlock, s);
+    kernelsPerStep_ = static_cast<int>(launches_ - before);
+}
+
+void Arena::enqueueSteps(uint64_t n)
+{
+    if (n == 0) return;
+    if (!graphExec_) {
+        cudaGraph_t graph;
+        AB_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        const uint64_t before = launches_;
+        try {
+            enqueueStep();
+        } catch (...) {
+            cudaStreamEndCapture(stream_, &graph);
+            throw;
+        }
+        launches_ = before;  // captured, not launched
+        AB_CK(cudaStreamEndCapture(stream_, &graph));
+        cudaError_t e = cudaGraphInstantiate(&graphExec_, graph, 0);
+        cudaGraphDestroy(graph);
+        AB_CK(e);
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+        AB_CK(cudaGraphLaunch(graphExec_, stream_));
+        launches_ += kernelsPerStep_;
+    }
+}
+
+void Arena::sync()
+{
+    AB_CK(cudaStreamSynchronize(stream_));
+    uint32_t flags = 0;
+    AB_CK(cudaMemcpy(&flags, s_.errorFlags, sizeof(flags), cudaMemcpyDeviceToHost));
+    if (flags & 1u) {
+        AB_CK(cudaMemset(s_.errorFlags, 0, sizeof(uint32_t)));
+        throw Error(ALIEN_B200_ERR_CAPACITY, "particle capacity exceeded: energy particles were dropped");
+    }
+}
+
+std::vector<WorldCounters> Arena::readCounters()
+{
+    std::vector<WorldCounters> c(worlds_.size());
+    AB_CK(cudaMemcpyAsync(c.data(), s_.counters, sizeof(WorldCounters) * c.size(), cudaMemcpyDeviceToHost, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+    return c;
+}
+
+// keep at least half of each world's particle slots free: compact when the
+// used slots pass 50 %, grow (rebuild) when live particles pass 50 %
+void Arena::ensureParticleCapacity()
+{
+    std::vector<WorldCounters> c = readCounters();
+    std::vector<int> grow;
+    for (int w = 0; w < numWorlds(); ++w) {
+        const long long cap = worlds_[w].info.partCap;
+        if (c[w].numParticles * 2ll <= cap) continue;
+        compactParticles(w);
+        uint64_t live = 0, dummy = 0;
+        countData(w, &dummy, &live);
+        if (static_cast<long long>(live) * 2 > cap) grow.push_back(w);
+    }
+    if (grow.empty()) return;
+    // resize (the counterpart of _SimulationCudaFacade::resizeArrays,
+    // SimulationCudaFacade.cu:619-655): export, rebuild larger, re-import
+    std::vector<std::vector<AlienCellTO>> cells(numWorlds());
+    std::vector<std::vector<AlienParticleTO>> parts(numWorlds());
+    std::vector<uint64_t> extra(numWorlds(), 0);
+    for (int w = 0; w < numWorlds(); ++w) {
+        uint64_t nc = 0, np = 0, na = worlds_[w].aux.size();
+        countData(w, &nc, &np);
+        cells[w].resize(nc);
+        parts[w].resize(np);
+        std::vector<uint8_t> auxTmp(std::max<uint64_t>(na, 1));
+        AlienDataTO to{&nc, cells[w].data(), &np, parts[w].data(), &na, auxTmp.data()};
+        getData(w, false, AlienInt2{0, 0}, AlienInt2{0, 0}, &to);
+        extra[w] = std::find(grow.begin(), grow.end(), w) != grow.end() ? 2 * worlds_[w].info.partCap : 0;
+    }
+    rebuildFromHost(cells, parts, extra);
+}
+
+void Arena::rebuildFromHost(const std::vector<std::vector<AlienCellTO>>& cells, const std::vector<std::vector<AlienParticleTO>>& parts,
+                            const std::vector<uint64_t>& extra)
+{
+    std::vector<WorldCounters> c = readCounters();
+    std::vector<HostWorld> old = worlds_;
+    std::vector<WorldSetup> setups(old.size());
+    for (size_t w = 0; w < old.size(); ++w) {
+        WorldSetup& ws = setups[w];
+        ws.W = old[w].info.W;
+        ws.H = old[w].info.H;
+        ws.params = old[w].params;
+        ws.timestep = c[w].timestep;
+        ws.cells = cells[w].data();
+        ws.numCells = cells[w].size();
+        ws.particles = parts[w].data();
+        ws.numParticles = parts[w].size();
+        ws.aux = old[w].aux.data();
+        ws.numAux = old[w].aux.size();
+        ws.extraParticles = extra[w];
+    }
+    build(setups);
+    // ids continue where they were, not at max(id)+1 of the surviving objects
+    std::vector<WorldCounters> now = readCounters();
+    for (size_t w = 0; w < old.size(); ++w) now[w].nextId = std::max(now[w].nextId, c[w].nextId);
+    AB_CK(cudaMemcpy(s_.counters, now.data(), sizeof(WorldCounters) * now.size(), cudaMemcpyHostToDevice));
+}
+
+void Arena::calcTimesteps(uint64_t n)
+{
+    const uint64_t chunk = 64;
+    while (n > 0) {
+        const uint64_t k = std::min(n, chunk);
+        enqueueSteps(k);
+        n -= k;
+        stepsSinceCheck_ += k;
+        if (stepsSinceCheck_ >= chunk || n == 0) {
+            sync();
+            ensureParticleCapacity();
+            stepsSinceCheck_ = 0;
+        }
+    }
+    sync();
+}
+
+void Arena::setParams(int w, const AlienPhysicsParams& p)
+{
+    HostWorld& hw = worlds_[w];
+    validateParams(p, hw.info.W, hw.info.H);
+    const bool relayout = scanRadius(p) != hw.info.radiusInt || p.motionType != hw.info.motionType;
+    if (relayout) {
+        // the tile grid depends on the interaction radius: rebuild the arena
+        std::vector<std::vector<AlienCellTO>> cells(numWorlds());
+        std::vector<std::vector<AlienParticleTO>> parts(numWorlds());
+        for (int v = 0; v < numWorlds(); ++v) {
+            uint64_t nc = 0, np = 0, na = worlds_[v].aux.size();
+            countData(v, &nc, &np);
+            cells[v].resize(nc);
+            parts[v].resize(np);
+            std::vector<uint8_t> auxTmp(std::max<uint64_t>(na, 1));
+            AlienDataTO to{&nc, cells[v].data(), &np, parts[v].data(), &na, auxTmp.data()};
+            getData(v, false, AlienInt2{0, 0}, AlienInt2{0, 0}, &to);
+        }
+        hw.params = p;
+        rebuildFromHost(cells, parts, std::vector<uint64_t>(numWorlds(), 0));
+        return;
+    }
+    hw.params = p;
+    AB_CK(cudaMemcpyAsync(const_cast<AlienPhysicsParams*>(s_.params) + w, &p, sizeof(p), cudaMemcpyHostToDevice, stream_));
+    // prepareForSimulationParametersChanges -> cudaResetDensity (SimulationKernelsLauncher.cu:93-97)
+    launch(kResetDensity, hw.info.numCellBlocks, kBlock, s_, w);
+    sync();
+}
+
+void Arena::setTimestep(int w, uint64_t t)
+{
+    std::vector<WorldCounters> c = readCounters();
+    c[w].timestep = t;
+    AB_CK(cudaMemcpy(s_.counters, c.data(), sizeof(WorldCounters) * c.size(), cudaMemcpyHostToDevice));
+}
+
+// ----------------------------------------------------------- egress ------
+void Arena::countData(int w, uint64_t* cells, uint64_t* particles)
+{
+    const WorldInfo& wi = worlds_[w].info;
+    launch(kSelectCells, wi.numCellBlocks, kBlock, s_, w, 0, 0, 0, 0, 0, rankCells_, blockCount_);
+    launch(kScanPartials, 1, kBlock, blockCount_, wi.numCellBlocks);
+    uint32_t nc = 0, np = 0;
+    AB_CK(cudaMemcpyAsync(&nc, blockCount_ + wi.numCellBlocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+    launch(kSelectParticles, wi.numPartBlocks, kBlock, s_, w, 0, 0, 0, 0, 0, rankParts_, blockCount_);
+    launch(kScanPartials, 1, kBlock, blockCount_, wi.numPartBlocks);
+    AB_CK(cudaMemcpyAsync(&np, blockCount_ + wi.numPartBlocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+    *cells = nc;
+    *particles = np;
+}
+
+void Arena::getData(int w, bool useRect, AlienInt2 ul, AlienInt2 lr, const AlienDataTO* out)
+{
+    if (!out || !out->numCells || !out->numParticles || !out->numAuxiliaryData)
+        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "DataTO counters must not be null");
+    const WorldInfo& wi = worlds_[w].info;
+    if (!egressCells_) egressCells_ = mem_.alloc<AlienCellTO>(static_cast<size_t>(maxWorldCells_));
+    if (!egressParts_) egressParts_ = mem_.alloc<AlienParticleTO>(static_cast<size_t>(maxWorldParts_));
+    const int u = useRect ? 1 : 0;
+    uint32_t nc = 0, np = 0;
+    launch(kSelectCells, wi.numCellBlocks, kBlock, s_, w, u, ul.x, ul.y, lr.x, lr.y, rankCells_, blockCount_);
+    launch(kScanPartials, 1, kBlock, blockCount_, wi.numCellBlocks);
+    launch(kFinishRanks, wi.numCellBlocks, kBlock, wi.cellBase, rankCells_, static_cast<const uint32_t*>(blockCount_));
+    AB_CK(cudaMemcpyAsync(&nc, blockCount_ + wi.numCellBlocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    launch(kEgressCells, wi.numCellBlocks, kBlock, s_, w, static_cast<const int*>(rankCells_), static_cast<const AlienCellTO*>(cold_),
+           egressCells_);
+    AB_CK(cudaStreamSynchronize(stream_));
+    launch(kSelectParticles, wi.numPartBlocks, kBlock, s_, w, u, ul.x, ul.y, lr.x, lr.y, rankParts_, blockCount_);
+    launch(kScanPartials, 1, kBlock, blockCount_, wi.numPartBlocks);
+    launch(kFinishRanks, wi.numPartBlocks, kBlock, wi.partBase, rankParts_, static_cast<const uint32_t*>(blockCount_));
+    AB_CK(cudaMemcpyAsync(&np, blockCount_ + wi.numPartBlocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    launch(kEgressParticles, wi.numPartBlocks, kBlock, s_, w, static_cast<const int*>(rankParts_), egressParts_);
+    AB_CK(cudaStreamSynchronize(stream_));
+    if (nc && !out->cells) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "DataTO.cells is null");
+    if (np && !out->particles) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "DataTO.particles is null");
+    if (nc) AB_CK(cudaMemcpyAsync(out->cells, egressCells_, sizeof(AlienCellTO) * nc, cudaMemcpyDeviceToHost, stream_));
+    if (np) AB_CK(cudaMemcpyAsync(out->particles, egressParts_, sizeof(AlienParticleTO) * np, cudaMemcpyDeviceToHost, stream_));
+    const std::vector<uint8_t>& aux = worlds_[w].aux;
+    if (!aux.empty()) {
+        if (!out->auxiliaryData) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "DataTO.auxiliaryData is null");
+        std::memcpy(out->auxiliaryData, aux.data(), aux.size());
+    }
+    AB_CK(cudaStreamSynchronize(stream_));
+    *out->numCells = nc;
+    *out->numParticles = np;
+    *out->numAuxiliaryData = aux.size();
+}
+
+void Arena::compactParticles(int w)
+{
+    const WorldInfo& wi = worlds_[w].info;
+    launch(kSelectParticles, wi.numPartBlocks, kBlock, s_, w, 0, 0, 0, 0, 0, rankParts_, blockCount_);
+    launch(kScanPartials, 1, kBlock, blockCount_, wi.numPartBlocks);
+    launch(kFinishRanks, wi.numPartBlocks, kBlock, wi.partBase, rankParts_, static_cast<const uint32_t*>(blockCount_));
+    uint32_t live = 0;
+    AB_CK(cudaMemcpyAsync(&live, blockCount_ + wi.numPartBlocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+    const size_t cap = static_cast<size_t>(wi.partCap);
+    unsigned long long *tid, *tlast;
+    float2 *tpos, *tvel;
+    float* te;
+    uint8_t *tc, *tsel;
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&tid), cap * 8, stream_));
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&tlast), cap * 8, stream_));
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&tpos), cap * 8, stream_));
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&tvel), cap * 8, stream_));
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&te), cap * 4, stream_));
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&tc), cap, stream_));
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&tsel), cap, stream_));
+    launch(kCompactParticlesGather, wi.numPartBlocks, kBlock, s_, w, static_cast<const int*>(rankParts_), tid, tpos, tvel, te, tc, tsel,
+           tlast);
+    launch(kCompactParticlesScatter, wi.numPartBlocks, kBlock, s_, w, static_cast<long long>(live),
+           static_cast<const unsigned long long*>(tid), static_cast<const float2*>(tpos), static_cast<const float2*>(tvel),
+           static_cast<const float*>(te), static_cast<const uint8_t*>(tc), static_cast<const uint8_t*>(tsel),
+           static_cast<const unsigned long long*>(tlast));
+    for (void* p : {static_cast<void*>(tid), static_cast<void*>(tlast), static_cast<void*>(tpos), static_cast<void*>(tvel),
+                    static_cast<void*>(te), static_cast<void*>(tc), static_cast<void*>(tsel)})
+        AB_CK(cudaFreeAsync(p, stream_));
+    std::vector<WorldCounters> c = readCounters();
+    c[w].numParticles = live;
+    c[w].deadParticles = 0;
+    AB_CK(cudaMemcpyAsync(s_.counters + w, &c[w], sizeof(WorldCounters), cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+}
+
+AlienRawStatistics Arena::statistics(int w)
+{
+    AB_CK(cudaMemsetAsync(stats_, 0, sizeof(StatsAcc) * worlds_.size(), stream_));
+    launch(kStatsCells, s_.numCellBlocks, kBlock, s_, stats_);
+    launch(kStatsParticles, s_.numPartBlocks, kBlock, s_, stats_);
+    StatsAcc a;
+    AB_CK(cudaMemcpyAsync(&a, stats_ + w, sizeof(a), cudaMemcpyDeviceToHost, stream_));
+    WorldCounters c;
+    AB_CK(cudaMemcpyAsync(&c, s_.counters + w, sizeof(c), cudaMemcpyDeviceToHost, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+    AlienRawStatistics r;
+    std::memset(&r, 0, sizeof(r));
+    r.timestep = c.timestep;
+    r.numCells = a.numCells;
+    r.numParticles = a.numParticles;
+    r.numConnections = a.numConnections;
+    for (int i = 0; i < ALIEN_B200_MAX_COLORS; ++i) r.numCellsByColor[i] = a.numCellsByColor[i];
+    r.totalCellEnergy = static_cast<double>(a.cellEnergyFix) / 65536.0;
+    r.totalParticleEnergy = static_cast<double>(a.particleEnergyFix) / 65536.0;
+    return r;
+}
+
+template <class F>
+static int guarded(F&& f)
+{
+    try {
+        f();
+        return ALIEN_B200_OK;
+    } catch (const Error& e) {
+        g_lastError = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_lastError = "host allocation failed";
+        return ALIEN_B200_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        g_lastError = e.what();
+        return ALIEN_B200_ERR_CUDA;
+    }
+}
+
+static void ensureDevice()
+{
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        throw Error(ALIEN_B200_ERR_NO_DEVICE, "no CUDA device available");
+    }
+}
+
+static void checkDataTO(const AlienDataTO* d)
+{
+    if (!d || !d->numCells || !d->numParticles || !d->numAuxiliaryData)
+        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "DataTO counters must not be null");
+    if (*d->numCells && !d->cells) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "DataTO.cells is null");
+    if (*d->numParticles && !d->particles) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "DataTO.particles is null");
+    if (*d->numAuxiliaryData && !d->auxiliaryData) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "DataTO.auxiliaryData is null");
+    for (uint64_t i = 0; i < *d->numCells; ++i) {
+        const AlienCellTO& c = d->cells[i];
+        if (c.numConnections > ALIEN_B200_MAX_CELL_BONDS) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "numConnections above 6");
+        for (int k = 0; k < c.numConnections; ++k)
+            if (c.connections[k].cellIndex < 0 || static_cast<uint64_t>(c.connections[k].cellIndex) >= *d->numCells)
+                throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "connection cellIndex out of range");
+    }
+}
+
+static WorldSetup setupFrom(const AlienGeneralSettings& g, const AlienPhysicsParams& p, uint64_t timestep, const AlienDataTO* d)
+{
+    WorldSetup ws;
+    ws.W = g.worldSizeX;
+    ws.H = g.worldSizeY;
+    ws.params = p;
+    ws.timestep = timestep;
+    if (d) {
+        ws.cells = d->cells;
+        ws.numCells = *d->numCells;
+        ws.particles = d->particles;
+        ws.numParticles = *d->numParticles;
+        ws.aux = d->auxiliaryData;
+        ws.numAux = *d->numAuxiliaryData;
+    }
+    return ws;
+}
+
+}  // namespace ab
+
+using namespace ab;
+
+struct alien_b200_simulation {
+    cudaStream_t stream = nullptr;
+    AlienGeneralSettings general{};
+    AlienPhysicsParams params{};
+    uint64_t extraParticles = 0;
+    std::unique_ptr<Arena> arena;
+};
+
+struct alien_b200_batch {
+    cudaStream_t stream = nullptr;
+    std::unique_ptr<Arena> arena;
+};
+
+extern "C" {
+
+int alien_b200_version(void) { return 1; }
+
+void alien_b200_default_parameters(AlienPhysicsParams* p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->timestepSize = 1.0f;
+    p->motionType = ALIEN_B200_MOTION_FLUID;
+    p->smoothingLength = 0.8f;
+    p->viscosityStrength = 0.1f;
+    p->pressureStrength = 0.1f;
+    p->cellMaxCollisionDistance = 1.3f;
+    p->cellRepulsionStrength = 0.08f;
+    p->innerFriction = 0.3f;
+    p->cellMaxVelocity = 2.0f;
+    p->cellMinDistance = 0.3f;
+    p->cellMaxForceDecayProb = 0.2f;
+    p->radiationProb = 0.03f;
+    p->radiationVelocityMultiplier = 1.0f;
+    p->radiationVelocityPerturbation = 0.5f;
+    p->cellDeathConsequences = ALIEN_B200_DEATH_DETACHED_PARTS_DIE;
+    p->friction = 0.001f;
+    p->rigidity = 0.0f;
+    p->cellFusionVelocity = 0.6f;
+    p->cellMaxBindingEnergy = 3.4028234663852886e38f;
+    for (int i = 0; i < ALIEN_B200_MAX_COLORS; ++i) {
+        p->cellMaxBindingDistance[i] = 3.6f;
+        p->radiationMinCellAge[i] = 0;
+        p->highRadiationFactor[i] = 0.0f;
+        p->highRadiationMinCellEnergy[i] = 500.0f;
+        p->cellMaxAge[i] = 2147483647;
+        p->particleSplitEnergy[i] = 3.4028234663852886e38f;
+        p->radiationAbsorption[i] = 1.0f;
+        p->radiationCellAgeStrength[i] = 0.00002f;
+        p->cellMaxForce[i] = 0.8f;
+        p->cellMinEnergy[i] = 50.0f;
+        p->cellDeathProbability[i] = 0.001f;
+    }
+}
+
+int alien_b200_last_error(char* buffer, size_t size)
+{
+    if (!buffer || size == 0) return static_cast<int>(g_lastError.size());
+    std::snprintf(buffer, size, "%s", g_lastError.c_str());
+    return static_cast<int>(g_lastError.size());
+}
+
+int alien_b200_create(const AlienGeneralSettings* general, const AlienPhysicsParams* params, uint64_t timestep,
+                      alien_b200_simulation** out)
+{
+    return guarded([&] {
+        if (!general || !params || !out) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        ensureDevice();
+        validateParams(*params, general->worldSizeX, general->worldSizeY);
+        auto sim = std::make_unique<alien_b200_simulation>();
+        sim->general = *general;
+        sim->params = *params;
+        AB_CK(cudaStreamCreateWithFlags(&sim->stream, cudaStreamNonBlocking));
+        sim->arena = std::make_unique<Arena>(sim->stream);
+        sim->arena->build({setupFrom(*general, *params, timestep, nullptr)});
+        *out = sim.release();
+    });
+}
+
+int alien_b200_destroy(alien_b200_simulation* sim)
+{
+    return guarded([&] {
+        if (!sim) return;
+        if (sim->stream) cudaStreamSynchronize(sim->stream);
+        sim->arena.reset();
+        if (sim->stream) cudaStreamDestroy(sim->stream);
+        delete sim;
+    });
+}
+
+int alien_b200_calc_timesteps(alien_b200_simulation* sim, uint64_t timesteps)
+{
+    return guarded([&] {
+        if (!sim) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
+        sim->arena->calcTimesteps(timesteps);
+    });
+}
+
+int alien_b200_enqueue_timesteps(alien_b200_simulation* sim, uint64_t timesteps)
+{
+    return guarded([&] {
+        if (!sim) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
+        sim->arena->enqueueSteps(timesteps);
+    });
+}
+
+void* alien_b200_stream(alien_b200_simulation* sim) { return sim ? static_cast<void*>(sim->stream) : nullptr; }
+
+uint64_t alien_b200_kernel_launch_count(alien_b200_simulation* sim) { return sim && sim->arena ? sim->arena->launches() : 0; }
+
+int alien_b200_set_data(alien_b200_simulation* sim, const AlienDataTO* data)
+{
+    return guarded([&] {
+        if (!sim) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
+        checkDataTO(data);
+        const uint64_t t = sim->arena->readCounters()[0].timestep;
+        WorldSetup ws = setupFrom(sim->general, sim->params, t, data);
+        ws.extraParticles = sim->extraParticles;
+        sim->arena->build({ws});
+    });
+}
+
+int alien_b200_get_data(alien_b200_simulation* sim, AlienInt2 upperLeft, AlienInt2 lowerRight, const AlienDataTO* data)
+{
+    return guarded([&] {
+        if (!sim) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
+        sim->arena->getData(0, true, upperLeft, lowerRight, data);
+    });
+}
+
+int alien_b200_set_parameters(alien_b200_simulation* sim, const AlienPhysicsParams* params)
+{
+    return guarded([&] {
+        if (!sim || !params) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        sim->arena->setParams(0, *params);
+        sim->params = *params;
+    });
+}
+
+int alien_b200_get_parameters(alien_b200_simulation* sim, AlienPhysicsParams* params)
+{
+    return guarded([&] {
+        if (!sim || !params) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        *params = sim->params;
+    });
+}
+
+int alien_b200_get_array_sizes(alien_b200_simulation* sim, AlienArraySizes* sizes)
+{
+    return guarded([&] {
+        if (!sim || !sizes) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        const WorldInfo& wi = sim->arena->world(0).info;
+        sizes->cellArraySize = static_cast<uint64_t>(wi.cellCap);
+        sizes->particleArraySize = static_cast<uint64_t>(wi.partCap);
+        sizes->auxiliaryDataSize = sim->arena->world(0).aux.size();
+    });
+}
+
+int alien_b200_resize_arrays_if_necessary(alien_b200_simulation* sim, const AlienArraySizes* additionals)
+{
+    return guarded([&] {
+        if (!sim || !additionals) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        // cells enter only through set_data, which sizes the arrays itself;
+        // particle headroom is kept for the next set_data and applied now
+        sim->extraParticles = std::max<uint64_t>(sim->extraParticles, additionals->particleArraySize);
+        const WorldInfo& wi = sim->arena->world(0).info;
+        uint64_t nc = 0, np = 0;
+        sim->arena->countData(0, &nc, &np);
+        if (np + additionals->particleArraySize + 4096 > static_cast<uint64_t>(wi.partCap) / 2) {
+            std::vector<AlienCellTO> cells(nc);
+            std::vector<AlienParticleTO> parts(np);
+            uint64_t na = sim->arena->world(0).aux.size();
+            std::vector<uint8_t> aux(std::max<uint64_t>(na, 1));
+            AlienDataTO to{&nc, cells.data(), &np, parts.data(), &na, aux.data()};
+            sim->arena->getData(0, false, AlienInt2{0, 0}, AlienInt2{0, 0}, &to);
+            const uint64_t t = sim->arena->readCounters()[0].timestep;
+            WorldSetup ws = setupFrom(sim->general, sim->params, t, &to);
+            ws.extraParticles = sim->extraParticles;
+            sim->arena->build({ws});
+        }
+    });
+}
+
+int alien_b200_get_current_timestep(alien_b200_simulation* sim, uint64_t* timestep)
+{
+    return guarded([&] {
+        if (!sim || !timestep) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        *timestep = sim->arena->readCounters()[0].timestep;
+    });
+}
+
+int alien_b200_set_current_timestep(alien_b200_simulation* sim, uint64_t timestep)
+{
+    return guarded([&] {
+        if (!sim) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
+        sim->arena->setTimestep(0, timestep);
+    });
+}
+
+int alien_b200_clear(alien_b200_simulation* sim)
+{
+    return guarded([&] {
+        if (!sim) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
+        const uint64_t t = sim->arena->readCounters()[0].timestep;
+        sim->arena->build({setupFrom(sim->general, sim->params, t, nullptr)});
+    });
+}
+
+int alien_b200_get_raw_statistics(alien_b200_simulation* sim, AlienRawStatistics* statistics)
+{
+    return guarded([&] {
+        if (!sim || !statistics) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        *statistics = sim->arena->statistics(0);
+    });
+}
+
+// ------------------------------------------------------------- batch -----
+int alien_b200_batch_create(int numWorlds, const AlienGeneralSettings* general, const AlienPhysicsParams* params,
+                            const AlienDataTO* data, uint64_t timestep, alien_b200_batch** out)
+{
+    return guarded([&] {
+        if (numWorlds <= 0 || numWorlds > 65535 || !general || !params || !data || !out)
+            throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid batch arguments");
+        *out = nullptr;
+        ensureDevice();
+        std::vector<WorldSetup> setups;
+        for (int w = 0; w < numWorlds; ++w) {
+            checkDataTO(&data[w]);
+            setups.push_back(setupFrom(general[w], params[w], timestep, &data[w]));
+        }
+        auto b = std::make_unique<alien_b200_batch>();
+        AB_CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        b->arena = std::make_unique<Arena>(b->stream);
+        b->arena->build(setups);
+        *out = b.release();
+    });
+}
+
+int alien_b200_batch_destroy(alien_b200_batch* b)
+{
+    return guarded([&] {
+        if (!b) return;
+        if (b->stream) cudaStreamSynchronize(b->stream);
+        b->arena.reset();
+        if (b->stream) cudaStreamDestroy(b->stream);
+        delete b;
+    });
+}
+
+int alien_b200_batch_num_worlds(alien_b200_batch* b) { return b && b->arena ? b->arena->numWorlds() : 0; }
+
+int alien_b200_batch_calc_timesteps(alien_b200_batch* b, uint64_t timesteps)
+{
+    return guarded([&] {
+        if (!b) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
+        b->arena->calcTimesteps(timesteps);
+    });
+}
+
+int alien_b200_batch_enqueue_timesteps(alien_b200_batch* b, uint64_t timesteps)
+{
+    return guarded([&] {
+        if (!b) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
+        b->arena->enqueueSteps(timesteps);
+    });
+}
+
+int alien_b200_batch_get_data(alien_b200_batch* b, int world, const AlienDataTO* data)
+{
+    return guarded([&] {
+        if (!b || world < 0 || world >= b->arena->numWorlds()) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        b->arena->getData(world, false, AlienInt2{0, 0}, AlienInt2{0, 0}, data);
+    });
+}
+
+int alien_b200_batch_get_array_sizes(alien_b200_batch* b, int world, AlienArraySizes* sizes)
+{
+    return guarded([&] {
+        if (!b || !sizes || world < 0 || world >= b->arena->numWorlds()) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        const WorldInfo& wi = b->arena->world(world).info;
+        sizes->cellArraySize = static_cast<uint64_t>(wi.cellCap);
+        sizes->particleArraySize = static_cast<uint64_t>(wi.partCap);
+        sizes->auxiliaryDataSize = b->arena->world(world).aux.size();
+    });
+}
+
+int alien_b200_batch_get_raw_statistics(alien_b200_batch* b, int world, AlienRawStatistics* statistics)
+{
+    return guarded([&] {
+        if (!b || !statistics || world < 0 || world >= b->arena->numWorlds())
+            throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        *statistics = b->arena->statistics(world);
+    });
+}
+
+void* alien_b200_batch_stream(alien_b200_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
+
+uint64_t alien_b200_batch_kernel_launch_count(alien_b200_batch* b) { return b && b->arena ? b->arena->launches() : 0; }
+
+int alien_b200_batch_kernels_per_step(alien_b200_batch* b) { return b && b->arena ? b->arena->kernelsPerStep() : 0; }
+
+}  // extern "C"

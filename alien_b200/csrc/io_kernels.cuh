@@ -1,0 +1,266 @@
+// io_kernels.cuh - data transfer between the reference's DataTO format and
+// the engine's SoA state, statistics, and stable particle compaction.
+//
+// Ingest restates cudaCreateDataFromTO / ObjectFactory::createCellFromTO
+// (source/EngineGpuKernels/DataAccessKernels.cu:363-387,
+// ObjectFactory.cuh:46-86); egress restates cudaGetCellDataWithoutConnections
+// + cudaResolveConnections + cudaGetParticleData (DataAccessKernels.cu
+// :312-362) with a stable, rank-based order instead of atomic slots.  All
+// kernels here work on one world w; their grid covers the world's padded
+// slot range block by block.
+#pragma once
+
+#include "device_common.cuh"
+
+namespace ab {
+
+// ---- ingest ----
+__global__ void __launch_bounds__(kBlock) kIngestCells(DevState s, int w, const AlienCellTO* to, long long n, AlienCellTO* cold,
+                                                       long long coldBase)
+{
+    const long long i = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    if (i >= n) return;
+    const WorldInfo& wi = s.worlds[w];
+    const long long g = wi.cellBase + i;
+    const AlienCellTO& c = to[i];
+    cold[coldBase + i] = c;
+    s.coldIdx[g] = static_cast<uint32_t>(coldBase + i);
+    s.id[g] = c.id;
+    s.posA[g] = correctPosition(f2(c.pos.x, c.pos.y), wi.W, wi.H);
+    s.velA[g] = f2(c.vel.x, c.vel.y);
+    s.energy[g] = c.energy;
+    s.stiffness[g] = c.stiffness;
+    s.density[g] = 1.0f;  // ObjectFactory.cuh:84
+    s.color[g] = c.color;
+    s.maxConn[g] = c.maxConnections;
+    const int n6 = c.numConnections > kMaxBonds ? kMaxBonds : c.numConnections;
+    s.numConn[g] = static_cast<uint8_t>(n6);
+    s.barrier[g] = c.barrier ? 1 : 0;
+    s.alive[g] = 1;
+    s.livingState[g] = static_cast<uint8_t>(c.livingState);
+    s.age[g] = c.age;
+    s.activationTime[g] = c.activationTime;
+    s.creatureId[g] = c.creatureId;
+    for (int k = 0; k < kMaxBonds; ++k) {
+        const bool used = k < n6;
+        s.bond[g * kMaxBonds + k] = used ? static_cast<int>(wi.cellBase + c.connections[k].cellIndex) : -1;
+        s.bondDist[g * kMaxBonds + k] = c.connections[k].distance;
+        s.bondAngle[g * kMaxBonds + k] = c.connections[k].angleFromPrevious;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) kIngestParticles(DevState s, int w, const AlienParticleTO* to, long long n)
+{
+    const long long i = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    if (i >= n) return;
+    const WorldInfo& wi = s.worlds[w];
+    const long long q = wi.partBase + i;
+    const AlienParticleTO& p = to[i];
+    s.pid[q] = p.id;
+    s.ppos[q] = correctPosition(f2(p.pos.x, p.pos.y), wi.W, wi.H);
+    s.pvel[q] = f2(p.vel.x, p.vel.y);
+    s.penergy[q] = p.energy;
+    s.pcolor[q] = p.color;
+    s.pselected[q] = p.selected;
+    s.palive[q] = 1;
+    s.plast[q] = ~0ull;
+}
+
+// ids stay unique: the world's id counter continues after the largest id
+// (cudaAdaptNumberGenerator, DataAccessKernels.cu:389-410)
+__global__ void __launch_bounds__(kBlock) kMaxId(DevState s, int w, const AlienCellTO* cells, long long nc,
+                                                 const AlienParticleTO* parts, long long np)
+{
+    const long long i = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    unsigned long long m = 0;
+    if (i < nc) m = cells[i].id + 1;
+    if (i < np && parts[i].id + 1 > m) m = parts[i].id + 1;
+    if (m) atomicMax(&s.counters[w].nextId, m);
+}
+
+// ---- selection + ranks (egress and compaction) ----
+__device__ __forceinline__ bool inRect(float2 p, int ulx, int uly, int lrx, int lry)
+{
+    return p.x >= ulx && p.x <= lrx && p.y >= uly && p.y <= lry;  // isContainedInRect, Base.cuh:92-97
+}
+
+// rank[g] = 1 if the cell is selected (0 otherwise); blockCount = block sums
+__global__ void __launch_bounds__(kBlock) kSelectCells(DevState s, int w, int useRect, int ulx, int uly, int lrx, int lry,
+                                                       int* rank, uint32_t* blockCount)
+{
+    const WorldInfo& wi = s.worlds[w];
+    const long long g = wi.cellBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    uint32_t v = 0;
+    if (g < wi.cellBase + s.counters[w].numCells && s.alive[g])
+        v = (!useRect || inRect(s.posA[g], ulx, uly, lrx, lry)) ? 1u : 0u;
+    uint32_t total;
+    const uint32_t ex = blockExclusiveScan(v, &total);
+    rank[g] = v ? static_cast<int>(ex) : -1;
+    if (threadIdx.x == 0) blockCount[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kBlock) kSelectParticles(DevState s, int w, int useRect, int ulx, int uly, int lrx, int lry,
+                                                           int* rank, uint32_t* blockCount)
+{
+    const WorldInfo& wi = s.worlds[w];
+    const long long q = wi.partBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    uint32_t v = 0;
+    if (q < wi.partBase + s.counters[w].numParticles && s.palive[q])
+        v = (!useRect || inRect(s.ppos[q], ulx, uly, lrx, lry)) ? 1u : 0u;
+    uint32_t total;
+    const uint32_t ex = blockExclusiveScan(v, &total);
+    rank[q] = v ? static_cast<int>(ex) : -1;
+    if (threadIdx.x == 0) blockCount[blockIdx.x] = total;
+}
+
+// blockCount (exclusive scan, numBlocks + 1 entries) -> global ranks
+__global__ void __launch_bounds__(kBlock) kFinishRanks(long long base, int* rank, const uint32_t* blockOffset)
+{
+    const long long i = base + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    if (rank[i] >= 0) rank[i] += static_cast<int>(blockOffset[blockIdx.x]);
+}
+
+// ---- egress (createCellTO, DataAccessKernels.cu:18-110) ----
+__global__ void __launch_bounds__(kBlock) kEgressCells(DevState s, int w, const int* rank, const AlienCellTO* cold, AlienCellTO* out)
+{
+    const WorldInfo& wi = s.worlds[w];
+    const long long g = wi.cellBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    const int r = rank[g];
+    if (r < 0) return;
+    AlienCellTO c = cold[s.coldIdx[g]];
+    c.id = s.id[g];
+    const float2 p = s.posA[g], v = s.velA[g];
+    c.pos.x = p.x;
+    c.pos.y = p.y;
+    c.vel.x = v.x;
+    c.vel.y = v.y;
+    c.energy = s.energy[g];
+    c.stiffness = s.stiffness[g];
+    c.color = s.color[g];
+    c.maxConnections = s.maxConn[g];
+    const int n = s.numConn[g];
+    c.numConnections = static_cast<uint8_t>(n);
+    c.barrier = s.barrier[g];
+    c.livingState = s.livingState[g];
+    c.age = s.age[g];
+    c.activationTime = s.activationTime[g];
+    for (int k = 0; k < kMaxBonds; ++k) {
+        if (k < n) {
+            c.connections[k].cellIndex = rank[s.bond[g * kMaxBonds + k]];  // -1 when the partner is not exported
+            c.connections[k].distance = s.bondDist[g * kMaxBonds + k];
+            c.connections[k].angleFromPrevious = s.bondAngle[g * kMaxBonds + k];
+        } else {
+            c.connections[k].cellIndex = 0;
+            c.connections[k].distance = 0.0f;
+            c.connections[k].angleFromPrevious = 0.0f;
+        }
+    }
+    out[r] = c;
+}
+
+__global__ void __launch_bounds__(kBlock) kEgressParticles(DevState s, int w, const int* rank, AlienParticleTO* out)
+{
+    const WorldInfo& wi = s.worlds[w];
+    const long long q = wi.partBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    const int r = rank[q];
+    if (r < 0) return;
+    AlienParticleTO p;
+    memset(&p, 0, sizeof(p));
+    p.id = s.pid[q];
+    p.energy = s.penergy[q];
+    const float2 pos = s.ppos[q], vel = s.pvel[q];
+    p.pos.x = pos.x;
+    p.pos.y = pos.y;
+    p.vel.x = vel.x;
+    p.vel.y = vel.y;
+    p.color = s.pcolor[q];
+    p.selected = s.pselected[q];
+    out[r] = p;
+}
+
+// ---- stable particle compaction of one world (GarbageCollectorKernels.cu
+// :177-196 without the reordering): live particles move to partBase + rank
+__global__ void __launch_bounds__(kBlock) kCompactParticlesGather(DevState s, int w, const int* rank, unsigned long long* tid,
+                                                                  float2* tpos, float2* tvel, float* tenergy, uint8_t* tcolor,
+                                                                  uint8_t* tsel, unsigned long long* tlast)
+{
+    const WorldInfo& wi = s.worlds[w];
+    const long long q = wi.partBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    const int r = rank[q];
+    if (r < 0) return;
+    tid[r] = s.pid[q];
+    tpos[r] = s.ppos[q];
+    tvel[r] = s.pvel[q];
+    tenergy[r] = s.penergy[q];
+    tcolor[r] = s.pcolor[q];
+    tsel[r] = s.pselected[q];
+    tlast[r] = s.plast[q];
+}
+
+__global__ void __launch_bounds__(kBlock) kCompactParticlesScatter(DevState s, int w, long long count, const unsigned long long* tid,
+                                                                   const float2* tpos, const float2* tvel, const float* tenergy,
+                                                                   const uint8_t* tcolor, const uint8_t* tsel,
+                                                                   const unsigned long long* tlast)
+{
+    const WorldInfo& wi = s.worlds[w];
+    const long long r = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    if (r >= wi.partCap) return;
+    const long long q = wi.partBase + r;
+    if (r < count) {
+        s.pid[q] = tid[r];
+        s.ppos[q] = tpos[r];
+        s.pvel[q] = tvel[r];
+        s.penergy[q] = tenergy[r];
+        s.pcolor[q] = tcolor[r];
+        s.pselected[q] = tsel[r];
+        s.plast[q] = tlast[r];
+        s.palive[q] = 1;
+    } else {
+        s.palive[q] = 0;
+    }
+}
+
+// ---- statistics (subset of RawStatisticsData; StatisticsKernels.cu:5-105) ----
+struct StatsAcc {
+    unsigned long long numCells, numParticles, numConnections;
+    unsigned long long numCellsByColor[ALIEN_B200_MAX_COLORS];
+    long long cellEnergyFix, particleEnergyFix;  // 2^-16 fixed point: order-independent sums
+};
+
+__global__ void __launch_bounds__(kBlock) kStatsCells(DevState s, StatsAcc* acc)
+{
+    const int b = blockIdx.x;
+    const int w = s.cellBlockWorld[b];
+    const WorldInfo& wi = s.worlds[w];
+    const long long g = static_cast<long long>(b) * kBlock + threadIdx.x;
+    if (g >= wi.cellBase + s.counters[w].numCells || !s.alive[g]) return;
+    StatsAcc& a = acc[w];
+    atomicAdd(&a.numCells, 1ull);
+    atomicAdd(&a.numConnections, static_cast<unsigned long long>(s.numConn[g]));
+    atomicAdd(&a.numCellsByColor[s.color[g] % ALIEN_B200_MAX_COLORS], 1ull);
+    atomicAdd(reinterpret_cast<unsigned long long*>(&a.cellEnergyFix),
+              static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(s.energy[g]) * 65536.0)));
+}
+
+__global__ void __launch_bounds__(kBlock) kStatsParticles(DevState s, StatsAcc* acc)
+{
+    const int pb = blockIdx.x;
+    const int w = s.partBlockWorld[pb];
+    const WorldInfo& wi = s.worlds[w];
+    const long long q = static_cast<long long>(pb) * kBlock + threadIdx.x;
+    if (q >= wi.partBase + s.counters[w].numParticles || !s.palive[q]) return;
+    StatsAcc& a = acc[w];
+    atomicAdd(&a.numParticles, 1ull);
+    atomicAdd(reinterpret_cast<unsigned long long*>(&a.particleEnergyFix),
+              static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(s.penergy[q]) * 65536.0)));
+}
+
+// prepareForSimulationParametersChanges -> resetDensity (CellProcessor.cuh:860-870)
+__global__ void __launch_bounds__(kBlock) kResetDensity(DevState s, int w)
+{
+    const WorldInfo& wi = s.worlds[w];
+    const long long g = wi.cellBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    if (g < wi.cellBase + wi.cellCap) s.density[g] = 1.0f;
+}
+
+}  // namespace ab

@@ -1,0 +1,1209 @@
+// kernels.cuh - the per-timestep physics stage of the B200 engine.
+//
+// One timestep = the launch sequence in Arena::enqueueStep (engine.cu).  The
+// phases follow _SimulationKernelsLauncher::calcTimestep
+// (source/EngineGpuKernels/SimulationKernelsLauncher.cu:25-91) for the
+// physics kernels; every phase boundary that the reference crosses by racing
+// threads inside one kernel is a kernel boundary here, so each kernel reads
+// only values that are final (deterministic step definition, identical to
+// the CPU oracle):
+//
+//   kBin        cell map binning by tile + radiation + per-step resets,
+//               particle map (physics_init / physics_fillMaps)
+//   scan        exclusive scan of per-tile counts
+//   kScatter    cell slots grouped by tile
+//   kStage      per-slot rank (scan visibility) + sorted SoA copy
+//   kPairs*     fluid or collision pair forces (physics_calc*Forces)
+//   kApplyBond1 checkForces, applyForces, bond forces #1 | particle movement
+//   kVerletPos  verletPositionUpdate                     | particle targets
+//   kBond2      checkConnections, bond forces #2         | particle merges
+//   kVerletVel  verletVelocityUpdate, aging              | absorption
+//   kTransition living-state transition, inner friction  | splitting
+//   kDecay      friction, decay                          | particle map reset
+//   kResolve    dying/detaching resolution, bond additions (scratch)
+//   kCommit     bond additions, cell deletion, bond deletion
+//   kEvent*     ids and slots of new energy particles, append
+#pragma once
+
+#include "device_common.cuh"
+
+namespace ab {
+
+// ------------------------------------------------------------ helpers ----
+
+struct CellCtx {
+    int w;
+    long long g;
+    bool valid;
+};
+
+__device__ __forceinline__ CellCtx cellCtx(const DevState& s)
+{
+    CellCtx c;
+    int b = blockIdx.x;
+    c.w = s.cellBlockWorld[b];
+    c.g = static_cast<long long>(b) * kBlock + threadIdx.x;
+    const WorldInfo& wi = s.worlds[c.w];
+    c.valid = c.g < wi.cellBase + s.counters[c.w].numCells && s.alive[c.g];
+    return c;
+}
+
+// particle part of a combined launch: blocks [numCellBlocks, numCellBlocks + numPartBlocks)
+struct PartCtx {
+    int w;
+    long long q;
+    bool inRange;  // slot used at step start (orig particles)
+};
+__device__ __forceinline__ PartCtx partCtx(const DevState& s, int pb)
+{
+    PartCtx c;
+    c.w = s.partBlockWorld[pb];
+    c.q = static_cast<long long>(pb) * kBlock + threadIdx.x;
+    const WorldInfo& wi = s.worlds[c.w];
+    c.inRange = c.q < wi.partBase + s.counters[c.w].numParticles;
+    return c;
+}
+
+__device__ __forceinline__ bool isBondedTo(const int* bonds, int n, int j)
+{
+    bool r = false;
+    for (int k = 0; k < n; ++k) r |= (bonds[k] == j);
+    return r;
+}
+
+// distinct tile coordinates covering slots s-r .. s+r (wrapped)
+__device__ __forceinline__ int tileCoords(int s, int r, int size, int T, int* out)
+{
+    int n = 0;
+    for (int d = -r; d <= r; ++d) {
+        int t = wrapInt(s + d, size) / T;
+        bool dup = false;
+        for (int m = 0; m < n; ++m) dup |= (out[m] == t);
+        if (!dup) out[n++] = t;
+    }
+    return n;
+}
+constexpr int kMaxRadius = 15;
+
+// ---------------------------------------------------------------- kBin ----
+// cells: reset per-step scratch, tile binning (CellMap::set_block,
+// Map.cuh:95-130, by tile instead of a pointer chain), radiation
+// (CellProcessor::radiation, CellProcessor.cuh:725-773).
+// particles: reset, particle map (ParticleMap::set_block, Map.cuh:236-258;
+// the highest storage index wins).
+__global__ void __launch_bounds__(kBlock) kBin(DevState s)
+{
+    if (blockIdx.x < s.numCellBlocks) {
+        CellCtx c = cellCtx(s);
+        const long long g = c.g;
+        s.flags[g] = 0;
+        s.best[g] = -1;
+        s.newPartner[g] = -1;
+        s.angleAcc[4 * g + 0] = 0;
+        s.angleAcc[4 * g + 1] = 0;
+        s.angleAcc[4 * g + 2] = 0;
+        s.angleAcc[4 * g + 3] = 0;
+        s.energyAcc[g] = 0;
+        if (!c.valid) return;
+        const WorldInfo& wi = s.worlds[c.w];
+        const AlienPhysicsParams& p = s.params[wi.paramIndex];
+        float2 pos = s.posA[g];
+        int sx = slotX(pos.x, wi.W), sy = slotX(pos.y, wi.H);
+        uint32_t tile = static_cast<uint32_t>(wi.tileBase + (sx / wi.T) + static_cast<long long>(sy / wi.T) * wi.nTX);
+        s.tileOf[g] = tile;
+        s.tileOff[g] = atomicAdd(&s.tileCount[tile], 1u);
+
+        if (s.barrier[g]) return;
+        const uint64_t T = s.counters[c.w].timestep;
+        const uint64_t id = s.id[g];
+        if (!(draw(id, T, kSiteRadiation) < p.radiationProb)) return;
+        int col = s.color[g] % ALIEN_B200_MAX_COLORS;
+        float e = s.energy[g];
+        float factor = 0.0f;
+        if (e > p.highRadiationMinCellEnergy[col]) factor += p.highRadiationFactor[col];
+        if (static_cast<long long>(s.age[g]) > static_cast<long long>(p.radiationMinCellAge[col]))
+            factor += p.radiationCellAgeStrength[col];
+        if (!(factor > 0.0f)) return;
+        float loss = e * factor;
+        loss = loss / p.radiationProb;
+        loss = 2.0f * loss * draw(id, T, kSiteRadiationEnergy);
+        if (e > 1.0f) {
+            float2 v = s.velA[g];
+            float2 pv = v * p.radiationVelocityMultiplier
+                + unitVectorOfAngle(draw(id, T, kSiteRadiationAngle) * 360.0f) * p.radiationVelocityPerturbation;
+            float2 pp = pos + normalized2(pv) * 1.5f - pv;
+            pp = correctPosition(pp, wi.W, wi.H);
+            if (loss > e - 1.0f) loss = e - 1.0f;
+            s.energy[g] = e - loss;
+            if (loss > kNearZero) {  // createEnergyParticle drops energy <= NEAR_ZERO
+                s.radPos[g] = pp;
+                s.radVel[g] = pv;
+                s.radEnergy[g] = loss;
+                atomicOr(&s.flags[g], kFlagRadiation);
+            }
+        }
+    } else {
+        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
+        const long long q = c.q;
+        s.pflag[q] = 0;
+        s.ptarget[q] = -1;
+        s.pslot[q] = -1;
+        s.pmerge[3 * q + 0] = 0;
+        s.pmerge[3 * q + 1] = 0;
+        s.pmerge[3 * q + 2] = 0;
+        if (!c.inRange || !s.palive[q]) return;
+        const WorldInfo& wi = s.worlds[c.w];
+        float2 pp = s.ppos[q];
+        int slot = slotX(pp.x, wi.W) + slotX(pp.y, wi.H) * wi.W;
+        s.pslot[q] = slot;
+        atomicMax(&s.pmap[wi.pmapBase + slot], static_cast<int>(q));
+    }
+}
+
+// ------------------------------------------------------------- scan ------
+// exclusive scan of n uint32 values: kScanReduce -> kScanPartials -> kScanDown
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kBlock * kScanItems;
+
+__global__ void __launch_bounds__(kBlock) kScanReduce(const uint32_t* in, long long n, uint32_t* partials)
+{
+    long long base = static_cast<long long>(blockIdx.x) * kScanTile;
+    uint32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        long long k = base + static_cast<long long>(i) * kBlock + threadIdx.x;
+        if (k < n) sum += in[k];
+    }
+    uint32_t total;
+    blockExclusiveScan(sum, &total);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kBlock) kScanPartials(uint32_t* partials, int numPartials)
+{
+    // one block; sequential chunks of kBlock
+    uint32_t carry = 0;
+    for (int base = 0; base < numPartials; base += kBlock) {
+        int k = base + threadIdx.x;
+        uint32_t v = k < numPartials ? partials[k] : 0;
+        uint32_t total;
+        uint32_t ex = blockExclusiveScan(v, &total);
+        if (k < numPartials) partials[k] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) partials[numPartials] = carry;
+}
+
+__global__ void __launch_bounds__(kBlock) kScanDown(const uint32_t* in, long long n, const uint32_t* partials, uint32_t* out)
+{
+    long long base = static_cast<long long>(blockIdx.x) * kScanTile + static_cast<long long>(threadIdx.x) * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        long long k = base + i;
+        v[i] = k < n ? in[k] : 0;
+        sum += v[i];
+    }
+    uint32_t total;
+    uint32_t ex = blockExclusiveScan(sum, &total) + partials[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        long long k = base + i;
+        if (k < n) out[k] = ex;
+        ex += v[i];
+        if (k == n - 1) out[n] = ex;
+    }
+}
+
+// ----------------------------------------------------------- kScatter ----
+__global__ void __launch_bounds__(kBlock) kScatter(DevState s)
+{
+    CellCtx c = cellCtx(s);
+    if (!c.valid) return;
+    s.sorted[s.tileStart[s.tileOf[c.g]] + s.tileOff[c.g]] = static_cast<uint32_t>(c.g);
+}
+
+// ------------------------------------------------------------- kStage ----
+// Rank of each cell among the cells of its slot in storage order (the
+// reference chains at most 11 cells per slot and scans 10 of them,
+// Map.cuh:113-125, CellProcessor.cuh:165) and a sorted SoA copy of the
+// fields the pair phase reads.
+__global__ void __launch_bounds__(kBlock) kStage(DevState s)
+{
+    long long k = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    if (k >= s.tileStart[s.numTiles]) return;
+    const uint32_t g = s.sorted[k];
+    const int w = s.cellBlockWorld[g / kBlock];
+    const WorldInfo& wi = s.worlds[w];
+    const uint32_t t = s.tileOf[g];
+    const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
+    const float2 pos = s.posA[g];
+    const int slot = slotX(pos.x, wi.W) + slotX(pos.y, wi.H) * wi.W;
+    int rank = 0;
+    for (uint32_t m = k0; m < k1; ++m) {
+        uint32_t g2 = s.sorted[m];
+        if (g2 >= g) continue;
+        float2 p2 = s.posA[g2];
+        rank += (slotX(p2.x, wi.W) + slotX(p2.y, wi.H) * wi.W) == slot;
+    }
+    const float2 vel = s.velA[g];
+    int fl = (s.barrier[g] ? kStageBarrier : 0) | (rank < kSlotScanLevels ? kStageVisible : 0) | (rank == 0 ? kStageHead : 0);
+    fl |= (static_cast<int>(s.numConn[g]) & 0xf) << 4;
+    fl |= static_cast<int>(s.maxConn[g]) << 8;
+    fl |= w << 16;
+    s.stagedPV[k] = make_float4(pos.x, pos.y, vel.x, vel.y);
+    s.stagedMeta[k] = make_int4(static_cast<int>(g), fl, __float_as_int(s.density[g]), __float_as_int(s.energy[g]));
+}
+
+// -------------------------------------------------------- kPairsFluid ----
+// CellProcessor::calcFluidForces_reconnectCells_correctOverlap,
+// CellProcessor.cuh:122-283: one thread per cell in tile order; neighbours
+// come from the staged copies of the (2r+1)^2-slot window's tiles.
+__device__ __forceinline__ void pairsFluid(const DevState& s, long long k)
+{
+    const int4 me = s.stagedMeta[k];
+    const float4 mpv = s.stagedPV[k];
+    const int g = me.x;
+    const int w = (me.y >> 16) & 0xffff;
+    const WorldInfo& wi = s.worlds[w];
+    const AlienPhysicsParams& p = s.params[wi.paramIndex];
+    const int W = wi.W, H = wi.H;
+    const float h = p.smoothingLength, R = h * 2.0f, minDist = p.cellMinDistance;
+    const float2 pi = f2(mpv.x, mpv.y), vi = f2(mpv.z, mpv.w);
+    const bool barrierI = me.y & kStageBarrier;
+    const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
+    const float densI = __int_as_float(me.z), energyI = __int_as_float(me.w);
+    int bondsI[kMaxBonds];
+#pragma unroll
+    for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? s.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
+
+    long long qDens = 0, qFpx = 0, qFpy = 0, qFvx = 0, qFvy = 0, qDx = 0, qDy = 0;
+    int bestBarrier = -1;
+    float bestBarrierDist = 0.0f;
+    int best = -1;
+    unsigned long long bestId = ~0ull;
+    const bool fusionI = !barrierI && nI < maxI && energyI <= p.cellMaxBindingEnergy;
+
+    const int r = wi.radiusInt;
+    const int sx = slotX(pi.x, W), sy = slotX(pi.y, H);
+    int tx[2 * kMaxRadius + 1], ty[2 * kMaxRadius + 1];
+    const int ntx = tileCoords(sx, r, W, wi.T, tx), nty = tileCoords(sy, r, H, wi.T, ty);
+    for (int a = 0; a < nty; ++a) {
+        for (int b = 0; b < ntx; ++b) {
+            const long long t = wi.tileBase + tx[b] + static_cast<long long>(ty[a]) * wi.nTX;
+            const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
+            for (uint32_t m = k0; m < k1; ++m) {
+                const int4 om = s.stagedMeta[m];
+                if (!(om.y & kStageVisible)) continue;
+                const float4 opv = s.stagedPV[m];
+                const float2 pd = correctDirection(pi - f2(opv.x, opv.y), W, H);
+                const float d = len2(pd);
+                if (!(d <= R)) continue;
+                const int j = om.x;
+                if (om.y & kStageBarrier) {
+                    if (bestBarrier < 0 || d < bestBarrierDist || (d == bestBarrierDist && j < bestBarrier)) {
+                        bestBarrier = j;
+                        bestBarrierDist = d;
+                    }
+                    continue;
+                }
+                qDens += toFix(sphKernel(d / h) / (h * h));
+                if (j == g) continue;
+                if (!barrierI && d < minDist) {
+                    qDx += toFix(pd.x * minDist / 5.0f);
+                    qDy += toFix(pd.y * minDist / 5.0f);
+                }
+                if (isBondedTo(bondsI, nI, j)) continue;
+                const float2 vd = vi - f2(opv.z, opv.w);
+                const float densJ = __int_as_float(om.z);
+                const float factor = densI / (densI * densI) + densJ / (densJ * densJ);
+                if (fabsf(d) > kNearZero) {
+                    const float kd = sphKernelD(d / h) / (h * h * h);
+                    const float2 fp = pd / (-d) * factor * kd;
+                    const float2 fv = vd / densJ * d * kd / (d * d + 0.25f);
+                    qFpx += toFix(fp.x);
+                    qFpy += toFix(fp.y);
+                    qFvx += toFix(fv.x);
+                    qFvy += toFix(fv.y);
+                }
+                if (fusionI && len2(vd) >= p.cellFusionVelocity) {
+                    const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
+                    if (nJ < maxJ && __int_as_float(om.w) <= p.cellMaxBindingEnergy) {
+                        const unsigned long long idJ = s.id[j];
+                        if (idJ < bestId) {
+                            bestId = idJ;
+                            best = j;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    float2 F = f2(0.0f, 0.0f);
+    if (bestBarrier >= 0) {
+        const long long b = bestBarrier;
+        const float2 pb = s.posA[b];
+        float2 rr = f2(0.0f, 0.0f);
+        const int nb = s.numConn[b];
+        if (nb <= 1) {
+            rr = correctDirection(pi - pb, W, H);
+        } else {
+            const float angleToCell = angleOfVector(correctDirection(pi - pb, W, H));
+            for (int m = 0; m < nb; ++m) {
+                const int c1 = s.bond[b * kMaxBonds + m], c2 = s.bond[b * kMaxBonds + (m + 1) % nb];
+                const float a1 = angleOfVector(correctDirection(s.posA[c1] - pb, W, H));
+                const float a2 = angleOfVector(correctDirection(s.posA[c2] - pb, W, H));
+                if (isAngleInBetween(a1, a2, angleToCell)) {
+                    rr = rotCCW(s.posA[c2] - s.posA[c1]);
+                    break;
+                }
+            }
+        }
+        const float2 vb = s.velA[b];
+        const float2 vr = vi - vb;
+        const float dvr = dot2(vr, rr);
+        if (dvr < 0.0f) {
+            const float trr = fmaxf(0.05f, lensq2(rr));
+            const float td = fmaxf(0.05f, bestBarrierDist);
+            F = (vr - rr * 2.0f * dvr / trr + vb - vi) / td;
+        }
+    }
+    const float2 Fp = f2(fromFix(qFpx), fromFix(qFpy)), Fv = f2(fromFix(qFvx), fromFix(qFvy));
+    F = F + (Fp * p.pressureStrength + Fv * p.viscosityStrength);
+    s.force[g] = F;
+    s.posB[g] = pi + f2(fromFix(qDx), fromFix(qDy));
+    s.densNew[g] = fromFix(qDens);
+    s.best[g] = best;
+}
+
+// ---------------------------------------------------- kPairsCollision ----
+// CellProcessor::calcCollisions_reconnectCells_correctOverlap,
+// CellProcessor.cuh:285-365 with CellMap::executeForEach (Map.cuh:175-196,
+// distance test on the uncorrected difference).  The reference adds each
+// pair force to both cells from the scanning cell; here every cell gathers
+// f(i,j) from its own scan and -f(j,i) from the scans that see it.
+__device__ __forceinline__ float2 collisionForce(float2 pd, float d, float2 vCell, float2 vOther, bool barrierCell,
+                                                 const AlienPhysicsParams& p)
+{
+    const float2 vd = vCell - vOther;
+    const bool approaching = dot2(pd, vd) < 0.0f;
+    const float bf = barrierCell ? 2.0f : 1.0f;
+    if (len2(vCell) > 0.5f && approaching) {
+        const float ds = d * d + 0.25f;
+        return pd * dot2(vd, pd) / (-2.0f * ds) * bf;
+    }
+    return normalized2(pd) * (p.cellMaxCollisionDistance - len2(pd)) * p.cellRepulsionStrength * bf;
+}
+
+__device__ __forceinline__ void pairsCollision(const DevState& s, long long k)
+{
+    const int4 me = s.stagedMeta[k];
+    const float4 mpv = s.stagedPV[k];
+    const int g = me.x;
+    const int w = (me.y >> 16) & 0xffff;
+    const WorldInfo& wi = s.worlds[w];
+    const AlienPhysicsParams& p = s.params[wi.paramIndex];
+    const int W = wi.W, H = wi.H;
+    const float R = p.cellMaxCollisionDistance, minDist = p.cellMinDistance;
+    const float2 pi = f2(mpv.x, mpv.y), vi = f2(mpv.z, mpv.w);
+    const bool barrierI = me.y & kStageBarrier;
+    const bool visibleI = me.y & kStageVisible;
+    const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
+    const float energyI = __int_as_float(me.w);
+    int bondsI[kMaxBonds];
+#pragma unroll
+    for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? s.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
+    const bool fusionI = !barrierI && nI < maxI && energyI <= p.cellMaxBindingEnergy;
+
+    long long qFx = 0, qFy = 0, qDx = 0, qDy = 0;
+    int best = -1;
+    unsigned long long bestId = ~0ull;
+    const int r = wi.radiusInt;
+    const int sx = slotX(pi.x, W), sy = slotX(pi.y, H);
+    int tx[2 * kMaxRadius + 1], ty[2 * kMaxRadius + 1];
+    const int ntx = tileCoords(sx, r, W, wi.T, tx), nty = tileCoords(sy, r, H, wi.T, ty);
+    for (int a = 0; a < nty; ++a) {
+        for (int b = 0; b < ntx; ++b) {
+            const long long t = wi.tileBase + tx[b] + static_cast<long long>(ty[a]) * wi.nTX;
+            const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
+            for (uint32_t m = k0; m < k1; ++m) {
+                const int4 om = s.stagedMeta[m];
+                const int j = om.x;
+                if (j == g) continue;
+                const float4 opv = s.stagedPV[m];
+                const float2 pj = f2(opv.x, opv.y);
+                if (!(len2(pj - pi) <= R)) continue;
+                const bool visibleJ = om.y & kStageVisible;
+                if (!visibleJ && !visibleI) continue;
+                const float2 pd = correctDirection(pi - pj, W, H);
+                const float d = len2(pd);
+                const bool bonded = isBondedTo(bondsI, nI, j);
+                const float2 vj = f2(opv.z, opv.w);
+                if (visibleJ) {  // i's own scan sees j
+                    if (!barrierI && d < minDist) {
+                        qDx += toFix(pd.x * minDist / 5.0f);
+                        qDy += toFix(pd.y * minDist / 5.0f);
+                    }
+                    if (!bonded) {
+                        const float2 f = collisionForce(pd, d, vi, vj, barrierI, p);
+                        qFx += toFix(f.x);
+                        qFy += toFix(f.y);
+                        const float2 vd = vi - vj;
+                        if (fusionI && len2(vd) >= p.cellFusionVelocity && dot2(pd, vd) < 0.0f) {
+                            const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
+                            if (nJ < maxJ && !(om.y & kStageBarrier) && __int_as_float(om.w) <= p.cellMaxBindingEnergy) {
+                                const unsigned long long idJ = s.id[j];
+                                if (idJ < bestId) {
+                                    bestId = idJ;
+                                    best = j;
+                                }
+                            }
+                        }
+                    }
+                }
+                if (visibleI && !bonded) {  // j's scan sees i and applies -f(j,i) to i
+                    const float2 pdj = correctDirection(pj - pi, W, H);
+                    const float2 f = collisionForce(pdj, len2(pdj), vj, vi, om.y & kStageBarrier, p);
+                    qFx -= toFix(f.x);
+                    qFy -= toFix(f.y);
+                }
+            }
+        }
+    }
+    s.force[g] = f2(fromFix(qFx), fromFix(qFy));
+    s.posB[g] = pi + f2(fromFix(qDx), fromFix(qDy));
+    s.densNew[g] = __int_as_float(me.z);
+    s.best[g] = best;
+}
+
+// one thread per staged cell; the world's motion type selects the pair law
+__global__ void __launch_bounds__(kBlock) kPairs(DevState s)
+{
+    const long long k = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    if (k >= s.tileStart[s.numTiles]) return;
+    const int w = (s.stagedMeta[k].y >> 16) & 0xffff;
+    if (s.worlds[w].motionType == ALIEN_B200_MOTION_FLUID)
+        pairsFluid(s, k);
+    else
+        pairsCollision(s, k);
+}
+
+// ------------------------------------------------------- bond forces -----
+// CellProcessor::calcConnectionForces, CellProcessor.cuh:408-491: spring
+// forces in bond order; angle forces (every third step) are scattered to
+// the two partners as fixed-point integers into angleAcc[4*j + accOffset].
+__device__ __forceinline__ float2 bondForce(const DevState& s, long long g, const float2* P, bool considerAngles,
+                                            int W, int H, float minDist, int accOffset)
+{
+    float2 F = f2(0.0f, 0.0f);
+    const int n = s.numConn[g];
+    if (n == 0 || s.barrier[g]) return F;
+    const long long bb = g * kMaxBonds;
+    const float2 pi = P[g];
+    float2 prevDisp = correctDirection(P[s.bond[bb + n - 1]] - pi, W, H);
+    const float si = s.stiffness[g];
+    const float s2 = si * si;
+    for (int k = 0; k < n; ++k) {
+        const int j = s.bond[bb + k];
+        const float sj = s.stiffness[j];
+        const float sj2 = sj * sj;
+        const float2 disp = correctDirection(P[j] - pi, W, H);
+        const float dist = len2(disp);
+        const float dev = dist - s.bondDist[bb + k];
+        F = F + normalized2(disp) * dev * (s2 + sj2) / 6.0f;
+        if (considerAngles && (n > 2 || (n == 2 && k == 0))) {
+            const int last = (k + n - 1) % n;
+            const int jl = s.bond[bb + last];
+            const int nj = s.numConn[j];
+            bool tri = false;
+            for (int m = 0; m < nj; ++m) tri |= (s.bond[static_cast<long long>(j) * kMaxBonds + m] == jl);
+            if (!tri) {
+                const float a = angleOfVector(disp), pa = angleOfVector(prevDisp);
+                const float act = subtractAngle(a, pa);
+                if (act < 0.0f) continue;
+                const float ref = s.bondAngle[bb + k];
+                const float strength = fabsf(ref - act) / 2000.0f * s2;
+                float2 f1 = rotCW(normalized2(disp) / fmaxf(len2(disp), minDist) * strength);
+                float2 f2v = rotCCW(normalized2(prevDisp) / fmaxf(len2(prevDisp), minDist) * strength);
+                if (ref < act) {
+                    f1 = f1 * -1.0f;
+                    f2v = f2v * -1.0f;
+                }
+                if (!s.barrier[j]) {
+                    atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * j + accOffset]),
+                              static_cast<unsigned long long>(toFix(f1.x)));
+                    atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * j + accOffset + 1]),
+                              static_cast<unsigned long long>(toFix(f1.y)));
+                }
+                if (!s.barrier[jl]) {
+                    atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * jl + accOffset]),
+                              static_cast<unsigned long long>(toFix(f2v.x)));
+                    atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * jl + accOffset + 1]),
+                              static_cast<unsigned long long>(toFix(f2v.y)));
+                }
+                F = F - (f1 + f2v);
+            }
+        }
+        prevDisp = disp;
+    }
+    return F;
+}
+
+// -------------------------------------------------------- kApplyBond1 ----
+// cells: checkForces + applyForces (CellProcessor.cuh:367-406), bond forces
+// #1 at the overlap-corrected positions.  particles: movement
+// (RadiationProcessor::movement, RadiationProcessor.cuh:61-70).
+__global__ void __launch_bounds__(kBlock) kApplyBond1(DevState s)
+{
+    if (blockIdx.x < s.numCellBlocks) {
+        CellCtx c = cellCtx(s);
+        if (!c.valid) return;
+        const long long g = c.g;
+        const WorldInfo& wi = s.worlds[c.w];
+        const AlienPhysicsParams& p = s.params[wi.paramIndex];
+        const uint64_t T = s.counters[c.w].timestep;
+        if (p.motionType == ALIEN_B200_MOTION_FLUID) s.density[g] = s.densNew[g];
+        if (!s.barrier[g]) {
+            const int col = s.color[g] % ALIEN_B200_MAX_COLORS;
+            const float2 F = s.force[g];
+            if (len2(F) > p.cellMaxForce[col]) {
+                if (draw(s.id[g], T, kSiteForceDecay) < p.cellMaxForceDecayProb) atomicOr(&s.flags[g], kFlagDelAll);
+            }
+            float2 v = s.velA[g] + F;
+            if (len2(v) > p.cellMaxVelocity) v = normalized2(v) * p.cellMaxVelocity;
+            s.velA[g] = v;
+        }
+        s.force1[g] = bondForce(s, g, s.posB, T % 3 == 0, wi.W, wi.H, p.cellMinDistance, 0);
+    } else {
+        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
+        if (!c.inRange || !s.palive[c.q]) return;
+        const WorldInfo& wi = s.worlds[c.w];
+        const AlienPhysicsParams& p = s.params[wi.paramIndex];
+        s.ppos[c.q] = correctPosition(s.ppos[c.q] + s.pvel[c.q] * p.timestepSize, wi.W, wi.H);
+    }
+}
+
+// --------------------------------------------------------- kVerletPos ----
+// cells: verletPositionUpdate (CellProcessor.cuh:525-544).
+// particles: merge target (RadiationProcessor::collision, :78-80).
+__global__ void __launch_bounds__(kBlock) kVerletPos(DevState s)
+{
+    if (blockIdx.x < s.numCellBlocks) {
+        CellCtx c = cellCtx(s);
+        if (!c.valid) return;
+        const long long g = c.g;
+        const WorldInfo& wi = s.worlds[c.w];
+        const AlienPhysicsParams& p = s.params[wi.paramIndex];
+        const float dt = p.timestepSize;
+        const float2 v = s.velA[g];
+        const float2 pb = s.posB[g];
+        float2 np;
+        if (s.barrier[g]) {
+            np = pb + v * dt;
+        } else {
+            const float2 F1 = s.force1[g] + f2(fromFix(s.angleAcc[4 * g + 0]), fromFix(s.angleAcc[4 * g + 1]));
+            s.force1[g] = F1;
+            np = pb + (v * dt + F1 * dt * dt / 2.0f);
+        }
+        s.posA[g] = correctPosition(np, wi.W, wi.H);
+    } else {
+        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
+        if (!c.inRange || !s.palive[c.q]) return;
+        const WorldInfo& wi = s.worlds[c.w];
+        const float2 pp = s.ppos[c.q];
+        const int o = s.pmap[wi.pmapBase + slotX(pp.x, wi.W) + slotX(pp.y, wi.H) * wi.W];
+        if (o >= 0 && o != c.q && lensq2(pp - s.ppos[o]) < 0.5f) s.ptarget[c.q] = o;
+    }
+}
+
+// ------------------------------------------------------------- kBond2 ----
+// cells: checkConnections (CellProcessor.cuh:493-523) at the new positions,
+// bond forces #2.  particles: merges into particles that do not merge
+// themselves (RadiationProcessor.cuh:82-96 under the fixed rule).
+__global__ void __launch_bounds__(kBlock) kBond2(DevState s)
+{
+    if (blockIdx.x < s.numCellBlocks) {
+        CellCtx c = cellCtx(s);
+        if (!c.valid) return;
+        const long long g = c.g;
+        const WorldInfo& wi = s.worlds[c.w];
+        const AlienPhysicsParams& p = s.params[wi.paramIndex];
+        const uint64_t T = s.counters[c.w].timestep;
+        if (!s.barrier[g]) {
+            const int n = s.numConn[g];
+            const float maxDist = p.cellMaxBindingDistance[s.color[g] % ALIEN_B200_MAX_COLORS];
+            const float2 pi = s.posA[g];
+            bool destroy = false;
+            for (int k = 0; k < n; ++k) {
+                const int j = s.bond[g * kMaxBonds + k];
+                if (len2(correctDirection(s.posA[j] - pi, wi.W, wi.H)) > maxDist) destroy = true;
+            }
+            if (destroy) {
+                atomicOr(&s.flags[g], kFlagDelAll);
+                for (int k = 0; k < n; ++k) atomicOr(&s.flags[s.bond[g * kMaxBonds + k]], kFlagDetach);
+            }
+        }
+        s.force[g] = bondForce(s, g, s.posA, T % 3 == 0, wi.W, wi.H, p.cellMinDistance, 2);
+    } else {
+        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
+        if (!c.inRange || !s.palive[c.q]) return;
+        const long long q = c.q;
+        const int o = s.ptarget[q];
+        if (o < 0 || s.ptarget[o] >= 0) return;
+        const float eq = s.penergy[q];
+        if (!(eq > kNearZero && s.penergy[o] > kNearZero)) return;
+        const float2 vq = s.pvel[q];
+        atomicOr(&s.pflag[o], 1u);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.pmerge[3LL * o + 0]), static_cast<unsigned long long>(toFix(eq)));
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.pmerge[3LL * o + 1]), static_cast<unsigned long long>(toFix(eq * vq.x)));
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.pmerge[3LL * o + 2]), static_cast<unsigned long long>(toFix(eq * vq.y)));
+        s.palive[q] = 0;
+        atomicAdd(&s.counters[c.w].deadParticles, 1u);
+    }
+}
+
+// head cell (rank 0) of a slot, from the staged tile lists
+__device__ __forceinline__ int slotHead(const DevState& s, const WorldInfo& wi, float2 pos)
+{
+    const int sx = slotX(pos.x, wi.W), sy = slotX(pos.y, wi.H);
+    const long long t = wi.tileBase + sx / wi.T + static_cast<long long>(sy / wi.T) * wi.nTX;
+    const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
+    for (uint32_t m = k0; m < k1; ++m) {
+        const int4 om = s.stagedMeta[m];
+        if (!(om.y & kStageHead)) continue;
+        const float4 opv = s.stagedPV[m];
+        if (slotX(opv.x, wi.W) == sx && slotX(opv.y, wi.H) == sy) return om.x;
+    }
+    return -1;
+}
+
+// --------------------------------------------------------- kVerletVel ----
+// cells: verletVelocityUpdate (CellProcessor.cuh:546-559), detaching from
+// checkConnections, aging (CellProcessor.cuh:561-593).
+// particles: merged particles, absorption into / reflection at the cell
+// under the particle (RadiationProcessor.cuh:97-168).
+__global__ void __launch_bounds__(kBlock) kVerletVel(DevState s)
+{
+    if (blockIdx.x < s.numCellBlocks) {
+        CellCtx c = cellCtx(s);
+        if (!c.valid) return;
+        const long long g = c.g;
+        const WorldInfo& wi = s.worlds[c.w];
+        const AlienPhysicsParams& p = s.params[wi.paramIndex];
+        const float2 v = s.velA[g];
+        if (s.barrier[g]) {
+            s.velB[g] = v;
+        } else {
+            const float2 F2 = s.force[g] + f2(fromFix(s.angleAcc[4 * g + 2]), fromFix(s.angleAcc[4 * g + 3]));
+            s.velB[g] = v + (F2 + s.force1[g]) / 2.0f * p.timestepSize;
+        }
+        if (s.flags[g] & kFlagDetach) s.livingState[g] = ALIEN_B200_LIVING_DETACHING;
+        if (!s.barrier[g]) {
+            ++s.age[g];
+            if (s.livingState[g] == ALIEN_B200_LIVING_READY && s.activationTime[g] > 0) --s.activationTime[g];
+        }
+    } else {
+        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
+        if (!c.inRange || !s.palive[c.q]) return;
+        const long long q = c.q;
+        const WorldInfo& wi = s.worlds[c.w];
+        const AlienPhysicsParams& p = s.params[wi.paramIndex];
+        if (s.pflag[q] & 1u) {
+            const float eq = s.penergy[q];
+            const float e = eq + fromFix(s.pmerge[3 * q + 0]);
+            const float2 vq = s.pvel[q];
+            s.pvel[q] = f2((eq * vq.x + fromFix(s.pmerge[3 * q + 1])) / e, (eq * vq.y + fromFix(s.pmerge[3 * q + 2])) / e);
+            s.penergy[q] = e;
+            s.plast[q] = ~0ull;
+            return;
+        }
+        if (s.ptarget[q] >= 0) return;
+        const float2 pp = s.ppos[q], pv = s.pvel[q];
+        const int cell = slotHead(s, wi, pp + pv);
+        if (cell < 0) return;
+        if (s.barrier[cell]) {
+            const float2 vc = s.velA[cell];
+            const float2 vr = pv - vc;
+            const float2 r = correctDirection(pp - s.posB[cell], wi.W, wi.H);
+            const float dvr = dot2(vr, r);
+            if (dvr < 0.0f) {
+                const float trr = fmaxf(0.1f, lensq2(r));
+                s.pvel[q] = vr - r * 2.0f * dvr / trr + vc;
+            }
+            return;
+        }
+        const unsigned long long cellId = s.id[cell];
+        if (s.plast[q] == cellId) return;
+        const float absorption = p.radiationAbsorption[s.color[cell] % ALIEN_B200_MAX_COLORS];
+        if (absorption < kNearZero) return;
+        float e = s.penergy[q];
+        float transfer = e * absorption;
+        if (e < 0.01f) transfer = e;
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.energyAcc[cell]), static_cast<unsigned long long>(toFix(transfer)));
+        e -= transfer;
+        s.penergy[q] = e;
+        if (e < kNearZero) {
+            s.palive[q] = 0;
+            atomicAdd(&s.counters[c.w].deadParticles, 1u);
+        } else {
+            s.plast[q] = cellId;
+        }
+    }
+}
+
+// -------------------------------------------------------- kTransition ----
+// cells: living-state transition (CellProcessor.cuh:596-664), inner friction
+// (every third step: one Jacobi sweep with one pair average per bond,
+// CellProcessor.cuh:678-705), absorbed energy.
+// particles: splitting (RadiationProcessor::splitting, :172-204).
+__global__ void __launch_bounds__(kBlock) kTransition(DevState s)
+{
+    if (blockIdx.x < s.numCellBlocks) {
+        CellCtx c = cellCtx(s);
+        if (!c.valid) return;
+        const long long g = c.g;
+        const WorldInfo& wi = s.worlds[c.w];
+        const AlienPhysicsParams& p = s.params[wi.paramIndex];
+        const uint64_t T = s.counters[c.w].timestep;
+        const int n = s.numConn[g];
+        const uint32_t cr = s.creatureId[g];
+        bool sameDetaching = false, otherDetaching = false, sameReviving = false, activating = false;
+        float2 acc = f2(0.0f, 0.0f);
+        const float2 vi = s.velB[g];
+        for (int k = 0; k < n; ++k) {
+            const int j = s.bond[g * kMaxBonds + k];
+            const int ls = s.livingState[j];
+            if (s.creatureId[j] == cr) {
+                if (ls == ALIEN_B200_LIVING_DETACHING) sameDetaching = true;
+                else if (ls == ALIEN_B200_LIVING_REVIVING) sameReviving = true;
+                else if (ls == ALIEN_B200_LIVING_ACTIVATING) activating = true;
+            } else if (ls == ALIEN_B200_LIVING_DETACHING) {
+                otherDetaching = true;
+            }
+            if (!s.barrier[j]) acc = acc + (s.velB[j] - vi);
+        }
+        const int orig = s.livingState[g];
+        int ls = orig;
+        const int dc = p.cellDeathConsequences;
+        if (s.barrier[g])
+            ls = ALIEN_B200_LIVING_READY;
+        else if (orig == ALIEN_B200_LIVING_ACTIVATING || orig == ALIEN_B200_LIVING_REVIVING)
+            ls = ALIEN_B200_LIVING_READY;
+        else if (orig == ALIEN_B200_LIVING_UNDER_CONSTRUCTION) {
+            if (activating) ls = ALIEN_B200_LIVING_ACTIVATING;
+            if (otherDetaching && dc != ALIEN_B200_DEATH_NONE) ls = ALIEN_B200_LIVING_DETACHING;
+        } else if (orig == ALIEN_B200_LIVING_DETACHING) {
+            if (sameReviving && dc == ALIEN_B200_DEATH_DETACHED_PARTS_DIE) ls = ALIEN_B200_LIVING_REVIVING;
+            if (dc == ALIEN_B200_DEATH_NONE) ls = ALIEN_B200_LIVING_READY;
+        } else if (orig == ALIEN_B200_LIVING_READY) {
+            if (sameDetaching && dc != ALIEN_B200_DEATH_NONE) ls = ALIEN_B200_LIVING_DETACHING;
+        }
+        s.nextState[g] = static_cast<uint8_t>(ls);
+        if (T % 3 == 0 && !s.barrier[g])
+            s.velA[g] = vi + acc * (p.innerFriction / 2.0f);
+        else
+            s.velA[g] = vi;
+        s.energy[g] += fromFix(s.energyAcc[g]);
+    } else {
+        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
+        if (!c.inRange) return;
+        const long long q = c.q;
+        const WorldInfo& wi = s.worlds[c.w];
+        if (s.pslot[q] >= 0) s.pmap[wi.pmapBase + s.pslot[q]] = -1;
+        if (!s.palive[q]) return;
+        const AlienPhysicsParams& p = s.params[wi.paramIndex];
+        const uint64_t T = s.counters[c.w].timestep;
+        const unsigned long long id = s.pid[q];
+        if (draw(id, T, kSiteSplit) >= 0.01f) return;
+        float e = s.penergy[q];
+        if (!(e > p.particleSplitEnergy[s.pcolor[q] % ALIEN_B200_MAX_COLORS])) return;
+        e *= 0.5f;
+        s.penergy[q] = e;
+        float2 vp = unitVectorOfAngle(draw(id, T, kSiteSplitAngle) * 360.0f);
+        const float2 pp = s.ppos[q];
+        const float2 otherPos = correctPosition(pp + vp / 5.0f, wi.W, wi.H);
+        s.ppos[q] = correctPosition(pp - vp / 5.0f, wi.W, wi.H);
+        vp = vp * (p.radiationVelocityPerturbation / (e + 1.0f));
+        const float2 pv = s.pvel[q];
+        s.pvel[q] = pv - vp;
+        if (e > kNearZero) {
+            s.splitPos[q] = otherPos;
+            s.splitVel[q] = pv + vp;
+            s.splitEnergy[q] = e;
+            s.pflag[q] |= 2u;
+        }
+    }
+}
+
+// ------------------------------------------------------------- kDecay ----
+// applyFriction + decay (CellProcessor.cuh:707-723, 775-858).
+__global__ void __launch_bounds__(kBlock) kDecay(DevState s)
+{
+    CellCtx c = cellCtx(s);
+    if (!c.valid) return;
+    const long long g = c.g;
+    const WorldInfo& wi = s.worlds[c.w];
+    const AlienPhysicsParams& p = s.params[wi.paramIndex];
+    const uint64_t T = s.counters[c.w].timestep;
+    const int ls = s.nextState[g];
+    s.livingState[g] = static_cast<uint8_t>(ls);
+    if (s.barrier[g]) return;
+    s.velA[g] = s.velA[g] * (1.0f - p.friction);
+    const int col = s.color[g] % ALIEN_B200_MAX_COLORS;
+    const float e = s.energy[g];
+    uint32_t f = 0;
+    if (e > p.cellMaxBindingEnergy) f |= kFlagDelAll;
+    if (ls == ALIEN_B200_LIVING_DYING || ls == ALIEN_B200_LIVING_DETACHING) {
+        if (draw(s.id[g], T, kSiteDeath) < p.cellDeathProbability[col]) f |= kFlagDelCell;
+    }
+    bool destroy = e < p.cellMinEnergy[col];
+    const long long maxAge = p.cellMaxAge[col];
+    if (maxAge > 0 && static_cast<long long>(s.age[g]) > maxAge) destroy = true;
+    if (destroy) {
+        f |= kFlagSetDying;
+        if (ls != ALIEN_B200_LIVING_DYING) {
+            f |= kFlagNewDying;
+            const int n = s.numConn[g];
+            for (int k = 0; k < n; ++k) atomicOr(&s.flags[s.bond[g * kMaxBonds + k]], kFlagDetachFromDying);
+        }
+    }
+    if (f) atomicOr(&s.flags[g], f);
+}
+
+// ---------------------------------------------------- bond additions -----
+// CellConnectionProcessor::tryAddConnectionOneWay (CellConnectionProcessor.cuh
+// :274-427, angle alignment None) on a register copy of the bond list;
+// partner lists are read from the arrays, which no thread changes in this
+// phase.
+struct BondList {
+    int n;
+    int b[kMaxBonds];
+    float d[kMaxBonds], a[kMaxBonds];
+};
+
+__device__ inline void loadBonds(const DevState& s, long long g, BondList& l)
+{
+    l.n = s.numConn[g];
+    for (int k = 0; k < kMaxBonds; ++k) {
+        l.b[k] = s.bond[g * kMaxBonds + k];
+        l.d[k] = s.bondDist[g * kMaxBonds + k];
+        l.a[k] = s.bondAngle[g * kMaxBonds + k];
+    }
+}
+
+__device__ inline bool tryAddOneWay(const DevState& s, const WorldInfo& wi, long long c1, long long c2, float2 posDelta, BondList& out)
+{
+    loadBonds(s, c1, out);
+    const int n = out.n;
+    if (n == kMaxBonds) return false;
+    const float2 p1 = s.posA[c1], p2 = s.posA[c2];
+    if (n >= 2) {  // wouldResultInOverlappingConnection, CellConnectionProcessor.cuh:476-500
+        for (int k = 0; k < n; ++k) {
+            const int cc = out.b[k], nc = out.b[(k + 1) % n];
+            const int ncc = s.numConn[cc];
+            bool both = false;
+            for (int m = 0; m < ncc; ++m) both |= (s.bond[static_cast<long long>(cc) * kMaxBonds + m] == nc);
+            if (!both) continue;
+            if (crossing(p1, p2, s.posA[cc], s.posA[nc])) return false;
+        }
+    }
+    const float newAngle = angleOfVector(posDelta);
+    const float desired = len2(posDelta);
+    if (n == 0) {
+        out.n = 1;
+        out.b[0] = static_cast<int>(c2);
+        out.d[0] = desired;
+        out.a[0] = 360.0f;
+        return true;
+    }
+    if (n == 1) {
+        const float prevAngle = angleOfVector(correctDirection(s.posA[out.b[0]] - p1, wi.W, wi.H));
+        float diff = newAngle - prevAngle;
+        if (diff < 0) diff += 360.0f;
+        if (fabsf(diff) < kNearZero || fabsf(diff - 360.0f) < kNearZero || fabsf(diff + 360.0f) < kNearZero) return false;
+        out.a[1] = diff;
+        out.a[0] = 360.0f - diff;
+        out.n = 2;
+        out.b[1] = static_cast<int>(c2);
+        out.d[1] = desired;
+        return true;
+    }
+    int index = 0;
+    float prevAngle = 0.0f, nextAngle = 0.0f;
+    for (; index < n; ++index) {
+        const int prevIndex = (index + n - 1) % n;
+        prevAngle = angleOfVector(correctDirection(s.posA[out.b[prevIndex]] - p1, wi.W, wi.H));
+        nextAngle = angleOfVector(correctDirection(s.posA[out.b[index]] - p1, wi.W, wi.H));
+        if (isAngleInBetween(prevAngle, nextAngle, newAngle) || prevIndex == index) break;
+    }
+    if (index == n) return false;
+    const float refAngle = out.a[index];
+    const float d1 = subtractAngle(newAngle, prevAngle), d2 = subtractAngle(nextAngle, prevAngle);
+    const float fraction = d2 != 0.0f ? d1 / d2 : 0.5f;
+    const float afp = fminf(refAngle * fraction, refAngle);
+    if (afp < kNearZero) return false;
+    if (index == 0) index = n;
+    for (int j = n; j > index; --j) {
+        out.b[j] = out.b[j - 1];
+        out.d[j] = out.d[j - 1];
+        out.a[j] = out.a[j - 1];
+    }
+    out.b[index] = static_cast<int>(c2);
+    out.d[index] = desired;
+    out.a[index] = afp;
+    out.a[(index + 1) % (n + 1)] = refAngle - afp;
+    out.n = n + 1;
+    return true;
+}
+
+// ----------------------------------------------------------- kResolve ----
+// dying / detaching resolution of decay (CellProcessor.cuh:840-850) and the
+// bond additions of mutually chosen fusion pairs (processAddOperations,
+// CellConnectionProcessor.cuh:130-143, 211-272), written to scratch.
+__global__ void __launch_bounds__(kBlock) kResolve(DevState s)
+{
+    CellCtx c = cellCtx(s);
+    if (!c.valid) return;
+    const long long g = c.g;
+    const uint32_t f = s.flags[g];
+    if (f & kFlagSetDying)
+        s.livingState[g] = ALIEN_B200_LIVING_DYING;
+    else if ((f & kFlagDetachFromDying) && s.livingState[g] != ALIEN_B200_LIVING_DYING)
+        s.livingState[g] = ALIEN_B200_LIVING_DETACHING;
+
+    const int j = s.best[g];
+    if (j < 0 || j <= g || s.best[j] != g) return;
+    const WorldInfo& wi = s.worlds[c.w];
+    const bool gFirst = s.id[g] < s.id[j];
+    const long long c1 = gFirst ? g : j, c2 = gFirst ? j : g;
+    const float2 pd = correctDirection(s.posA[c2] - s.posA[c1], wi.W, wi.H);
+    BondList l1, l2;
+    if (!tryAddOneWay(s, wi, c1, c2, pd, l1)) return;
+    if (!tryAddOneWay(s, wi, c2, c1, pd * -1.0f, l2)) return;
+    const BondList* ls[2] = {&l1, &l2};
+    const long long cs[2] = {c1, c2};
+    for (int m = 0; m < 2; ++m) {
+        const long long x = cs[m];
+        s.addNum[x] = static_cast<uint8_t>(ls[m]->n);
+        for (int k = 0; k < kMaxBonds; ++k) {
+            s.addBond[x * kMaxBonds + k] = k < ls[m]->n ? ls[m]->b[k] : -1;
+            s.addDist[x * kMaxBonds + k] = ls[m]->d[k];
+            s.addAngle[x * kMaxBonds + k] = ls[m]->a[k];
+        }
+    }
+    s.newPartner[c1] = static_cast<int>(c2);
+    s.newPartner[c2] = static_cast<int>(c1);
+}
+
+// ------------------------------------------------------------ kCommit ----
+// bond additions, cell deletion (processDeleteCellOperations,
+// CellConnectionProcessor.cuh:145-174) and bond deletion
+// (processDeleteConnectionOperations :176-209 with deleteConnectionOneWay
+// :429-448): a bond is dropped when its partner is deleted, or when either
+// end scheduled "delete all bonds" and the bond is not this step's addition.
+__global__ void __launch_bounds__(kBlock) kCommit(DevState s)
+{
+    CellCtx c = cellCtx(s);
+    if (!c.valid) return;
+    const long long g = c.g;
+    const uint32_t f = s.flags[g];
+    if (f & kFlagDelCell) {
+        s.alive[g] = 0;
+        atomicAdd(&s.counters[c.w].deadCells, 1u);
+        return;
+    }
+    const int np = s.newPartner[g];
+    BondList l;
+    if (np >= 0) {
+        l.n = s.addNum[g];
+        for (int k = 0; k < kMaxBonds; ++k) {
+            l.b[k] = s.addBond[g * kMaxBonds + k];
+            l.d[k] = s.addDist[g * kMaxBonds + k];
+            l.a[k] = s.addAngle[g * kMaxBonds + k];
+        }
+    } else {
+        loadBonds(s, g, l);
+    }
+    const bool delAllG = f & kFlagDelAll;
+    int drop[kMaxBonds];
+    int nd = 0;
+    for (int k = 0; k < l.n; ++k) {
+        const int j = l.b[k];
+        const uint32_t fj = s.flags[j];
+        if ((fj & kFlagDelCell) || ((delAllG || (fj & kFlagDelAll)) && j != np)) drop[nd++] = j;
+    }
+    if (np < 0 && nd == 0) return;
+    for (int m = 0; m < nd; ++m) {
+        const int n = l.n;
+        for (int k = 0; k < n; ++k) {
+            if (l.b[k] != drop[m]) continue;
+            const float add = l.a[k];
+            for (int j = k; j < n - 1; ++j) {
+                l.b[j] = l.b[j + 1];
+                l.d[j] = l.d[j + 1];
+                l.a[j] = l.a[j + 1];
+            }
+            if (k < n - 1)
+                l.a[k] += add;
+            else
+                l.a[0] += add;
+            l.b[n - 1] = -1;
+            l.n = n - 1;
+            break;
+        }
+    }
+    s.numConn[g] = static_cast<uint8_t>(l.n);
+    for (int k = 0; k < kMaxBonds; ++k) {
+        s.bond[g * kMaxBonds + k] = k < l.n ? l.b[k] : -1;
+        s.bondDist[g * kMaxBonds + k] = l.d[k];
+        s.bondAngle[g * kMaxBonds + k] = l.a[k];
+    }
+}
+
+// ------------------------------------------------------------- events ----
+// New energy particles (RadiationProcessor::createEnergyParticle without
+// sources, :248-364, and ObjectFactory::createParticle, ObjectFactory.cuh
+// :242-256) in the order radiation (cell order), splitting (particle order),
+// deleted cells (cell order); ids continue the world's id counter.
+__device__ __forceinline__ bool delEvent(const DevState& s, long long g)
+{
+    return (s.flags[g] & kFlagDelCell) && s.energy[g] > kNearZero;
+}
+
+__global__ void __launch_bounds__(kBlock) kEventCount(DevState s)
+{
+    __shared__ uint32_t red[2][kBlock / 32];
+    uint32_t a = 0, b = 0;
+    if (blockIdx.x < s.numCellBlocks) {
+        const long long g = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+        const int w = s.cellBlockWorld[blockIdx.x];
+        if (g < s.worlds[w].cellBase + s.counters[w].numCells) {
+            a = (s.flags[g] & kFlagRadiation) ? 1u : 0u;
+            b = delEvent(s, g) ? 1u : 0u;
+        }
+    } else {
+        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
+        if (c.inRange) a = (s.pflag[c.q] & 2u) ? 1u : 0u;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    a = __reduce_add_sync(0xffffffffu, a);
+    b = __reduce_add_sync(0xffffffffu, b);
+    if (lane == 0) {
+        red[0][warp] = a;
+        red[1][warp] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t ta = 0, tb = 0;
+        for (int i = 0; i < kBlock / 32; ++i) {
+            ta += red[0][i];
+            tb += red[1][i];
+        }
+        if (blockIdx.x < s.numCellBlocks) {
+            s.blockRad[blockIdx.x] = ta;
+            s.blockDel[blockIdx.x] = tb;
+        } else {
+            s.blockSplit[blockIdx.x - s.numCellBlocks] = ta;
+        }
+    }
+}
+
+__device__ uint32_t warpScanBlocks(uint32_t* arr, int first, int count)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t carry = 0;
+    for (int base = 0; base < count; base += 32) {
+        const int k = base + lane;
+        const uint32_t v = k < count ? arr[first + k] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (k < count) arr[first + k] = carry + x - v;
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+    return carry;
+}
+
+// one warp per world: block offsets, id and slot bases, timestep advance
+__global__ void kEventWorld(DevState s)
+{
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= s.numWorlds) return;
+    const WorldInfo& wi = s.worlds[w];
+    const uint32_t R = warpScanBlocks(s.blockRad, wi.firstCellBlock, wi.numCellBlocks);
+    const uint32_t D = warpScanBlocks(s.blockDel, wi.firstCellBlock, wi.numCellBlocks);
+    const uint32_t S = warpScanBlocks(s.blockSplit, wi.firstPartBlock, wi.numPartBlocks);
+    if ((threadIdx.x & 31) != 0) return;
+    WorldCounters& wc = s.counters[w];
+    const unsigned long long id0 = wc.nextId;
+    const uint32_t slot0 = wc.numParticles;
+    wc.radIdBase = id0;
+    wc.splitIdBase = id0 + R;
+    wc.delIdBase = id0 + R + S;
+    wc.radSlotBase = slot0;
+    wc.splitSlotBase = slot0 + R;
+    wc.delSlotBase = slot0 + R + S;
+    wc.numEvents = R + S + D;
+    wc.nextId = id0 + R + S + D;
+    const unsigned long long want = static_cast<unsigned long long>(slot0) + R + S + D;
+    if (want > static_cast<unsigned long long>(wi.partCap)) {
+        wc.droppedParticles += static_cast<uint32_t>(want - wi.partCap);
+        wc.numParticles = static_cast<uint32_t>(wi.partCap);
+        atomicOr(s.errorFlags, 1u);
+    } else {
+        wc.numParticles = static_cast<uint32_t>(want);
+    }
+    wc.timestep += 1;
+}
+
+__device__ __forceinline__ void emitParticle(const DevState& s, const WorldInfo& wi, uint32_t slotRel, unsigned long long id,
+                                             float2 pos, float2 vel, float energy, uint8_t color)
+{
+    if (slotRel >= wi.partCap) return;
+    const long long q = wi.partBase + slotRel;
+    pos = correctPosition(pos, wi.W, wi.H);
+    s.pid[q] = id;
+    s.ppos[q] = pos;
+    s.pvel[q] = vel;
+    s.penergy[q] = energy;
+    s.pcolor[q] = color;
+    s.pselected[q] = 0;
+    s.palive[q] = 1;
+    s.plast[q] = ~0ull;
+}
+
+__global__ void __launch_bounds__(kBlock) kEventEmit(DevState s)
+{
+    if (blockIdx.x < s.numCellBlocks) {
+        const int w = s.cellBlockWorld[blockIdx.x];
+        const WorldCounters& wc = s.counters[w];
+        if (wc.numEvents == 0) return;
+        const WorldInfo& wi = s.worlds[w];
+        const long long g = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+        const bool inRange = g < wi.cellBase + wc.numCells;
+        const uint32_t rad = inRange && (s.flags[g] & kFlagRadiation) ? 1u : 0u;
+        const uint32_t del = inRange && delEvent(s, g) ? 1u : 0u;
+        const uint32_t rr = blockExclusiveScan(rad, nullptr) + s.blockRad[blockIdx.x];
+        const uint32_t dr = blockExclusiveScan(del, nullptr) + s.blockDel[blockIdx.x];
+        if (rad) emitParticle(s, wi, wc.radSlotBase + rr, wc.radIdBase + rr, s.radPos[g], s.radVel[g], s.radEnergy[g], s.color[g]);
+        if (del) emitParticle(s, wi, wc.delSlotBase + dr, wc.delIdBase + dr, s.posA[g], s.velA[g], s.energy[g], s.color[g]);
+    } else {
+        const int pb = blockIdx.x - s.numCellBlocks;
+        const int w = s.partBlockWorld[pb];
+        const WorldCounters& wc = s.counters[w];
+        if (wc.numEvents == 0) return;
+        const WorldInfo& wi = s.worlds[w];
+        const long long q = static_cast<long long>(pb) * kBlock + threadIdx.x;
+        // particles appended by this step sit beyond the old count: their
+        // pflag is clear (reset in kBin for the whole range)
+        const uint32_t split = (s.pflag[q] & 2u) ? 1u : 0u;
+        const uint32_t sr = blockExclusiveScan(split, nullptr) + s.blockSplit[pb];
+        if (split) emitParticle(s, wi, wc.splitSlotBase + sr, wc.splitIdBase + sr, s.splitPos[q], s.splitVel[q], s.splitEnergy[q], s.pcolor[q]);
+    }
+}
+
+}  // namespace ab

@@ -1,0 +1,182 @@
+"""Python mirror of the reference's engine surface for the physics stage.
+
+``SimulationFacade`` follows ``_SimulationFacade``
+(source/EngineInterface/SimulationFacade.h:13-110) at the DataTO level of
+``_SimulationCudaFacade`` (source/EngineGpuKernels/SimulationCudaFacade.cuh
+:27-139): the same operations, argument meaning and error behaviour
+(failures raise).  Every call goes through the C ABI of ``libalien_b200.so``.
+``BatchSimulation`` steps many worlds in one arena.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import ArraySizes, GeneralSettings, Int2, RawStatistics, check
+from .params import PhysicsParams
+from .to import CELL_TO, PARTICLE_TO, DataTO
+
+
+class SimulationFacade:
+    """One world on the current CUDA device."""
+
+    def __init__(self):
+        self._lib = _lib.load()
+        self._h = ctypes.c_void_p()
+        self._world = None
+
+    # _SimulationFacade::newSimulation (SimulationFacade.h:18)
+    def new_simulation(self, timestep: int, world_size, parameters: PhysicsParams) -> None:
+        self.close_simulation()
+        g = GeneralSettings(int(world_size[0]), int(world_size[1]))
+        check(self._lib.alien_b200_create(ctypes.byref(g), ctypes.byref(parameters), int(timestep), ctypes.byref(self._h)))
+        self._world = (int(world_size[0]), int(world_size[1]))
+
+    # closeSimulation (:67)
+    def close_simulation(self) -> None:
+        if self._h:
+            check(self._lib.alien_b200_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close_simulation()
+        except Exception:
+            pass
+
+    def _handle(self):
+        if not self._h:
+            raise RuntimeError("no simulation: call new_simulation first")
+        return self._h
+
+    @property
+    def world_size(self):
+        return self._world
+
+    # calcTimesteps (:60)
+    def calc_timesteps(self, timesteps: int) -> None:
+        check(self._lib.alien_b200_calc_timesteps(self._handle(), int(timesteps)))
+
+    def enqueue_timesteps(self, timesteps: int) -> None:
+        check(self._lib.alien_b200_enqueue_timesteps(self._handle(), int(timesteps)))
+
+    # setSimulationData (:47)
+    def set_simulation_data(self, data: DataTO) -> None:
+        check(self._lib.alien_b200_set_data(self._handle(), ctypes.cast(data.c_ptr(), ctypes.c_void_p)))
+
+    # getSimulationData (:40); the reference reads the world +- 10
+    # (EngineImpl/SimulationFacadeImpl.cpp:87-91)
+    def get_simulation_data(self, upper_left=None, lower_right=None, out: DataTO | None = None) -> DataTO:
+        if upper_left is None:
+            upper_left = (-10, -10)
+        if lower_right is None:
+            lower_right = (self._world[0] + 10, self._world[1] + 10)
+        if out is None:
+            sizes = self.get_array_sizes()
+            out = DataTO(np.zeros(0, CELL_TO), np.zeros(0, PARTICLE_TO), None, cell_capacity=sizes.cellArraySize,
+                         particle_capacity=sizes.particleArraySize, aux_capacity=sizes.auxiliaryDataSize)
+        check(self._lib.alien_b200_get_data(self._handle(), Int2(*upper_left), Int2(*lower_right),
+                                            ctypes.cast(out.c_ptr(), ctypes.c_void_p)))
+        return out
+
+    # get/setSimulationParameters (:75-79)
+    def set_simulation_parameters(self, parameters: PhysicsParams) -> None:
+        check(self._lib.alien_b200_set_parameters(self._handle(), ctypes.byref(parameters)))
+
+    def get_simulation_parameters(self) -> PhysicsParams:
+        p = PhysicsParams()
+        check(self._lib.alien_b200_get_parameters(self._handle(), ctypes.byref(p)))
+        return p
+
+    def get_array_sizes(self) -> ArraySizes:
+        s = ArraySizes()
+        check(self._lib.alien_b200_get_array_sizes(self._handle(), ctypes.byref(s)))
+        return s
+
+    def resize_arrays_if_necessary(self, cells: int = 0, particles: int = 0, aux: int = 0) -> None:
+        s = ArraySizes(cells, particles, aux)
+        check(self._lib.alien_b200_resize_arrays_if_necessary(self._handle(), ctypes.byref(s)))
+
+    # getCurrentTimestep / setCurrentTimestep (:69-70)
+    def get_current_timestep(self) -> int:
+        t = ctypes.c_uint64()
+        check(self._lib.alien_b200_get_current_timestep(self._handle(), ctypes.byref(t)))
+        return t.value
+
+    def set_current_timestep(self, timestep: int) -> None:
+        check(self._lib.alien_b200_set_current_timestep(self._handle(), int(timestep)))
+
+    def clear(self) -> None:
+        check(self._lib.alien_b200_clear(self._handle()))
+
+    # getRawStatistics (:98)
+    def get_raw_statistics(self) -> RawStatistics:
+        r = RawStatistics()
+        check(self._lib.alien_b200_get_raw_statistics(self._handle(), ctypes.byref(r)))
+        return r
+
+    def stream(self) -> int:
+        return int(self._lib.alien_b200_stream(self._handle()) or 0)
+
+    def kernel_launches(self) -> int:
+        return int(self._lib.alien_b200_kernel_launch_count(self._handle()))
+
+
+class BatchSimulation:
+    """Many independent worlds stepped together in one arena."""
+
+    def __init__(self, worlds, timestep: int = 0):
+        """``worlds``: list of (DataTO, (sizeX, sizeY), PhysicsParams)."""
+        self._lib = _lib.load()
+        n = len(worlds)
+        self._datas = [w[0] for w in worlds]
+        self._sizes = [tuple(w[1]) for w in worlds]
+        gs = (GeneralSettings * n)(*[GeneralSettings(int(s[0]), int(s[1])) for s in self._sizes])
+        ps = (PhysicsParams * n)(*[w[2] for w in worlds])
+        from .to import CDataTO
+        tos = (CDataTO * n)(*[d._c for d in self._datas])
+        self._h = ctypes.c_void_p()
+        check(self._lib.alien_b200_batch_create(n, gs, ps, ctypes.cast(tos, ctypes.c_void_p), int(timestep),
+                                                ctypes.byref(self._h)))
+        self.num_worlds = n
+
+    def close(self) -> None:
+        if self._h:
+            check(self._lib.alien_b200_batch_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def calc_timesteps(self, timesteps: int) -> None:
+        check(self._lib.alien_b200_batch_calc_timesteps(self._h, int(timesteps)))
+
+    def enqueue_timesteps(self, timesteps: int) -> None:
+        check(self._lib.alien_b200_batch_enqueue_timesteps(self._h, int(timesteps)))
+
+    def get_simulation_data(self, world: int) -> DataTO:
+        s = ArraySizes()
+        check(self._lib.alien_b200_batch_get_array_sizes(self._h, int(world), ctypes.byref(s)))
+        out = DataTO(np.zeros(0, CELL_TO), np.zeros(0, PARTICLE_TO), None, cell_capacity=s.cellArraySize,
+                     particle_capacity=s.particleArraySize, aux_capacity=s.auxiliaryDataSize)
+        check(self._lib.alien_b200_batch_get_data(self._h, int(world), ctypes.cast(out.c_ptr(), ctypes.c_void_p)))
+        return out
+
+    def get_raw_statistics(self, world: int) -> RawStatistics:
+        r = RawStatistics()
+        check(self._lib.alien_b200_batch_get_raw_statistics(self._h, int(world), ctypes.byref(r)))
+        return r
+
+    def stream(self) -> int:
+        return int(self._lib.alien_b200_batch_stream(self._h) or 0)
+
+    def kernel_launches(self) -> int:
+        return int(self._lib.alien_b200_batch_kernel_launch_count(self._h))
+
+    def kernels_per_step(self) -> int:
+        return int(self._lib.alien_b200_batch_kernels_per_step(self._h))

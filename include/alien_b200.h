@@ -1,0 +1,329 @@
+/*
+ * alien_b200.h - C ABI of the B200-native ALIEN physics-stage engine.
+ *
+ * The functions below replace, one for one, the engine surface that the
+ * reference's host code drives for the per-timestep physics stage:
+ *
+ *   reference (chrxh/alien 4.12.2)                          this ABI
+ *   -----------------------------------------------------   -------------------------------
+ *   _SimulationCudaFacade(timestep, Settings)                alien_b200_create
+ *     source/EngineGpuKernels/SimulationCudaFacade.cuh:37
+ *   ~_SimulationCudaFacade()            (.cu:89-112)         alien_b200_destroy
+ *   calcTimestep(timesteps, forceUpdateStatistics)  (:42)    alien_b200_calc_timesteps
+ *   setSimulationData(DataTO const&)                (:51)    alien_b200_set_data
+ *   getSimulationData(upperLeft, lowerRight, DataTO) (:46)   alien_b200_get_data
+ *   setSimulationParameters(SimulationParameters)  (:74-76)  alien_b200_set_parameters
+ *   getSimulationParameters()                       (:73)    alien_b200_get_parameters
+ *   getArraySizes()                                 (:78)    alien_b200_get_array_sizes
+ *   resizeArraysIfNecessary(ArraySizes)             (:91)    alien_b200_resize_arrays_if_necessary
+ *   getCurrentTimestep / setCurrentTimestep      (:86-87)    alien_b200_get/set_current_timestep
+ *   clear()                                         (:89)    alien_b200_clear
+ *   getRawStatistics()                              (:80)    alien_b200_get_raw_statistics
+ *
+ * Data crosses the boundary in the reference's own transfer format: the
+ * structs AlienCellTO / AlienParticleTO / AlienDataTO below are byte-for-byte
+ * the reference's CellTO / ParticleTO / DataTO
+ * (source/EngineGpuKernels/TOs.cuh:10-236); the static asserts at the end pin
+ * every offset.  Parameters cross as AlienPhysicsParams, the subset of
+ * SimulationParameters (source/EngineInterface/SimulationParameters.h:18-206)
+ * that the physics stage reads, with the reference's field names.
+ *
+ * Conventions: every function returns an int status (ALIEN_B200_OK == 0);
+ * no C++ exception crosses the ABI; alien_b200_last_error() returns the text
+ * of the last failure on the calling thread.  A handle is not thread-safe:
+ * callers serialise calls per handle (the reference does the same through
+ * EngineWorkerGuard, source/EngineImpl/EngineWorker.cpp:608-632).
+ */
+#ifndef ALIEN_B200_H
+#define ALIEN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALIEN_B200_MAX_CELL_BONDS 6  /* EngineInterface/EngineConstants.h:3 */
+#define ALIEN_B200_MAX_CHANNELS 8    /* EngineInterface/EngineConstants.h:4 */
+#define ALIEN_B200_MAX_COLORS 7      /* EngineInterface/EngineConstants.h:6 */
+
+/* status codes */
+#define ALIEN_B200_OK 0
+#define ALIEN_B200_ERR_INVALID_ARGUMENT 1
+#define ALIEN_B200_ERR_OUT_OF_MEMORY 2
+#define ALIEN_B200_ERR_CUDA 3
+#define ALIEN_B200_ERR_DEVICE_FLAG 4
+#define ALIEN_B200_ERR_UNSUPPORTED 5
+#define ALIEN_B200_ERR_CAPACITY 6
+#define ALIEN_B200_ERR_NO_DEVICE 7
+
+/* motion types, EngineInterface/Motion.h:38-43 */
+#define ALIEN_B200_MOTION_FLUID 0
+#define ALIEN_B200_MOTION_COLLISION 1
+
+/* living states, EngineInterface/CellFunctionConstants.h:25-35 */
+#define ALIEN_B200_LIVING_READY 0
+#define ALIEN_B200_LIVING_UNDER_CONSTRUCTION 1
+#define ALIEN_B200_LIVING_ACTIVATING 2
+#define ALIEN_B200_LIVING_DETACHING 3
+#define ALIEN_B200_LIVING_REVIVING 4
+#define ALIEN_B200_LIVING_DYING 5
+
+/* cell death consequences, EngineInterface/SimulationParametersTypes.h */
+#define ALIEN_B200_DEATH_NONE 0
+#define ALIEN_B200_DEATH_CREATURE_DIES 1
+#define ALIEN_B200_DEATH_DETACHED_PARTS_DIE 2
+
+#define ALIEN_B200_CELL_FUNCTION_CONSTRUCTOR 2
+#define ALIEN_B200_CELL_FUNCTION_NONE 11
+
+#if defined(__cplusplus)
+#define ALIEN_B200_ALIGN8 alignas(8)
+#else
+#define ALIEN_B200_ALIGN8 _Alignas(8)
+#endif
+
+/* float2 / int2 with CUDA's alignment (float2 is 8-byte aligned) */
+typedef struct AlienFloat2 {
+    ALIEN_B200_ALIGN8 float x;
+    float y;
+} AlienFloat2;
+
+typedef struct AlienInt2 {
+    int32_t x;
+    int32_t y;
+} AlienInt2;
+
+/* ConnectionTO, TOs.cuh:30-35 */
+typedef struct AlienConnectionTO {
+    int32_t cellIndex; /* index into the same cell array */
+    float distance;
+    float angleFromPrevious;
+} AlienConnectionTO;
+
+/* SignalTO, TOs.cuh:37-43 */
+typedef struct AlienSignalTO {
+    float channels[ALIEN_B200_MAX_CHANNELS];
+    uint8_t origin;
+    float targetX;
+    float targetY;
+} AlienSignalTO;
+
+/* CellMetadataTO, TOs.cuh:21-28 */
+typedef struct AlienCellMetadataTO {
+    uint16_t nameSize;
+    uint64_t nameDataIndex;
+    uint16_t descriptionSize;
+    uint64_t descriptionDataIndex;
+} AlienCellMetadataTO;
+
+/* CellTO, TOs.cuh:158-193 (304 bytes).  The cell-function union
+ * (CellFunctionTO, TOs.cuh:143-156, 64 bytes) is carried opaquely: the
+ * physics stage never reads it, and egress returns it unchanged. */
+typedef struct AlienCellTO {
+    uint64_t id;
+    AlienConnectionTO connections[ALIEN_B200_MAX_CELL_BONDS];
+    AlienFloat2 pos;
+    AlienFloat2 vel;
+    float energy;
+    float stiffness;
+    uint8_t color;
+    uint8_t maxConnections;
+    uint8_t numConnections;
+    uint8_t barrier;
+    uint32_t age;
+    int32_t livingState;
+    uint32_t creatureId;
+    uint32_t mutationId;
+    uint8_t ancestorMutationId;
+    float genomeComplexity;
+    uint8_t executionOrderNumber;
+    int8_t inputExecutionOrderNumber;
+    uint8_t outputBlocked;
+    int32_t cellFunction;
+    uint64_t cellFunctionData[8];
+    AlienSignalTO signal;
+    uint32_t activationTime;
+    uint16_t detectedByCreatureId;
+    uint8_t cellFunctionUsed;
+    AlienCellMetadataTO metadata;
+    uint8_t selected;
+} AlienCellTO;
+
+/* ParticleTO, TOs.cuh:10-19 (40 bytes) */
+typedef struct AlienParticleTO {
+    uint64_t id;
+    float energy;
+    AlienFloat2 pos;
+    AlienFloat2 vel;
+    uint8_t color;
+    uint8_t selected;
+} AlienParticleTO;
+
+/* DataTO, TOs.cuh:195-236: caller-owned host buffers */
+typedef struct AlienDataTO {
+    uint64_t* numCells;
+    AlienCellTO* cells;
+    uint64_t* numParticles;
+    AlienParticleTO* particles;
+    uint64_t* numAuxiliaryData;
+    uint8_t* auxiliaryData;
+} AlienDataTO;
+
+/* ArraySizes, EngineInterface/ArraySizes.h:5-10 */
+typedef struct AlienArraySizes {
+    uint64_t cellArraySize;
+    uint64_t particleArraySize;
+    uint64_t auxiliaryDataSize;
+} AlienArraySizes;
+
+/* GeneralSettings, EngineInterface/GeneralSettings.h:3-7 */
+typedef struct AlienGeneralSettings {
+    int32_t worldSizeX;
+    int32_t worldSizeY;
+} AlienGeneralSettings;
+
+/* The physics-stage subset of SimulationParameters
+ * (EngineInterface/SimulationParameters.h:18-206, base values from
+ * SimulationParametersZoneValues.h:10-30, motion from Motion.h:7-36).
+ * alien_b200_default_parameters() fills the reference defaults. */
+typedef struct AlienPhysicsParams {
+    float timestepSize;                       /* SimulationParameters.h:61 */
+    int32_t motionType;                       /* :62 */
+    float smoothingLength;                    /* Motion.h:9 */
+    float viscosityStrength;                  /* Motion.h:10 */
+    float pressureStrength;                   /* Motion.h:11 */
+    float cellMaxCollisionDistance;           /* Motion.h:22 */
+    float cellRepulsionStrength;              /* Motion.h:23 */
+    float innerFriction;                      /* :65 */
+    float cellMaxVelocity;                    /* :66 */
+    float cellMaxBindingDistance[ALIEN_B200_MAX_COLORS]; /* :67 */
+    float cellMinDistance;                    /* :70 */
+    float cellMaxForceDecayProb;              /* :71 */
+    float radiationProb;                      /* :79 */
+    float radiationVelocityMultiplier;        /* :80 */
+    float radiationVelocityPerturbation;      /* :81 */
+    int32_t radiationMinCellAge[ALIEN_B200_MAX_COLORS];  /* :82 */
+    float highRadiationFactor[ALIEN_B200_MAX_COLORS];    /* :85 */
+    float highRadiationMinCellEnergy[ALIEN_B200_MAX_COLORS]; /* :86 */
+    int32_t cellDeathConsequences;            /* :87 */
+    int32_t cellMaxAge[ALIEN_B200_MAX_COLORS];           /* :88 */
+    float particleSplitEnergy[ALIEN_B200_MAX_COLORS];    /* :114 */
+    /* baseValues (SimulationParametersZoneValues.h) */
+    float friction;                           /* :12 */
+    float rigidity;                           /* :13 */
+    float radiationAbsorption[ALIEN_B200_MAX_COLORS];    /* :14 */
+    float radiationCellAgeStrength[ALIEN_B200_MAX_COLORS]; /* :17 */
+    float cellMaxForce[ALIEN_B200_MAX_COLORS];           /* :19 */
+    float cellMinEnergy[ALIEN_B200_MAX_COLORS];          /* :20 */
+    float cellDeathProbability[ALIEN_B200_MAX_COLORS];   /* :21 */
+    float cellFusionVelocity;                 /* :23 */
+    float cellMaxBindingEnergy;               /* :24 */
+    /* features and subsystems outside the physics stage: must be zero
+     * (checked; a nonzero value returns ALIEN_B200_ERR_UNSUPPORTED) */
+    int32_t numZones;                         /* :39 */
+    int32_t numRadiationSources;              /* :27 */
+    uint8_t particleTransformationAllowed;    /* :111 */
+    uint8_t cellAgeLimiter;                   /* Features.h */
+    uint8_t cellColorTransitionRules;         /* Features.h */
+    uint8_t advancedAbsorptionControl;        /* Features.h */
+    uint8_t externalEnergyControl;            /* Features.h */
+    uint8_t reserved[3];
+} AlienPhysicsParams;
+
+/* Subset of RawStatisticsData (EngineGpuKernels/SimulationStatistics.cuh)
+ * that the physics stage maintains. */
+typedef struct AlienRawStatistics {
+    uint64_t timestep;
+    uint64_t numCells;
+    uint64_t numParticles;
+    uint64_t numConnections;          /* directed bonds: sum of numConnections */
+    uint64_t numCellsByColor[ALIEN_B200_MAX_COLORS];
+    double totalCellEnergy;
+    double totalParticleEnergy;
+} AlienRawStatistics;
+
+typedef struct alien_b200_simulation alien_b200_simulation;
+
+/* library / defaults */
+int alien_b200_version(void);
+void alien_b200_default_parameters(AlienPhysicsParams* params);
+int alien_b200_last_error(char* buffer, size_t size);
+
+/* facade.  alien_b200_create replaces the _SimulationCudaFacade constructor
+ * (SimulationCudaFacade.cu:51-87): it selects the device (the current CUDA
+ * device of the calling thread), and allocates the world-sized structures. */
+int alien_b200_create(const AlienGeneralSettings* general, const AlienPhysicsParams* params,
+                      uint64_t timestep, alien_b200_simulation** out);
+int alien_b200_destroy(alien_b200_simulation* sim);
+int alien_b200_calc_timesteps(alien_b200_simulation* sim, uint64_t timesteps);
+int alien_b200_set_data(alien_b200_simulation* sim, const AlienDataTO* data);
+int alien_b200_get_data(alien_b200_simulation* sim, AlienInt2 upperLeft, AlienInt2 lowerRight,
+                        const AlienDataTO* data);
+int alien_b200_set_parameters(alien_b200_simulation* sim, const AlienPhysicsParams* params);
+int alien_b200_get_parameters(alien_b200_simulation* sim, AlienPhysicsParams* params);
+int alien_b200_get_array_sizes(alien_b200_simulation* sim, AlienArraySizes* sizes);
+int alien_b200_resize_arrays_if_necessary(alien_b200_simulation* sim, const AlienArraySizes* additionals);
+int alien_b200_get_current_timestep(alien_b200_simulation* sim, uint64_t* timestep);
+int alien_b200_set_current_timestep(alien_b200_simulation* sim, uint64_t timestep);
+int alien_b200_clear(alien_b200_simulation* sim);
+int alien_b200_get_raw_statistics(alien_b200_simulation* sim, AlienRawStatistics* statistics);
+
+/* Device-resident timing hook: steps `timesteps` times on the handle's
+ * stream without the end-of-call synchronisation and error read-back that
+ * alien_b200_calc_timesteps performs.  For benchmarks that bracket the
+ * steps with their own events; errors surface at the next synchronising
+ * call.  No counterpart in the reference (its calcTimestep synchronises
+ * after every step, SimulationCudaFacade.cu:578-582). */
+int alien_b200_enqueue_timesteps(alien_b200_simulation* sim, uint64_t timesteps);
+/* The CUDA stream (cudaStream_t) all of the handle's work is issued on. */
+void* alien_b200_stream(alien_b200_simulation* sim);
+/* Number of kernel launches issued by the handle since creation. */
+uint64_t alien_b200_kernel_launch_count(alien_b200_simulation* sim);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+/* ---- layout pins: must equal the reference's TOs.cuh layout ---- */
+#ifdef __cplusplus
+#define ALIEN_B200_STATIC_ASSERT(c, m) static_assert(c, m)
+#else
+#define ALIEN_B200_STATIC_ASSERT(c, m) _Static_assert(c, m)
+#endif
+ALIEN_B200_STATIC_ASSERT(sizeof(AlienCellTO) == 304, "CellTO is 304 bytes");
+ALIEN_B200_STATIC_ASSERT(sizeof(AlienParticleTO) == 40, "ParticleTO is 40 bytes");
+ALIEN_B200_STATIC_ASSERT(sizeof(AlienConnectionTO) == 12, "ConnectionTO is 12 bytes");
+ALIEN_B200_STATIC_ASSERT(sizeof(AlienSignalTO) == 44, "SignalTO is 44 bytes");
+ALIEN_B200_STATIC_ASSERT(sizeof(AlienCellMetadataTO) == 32, "CellMetadataTO is 32 bytes");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, connections) == 8, "CellTO.connections");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, pos) == 80, "CellTO.pos");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, vel) == 88, "CellTO.vel");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, energy) == 96, "CellTO.energy");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, stiffness) == 100, "CellTO.stiffness");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, color) == 104, "CellTO.color");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, barrier) == 107, "CellTO.barrier");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, age) == 108, "CellTO.age");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, livingState) == 112, "CellTO.livingState");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, creatureId) == 116, "CellTO.creatureId");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, ancestorMutationId) == 124, "CellTO.ancestorMutationId");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, genomeComplexity) == 128, "CellTO.genomeComplexity");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, executionOrderNumber) == 132, "CellTO.executionOrderNumber");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, cellFunction) == 136, "CellTO.cellFunction");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, cellFunctionData) == 144, "CellTO.cellFunctionData");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, signal) == 208, "CellTO.signal");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, activationTime) == 252, "CellTO.activationTime");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, detectedByCreatureId) == 256, "CellTO.detectedByCreatureId");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, cellFunctionUsed) == 258, "CellTO.cellFunctionUsed");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, metadata) == 264, "CellTO.metadata");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellTO, selected) == 296, "CellTO.selected");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienParticleTO, energy) == 8, "ParticleTO.energy");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienParticleTO, pos) == 16, "ParticleTO.pos");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienParticleTO, vel) == 24, "ParticleTO.vel");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienParticleTO, color) == 32, "ParticleTO.color");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienSignalTO, targetX) == 36, "SignalTO.targetX");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellMetadataTO, nameDataIndex) == 8, "CellMetadataTO.nameDataIndex");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellMetadataTO, descriptionDataIndex) == 24, "CellMetadataTO.descriptionDataIndex");
+
+#endif /* ALIEN_B200_H */

@@ -1,0 +1,42 @@
+/*
+ * alien_b200_batch.h - batched multi-world stepping on one GPU.
+ *
+ * No counterpart in the reference: its facade owns exactly one world
+ * (_SimulationCudaFacade, source/EngineGpuKernels/SimulationCudaFacade.cuh
+ * :27-139).  A batch holds many independent worlds of different sizes and
+ * parameters in one device arena; one timestep of all of them is one launch
+ * per phase, replayed from a CUDA graph.  Each world evolves exactly as it
+ * would alone in an alien_b200_simulation (same deterministic step).
+ */
+#ifndef ALIEN_B200_BATCH_H
+#define ALIEN_B200_BATCH_H
+
+#include "alien_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct alien_b200_batch alien_b200_batch;
+
+/* general[w], params[w], data[w] describe world w (0 <= w < numWorlds). */
+int alien_b200_batch_create(int numWorlds, const AlienGeneralSettings* general, const AlienPhysicsParams* params,
+                            const AlienDataTO* data, uint64_t timestep, alien_b200_batch** out);
+int alien_b200_batch_destroy(alien_b200_batch* batch);
+int alien_b200_batch_num_worlds(alien_b200_batch* batch);
+/* steps every world `timesteps` times and synchronises */
+int alien_b200_batch_calc_timesteps(alien_b200_batch* batch, uint64_t timesteps);
+/* enqueues the steps on the batch's stream without synchronising */
+int alien_b200_batch_enqueue_timesteps(alien_b200_batch* batch, uint64_t timesteps);
+int alien_b200_batch_get_data(alien_b200_batch* batch, int world, const AlienDataTO* data);
+int alien_b200_batch_get_array_sizes(alien_b200_batch* batch, int world, AlienArraySizes* sizes);
+int alien_b200_batch_get_raw_statistics(alien_b200_batch* batch, int world, AlienRawStatistics* statistics);
+void* alien_b200_batch_stream(alien_b200_batch* batch);
+uint64_t alien_b200_batch_kernel_launch_count(alien_b200_batch* batch);
+int alien_b200_batch_kernels_per_step(alien_b200_batch* batch);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* ALIEN_B200_BATCH_H */
