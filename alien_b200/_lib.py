@@ -57,16 +57,17 @@ class RawStatistics(ctypes.Structure):
 
 # every symbol declared in include/alien_b200.h and include/alien_b200_batch.h
 EXPORTED_SYMBOLS = [
-    "alien_b200_version", "alien_b200_default_parameters", "alien_b200_last_error", "alien_b200_create",
+    "alien_b200_version", "alien_b200_select_device", "alien_b200_time_timesteps",
+    "alien_b200_batch_time_timesteps", "alien_b200_default_parameters", "alien_b200_last_error", "alien_b200_create",
     "alien_b200_destroy", "alien_b200_calc_timesteps", "alien_b200_set_data", "alien_b200_get_data",
     "alien_b200_set_parameters", "alien_b200_get_parameters", "alien_b200_get_array_sizes",
     "alien_b200_resize_arrays_if_necessary", "alien_b200_get_current_timestep", "alien_b200_set_current_timestep",
     "alien_b200_clear", "alien_b200_get_raw_statistics", "alien_b200_enqueue_timesteps", "alien_b200_stream",
-    "alien_b200_kernel_launch_count",
+    "alien_b200_kernel_launch_count", "alien_b200_timed_timesteps", "alien_b200_step_kernel_name",
     "alien_b200_batch_create", "alien_b200_batch_destroy", "alien_b200_batch_num_worlds",
     "alien_b200_batch_calc_timesteps", "alien_b200_batch_enqueue_timesteps", "alien_b200_batch_get_data",
     "alien_b200_batch_get_array_sizes", "alien_b200_batch_get_raw_statistics", "alien_b200_batch_stream",
-    "alien_b200_batch_kernel_launch_count", "alien_b200_batch_kernels_per_step",
+    "alien_b200_batch_kernel_launch_count", "alien_b200_batch_kernels_per_step", "alien_b200_batch_timed_timesteps",
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -116,8 +117,19 @@ def load() -> ctypes.CDLL:
     lib.alien_b200_batch_kernel_launch_count.argtypes = [vp]
     lib.alien_b200_batch_kernel_launch_count.restype = u64
     lib.alien_b200_batch_kernels_per_step.argtypes = [vp]
+    lib.alien_b200_timed_timesteps.argtypes = [vp, u64, P(ctypes.c_double), i32, P(i32)]
+    lib.alien_b200_batch_timed_timesteps.argtypes = [vp, u64, P(ctypes.c_double), i32, P(i32)]
+    lib.alien_b200_select_device.argtypes = [i32]
+    lib.alien_b200_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]
+    lib.alien_b200_batch_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]
+    lib.alien_b200_step_kernel_name.argtypes = [i32]
+    lib.alien_b200_step_kernel_name.restype = ctypes.c_char_p
     _lib = lib
     return lib
+
+
+def select_device(device: int) -> None:
+    check(load().alien_b200_select_device(int(device)))
 
 
 def last_error() -> str:

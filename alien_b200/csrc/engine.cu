@@ -129,6 +129,11 @@ public:
     void build(const std::vector<WorldSetup>& setups);
     void enqueueStep();
     void enqueueSteps(uint64_t n);
+    // n graph steps bracketed by CUDA events on the arena's stream
+    double timeSteps(uint64_t n);
+    // n steps without the graph, an event after every launch; returns the
+    // summed milliseconds per launch position of the step
+    std::vector<double> timedSteps(uint64_t n);
     void calcTimesteps(uint64_t n);
     void sync();
     void setParams(int w, const AlienPhysicsParams& p);
@@ -155,7 +160,14 @@ private:
         kernel<<<grid, block, 0, stream_>>>(args...);
         ++launches_;
         AB_CK(cudaGetLastError());
+        if (timingEvents_) {
+            cudaEvent_t e;
+            AB_CK(cudaEventCreate(&e));
+            AB_CK(cudaEventRecord(e, stream_));
+            timingEvents_->push_back(e);
+        }
     }
+    std::vector<cudaEvent_t>* timingEvents_ = nullptr;
     void scan(const uint32_t* in, long long n, uint32_t* out);
     void releaseGraph()
     {
@@ -446,6 +458,60 @@ void Arena::enqueueSteps(uint64_t n)
         AB_CK(cudaGraphLaunch(graphExec_, stream_));
         launches_ += kernelsPerStep_;
     }
+}
+
+std::vector<double> Arena::timedSteps(uint64_t n)
+{
+    std::vector<double> sums;
+    std::vector<cudaEvent_t> events;
+    for (uint64_t i = 0; i < n; ++i) {
+        events.clear();
+        cudaEvent_t start;
+        AB_CK(cudaEventCreate(&start));
+        AB_CK(cudaEventRecord(start, stream_));
+        events.push_back(start);
+        timingEvents_ = &events;
+        try {
+            enqueueStep();
+        } catch (...) {
+            timingEvents_ = nullptr;
+            throw;
+        }
+        timingEvents_ = nullptr;
+        AB_CK(cudaStreamSynchronize(stream_));
+        if (sums.size() < events.size() - 1) sums.resize(events.size() - 1, 0.0);
+        for (size_t k = 1; k < events.size(); ++k) {
+            float ms = 0.0f;
+            AB_CK(cudaEventElapsedTime(&ms, events[k - 1], events[k]));
+            sums[k - 1] += ms;
+        }
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+    }
+    sync();
+    return sums;
+}
+
+double Arena::timeSteps(uint64_t n)
+{
+    enqueueSteps(0);
+    if (!graphExec_) {  // build the graph outside the timed region
+        enqueueSteps(1);
+        sync();
+    }
+    cudaEvent_t a, b;
+    AB_CK(cudaEventCreate(&a));
+    AB_CK(cudaEventCreate(&b));
+    AB_CK(cudaStreamSynchronize(stream_));
+    AB_CK(cudaEventRecord(a, stream_));
+    enqueueSteps(n);
+    AB_CK(cudaEventRecord(b, stream_));
+    AB_CK(cudaEventSynchronize(b));
+    float ms = 0.0f;
+    AB_CK(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    sync();
+    return ms;
 }
 
 void Arena::sync()
@@ -776,6 +842,14 @@ extern "C" {
 
 int alien_b200_version(void) { return 1; }
 
+int alien_b200_select_device(int device)
+{
+    return guarded([&] {
+        ensureDevice();
+        AB_CK(cudaSetDevice(device));
+    });
+}
+
 void alien_b200_default_parameters(AlienPhysicsParams* p)
 {
     if (!p) return;
@@ -867,6 +941,41 @@ int alien_b200_enqueue_timesteps(alien_b200_simulation* sim, uint64_t timesteps)
 }
 
 void* alien_b200_stream(alien_b200_simulation* sim) { return sim ? static_cast<void*>(sim->stream) : nullptr; }
+
+int alien_b200_time_timesteps(alien_b200_simulation* sim, uint64_t timesteps, double* milliseconds)
+{
+    return guarded([&] {
+        if (!sim || !milliseconds) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        *milliseconds = sim->arena->timeSteps(timesteps);
+    });
+}
+
+static const char* const kKernelNames[] = {"kBin", "kScanReduce", "kScanPartials", "kScanDown", "kScatter", "kStage",
+                                           "kPairs", "kApplyBond1", "kVerletPos", "kBond2", "kVerletVel", "kTransition",
+                                           "kDecay", "kResolve", "kCommit", "kEventCount", "kEventWorld", "kEventEmit"};
+
+const char* alien_b200_step_kernel_name(int index)
+{
+    const int n = static_cast<int>(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
+    return index >= 0 && index < n ? kKernelNames[index] : nullptr;
+}
+
+static int timedInto(Arena& a, uint64_t timesteps, double* kernelMs, int maxKernels, int* numKernels)
+{
+    std::vector<double> sums = a.timedSteps(timesteps);
+    const int n = static_cast<int>(sums.size());
+    if (numKernels) *numKernels = n;
+    for (int k = 0; k < n && k < maxKernels; ++k) kernelMs[k] = sums[k];
+    return n;
+}
+
+int alien_b200_timed_timesteps(alien_b200_simulation* sim, uint64_t timesteps, double* kernelMs, int maxKernels, int* numKernels)
+{
+    return guarded([&] {
+        if (!sim || (!kernelMs && maxKernels > 0)) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        timedInto(*sim->arena, timesteps, kernelMs, maxKernels, numKernels);
+    });
+}
 
 uint64_t alien_b200_kernel_launch_count(alien_b200_simulation* sim) { return sim && sim->arena ? sim->arena->launches() : 0; }
 
@@ -1060,5 +1169,21 @@ void* alien_b200_batch_stream(alien_b200_batch* b) { return b ? static_cast<void
 uint64_t alien_b200_batch_kernel_launch_count(alien_b200_batch* b) { return b && b->arena ? b->arena->launches() : 0; }
 
 int alien_b200_batch_kernels_per_step(alien_b200_batch* b) { return b && b->arena ? b->arena->kernelsPerStep() : 0; }
+
+int alien_b200_batch_time_timesteps(alien_b200_batch* b, uint64_t timesteps, double* milliseconds)
+{
+    return guarded([&] {
+        if (!b || !milliseconds) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        *milliseconds = b->arena->timeSteps(timesteps);
+    });
+}
+
+int alien_b200_batch_timed_timesteps(alien_b200_batch* b, uint64_t timesteps, double* kernelMs, int maxKernels, int* numKernels)
+{
+    return guarded([&] {
+        if (!b || (!kernelMs && maxKernels > 0)) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        timedInto(*b->arena, timesteps, kernelMs, maxKernels, numKernels);
+    });
+}
 
 }  // extern "C"

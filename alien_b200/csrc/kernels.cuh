@@ -366,7 +366,10 @@ __device__ __forceinline__ void pairsFluid(const DevState& s, long long k)
         if (dvr < 0.0f) {
             const float trr = fmaxf(0.05f, lensq2(rr));
             const float td = fmaxf(0.05f, bestBarrierDist);
-            F = (vr - rr * 2.0f * dvr / trr + vb - vi) / td;
+            // (vr - rr*2*dvr/trr + vb - vi) / td of CellProcessor.cuh:272 with
+            // vr + vb - vi = 0 cancelled algebraically (the FP32 form loses
+            // ~ulp(|v|)/td to that cancellation)
+            F = rr * (-2.0f * dvr / trr) / td;
         }
     }
     const float2 Fp = f2(fromFix(qFpx), fromFix(qFpy)), Fv = f2(fromFix(qFvx), fromFix(qFvy));

@@ -62,6 +62,12 @@ class SimulationFacade:
     def enqueue_timesteps(self, timesteps: int) -> None:
         check(self._lib.alien_b200_enqueue_timesteps(self._handle(), int(timesteps)))
 
+    def time_timesteps(self, timesteps: int) -> float:
+        """milliseconds of ``timesteps`` steps between CUDA events on the engine stream"""
+        ms = ctypes.c_double()
+        check(self._lib.alien_b200_time_timesteps(self._handle(), int(timesteps), ctypes.byref(ms)))
+        return ms.value
+
     # setSimulationData (:47)
     def set_simulation_data(self, data: DataTO) -> None:
         check(self._lib.alien_b200_set_data(self._handle(), ctypes.cast(data.c_ptr(), ctypes.c_void_p)))
@@ -123,6 +129,10 @@ class SimulationFacade:
     def kernel_launches(self) -> int:
         return int(self._lib.alien_b200_kernel_launch_count(self._handle()))
 
+    def timed_timesteps(self, timesteps: int):
+        """{kernel name: summed ms} over ``timesteps`` steps, launch by launch"""
+        return _timed(self._lib, self._lib.alien_b200_timed_timesteps, self._handle(), timesteps)
+
 
 class BatchSimulation:
     """Many independent worlds stepped together in one arena."""
@@ -159,6 +169,11 @@ class BatchSimulation:
     def enqueue_timesteps(self, timesteps: int) -> None:
         check(self._lib.alien_b200_batch_enqueue_timesteps(self._h, int(timesteps)))
 
+    def time_timesteps(self, timesteps: int) -> float:
+        ms = ctypes.c_double()
+        check(self._lib.alien_b200_batch_time_timesteps(self._h, int(timesteps), ctypes.byref(ms)))
+        return ms.value
+
     def get_simulation_data(self, world: int) -> DataTO:
         s = ArraySizes()
         check(self._lib.alien_b200_batch_get_array_sizes(self._h, int(world), ctypes.byref(s)))
@@ -180,3 +195,17 @@ class BatchSimulation:
 
     def kernels_per_step(self) -> int:
         return int(self._lib.alien_b200_batch_kernels_per_step(self._h))
+
+    def timed_timesteps(self, timesteps: int):
+        return _timed(self._lib, self._lib.alien_b200_batch_timed_timesteps, self._h, timesteps)
+
+
+def _timed(lib, fn, handle, timesteps):
+    buf = (ctypes.c_double * 64)()
+    n = ctypes.c_int()
+    check(fn(handle, int(timesteps), buf, 64, ctypes.byref(n)))
+    out = {}
+    for k in range(n.value):
+        name = lib.alien_b200_step_kernel_name(k)
+        out[name.decode() if name else f"k{k}"] = buf[k]
+    return out

@@ -90,6 +90,12 @@ def empty_cells(n: int) -> np.ndarray:
     return cells
 
 
+def _grown(arr: np.ndarray, cap: int) -> np.ndarray:
+    out = np.zeros(cap, arr.dtype)
+    out[: len(arr)] = arr
+    return out
+
+
 class DataTO:
     """Host-side DataTO with owned numpy buffers (``DataTO::init``,
     TOs.cuh:204-215).  ``capacity`` sizes the arrays for egress."""
@@ -104,12 +110,9 @@ class DataTO:
         ncap = max(len(cells), cell_capacity or 0, 1)
         pcap = max(len(particles), particle_capacity or 0, 1)
         acap = max(len(aux), aux_capacity or 0, 1)
-        self._cells = np.zeros(ncap, CELL_TO)
-        self._cells[: len(cells)] = cells
-        self._particles = np.zeros(pcap, PARTICLE_TO)
-        self._particles[: len(particles)] = particles
-        self._aux = np.zeros(acap, np.uint8)
-        self._aux[: len(aux)] = aux
+        self._cells = cells if len(cells) == ncap else _grown(cells, ncap)
+        self._particles = particles if len(particles) == pcap else _grown(particles, pcap)
+        self._aux = aux if len(aux) == acap else _grown(aux, acap)
         self._counts = np.array([len(cells), len(particles), len(aux)], dtype=np.uint64)
         self._c = CDataTO()
         base = self._counts.ctypes.data

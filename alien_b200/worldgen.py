@@ -145,8 +145,28 @@ class ClusterTemplate:
         self.radius = float(np.hypot(pos[:, 0], pos[:, 1]).max())
 
 
+def _place_clusters_stratified(rng, count, world, radius):
+    """Non-overlapping centres for large counts: ``count`` distinct cells of a
+    grid of side 2*radius + 2, chosen uniformly at random, each with a
+    uniform jitter that keeps the cluster inside its grid cell."""
+    sx, sy = world
+    d = 2.0 * radius + 2.0
+    nx, ny = int(sx // d), int(sy // d)
+    if nx * ny < count:
+        raise RuntimeError("world too small for the clusters")
+    pick = rng.choice(nx * ny, size=count, replace=False)
+    gx, gy = pick % nx, pick // nx
+    slack = d - (2.0 * radius + 1.0)
+    cx = gx * d + radius + 0.5 + rng.uniform(0, slack, count)
+    cy = gy * d + radius + 0.5 + rng.uniform(0, slack, count)
+    return np.stack([cx, cy], axis=1)
+
+
 def _place_clusters(rng, count, world, radius, max_tries=200):
-    """Uniform cluster centres, rejecting overlaps (bins of side 2*radius)."""
+    """Uniform cluster centres, rejecting overlaps (bins of side 2*radius);
+    stratified placement beyond 2000 clusters."""
+    if count > 2000:
+        return _place_clusters_stratified(rng, count, world, radius)
     sx, sy = world
     min_d = 2.0 * radius + 1.0
     centres = np.zeros((count, 2), np.float64)

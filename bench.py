@@ -1,0 +1,400 @@
+"""Benchmark of the B200 physics stage: Mcell-steps/s on seeded synthetic worlds.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                [--config hex4m|fluid1m|softbody|batched256]
+
+One step = one timestep of the per-timestep physics stage over the whole
+world (cell map, pair forces, bond forces, Verlet, energy particles,
+structural operations).  Default workload: the soft-body-heavy world, 4M
+cells in 40k hexagonal 100-cell clusters on a 4096x4096 torus, collision
+motion, bond breaking on.  State is larger than L2 (126 MB), so no flush is
+needed between steps.  Prints one JSON line (rank 0).
+
+--impl reference times the reference's own implementation of the path on
+this machine; the reference ships only a CUDA engine, whose harness is
+oracle/ref (built from the reference sources when they are present); without
+it, the CPU restatement of the same step (oracle, FP32, OpenMP over all host
+threads) is timed and reported as a port.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s"
+
+# algorithmic bytes per cell per launch of each step kernel (FP32 SoA):
+# P1 hash build 24; P2 pair forces 40; P3 apply 24 + P4 bond forces 20+12b;
+# P5 Verlet x 32; P6 bond forces 20+12b; P7 Verlet v 32
+def algorithmic_bytes(kernel: str, bonds_per_cell: float) -> float:
+    b = bonds_per_cell
+    return {
+        "kBin": 24.0,
+        "kPairs": 40.0,
+        "kApplyBond1": 24.0 + 20.0 + 12.0 * b,
+        "kVerletPos": 32.0,
+        "kBond2": 20.0 + 12.0 * b,
+        "kVerletVel": 32.0,
+    }.get(kernel, 0.0)
+
+
+def load_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region"""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(config: str, rank: int = 0):
+    from alien_b200 import params as P
+    from alien_b200 import worldgen
+
+    seed = 1000 * rank
+    if config == "hex4m":
+        data, world = worldgen.hex_world(seed=seed)
+        prm = P.benchmark_parameters(P.MOTION_COLLISION)
+        desc = "soft-body heavy: 4096x4096 torus, 4M cells in 40k hexagonal 100-cell clusters, collisions + bond breaking"
+    elif config == "fluid1m":
+        data, world = worldgen.fluid_world(seed=seed)
+        prm = P.benchmark_parameters(P.MOTION_FLUID)
+        desc = "SPH fluid stress: 2048x2048 torus, 1M unbonded cells, density 0.24, velocity sigma 0.5"
+    elif config == "softbody":
+        data, world = worldgen.soft_body_world(seed=seed)
+        prm = P.benchmark_parameters(P.MOTION_FLUID)
+        desc = "plain small: 512x512 torus, 200 10x10 lattice clusters (20k cells) + 20k energy particles"
+    else:
+        raise ValueError(config)
+    return data, world, prm, desc
+
+
+def pin(arr):
+    """page-lock a numpy buffer for the host<->device copies of the e2e leg"""
+    import torch
+    if arr.nbytes == 0:
+        return None
+    rc = torch.cuda.cudart().cudaHostRegister(arr.ctypes.data, arr.nbytes, 0)
+    return arr.ctypes.data if int(rc) == 0 else None
+
+
+def unpin(ptr):
+    import torch
+    if ptr:
+        torch.cuda.cudart().cudaHostUnregister(ptr)
+
+
+def cpu_baseline(data, world, prm, budget_s: float = 20.0, max_steps: int = 1000, precision: str = "f32"):
+    """The CPU restatement (FP32, OpenMP) stepping the same world: a bounded
+    sample of about ``budget_s`` seconds."""
+    from oracle.oracle import OracleSimulation, library
+
+    threads = library(precision).oracle_num_threads()
+    sim = OracleSimulation(world, prm, 0, precision=precision)
+    sim.set_simulation_data(data)
+    t0 = time.perf_counter()
+    sim.calc_timesteps(1)  # warm-up step
+    first = time.perf_counter() - t0
+    steps = max(1, min(max_steps, int(budget_s / max(first, 1e-6))))
+    t0 = time.perf_counter()
+    sim.calc_timesteps(steps)
+    dt = time.perf_counter() - t0
+    sim.close()
+    value = data.num_cells * steps / dt / 1e6
+    return {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{steps} steps of the same world after 1 warm-up step ({dt:.1f} s, {threads} threads)"}, steps, dt
+
+
+def run_reference(args, config, rank, world_size):
+    """--impl reference: the reference path timed on this machine"""
+    if rank != 0:
+        return 0
+    data, world, prm, desc = build_workload(config)
+    base, steps, dt = cpu_baseline(data, world, prm, budget_s=min(120.0, 5.0 + 2.0 * args.steps))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": base["value"], "unit": METRIC, "n_gpus": 0,
+        "steps": steps, "warmup": 1, "ms_per_step": 1000.0 * dt / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": config, "description": desc, "cells": data.num_cells},
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference ships no CPU engine; this is the CPU restatement of the same step (oracle, FP32, OpenMP)",
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_batched(args, rank, world_size):
+    """256 worlds, log-uniform 1k-200k cells: one arena stepped together vs
+    the plain engine stepping the same worlds one after another"""
+    from alien_b200 import params as P
+    from alien_b200 import worldgen
+    from alien_b200.facade import BatchSimulation, SimulationFacade
+
+    sizes = worldgen.batched_sizes(seed=rank, count=256)
+    worlds = []
+    for i, n in enumerate(sizes):
+        d, w = worldgen.mixed_world(seed=10_000 * rank + i, num_cells=int(n))
+        worlds.append((d, w, P.benchmark_parameters(P.MOTION_FLUID)))
+    total = sum(d.num_cells for d, _, _ in worlds)
+    batch = BatchSimulation(worlds)
+    batch.calc_timesteps(args.warmup)
+    launches0 = batch.kernel_launches()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        ms = batch.time_timesteps(args.steps)
+    launches = batch.kernel_launches() - launches0
+    batch.close()
+    # plain: each world its own facade, stepped sequentially (same step count)
+    plain_steps = max(3, args.steps // 10)
+    sims = []
+    for d, w, p in worlds:
+        s = SimulationFacade()
+        s.new_simulation(0, w, p)
+        s.set_simulation_data(d)
+        s.calc_timesteps(1)
+        sims.append(s)
+    t_plain = 0.0
+    for s in sims:
+        t_plain += s.time_timesteps(plain_steps)
+    for s in sims:
+        s.close_simulation()
+    plain_value = total * plain_steps / (t_plain / 1000.0) / 1e6
+    value = total * args.steps / (ms / 1000.0) / 1e6
+    return {"value": value, "ms": ms, "launches": launches, "clocks": clk.summary(), "total": total,
+            "plain_value": plain_value, "plain_ms_per_step": t_plain / plain_steps}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="hex4m", choices=["hex4m", "fluid1m", "softbody", "batched256"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", 0))
+    world_size = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, args.config, rank, world_size)
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    if world_size > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from alien_b200 import _lib
+    from alien_b200.facade import SimulationFacade
+
+    _lib.select_device(local_rank)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world_size > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world_size == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if world_size == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    peak, peak_kind = load_peak()
+    if args.config == "batched256":
+        r = run_batched(args, rank, world_size)
+        ms = max_over_ranks(r["ms"])
+        total = sum_over_ranks(r["total"])
+        if rank == 0:
+            line = {
+                "metric": METRIC, "value": total * args.steps / (ms / 1000.0) / 1e6, "unit": METRIC,
+                "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "batched256", "worlds": 256, "cells": r["total"],
+                           "description": "256 worlds, log-uniform 1k-200k cells, density 0.2, half fluid cells and half 10x10 lattices",
+                           "l2": "state larger than L2, no flush"},
+                "batched_vs_plain": r["value"] / r["plain_value"],
+                "plain": {"value": r["plain_value"], "ms_per_step": r["plain_ms_per_step"]},
+                "clocks": r["clocks"], "gpu_launches": r["launches"],
+            }
+            print(json.dumps(line))
+        if world_size > 1:
+            dist.destroy_process_group()
+        return 0
+
+    data, world, prm, desc = build_workload(args.config, rank)
+    n_cells = data.num_cells
+    sim = SimulationFacade()
+    sim.new_simulation(0, world, prm)
+    sim.set_simulation_data(data)
+    sim.calc_timesteps(args.warmup)
+    stats0 = sim.get_raw_statistics()
+    launches0 = sim.kernel_launches()
+    barrier()
+    with ClockSampler(local_rank) as clk:
+        ms = sim.time_timesteps(args.steps)
+    barrier()
+    launches = sim.kernel_launches() - launches0
+    stats1 = sim.get_raw_statistics()
+    ms = max_over_ranks(ms)
+    cells_mean = 0.5 * (stats0.numCells + stats1.numCells)
+    total_cells = sum_over_ranks(cells_mean)
+    value = total_cells * args.steps / (ms / 1000.0) / 1e6
+
+    # per-kernel CUDA-event breakdown over a second stretch of the same run
+    timed_steps = max(3, min(args.steps, 50))
+    kernel_ms = sim.timed_timesteps(timed_steps)
+    bonds = stats1.numConnections / max(1, stats1.numCells)
+    dominant = max((k for k in kernel_ms if algorithmic_bytes(k, bonds) > 0), key=lambda k: kernel_ms[k])
+    per_launch_ms = kernel_ms[dominant] / timed_steps
+    alg_bytes = algorithmic_bytes(dominant, bonds) * stats1.numCells
+    achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", f"{dominant}_{args.config}_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+
+    # end to end through the C ABI with host buffers: H2D of the world,
+    # every step calc_timesteps(1) + a statistics read-back, D2H of the world
+    e2e = None
+    if not args.no_e2e:
+        pins = [pin(data._cells), pin(data._particles)]
+        sizes = None
+        sim2 = SimulationFacade()
+        sim2.new_simulation(0, world, prm)
+        sim2.set_simulation_data(data)
+        out = sim2.get_simulation_data()
+        out_pins = [pin(out._cells), pin(out._particles)]
+        e2e_steps = args.steps
+        barrier()
+        t0 = time.perf_counter()
+        sim2.set_simulation_data(data)
+        for _ in range(e2e_steps):
+            sim2.calc_timesteps(1)
+            sim2.get_raw_statistics()
+        sim2.get_simulation_data(out=out)
+        barrier()
+        t_e2e = max_over_ranks(time.perf_counter() - t0)
+        sim2.close_simulation()
+        for p in pins + out_pins:
+            unpin(p)
+        h2d = data.nbytes() / e2e_steps
+        d2h = (out.nbytes() + 112 * e2e_steps) / e2e_steps
+        e2e = {"value": sum_over_ranks(n_cells) * e2e_steps / t_e2e / 1e6, "unit": METRIC,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "note": "set_simulation_data + per step (calc_timesteps(1) + get_raw_statistics) + get_simulation_data, pinned host buffers"}
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        cpu, _, _ = cpu_baseline(data, world, prm)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak" if world_size > 1 else "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": args.config, "description": desc, "cells": n_cells,
+                       "world": list(world), "bonds_per_cell": round(bonds, 3),
+                       "parallelism": f"replicas x{world_size}" if world_size > 1 else "single world",
+                       "l2": "state larger than L2 (126 MB), no flush between steps"},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": per_launch_ms},
+            "kernel_ms_per_step": {k: v / timed_steps for k, v in kernel_ms.items()},
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    sim.close_simulation()
+    if world_size > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

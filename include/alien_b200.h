@@ -248,6 +248,10 @@ typedef struct alien_b200_simulation alien_b200_simulation;
 
 /* library / defaults */
 int alien_b200_version(void);
+/* Makes `device` the CUDA device of the calling thread for handles created
+ * afterwards (the reference picks the device with the highest compute
+ * capability itself, SimulationCudaFacade.cu:517-576). */
+int alien_b200_select_device(int device);
 void alien_b200_default_parameters(AlienPhysicsParams* params);
 int alien_b200_last_error(char* buffer, size_t size);
 
@@ -277,10 +281,20 @@ int alien_b200_get_raw_statistics(alien_b200_simulation* sim, AlienRawStatistics
  * call.  No counterpart in the reference (its calcTimestep synchronises
  * after every step, SimulationCudaFacade.cu:578-582). */
 int alien_b200_enqueue_timesteps(alien_b200_simulation* sim, uint64_t timesteps);
+/* Steps `timesteps` times on the handle's stream between two CUDA events
+ * (the stream is synchronised first) and returns the elapsed milliseconds. */
+int alien_b200_time_timesteps(alien_b200_simulation* sim, uint64_t timesteps, double* milliseconds);
 /* The CUDA stream (cudaStream_t) all of the handle's work is issued on. */
 void* alien_b200_stream(alien_b200_simulation* sim);
 /* Number of kernel launches issued by the handle since creation. */
 uint64_t alien_b200_kernel_launch_count(alien_b200_simulation* sim);
+/* Steps `timesteps` times launch by launch (no graph) with a CUDA event
+ * after every kernel; kernelMs[k] receives the summed milliseconds of the
+ * k-th kernel of the step (names: alien_b200_step_kernel_name(k)).  A
+ * profiling hook without a reference counterpart. */
+int alien_b200_timed_timesteps(alien_b200_simulation* sim, uint64_t timesteps, double* kernelMs, int maxKernels,
+                               int* numKernels);
+const char* alien_b200_step_kernel_name(int index);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -34,6 +34,11 @@ int alien_b200_batch_get_raw_statistics(alien_b200_batch* batch, int world, Alie
 void* alien_b200_batch_stream(alien_b200_batch* batch);
 uint64_t alien_b200_batch_kernel_launch_count(alien_b200_batch* batch);
 int alien_b200_batch_kernels_per_step(alien_b200_batch* batch);
+/* event-timed steps as alien_b200_time_timesteps, for all worlds */
+int alien_b200_batch_time_timesteps(alien_b200_batch* batch, uint64_t timesteps, double* milliseconds);
+/* per-kernel timing as alien_b200_timed_timesteps, for all worlds */
+int alien_b200_batch_timed_timesteps(alien_b200_batch* batch, uint64_t timesteps, double* kernelMs, int maxKernels,
+                                     int* numKernels);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -643,7 +643,9 @@ static void fluidPhase(OracleWorld* w)
             if (dvr < 0) {
                 real trr = rmax((real)0.05, vlen2(r));
                 real td = rmax((real)0.05, bestBarrierDist);
-                F = vdiv(vadd(vsub(vr, vmul(r, 2 * dvr / trr)), vsub(w->vel[b], vi)), td);
+                /* (vr - r*2*dvr/trr + vb - vi) / td, CellProcessor.cuh:272,
+                 * with vr + vb - vi = 0 cancelled algebraically */
+                F = vdiv(vmul(r, -2 * dvr / trr), td);
             }
         }
         F = vadd(F, vadd(vmul(Fp, (real)p->pressureStrength), vmul(Fv, (real)p->viscosityStrength)));

@@ -4,7 +4,8 @@ Objects are matched by id (the reference's own tests sort by id,
 EngineTests/IntegrationTestFramework.cpp:135-142).  Floating-point fields
 are compared with the one-step tolerance of the engine against the FP64
 oracle: |a - b| <= RTOL * max(|b|, 1) per component (positions compared
-through the torus-wrapped difference).  Integer and index fields
+through the torus-wrapped difference; bond angles in degrees with
+max(|b|, 360)).  Integer and index fields
 (ids, bond partners, counts, living states) must match exactly.
 """
 from __future__ import annotations
@@ -76,8 +77,11 @@ def compare_cells(got, ref, world, rtol=RTOL, check_bonds=True, report=None):
         n = r["numConnections"].astype(np.int64)
         mask = np.arange(6)[None, :] < n[:, None]
         errs["bondDist"] = float(np.max(rel_err(g["connections"]["distance"][mask], r["connections"]["distance"][mask]), initial=0))
+        # angles of bonds created this step derive from FP32 positions through
+        # asin: their error floor is absolute (~1e-6 rad), so they are scaled
+        # by the full circle (360 degrees) instead of their own magnitude
         errs["bondAngle"] = float(np.max(rel_err(g["connections"]["angleFromPrevious"][mask],
-                                                 r["connections"]["angleFromPrevious"][mask]), initial=0))
+                                                 r["connections"]["angleFromPrevious"][mask], 360.0), initial=0))
     for k, v in errs.items():
         assert v <= rtol, f"{k}: max relative error {v:.3g} > {rtol}"
     return errs

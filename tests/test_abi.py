@@ -18,7 +18,7 @@ def declared_functions():
     names = set()
     for h in ("alien_b200.h", "alien_b200_batch.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
-        names |= set(re.findall(r"^\s*(?:int|void\*?|uint64_t|void)\s+\*?(alien_b200_\w+)\s*\(", text, re.M))
+        names |= set(re.findall(r"^\s*(?:const\s+)?(?:int|void|uint64_t|char)\s*\*?\s*(alien_b200_\w+)\s*\(", text, re.M))
     return names
 
 
