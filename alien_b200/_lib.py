@@ -68,6 +68,8 @@ EXPORTED_SYMBOLS = [
     "alien_b200_batch_calc_timesteps", "alien_b200_batch_enqueue_timesteps", "alien_b200_batch_get_data",
     "alien_b200_batch_get_array_sizes", "alien_b200_batch_get_raw_statistics", "alien_b200_batch_stream",
     "alien_b200_batch_kernel_launch_count", "alien_b200_batch_kernels_per_step", "alien_b200_batch_timed_timesteps",
+    "alien_b200_batch_set_step_budget", "alien_b200_batch_world_status", "alien_b200_batch_num_active",
+    "alien_b200_batch_device_bytes",
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -119,6 +121,11 @@ def load() -> ctypes.CDLL:
     lib.alien_b200_batch_kernels_per_step.argtypes = [vp]
     lib.alien_b200_timed_timesteps.argtypes = [vp, u64, P(ctypes.c_double), i32, P(i32)]
     lib.alien_b200_batch_timed_timesteps.argtypes = [vp, u64, P(ctypes.c_double), i32, P(i32)]
+    lib.alien_b200_batch_set_step_budget.argtypes = [vp, i32, u64]
+    lib.alien_b200_batch_world_status.argtypes = [vp, i32, P(u64), P(u64), P(i32)]
+    lib.alien_b200_batch_num_active.argtypes = [vp]
+    lib.alien_b200_batch_device_bytes.argtypes = [vp]
+    lib.alien_b200_batch_device_bytes.restype = u64
     lib.alien_b200_select_device.argtypes = [i32]
     lib.alien_b200_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]
     lib.alien_b200_batch_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]

@@ -75,6 +75,11 @@ struct WorldCounters {
     // event bases of the current step (ids and slots of appended particles)
     unsigned long long radIdBase, splitIdBase, delIdBase;
     unsigned int radSlotBase, splitSlotBase, delSlotBase, numEvents;
+    // a world steps while active; stepsRemaining counts down to 0 and then
+    // clears active (~0 = no limit)
+    unsigned long long stepsRemaining;
+    unsigned int active;
+    unsigned int pad2;
 };
 
 struct DevState {

@@ -142,6 +142,7 @@ public:
     void countData(int w, uint64_t* cells, uint64_t* particles);
     AlienRawStatistics statistics(int w);
     void setTimestep(int w, uint64_t t);
+    void setStepBudget(int w, uint64_t steps);
     void compactParticles(int w);
     void ensureParticleCapacity();
 
@@ -360,6 +361,8 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         wc.nextId = 1;
         wc.numCells = static_cast<unsigned int>(setups[w].numCells);
         wc.numParticles = static_cast<unsigned int>(setups[w].numParticles);
+        wc.stepsRemaining = ~0ull;
+        wc.active = 1;
     }
     AB_CK(cudaMemcpyAsync(worldsDev, infos.data(), sizeof(WorldInfo) * n, cudaMemcpyHostToDevice, stream_));
     AB_CK(cudaMemcpyAsync(paramsDev, params.data(), sizeof(AlienPhysicsParams) * n, cudaMemcpyHostToDevice, stream_));
@@ -372,6 +375,10 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     AB_CK(cudaMemsetAsync(s.pflag, 0, P * sizeof(uint32_t), stream_));
     AB_CK(cudaMemsetAsync(s.pmap, 0xff, static_cast<size_t>(pmapSlots) * sizeof(int), stream_));
     AB_CK(cudaMemsetAsync(s.flags, 0, C * sizeof(uint32_t), stream_));
+    AB_CK(cudaMemsetAsync(s.angleAcc, 0, C * 4 * sizeof(long long), stream_));
+    AB_CK(cudaMemsetAsync(s.energyAcc, 0, C * sizeof(long long), stream_));
+    AB_CK(cudaMemsetAsync(s.newPartner, 0xff, C * sizeof(int), stream_));
+    AB_CK(cudaMemsetAsync(s.best, 0xff, C * sizeof(int), stream_));
 
     // ingest: host TOs -> device staging -> SoA (cudaCreateDataFromTO)
     long long coldBase = 0;
@@ -426,7 +433,6 @@ void Arena::enqueueStep()
     launch(kBond2, both, kBlock, s);
     launch(kVerletVel, both, kBlock, s);
     launch(kTransition, both, kBlock, s);
-    launch(kDecay, cells, kBlock, s);
     launch(kResolve, cells, kBlock, s);
     launch(kCommit, cells, kBlock, s);
     launch(kEventCount, both, kBlock, s);
@@ -589,7 +595,11 @@ void Arena::rebuildFromHost(const std::vector<std::vector<AlienCellTO>>& cells, 
     build(setups);
     // ids continue where they were, not at max(id)+1 of the surviving objects
     std::vector<WorldCounters> now = readCounters();
-    for (size_t w = 0; w < old.size(); ++w) now[w].nextId = std::max(now[w].nextId, c[w].nextId);
+    for (size_t w = 0; w < old.size(); ++w) {
+        now[w].nextId = std::max(now[w].nextId, c[w].nextId);
+        now[w].stepsRemaining = c[w].stepsRemaining;
+        now[w].active = c[w].active;
+    }
     AB_CK(cudaMemcpy(s_.counters, now.data(), sizeof(WorldCounters) * now.size(), cudaMemcpyHostToDevice));
 }
 
@@ -637,6 +647,14 @@ void Arena::setParams(int w, const AlienPhysicsParams& p)
     // prepareForSimulationParametersChanges -> cudaResetDensity (SimulationKernelsLauncher.cu:93-97)
     launch(kResetDensity, hw.info.numCellBlocks, kBlock, s_, w);
     sync();
+}
+
+void Arena::setStepBudget(int w, uint64_t steps)
+{
+    std::vector<WorldCounters> c = readCounters();
+    c[w].stepsRemaining = steps == 0 ? ~0ull : steps;
+    c[w].active = 1;
+    AB_CK(cudaMemcpy(s_.counters, c.data(), sizeof(WorldCounters) * c.size(), cudaMemcpyHostToDevice));
 }
 
 void Arena::setTimestep(int w, uint64_t t)
@@ -952,7 +970,7 @@ int alien_b200_time_timesteps(alien_b200_simulation* sim, uint64_t timesteps, do
 
 static const char* const kKernelNames[] = {"kBin", "kScanReduce", "kScanPartials", "kScanDown", "kScatter", "kStage",
                                            "kPairs", "kApplyBond1", "kVerletPos", "kBond2", "kVerletVel", "kTransition",
-                                           "kDecay", "kResolve", "kCommit", "kEventCount", "kEventWorld", "kEventEmit"};
+                                           "kResolve", "kCommit", "kEventCount", "kEventWorld", "kEventEmit"};
 
 const char* alien_b200_step_kernel_name(int index)
 {
@@ -1154,6 +1172,40 @@ int alien_b200_batch_get_array_sizes(alien_b200_batch* b, int world, AlienArrayS
         sizes->auxiliaryDataSize = b->arena->world(world).aux.size();
     });
 }
+
+int alien_b200_batch_set_step_budget(alien_b200_batch* b, int world, uint64_t steps)
+{
+    return guarded([&] {
+        if (!b || world < 0 || world >= b->arena->numWorlds()) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        b->arena->setStepBudget(world, steps);
+    });
+}
+
+int alien_b200_batch_world_status(alien_b200_batch* b, int world, uint64_t* timestep, uint64_t* stepsRemaining, int* active)
+{
+    return guarded([&] {
+        if (!b || world < 0 || world >= b->arena->numWorlds()) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        std::vector<WorldCounters> c = b->arena->readCounters();
+        if (timestep) *timestep = c[world].timestep;
+        if (stepsRemaining) *stepsRemaining = c[world].stepsRemaining == ~0ull ? 0 : c[world].stepsRemaining;
+        if (active) *active = static_cast<int>(c[world].active);
+    });
+}
+
+int alien_b200_batch_num_active(alien_b200_batch* b)
+{
+    if (!b || !b->arena) return -1;
+    try {
+        std::vector<WorldCounters> c = b->arena->readCounters();
+        int n = 0;
+        for (const WorldCounters& x : c) n += x.active ? 1 : 0;
+        return n;
+    } catch (...) {
+        return -1;
+    }
+}
+
+uint64_t alien_b200_batch_device_bytes(alien_b200_batch* b) { return b && b->arena ? b->arena->deviceBytes() : 0; }
 
 int alien_b200_batch_get_raw_statistics(alien_b200_batch* b, int world, AlienRawStatistics* statistics)
 {

@@ -227,19 +227,38 @@ struct StatsAcc {
     long long cellEnergyFix, particleEnergyFix;  // 2^-16 fixed point: order-independent sums
 };
 
+// one block = one world (blocks never straddle worlds): warp sums, then one
+// atomic per warp and counter
+__device__ __forceinline__ unsigned long long warpSumU64(unsigned long long v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
 __global__ void __launch_bounds__(kBlock) kStatsCells(DevState s, StatsAcc* acc)
 {
     const int b = blockIdx.x;
     const int w = s.cellBlockWorld[b];
     const WorldInfo& wi = s.worlds[w];
     const long long g = static_cast<long long>(b) * kBlock + threadIdx.x;
-    if (g >= wi.cellBase + s.counters[w].numCells || !s.alive[g]) return;
+    const bool live = g < wi.cellBase + s.counters[w].numCells && s.alive[g];
+    unsigned long long cells = live ? 1 : 0;
+    unsigned long long bonds = live ? s.numConn[g] : 0;
+    long long e = live ? __double2ll_rn(static_cast<double>(s.energy[g]) * 65536.0) : 0;
+    const int col = live ? s.color[g] % ALIEN_B200_MAX_COLORS : -1;
     StatsAcc& a = acc[w];
-    atomicAdd(&a.numCells, 1ull);
-    atomicAdd(&a.numConnections, static_cast<unsigned long long>(s.numConn[g]));
-    atomicAdd(&a.numCellsByColor[s.color[g] % ALIEN_B200_MAX_COLORS], 1ull);
-    atomicAdd(reinterpret_cast<unsigned long long*>(&a.cellEnergyFix),
-              static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(s.energy[g]) * 65536.0)));
+    cells = warpSumU64(cells);
+    bonds = warpSumU64(bonds);
+    e = static_cast<long long>(warpSumU64(static_cast<unsigned long long>(e)));
+    if ((threadIdx.x & 31) == 0 && cells) {
+        atomicAdd(&a.numCells, cells);
+        atomicAdd(&a.numConnections, bonds);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&a.cellEnergyFix), static_cast<unsigned long long>(e));
+    }
+    for (int c = 0; c < ALIEN_B200_MAX_COLORS; ++c) {
+        const unsigned long long n = warpSumU64(col == c ? 1ull : 0ull);
+        if ((threadIdx.x & 31) == 0 && n) atomicAdd(&a.numCellsByColor[c], n);
+    }
 }
 
 __global__ void __launch_bounds__(kBlock) kStatsParticles(DevState s, StatsAcc* acc)
@@ -248,11 +267,14 @@ __global__ void __launch_bounds__(kBlock) kStatsParticles(DevState s, StatsAcc* 
     const int w = s.partBlockWorld[pb];
     const WorldInfo& wi = s.worlds[w];
     const long long q = static_cast<long long>(pb) * kBlock + threadIdx.x;
-    if (q >= wi.partBase + s.counters[w].numParticles || !s.palive[q]) return;
-    StatsAcc& a = acc[w];
-    atomicAdd(&a.numParticles, 1ull);
-    atomicAdd(reinterpret_cast<unsigned long long*>(&a.particleEnergyFix),
-              static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(s.penergy[q]) * 65536.0)));
+    const bool live = q < wi.partBase + s.counters[w].numParticles && s.palive[q];
+    unsigned long long n = warpSumU64(live ? 1ull : 0ull);
+    long long e = live ? __double2ll_rn(static_cast<double>(s.penergy[q]) * 65536.0) : 0;
+    e = static_cast<long long>(warpSumU64(static_cast<unsigned long long>(e)));
+    if ((threadIdx.x & 31) == 0 && n) {
+        atomicAdd(&acc[w].numParticles, n);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&acc[w].particleEnergyFix), static_cast<unsigned long long>(e));
+    }
 }
 
 // prepareForSimulationParametersChanges -> resetDensity (CellProcessor.cuh:860-870)

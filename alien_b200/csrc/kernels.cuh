@@ -18,9 +18,9 @@
 //   kVerletPos  verletPositionUpdate                     | particle targets
 //   kBond2      checkConnections, bond forces #2         | particle merges
 //   kVerletVel  verletVelocityUpdate, aging              | absorption
-//   kTransition living-state transition, inner friction  | splitting
-//   kDecay      friction, decay                          | particle map reset
-//   kResolve    dying/detaching resolution, bond additions (scratch)
+//   kTransition living-state transition, inner friction, | splitting,
+//               friction, decay                          | particle map reset
+//   kResolve    new living states, bond additions (scratch)
 //   kCommit     bond additions, cell deletion, bond deletion
 //   kEvent*     ids and slots of new energy particles, append
 #pragma once
@@ -44,7 +44,8 @@ __device__ __forceinline__ CellCtx cellCtx(const DevState& s)
     c.w = s.cellBlockWorld[b];
     c.g = static_cast<long long>(b) * kBlock + threadIdx.x;
     const WorldInfo& wi = s.worlds[c.w];
-    c.valid = c.g < wi.cellBase + s.counters[c.w].numCells && s.alive[c.g];
+    const WorldCounters& wc = s.counters[c.w];
+    c.valid = wc.active && c.g < wi.cellBase + wc.numCells && s.alive[c.g];
     return c;
 }
 
@@ -60,7 +61,8 @@ __device__ __forceinline__ PartCtx partCtx(const DevState& s, int pb)
     c.w = s.partBlockWorld[pb];
     c.q = static_cast<long long>(pb) * kBlock + threadIdx.x;
     const WorldInfo& wi = s.worlds[c.w];
-    c.inRange = c.q < wi.partBase + s.counters[c.w].numParticles;
+    const WorldCounters& wc = s.counters[c.w];
+    c.inRange = wc.active && c.q < wi.partBase + wc.numParticles;
     return c;
 }
 
@@ -71,19 +73,36 @@ __device__ __forceinline__ bool isBondedTo(const int* bonds, int n, int j)
     return r;
 }
 
-// distinct tile coordinates covering slots s-r .. s+r (wrapped)
-__device__ __forceinline__ int tileCoords(int s, int r, int size, int T, int* out)
-{
-    int n = 0;
-    for (int d = -r; d <= r; ++d) {
-        int t = wrapInt(s + d, size) / T;
-        bool dup = false;
-        for (int m = 0; m < n; ++m) dup |= (out[m] == t);
-        if (!dup) out[n++] = t;
-    }
-    return n;
-}
 constexpr int kMaxRadius = 15;
+
+// Calls f(tile) once for every tile that the (2r+1)^2-slot scan window of
+// slot (sx, sy) touches.  Along each axis the wrapped slots s-r..s+r map to
+// non-decreasing tiles with at most one wrap (the world is at least 2r+1
+// wide), so skipping repeats of the previous tile lists each tile once.
+template <class F>
+__device__ __forceinline__ void forEachWindowTile(const WorldInfo& wi, int sx, int sy, F&& f)
+{
+    const int r = wi.radiusInt;
+    int prevTy = -1;
+    for (int dy = -r; dy <= r; ++dy) {
+        int y = sy + dy;
+        y += y < 0 ? wi.H : 0;
+        y -= y >= wi.H ? wi.H : 0;
+        const int ty = y / wi.T;
+        if (ty == prevTy) continue;
+        prevTy = ty;
+        int prevTx = -1;
+        for (int dx = -r; dx <= r; ++dx) {
+            int x = sx + dx;
+            x += x < 0 ? wi.W : 0;
+            x -= x >= wi.W ? wi.W : 0;
+            const int tx = x / wi.T;
+            if (tx == prevTx) continue;
+            prevTx = tx;
+            f(wi.tileBase + tx + static_cast<long long>(ty) * wi.nTX);
+        }
+    }
+}
 
 // ---------------------------------------------------------------- kBin ----
 // cells: reset per-step scratch, tile binning (CellMap::set_block,
@@ -94,16 +113,11 @@ constexpr int kMaxRadius = 15;
 __global__ void __launch_bounds__(kBlock) kBin(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
+        // per-step scratch needs no reset here: flags are cleared by
+        // kEventEmit, the fixed-point accumulators and newPartner by the
+        // kernels that consume them, and best is written for every live cell
         CellCtx c = cellCtx(s);
         const long long g = c.g;
-        s.flags[g] = 0;
-        s.best[g] = -1;
-        s.newPartner[g] = -1;
-        s.angleAcc[4 * g + 0] = 0;
-        s.angleAcc[4 * g + 1] = 0;
-        s.angleAcc[4 * g + 2] = 0;
-        s.angleAcc[4 * g + 3] = 0;
-        s.energyAcc[g] = 0;
         if (!c.valid) return;
         const WorldInfo& wi = s.worlds[c.w];
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
@@ -285,13 +299,8 @@ __device__ __forceinline__ void pairsFluid(const DevState& s, long long k)
     unsigned long long bestId = ~0ull;
     const bool fusionI = !barrierI && nI < maxI && energyI <= p.cellMaxBindingEnergy;
 
-    const int r = wi.radiusInt;
     const int sx = slotX(pi.x, W), sy = slotX(pi.y, H);
-    int tx[2 * kMaxRadius + 1], ty[2 * kMaxRadius + 1];
-    const int ntx = tileCoords(sx, r, W, wi.T, tx), nty = tileCoords(sy, r, H, wi.T, ty);
-    for (int a = 0; a < nty; ++a) {
-        for (int b = 0; b < ntx; ++b) {
-            const long long t = wi.tileBase + tx[b] + static_cast<long long>(ty[a]) * wi.nTX;
+    forEachWindowTile(wi, sx, sy, [&](long long t) {
             const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
             for (uint32_t m = k0; m < k1; ++m) {
                 const int4 om = s.stagedMeta[m];
@@ -338,8 +347,7 @@ __device__ __forceinline__ void pairsFluid(const DevState& s, long long k)
                     }
                 }
             }
-        }
-    }
+    });
     float2 F = f2(0.0f, 0.0f);
     if (bestBarrier >= 0) {
         const long long b = bestBarrier;
@@ -422,13 +430,8 @@ __device__ __forceinline__ void pairsCollision(const DevState& s, long long k)
     long long qFx = 0, qFy = 0, qDx = 0, qDy = 0;
     int best = -1;
     unsigned long long bestId = ~0ull;
-    const int r = wi.radiusInt;
     const int sx = slotX(pi.x, W), sy = slotX(pi.y, H);
-    int tx[2 * kMaxRadius + 1], ty[2 * kMaxRadius + 1];
-    const int ntx = tileCoords(sx, r, W, wi.T, tx), nty = tileCoords(sy, r, H, wi.T, ty);
-    for (int a = 0; a < nty; ++a) {
-        for (int b = 0; b < ntx; ++b) {
-            const long long t = wi.tileBase + tx[b] + static_cast<long long>(ty[a]) * wi.nTX;
+    forEachWindowTile(wi, sx, sy, [&](long long t) {
             const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
             for (uint32_t m = k0; m < k1; ++m) {
                 const int4 om = s.stagedMeta[m];
@@ -472,8 +475,7 @@ __device__ __forceinline__ void pairsCollision(const DevState& s, long long k)
                     qFy -= toFix(f.y);
                 }
             }
-        }
-    }
+    });
     s.force[g] = f2(fromFix(qFx), fromFix(qFy));
     s.posB[g] = pi + f2(fromFix(qDx), fromFix(qDy));
     s.densNew[g] = __int_as_float(me.z);
@@ -605,7 +607,12 @@ __global__ void __launch_bounds__(kBlock) kVerletPos(DevState s)
         if (s.barrier[g]) {
             np = pb + v * dt;
         } else {
-            const float2 F1 = s.force1[g] + f2(fromFix(s.angleAcc[4 * g + 0]), fromFix(s.angleAcc[4 * g + 1]));
+            const long long ax = s.angleAcc[4 * g + 0], ay = s.angleAcc[4 * g + 1];
+            if (ax | ay) {
+                s.angleAcc[4 * g + 0] = 0;
+                s.angleAcc[4 * g + 1] = 0;
+            }
+            const float2 F1 = s.force1[g] + f2(fromFix(ax), fromFix(ay));
             s.force1[g] = F1;
             np = pb + (v * dt + F1 * dt * dt / 2.0f);
         }
@@ -698,7 +705,12 @@ __global__ void __launch_bounds__(kBlock) kVerletVel(DevState s)
         if (s.barrier[g]) {
             s.velB[g] = v;
         } else {
-            const float2 F2 = s.force[g] + f2(fromFix(s.angleAcc[4 * g + 2]), fromFix(s.angleAcc[4 * g + 3]));
+            const long long ax = s.angleAcc[4 * g + 2], ay = s.angleAcc[4 * g + 3];
+            if (ax | ay) {
+                s.angleAcc[4 * g + 2] = 0;
+                s.angleAcc[4 * g + 3] = 0;
+            }
+            const float2 F2 = s.force[g] + f2(fromFix(ax), fromFix(ay));
             s.velB[g] = v + (F2 + s.force1[g]) / 2.0f * p.timestepSize;
         }
         if (s.flags[g] & kFlagDetach) s.livingState[g] = ALIEN_B200_LIVING_DETACHING;
@@ -756,9 +768,10 @@ __global__ void __launch_bounds__(kBlock) kVerletVel(DevState s)
 }
 
 // -------------------------------------------------------- kTransition ----
-// cells: living-state transition (CellProcessor.cuh:596-664), inner friction
-// (every third step: one Jacobi sweep with one pair average per bond,
-// CellProcessor.cuh:678-705), absorbed energy.
+// cells: living-state transition (CellProcessor.cuh:596-664; the new state
+// is applied in kResolve, after every cell has read its partners' states),
+// absorbed energy, inner friction (every third step: one Jacobi sweep with
+// one pair average per bond, CellProcessor.cuh:678-705), friction and decay.
 // particles: splitting (RadiationProcessor::splitting, :172-204).
 __global__ void __launch_bounds__(kBlock) kTransition(DevState s)
 {
@@ -803,11 +816,39 @@ __global__ void __launch_bounds__(kBlock) kTransition(DevState s)
             if (sameDetaching && dc != ALIEN_B200_DEATH_NONE) ls = ALIEN_B200_LIVING_DETACHING;
         }
         s.nextState[g] = static_cast<uint8_t>(ls);
-        if (T % 3 == 0 && !s.barrier[g])
-            s.velA[g] = vi + acc * (p.innerFriction / 2.0f);
-        else
+        const long long ea = s.energyAcc[g];
+        float e = s.energy[g];
+        if (ea) {
+            e += fromFix(ea);
+            s.energy[g] = e;
+            s.energyAcc[g] = 0;
+        }
+        if (s.barrier[g]) {
             s.velA[g] = vi;
-        s.energy[g] += fromFix(s.energyAcc[g]);
+            return;
+        }
+        // applyInnerFriction (every third step) + applyFriction
+        // (CellProcessor.cuh:678-723)
+        const float2 vf = T % 3 == 0 ? vi + acc * (p.innerFriction / 2.0f) : vi;
+        s.velA[g] = vf * (1.0f - p.friction);
+        // decay (CellProcessor.cuh:775-858) on the state after the transition
+        const int col = s.color[g] % ALIEN_B200_MAX_COLORS;
+        uint32_t f = 0;
+        if (e > p.cellMaxBindingEnergy) f |= kFlagDelAll;
+        if (ls == ALIEN_B200_LIVING_DYING || ls == ALIEN_B200_LIVING_DETACHING) {
+            if (draw(s.id[g], T, kSiteDeath) < p.cellDeathProbability[col]) f |= kFlagDelCell;
+        }
+        bool destroy = e < p.cellMinEnergy[col];
+        const long long maxAge = p.cellMaxAge[col];
+        if (maxAge > 0 && static_cast<long long>(s.age[g]) > maxAge) destroy = true;
+        if (destroy) {
+            f |= kFlagSetDying;
+            if (ls != ALIEN_B200_LIVING_DYING) {
+                f |= kFlagNewDying;
+                for (int k = 0; k < n; ++k) atomicOr(&s.flags[s.bond[g * kMaxBonds + k]], kFlagDetachFromDying);
+            }
+        }
+        if (f) atomicOr(&s.flags[g], f);
     } else {
         PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
         if (!c.inRange) return;
@@ -837,41 +878,6 @@ __global__ void __launch_bounds__(kBlock) kTransition(DevState s)
             s.pflag[q] |= 2u;
         }
     }
-}
-
-// ------------------------------------------------------------- kDecay ----
-// applyFriction + decay (CellProcessor.cuh:707-723, 775-858).
-__global__ void __launch_bounds__(kBlock) kDecay(DevState s)
-{
-    CellCtx c = cellCtx(s);
-    if (!c.valid) return;
-    const long long g = c.g;
-    const WorldInfo& wi = s.worlds[c.w];
-    const AlienPhysicsParams& p = s.params[wi.paramIndex];
-    const uint64_t T = s.counters[c.w].timestep;
-    const int ls = s.nextState[g];
-    s.livingState[g] = static_cast<uint8_t>(ls);
-    if (s.barrier[g]) return;
-    s.velA[g] = s.velA[g] * (1.0f - p.friction);
-    const int col = s.color[g] % ALIEN_B200_MAX_COLORS;
-    const float e = s.energy[g];
-    uint32_t f = 0;
-    if (e > p.cellMaxBindingEnergy) f |= kFlagDelAll;
-    if (ls == ALIEN_B200_LIVING_DYING || ls == ALIEN_B200_LIVING_DETACHING) {
-        if (draw(s.id[g], T, kSiteDeath) < p.cellDeathProbability[col]) f |= kFlagDelCell;
-    }
-    bool destroy = e < p.cellMinEnergy[col];
-    const long long maxAge = p.cellMaxAge[col];
-    if (maxAge > 0 && static_cast<long long>(s.age[g]) > maxAge) destroy = true;
-    if (destroy) {
-        f |= kFlagSetDying;
-        if (ls != ALIEN_B200_LIVING_DYING) {
-            f |= kFlagNewDying;
-            const int n = s.numConn[g];
-            for (int k = 0; k < n; ++k) atomicOr(&s.flags[s.bond[g * kMaxBonds + k]], kFlagDetachFromDying);
-        }
-    }
-    if (f) atomicOr(&s.flags[g], f);
 }
 
 // ---------------------------------------------------- bond additions -----
@@ -970,10 +976,12 @@ __global__ void __launch_bounds__(kBlock) kResolve(DevState s)
     if (!c.valid) return;
     const long long g = c.g;
     const uint32_t f = s.flags[g];
+    int ls = s.nextState[g];
     if (f & kFlagSetDying)
-        s.livingState[g] = ALIEN_B200_LIVING_DYING;
-    else if ((f & kFlagDetachFromDying) && s.livingState[g] != ALIEN_B200_LIVING_DYING)
-        s.livingState[g] = ALIEN_B200_LIVING_DETACHING;
+        ls = ALIEN_B200_LIVING_DYING;
+    else if ((f & kFlagDetachFromDying) && ls != ALIEN_B200_LIVING_DYING)
+        ls = ALIEN_B200_LIVING_DETACHING;
+    s.livingState[g] = static_cast<uint8_t>(ls);
 
     const int j = s.best[g];
     if (j < 0 || j <= g || s.best[j] != g) return;
@@ -984,15 +992,15 @@ __global__ void __launch_bounds__(kBlock) kResolve(DevState s)
     BondList l1, l2;
     if (!tryAddOneWay(s, wi, c1, c2, pd, l1)) return;
     if (!tryAddOneWay(s, wi, c2, c1, pd * -1.0f, l2)) return;
-    const BondList* ls[2] = {&l1, &l2};
+    const BondList* lists[2] = {&l1, &l2};
     const long long cs[2] = {c1, c2};
     for (int m = 0; m < 2; ++m) {
         const long long x = cs[m];
-        s.addNum[x] = static_cast<uint8_t>(ls[m]->n);
+        s.addNum[x] = static_cast<uint8_t>(lists[m]->n);
         for (int k = 0; k < kMaxBonds; ++k) {
-            s.addBond[x * kMaxBonds + k] = k < ls[m]->n ? ls[m]->b[k] : -1;
-            s.addDist[x * kMaxBonds + k] = ls[m]->d[k];
-            s.addAngle[x * kMaxBonds + k] = ls[m]->a[k];
+            s.addBond[x * kMaxBonds + k] = k < lists[m]->n ? lists[m]->b[k] : -1;
+            s.addDist[x * kMaxBonds + k] = lists[m]->d[k];
+            s.addAngle[x * kMaxBonds + k] = lists[m]->a[k];
         }
     }
     s.newPartner[c1] = static_cast<int>(c2);
@@ -1019,6 +1027,7 @@ __global__ void __launch_bounds__(kBlock) kCommit(DevState s)
     const int np = s.newPartner[g];
     BondList l;
     if (np >= 0) {
+        s.newPartner[g] = -1;
         l.n = s.addNum[g];
         for (int k = 0; k < kMaxBonds; ++k) {
             l.b[k] = s.addBond[g * kMaxBonds + k];
@@ -1142,6 +1151,10 @@ __global__ void kEventWorld(DevState s)
     const uint32_t S = warpScanBlocks(s.blockSplit, wi.firstPartBlock, wi.numPartBlocks);
     if ((threadIdx.x & 31) != 0) return;
     WorldCounters& wc = s.counters[w];
+    if (!wc.active) {
+        wc.numEvents = 0;
+        return;
+    }
     const unsigned long long id0 = wc.nextId;
     const uint32_t slot0 = wc.numParticles;
     wc.radIdBase = id0;
@@ -1161,6 +1174,7 @@ __global__ void kEventWorld(DevState s)
         wc.numParticles = static_cast<uint32_t>(want);
     }
     wc.timestep += 1;
+    if (wc.stepsRemaining != ~0ull && --wc.stepsRemaining == 0) wc.active = 0;
 }
 
 __device__ __forceinline__ void emitParticle(const DevState& s, const WorldInfo& wi, uint32_t slotRel, unsigned long long id,
@@ -1184,12 +1198,14 @@ __global__ void __launch_bounds__(kBlock) kEventEmit(DevState s)
     if (blockIdx.x < s.numCellBlocks) {
         const int w = s.cellBlockWorld[blockIdx.x];
         const WorldCounters& wc = s.counters[w];
+        const long long g = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+        const uint32_t fl = s.flags[g];
+        if (fl) s.flags[g] = 0;  // the step's flags end here
         if (wc.numEvents == 0) return;
         const WorldInfo& wi = s.worlds[w];
-        const long long g = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
         const bool inRange = g < wi.cellBase + wc.numCells;
-        const uint32_t rad = inRange && (s.flags[g] & kFlagRadiation) ? 1u : 0u;
-        const uint32_t del = inRange && delEvent(s, g) ? 1u : 0u;
+        const uint32_t rad = inRange && (fl & kFlagRadiation) ? 1u : 0u;
+        const uint32_t del = inRange && (fl & kFlagDelCell) && s.energy[g] > kNearZero ? 1u : 0u;
         const uint32_t rr = blockExclusiveScan(rad, nullptr) + s.blockRad[blockIdx.x];
         const uint32_t dr = blockExclusiveScan(del, nullptr) + s.blockDel[blockIdx.x];
         if (rad) emitParticle(s, wi, wc.radSlotBase + rr, wc.radIdBase + rr, s.radPos[g], s.radVel[g], s.radEnergy[g], s.color[g]);

@@ -187,6 +187,26 @@ class BatchSimulation:
         check(self._lib.alien_b200_batch_get_raw_statistics(self._h, int(world), ctypes.byref(r)))
         return r
 
+    def set_step_budget(self, world: int, steps: int) -> None:
+        """world steps ``steps`` more times and then stops (0 = no limit)"""
+        check(self._lib.alien_b200_batch_set_step_budget(self._h, int(world), int(steps)))
+
+    def world_status(self, world: int):
+        """(timestep, steps remaining, active)"""
+        t, r, a = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int()
+        check(self._lib.alien_b200_batch_world_status(self._h, int(world), ctypes.byref(t), ctypes.byref(r),
+                                                      ctypes.byref(a)))
+        return t.value, r.value, bool(a.value)
+
+    def num_active(self) -> int:
+        n = int(self._lib.alien_b200_batch_num_active(self._h))
+        if n < 0:
+            raise RuntimeError(_lib.last_error())
+        return n
+
+    def device_bytes(self) -> int:
+        return int(self._lib.alien_b200_batch_device_bytes(self._h))
+
     def stream(self) -> int:
         return int(self._lib.alien_b200_batch_stream(self._h) or 0)
 

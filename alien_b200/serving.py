@@ -1,0 +1,187 @@
+"""Continuous-batching serving loop for simulation requests.
+
+No counterpart in the reference (its EngineWorker serves one world).  A
+request is a world (DataTO, size, parameters) and a number of timesteps.  The
+loop keeps every admitted world resident on the device and steps all of them
+together:
+
+* admission: a waiting request is admitted when its estimated device bytes fit
+  into the HBM budget next to the resident worlds; requests that arrive while
+  others run are admitted at the next tick (no queue barrier);
+* cohorts: each admission wave becomes one batch arena (alien_b200_batch)
+  whose worlds carry per-world step budgets, so a world stops exactly after
+  its requested steps without host synchronisation;
+* a tick = one timestep of every cohort with active worlds, issued back to
+  back on the GPU; its duration is the per-step latency every running request
+  sees (p50 / p99 reported);
+* a cohort whose worlds are all done is read back (results) and freed, which
+  returns its bytes to the budget.
+
+Results do not depend on what else is resident: every world evolves under the
+same deterministic step as alone (tests/test_batch_gpu.py checks alone vs in
+the mix).
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+from typing import Callable
+
+import numpy as np
+
+from .facade import BatchSimulation
+from .params import PhysicsParams
+from .to import DataTO
+
+# device bytes per cell and per particle slot of an arena (engine.cu::build),
+# plus the per-world particle map; used for admission before allocating
+BYTES_PER_CELL_SLOT = 760
+BYTES_PER_PARTICLE_SLOT = 130
+
+
+def estimate_bytes(data: DataTO, world) -> int:
+    n, p = data.num_cells, data.num_particles
+    cell_slots = n + 256
+    part_slots = p + n + max(4096, (p + n) // 2) + 256
+    return (BYTES_PER_CELL_SLOT * cell_slots + BYTES_PER_PARTICLE_SLOT * part_slots
+            + 4 * world[0] * world[1] + 304 * n)
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    data: DataTO
+    world: tuple
+    params: PhysicsParams
+    steps: int
+    arrival: float = 0.0
+    admitted: float | None = None
+    finished: float | None = None
+    result: DataTO | None = None
+    cells: int = 0
+
+
+class _Cohort:
+    def __init__(self, requests: list[Request]):
+        self.requests = requests
+        self.batch = BatchSimulation([(r.data, r.world, r.params) for r in requests])
+        for w, r in enumerate(requests):
+            self.batch.set_step_budget(w, r.steps)
+        self.bytes = self.batch.device_bytes()
+        self.max_steps = max(r.steps for r in requests)
+        self.steps_done = 0
+
+    @property
+    def done(self) -> bool:
+        return self.steps_done >= self.max_steps
+
+    def close(self, now: float, keep_results: bool):
+        for w, r in enumerate(self.requests):
+            r.finished = now
+            if keep_results:
+                r.result = self.batch.get_simulation_data(w)
+        self.batch.close()
+
+
+class ServingLoop:
+    def __init__(self, hbm_budget_bytes: int, keep_results: bool = False, max_cohort_worlds: int = 256):
+        self.budget = int(hbm_budget_bytes)
+        self.keep_results = keep_results
+        self.max_cohort_worlds = max_cohort_worlds
+        self.waiting: list[Request] = []
+        self.cohorts: list[_Cohort] = []
+        self.finished: list[Request] = []
+        self.tick_ms: list[float] = []
+        self.cell_steps = 0
+
+    def resident_bytes(self) -> int:
+        return sum(c.bytes for c in self.cohorts)
+
+    def submit(self, req: Request) -> None:
+        self.waiting.append(req)
+
+    def _admit(self, now: float) -> None:
+        free = self.budget - self.resident_bytes()
+        wave, wave_bytes = [], 0
+        rest = []
+        for r in self.waiting:
+            b = estimate_bytes(r.data, r.world)
+            if len(wave) < self.max_cohort_worlds and wave_bytes + b <= free:
+                wave.append(r)
+                wave_bytes += b
+            else:
+                rest.append(r)
+        self.waiting = rest
+        if wave:
+            for r in wave:
+                r.admitted = now
+                r.cells = r.data.num_cells
+            self.cohorts.append(_Cohort(wave))
+
+    def tick(self, now: float) -> float:
+        """admit, then one timestep of every running cohort; returns ms"""
+        self._admit(now)
+        if not self.cohorts:
+            return 0.0
+        ms = 0.0
+        for c in self.cohorts:
+            ms += c.batch.time_timesteps(1)
+            live = sum(r.cells for r in c.requests if c.steps_done < r.steps)
+            self.cell_steps += live
+            c.steps_done += 1
+        self.tick_ms.append(ms)
+        done_now = time.perf_counter()
+        keep = []
+        for c in self.cohorts:
+            if c.done:
+                c.close(done_now, self.keep_results)
+                self.finished.extend(c.requests)
+            else:
+                keep.append(c)
+        self.cohorts = keep
+        return ms
+
+    def idle(self) -> bool:
+        return not self.cohorts and not self.waiting
+
+    def report(self, wall_s: float) -> dict:
+        t = np.array(self.tick_ms) if self.tick_ms else np.zeros(1)
+        return {
+            "requests_finished": len(self.finished),
+            "requests_waiting": len(self.waiting),
+            "ticks": len(self.tick_ms),
+            "p50_step_ms": float(np.percentile(t, 50)),
+            "p99_step_ms": float(np.percentile(t, 99)),
+            "cell_steps": int(self.cell_steps),
+            "mcell_steps_per_s": self.cell_steps / max(wall_s, 1e-9) / 1e6,
+        }
+
+
+def run_poisson(make_request: Callable[[int, np.random.Generator], Request], rate_per_s: float, duration_s: float,
+                hbm_budget_bytes: int, seed: int = 0, keep_results: bool = False, drain: bool = True) -> dict:
+    """Poisson arrivals at ``rate_per_s`` for ``duration_s`` seconds of wall
+    time; requests are built by ``make_request(rid, rng)``."""
+    rng = np.random.default_rng(seed)
+    loop = ServingLoop(hbm_budget_bytes, keep_results)
+    t0 = time.perf_counter()
+    next_arrival = rng.exponential(1.0 / rate_per_s)
+    rid = 0
+    while True:
+        now = time.perf_counter() - t0
+        while now < duration_s and next_arrival <= now:
+            req = make_request(rid, rng)
+            req.arrival = next_arrival
+            loop.submit(req)
+            rid += 1
+            next_arrival += rng.exponential(1.0 / rate_per_s)
+        if now >= duration_s and (not drain or loop.idle()):
+            break
+        if loop.idle():
+            time.sleep(max(0.0, min(next_arrival - now, 0.01)))
+            continue
+        loop.tick(now)
+    wall = time.perf_counter() - t0
+    out = loop.report(wall)
+    out["requests_submitted"] = rid
+    out["wall_s"] = wall
+    return out

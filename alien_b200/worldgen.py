@@ -373,3 +373,84 @@ def random_test_world(seed: int, world=(64, 64), clusters: int = 6, free_cells: 
     parts["energy"] = rng.uniform(0.005, 3.0, particles).astype(np.float32)
     parts_list.append(parts)
     return DataTO(cells, np.concatenate(parts_list)), world
+
+
+def _separated_points(rng, count, world, occupied: np.ndarray, min_sep: float, max_tries: int = 200):
+    """uniform points at least ``min_sep`` from each other and from ``occupied``"""
+    sx, sy = world
+    pts = [p for p in occupied]
+    out = []
+    cell = max(min_sep, 1.0)
+    nbx, nby = max(1, int(sx // cell)), max(1, int(sy // cell))
+    grid = {}
+
+    def key(p):
+        return int(p[0] // cell) % nbx, int(p[1] // cell) % nby
+
+    for i, p in enumerate(pts):
+        grid.setdefault(key(p), []).append(p)
+    tries = 0
+    while len(out) < count:
+        tries += 1
+        if tries > max_tries * max(count, 1):
+            raise RuntimeError("cannot place separated points")
+        c = rng.uniform(0, 1, 2) * (sx, sy)
+        bx, by = key(c)
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for q in grid.get(((bx + dx) % nbx, (by + dy) % nby), ()):
+                    d = c - q
+                    d -= np.round(d / (sx, sy)) * (sx, sy)
+                    if d[0] * d[0] + d[1] * d[1] < min_sep * min_sep:
+                        ok = False
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if ok:
+            out.append(c)
+            grid.setdefault((bx, by), []).append(c)
+    return np.array(out, np.float64).reshape(-1, 2)
+
+
+def calm_test_world(seed: int, world=(64, 64), clusters: int = 4, hex_clusters: int = 1, free_cells: int = 120,
+                    particles: int = 20, vmax: float = 0.05, particle_speed: float = 0.3):
+    """A world in which no lock, no random draw and no in-place update of the
+    reference can change the outcome of a step: slow objects (no fusion, no
+    force decay), free cells and particles at least 1.5 apart from everything,
+    energies above cellMinEnergy.  Used to pin the oracle against the
+    reference engine step for step."""
+    rng = np.random.default_rng(seed)
+    rect, hexa = rect_template(), hex_template()
+    centres = _place_clusters(rng, clusters + hex_clusters, world, max(rect.radius, hexa.radius) + 1.0)
+    parts_cells = []
+    next_id, offset = 1, 0
+    for tmpl, cs in ((rect, centres[:clusters]), (hexa, centres[clusters:])):
+        if len(cs) == 0:
+            continue
+        c = _clusters_to_cells(tmpl, cs, rng.uniform(-vmax, vmax, (len(cs), 2)), rng.uniform(-0.005, 0.005, len(cs)),
+                               100.0, next_id, world, creature_base=1 + len(parts_cells))
+        c["connections"]["cellIndex"] += np.where(np.arange(6)[None, :] < c["numConnections"][:, None], offset, 0).astype(np.int32)
+        next_id += len(c)
+        offset += len(c)
+        parts_cells.append(c)
+    cluster_cells = np.concatenate(parts_cells)
+    occupied = cluster_cells["pos"].astype(np.float64)
+    free_pos = _separated_points(rng, free_cells, world, occupied, 1.5)
+    free = empty_cells(free_cells)
+    free["id"] = np.arange(next_id, next_id + free_cells, dtype=np.uint64)
+    free["pos"] = free_pos.astype(np.float32)
+    free["vel"] = rng.uniform(-vmax, vmax, (free_cells, 2)).astype(np.float32)
+    free["energy"] = rng.uniform(60, 120, free_cells).astype(np.float32)
+    free["maxConnections"] = 6
+    next_id += free_cells
+    cells = np.concatenate([cluster_cells, free])
+    ppos = _separated_points(rng, particles, world, cells["pos"].astype(np.float64), 3.0)
+    parts = np.zeros(particles, PARTICLE_TO)
+    parts["id"] = np.arange(next_id, next_id + particles, dtype=np.uint64)
+    parts["pos"] = ppos.astype(np.float32)
+    parts["vel"] = rng.uniform(-particle_speed, particle_speed, (particles, 2)).astype(np.float32)
+    parts["energy"] = rng.uniform(0.5, 2.0, particles).astype(np.float32)
+    return DataTO(cells, parts), world

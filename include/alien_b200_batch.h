@@ -31,6 +31,15 @@ int alien_b200_batch_enqueue_timesteps(alien_b200_batch* batch, uint64_t timeste
 int alien_b200_batch_get_data(alien_b200_batch* batch, int world, const AlienDataTO* data);
 int alien_b200_batch_get_array_sizes(alien_b200_batch* batch, int world, AlienArraySizes* sizes);
 int alien_b200_batch_get_raw_statistics(alien_b200_batch* batch, int world, AlienRawStatistics* statistics);
+/* World `world` steps `steps` more times and then stops (its state stays
+ * resident and readable); 0 = no limit.  Worlds start active, unlimited. */
+int alien_b200_batch_set_step_budget(alien_b200_batch* batch, int world, uint64_t steps);
+int alien_b200_batch_world_status(alien_b200_batch* batch, int world, uint64_t* timestep, uint64_t* stepsRemaining,
+                                  int* active);
+/* number of worlds still stepping (-1 on error) */
+int alien_b200_batch_num_active(alien_b200_batch* batch);
+/* device memory held by the batch's arena */
+uint64_t alien_b200_batch_device_bytes(alien_b200_batch* batch);
 void* alien_b200_batch_stream(alien_b200_batch* batch);
 uint64_t alien_b200_batch_kernel_launch_count(alien_b200_batch* batch);
 int alien_b200_batch_kernels_per_step(alien_b200_batch* batch);

@@ -1,0 +1,174 @@
+// ref_run - drives the reference's own CUDA engine (_SimulationCudaFacade,
+// source/EngineGpuKernels/SimulationCudaFacade.cuh:27-139) at the DataTO
+// level.  TEST INFRASTRUCTURE: it is the reference arm of the benchmark and
+// the pin of the CPU oracle; the B200 engine never calls it.
+//
+//   ref_run <input> <output>
+//
+// input : "ALRF" u32 version, i32 W, i32 H, u64 timestep, u64 warmup,
+//         u64 steps, AlienPhysicsParams, u64 numCells, u64 numParticles,
+//         u64 numAux, CellTO[numCells], ParticleTO[numParticles], aux bytes
+// output: "ALRO" u32 version, u64 numCells, u64 numParticles, u64 numAux,
+//         double seconds (timed steps, wall clock around calcTimestep),
+//         u64 timestep, CellTO[], ParticleTO[], aux bytes
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <vector>
+
+#include "EngineGpuKernels/SimulationCudaFacade.cuh"
+#include "EngineGpuKernels/TOs.cuh"
+#include "EngineInterface/Settings.h"
+
+#include "../../include/alien_b200.h"
+
+static_assert(sizeof(CellTO) == sizeof(AlienCellTO), "CellTO layout");
+static_assert(sizeof(ParticleTO) == sizeof(AlienParticleTO), "ParticleTO layout");
+
+namespace
+{
+template <class T>
+void readOrThrow(FILE* f, T* p, size_t n = 1)
+{
+    if (n && fread(p, sizeof(T), n, f) != n) throw std::runtime_error("short read");
+}
+template <class T>
+void writeOrThrow(FILE* f, T const* p, size_t n = 1)
+{
+    if (n && fwrite(p, sizeof(T), n, f) != n) throw std::runtime_error("short write");
+}
+
+// AlienPhysicsParams -> SimulationParameters (the fields the physics stage
+// reads; everything else keeps the reference defaults)
+SimulationParameters toReference(AlienPhysicsParams const& a)
+{
+    SimulationParameters p;
+    p.timestepSize = a.timestepSize;
+    p.motionType = a.motionType;
+    if (a.motionType == MotionType_Fluid) {
+        p.motionData.fluidMotion.smoothingLength = a.smoothingLength;
+        p.motionData.fluidMotion.viscosityStrength = a.viscosityStrength;
+        p.motionData.fluidMotion.pressureStrength = a.pressureStrength;
+    } else {
+        p.motionData.collisionMotion.cellMaxCollisionDistance = a.cellMaxCollisionDistance;
+        p.motionData.collisionMotion.cellRepulsionStrength = a.cellRepulsionStrength;
+    }
+    p.innerFriction = a.innerFriction;
+    p.cellMaxVelocity = a.cellMaxVelocity;
+    p.cellMinDistance = a.cellMinDistance;
+    p.cellMaxForceDecayProb = a.cellMaxForceDecayProb;
+    p.radiationProb = a.radiationProb;
+    p.radiationVelocityMultiplier = a.radiationVelocityMultiplier;
+    p.radiationVelocityPerturbation = a.radiationVelocityPerturbation;
+    p.cellDeathConsequences = a.cellDeathConsequences;
+    p.baseValues.friction = a.friction;
+    p.baseValues.rigidity = a.rigidity;
+    p.baseValues.cellFusionVelocity = a.cellFusionVelocity;
+    p.baseValues.cellMaxBindingEnergy = a.cellMaxBindingEnergy;
+    for (int c = 0; c < MAX_COLORS; ++c) {
+        p.cellMaxBindingDistance[c] = a.cellMaxBindingDistance[c];
+        p.radiationMinCellAge[c] = a.radiationMinCellAge[c];
+        p.highRadiationFactor[c] = a.highRadiationFactor[c];
+        p.highRadiationMinCellEnergy[c] = a.highRadiationMinCellEnergy[c];
+        p.cellMaxAge[c] = a.cellMaxAge[c];
+        p.particleSplitEnergy[c] = a.particleSplitEnergy[c];
+        p.baseValues.radiationAbsorption[c] = a.radiationAbsorption[c];
+        p.baseValues.radiationCellAgeStrength[c] = a.radiationCellAgeStrength[c];
+        p.baseValues.cellMaxForce[c] = a.cellMaxForce[c];
+        p.baseValues.cellMinEnergy[c] = a.cellMinEnergy[c];
+        p.baseValues.cellDeathProbability[c] = a.cellDeathProbability[c];
+    }
+    return p;
+}
+}  // namespace
+
+int main(int argc, char** argv)
+{
+    if (argc != 3) {
+        fprintf(stderr, "usage: ref_run <input> <output>\n");
+        return 2;
+    }
+    try {
+        FILE* in = fopen(argv[1], "rb");
+        if (!in) throw std::runtime_error("cannot open input");
+        char magic[4];
+        uint32_t version;
+        int32_t W, H;
+        uint64_t timestep, warmup, steps, nc, np, na;
+        AlienPhysicsParams params;
+        readOrThrow(in, magic, 4);
+        if (std::memcmp(magic, "ALRF", 4) != 0) throw std::runtime_error("bad magic");
+        readOrThrow(in, &version);
+        readOrThrow(in, &W);
+        readOrThrow(in, &H);
+        readOrThrow(in, &timestep);
+        readOrThrow(in, &warmup);
+        readOrThrow(in, &steps);
+        readOrThrow(in, &params);
+        readOrThrow(in, &nc);
+        readOrThrow(in, &np);
+        readOrThrow(in, &na);
+        std::vector<CellTO> cells(nc + 1);
+        std::vector<ParticleTO> particles(np + 1);
+        std::vector<uint8_t> aux(na + 1);
+        readOrThrow(in, cells.data(), nc);
+        readOrThrow(in, particles.data(), np);
+        readOrThrow(in, aux.data(), na);
+        fclose(in);
+
+        Settings settings;
+        settings.generalSettings.worldSizeX = W;
+        settings.generalSettings.worldSizeY = H;
+        settings.simulationParameters = toReference(params);
+        auto facade = std::make_shared<_SimulationCudaFacade>(timestep, settings);
+
+        // pre-size the arrays: no timed step includes a resize
+        ArraySizes additional{nc * 2 + 1000, (np + nc) * 2 + 1000, na + 1000};
+        facade->resizeArraysIfNecessary(additional);
+
+        DataTO to;
+        uint64_t ncIn = nc, npIn = np, naIn = na;
+        to.numCells = &ncIn;
+        to.cells = cells.data();
+        to.numParticles = &npIn;
+        to.particles = particles.data();
+        to.numAuxiliaryData = &naIn;
+        to.auxiliaryData = aux.data();
+        facade->setSimulationData(to);
+
+        facade->calcTimestep(warmup, false);
+        auto t0 = std::chrono::steady_clock::now();
+        facade->calcTimestep(steps, false);
+        auto t1 = std::chrono::steady_clock::now();
+        double seconds = std::chrono::duration<double>(t1 - t0).count();
+
+        ArraySizes sizes = facade->getArraySizes();
+        DataTO out;
+        out.init(sizes);
+        facade->getSimulationData({-10, -10}, {W + 10, H + 10}, out);
+        uint64_t ts = facade->getCurrentTimestep();
+
+        FILE* o = fopen(argv[2], "wb");
+        if (!o) throw std::runtime_error("cannot open output");
+        writeOrThrow(o, "ALRO", 4);
+        uint32_t v = 1;
+        writeOrThrow(o, &v);
+        writeOrThrow(o, out.numCells);
+        writeOrThrow(o, out.numParticles);
+        writeOrThrow(o, out.numAuxiliaryData);
+        writeOrThrow(o, &seconds);
+        writeOrThrow(o, &ts);
+        writeOrThrow(o, out.cells, *out.numCells);
+        writeOrThrow(o, out.particles, *out.numParticles);
+        writeOrThrow(o, out.auxiliaryData, *out.numAuxiliaryData);
+        fclose(o);
+        out.destroy();
+        facade.reset();
+    } catch (std::exception const& e) {
+        fprintf(stderr, "ref_run: %s\n", e.what());
+        return 1;
+    }
+    return 0;
+}

@@ -1,0 +1,101 @@
+"""Generates the golden fixtures of the reference engine (run on a GPU box).
+
+    python tests/golden/make_golden.py <out_dir>
+
+For each seeded input below it runs the reference's own CUDA engine
+(oracle/_ref/ref_run, built from the reference sources by oracle/ref/Makefile)
+and stores the input DataTO and the reference's output (one step) as
+compressed npz, or, for long runs, the reference's aggregate observables as
+JSON.  The CPU tests (tests/test_golden.py) check the oracle against these
+files; the inputs are regenerated from their seeds and compared byte for
+byte with the stored copy.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from alien_b200 import params as P  # noqa: E402
+from alien_b200 import worldgen  # noqa: E402
+from oracle import refrun  # noqa: E402
+
+ONE_STEP = [
+    # name, seed, motion, timestep
+    ("calm_fluid_t0", 21, P.MOTION_FLUID, 0),
+    ("calm_fluid_t1", 22, P.MOTION_FLUID, 1),
+    ("calm_collision_t0", 23, P.MOTION_COLLISION, 0),
+    ("calm_collision_t2", 24, P.MOTION_COLLISION, 2),
+]
+
+
+def calm(seed):
+    return worldgen.calm_test_world(seed)
+
+
+def observables(data):
+    c, p = data.cells, data.particles
+    speed = np.hypot(c["vel"][:, 0].astype(np.float64), c["vel"][:, 1].astype(np.float64))
+    hist, _ = np.histogram(speed, bins=20, range=(0.0, 2.0))
+    return {
+        "cells": int(len(c)), "particles": int(len(p)),
+        "bonds": int(np.sum(c["numConnections"])),
+        "cell_energy": float(np.sum(c["energy"], dtype=np.float64)),
+        "particle_energy": float(np.sum(p["energy"], dtype=np.float64)),
+        "mean_speed": float(speed.mean()) if len(c) else 0.0,
+        "speed_hist": hist.tolist(),
+        "dying_or_detaching": int(np.sum((c["livingState"] == 3) | (c["livingState"] == 5))),
+    }
+
+
+LONG_RUNS = {
+    # name: (builder, motion, steps)
+    "stats_softbody": (lambda: worldgen.soft_body_world(seed=5, world=(128, 128), clusters=20, particles=1500), P.MOTION_FLUID, 300),
+    "stats_fluid": (lambda: worldgen.fluid_world(seed=6, world=(128, 128), cells=3900), P.MOTION_FLUID, 300),
+    "stats_hex": (lambda: worldgen.hex_world(seed=7, world=(256, 256), clusters=120), P.MOTION_COLLISION, 300),
+}
+
+
+def decay_input():
+    """CellConnectionTests.decay (EngineTests/CellConnectionTests.cpp:19-37)"""
+    tmpl = worldgen.rect_template()
+    cells = worldgen._clusters_to_cells(tmpl, np.zeros((1, 2)), np.zeros((1, 2)), np.zeros(1), 25.0, 1, (1000, 1000))
+    prm = P.benchmark_parameters()
+    prm.radiationAbsorption[0] = 0.0
+    prm.cellDeathConsequences = 1
+    prm.cellDeathProbability[0] = 0.5
+    from alien_b200.to import DataTO
+    return DataTO(cells), (1000, 1000), prm
+
+
+def main(out_dir):
+    os.makedirs(out_dir, exist_ok=True)
+    for name, seed, motion, t in ONE_STEP:
+        data, world = calm(seed)
+        prm = P.benchmark_parameters(motion)
+        out, _, ts = refrun.run(data, world, prm, steps=1, timestep=t)
+        np.savez_compressed(os.path.join(out_dir, f"ref_{name}.npz"), in_cells=data.cells, in_particles=data.particles,
+                            out_cells=out.cells, out_particles=out.particles,
+                            meta=np.array([seed, motion, t, world[0], world[1], ts], np.int64))
+        print(name, out.num_cells, out.num_particles, ts)
+    summary = {}
+    for name, (builder, motion, steps) in LONG_RUNS.items():
+        data, world = builder()
+        prm = P.benchmark_parameters(motion)
+        out, seconds, ts = refrun.run(data, world, prm, steps=steps)
+        summary[name] = {"steps": steps, "motion": motion, "world": list(world), "initial": observables(data),
+                         "final": observables(out)}
+        print(name, summary[name]["final"])
+    data, world, prm = decay_input()
+    out, _, _ = refrun.run(data, world, prm, steps=1000)
+    summary["decay"] = {"steps": 1000, "initial": observables(data), "final": observables(out)}
+    print("decay", summary["decay"]["final"])
+    with open(os.path.join(out_dir, "ref_observables.json"), "w") as f:
+        json.dump(summary, f, indent=1)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))

@@ -1,0 +1,106 @@
+"""The oracle against the reference engine's own outputs.
+
+tests/golden/ref_*.npz and ref_observables.json were produced by the
+reference's CUDA engine (oracle/_ref/ref_run built from its sources) on a
+B200 by tests/golden/make_golden.py.  These CPU tests pin the oracle:
+
+* one step from "calm" worlds (no lock, random draw or in-place update of the
+  reference can change the outcome): ids, bond partners, bond counts, living
+  states and ages identical; positions, velocities and energies within
+  REF_RTOL * max(|x|, 1) -- the reference is built with -use_fast_math and
+  sums forces with float atomics, so it is not bit-reproducible itself;
+* long runs: aggregate observables (counts, energy, mean speed, speed
+  histogram) agree statistically, since the reference's races make its
+  trajectories nondeterministic.
+"""
+import glob
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from alien_b200 import params as P
+from alien_b200 import worldgen
+from alien_b200.to import DataTO
+from oracle.oracle import OracleSimulation
+from tests.helpers import compare_cells, compare_particles
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden")
+sys.path.insert(0, GOLDEN)
+import make_golden  # noqa: E402
+
+REF_RTOL = 2e-4
+FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "ref_calm_*.npz")))
+HAVE_OBSERVABLES = os.path.exists(os.path.join(GOLDEN, "ref_observables.json"))
+needs_observables = pytest.mark.skipif(not HAVE_OBSERVABLES, reason="reference observables not generated yet")
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p) for p in FIXTURES])
+def test_oracle_matches_reference_one_step(path):
+    f = np.load(path)
+    seed, motion, t, wx, wy, ts = (int(v) for v in f["meta"])
+    data, world = worldgen.calm_test_world(seed)
+    assert world == (wx, wy)
+    assert np.array_equal(data.cells, f["in_cells"]) and np.array_equal(data.particles, f["in_particles"]), \
+        "the seeded generator no longer reproduces the fixture input"
+    o = OracleSimulation(world, P.benchmark_parameters(motion), t)
+    o.set_simulation_data(data)
+    o.calc_timesteps(1)
+    assert o.current_timestep() == ts
+    got = o.get_simulation_data()
+    compare_cells(got.cells, f["out_cells"], world, rtol=REF_RTOL)
+    compare_particles(got.particles, f["out_particles"], world, rtol=REF_RTOL)
+
+
+@pytest.mark.skipif(not FIXTURES, reason="reference fixtures not generated yet")
+def test_fixtures_present():
+    assert len(FIXTURES) >= 4, "reference fixtures missing: run tests/golden/make_golden.py on a GPU box"
+    assert HAVE_OBSERVABLES
+
+
+def _obs(name):
+    with open(os.path.join(GOLDEN, "ref_observables.json")) as f:
+        return json.load(f)[name]
+
+
+def tv_distance(h1, h2):
+    a = np.asarray(h1, np.float64)
+    b = np.asarray(h2, np.float64)
+    return 0.5 * np.abs(a / max(a.sum(), 1) - b / max(b.sum(), 1)).sum()
+
+
+@needs_observables
+@pytest.mark.parametrize("name", list(make_golden.LONG_RUNS))
+def test_oracle_statistics_match_reference(name):
+    ref = _obs(name)
+    builder, motion, steps = make_golden.LONG_RUNS[name]
+    data, world = builder()
+    assert make_golden.observables(data) == ref["initial"]
+    o = OracleSimulation(world, P.benchmark_parameters(motion))
+    o.set_simulation_data(data)
+    o.calc_timesteps(steps)
+    got = make_golden.observables(o.get_simulation_data())
+    want = ref["final"]
+    e_got = got["cell_energy"] + got["particle_energy"]
+    e_want = want["cell_energy"] + want["particle_energy"]
+    assert abs(e_got - e_want) / e_want < 1e-3
+    assert abs(got["cells"] - want["cells"]) <= max(3, 0.02 * want["cells"])
+    assert abs(got["mean_speed"] - want["mean_speed"]) <= 0.1 * want["mean_speed"] + 1e-3
+    assert tv_distance(got["speed_hist"], want["speed_hist"]) < 0.1
+
+
+@needs_observables
+def test_decay_matches_reference():
+    ref = _obs("decay")
+    data, world, prm = make_golden.decay_input()
+    o = OracleSimulation(world, prm)
+    o.set_simulation_data(data)
+    o.calc_timesteps(ref["steps"])
+    got = make_golden.observables(o.get_simulation_data())
+    assert got["cells"] == ref["final"]["cells"] == 0
+    e_got = got["cell_energy"] + got["particle_energy"]
+    e_ref = ref["final"]["cell_energy"] + ref["final"]["particle_energy"]
+    assert abs(e_got - e_ref) / e_ref < 1e-3
