@@ -193,15 +193,16 @@ __device__ __forceinline__ float2 normalized2(float2 a)
 __device__ __forceinline__ float2 rotCW(float2 a) { return f2(-a.y, a.x); }
 __device__ __forceinline__ float2 rotCCW(float2 a) { return f2(a.y, -a.x); }
 
-// Math::angleOfVector, Math.cuh:140-155 (degrees, 0 = (0,-1))
+// Math::angleOfVector, Math.cuh:140-155 (degrees clockwise from (0,-1)).
+// The reference evaluates 90 - asin(-v.y/|v|) (v.x >= 0) or asin(..) + 270;
+// both branches equal 90 - atan2(-v.y, v.x) taken mod 360, which is evaluated
+// here because asin loses ~sqrt(eps) radians for near-vertical vectors.
 __device__ __forceinline__ float angleOfVector(float2 v)
 {
     float l = len2(v);
     if (l < kNearZero) return 0.0f;
-    float ny = -v.y / l;
-    ny = fmaxf(-1.0f, fminf(1.0f, ny));
-    float s = asinf(ny) * (180.0f / kPi);
-    return v.x >= 0.0f ? 90.0f - s : s + 270.0f;
+    float a = 90.0f - atan2f(-v.y, v.x) * (180.0f / kPi);
+    return a < 0.0f ? a + 360.0f : a;
 }
 // Math::unitVectorOfAngle, Math.cuh:134-138
 __device__ __forceinline__ float2 unitVectorOfAngle(float a)

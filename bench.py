@@ -32,6 +32,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Mcell-steps/s"
+T0 = time.perf_counter()
+
+
+def log(msg: str) -> None:
+    """progress on stderr (the JSON line is the only stdout output)"""
+    print(f"[bench {time.perf_counter() - T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
 # algorithmic bytes per cell per launch of each step kernel (FP32 SoA):
 # P1 hash build 24; P2 pair forces 40; P3 apply 24 + P4 bond forces 20+12b;
@@ -158,12 +164,14 @@ def cpu_baseline(data, world, prm, budget_s: float = 20.0, max_steps: int = 1000
     from oracle.oracle import OracleSimulation, library
 
     threads = library(precision).oracle_num_threads()
+    log(f"cpu baseline: {threads} threads")
     sim = OracleSimulation(world, prm, 0, precision=precision)
     sim.set_simulation_data(data)
     t0 = time.perf_counter()
     sim.calc_timesteps(1)  # warm-up step
     first = time.perf_counter() - t0
     steps = max(1, min(max_steps, int(budget_s / max(first, 1e-6))))
+    log(f"cpu baseline: first step {first:.2f} s, timing {steps} steps")
     t0 = time.perf_counter()
     sim.calc_timesteps(steps)
     dt = time.perf_counter() - t0
@@ -303,13 +311,17 @@ def main():
             dist.destroy_process_group()
         return 0
 
+    log(f"building workload {args.config}")
     data, world, prm, desc = build_workload(args.config, rank)
     n_cells = data.num_cells
+    log(f"workload: {n_cells} cells, {data.num_particles} particles")
     sim = SimulationFacade()
     sim.new_simulation(0, world, prm)
     sim.set_simulation_data(data)
+    log("set_simulation_data done; warm-up")
     sim.calc_timesteps(args.warmup)
     stats0 = sim.get_raw_statistics()
+    log("timed region")
     launches0 = sim.kernel_launches()
     barrier()
     with ClockSampler(local_rank) as clk:
@@ -322,6 +334,7 @@ def main():
     total_cells = sum_over_ranks(cells_mean)
     value = total_cells * args.steps / (ms / 1000.0) / 1e6
 
+    log(f"timed region: {ms / args.steps:.3f} ms/step")
     # per-kernel CUDA-event breakdown over a second stretch of the same run
     timed_steps = max(3, min(args.steps, 50))
     kernel_ms = sim.timed_timesteps(timed_steps)
@@ -338,6 +351,7 @@ def main():
 
     # end to end through the C ABI with host buffers: H2D of the world,
     # every step calc_timesteps(1) + a statistics read-back, D2H of the world
+    log("kernel breakdown done")
     e2e = None
     if not args.no_e2e:
         pins = [pin(data._cells), pin(data._particles)]
@@ -366,6 +380,7 @@ def main():
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "note": "set_simulation_data + per step (calc_timesteps(1) + get_raw_statistics) + get_simulation_data, pinned host buffers"}
 
+    log("e2e done")
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         cpu, _, _ = cpu_baseline(data, world, prm)

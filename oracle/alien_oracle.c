@@ -53,7 +53,7 @@ typedef REAL real;
 
 #if REAL_IS_FLOAT
 #define R_SQRT sqrtf
-#define R_ASIN asinf
+#define R_ATAN2 atan2f
 #define R_SIN sinf
 #define R_COS cosf
 #define R_REM remainderf
@@ -61,7 +61,7 @@ typedef REAL real;
 #define R_PI 3.1415926535897932384626433832795f
 #else
 #define R_SQRT sqrt
-#define R_ASIN asin
+#define R_ATAN2 atan2
 #define R_SIN sin
 #define R_COS cos
 #define R_REM remainder
@@ -97,16 +97,15 @@ static inline vec2 vnormalized(vec2 a)
 static inline vec2 rotCW(vec2 a) { return v2(-a.y, a.x); }
 static inline vec2 rotCCW(vec2 a) { return v2(a.y, -a.x); }
 
-/* Math::angleOfVector, Math.cuh:140-155 (0 degrees = (0,-1)) */
+/* Math::angleOfVector, Math.cuh:140-155 (degrees clockwise from (0,-1)):
+ * 90 - asin(-v.y/|v|) for v.x >= 0, asin(..) + 270 otherwise; both equal
+ * 90 - atan2(-v.y, v.x) mod 360, the well-conditioned form used here */
 static real angleOfVector(vec2 v)
 {
     real l = vlen(v);
     if (l < NEAR_ZERO) return 0;
-    real ny = -v.y / l;
-    ny = rmax((real)-1, rmin((real)1, ny));
-    real s = R_ASIN(ny) * RAD_TO_DEG;
-    if (v.x >= (real)0) return (real)90 - s;
-    return s + (real)270;
+    real a = (real)90 - R_ATAN2(-v.y, v.x) * RAD_TO_DEG;
+    return a < 0 ? a + (real)360 : a;
 }
 /* Math::unitVectorOfAngle, Math.cuh:134-138 */
 static vec2 unitVectorOfAngle(real a)
@@ -1281,6 +1280,15 @@ int64_t oracle_cell_slots(OracleWorld* w, int32_t* out, int64_t cap)
             ++n;
         }
     return n;
+}
+
+void oracle_set_threads(int n)
+{
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
 }
 
 int oracle_num_threads(void)

@@ -40,7 +40,22 @@ def _load(name: str) -> ctypes.CDLL:
     lib.oracle_cell_slots.restype = ctypes.c_int64
     lib.oracle_cell_slots.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
     lib.oracle_num_threads.restype = ctypes.c_int
+    lib.oracle_set_threads.argtypes = [ctypes.c_int]
     return lib
+
+
+def available_cpus() -> int:
+    """CPUs this process may use: the affinity mask, capped by a cgroup
+    CPU quota when one is set"""
+    n = len(os.sched_getaffinity(0))
+    try:
+        with open("/sys/fs/cgroup/cpu.max") as f:
+            quota, period = f.read().split()[:2]
+        if quota != "max":
+            n = min(n, max(1, int(int(quota) // int(period))))
+    except (OSError, ValueError):
+        pass
+    return max(1, n)
 
 
 _LIBS: dict[str, ctypes.CDLL] = {}
@@ -49,7 +64,12 @@ _LIBS: dict[str, ctypes.CDLL] = {}
 def library(precision: str = "f64") -> ctypes.CDLL:
     name = {"f64": "liboracle_f64.so", "f32": "liboracle_f32.so"}[precision]
     if name not in _LIBS:
+        # OpenMP threads must not outnumber the CPUs: spinning waiters on an
+        # oversubscribed host stall every barrier
+        os.environ.setdefault("OMP_WAIT_POLICY", "PASSIVE")
+        os.environ.setdefault("OMP_NUM_THREADS", str(available_cpus()))
         _LIBS[name] = _load(name)
+        _LIBS[name].oracle_set_threads(available_cpus())
     return _LIBS[name]
 
 
