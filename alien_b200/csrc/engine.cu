@@ -43,6 +43,8 @@ struct Error : std::runtime_error {
         }                                                                                                  \
     } while (0)
 
+#define launch(kernel, ...) launchNamed(#kernel, kernel, __VA_ARGS__)
+
 static inline long long roundUp(long long v, long long m) { return (v + m - 1) / m * m; }
 static inline int divUp(long long v, long long m) { return static_cast<int>((v + m - 1) / m); }
 
@@ -155,7 +157,7 @@ public:
 
 private:
     template <class K, class... A>
-    void launch(K kernel, int grid, int block, A... args)
+    void launchNamed(const char* name, K kernel, int grid, int block, A... args)
     {
         if (grid <= 0) return;
         kernel<<<grid, block, 0, stream_>>>(args...);
@@ -166,9 +168,16 @@ private:
             AB_CK(cudaEventCreate(&e));
             AB_CK(cudaEventRecord(e, stream_));
             timingEvents_->push_back(e);
+            timingNames_.push_back(name);
         }
     }
     std::vector<cudaEvent_t>* timingEvents_ = nullptr;
+    std::vector<const char*> timingNames_;
+
+public:
+    std::vector<std::string> lastTimedNames;
+
+private:
     void scan(const uint32_t* in, long long n, uint32_t* out);
     void releaseGraph()
     {
@@ -194,6 +203,7 @@ private:
     int kernelsPerStep_ = 0;
     cudaGraphExec_t graphExec_ = nullptr;
     uint64_t stepsSinceCheck_ = 0;
+    bool hasFluid_ = false, hasCollision_ = false;
 };
 
 // ------------------------------------------------------------- build -----
@@ -246,6 +256,13 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         maxWorldParts_ = std::max(maxWorldParts_, wi.partCap);
         if (ws.numAux) hw.aux.assign(ws.aux, ws.aux + ws.numAux);
         worlds_.push_back(std::move(hw));
+    }
+    hasFluid_ = hasCollision_ = false;
+    for (const HostWorld& hw : worlds_) {
+        if (hw.info.motionType == ALIEN_B200_MOTION_FLUID)
+            hasFluid_ = true;
+        else
+            hasCollision_ = true;
     }
     if (cellSlots >= (1ll << 31) || partSlots >= (1ll << 31) || tiles >= (1ll << 32) - 2)
         throw Error(ALIEN_B200_ERR_CAPACITY, "arena exceeds 2^31 slots");
@@ -427,7 +444,8 @@ void Arena::enqueueStep()
     scan(s.tileCount, s.numTiles, s.tileStart);
     launch(kScatter, cells, kBlock, s);
     launch(kStage, cells, kBlock, s);
-    launch(kPairs, cells, kBlock, s);
+    if (hasFluid_) launch(kPairsFluid, cells, kBlock, s);
+    if (hasCollision_) launch(kPairsCollision, cells, kBlock, s);
     launch(kApplyBond1, both, kBlock, s);
     launch(kVerletPos, both, kBlock, s);
     launch(kBond2, both, kBlock, s);
@@ -436,7 +454,7 @@ void Arena::enqueueStep()
     launch(kResolve, cells, kBlock, s);
     launch(kCommit, cells, kBlock, s);
     launch(kEventCount, both, kBlock, s);
-    launch(kEventWorld, divUp(static_cast<long long>(s.numWorlds) * 32, kBlock), kBlock, s);
+    launch(kEventWorld, s.numWorlds, kBlock, s);
     launch(kEventEmit, both, kBlock, s);
     kernelsPerStep_ = static_cast<int>(launches_ - before);
 }
@@ -477,6 +495,7 @@ std::vector<double> Arena::timedSteps(uint64_t n)
         AB_CK(cudaEventRecord(start, stream_));
         events.push_back(start);
         timingEvents_ = &events;
+        timingNames_.clear();
         try {
             enqueueStep();
         } catch (...) {
@@ -484,6 +503,7 @@ std::vector<double> Arena::timedSteps(uint64_t n)
             throw;
         }
         timingEvents_ = nullptr;
+        lastTimedNames.assign(timingNames_.begin(), timingNames_.end());
         AB_CK(cudaStreamSynchronize(stream_));
         if (sums.size() < events.size() - 1) sums.resize(events.size() - 1, 0.0);
         for (size_t k = 1; k < events.size(); ++k) {
@@ -968,19 +988,17 @@ int alien_b200_time_timesteps(alien_b200_simulation* sim, uint64_t timesteps, do
     });
 }
 
-static const char* const kKernelNames[] = {"kBin", "kScanReduce", "kScanPartials", "kScanDown", "kScatter", "kStage",
-                                           "kPairs", "kApplyBond1", "kVerletPos", "kBond2", "kVerletVel", "kTransition",
-                                           "kResolve", "kCommit", "kEventCount", "kEventWorld", "kEventEmit"};
+thread_local std::vector<std::string> g_timedNames;
 
 const char* alien_b200_step_kernel_name(int index)
 {
-    const int n = static_cast<int>(sizeof(kKernelNames) / sizeof(kKernelNames[0]));
-    return index >= 0 && index < n ? kKernelNames[index] : nullptr;
+    return index >= 0 && index < static_cast<int>(g_timedNames.size()) ? g_timedNames[index].c_str() : nullptr;
 }
 
 static int timedInto(Arena& a, uint64_t timesteps, double* kernelMs, int maxKernels, int* numKernels)
 {
     std::vector<double> sums = a.timedSteps(timesteps);
+    g_timedNames = a.lastTimedNames;
     const int n = static_cast<int>(sums.size());
     if (numKernels) *numKernels = n;
     for (int k = 0; k < n && k < maxKernels; ++k) kernelMs[k] = sums[k];

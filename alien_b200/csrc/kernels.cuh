@@ -66,11 +66,22 @@ __device__ __forceinline__ PartCtx partCtx(const DevState& s, int pb)
     return c;
 }
 
-__device__ __forceinline__ bool isBondedTo(const int* bonds, int n, int j)
+// bonds[] holds kMaxBonds entries, unused ones -1: a fixed-trip compare
+// keeps the list in registers
+__device__ __forceinline__ bool isBondedTo(const int* bonds, int j)
 {
     bool r = false;
-    for (int k = 0; k < n; ++k) r |= (bonds[k] == j);
+#pragma unroll
+    for (int k = 0; k < kMaxBonds; ++k) r |= (bonds[k] == j);
     return r;
+}
+
+// sqrtf(q) <= R decided exactly, with a cheap reject for the common far case
+__device__ __forceinline__ bool withinRadius(float q, float R, float R2reject, float& d)
+{
+    if (q > R2reject) return false;
+    d = sqrtf(q);
+    return d <= R;
 }
 
 constexpr int kMaxRadius = 15;
@@ -284,6 +295,7 @@ __device__ __forceinline__ void pairsFluid(const DevState& s, long long k)
     const AlienPhysicsParams& p = s.params[wi.paramIndex];
     const int W = wi.W, H = wi.H;
     const float h = p.smoothingLength, R = h * 2.0f, minDist = p.cellMinDistance;
+    const float R2reject = R * R * 1.0001f + 1e-6f;
     const float2 pi = f2(mpv.x, mpv.y), vi = f2(mpv.z, mpv.w);
     const bool barrierI = me.y & kStageBarrier;
     const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
@@ -307,8 +319,8 @@ __device__ __forceinline__ void pairsFluid(const DevState& s, long long k)
                 if (!(om.y & kStageVisible)) continue;
                 const float4 opv = s.stagedPV[m];
                 const float2 pd = correctDirection(pi - f2(opv.x, opv.y), W, H);
-                const float d = len2(pd);
-                if (!(d <= R)) continue;
+                float d;
+                if (!withinRadius(pd.x * pd.x + pd.y * pd.y, R, R2reject, d)) continue;
                 const int j = om.x;
                 if (om.y & kStageBarrier) {
                     if (bestBarrier < 0 || d < bestBarrierDist || (d == bestBarrierDist && j < bestBarrier)) {
@@ -323,7 +335,7 @@ __device__ __forceinline__ void pairsFluid(const DevState& s, long long k)
                     qDx += toFix(pd.x * minDist / 5.0f);
                     qDy += toFix(pd.y * minDist / 5.0f);
                 }
-                if (isBondedTo(bondsI, nI, j)) continue;
+                if (isBondedTo(bondsI, j)) continue;
                 const float2 vd = vi - f2(opv.z, opv.w);
                 const float densJ = __int_as_float(om.z);
                 const float factor = densI / (densI * densI) + densJ / (densJ * densJ);
@@ -417,6 +429,7 @@ __device__ __forceinline__ void pairsCollision(const DevState& s, long long k)
     const AlienPhysicsParams& p = s.params[wi.paramIndex];
     const int W = wi.W, H = wi.H;
     const float R = p.cellMaxCollisionDistance, minDist = p.cellMinDistance;
+    const float R2reject = R * R * 1.0001f + 1e-6f;
     const float2 pi = f2(mpv.x, mpv.y), vi = f2(mpv.z, mpv.w);
     const bool barrierI = me.y & kStageBarrier;
     const bool visibleI = me.y & kStageVisible;
@@ -439,12 +452,14 @@ __device__ __forceinline__ void pairsCollision(const DevState& s, long long k)
                 if (j == g) continue;
                 const float4 opv = s.stagedPV[m];
                 const float2 pj = f2(opv.x, opv.y);
-                if (!(len2(pj - pi) <= R)) continue;
+                const float2 raw = pj - pi;
+                float draw_;
+                if (!withinRadius(raw.x * raw.x + raw.y * raw.y, R, R2reject, draw_)) continue;
                 const bool visibleJ = om.y & kStageVisible;
                 if (!visibleJ && !visibleI) continue;
                 const float2 pd = correctDirection(pi - pj, W, H);
                 const float d = len2(pd);
-                const bool bonded = isBondedTo(bondsI, nI, j);
+                const bool bonded = isBondedTo(bondsI, j);
                 const float2 vj = f2(opv.z, opv.w);
                 if (visibleJ) {  // i's own scan sees j
                     if (!barrierI && d < minDist) {
@@ -482,16 +497,22 @@ __device__ __forceinline__ void pairsCollision(const DevState& s, long long k)
     s.best[g] = best;
 }
 
-// one thread per staged cell; the world's motion type selects the pair law
-__global__ void __launch_bounds__(kBlock) kPairs(DevState s)
+// one thread per staged cell; a launch serves the worlds of one motion type
+// (the host launches the kernel of every motion type present in the arena)
+__global__ void __launch_bounds__(kBlock, 3) kPairsFluid(DevState s)
 {
     const long long k = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
     if (k >= s.tileStart[s.numTiles]) return;
     const int w = (s.stagedMeta[k].y >> 16) & 0xffff;
-    if (s.worlds[w].motionType == ALIEN_B200_MOTION_FLUID)
-        pairsFluid(s, k);
-    else
-        pairsCollision(s, k);
+    if (s.worlds[w].motionType == ALIEN_B200_MOTION_FLUID) pairsFluid(s, k);
+}
+
+__global__ void __launch_bounds__(kBlock, 3) kPairsCollision(DevState s)
+{
+    const long long k = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    if (k >= s.tileStart[s.numTiles]) return;
+    const int w = (s.stagedMeta[k].y >> 16) & 0xffff;
+    if (s.worlds[w].motionType != ALIEN_B200_MOTION_FLUID) pairsCollision(s, k);
 }
 
 // ------------------------------------------------------- bond forces -----
@@ -1121,40 +1142,36 @@ __global__ void __launch_bounds__(kBlock) kEventCount(DevState s)
     }
 }
 
-__device__ uint32_t warpScanBlocks(uint32_t* arr, int first, int count)
+// exclusive scan of arr[first .. first+count) in place by one block;
+// returns the total
+__device__ uint32_t blockScanBlocks(uint32_t* arr, int first, int count)
 {
-    const int lane = threadIdx.x & 31;
     uint32_t carry = 0;
-    for (int base = 0; base < count; base += 32) {
-        const int k = base + lane;
+    for (int base = 0; base < count; base += kBlock) {
+        const int k = base + threadIdx.x;
         const uint32_t v = k < count ? arr[first + k] : 0u;
-        uint32_t x = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (k < count) arr[first + k] = carry + x - v;
-        carry += __shfl_sync(0xffffffffu, x, 31);
+        uint32_t total;
+        const uint32_t ex = blockExclusiveScan(v, &total);
+        if (k < count) arr[first + k] = carry + ex;
+        carry += total;
     }
     return carry;
 }
 
-// one warp per world: block offsets, id and slot bases, timestep advance
-__global__ void kEventWorld(DevState s)
+// one block per world: block offsets, id and slot bases, timestep advance
+__global__ void __launch_bounds__(kBlock) kEventWorld(DevState s)
 {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (w >= s.numWorlds) return;
-    const WorldInfo& wi = s.worlds[w];
-    const uint32_t R = warpScanBlocks(s.blockRad, wi.firstCellBlock, wi.numCellBlocks);
-    const uint32_t D = warpScanBlocks(s.blockDel, wi.firstCellBlock, wi.numCellBlocks);
-    const uint32_t S = warpScanBlocks(s.blockSplit, wi.firstPartBlock, wi.numPartBlocks);
-    if ((threadIdx.x & 31) != 0) return;
+    const int w = blockIdx.x;
     WorldCounters& wc = s.counters[w];
     if (!wc.active) {
-        wc.numEvents = 0;
+        if (threadIdx.x == 0) wc.numEvents = 0;
         return;
     }
+    const WorldInfo& wi = s.worlds[w];
+    const uint32_t R = blockScanBlocks(s.blockRad, wi.firstCellBlock, wi.numCellBlocks);
+    const uint32_t D = blockScanBlocks(s.blockDel, wi.firstCellBlock, wi.numCellBlocks);
+    const uint32_t S = blockScanBlocks(s.blockSplit, wi.firstPartBlock, wi.numPartBlocks);
+    if (threadIdx.x != 0) return;
     const unsigned long long id0 = wc.nextId;
     const uint32_t slot0 = wc.numParticles;
     wc.radIdBase = id0;

@@ -44,9 +44,10 @@ def log(msg: str) -> None:
 # P5 Verlet x 32; P6 bond forces 20+12b; P7 Verlet v 32
 def algorithmic_bytes(kernel: str, bonds_per_cell: float) -> float:
     b = bonds_per_cell
+    if kernel.startswith("kPairs"):
+        return 40.0
     return {
         "kBin": 24.0,
-        "kPairs": 40.0,
         "kApplyBond1": 24.0 + 20.0 + 12.0 * b,
         "kVerletPos": 32.0,
         "kBond2": 20.0 + 12.0 * b,
@@ -130,6 +131,10 @@ def build_workload(config: str, rank: int = 0):
         data, world = worldgen.hex_world(seed=seed)
         prm = P.benchmark_parameters(P.MOTION_COLLISION)
         desc = "soft-body heavy: 4096x4096 torus, 4M cells in 40k hexagonal 100-cell clusters, collisions + bond breaking"
+    elif config == "hex1m":
+        data, world = worldgen.hex_world(seed=seed, world=(2048, 2048), clusters=10000)
+        prm = P.benchmark_parameters(P.MOTION_COLLISION)
+        desc = "soft-body, profiling size: 2048x2048 torus, 1M cells in 10k hexagonal 100-cell clusters"
     elif config == "fluid1m":
         data, world = worldgen.fluid_world(seed=seed)
         prm = P.benchmark_parameters(P.MOTION_FLUID)
@@ -246,7 +251,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="hex4m", choices=["hex4m", "fluid1m", "softbody", "batched256"])
+    ap.add_argument("--config", default="hex4m", choices=["hex4m", "hex1m", "fluid1m", "softbody", "batched256"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()

@@ -290,8 +290,9 @@ void* alien_b200_stream(alien_b200_simulation* sim);
 uint64_t alien_b200_kernel_launch_count(alien_b200_simulation* sim);
 /* Steps `timesteps` times launch by launch (no graph) with a CUDA event
  * after every kernel; kernelMs[k] receives the summed milliseconds of the
- * k-th kernel of the step (names: alien_b200_step_kernel_name(k)).  A
- * profiling hook without a reference counterpart. */
+ * k-th kernel of the step, alien_b200_step_kernel_name(k) its name (valid on
+ * the calling thread until the next timed call).  A profiling hook without
+ * a reference counterpart. */
 int alien_b200_timed_timesteps(alien_b200_simulation* sim, uint64_t timesteps, double* kernelMs, int maxKernels,
                                int* numKernels);
 const char* alien_b200_step_kernel_name(int index);

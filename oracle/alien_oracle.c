@@ -525,10 +525,11 @@ static void buildCellMap(OracleWorld* w)
         for (int32_t c = (int32_t)i; c >= 0; c = w->slotNext[c]) w->slotRank[c] = r++;
     }
 }
+/* every cell of the step was inserted (all are alive at the step start);
+ * cells deleted during the step must be cleared as well */
 static void clearCellMap(OracleWorld* w)
 {
-    for (int64_t i = 0; i < w->nCells; ++i)
-        if (w->alive[i]) w->slotHead[w->slotOf[i]] = -1;
+    for (int64_t i = 0; i < w->nCells; ++i) w->slotHead[w->slotOf[i]] = -1;
 }
 
 /* ---- CellProcessor::radiation, CellProcessor.cuh:725-773 */

@@ -24,12 +24,22 @@ from alien_b200 import worldgen  # noqa: E402
 from oracle import refrun  # noqa: E402
 
 ONE_STEP = [
-    # name, seed, motion, timestep
-    ("calm_fluid_t0", 21, P.MOTION_FLUID, 0),
-    ("calm_fluid_t1", 22, P.MOTION_FLUID, 1),
-    ("calm_collision_t0", 23, P.MOTION_COLLISION, 0),
-    ("calm_collision_t2", 24, P.MOTION_COLLISION, 2),
+    # name, seed, motion, timestep, innerFriction (None = default)
+    ("calm_fluid_t0", 21, P.MOTION_FLUID, 0, None),
+    ("calm_fluid_t1", 22, P.MOTION_FLUID, 1, None),
+    ("calm_collision_t0", 23, P.MOTION_COLLISION, 0, None),
+    ("calm_collision_t2", 24, P.MOTION_COLLISION, 2, None),
+    # angle forces on, lock-guarded inner friction off
+    ("calm_fluid_t3_nofric", 25, P.MOTION_FLUID, 3, 0.0),
+    ("calm_collision_t3_nofric", 26, P.MOTION_COLLISION, 3, 0.0),
 ]
+
+
+def one_step_params(motion, inner_friction):
+    prm = P.benchmark_parameters(motion)
+    if inner_friction is not None:
+        prm.innerFriction = inner_friction
+    return prm
 
 
 def calm(seed):
@@ -73,12 +83,13 @@ def decay_input():
 
 def main(out_dir):
     os.makedirs(out_dir, exist_ok=True)
-    for name, seed, motion, t in ONE_STEP:
+    for name, seed, motion, t, fric in ONE_STEP:
         data, world = calm(seed)
-        prm = P.benchmark_parameters(motion)
+        prm = one_step_params(motion, fric)
         out, _, ts = refrun.run(data, world, prm, steps=1, timestep=t)
         np.savez_compressed(os.path.join(out_dir, f"ref_{name}.npz"), in_cells=data.cells, in_particles=data.particles,
                             out_cells=out.cells, out_particles=out.particles,
+                            params=np.frombuffer(bytes(prm), np.uint8),
                             meta=np.array([seed, motion, t, world[0], world[1], ts], np.int64))
         print(name, out.num_cells, out.num_particles, ts)
     summary = {}

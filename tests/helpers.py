@@ -57,8 +57,9 @@ def rel_err(a, b, scale=1.0):
 def compare_cells(got, ref, world, rtol=RTOL, check_bonds=True, report=None):
     """Returns a dict of max errors; asserts exact integer agreement."""
     assert len(got) == len(ref), f"cell count {len(got)} != {len(ref)}"
-    g = got[index_by_id(got)]
-    r = ref[index_by_id(ref)]
+    og, orr = index_by_id(got), index_by_id(ref)
+    g = got[og]
+    r = ref[orr]
     assert np.array_equal(g["id"], r["id"]), "cell id sets differ"
     errs = {}
     W, H = world
@@ -71,8 +72,9 @@ def compare_cells(got, ref, world, rtol=RTOL, check_bonds=True, report=None):
     assert np.array_equal(g["age"], r["age"]), "ages differ"
     assert np.array_equal(g["numConnections"], r["numConnections"]), "bond counts differ"
     if check_bonds:
-        pg = partner_ids(g)
-        pr = partner_ids(r)
+        # cellIndex refers to positions in the transfer array as returned
+        pg = partner_ids(got)[og]
+        pr = partner_ids(ref)[orr]
         assert np.array_equal(pg, pr), "bond partners (order included) differ"
         n = r["numConnections"].astype(np.int64)
         mask = np.arange(6)[None, :] < n[:, None]

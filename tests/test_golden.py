@@ -33,6 +33,14 @@ sys.path.insert(0, GOLDEN)
 import make_golden  # noqa: E402
 
 REF_RTOL = 2e-4
+# On steps with T % 3 == 0 the reference applies inner friction pair by pair
+# under SystemDoubleLock::tryLock (CellProcessor.cuh:695-702): which pair
+# averages run depends on lock contention, so its velocities scatter by
+# ~innerFriction/2 * |v_i - v_j| around any deterministic rule (up to ~1e-3
+# for the slowly rotating calm clusters).  Those fixtures are compared with
+# this wider velocity tolerance; the "_nofric" fixtures pin the same steps'
+# angle forces with REF_RTOL.
+REF_RTOL_LOCKED_FRICTION = 4e-3
 FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "ref_calm_*.npz")))
 HAVE_OBSERVABLES = os.path.exists(os.path.join(GOLDEN, "ref_observables.json"))
 needs_observables = pytest.mark.skipif(not HAVE_OBSERVABLES, reason="reference observables not generated yet")
@@ -46,18 +54,24 @@ def test_oracle_matches_reference_one_step(path):
     assert world == (wx, wy)
     assert np.array_equal(data.cells, f["in_cells"]) and np.array_equal(data.particles, f["in_particles"]), \
         "the seeded generator no longer reproduces the fixture input"
-    o = OracleSimulation(world, P.benchmark_parameters(motion), t)
+    if "params" in f:
+        prm = P.PhysicsParams.from_buffer_copy(f["params"].tobytes())
+    else:
+        prm = P.benchmark_parameters(motion)
+    o = OracleSimulation(world, prm, t)
     o.set_simulation_data(data)
     o.calc_timesteps(1)
     assert o.current_timestep() == ts
     got = o.get_simulation_data()
-    compare_cells(got.cells, f["out_cells"], world, rtol=REF_RTOL)
+    locked = t % 3 == 0 and prm.innerFriction != 0.0
+    tol = REF_RTOL_LOCKED_FRICTION if locked else REF_RTOL
+    compare_cells(got.cells, f["out_cells"], world, rtol=tol)
     compare_particles(got.particles, f["out_particles"], world, rtol=REF_RTOL)
 
 
 @pytest.mark.skipif(not FIXTURES, reason="reference fixtures not generated yet")
 def test_fixtures_present():
-    assert len(FIXTURES) >= 4, "reference fixtures missing: run tests/golden/make_golden.py on a GPU box"
+    assert len(FIXTURES) >= 6, "reference fixtures missing: run tests/golden/make_golden.py on a GPU box"
     assert HAVE_OBSERVABLES
 
 
