@@ -61,6 +61,9 @@ struct WorldInfo {
     long long pmapBase;   // first slot of this world's particle map
     int firstCellBlock, numCellBlocks;
     int firstPartBlock, numPartBlocks;
+    // pair-phase regions: regW x regH tiles per CTA, nRX x nRY regions,
+    // first CTA regionBase; regionShared = 0 for worlds too small for them
+    int regW, regH, nRX, nRY, regionBase, regionShared;
 };
 
 struct WorldCounters {
@@ -92,6 +95,8 @@ struct DevState {
     const AlienPhysicsParams* params;
     const int* cellBlockWorld;
     const int* partBlockWorld;
+    const int* regionWorld;  // world of each pair-phase CTA
+    int numRegions;
     unsigned int* errorFlags;
 
     // cells

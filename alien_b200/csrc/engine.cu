@@ -215,6 +215,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     worlds_.clear();
     const int n = static_cast<int>(setups.size());
     long long cellSlots = 0, partSlots = 0, tiles = 0, pmapSlots = 0, coldTotal = 0;
+    int regions = 0;
     int cellBlocks = 0, partBlocks = 0;
     maxWorldCells_ = maxWorldParts_ = 0;
     for (int w = 0; w < n; ++w) {
@@ -246,6 +247,22 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         wi.firstPartBlock = partBlocks;
         wi.numPartBlocks = static_cast<int>(wi.partCap / kBlock);
         wi.pmapBase = pmapSlots;
+        // pair-phase regions: 16 x 8 tiles with a one-tile halo that never
+        // overlaps the region itself and lies within half a world (so that a
+        // seam shift gives the minimal image)
+        if (wi.nTX >= 4 && wi.nTY >= 4 && ws.W >= 4 * wi.T && ws.H >= 4 * wi.T) {
+            wi.regW = std::min(16, wi.nTX - 2);
+            wi.regH = std::min(8, wi.nTY - 2);
+            wi.regionShared = 1;
+        } else {
+            wi.regW = std::min(16, wi.nTX);
+            wi.regH = std::min(8, wi.nTY);
+            wi.regionShared = 0;
+        }
+        wi.nRX = divUp(wi.nTX, wi.regW);
+        wi.nRY = divUp(wi.nTY, wi.regH);
+        wi.regionBase = regions;
+        regions += wi.nRX * wi.nRY;
         pmapSlots += static_cast<long long>(ws.W) * ws.H;
         cellSlots += wi.cellCap;
         partSlots += wi.partCap;
@@ -282,6 +299,9 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     s.counters = mem_.alloc<WorldCounters>(n);
     auto* paramsDev = mem_.alloc<AlienPhysicsParams>(n);
     s.params = paramsDev;
+    auto* rgw = mem_.alloc<int>(regions);
+    s.regionWorld = rgw;
+    s.numRegions = regions;
     auto* cbw = mem_.alloc<int>(cellBlocks);
     auto* pbw = mem_.alloc<int>(partBlocks);
     s.cellBlockWorld = cbw;
@@ -365,13 +385,14 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     // host-side tables
     std::vector<WorldInfo> infos(n);
     std::vector<AlienPhysicsParams> params(n);
-    std::vector<int> cbwHost(cellBlocks), pbwHost(partBlocks);
+    std::vector<int> cbwHost(cellBlocks), pbwHost(partBlocks), rgwHost(regions);
     std::vector<WorldCounters> counters(n);
     for (int w = 0; w < n; ++w) {
         infos[w] = worlds_[w].info;
         params[w] = worlds_[w].params;
         for (int b = 0; b < infos[w].numCellBlocks; ++b) cbwHost[infos[w].firstCellBlock + b] = w;
         for (int b = 0; b < infos[w].numPartBlocks; ++b) pbwHost[infos[w].firstPartBlock + b] = w;
+        for (int r = 0; r < infos[w].nRX * infos[w].nRY; ++r) rgwHost[infos[w].regionBase + r] = w;
         WorldCounters& wc = counters[w];
         std::memset(&wc, 0, sizeof(wc));
         wc.timestep = setups[w].timestep;
@@ -386,6 +407,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     AB_CK(cudaMemcpyAsync(s.counters, counters.data(), sizeof(WorldCounters) * n, cudaMemcpyHostToDevice, stream_));
     if (cellBlocks) AB_CK(cudaMemcpyAsync(cbw, cbwHost.data(), sizeof(int) * cellBlocks, cudaMemcpyHostToDevice, stream_));
     if (partBlocks) AB_CK(cudaMemcpyAsync(pbw, pbwHost.data(), sizeof(int) * partBlocks, cudaMemcpyHostToDevice, stream_));
+    if (regions) AB_CK(cudaMemcpyAsync(rgw, rgwHost.data(), sizeof(int) * regions, cudaMemcpyHostToDevice, stream_));
     AB_CK(cudaMemsetAsync(s.errorFlags, 0, sizeof(uint32_t), stream_));
     AB_CK(cudaMemsetAsync(s.alive, 0, C, stream_));
     AB_CK(cudaMemsetAsync(s.palive, 0, P, stream_));
@@ -444,8 +466,8 @@ void Arena::enqueueStep()
     scan(s.tileCount, s.numTiles, s.tileStart);
     launch(kScatter, cells, kBlock, s);
     launch(kStage, cells, kBlock, s);
-    if (hasFluid_) launch(kPairsFluid, cells, kBlock, s);
-    if (hasCollision_) launch(kPairsCollision, cells, kBlock, s);
+    if (hasFluid_) launch(kPairsRegion<ALIEN_B200_MOTION_FLUID>, s.numRegions, kRegionThreads, s);
+    if (hasCollision_) launch(kPairsRegion<ALIEN_B200_MOTION_COLLISION>, s.numRegions, kRegionThreads, s);
     launch(kApplyBond1, both, kBlock, s);
     launch(kVerletPos, both, kBlock, s);
     launch(kBond2, both, kBlock, s);

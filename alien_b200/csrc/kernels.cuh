@@ -281,131 +281,152 @@ __global__ void __launch_bounds__(kBlock) kStage(DevState s)
     s.stagedMeta[k] = make_int4(static_cast<int>(g), fl, __float_as_int(s.density[g]), __float_as_int(s.energy[g]));
 }
 
-// -------------------------------------------------------- kPairsFluid ----
+// ---------------------------------------------------------- pair laws ----
+// The pair phase of the two motion types as accumulators: begin() with the
+// cell's staged record, visit() once per candidate neighbour, end() writes
+// the cell's results.  Two enumerations feed them: kPairsRegion (shared-
+// memory tiles, the fast path) and pairsGlobal (tile lists in global memory,
+// used where a region does not fit).
+
 // CellProcessor::calcFluidForces_reconnectCells_correctOverlap,
-// CellProcessor.cuh:122-283: one thread per cell in tile order; neighbours
-// come from the staged copies of the (2r+1)^2-slot window's tiles.
-__device__ __forceinline__ void pairsFluid(const DevState& s, long long k)
-{
-    const int4 me = s.stagedMeta[k];
-    const float4 mpv = s.stagedPV[k];
-    const int g = me.x;
-    const int w = (me.y >> 16) & 0xffff;
-    const WorldInfo& wi = s.worlds[w];
-    const AlienPhysicsParams& p = s.params[wi.paramIndex];
-    const int W = wi.W, H = wi.H;
-    const float h = p.smoothingLength, R = h * 2.0f, minDist = p.cellMinDistance;
-    const float R2reject = R * R * 1.0001f + 1e-6f;
-    const float2 pi = f2(mpv.x, mpv.y), vi = f2(mpv.z, mpv.w);
-    const bool barrierI = me.y & kStageBarrier;
-    const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
-    const float densI = __int_as_float(me.z), energyI = __int_as_float(me.w);
+// CellProcessor.cuh:122-283.  visit() takes pd = p_i - p_j already corrected
+// for the torus.
+struct FluidLaw {
+    const DevState* s;
+    const AlienPhysicsParams* p;
+    int g, W, H;
+    float h, R, R2reject, minDist;
+    float2 pi, vi;
+    bool barrierI, fusionI;
+    float densI;
     int bondsI[kMaxBonds];
+    long long qDens, qFpx, qFpy, qFvx, qFvy, qDx, qDy;
+    int bestBarrier;
+    float bestBarrierDist;
+    int best;
+    unsigned long long bestId;
+
+    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float4 mpv)
+    {
+        s = &st;
+        p = &st.params[wi.paramIndex];
+        g = me.x;
+        W = wi.W;
+        H = wi.H;
+        h = p->smoothingLength;
+        R = h * 2.0f;
+        R2reject = R * R * 1.0001f + 1e-6f;
+        minDist = p->cellMinDistance;
+        pi = f2(mpv.x, mpv.y);
+        vi = f2(mpv.z, mpv.w);
+        barrierI = me.y & kStageBarrier;
+        const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
+        densI = __int_as_float(me.z);
+        fusionI = !barrierI && nI < maxI && __int_as_float(me.w) <= p->cellMaxBindingEnergy;
 #pragma unroll
-    for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? s.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
+        for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? st.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
+        qDens = qFpx = qFpy = qFvx = qFvy = qDx = qDy = 0;
+        bestBarrier = -1;
+        bestBarrierDist = 0.0f;
+        best = -1;
+        bestId = ~0ull;
+    }
 
-    long long qDens = 0, qFpx = 0, qFpy = 0, qFvx = 0, qFvy = 0, qDx = 0, qDy = 0;
-    int bestBarrier = -1;
-    float bestBarrierDist = 0.0f;
-    int best = -1;
-    unsigned long long bestId = ~0ull;
-    const bool fusionI = !barrierI && nI < maxI && energyI <= p.cellMaxBindingEnergy;
-
-    const int sx = slotX(pi.x, W), sy = slotX(pi.y, H);
-    forEachWindowTile(wi, sx, sy, [&](long long t) {
-            const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
-            for (uint32_t m = k0; m < k1; ++m) {
-                const int4 om = s.stagedMeta[m];
-                if (!(om.y & kStageVisible)) continue;
-                const float4 opv = s.stagedPV[m];
-                const float2 pd = correctDirection(pi - f2(opv.x, opv.y), W, H);
-                float d;
-                if (!withinRadius(pd.x * pd.x + pd.y * pd.y, R, R2reject, d)) continue;
-                const int j = om.x;
-                if (om.y & kStageBarrier) {
-                    if (bestBarrier < 0 || d < bestBarrierDist || (d == bestBarrierDist && j < bestBarrier)) {
-                        bestBarrier = j;
-                        bestBarrierDist = d;
-                    }
-                    continue;
-                }
-                qDens += toFix(sphKernel(d / h) / (h * h));
-                if (j == g) continue;
-                if (!barrierI && d < minDist) {
-                    qDx += toFix(pd.x * minDist / 5.0f);
-                    qDy += toFix(pd.y * minDist / 5.0f);
-                }
-                if (isBondedTo(bondsI, j)) continue;
-                const float2 vd = vi - f2(opv.z, opv.w);
-                const float densJ = __int_as_float(om.z);
-                const float factor = densI / (densI * densI) + densJ / (densJ * densJ);
-                if (fabsf(d) > kNearZero) {
-                    const float kd = sphKernelD(d / h) / (h * h * h);
-                    const float2 fp = pd / (-d) * factor * kd;
-                    const float2 fv = vd / densJ * d * kd / (d * d + 0.25f);
-                    qFpx += toFix(fp.x);
-                    qFpy += toFix(fp.y);
-                    qFvx += toFix(fv.x);
-                    qFvy += toFix(fv.y);
-                }
-                if (fusionI && len2(vd) >= p.cellFusionVelocity) {
-                    const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
-                    if (nJ < maxJ && __int_as_float(om.w) <= p.cellMaxBindingEnergy) {
-                        const unsigned long long idJ = s.id[j];
-                        if (idJ < bestId) {
-                            bestId = idJ;
-                            best = j;
-                        }
-                    }
-                }
+    __device__ __forceinline__ void visit(int4 om, float4 opv, float2 pd)
+    {
+        if (!(om.y & kStageVisible)) return;
+        float d;
+        if (!withinRadius(pd.x * pd.x + pd.y * pd.y, R, R2reject, d)) return;
+        const int j = om.x;
+        if (om.y & kStageBarrier) {
+            if (bestBarrier < 0 || d < bestBarrierDist || (d == bestBarrierDist && j < bestBarrier)) {
+                bestBarrier = j;
+                bestBarrierDist = d;
             }
-    });
-    float2 F = f2(0.0f, 0.0f);
-    if (bestBarrier >= 0) {
-        const long long b = bestBarrier;
-        const float2 pb = s.posA[b];
-        float2 rr = f2(0.0f, 0.0f);
-        const int nb = s.numConn[b];
-        if (nb <= 1) {
-            rr = correctDirection(pi - pb, W, H);
-        } else {
-            const float angleToCell = angleOfVector(correctDirection(pi - pb, W, H));
-            for (int m = 0; m < nb; ++m) {
-                const int c1 = s.bond[b * kMaxBonds + m], c2 = s.bond[b * kMaxBonds + (m + 1) % nb];
-                const float a1 = angleOfVector(correctDirection(s.posA[c1] - pb, W, H));
-                const float a2 = angleOfVector(correctDirection(s.posA[c2] - pb, W, H));
-                if (isAngleInBetween(a1, a2, angleToCell)) {
-                    rr = rotCCW(s.posA[c2] - s.posA[c1]);
-                    break;
-                }
-            }
+            return;
         }
-        const float2 vb = s.velA[b];
-        const float2 vr = vi - vb;
-        const float dvr = dot2(vr, rr);
-        if (dvr < 0.0f) {
-            const float trr = fmaxf(0.05f, lensq2(rr));
-            const float td = fmaxf(0.05f, bestBarrierDist);
-            // (vr - rr*2*dvr/trr + vb - vi) / td of CellProcessor.cuh:272 with
-            // vr + vb - vi = 0 cancelled algebraically (the FP32 form loses
-            // ~ulp(|v|)/td to that cancellation)
-            F = rr * (-2.0f * dvr / trr) / td;
+        qDens += toFix(sphKernel(d / h) / (h * h));
+        if (j == g) return;
+        if (!barrierI && d < minDist) {
+            qDx += toFix(pd.x * minDist / 5.0f);
+            qDy += toFix(pd.y * minDist / 5.0f);
+        }
+        if (isBondedTo(bondsI, j)) return;
+        const float2 vd = vi - f2(opv.z, opv.w);
+        const float densJ = __int_as_float(om.z);
+        const float factor = densI / (densI * densI) + densJ / (densJ * densJ);
+        if (fabsf(d) > kNearZero) {
+            const float kd = sphKernelD(d / h) / (h * h * h);
+            const float2 fp = pd / (-d) * factor * kd;
+            const float2 fv = vd / densJ * d * kd / (d * d + 0.25f);
+            qFpx += toFix(fp.x);
+            qFpy += toFix(fp.y);
+            qFvx += toFix(fv.x);
+            qFvy += toFix(fv.y);
+        }
+        if (fusionI && len2(vd) >= p->cellFusionVelocity) {
+            const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
+            if (nJ < maxJ && __int_as_float(om.w) <= p->cellMaxBindingEnergy) {
+                const unsigned long long idJ = s->id[j];
+                if (idJ < bestId) {
+                    bestId = idJ;
+                    best = j;
+                }
+            }
         }
     }
-    const float2 Fp = f2(fromFix(qFpx), fromFix(qFpy)), Fv = f2(fromFix(qFvx), fromFix(qFvy));
-    F = F + (Fp * p.pressureStrength + Fv * p.viscosityStrength);
-    s.force[g] = F;
-    s.posB[g] = pi + f2(fromFix(qDx), fromFix(qDy));
-    s.densNew[g] = fromFix(qDens);
-    s.best[g] = best;
-}
 
-// ---------------------------------------------------- kPairsCollision ----
+    __device__ __forceinline__ void end()
+    {
+        const DevState& st = *s;
+        float2 F = f2(0.0f, 0.0f);
+        if (bestBarrier >= 0) {
+            const long long b = bestBarrier;
+            const float2 pb = st.posA[b];
+            float2 rr = f2(0.0f, 0.0f);
+            const int nb = st.numConn[b];
+            if (nb <= 1) {
+                rr = correctDirection(pi - pb, W, H);
+            } else {
+                const float angleToCell = angleOfVector(correctDirection(pi - pb, W, H));
+                for (int m = 0; m < nb; ++m) {
+                    const int c1 = st.bond[b * kMaxBonds + m], c2 = st.bond[b * kMaxBonds + (m + 1) % nb];
+                    const float a1 = angleOfVector(correctDirection(st.posA[c1] - pb, W, H));
+                    const float a2 = angleOfVector(correctDirection(st.posA[c2] - pb, W, H));
+                    if (isAngleInBetween(a1, a2, angleToCell)) {
+                        rr = rotCCW(st.posA[c2] - st.posA[c1]);
+                        break;
+                    }
+                }
+            }
+            const float2 vb = st.velA[b];
+            const float2 vr = vi - vb;
+            const float dvr = dot2(vr, rr);
+            if (dvr < 0.0f) {
+                const float trr = fmaxf(0.05f, lensq2(rr));
+                const float td = fmaxf(0.05f, bestBarrierDist);
+                // (vr - rr*2*dvr/trr + vb - vi) / td of CellProcessor.cuh:272 with
+                // vr + vb - vi = 0 cancelled algebraically (the FP32 form loses
+                // ~ulp(|v|)/td to that cancellation)
+                F = rr * (-2.0f * dvr / trr) / td;
+            }
+        }
+        const float2 Fp = f2(fromFix(qFpx), fromFix(qFpy)), Fv = f2(fromFix(qFvx), fromFix(qFvy));
+        F = F + (Fp * p->pressureStrength + Fv * p->viscosityStrength);
+        st.force[g] = F;
+        st.posB[g] = pi + f2(fromFix(qDx), fromFix(qDy));
+        st.densNew[g] = fromFix(qDens);
+        st.best[g] = best;
+    }
+};
+
 // CellProcessor::calcCollisions_reconnectCells_correctOverlap,
 // CellProcessor.cuh:285-365 with CellMap::executeForEach (Map.cuh:175-196,
 // distance test on the uncorrected difference).  The reference adds each
 // pair force to both cells from the scanning cell; here every cell gathers
-// f(i,j) from its own scan and -f(j,i) from the scans that see it.
+// f(i,j) from its own scan and -f(j,i) from the scans that see it.  visit()
+// takes p_j as stored (candidates across the torus seam never pass the
+// uncorrected distance test, so they are not visited).
 __device__ __forceinline__ float2 collisionForce(float2 pd, float d, float2 vCell, float2 vOther, bool barrierCell,
                                                  const AlienPhysicsParams& p)
 {
@@ -419,100 +440,280 @@ __device__ __forceinline__ float2 collisionForce(float2 pd, float d, float2 vCel
     return normalized2(pd) * (p.cellMaxCollisionDistance - len2(pd)) * p.cellRepulsionStrength * bf;
 }
 
-__device__ __forceinline__ void pairsCollision(const DevState& s, long long k)
-{
-    const int4 me = s.stagedMeta[k];
-    const float4 mpv = s.stagedPV[k];
-    const int g = me.x;
-    const int w = (me.y >> 16) & 0xffff;
-    const WorldInfo& wi = s.worlds[w];
-    const AlienPhysicsParams& p = s.params[wi.paramIndex];
-    const int W = wi.W, H = wi.H;
-    const float R = p.cellMaxCollisionDistance, minDist = p.cellMinDistance;
-    const float R2reject = R * R * 1.0001f + 1e-6f;
-    const float2 pi = f2(mpv.x, mpv.y), vi = f2(mpv.z, mpv.w);
-    const bool barrierI = me.y & kStageBarrier;
-    const bool visibleI = me.y & kStageVisible;
-    const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
-    const float energyI = __int_as_float(me.w);
+struct CollisionLaw {
+    const DevState* s;
+    const AlienPhysicsParams* p;
+    int g, W, H;
+    float R, R2reject, minDist;
+    float2 pi, vi;
+    bool barrierI, visibleI, fusionI;
+    float densI;
     int bondsI[kMaxBonds];
-#pragma unroll
-    for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? s.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
-    const bool fusionI = !barrierI && nI < maxI && energyI <= p.cellMaxBindingEnergy;
+    long long qFx, qFy, qDx, qDy;
+    int best;
+    unsigned long long bestId;
 
-    long long qFx = 0, qFy = 0, qDx = 0, qDy = 0;
-    int best = -1;
-    unsigned long long bestId = ~0ull;
-    const int sx = slotX(pi.x, W), sy = slotX(pi.y, H);
-    forEachWindowTile(wi, sx, sy, [&](long long t) {
-            const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
-            for (uint32_t m = k0; m < k1; ++m) {
-                const int4 om = s.stagedMeta[m];
-                const int j = om.x;
-                if (j == g) continue;
-                const float4 opv = s.stagedPV[m];
-                const float2 pj = f2(opv.x, opv.y);
-                const float2 raw = pj - pi;
-                float draw_;
-                if (!withinRadius(raw.x * raw.x + raw.y * raw.y, R, R2reject, draw_)) continue;
-                const bool visibleJ = om.y & kStageVisible;
-                if (!visibleJ && !visibleI) continue;
-                const float2 pd = correctDirection(pi - pj, W, H);
-                const float d = len2(pd);
-                const bool bonded = isBondedTo(bondsI, j);
-                const float2 vj = f2(opv.z, opv.w);
-                if (visibleJ) {  // i's own scan sees j
-                    if (!barrierI && d < minDist) {
-                        qDx += toFix(pd.x * minDist / 5.0f);
-                        qDy += toFix(pd.y * minDist / 5.0f);
-                    }
-                    if (!bonded) {
-                        const float2 f = collisionForce(pd, d, vi, vj, barrierI, p);
-                        qFx += toFix(f.x);
-                        qFy += toFix(f.y);
-                        const float2 vd = vi - vj;
-                        if (fusionI && len2(vd) >= p.cellFusionVelocity && dot2(pd, vd) < 0.0f) {
-                            const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
-                            if (nJ < maxJ && !(om.y & kStageBarrier) && __int_as_float(om.w) <= p.cellMaxBindingEnergy) {
-                                const unsigned long long idJ = s.id[j];
-                                if (idJ < bestId) {
-                                    bestId = idJ;
-                                    best = j;
-                                }
-                            }
+    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float4 mpv)
+    {
+        s = &st;
+        p = &st.params[wi.paramIndex];
+        g = me.x;
+        W = wi.W;
+        H = wi.H;
+        R = p->cellMaxCollisionDistance;
+        R2reject = R * R * 1.0001f + 1e-6f;
+        minDist = p->cellMinDistance;
+        pi = f2(mpv.x, mpv.y);
+        vi = f2(mpv.z, mpv.w);
+        barrierI = me.y & kStageBarrier;
+        visibleI = me.y & kStageVisible;
+        const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
+        densI = __int_as_float(me.z);
+        fusionI = !barrierI && nI < maxI && __int_as_float(me.w) <= p->cellMaxBindingEnergy;
+#pragma unroll
+        for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? st.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
+        qFx = qFy = qDx = qDy = 0;
+        best = -1;
+        bestId = ~0ull;
+    }
+
+    __device__ __forceinline__ void visit(int4 om, float4 opv)
+    {
+        const int j = om.x;
+        if (j == g) return;
+        const float2 pj = f2(opv.x, opv.y);
+        const float2 raw = pj - pi;
+        float dRaw;
+        if (!withinRadius(raw.x * raw.x + raw.y * raw.y, R, R2reject, dRaw)) return;
+        const bool visibleJ = om.y & kStageVisible;
+        if (!visibleJ && !visibleI) return;
+        const float2 pd = correctDirection(pi - pj, W, H);
+        const float d = len2(pd);
+        const bool bonded = isBondedTo(bondsI, j);
+        const float2 vj = f2(opv.z, opv.w);
+        if (visibleJ) {  // i's own scan sees j
+            if (!barrierI && d < minDist) {
+                qDx += toFix(pd.x * minDist / 5.0f);
+                qDy += toFix(pd.y * minDist / 5.0f);
+            }
+            if (!bonded) {
+                const float2 f = collisionForce(pd, d, vi, vj, barrierI, *p);
+                qFx += toFix(f.x);
+                qFy += toFix(f.y);
+                const float2 vd = vi - vj;
+                if (fusionI && len2(vd) >= p->cellFusionVelocity && dot2(pd, vd) < 0.0f) {
+                    const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
+                    if (nJ < maxJ && !(om.y & kStageBarrier) && __int_as_float(om.w) <= p->cellMaxBindingEnergy) {
+                        const unsigned long long idJ = s->id[j];
+                        if (idJ < bestId) {
+                            bestId = idJ;
+                            best = j;
                         }
                     }
                 }
-                if (visibleI && !bonded) {  // j's scan sees i and applies -f(j,i) to i
-                    const float2 pdj = correctDirection(pj - pi, W, H);
-                    const float2 f = collisionForce(pdj, len2(pdj), vj, vi, om.y & kStageBarrier, p);
-                    qFx -= toFix(f.x);
-                    qFy -= toFix(f.y);
-                }
             }
-    });
-    s.force[g] = f2(fromFix(qFx), fromFix(qFy));
-    s.posB[g] = pi + f2(fromFix(qDx), fromFix(qDy));
-    s.densNew[g] = __int_as_float(me.z);
-    s.best[g] = best;
+        }
+        if (visibleI && !bonded) {  // j's scan sees i and applies -f(j,i) to i
+            const float2 pdj = correctDirection(pj - pi, W, H);
+            const float2 f = collisionForce(pdj, len2(pdj), vj, vi, om.y & kStageBarrier, *p);
+            qFx -= toFix(f.x);
+            qFy -= toFix(f.y);
+        }
+    }
+
+    __device__ __forceinline__ void end()
+    {
+        const DevState& st = *s;
+        st.force[g] = f2(fromFix(qFx), fromFix(qFy));
+        st.posB[g] = pi + f2(fromFix(qDx), fromFix(qDy));
+        st.densNew[g] = densI;
+        st.best[g] = best;
+    }
+};
+
+// the pair phase of the staged cell k, neighbours from the global tile lists
+template <int Motion>
+__device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
+{
+    const int4 me = s.stagedMeta[k];
+    const float4 mpv = s.stagedPV[k];
+    const int w = (me.y >> 16) & 0xffff;
+    const WorldInfo& wi = s.worlds[w];
+    const float2 pi = f2(mpv.x, mpv.y);
+    const int sx = slotX(pi.x, wi.W), sy = slotX(pi.y, wi.H);
+    if (Motion == ALIEN_B200_MOTION_FLUID) {
+        FluidLaw law;
+        law.begin(s, wi, me, mpv);
+        forEachWindowTile(wi, sx, sy, [&](long long t) {
+            const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
+            for (uint32_t m = k0; m < k1; ++m) {
+                const float4 opv = s.stagedPV[m];
+                law.visit(s.stagedMeta[m], opv, correctDirection(pi - f2(opv.x, opv.y), wi.W, wi.H));
+            }
+        });
+        law.end();
+    } else {
+        CollisionLaw law;
+        law.begin(s, wi, me, mpv);
+        forEachWindowTile(wi, sx, sy, [&](long long t) {
+            const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
+            for (uint32_t m = k0; m < k1; ++m) law.visit(s.stagedMeta[m], s.stagedPV[m]);
+        });
+        law.end();
+    }
 }
 
-// one thread per staged cell; a launch serves the worlds of one motion type
-// (the host launches the kernel of every motion type present in the arena)
-__global__ void __launch_bounds__(kBlock, 3) kPairsFluid(DevState s)
-{
-    const long long k = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
-    if (k >= s.tileStart[s.numTiles]) return;
-    const int w = (s.stagedMeta[k].y >> 16) & 0xffff;
-    if (s.worlds[w].motionType == ALIEN_B200_MOTION_FLUID) pairsFluid(s, k);
-}
+// ------------------------------------------------------- kPairsRegion ----
+// One CTA per region of regW x regH tiles of one world.  It copies the staged
+// records of the region and of its one-tile halo from the tile-sorted arrays
+// into shared memory (each tile a contiguous run), shifting halo tiles that
+// lie across the torus seam by +-W / +-H so that plain differences are the
+// minimal-image displacements, and then runs the pair law of every cell of
+// the region against the 3x3 local tiles around its tile.  Regions whose
+// records exceed the shared buffer, and worlds too small for regions, use
+// pairsGlobal for their cells.
+constexpr int kRegionThreads = 256;
+constexpr int kRegionCap = 1280;          // staged records per CTA (halo included)
+constexpr int kRegionMaxTiles = 18 * 10;  // (regW + 2) x (regH + 2) for 16 x 8 regions
 
-__global__ void __launch_bounds__(kBlock, 3) kPairsCollision(DevState s)
+template <int Motion>
+__global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
 {
-    const long long k = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
-    if (k >= s.tileStart[s.numTiles]) return;
-    const int w = (s.stagedMeta[k].y >> 16) & 0xffff;
-    if (s.worlds[w].motionType != ALIEN_B200_MOTION_FLUID) pairsCollision(s, k);
+    __shared__ float4 sPV[kRegionCap];
+    __shared__ int4 sMeta[kRegionCap];
+    __shared__ uint8_t sTile[kRegionCap];
+    __shared__ int tStart[kRegionMaxTiles + 1];   // shared-memory offset of each local tile
+    __shared__ int tCount[kRegionMaxTiles];
+    __shared__ int tGlobal[kRegionMaxTiles];      // first sorted index of the tile
+    __shared__ float2 tShift[kRegionMaxTiles];
+    __shared__ int sOwnTotal, sTotal;
+
+    const int w = s.regionWorld[blockIdx.x];
+    const WorldInfo& wi = s.worlds[w];
+    if ((wi.motionType == ALIEN_B200_MOTION_FLUID) != (Motion == ALIEN_B200_MOTION_FLUID)) return;
+    if (!s.counters[w].active) return;
+    const int idx = blockIdx.x - wi.regionBase;
+    const int rx = idx % wi.nRX, ry = idx / wi.nRX;
+    const int tx0 = rx * wi.regW, ty0 = ry * wi.regH;
+    const int ownW = min(wi.regW, wi.nTX - tx0), ownH = min(wi.regH, wi.nTY - ty0);
+
+    if (!wi.regionShared) {
+        // world too small for halo regions: its own tiles from global memory
+        for (int ly = 0; ly < ownH; ++ly)
+            for (int lx = 0; lx < ownW; ++lx) {
+                const long long t = wi.tileBase + (tx0 + lx) + static_cast<long long>(ty0 + ly) * wi.nTX;
+                for (uint32_t k = s.tileStart[t] + threadIdx.x; k < s.tileStart[t + 1]; k += kRegionThreads)
+                    pairsGlobal<Motion>(s, k);
+            }
+        return;
+    }
+
+    const int LW = ownW + 2, LH = ownH + 2, NT = LW * LH;
+    // 1. local tile table (NT <= kRegionMaxTiles <= kRegionThreads)
+    int cnt = 0;
+    bool own = false;
+    const int lt = threadIdx.x;
+    if (lt < NT) {
+        const int lx = lt % LW, ly = lt / LW;
+        int gx = tx0 - 1 + lx, gy = ty0 - 1 + ly;
+        float2 sh = f2(0.0f, 0.0f);
+        if (gx < 0) {
+            gx += wi.nTX;
+            sh.x = -static_cast<float>(wi.W);
+        } else if (gx >= wi.nTX) {
+            gx -= wi.nTX;
+            sh.x = static_cast<float>(wi.W);
+        }
+        if (gy < 0) {
+            gy += wi.nTY;
+            sh.y = -static_cast<float>(wi.H);
+        } else if (gy >= wi.nTY) {
+            gy -= wi.nTY;
+            sh.y = static_cast<float>(wi.H);
+        }
+        const long long t = wi.tileBase + gx + static_cast<long long>(gy) * wi.nTX;
+        const uint32_t k0 = s.tileStart[t];
+        cnt = static_cast<int>(s.tileStart[t + 1] - k0);
+        tGlobal[lt] = static_cast<int>(k0);
+        tCount[lt] = cnt;
+        tShift[lt] = sh;
+        own = lx >= 1 && lx <= ownW && ly >= 1 && ly <= ownH;
+    }
+    // own tiles first, then the halo
+    uint32_t ownTotal, haloTotal;
+    const uint32_t ownOff = blockExclusiveScan(own ? cnt : 0, &ownTotal);
+    const uint32_t haloOff = blockExclusiveScan(own ? 0 : cnt, &haloTotal);
+    if (lt < NT) tStart[lt] = static_cast<int>(own ? ownOff : ownTotal + haloOff);
+    if (threadIdx.x == 0) {
+        sOwnTotal = static_cast<int>(ownTotal);
+        sTotal = static_cast<int>(ownTotal + haloTotal);
+    }
+    __syncthreads();
+    const int total = sTotal;
+    if (total > kRegionCap) {
+        // denser than the shared buffer: the region's own cells from global memory
+        for (int ly = 1; ly <= ownH; ++ly)
+            for (int lx = 1; lx <= ownW; ++lx) {
+                const int q = ly * LW + lx;
+                for (int k = tGlobal[q] + threadIdx.x; k < tGlobal[q] + tCount[q]; k += kRegionThreads)
+                    pairsGlobal<Motion>(s, k);
+            }
+        return;
+    }
+    // 2. copy: one warp per local tile
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int q = warp; q < NT; q += kRegionThreads / 32) {
+        const int n = tCount[q], src = tGlobal[q], dst = tStart[q];
+        const float2 sh = tShift[q];
+        for (int e = lane; e < n; e += 32) {
+            float4 pv = s.stagedPV[src + e];
+            pv.x += sh.x;
+            pv.y += sh.y;
+            sPV[dst + e] = pv;
+            sMeta[dst + e] = s.stagedMeta[src + e];
+            sTile[dst + e] = static_cast<uint8_t>(q);
+        }
+    }
+    __syncthreads();
+    // 3. pair law of every own cell against its 3x3 local tiles
+    const int ownN = sOwnTotal;
+    for (int e = threadIdx.x; e < ownN; e += kRegionThreads) {
+        const int q = sTile[e];
+        const int lx = q % LW, ly = q / LW;
+        const int4 me = sMeta[e];
+        const float4 mpv = sPV[e];
+        if (Motion == ALIEN_B200_MOTION_FLUID) {
+            FluidLaw law;
+            law.begin(s, wi, me, mpv);
+            const float2 pi = f2(mpv.x, mpv.y);
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll 1
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int q2 = (ly + dy) * LW + (lx + dx);
+                    const int b0 = tStart[q2], b1 = b0 + tCount[q2];
+                    for (int m = b0; m < b1; ++m) {
+                        const float4 opv = sPV[m];
+                        law.visit(sMeta[m], opv, pi - f2(opv.x, opv.y));
+                    }
+                }
+            law.end();
+        } else {
+            CollisionLaw law;
+            law.begin(s, wi, me, mpv);
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll 1
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int q2 = (ly + dy) * LW + (lx + dx);
+                    const float2 sh = tShift[q2];
+                    if (sh.x != 0.0f || sh.y != 0.0f) continue;  // across the seam: uncorrected distance > R
+                    const int b0 = tStart[q2], b1 = b0 + tCount[q2];
+                    for (int m = b0; m < b1; ++m) law.visit(sMeta[m], sPV[m]);
+                }
+            law.end();
+        }
+    }
 }
 
 // ------------------------------------------------------- bond forces -----

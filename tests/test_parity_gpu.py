@@ -109,3 +109,23 @@ def test_multi_step_statistics(motion):
     eng.calc_timesteps(30)
     again = eng.get_simulation_data()
     assert np.array_equal(again.cells, got.cells) and np.array_equal(again.particles, got.particles)
+
+
+@pytest.mark.parametrize("motion", [P.MOTION_FLUID, P.MOTION_COLLISION])
+def test_world_too_small_for_regions(motion):
+    """7x7 torus: the pair phase reads neighbours from global tile lists"""
+    data, world = worldgen.random_test_world(41, world=(7, 7), clusters=0, hex_clusters=0, free_cells=30,
+                                             particles=5)
+    got, ref = run_both(data, world, P.benchmark_parameters(motion), 1, 0)
+    compare_cells(got.cells, ref.cells, world)
+    compare_particles(got.particles, ref.particles, world)
+
+
+@pytest.mark.parametrize("motion", [P.MOTION_FLUID, P.MOTION_COLLISION])
+def test_region_denser_than_shared_buffer(motion):
+    """about 6 cells per slot: a region's halo exceeds the shared buffer"""
+    data, world = worldgen.random_test_world(42, world=(16, 16), clusters=0, hex_clusters=0, free_cells=1500,
+                                             particles=20, vmax=0.2)
+    got, ref = run_both(data, world, P.benchmark_parameters(motion), 1, 1)
+    compare_cells(got.cells, ref.cells, world)
+    compare_particles(got.particles, ref.particles, world)
