@@ -586,6 +586,7 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
     __shared__ int tCount[kRegionMaxTiles];
     __shared__ int tGlobal[kRegionMaxTiles];      // first sorted index of the tile
     __shared__ float2 tShift[kRegionMaxTiles];
+    __shared__ int sOrder[kRegionMaxTiles];
     __shared__ int sOwnTotal, sTotal;
 
     const int w = s.regionWorld[blockIdx.x];
@@ -640,9 +641,11 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
         own = lx >= 1 && lx <= ownW && ly >= 1 && ly <= ownH;
     }
     // own tiles first, then the halo
-    uint32_t ownTotal, haloTotal;
+    uint32_t ownTotal, haloTotal, ownTiles, haloTiles;
     const uint32_t ownOff = blockExclusiveScan(own ? cnt : 0, &ownTotal);
     const uint32_t haloOff = blockExclusiveScan(own ? 0 : cnt, &haloTotal);
+    const uint32_t ownRank = blockExclusiveScan(own ? 1u : 0u, &ownTiles);
+    const uint32_t haloRank = blockExclusiveScan((lt < NT && !own) ? 1u : 0u, &haloTiles);
     if (lt < NT) tStart[lt] = static_cast<int>(own ? ownOff : ownTotal + haloOff);
     if (threadIdx.x == 0) {
         sOwnTotal = static_cast<int>(ownTotal);
@@ -660,19 +663,30 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
             }
         return;
     }
-    // 2. copy: one warp per local tile
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int q = warp; q < NT; q += kRegionThreads / 32) {
-        const int n = tCount[q], src = tGlobal[q], dst = tStart[q];
-        const float2 sh = tShift[q];
-        for (int e = lane; e < n; e += 32) {
-            float4 pv = s.stagedPV[src + e];
-            pv.x += sh.x;
-            pv.y += sh.y;
-            sPV[dst + e] = pv;
-            sMeta[dst + e] = s.stagedMeta[src + e];
-            sTile[dst + e] = static_cast<uint8_t>(q);
+    // 2. copy: every thread one record per round; its local tile is found by
+    //    binary search in the offset table (own tiles first, then the halo,
+    //    each group in tile order, so offsets increase along the search order)
+    //    sOrder lists the local tiles by shared-memory offset.
+    if (lt < NT) sOrder[own ? static_cast<int>(ownRank) : static_cast<int>(ownTiles + haloRank)] = lt;
+    __syncthreads();
+    for (int e = threadIdx.x; e < total; e += kRegionThreads) {
+        int lo = 0, hi = NT - 1;  // last tile in offset order whose start <= e
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tStart[sOrder[mid]] <= e)
+                lo = mid;
+            else
+                hi = mid - 1;
         }
+        const int q = sOrder[lo];
+        const int src = tGlobal[q] + (e - tStart[q]);
+        const float2 sh = tShift[q];
+        float4 pv = s.stagedPV[src];
+        pv.x += sh.x;
+        pv.y += sh.y;
+        sPV[e] = pv;
+        sMeta[e] = s.stagedMeta[src];
+        sTile[e] = static_cast<uint8_t>(q);
     }
     __syncthreads();
     // 3. pair law of every own cell against its 3x3 local tiles
@@ -1343,20 +1357,24 @@ __global__ void __launch_bounds__(kBlock) kEventCount(DevState s)
     }
 }
 
-// exclusive scan of arr[first .. first+count) in place by one block;
-// returns the total
+// exclusive scan of arr[first .. first+count) in place by one block: each
+// thread scans a contiguous chunk, the chunk sums are scanned across the
+// block; returns the total
 __device__ uint32_t blockScanBlocks(uint32_t* arr, int first, int count)
 {
-    uint32_t carry = 0;
-    for (int base = 0; base < count; base += kBlock) {
-        const int k = base + threadIdx.x;
-        const uint32_t v = k < count ? arr[first + k] : 0u;
-        uint32_t total;
-        const uint32_t ex = blockExclusiveScan(v, &total);
-        if (k < count) arr[first + k] = carry + ex;
-        carry += total;
+    const int chunk = (count + kBlock - 1) / kBlock;
+    const int b0 = threadIdx.x * chunk;
+    const int b1 = min(b0 + chunk, count);
+    uint32_t sum = 0;
+    for (int k = b0; k < b1; ++k) sum += arr[first + k];
+    uint32_t total;
+    uint32_t run = blockExclusiveScan(sum, &total);
+    for (int k = b0; k < b1; ++k) {
+        const uint32_t v = arr[first + k];
+        arr[first + k] = run;
+        run += v;
     }
-    return carry;
+    return total;
 }
 
 // one block per world: block offsets, id and slot bases, timestep advance
