@@ -44,6 +44,7 @@ struct Error : std::runtime_error {
     } while (0)
 
 #define launch(kernel, ...) launchNamed(#kernel, kernel, __VA_ARGS__)
+#define launchSmem(kernel, ...) launchNamedSmem(#kernel, kernel, __VA_ARGS__)
 
 static inline long long roundUp(long long v, long long m) { return (v + m - 1) / m * m; }
 static inline int divUp(long long v, long long m) { return static_cast<int>((v + m - 1) / m); }
@@ -159,8 +160,13 @@ private:
     template <class K, class... A>
     void launchNamed(const char* name, K kernel, int grid, int block, A... args)
     {
+        launchNamedSmem(name, kernel, grid, block, 0, args...);
+    }
+    template <class K, class... A>
+    void launchNamedSmem(const char* name, K kernel, int grid, int block, size_t smem, A... args)
+    {
         if (grid <= 0) return;
-        kernel<<<grid, block, 0, stream_>>>(args...);
+        kernel<<<grid, block, smem, stream_>>>(args...);
         ++launches_;
         AB_CK(cudaGetLastError());
         if (timingEvents_) {
@@ -251,12 +257,12 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         // overlaps the region itself and lies within half a world (so that a
         // seam shift gives the minimal image)
         if (wi.nTX >= 4 && wi.nTY >= 4 && ws.W >= 4 * wi.T && ws.H >= 4 * wi.T) {
-            wi.regW = std::min(16, wi.nTX - 2);
-            wi.regH = std::min(8, wi.nTY - 2);
+            wi.regW = std::min(kRegionMaxW, wi.nTX - 2);
+            wi.regH = std::min(kRegionMaxH, wi.nTY - 2);
             wi.regionShared = 1;
         } else {
-            wi.regW = std::min(16, wi.nTX);
-            wi.regH = std::min(8, wi.nTY);
+            wi.regW = std::min(kRegionMaxW, wi.nTX);
+            wi.regH = std::min(kRegionMaxH, wi.nTY);
             wi.regionShared = 0;
         }
         wi.nRX = divUp(wi.nTX, wi.regW);
@@ -284,6 +290,12 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     if (cellSlots >= (1ll << 31) || partSlots >= (1ll << 31) || tiles >= (1ll << 32) - 2)
         throw Error(ALIEN_B200_ERR_CAPACITY, "arena exceeds 2^31 slots");
 
+    // the pair-phase regions stage up to kRegionCap records in dynamic
+    // shared memory (above the 48 KB default)
+    AB_CK(cudaFuncSetAttribute(kPairsRegion<ALIEN_B200_MOTION_FLUID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(kRegionDynSmem)));
+    AB_CK(cudaFuncSetAttribute(kPairsRegion<ALIEN_B200_MOTION_COLLISION>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(kRegionDynSmem)));
     DevState& s = s_;
     s = DevState{};
     s.numWorlds = n;
@@ -466,8 +478,9 @@ void Arena::enqueueStep()
     scan(s.tileCount, s.numTiles, s.tileStart);
     launch(kScatter, cells, kBlock, s);
     launch(kStage, cells, kBlock, s);
-    if (hasFluid_) launch(kPairsRegion<ALIEN_B200_MOTION_FLUID>, s.numRegions, kRegionThreads, s);
-    if (hasCollision_) launch(kPairsRegion<ALIEN_B200_MOTION_COLLISION>, s.numRegions, kRegionThreads, s);
+    if (hasFluid_) launchSmem(kPairsRegion<ALIEN_B200_MOTION_FLUID>, s.numRegions, kRegionThreads, kRegionDynSmem, s);
+    if (hasCollision_)
+        launchSmem(kPairsRegion<ALIEN_B200_MOTION_COLLISION>, s.numRegions, kRegionThreads, kRegionDynSmem, s);
     launch(kApplyBond1, both, kBlock, s);
     launch(kVerletPos, both, kBlock, s);
     launch(kBond2, both, kBlock, s);

@@ -76,13 +76,6 @@ __device__ __forceinline__ bool isBondedTo(const int* bonds, int j)
     return r;
 }
 
-// sqrtf(q) <= R decided exactly, with a cheap reject for the common far case
-__device__ __forceinline__ bool withinRadius(float q, float R, float R2reject, float& d)
-{
-    if (q > R2reject) return false;
-    d = sqrtf(q);
-    return d <= R;
-}
 
 constexpr int kMaxRadius = 15;
 
@@ -252,8 +245,8 @@ __global__ void __launch_bounds__(kBlock) kScatter(DevState s)
 // ------------------------------------------------------------- kStage ----
 // Rank of each cell among the cells of its slot in storage order (the
 // reference chains at most 11 cells per slot and scans 10 of them,
-// Map.cuh:113-125, CellProcessor.cuh:165) and a sorted SoA copy of the
-// fields the pair phase reads.
+// Map.cuh:113-125, CellProcessor.cuh:165) and a tile-sorted SoA copy of the
+// fields the pair phase reads, each tile's records in storage order.
 __global__ void __launch_bounds__(kBlock) kStage(DevState s)
 {
     long long k = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
@@ -265,13 +258,17 @@ __global__ void __launch_bounds__(kBlock) kStage(DevState s)
     const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
     const float2 pos = s.posA[g];
     const int slot = slotX(pos.x, wi.W) + slotX(pos.y, wi.H) * wi.W;
-    int rank = 0;
+    int rank = 0, rankInTile = 0;
     for (uint32_t m = k0; m < k1; ++m) {
         uint32_t g2 = s.sorted[m];
         if (g2 >= g) continue;
+        ++rankInTile;
         float2 p2 = s.posA[g2];
         rank += (slotX(p2.x, wi.W) + slotX(p2.y, wi.H) * wi.W) == slot;
     }
+    // records of a tile in storage order: a fixed visiting order for the
+    // pair phase, whatever order the binning atomics produced
+    k = k0 + rankInTile;
     const float2 vel = s.velA[g];
     int fl = (s.barrier[g] ? kStageBarrier : 0) | (rank < kSlotScanLevels ? kStageVisible : 0) | (rank == 0 ? kStageHead : 0);
     fl |= (static_cast<int>(s.numConn[g]) & 0xf) << 4;
@@ -283,30 +280,40 @@ __global__ void __launch_bounds__(kBlock) kStage(DevState s)
 
 // ---------------------------------------------------------- pair laws ----
 // The pair phase of the two motion types as accumulators: begin() with the
-// cell's staged record, visit() once per candidate neighbour, end() writes
-// the cell's results.  Two enumerations feed them: kPairsRegion (shared-
-// memory tiles, the fast path) and pairsGlobal (tile lists in global memory,
-// used where a region does not fit).
+// cell's staged record, near() as a cheap reject on the squared distance,
+// visit() for the survivors, end() writes the cell's results.  Neighbours
+// are visited tile by tile (3x3 tiles around the cell, in row order) and,
+// within a tile, in storage order, so the FP32 sums are reproducible run to
+// run and identical alone or in a batch.  Two enumerations feed the laws:
+// kPairsRegion (shared-memory regions, the fast path) and pairsGlobal (tile
+// lists in global memory, for regions that do not fit).
+
+// sqrtf(q) <= R decided exactly (the reject bound is above R^2)
+__device__ __forceinline__ bool withinRadius(float q, float R, float& d)
+{
+    d = sqrtf(q);
+    return d <= R;
+}
 
 // CellProcessor::calcFluidForces_reconnectCells_correctOverlap,
-// CellProcessor.cuh:122-283.  visit() takes pd = p_i - p_j already corrected
-// for the torus.
+// CellProcessor.cuh:122-283.  pd = p_i - p_j already corrected for the torus.
 struct FluidLaw {
     const DevState* s;
     const AlienPhysicsParams* p;
     int g, W, H;
-    float h, R, R2reject, minDist;
+    float h, R, R2reject, minDist, fusionVelocity, maxBindingEnergy;
     float2 pi, vi;
     bool barrierI, fusionI;
     float densI;
     int bondsI[kMaxBonds];
-    long long qDens, qFpx, qFpy, qFvx, qFvy, qDx, qDy;
+    float dens;
+    float2 Fp, Fv, dx;
     int bestBarrier;
     float bestBarrierDist;
     int best;
     unsigned long long bestId;
 
-    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float4 mpv)
+    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float2 pos, float2 vel)
     {
         s = &st;
         p = &st.params[wi.paramIndex];
@@ -317,26 +324,31 @@ struct FluidLaw {
         R = h * 2.0f;
         R2reject = R * R * 1.0001f + 1e-6f;
         minDist = p->cellMinDistance;
-        pi = f2(mpv.x, mpv.y);
-        vi = f2(mpv.z, mpv.w);
+        fusionVelocity = p->cellFusionVelocity;
+        maxBindingEnergy = p->cellMaxBindingEnergy;
+        pi = pos;
+        vi = vel;
         barrierI = me.y & kStageBarrier;
         const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
         densI = __int_as_float(me.z);
-        fusionI = !barrierI && nI < maxI && __int_as_float(me.w) <= p->cellMaxBindingEnergy;
+        fusionI = !barrierI && nI < maxI && __int_as_float(me.w) <= maxBindingEnergy;
 #pragma unroll
         for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? st.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
-        qDens = qFpx = qFpy = qFvx = qFvy = qDx = qDy = 0;
+        dens = 0.0f;
+        Fp = Fv = dx = f2(0.0f, 0.0f);
         bestBarrier = -1;
         bestBarrierDist = 0.0f;
         best = -1;
         bestId = ~0ull;
     }
 
-    __device__ __forceinline__ void visit(int4 om, float4 opv, float2 pd)
+    __device__ __forceinline__ bool near(float2 pd) const { return pd.x * pd.x + pd.y * pd.y <= R2reject; }
+
+    __device__ __forceinline__ void visit(int4 om, float2 vj, float2 pd)
     {
         if (!(om.y & kStageVisible)) return;
         float d;
-        if (!withinRadius(pd.x * pd.x + pd.y * pd.y, R, R2reject, d)) return;
+        if (!withinRadius(pd.x * pd.x + pd.y * pd.y, R, d)) return;
         const int j = om.x;
         if (om.y & kStageBarrier) {
             if (bestBarrier < 0 || d < bestBarrierDist || (d == bestBarrierDist && j < bestBarrier)) {
@@ -345,28 +357,21 @@ struct FluidLaw {
             }
             return;
         }
-        qDens += toFix(sphKernel(d / h) / (h * h));
+        dens += sphKernel(d / h) / (h * h);
         if (j == g) return;
-        if (!barrierI && d < minDist) {
-            qDx += toFix(pd.x * minDist / 5.0f);
-            qDy += toFix(pd.y * minDist / 5.0f);
-        }
+        if (!barrierI && d < minDist) dx = dx + pd * (minDist / 5.0f);
         if (isBondedTo(bondsI, j)) return;
-        const float2 vd = vi - f2(opv.z, opv.w);
+        const float2 vd = vi - vj;
         const float densJ = __int_as_float(om.z);
         const float factor = densI / (densI * densI) + densJ / (densJ * densJ);
         if (fabsf(d) > kNearZero) {
             const float kd = sphKernelD(d / h) / (h * h * h);
-            const float2 fp = pd / (-d) * factor * kd;
-            const float2 fv = vd / densJ * d * kd / (d * d + 0.25f);
-            qFpx += toFix(fp.x);
-            qFpy += toFix(fp.y);
-            qFvx += toFix(fv.x);
-            qFvy += toFix(fv.y);
+            Fp = Fp + pd / (-d) * factor * kd;
+            Fv = Fv + vd / densJ * d * kd / (d * d + 0.25f);
         }
-        if (fusionI && len2(vd) >= p->cellFusionVelocity) {
+        if (fusionI && len2(vd) >= fusionVelocity) {
             const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
-            if (nJ < maxJ && __int_as_float(om.w) <= p->cellMaxBindingEnergy) {
+            if (nJ < maxJ && __int_as_float(om.w) <= maxBindingEnergy) {
                 const unsigned long long idJ = s->id[j];
                 if (idJ < bestId) {
                     bestId = idJ;
@@ -411,11 +416,10 @@ struct FluidLaw {
                 F = rr * (-2.0f * dvr / trr) / td;
             }
         }
-        const float2 Fp = f2(fromFix(qFpx), fromFix(qFpy)), Fv = f2(fromFix(qFvx), fromFix(qFvy));
         F = F + (Fp * p->pressureStrength + Fv * p->viscosityStrength);
         st.force[g] = F;
-        st.posB[g] = pi + f2(fromFix(qDx), fromFix(qDy));
-        st.densNew[g] = fromFix(qDens);
+        st.posB[g] = pi + dx;
+        st.densNew[g] = dens;
         st.best[g] = best;
     }
 };
@@ -424,9 +428,10 @@ struct FluidLaw {
 // CellProcessor.cuh:285-365 with CellMap::executeForEach (Map.cuh:175-196,
 // distance test on the uncorrected difference).  The reference adds each
 // pair force to both cells from the scanning cell; here every cell gathers
-// f(i,j) from its own scan and -f(j,i) from the scans that see it.  visit()
-// takes p_j as stored (candidates across the torus seam never pass the
-// uncorrected distance test, so they are not visited).
+// f(i,j) from its own scan and -f(j,i) from the scans that see it.  near()
+// and visit() take raw = p_j - p_i as stored: candidates across the torus
+// seam never pass the uncorrected test, and for |raw| <= R < W/2 the
+// corrected displacement is -raw exactly.
 __device__ __forceinline__ float2 collisionForce(float2 pd, float d, float2 vCell, float2 vOther, bool barrierCell,
                                                  const AlienPhysicsParams& p)
 {
@@ -443,67 +448,60 @@ __device__ __forceinline__ float2 collisionForce(float2 pd, float d, float2 vCel
 struct CollisionLaw {
     const DevState* s;
     const AlienPhysicsParams* p;
-    int g, W, H;
-    float R, R2reject, minDist;
+    int g;
+    float R, R2reject, minDist, fusionVelocity, maxBindingEnergy;
     float2 pi, vi;
     bool barrierI, visibleI, fusionI;
     float densI;
     int bondsI[kMaxBonds];
-    long long qFx, qFy, qDx, qDy;
+    float2 F, dx;
     int best;
     unsigned long long bestId;
 
-    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float4 mpv)
+    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float2 pos, float2 vel)
     {
         s = &st;
         p = &st.params[wi.paramIndex];
         g = me.x;
-        W = wi.W;
-        H = wi.H;
         R = p->cellMaxCollisionDistance;
         R2reject = R * R * 1.0001f + 1e-6f;
         minDist = p->cellMinDistance;
-        pi = f2(mpv.x, mpv.y);
-        vi = f2(mpv.z, mpv.w);
+        fusionVelocity = p->cellFusionVelocity;
+        maxBindingEnergy = p->cellMaxBindingEnergy;
+        pi = pos;
+        vi = vel;
         barrierI = me.y & kStageBarrier;
         visibleI = me.y & kStageVisible;
         const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
         densI = __int_as_float(me.z);
-        fusionI = !barrierI && nI < maxI && __int_as_float(me.w) <= p->cellMaxBindingEnergy;
+        fusionI = !barrierI && nI < maxI && __int_as_float(me.w) <= maxBindingEnergy;
 #pragma unroll
         for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? st.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
-        qFx = qFy = qDx = qDy = 0;
+        F = dx = f2(0.0f, 0.0f);
         best = -1;
         bestId = ~0ull;
     }
 
-    __device__ __forceinline__ void visit(int4 om, float4 opv)
+    __device__ __forceinline__ bool near(float2 raw) const { return raw.x * raw.x + raw.y * raw.y <= R2reject; }
+
+    __device__ __forceinline__ void visit(int4 om, float2 vj, float2 raw)
     {
         const int j = om.x;
         if (j == g) return;
-        const float2 pj = f2(opv.x, opv.y);
-        const float2 raw = pj - pi;
-        float dRaw;
-        if (!withinRadius(raw.x * raw.x + raw.y * raw.y, R, R2reject, dRaw)) return;
+        float d;
+        if (!withinRadius(raw.x * raw.x + raw.y * raw.y, R, d)) return;
         const bool visibleJ = om.y & kStageVisible;
         if (!visibleJ && !visibleI) return;
-        const float2 pd = correctDirection(pi - pj, W, H);
-        const float d = len2(pd);
+        const float2 pd = f2(-raw.x, -raw.y);
         const bool bonded = isBondedTo(bondsI, j);
-        const float2 vj = f2(opv.z, opv.w);
         if (visibleJ) {  // i's own scan sees j
-            if (!barrierI && d < minDist) {
-                qDx += toFix(pd.x * minDist / 5.0f);
-                qDy += toFix(pd.y * minDist / 5.0f);
-            }
+            if (!barrierI && d < minDist) dx = dx + pd * (minDist / 5.0f);
             if (!bonded) {
-                const float2 f = collisionForce(pd, d, vi, vj, barrierI, *p);
-                qFx += toFix(f.x);
-                qFy += toFix(f.y);
+                F = F + collisionForce(pd, d, vi, vj, barrierI, *p);
                 const float2 vd = vi - vj;
-                if (fusionI && len2(vd) >= p->cellFusionVelocity && dot2(pd, vd) < 0.0f) {
+                if (fusionI && len2(vd) >= fusionVelocity && dot2(pd, vd) < 0.0f) {
                     const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
-                    if (nJ < maxJ && !(om.y & kStageBarrier) && __int_as_float(om.w) <= p->cellMaxBindingEnergy) {
+                    if (nJ < maxJ && !(om.y & kStageBarrier) && __int_as_float(om.w) <= maxBindingEnergy) {
                         const unsigned long long idJ = s->id[j];
                         if (idJ < bestId) {
                             bestId = idJ;
@@ -513,25 +511,22 @@ struct CollisionLaw {
                 }
             }
         }
-        if (visibleI && !bonded) {  // j's scan sees i and applies -f(j,i) to i
-            const float2 pdj = correctDirection(pj - pi, W, H);
-            const float2 f = collisionForce(pdj, len2(pdj), vj, vi, om.y & kStageBarrier, *p);
-            qFx -= toFix(f.x);
-            qFy -= toFix(f.y);
-        }
+        if (visibleI && !bonded)  // j's scan sees i and applies -f(j,i) to i
+            F = F - collisionForce(raw, d, vj, vi, om.y & kStageBarrier, *p);
     }
 
     __device__ __forceinline__ void end()
     {
         const DevState& st = *s;
-        st.force[g] = f2(fromFix(qFx), fromFix(qFy));
-        st.posB[g] = pi + f2(fromFix(qDx), fromFix(qDy));
+        st.force[g] = F;
+        st.posB[g] = pi + dx;
         st.densNew[g] = densI;
         st.best[g] = best;
     }
 };
 
 // the pair phase of the staged cell k, neighbours from the global tile lists
+// (tiles in the same row order as the regions' 3x3 scan)
 template <int Motion>
 __device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
 {
@@ -543,50 +538,61 @@ __device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
     const int sx = slotX(pi.x, wi.W), sy = slotX(pi.y, wi.H);
     if (Motion == ALIEN_B200_MOTION_FLUID) {
         FluidLaw law;
-        law.begin(s, wi, me, mpv);
+        law.begin(s, wi, me, pi, f2(mpv.z, mpv.w));
         forEachWindowTile(wi, sx, sy, [&](long long t) {
             const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
             for (uint32_t m = k0; m < k1; ++m) {
                 const float4 opv = s.stagedPV[m];
-                law.visit(s.stagedMeta[m], opv, correctDirection(pi - f2(opv.x, opv.y), wi.W, wi.H));
+                const float2 pd = correctDirection(pi - f2(opv.x, opv.y), wi.W, wi.H);
+                if (law.near(pd)) law.visit(s.stagedMeta[m], f2(opv.z, opv.w), pd);
             }
         });
         law.end();
     } else {
         CollisionLaw law;
-        law.begin(s, wi, me, mpv);
+        law.begin(s, wi, me, pi, f2(mpv.z, mpv.w));
         forEachWindowTile(wi, sx, sy, [&](long long t) {
             const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
-            for (uint32_t m = k0; m < k1; ++m) law.visit(s.stagedMeta[m], s.stagedPV[m]);
+            for (uint32_t m = k0; m < k1; ++m) {
+                const float4 opv = s.stagedPV[m];
+                const float2 raw = f2(opv.x, opv.y) - pi;
+                if (law.near(raw)) law.visit(s.stagedMeta[m], f2(opv.z, opv.w), raw);
+            }
         });
         law.end();
     }
 }
 
 // ------------------------------------------------------- kPairsRegion ----
-// One CTA per region of regW x regH tiles of one world.  It copies the staged
-// records of the region and of its one-tile halo from the tile-sorted arrays
-// into shared memory (each tile a contiguous run), shifting halo tiles that
-// lie across the torus seam by +-W / +-H so that plain differences are the
-// minimal-image displacements, and then runs the pair law of every cell of
-// the region against the 3x3 local tiles around its tile.  Regions whose
-// records exceed the shared buffer, and worlds too small for regions, use
-// pairsGlobal for their cells.
+// One CTA per region of regW x regH tiles (up to 32 x 16) of one world.  It
+// copies the staged records of the region and of its one-tile halo from the
+// tile-sorted arrays into shared memory (each tile a contiguous run),
+// shifting halo tiles that lie across the torus seam by +-W / +-H so that
+// plain differences are the minimal-image displacements, and then runs the
+// pair law of every cell of the region against the 3x3 local tiles around
+// its tile.  The inner loop reads positions only until a candidate passes
+// the distance reject.  Regions whose records exceed the shared buffer, and
+// worlds too small for regions, use pairsGlobal for their cells.
 constexpr int kRegionThreads = 256;
-constexpr int kRegionCap = 1280;          // staged records per CTA (halo included)
-constexpr int kRegionMaxTiles = 18 * 10;  // (regW + 2) x (regH + 2) for 16 x 8 regions
+constexpr int kRegionMaxW = 32, kRegionMaxH = 16;
+constexpr int kRegionMaxTiles = (kRegionMaxW + 2) * (kRegionMaxH + 2);
+constexpr int kRegionCap = 2304;  // staged records per CTA (halo included)
+constexpr size_t kRegionDynSmem = static_cast<size_t>(kRegionCap) * (sizeof(int4) + 2 * sizeof(float2) + sizeof(uint16_t));
 
 template <int Motion>
 __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
 {
-    __shared__ float4 sPV[kRegionCap];
-    __shared__ int4 sMeta[kRegionCap];
-    __shared__ uint8_t sTile[kRegionCap];
-    __shared__ int tStart[kRegionMaxTiles + 1];   // shared-memory offset of each local tile
+    extern __shared__ int4 dyn[];
+    int4* sMeta = dyn;
+    float2* sPos = reinterpret_cast<float2*>(sMeta + kRegionCap);
+    float2* sVel = sPos + kRegionCap;
+    uint16_t* sTile = reinterpret_cast<uint16_t*>(sVel + kRegionCap);
+    __shared__ int tStart[kRegionMaxTiles];   // shared-memory offset of each local tile
     __shared__ int tCount[kRegionMaxTiles];
-    __shared__ int tGlobal[kRegionMaxTiles];      // first sorted index of the tile
+    __shared__ int tGlobal[kRegionMaxTiles];  // first sorted index of the tile
+    __shared__ int sOrder[kRegionMaxTiles];   // local tiles by increasing offset
     __shared__ float2 tShift[kRegionMaxTiles];
-    __shared__ int sOrder[kRegionMaxTiles];
+    __shared__ uint8_t tOwn[kRegionMaxTiles];
     __shared__ int sOwnTotal, sTotal;
 
     const int w = s.regionWorld[blockIdx.x];
@@ -610,11 +616,8 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
     }
 
     const int LW = ownW + 2, LH = ownH + 2, NT = LW * LH;
-    // 1. local tile table (NT <= kRegionMaxTiles <= kRegionThreads)
-    int cnt = 0;
-    bool own = false;
-    const int lt = threadIdx.x;
-    if (lt < NT) {
+    // 1. local tile table
+    for (int lt = threadIdx.x; lt < NT; lt += kRegionThreads) {
         const int lx = lt % LW, ly = lt / LW;
         int gx = tx0 - 1 + lx, gy = ty0 - 1 + ly;
         float2 sh = f2(0.0f, 0.0f);
@@ -634,22 +637,47 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
         }
         const long long t = wi.tileBase + gx + static_cast<long long>(gy) * wi.nTX;
         const uint32_t k0 = s.tileStart[t];
-        cnt = static_cast<int>(s.tileStart[t + 1] - k0);
         tGlobal[lt] = static_cast<int>(k0);
-        tCount[lt] = cnt;
+        tCount[lt] = static_cast<int>(s.tileStart[t + 1] - k0);
         tShift[lt] = sh;
-        own = lx >= 1 && lx <= ownW && ly >= 1 && ly <= ownH;
+        tOwn[lt] = (lx >= 1 && lx <= ownW && ly >= 1 && ly <= ownH) ? 1 : 0;
     }
-    // own tiles first, then the halo
-    uint32_t ownTotal, haloTotal, ownTiles, haloTiles;
-    const uint32_t ownOff = blockExclusiveScan(own ? cnt : 0, &ownTotal);
-    const uint32_t haloOff = blockExclusiveScan(own ? 0 : cnt, &haloTotal);
-    const uint32_t ownRank = blockExclusiveScan(own ? 1u : 0u, &ownTiles);
-    const uint32_t haloRank = blockExclusiveScan((lt < NT && !own) ? 1u : 0u, &haloTiles);
-    if (lt < NT) tStart[lt] = static_cast<int>(own ? ownOff : ownTotal + haloOff);
-    if (threadIdx.x == 0) {
-        sOwnTotal = static_cast<int>(ownTotal);
-        sTotal = static_cast<int>(ownTotal + haloTotal);
+    __syncthreads();
+    // offsets: own tiles first, then the halo, each in tile order; every
+    // thread handles a contiguous chunk of tiles
+    {
+        const int chunk = (NT + kRegionThreads - 1) / kRegionThreads;
+        const int c0 = min(NT, static_cast<int>(threadIdx.x) * chunk), c1 = min(NT, c0 + chunk);
+        uint32_t ownCnt = 0, haloCnt = 0, ownT = 0, haloT = 0;
+        for (int lt = c0; lt < c1; ++lt) {
+            if (tOwn[lt]) {
+                ownCnt += tCount[lt];
+                ++ownT;
+            } else {
+                haloCnt += tCount[lt];
+                ++haloT;
+            }
+        }
+        uint32_t ownTotal, haloTotal, ownTiles, haloTiles;
+        uint32_t oc = blockExclusiveScan(ownCnt, &ownTotal);
+        uint32_t hc = blockExclusiveScan(haloCnt, &haloTotal);
+        uint32_t ot = blockExclusiveScan(ownT, &ownTiles);
+        uint32_t ht = blockExclusiveScan(haloT, &haloTiles);
+        for (int lt = c0; lt < c1; ++lt) {
+            if (tOwn[lt]) {
+                tStart[lt] = static_cast<int>(oc);
+                oc += tCount[lt];
+                sOrder[ot++] = lt;
+            } else {
+                tStart[lt] = static_cast<int>(ownTotal + hc);
+                hc += tCount[lt];
+                sOrder[ownTiles + ht++] = lt;
+            }
+        }
+        if (threadIdx.x == 0) {
+            sOwnTotal = static_cast<int>(ownTotal);
+            sTotal = static_cast<int>(ownTotal + haloTotal);
+        }
     }
     __syncthreads();
     const int total = sTotal;
@@ -663,14 +691,10 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
             }
         return;
     }
-    // 2. copy: every thread one record per round; its local tile is found by
-    //    binary search in the offset table (own tiles first, then the halo,
-    //    each group in tile order, so offsets increase along the search order)
-    //    sOrder lists the local tiles by shared-memory offset.
-    if (lt < NT) sOrder[own ? static_cast<int>(ownRank) : static_cast<int>(ownTiles + haloRank)] = lt;
-    __syncthreads();
+    // 2. copy: every thread one record per round; its local tile is the last
+    //    one in offset order that starts at or before the record
     for (int e = threadIdx.x; e < total; e += kRegionThreads) {
-        int lo = 0, hi = NT - 1;  // last tile in offset order whose start <= e
+        int lo = 0, hi = NT - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
             if (tStart[sOrder[mid]] <= e)
@@ -681,12 +705,11 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
         const int q = sOrder[lo];
         const int src = tGlobal[q] + (e - tStart[q]);
         const float2 sh = tShift[q];
-        float4 pv = s.stagedPV[src];
-        pv.x += sh.x;
-        pv.y += sh.y;
-        sPV[e] = pv;
+        const float4 pv = s.stagedPV[src];
+        sPos[e] = f2(pv.x + sh.x, pv.y + sh.y);
+        sVel[e] = f2(pv.z, pv.w);
         sMeta[e] = s.stagedMeta[src];
-        sTile[e] = static_cast<uint8_t>(q);
+        sTile[e] = static_cast<uint16_t>(q);
     }
     __syncthreads();
     // 3. pair law of every own cell against its 3x3 local tiles
@@ -694,12 +717,10 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
     for (int e = threadIdx.x; e < ownN; e += kRegionThreads) {
         const int q = sTile[e];
         const int lx = q % LW, ly = q / LW;
-        const int4 me = sMeta[e];
-        const float4 mpv = sPV[e];
+        const float2 pi = sPos[e];
         if (Motion == ALIEN_B200_MOTION_FLUID) {
             FluidLaw law;
-            law.begin(s, wi, me, mpv);
-            const float2 pi = f2(mpv.x, mpv.y);
+            law.begin(s, wi, sMeta[e], pi, sVel[e]);
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy)
 #pragma unroll 1
@@ -707,14 +728,14 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
                     const int q2 = (ly + dy) * LW + (lx + dx);
                     const int b0 = tStart[q2], b1 = b0 + tCount[q2];
                     for (int m = b0; m < b1; ++m) {
-                        const float4 opv = sPV[m];
-                        law.visit(sMeta[m], opv, pi - f2(opv.x, opv.y));
+                        const float2 pd = pi - sPos[m];
+                        if (law.near(pd)) law.visit(sMeta[m], sVel[m], pd);
                     }
                 }
             law.end();
         } else {
             CollisionLaw law;
-            law.begin(s, wi, me, mpv);
+            law.begin(s, wi, sMeta[e], pi, sVel[e]);
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy)
 #pragma unroll 1
@@ -723,7 +744,10 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
                     const float2 sh = tShift[q2];
                     if (sh.x != 0.0f || sh.y != 0.0f) continue;  // across the seam: uncorrected distance > R
                     const int b0 = tStart[q2], b1 = b0 + tCount[q2];
-                    for (int m = b0; m < b1; ++m) law.visit(sMeta[m], sPV[m]);
+                    for (int m = b0; m < b1; ++m) {
+                        const float2 raw = sPos[m] - pi;
+                        if (law.near(raw)) law.visit(sMeta[m], sVel[m], raw);
+                    }
                 }
             law.end();
         }
