@@ -1,7 +1,8 @@
 """Build of ``libalien_b200.so`` for sm_100a (nvcc, in-tree output).
 
 ``python -m alien_b200.build`` compiles alien_b200/csrc/engine.cu (which
-includes the kernel headers) into alien_b200/libalien_b200.so.  No torch
+includes the kernel headers) and alien_b200/csrc/no_alloc.cu into
+alien_b200/libalien_b200.so.  No torch
 types cross the library boundary; the C ABI is include/alien_b200.h.
 """
 from __future__ import annotations
@@ -46,7 +47,7 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, os.path.join(CSRC, "engine.cu"), "-o", OUT + ".tmp"]
+    cmd = [nvcc(), *NVCC_FLAGS, os.path.join(CSRC, "engine.cu"), os.path.join(CSRC, "no_alloc.cu"), "-o", OUT + ".tmp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)

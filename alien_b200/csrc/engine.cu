@@ -29,6 +29,8 @@ namespace ab {
 
 thread_local std::string g_lastError;
 
+void setLastError(const std::string& message) { g_lastError = message; }
+
 struct Error : std::runtime_error {
     int code;
     Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}

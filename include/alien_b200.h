@@ -297,6 +297,24 @@ int alien_b200_timed_timesteps(alien_b200_simulation* sim, uint64_t timesteps, d
                                int* numKernels);
 const char* alien_b200_step_kernel_name(int index);
 
+/* Statistics of transfer objects that already sit in device memory,
+ * computed without allocating anything on the device.  No counterpart in
+ * the reference.  For callers that cannot call cudaMalloc when they need the
+ * numbers: a host runtime that reserved the whole HBM budget up front and
+ * lends out only its own buffers, or code running while another component
+ * owns the allocator.  cells / particles / statistics are device pointers
+ * owned by the caller (statistics: one AlienRawStatistics written on
+ * `stream`, a cudaStream_t or NULL); the result equals
+ * alien_b200_get_raw_statistics for the same objects.  The only scratch is a
+ * fixed 704 KB array inside the library that every GPU loading it keeps
+ * until exit, which bounds one call to 8,388,608 cells and as many
+ * particles; larger inputs return ALIEN_B200_ERR_CAPACITY.  The first call
+ * on a device looks up the array's device address, so make it before any
+ * stream capture.  Calls that overlap on the GPU share the array and race. */
+int alien_b200_statistics_no_alloc(const AlienCellTO* cells, uint64_t numCells, const AlienParticleTO* particles,
+                                   uint64_t numParticles, uint64_t timestep, AlienRawStatistics* statistics,
+                                   void* stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
