@@ -11,10 +11,10 @@ motion, bond breaking on.  State is larger than L2 (126 MB), so no flush is
 needed between steps.  Prints one JSON line (rank 0).
 
 --impl reference times the reference's own implementation of the path on
-this machine; the reference ships only a CUDA engine, whose harness is
-oracle/ref (built from the reference sources when they are present); without
-it, the CPU restatement of the same step (oracle, FP32, OpenMP over all host
-threads) is timed and reported as a port.
+this machine: the reference ships only a CUDA engine, built from its sources
+for sm_100a as oracle/_ref/ref_run and stepped from the same world; without
+that binary, the CPU restatement of the same step (oracle, FP32, OpenMP over
+all host threads) is timed and reported as a port.
 """
 from __future__ import annotations
 
@@ -187,10 +187,55 @@ def cpu_baseline(data, world, prm, budget_s: float = 20.0, max_steps: int = 1000
 
 
 def run_reference(args, config, rank, world_size):
-    """--impl reference: the reference path timed on this machine"""
+    """--impl reference: the reference path timed on this machine.
+
+    The reference's path is its CUDA engine (_SimulationCudaFacade::
+    calcTimestep, source/EngineGpuKernels/SimulationCudaFacade.cu:128-160),
+    built from the reference sources for sm_100a as oracle/_ref/ref_run and
+    driven through its own facade from the identical DataTO: W warm-up steps,
+    then K steps in one calcTimestep(K, false) call timed by wall clock (the
+    facade synchronises after every step).  Without that binary (or a GPU),
+    the CPU restatement of the same step is timed instead."""
     if rank != 0:
         return 0
-    data, world, prm, desc = build_workload(config)
+    from oracle import refrun
+
+    if config == "batched256":
+        return run_reference_batched(args, refrun)
+    # The reference engine holds at most about 1.83M cells in one world (its
+    # dynamic-memory bound in SimulationData::resizeObjects,
+    # SimulationData.cu:93, is an int that overflows for larger cell
+    # arrays); the 4M-cell world is timed on its 1M-cell quarter, which has
+    # the same density, cluster shape and velocity distribution.
+    sample_config = {"hex4m": "hex1m"}.get(config, config)
+    data, world, prm, desc = build_workload(sample_config)
+
+    gpu = False
+    try:
+        import torch
+        gpu = torch.cuda.is_available()
+    except ImportError:
+        pass
+    if refrun.available() and gpu:
+        log(f"reference CUDA engine: {args.warmup} warm-up + {args.steps} timed steps")
+        _, seconds, _ = refrun.run(data, world, prm, steps=args.steps, warmup=args.warmup, timeout=1500)
+        value = data.num_cells * args.steps / seconds / 1e6
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * seconds / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": config, "sample_workload": sample_config, "description": desc,
+                       "cells": data.num_cells},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": 1, "kind": "reference",
+                             "sample": f"the reference CUDA engine on cuda:0 (one host thread driving it), "
+                                       f"{sample_config} ({data.num_cells} cells): "
+                                       f"{args.steps} steps after {args.warmup} warm-up steps"},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference engine (source/EngineGpuKernels, all units) compiled for sm_100a with its own flags; "
+                    "timed around _SimulationCudaFacade::calcTimestep(K, false), which synchronises every step",
+        }
+        print(json.dumps(line))
+        return 0
     base, steps, dt = cpu_baseline(data, world, prm, budget_s=min(120.0, 5.0 + 2.0 * args.steps))
     line = {
         "impl": "reference", "metric": METRIC, "value": base["value"], "unit": METRIC, "n_gpus": 0,
@@ -199,7 +244,37 @@ def run_reference(args, config, rank, world_size):
         "config": {"workload": config, "description": desc, "cells": data.num_cells},
         "cpu_baseline": base,
         "e2e": {"value": base["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference ships no CPU engine; this is the CPU restatement of the same step (oracle, FP32, OpenMP)",
+        "note": "reference CUDA engine not built here; this is the CPU restatement of the same step "
+                "(oracle, FP32, OpenMP)",
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_reference_batched(args, refrun, sample: int = 32):
+    """the reference engine steps worlds of the 256-world batch one after
+    another (it holds one world per facade); timed on the first ``sample``
+    worlds, the same worlds as rank 0 of the batched arm"""
+    from alien_b200 import params as P
+    from alien_b200 import worldgen
+
+    sizes = worldgen.batched_sizes(seed=0, count=256)[:sample]
+    cells, seconds = 0, 0.0
+    for i, n in enumerate(sizes):
+        d, w = worldgen.mixed_world(seed=i, num_cells=int(n))
+        _, dt, _ = refrun.run(d, w, P.benchmark_parameters(P.MOTION_FLUID), steps=args.steps, warmup=args.warmup)
+        cells += d.num_cells
+        seconds += dt
+    value = cells * args.steps / seconds / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * seconds / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batched256", "worlds_timed": sample, "cells": cells},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": 1, "kind": "reference",
+                         "sample": f"the reference CUDA engine stepping the first {sample} of the 256 worlds one "
+                                   f"after another, {args.steps} steps each after {args.warmup} warm-up steps"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
@@ -349,7 +424,7 @@ def main():
     alg_bytes = algorithmic_bytes(dominant, bonds) * stats1.numCells
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", f"{dominant}_{args.config}_traffic.json")
+    tpath = os.path.join(ROOT, "profiles", f"{dominant.split('<')[0]}_{args.config}_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             traffic = json.load(f).get("bytes_per_launch")

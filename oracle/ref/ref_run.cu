@@ -13,6 +13,7 @@
 //         u64 timestep, CellTO[], ParticleTO[], aux bytes
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -122,10 +123,20 @@ int main(int argc, char** argv)
         settings.generalSettings.worldSizeX = W;
         settings.generalSettings.worldSizeY = H;
         settings.simulationParameters = toReference(params);
-        auto facade = std::make_shared<_SimulationCudaFacade>(timestep, settings);
+        // never destroyed: when a CUDA call inside the facade throws, its
+        // destructor (run during unwinding) throws again from cudaFree and
+        // aborts the process before the first error is reported
+        auto* facade = new _SimulationCudaFacade(timestep, settings);
 
-        // pre-size the arrays: no timed step includes a resize
-        ArraySizes additional{nc * 2 + 1000, (np + nc) * 2 + 1000, na + 1000};
+        // pre-size the arrays as the reference's own setSimulationData path
+        // does (exact counts; the facade keeps 3x headroom), plus room for
+        // particles from dying cells, so that no timed step includes a
+        // resize.  Larger requests overflow the int bound of the dynamic
+        // memory in SimulationData::resizeObjects (SimulationData.cu:93):
+        // for cell arrays above 6,391,320 entries, i.e. worlds above about
+        // 1.83M cells, it wraps to an undersized buffer and the reference's
+        // kernels fail; oracle/refrun.py refuses such worlds.
+        ArraySizes additional{nc, np + nc / 4, na};
         facade->resizeArraysIfNecessary(additional);
 
         DataTO to;
@@ -165,7 +176,9 @@ int main(int argc, char** argv)
         writeOrThrow(o, out.auxiliaryData, *out.numAuxiliaryData);
         fclose(o);
         out.destroy();
-        facade.reset();
+        // process exit releases the facade's device memory
+        fflush(nullptr);
+        std::_Exit(0);
     } catch (std::exception const& e) {
         fprintf(stderr, "ref_run: %s\n", e.what());
         return 1;

@@ -46,10 +46,26 @@ def read_output(path):
     return DataTO(cells, parts, aux), seconds, ts
 
 
+# Largest cell count the reference engine can hold in one world.  Its
+# dynamic-memory bound (SimulationData::resizeObjects, SimulationData.cu:93)
+# is an int: 336 bytes x (cell array size + 1000), where the cell array is
+# 3 x (300000 + requested cells) after the facade's first resize
+# (SimulationData.cu:51-56, 121-126).  Above 6,391,320 array entries the
+# product wraps; a 4M-cell world then gets a dynamic memory of about 40 MB
+# instead of 4.3 GB, and its first step ended in cudaErrorLaunchFailure
+# (an out-of-bounds access inside the reference's kernels).  Such worlds
+# are refused here before the reference engine ever sees them.
+REF_MAX_CELLS = (2**31 - 1) // 336 - 1000
+REF_MAX_CELLS = REF_MAX_CELLS // 3 - 300000
+
+
 def run(data: DataTO, world, params: PhysicsParams, steps=1, warmup=0, timestep=0, timeout=1800):
     """returns (DataTO after warmup + steps, seconds of the timed steps, timestep)"""
     if not available():
         raise FileNotFoundError(f"{REF_RUN} not built")
+    if data.num_cells > REF_MAX_CELLS:
+        raise ValueError(f"the reference engine holds at most {REF_MAX_CELLS} cells in one world "
+                         f"(int overflow of its dynamic-memory bound), got {data.num_cells}")
     with tempfile.TemporaryDirectory() as d:
         inp, out = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
         write_input(inp, data, world, params, timestep, warmup, steps)
