@@ -566,18 +566,28 @@ __device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
 // ------------------------------------------------------- kPairsRegion ----
 // One CTA per region of regW x regH tiles (up to 32 x 16) of one world.  It
 // copies the staged records of the region and of its one-tile halo from the
-// tile-sorted arrays into shared memory (each tile a contiguous run),
-// shifting halo tiles that lie across the torus seam by +-W / +-H so that
-// plain differences are the minimal-image displacements, and then runs the
-// pair law of every cell of the region against the 3x3 local tiles around
-// its tile.  The inner loop reads positions only until a candidate passes
-// the distance reject.  Regions whose records exceed the shared buffer, and
-// worlds too small for regions, use pairsGlobal for their cells.
+// tile-sorted arrays into shared memory, all (regW+2) x (regH+2) local tiles
+// in row-major order (each tile a contiguous run in storage order), so that
+// the three tiles of one row of a cell's 3x3 window are one contiguous run.
+// Fluid worlds shift halo tiles that lie across the torus seam by +-W / +-H,
+// so that plain differences are the minimal-image displacements; collision
+// worlds keep stored positions (the reference's distance test is on the
+// uncorrected difference, so candidates across the seam never pass).
+// Every cell then scans its three runs with the cheap distance reject only,
+// appending survivors to a per-thread hit list in shared memory, and runs the
+// pair law on the hits afterwards: the scan loop stays convergent across the
+// warp, and the law runs once per hit instead of once per scan iteration in
+// which any lane of the warp had a hit.  Hits are visited in scan order (row
+// by row, tile by tile, storage order), so the FP32 sums do not change.
+// Regions whose records exceed the shared buffer, and worlds too small for
+// regions, use pairsGlobal for their cells.
 constexpr int kRegionThreads = 256;
 constexpr int kRegionMaxW = 32, kRegionMaxH = 16;
 constexpr int kRegionMaxTiles = (kRegionMaxW + 2) * (kRegionMaxH + 2);
 constexpr int kRegionCap = 2304;  // staged records per CTA (halo included)
-constexpr size_t kRegionDynSmem = static_cast<size_t>(kRegionCap) * (sizeof(int4) + 2 * sizeof(float2) + sizeof(uint16_t));
+constexpr int kHitCap = 24;       // hit-list entries per thread before a flush
+constexpr size_t kRegionDynSmem = static_cast<size_t>(kRegionCap) * (sizeof(int4) + 2 * sizeof(float2) + sizeof(uint16_t))
+                                  + static_cast<size_t>(kHitCap) * kRegionThreads * sizeof(uint16_t);
 
 template <int Motion>
 __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
@@ -587,13 +597,11 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
     float2* sPos = reinterpret_cast<float2*>(sMeta + kRegionCap);
     float2* sVel = sPos + kRegionCap;
     uint16_t* sTile = reinterpret_cast<uint16_t*>(sVel + kRegionCap);
-    __shared__ int tStart[kRegionMaxTiles];   // shared-memory offset of each local tile
-    __shared__ int tCount[kRegionMaxTiles];
-    __shared__ int tGlobal[kRegionMaxTiles];  // first sorted index of the tile
-    __shared__ int sOrder[kRegionMaxTiles];   // local tiles by increasing offset
+    uint16_t* sHits = sTile + kRegionCap;      // [kHitCap][kRegionThreads]
+    __shared__ int tStart[kRegionMaxTiles + 1];  // shared-memory offset of each local tile
+    __shared__ int tGlobal[kRegionMaxTiles];     // first sorted index of the tile
     __shared__ float2 tShift[kRegionMaxTiles];
-    __shared__ uint8_t tOwn[kRegionMaxTiles];
-    __shared__ int sOwnTotal, sTotal;
+    __shared__ int rowOwn[kRegionMaxH + 1];      // own records before own row r
 
     const int w = s.regionWorld[blockIdx.x];
     const WorldInfo& wi = s.worlds[w];
@@ -616,140 +624,125 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
     }
 
     const int LW = ownW + 2, LH = ownH + 2, NT = LW * LH;
-    // 1. local tile table
-    for (int lt = threadIdx.x; lt < NT; lt += kRegionThreads) {
-        const int lx = lt % LW, ly = lt / LW;
-        int gx = tx0 - 1 + lx, gy = ty0 - 1 + ly;
-        float2 sh = f2(0.0f, 0.0f);
-        if (gx < 0) {
-            gx += wi.nTX;
-            sh.x = -static_cast<float>(wi.W);
-        } else if (gx >= wi.nTX) {
-            gx -= wi.nTX;
-            sh.x = static_cast<float>(wi.W);
-        }
-        if (gy < 0) {
-            gy += wi.nTY;
-            sh.y = -static_cast<float>(wi.H);
-        } else if (gy >= wi.nTY) {
-            gy -= wi.nTY;
-            sh.y = static_cast<float>(wi.H);
-        }
-        const long long t = wi.tileBase + gx + static_cast<long long>(gy) * wi.nTX;
-        const uint32_t k0 = s.tileStart[t];
-        tGlobal[lt] = static_cast<int>(k0);
-        tCount[lt] = static_cast<int>(s.tileStart[t + 1] - k0);
-        tShift[lt] = sh;
-        tOwn[lt] = (lx >= 1 && lx <= ownW && ly >= 1 && ly <= ownH) ? 1 : 0;
-    }
-    __syncthreads();
-    // offsets: own tiles first, then the halo, each in tile order; every
-    // thread handles a contiguous chunk of tiles
+    // 1. local tile table (row-major over the region and its halo); every
+    //    thread handles a contiguous chunk of tiles for the offsets
     {
         const int chunk = (NT + kRegionThreads - 1) / kRegionThreads;
         const int c0 = min(NT, static_cast<int>(threadIdx.x) * chunk), c1 = min(NT, c0 + chunk);
-        uint32_t ownCnt = 0, haloCnt = 0, ownT = 0, haloT = 0;
+        uint32_t cnt = 0;
         for (int lt = c0; lt < c1; ++lt) {
-            if (tOwn[lt]) {
-                ownCnt += tCount[lt];
-                ++ownT;
-            } else {
-                haloCnt += tCount[lt];
-                ++haloT;
+            const int lx = lt % LW, ly = lt / LW;
+            int gx = tx0 - 1 + lx, gy = ty0 - 1 + ly;
+            float2 sh = f2(0.0f, 0.0f);
+            if (gx < 0) {
+                gx += wi.nTX;
+                sh.x = -static_cast<float>(wi.W);
+            } else if (gx >= wi.nTX) {
+                gx -= wi.nTX;
+                sh.x = static_cast<float>(wi.W);
             }
+            if (gy < 0) {
+                gy += wi.nTY;
+                sh.y = -static_cast<float>(wi.H);
+            } else if (gy >= wi.nTY) {
+                gy -= wi.nTY;
+                sh.y = static_cast<float>(wi.H);
+            }
+            const long long t = wi.tileBase + gx + static_cast<long long>(gy) * wi.nTX;
+            const uint32_t k0 = s.tileStart[t];
+            const uint32_t n = s.tileStart[t + 1] - k0;
+            tGlobal[lt] = static_cast<int>(k0);
+            tStart[lt] = static_cast<int>(n);  // count for now
+            tShift[lt] = Motion == ALIEN_B200_MOTION_FLUID ? sh : f2(0.0f, 0.0f);
+            cnt += n;
         }
-        uint32_t ownTotal, haloTotal, ownTiles, haloTiles;
-        uint32_t oc = blockExclusiveScan(ownCnt, &ownTotal);
-        uint32_t hc = blockExclusiveScan(haloCnt, &haloTotal);
-        uint32_t ot = blockExclusiveScan(ownT, &ownTiles);
-        uint32_t ht = blockExclusiveScan(haloT, &haloTiles);
+        uint32_t total;
+        uint32_t off = blockExclusiveScan(cnt, &total);
         for (int lt = c0; lt < c1; ++lt) {
-            if (tOwn[lt]) {
-                tStart[lt] = static_cast<int>(oc);
-                oc += tCount[lt];
-                sOrder[ot++] = lt;
-            } else {
-                tStart[lt] = static_cast<int>(ownTotal + hc);
-                hc += tCount[lt];
-                sOrder[ownTiles + ht++] = lt;
-            }
+            const int n = tStart[lt];
+            tStart[lt] = static_cast<int>(off);
+            off += n;
         }
-        if (threadIdx.x == 0) {
-            sOwnTotal = static_cast<int>(ownTotal);
-            sTotal = static_cast<int>(ownTotal + haloTotal);
-        }
+        if (threadIdx.x == 0) tStart[NT] = static_cast<int>(total);
     }
     __syncthreads();
-    const int total = sTotal;
+    const int total = tStart[NT];
+    if (threadIdx.x <= ownH) {
+        // own records of rows 1..r (own row segments are [tStart[r*LW+1], tStart[r*LW+ownW+1]))
+        int acc = 0;
+        for (int r = 1; r <= static_cast<int>(threadIdx.x); ++r) acc += tStart[r * LW + ownW + 1] - tStart[r * LW + 1];
+        rowOwn[threadIdx.x] = acc;
+    }
     if (total > kRegionCap) {
         // denser than the shared buffer: the region's own cells from global memory
         for (int ly = 1; ly <= ownH; ++ly)
             for (int lx = 1; lx <= ownW; ++lx) {
                 const int q = ly * LW + lx;
-                for (int k = tGlobal[q] + threadIdx.x; k < tGlobal[q] + tCount[q]; k += kRegionThreads)
-                    pairsGlobal<Motion>(s, k);
+                const int k0 = tGlobal[q], n = tStart[q + 1] - tStart[q];
+                for (int k = k0 + threadIdx.x; k < k0 + n; k += kRegionThreads) pairsGlobal<Motion>(s, k);
             }
         return;
     }
     // 2. copy: every thread one record per round; its local tile is the last
-    //    one in offset order that starts at or before the record
+    //    one that starts at or before the record
     for (int e = threadIdx.x; e < total; e += kRegionThreads) {
         int lo = 0, hi = NT - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (tStart[sOrder[mid]] <= e)
+            if (tStart[mid] <= e)
                 lo = mid;
             else
                 hi = mid - 1;
         }
-        const int q = sOrder[lo];
-        const int src = tGlobal[q] + (e - tStart[q]);
-        const float2 sh = tShift[q];
+        const int src = tGlobal[lo] + (e - tStart[lo]);
+        const float2 sh = tShift[lo];
         const float4 pv = s.stagedPV[src];
         sPos[e] = f2(pv.x + sh.x, pv.y + sh.y);
         sVel[e] = f2(pv.z, pv.w);
         sMeta[e] = s.stagedMeta[src];
-        sTile[e] = static_cast<uint16_t>(q);
+        sTile[e] = static_cast<uint16_t>(lo);
     }
     __syncthreads();
-    // 3. pair law of every own cell against its 3x3 local tiles
-    const int ownN = sOwnTotal;
-    for (int e = threadIdx.x; e < ownN; e += kRegionThreads) {
+    // 3. pair law of every own cell against the three runs of its window
+    const int ownN = rowOwn[ownH];
+    uint16_t* myHits = sHits + threadIdx.x;
+    for (int o = threadIdx.x; o < ownN; o += kRegionThreads) {
+        int r = 1;
+        while (rowOwn[r] <= o) ++r;
+        const int e = tStart[r * LW + 1] + (o - rowOwn[r - 1]);
         const int q = sTile[e];
         const int lx = q % LW, ly = q / LW;
         const float2 pi = sPos[e];
+        auto scan = [&](auto& law, auto diff) {
+            law.begin(s, wi, sMeta[e], pi, sVel[e]);
+            int nh = 0;
+            auto flush = [&]() {
+                for (int i = 0; i < nh; ++i) {
+                    const int m = myHits[i * kRegionThreads];
+                    law.visit(sMeta[m], sVel[m], diff(m));
+                }
+                nh = 0;
+            };
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int q0 = (ly + dy) * LW + lx - 1;
+                const int b0 = tStart[q0], b1 = tStart[q0 + 3];
+                for (int m = b0; m < b1; ++m) {
+                    if (law.near(diff(m))) {
+                        myHits[nh * kRegionThreads] = static_cast<uint16_t>(m);
+                        if (++nh == kHitCap) flush();
+                    }
+                }
+            }
+            flush();
+            law.end();
+        };
         if (Motion == ALIEN_B200_MOTION_FLUID) {
             FluidLaw law;
-            law.begin(s, wi, sMeta[e], pi, sVel[e]);
-#pragma unroll 1
-            for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll 1
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int q2 = (ly + dy) * LW + (lx + dx);
-                    const int b0 = tStart[q2], b1 = b0 + tCount[q2];
-                    for (int m = b0; m < b1; ++m) {
-                        const float2 pd = pi - sPos[m];
-                        if (law.near(pd)) law.visit(sMeta[m], sVel[m], pd);
-                    }
-                }
-            law.end();
+            scan(law, [&](int m) { return pi - sPos[m]; });
         } else {
             CollisionLaw law;
-            law.begin(s, wi, sMeta[e], pi, sVel[e]);
-#pragma unroll 1
-            for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll 1
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int q2 = (ly + dy) * LW + (lx + dx);
-                    const float2 sh = tShift[q2];
-                    if (sh.x != 0.0f || sh.y != 0.0f) continue;  // across the seam: uncorrected distance > R
-                    const int b0 = tStart[q2], b1 = b0 + tCount[q2];
-                    for (int m = b0; m < b1; ++m) {
-                        const float2 raw = sPos[m] - pi;
-                        if (law.near(raw)) law.visit(sMeta[m], sVel[m], raw);
-                    }
-                }
-            law.end();
+            scan(law, [&](int m) { return sPos[m] - pi; });
         }
     }
 }
