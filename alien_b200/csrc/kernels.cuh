@@ -568,17 +568,23 @@ __device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
 // copies the staged records of the region and of its one-tile halo from the
 // tile-sorted arrays into shared memory, all (regW+2) x (regH+2) local tiles
 // in row-major order (each tile a contiguous run in storage order), so that
-// the three tiles of one row of a cell's 3x3 window are one contiguous run.
+// the tiles of one row of a cell's window are one contiguous run.  A local
+// row is at most three contiguous global runs (left halo tile, own tiles,
+// right halo tile), so the copy finds its source with a search over rows.
 // Fluid worlds shift halo tiles that lie across the torus seam by +-W / +-H,
 // so that plain differences are the minimal-image displacements; collision
 // worlds keep stored positions (the reference's distance test is on the
 // uncorrected difference, so candidates across the seam never pass).
-// Every cell then scans its three runs with the cheap distance reject only,
-// appending survivors to a per-thread hit list in shared memory, and runs the
-// pair law on the hits afterwards: the scan loop stays convergent across the
-// warp, and the law runs once per hit instead of once per scan iteration in
-// which any lane of the warp had a hit.  Hits are visited in scan order (row
-// by row, tile by tile, storage order), so the FP32 sums do not change.
+// Every cell scans only the tiles of its 3x3 window that the disc of radius
+// R around it reaches (a neighbour tile is skipped when the cell is farther
+// than R, plus a rounding margin, from the shared edge: such tiles hold no
+// candidate within R), appending candidates that pass the cheap distance
+// reject to a per-thread hit list in shared memory, and runs the pair law on
+// the hits afterwards: the scan loop stays convergent across the warp, and
+// the law runs once per hit instead of once per scan iteration in which any
+// lane had a hit.  Hits are visited in scan order (row by row, tile by tile,
+// storage order), the order of the full 3x3 scan minus candidates that the
+// law ignores, so the FP32 sums do not depend on the pruning.
 // Regions whose records exceed the shared buffer, and worlds too small for
 // regions, use pairsGlobal for their cells.
 constexpr int kRegionThreads = 256;
@@ -586,7 +592,7 @@ constexpr int kRegionMaxW = 32, kRegionMaxH = 16;
 constexpr int kRegionMaxTiles = (kRegionMaxW + 2) * (kRegionMaxH + 2);
 constexpr int kRegionCap = 2304;  // staged records per CTA (halo included)
 constexpr int kHitCap = 24;       // hit-list entries per thread before a flush
-constexpr size_t kRegionDynSmem = static_cast<size_t>(kRegionCap) * (sizeof(int4) + 2 * sizeof(float2) + sizeof(uint16_t))
+constexpr size_t kRegionDynSmem = static_cast<size_t>(kRegionCap) * (sizeof(int4) + 2 * sizeof(float2))
                                   + static_cast<size_t>(kHitCap) * kRegionThreads * sizeof(uint16_t);
 
 template <int Motion>
@@ -596,8 +602,7 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
     int4* sMeta = dyn;
     float2* sPos = reinterpret_cast<float2*>(sMeta + kRegionCap);
     float2* sVel = sPos + kRegionCap;
-    uint16_t* sTile = reinterpret_cast<uint16_t*>(sVel + kRegionCap);
-    uint16_t* sHits = sTile + kRegionCap;      // [kHitCap][kRegionThreads]
+    uint16_t* sHits = reinterpret_cast<uint16_t*>(sVel + kRegionCap);  // [kHitCap][kRegionThreads]
     __shared__ int tStart[kRegionMaxTiles + 1];  // shared-memory offset of each local tile
     __shared__ int tGlobal[kRegionMaxTiles];     // first sorted index of the tile
     __shared__ float2 tShift[kRegionMaxTiles];
@@ -683,38 +688,48 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
             }
         return;
     }
-    // 2. copy: every thread one record per round; its local tile is the last
-    //    one that starts at or before the record
+    // 2. copy: a record's local row by binary search over the row starts,
+    //    then one of the row's three global runs
     for (int e = threadIdx.x; e < total; e += kRegionThreads) {
-        int lo = 0, hi = NT - 1;
+        int lo = 0, hi = LH - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (tStart[mid] <= e)
+            if (tStart[mid * LW] <= e)
                 lo = mid;
             else
                 hi = mid - 1;
         }
-        const int src = tGlobal[lo] + (e - tStart[lo]);
-        const float2 sh = tShift[lo];
+        const int b = lo * LW;
+        const int q = e < tStart[b + 1] ? b : (e < tStart[b + LW - 1] ? b + 1 : b + LW - 1);
+        const int src = tGlobal[q] + (e - tStart[q]);
+        const float2 sh = tShift[q];
         const float4 pv = s.stagedPV[src];
         sPos[e] = f2(pv.x + sh.x, pv.y + sh.y);
         sVel[e] = f2(pv.z, pv.w);
         sMeta[e] = s.stagedMeta[src];
-        sTile[e] = static_cast<uint16_t>(lo);
     }
     __syncthreads();
-    // 3. pair law of every own cell against the three runs of its window
+    // 3. pair law of every own cell against the tiles its disc reaches
     const int ownN = rowOwn[ownH];
     uint16_t* myHits = sHits + threadIdx.x;
+    const float T = static_cast<float>(wi.T);
     for (int o = threadIdx.x; o < ownN; o += kRegionThreads) {
-        int r = 1;
-        while (rowOwn[r] <= o) ++r;
-        const int e = tStart[r * LW + 1] + (o - rowOwn[r - 1]);
-        const int q = sTile[e];
-        const int lx = q % LW, ly = q / LW;
+        int ly = 1;
+        while (rowOwn[ly] <= o) ++ly;
+        const int e = tStart[ly * LW + 1] + (o - rowOwn[ly - 1]);
         const float2 pi = sPos[e];
+        // own tile column as binned (own tiles are not shifted)
+        const int gx = slotX(pi.x, wi.W) / wi.T;
+        const int lx = min(max(gx - tx0 + 1, 1), ownW);
+        const int gy = ty0 + ly - 1;
         auto scan = [&](auto& law, auto diff) {
             law.begin(s, wi, sMeta[e], pi, sVel[e]);
+            // reach: R plus a margin above the rounding of positions up to the world size
+            const float reach = law.R * 1.0001f + 1e-3f + 4.0f * static_cast<float>(max(wi.W, wi.H)) * 1.2e-7f;
+            const float left = static_cast<float>(gx) * T, right = fminf(static_cast<float>(gx + 1) * T, static_cast<float>(wi.W));
+            const float bottom = static_cast<float>(gy) * T, top = fminf(static_cast<float>(gy + 1) * T, static_cast<float>(wi.H));
+            const int c0 = lx - (pi.x - reach < left ? 1 : 0), c1 = lx + (pi.x + reach >= right ? 1 : 0);
+            const int r0 = ly - (pi.y - reach < bottom ? 1 : 0), r1 = ly + (pi.y + reach >= top ? 1 : 0);
             int nh = 0;
             auto flush = [&]() {
                 for (int i = 0; i < nh; ++i) {
@@ -724,9 +739,8 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
                 nh = 0;
             };
 #pragma unroll 1
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int q0 = (ly + dy) * LW + lx - 1;
-                const int b0 = tStart[q0], b1 = tStart[q0 + 3];
+            for (int r = r0; r <= r1; ++r) {
+                const int b0 = tStart[r * LW + c0], b1 = tStart[r * LW + c1 + 1];
                 for (int m = b0; m < b1; ++m) {
                     if (law.near(diff(m))) {
                         myHits[nh * kRegionThreads] = static_cast<uint16_t>(m);
@@ -751,59 +765,115 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
 // CellProcessor::calcConnectionForces, CellProcessor.cuh:408-491: spring
 // forces in bond order; angle forces (every third step) are scattered to
 // the two partners as fixed-point integers into angleAcc[4*j + accOffset].
-__device__ __forceinline__ float2 bondForce(const DevState& s, long long g, const float2* P, bool considerAngles,
-                                            int W, int H, float minDist, int accOffset)
+// The bond row of a cell and its partners' positions and stiffnesses are
+// gathered first (all loads of a cell in flight together), then the forces
+// are summed in bond order.
+struct BondRow {
+    int n;
+    int j[kMaxBonds];
+    float2 disp[kMaxBonds];  // corrected partner - cell
+};
+
+__device__ __forceinline__ void loadBondRow(const DevState& s, long long g, const float2* __restrict__ P, int W, int H,
+                                            BondRow& r)
+{
+    r.n = s.numConn[g];
+    const int2* row = reinterpret_cast<const int2*>(s.bond + g * kMaxBonds);
+    const float2 pi = P[g];
+#pragma unroll
+    for (int h = 0; h < kMaxBonds / 2; ++h) {
+        const int2 jj = 2 * h < r.n ? row[h] : make_int2(0, 0);
+        r.j[2 * h] = jj.x;
+        r.j[2 * h + 1] = jj.y;
+    }
+    float2 pj[kMaxBonds];
+#pragma unroll
+    for (int k = 0; k < kMaxBonds; ++k) pj[k] = k < r.n ? P[r.j[k]] : pi;
+#pragma unroll
+    for (int k = 0; k < kMaxBonds; ++k) r.disp[k] = correctDirection(pj[k] - pi, W, H);
+}
+
+__device__ __forceinline__ float2 bondForce(const DevState& s, long long g, const BondRow& r, bool considerAngles,
+                                            float minDist, int accOffset)
 {
     float2 F = f2(0.0f, 0.0f);
-    const int n = s.numConn[g];
+    const int n = r.n;
     if (n == 0 || s.barrier[g]) return F;
     const long long bb = g * kMaxBonds;
-    const float2 pi = P[g];
-    float2 prevDisp = correctDirection(P[s.bond[bb + n - 1]] - pi, W, H);
     const float si = s.stiffness[g];
     const float s2 = si * si;
-    for (int k = 0; k < n; ++k) {
-        const int j = s.bond[bb + k];
-        const float sj = s.stiffness[j];
-        const float sj2 = sj * sj;
-        const float2 disp = correctDirection(P[j] - pi, W, H);
-        const float dist = len2(disp);
-        const float dev = dist - s.bondDist[bb + k];
-        F = F + normalized2(disp) * dev * (s2 + sj2) / 6.0f;
-        if (considerAngles && (n > 2 || (n == 2 && k == 0))) {
-            const int last = (k + n - 1) % n;
-            const int jl = s.bond[bb + last];
-            const int nj = s.numConn[j];
-            bool tri = false;
-            for (int m = 0; m < nj; ++m) tri |= (s.bond[static_cast<long long>(j) * kMaxBonds + m] == jl);
-            if (!tri) {
-                const float a = angleOfVector(disp), pa = angleOfVector(prevDisp);
-                const float act = subtractAngle(a, pa);
-                if (act < 0.0f) continue;
-                const float ref = s.bondAngle[bb + k];
-                const float strength = fabsf(ref - act) / 2000.0f * s2;
-                float2 f1 = rotCW(normalized2(disp) / fmaxf(len2(disp), minDist) * strength);
-                float2 f2v = rotCCW(normalized2(prevDisp) / fmaxf(len2(prevDisp), minDist) * strength);
-                if (ref < act) {
-                    f1 = f1 * -1.0f;
-                    f2v = f2v * -1.0f;
-                }
-                if (!s.barrier[j]) {
-                    atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * j + accOffset]),
-                              static_cast<unsigned long long>(toFix(f1.x)));
-                    atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * j + accOffset + 1]),
-                              static_cast<unsigned long long>(toFix(f1.y)));
-                }
-                if (!s.barrier[jl]) {
-                    atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * jl + accOffset]),
-                              static_cast<unsigned long long>(toFix(f2v.x)));
-                    atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * jl + accOffset + 1]),
-                              static_cast<unsigned long long>(toFix(f2v.y)));
-                }
-                F = F - (f1 + f2v);
+    float sj[kMaxBonds], bd[kMaxBonds];
+    const float2* bdRow = reinterpret_cast<const float2*>(s.bondDist + bb);
+#pragma unroll
+    for (int h = 0; h < kMaxBonds / 2; ++h) {
+        const float2 d = 2 * h < n ? bdRow[h] : f2(0.0f, 0.0f);
+        bd[2 * h] = d.x;
+        bd[2 * h + 1] = d.y;
+    }
+#pragma unroll
+    for (int k = 0; k < kMaxBonds; ++k) sj[k] = k < n ? s.stiffness[r.j[k]] : 0.0f;
+#pragma unroll
+    for (int k = 0; k < kMaxBonds; ++k) {
+        if (k < n) {
+            const float2 disp = r.disp[k];
+            const float dev = len2(disp) - bd[k];
+            F = F + normalized2(disp) * dev * (s2 + sj[k] * sj[k]) / 6.0f;
+        }
+    }
+    if (!considerAngles || n < 2) return F;
+    // angle forces: partner rows for the triangle test, then the forces in bond order
+    int nj[kMaxBonds];
+#pragma unroll
+    for (int k = 0; k < kMaxBonds; ++k) nj[k] = k < n ? s.numConn[r.j[k]] : 0;
+#pragma unroll
+    for (int k = 0; k < kMaxBonds; ++k) {
+        if (k >= n || !(n > 2 || k == 0)) continue;
+        const int last = k == 0 ? n - 1 : k - 1;
+        int jl = r.j[0];
+        float2 prevDisp = r.disp[0];
+#pragma unroll
+        for (int m = 1; m < kMaxBonds; ++m)
+            if (m == last) {
+                jl = r.j[m];
+                prevDisp = r.disp[m];
+            }
+        const int j = r.j[k];
+        const int2* prow = reinterpret_cast<const int2*>(s.bond + static_cast<long long>(j) * kMaxBonds);
+        bool tri = false;
+#pragma unroll
+        for (int h = 0; h < kMaxBonds / 2; ++h) {
+            if (2 * h < nj[k]) {
+                const int2 pp = prow[h];
+                tri |= pp.x == jl;
+                tri |= (2 * h + 1 < nj[k]) && pp.y == jl;
             }
         }
-        prevDisp = disp;
+        if (tri) continue;
+        const float2 disp = r.disp[k];
+        const float a = angleOfVector(disp), pa = angleOfVector(prevDisp);
+        const float act = subtractAngle(a, pa);
+        if (act < 0.0f) continue;
+        const float ref = s.bondAngle[bb + k];
+        const float strength = fabsf(ref - act) / 2000.0f * s2;
+        float2 f1 = rotCW(normalized2(disp) / fmaxf(len2(disp), minDist) * strength);
+        float2 f2v = rotCCW(normalized2(prevDisp) / fmaxf(len2(prevDisp), minDist) * strength);
+        if (ref < act) {
+            f1 = f1 * -1.0f;
+            f2v = f2v * -1.0f;
+        }
+        if (!s.barrier[j]) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * j + accOffset]),
+                      static_cast<unsigned long long>(toFix(f1.x)));
+            atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * j + accOffset + 1]),
+                      static_cast<unsigned long long>(toFix(f1.y)));
+        }
+        if (!s.barrier[jl]) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * jl + accOffset]),
+                      static_cast<unsigned long long>(toFix(f2v.x)));
+            atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * jl + accOffset + 1]),
+                      static_cast<unsigned long long>(toFix(f2v.y)));
+        }
+        F = F - (f1 + f2v);
     }
     return F;
 }
@@ -832,7 +902,9 @@ __global__ void __launch_bounds__(kBlock) kApplyBond1(DevState s)
             if (len2(v) > p.cellMaxVelocity) v = normalized2(v) * p.cellMaxVelocity;
             s.velA[g] = v;
         }
-        s.force1[g] = bondForce(s, g, s.posB, T % 3 == 0, wi.W, wi.H, p.cellMinDistance, 0);
+        BondRow r;
+        loadBondRow(s, g, s.posB, wi.W, wi.H, r);
+        s.force1[g] = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 0);
     } else {
         PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
         if (!c.inRange || !s.palive[c.q]) return;
@@ -893,21 +965,22 @@ __global__ void __launch_bounds__(kBlock) kBond2(DevState s)
         const WorldInfo& wi = s.worlds[c.w];
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
         const uint64_t T = s.counters[c.w].timestep;
+        BondRow r;
+        loadBondRow(s, g, s.posA, wi.W, wi.H, r);
         if (!s.barrier[g]) {
-            const int n = s.numConn[g];
             const float maxDist = p.cellMaxBindingDistance[s.color[g] % ALIEN_B200_MAX_COLORS];
-            const float2 pi = s.posA[g];
             bool destroy = false;
-            for (int k = 0; k < n; ++k) {
-                const int j = s.bond[g * kMaxBonds + k];
-                if (len2(correctDirection(s.posA[j] - pi, wi.W, wi.H)) > maxDist) destroy = true;
-            }
+#pragma unroll
+            for (int k = 0; k < kMaxBonds; ++k)
+                if (k < r.n && len2(r.disp[k]) > maxDist) destroy = true;
             if (destroy) {
                 atomicOr(&s.flags[g], kFlagDelAll);
-                for (int k = 0; k < n; ++k) atomicOr(&s.flags[s.bond[g * kMaxBonds + k]], kFlagDetach);
+#pragma unroll
+                for (int k = 0; k < kMaxBonds; ++k)
+                    if (k < r.n) atomicOr(&s.flags[r.j[k]], kFlagDetach);
             }
         }
-        s.force[g] = bondForce(s, g, s.posA, T % 3 == 0, wi.W, wi.H, p.cellMinDistance, 2);
+        s.force[g] = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 2);
     } else {
         PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
         if (!c.inRange || !s.palive[c.q]) return;
