@@ -69,7 +69,7 @@ EXPORTED_SYMBOLS = [
     "alien_b200_batch_get_array_sizes", "alien_b200_batch_get_raw_statistics", "alien_b200_batch_stream",
     "alien_b200_batch_kernel_launch_count", "alien_b200_batch_kernels_per_step", "alien_b200_batch_timed_timesteps",
     "alien_b200_batch_set_step_budget", "alien_b200_batch_world_status", "alien_b200_batch_num_active",
-    "alien_b200_batch_device_bytes", "alien_b200_statistics_no_alloc",
+    "alien_b200_batch_device_bytes", "alien_b200_statistics_no_alloc", "alien_b200_batch_synchronize",
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -126,6 +126,7 @@ def load() -> ctypes.CDLL:
     lib.alien_b200_batch_num_active.argtypes = [vp]
     lib.alien_b200_batch_device_bytes.argtypes = [vp]
     lib.alien_b200_batch_device_bytes.restype = u64
+    lib.alien_b200_batch_synchronize.argtypes = [vp]
     lib.alien_b200_statistics_no_alloc.argtypes = [vp, u64, vp, u64, u64, vp, vp]
     lib.alien_b200_select_device.argtypes = [i32]
     lib.alien_b200_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]

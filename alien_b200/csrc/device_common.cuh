@@ -335,10 +335,13 @@ __device__ __forceinline__ float sphKernelD(float q)
     return r * (3.0f / (2.0f * kPi));
 }
 
-// exclusive scan across a block of kBlock threads; *total = block sum
-__device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* total)
+// exclusive scan across a block of Threads threads (a multiple of 32);
+// *total = block sum
+template <int Threads>
+__device__ __forceinline__ uint32_t blockExclusiveScanN(uint32_t v, uint32_t* total)
 {
-    __shared__ uint32_t warpSums[kBlock / 32];
+    static_assert(Threads % 32 == 0 && Threads <= 1024, "block size");
+    __shared__ uint32_t warpSums[Threads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t x = v;
 #pragma unroll
@@ -349,20 +352,26 @@ __device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* tot
     if (lane == 31) warpSums[warp] = x;
     __syncthreads();
     if (warp == 0) {
-        uint32_t ws = lane < kBlock / 32 ? warpSums[lane] : 0;
+        uint32_t ws = lane < Threads / 32 ? warpSums[lane] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             uint32_t y = __shfl_up_sync(0xffffffffu, ws, o);
             if (lane >= o) ws += y;
         }
-        if (lane < kBlock / 32) warpSums[lane] = ws;
+        if (lane < Threads / 32) warpSums[lane] = ws;
     }
     __syncthreads();
     uint32_t warpOffset = warp > 0 ? warpSums[warp - 1] : 0;
-    if (total) *total = warpSums[kBlock / 32 - 1];
+    if (total) *total = warpSums[Threads / 32 - 1];
     uint32_t r = warpOffset + x - v;
     __syncthreads();
     return r;
+}
+
+// exclusive scan across a block of kBlock threads; *total = block sum
+__device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* total)
+{
+    return blockExclusiveScanN<kBlock>(v, total);
 }
 
 __device__ __forceinline__ void setError(const DevState& s, uint32_t bit) { atomicOr(s.errorFlags, bit); }

@@ -1209,6 +1209,15 @@ int alien_b200_batch_enqueue_timesteps(alien_b200_batch* b, uint64_t timesteps)
     });
 }
 
+int alien_b200_batch_synchronize(alien_b200_batch* b)
+{
+    return guarded([&] {
+        if (!b) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
+        b->arena->sync();
+        b->arena->ensureParticleCapacity();
+    });
+}
+
 int alien_b200_batch_get_data(alien_b200_batch* b, int world, const AlienDataTO* data)
 {
     return guarded([&] {

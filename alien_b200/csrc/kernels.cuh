@@ -592,11 +592,12 @@ constexpr int kRegionMaxW = 32, kRegionMaxH = 16;
 constexpr int kRegionMaxTiles = (kRegionMaxW + 2) * (kRegionMaxH + 2);
 constexpr int kRegionCap = 2304;  // staged records per CTA (halo included)
 constexpr int kHitCap = 24;       // hit-list entries per thread before a flush
+constexpr int kRegionMinBlocks = 2;
 constexpr size_t kRegionDynSmem = static_cast<size_t>(kRegionCap) * (sizeof(int4) + 2 * sizeof(float2))
                                   + static_cast<size_t>(kHitCap) * kRegionThreads * sizeof(uint16_t);
 
 template <int Motion>
-__global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
+__global__ void __launch_bounds__(kRegionThreads, kRegionMinBlocks) kPairsRegion(DevState s)
 {
     extern __shared__ int4 dyn[];
     int4* sMeta = dyn;
@@ -662,7 +663,7 @@ __global__ void __launch_bounds__(kRegionThreads, 2) kPairsRegion(DevState s)
             cnt += n;
         }
         uint32_t total;
-        uint32_t off = blockExclusiveScan(cnt, &total);
+        uint32_t off = blockExclusiveScanN<kRegionThreads>(cnt, &total);
         for (int lt = c0; lt < c1; ++lt) {
             const int n = tStart[lt];
             tStart[lt] = static_cast<int>(off);

@@ -169,6 +169,10 @@ class BatchSimulation:
     def enqueue_timesteps(self, timesteps: int) -> None:
         check(self._lib.alien_b200_batch_enqueue_timesteps(self._h, int(timesteps)))
 
+    def synchronize(self) -> None:
+        """wait for enqueued steps; grow particle storage if needed"""
+        check(self._lib.alien_b200_batch_synchronize(self._h))
+
     def time_timesteps(self, timesteps: int) -> float:
         ms = ctypes.c_double()
         check(self._lib.alien_b200_batch_time_timesteps(self._h, int(timesteps), ctypes.byref(ms)))

@@ -11,9 +11,10 @@ together:
 * cohorts: each admission wave becomes one batch arena (alien_b200_batch)
   whose worlds carry per-world step budgets, so a world stops exactly after
   its requested steps without host synchronisation;
-* a tick = one timestep of every cohort with active worlds, issued back to
-  back on the GPU; its duration is the per-step latency every running request
-  sees (p50 / p99 reported);
+* a tick = a few timesteps (``steps_per_tick``) of every cohort with active
+  worlds, each cohort on its own CUDA stream so that their kernels overlap on
+  the device; the tick's wall time per step is the per-step latency every
+  running request sees (p50 / p99 reported);
 * a cohort whose worlds are all done is read back (results) and freed, which
   returns its bytes to the budget.
 
@@ -84,7 +85,11 @@ class _Cohort:
 
 
 class ServingLoop:
-    def __init__(self, hbm_budget_bytes: int, keep_results: bool = False, max_cohort_worlds: int = 256):
+    def __init__(self, hbm_budget_bytes: int, keep_results: bool = False, max_cohort_worlds: int = 256,
+                 steps_per_tick: int = 4):
+        if not 1 <= steps_per_tick <= 64:
+            raise ValueError("steps_per_tick must be in [1, 64]")
+        self.steps_per_tick = int(steps_per_tick)
         self.budget = int(hbm_budget_bytes)
         self.keep_results = keep_results
         self.max_cohort_worlds = max_cohort_worlds
@@ -119,16 +124,23 @@ class ServingLoop:
             self.cohorts.append(_Cohort(wave))
 
     def tick(self, now: float) -> float:
-        """admit, then one timestep of every running cohort; returns ms"""
+        """admit, then ``steps_per_tick`` timesteps of every running cohort,
+        each cohort on its own stream so that their kernels overlap; returns
+        the per-step latency in ms (wall time of the tick / steps)"""
         self._admit(now)
         if not self.cohorts:
             return 0.0
-        ms = 0.0
+        k = self.steps_per_tick
+        t0 = time.perf_counter()
         for c in self.cohorts:
-            ms += c.batch.time_timesteps(1)
-            live = sum(r.cells for r in c.requests if c.steps_done < r.steps)
-            self.cell_steps += live
-            c.steps_done += 1
+            c.batch.enqueue_timesteps(k)
+        for c in self.cohorts:
+            c.batch.synchronize()
+        ms = (time.perf_counter() - t0) * 1000.0 / k
+        for c in self.cohorts:
+            for r in c.requests:
+                self.cell_steps += r.cells * max(0, min(k, r.steps - c.steps_done))
+            c.steps_done += k
         self.tick_ms.append(ms)
         done_now = time.perf_counter()
         keep = []
@@ -158,11 +170,12 @@ class ServingLoop:
 
 
 def run_poisson(make_request: Callable[[int, np.random.Generator], Request], rate_per_s: float, duration_s: float,
-                hbm_budget_bytes: int, seed: int = 0, keep_results: bool = False, drain: bool = True) -> dict:
+                hbm_budget_bytes: int, seed: int = 0, keep_results: bool = False, drain: bool = True,
+                steps_per_tick: int = 4) -> dict:
     """Poisson arrivals at ``rate_per_s`` for ``duration_s`` seconds of wall
     time; requests are built by ``make_request(rid, rng)``."""
     rng = np.random.default_rng(seed)
-    loop = ServingLoop(hbm_budget_bytes, keep_results)
+    loop = ServingLoop(hbm_budget_bytes, keep_results, steps_per_tick=steps_per_tick)
     t0 = time.perf_counter()
     next_arrival = rng.exponential(1.0 / rate_per_s)
     rid = 0

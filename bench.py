@@ -320,13 +320,50 @@ def run_batched(args, rank, world_size):
             "plain_value": plain_value, "plain_ms_per_step": t_plain / plain_steps}
 
 
+def run_serving(args, rank):
+    """Poisson arrivals of simulation requests (worlds of log-uniform
+    5k-500k cells built as the batched worlds, log-uniform 100-5000 steps)
+    admitted against an HBM budget and stepped together by the continuous-
+    batching loop (alien_b200.serving).  The request worlds come from a pool
+    built before the run, so world generation on the host stays out of the
+    measured loop."""
+    import numpy as np
+    from alien_b200 import params as P
+    from alien_b200 import serving, worldgen
+
+    rng = np.random.default_rng(1000 + rank)
+    sizes = np.exp(rng.uniform(math.log(5_000), math.log(500_000), args.pool)).astype(int)
+    pool = []
+    for i, n in enumerate(sizes):
+        pool.append(worldgen.mixed_world(seed=100_000 * rank + i, num_cells=int(n)))
+    log(f"serving: pool of {len(pool)} worlds, {sum(d.num_cells for d, _ in pool)} cells")
+    prm = P.benchmark_parameters(P.MOTION_FLUID)
+
+    def make(rid, r):
+        d, w = pool[int(r.integers(len(pool)))]
+        steps = int(math.exp(r.uniform(math.log(100), math.log(5000))))
+        return serving.Request(rid, d, w, prm, steps)
+
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        out = serving.run_poisson(make, rate_per_s=args.rate, duration_s=args.duration,
+                                  hbm_budget_bytes=int(args.hbm_budget_gb * 1e9), seed=rank, drain=False,
+                                  steps_per_tick=4)
+    out["clocks"] = clk.summary()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="hex4m", choices=["hex4m", "hex1m", "fluid1m", "softbody", "batched256"])
+    ap.add_argument("--config", default="hex4m",
+                    choices=["hex4m", "hex1m", "fluid1m", "softbody", "batched256", "serving"])
+    ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
+    ap.add_argument("--rate", type=float, default=20.0, help="serving: mean requests per second")
+    ap.add_argument("--pool", type=int, default=32, help="serving: distinct request worlds")
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0, help="serving: admission budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -370,6 +407,27 @@ def main():
         return float(t.item())
 
     peak, peak_kind = load_peak()
+    if args.config == "serving":
+        r = run_serving(args, rank)
+        agg = sum_over_ranks(r["cell_steps"]) / max_over_ranks(r["wall_s"]) / 1e6
+        if rank == 0:
+            line = {
+                "metric": METRIC, "value": agg, "unit": METRIC, "n_gpus": world_size, "steps": r["ticks"],
+                "warmup": 0, "ms_per_step": r["p50_step_ms"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "serving", "rate_per_s": args.rate, "duration_s": args.duration,
+                           "hbm_budget_gb": args.hbm_budget_gb, "pool_worlds": args.pool,
+                           "description": "Poisson arrivals, worlds of log-uniform 5k-500k cells (half fluid, half "
+                                          "10x10 lattices), log-uniform 100-5000 steps, continuous batching"},
+                "p50_step_ms": r["p50_step_ms"], "p99_step_ms": r["p99_step_ms"],
+                "requests": {"submitted": r["requests_submitted"], "finished": r["requests_finished"],
+                             "waiting": r["requests_waiting"]},
+                "wall_s": r["wall_s"], "clocks": r["clocks"],
+            }
+            print(json.dumps(line))
+        if world_size > 1:
+            dist.destroy_process_group()
+        return 0
     if args.config == "batched256":
         r = run_batched(args, rank, world_size)
         ms = max_over_ranks(r["ms"])

@@ -28,6 +28,10 @@ int alien_b200_batch_num_worlds(alien_b200_batch* batch);
 int alien_b200_batch_calc_timesteps(alien_b200_batch* batch, uint64_t timesteps);
 /* enqueues the steps on the batch's stream without synchronising */
 int alien_b200_batch_enqueue_timesteps(alien_b200_batch* batch, uint64_t timesteps);
+/* waits for the enqueued steps, then grows particle storage where a world
+ * has filled half of it (calc_timesteps does this every 64 steps); call it
+ * at least every 64 enqueued steps */
+int alien_b200_batch_synchronize(alien_b200_batch* batch);
 int alien_b200_batch_get_data(alien_b200_batch* batch, int world, const AlienDataTO* data);
 int alien_b200_batch_get_array_sizes(alien_b200_batch* batch, int world, AlienArraySizes* sizes);
 int alien_b200_batch_get_raw_statistics(alien_b200_batch* batch, int world, AlienRawStatistics* statistics);
