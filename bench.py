@@ -376,35 +376,14 @@ def main():
         return run_reference(args, args.config, rank, world_size)
 
     import torch
-    import torch.distributed as dist
 
-    torch.cuda.set_device(local_rank)
-    if world_size > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from alien_b200 import _lib
     from alien_b200.facade import SimulationFacade
+    from alien_b200.replicas import Replicas
 
+    reps = Replicas()
     _lib.select_device(local_rank)
-
-    def barrier():
-        torch.cuda.synchronize()
-        if world_size > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world_size == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x: float) -> float:
-        if world_size == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    barrier, max_over_ranks, sum_over_ranks = reps.barrier, reps.max, reps.sum
 
     peak, peak_kind = load_peak()
     if args.config == "serving":
@@ -425,8 +404,7 @@ def main():
                 "wall_s": r["wall_s"], "clocks": r["clocks"],
             }
             print(json.dumps(line))
-        if world_size > 1:
-            dist.destroy_process_group()
+        reps.close()
         return 0
     if args.config == "batched256":
         r = run_batched(args, rank, world_size)
@@ -445,8 +423,7 @@ def main():
                 "clocks": r["clocks"], "gpu_launches": r["launches"],
             }
             print(json.dumps(line))
-        if world_size > 1:
-            dist.destroy_process_group()
+        reps.close()
         return 0
 
     log(f"building workload {args.config}")
@@ -544,8 +521,7 @@ def main():
         }
         print(json.dumps(line))
     sim.close_simulation()
-    if world_size > 1:
-        dist.destroy_process_group()
+    reps.close()
     return 0
 
 
