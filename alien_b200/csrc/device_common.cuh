@@ -83,6 +83,9 @@ struct WorldCounters {
     unsigned long long stepsRemaining;
     unsigned int active;
     unsigned int pad2;
+    // events counted this step (radiation, deleted cells, particle splits):
+    // the event scans run only when there are any
+    unsigned int evRad, evDel, evSplit, pad3;
 };
 
 struct DevState {

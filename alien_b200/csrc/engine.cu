@@ -209,6 +209,7 @@ private:
     long long maxWorldCells_ = 0, maxWorldParts_ = 0;
     uint64_t launches_ = 0;
     int kernelsPerStep_ = 0;
+    int partGrid_ = 1;  // blocks of the particle part of a combined launch
     cudaGraphExec_t graphExec_ = nullptr;
     uint64_t stepsSinceCheck_ = 0;
     bool hasFluid_ = false, hasCollision_ = false;
@@ -303,6 +304,14 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     s.numWorlds = n;
     s.numCellBlocks = cellBlocks;
     s.numPartBlocks = partBlocks;
+    {
+        // particle parts of the combined launches stride over the used
+        // particle blocks with at most 16 blocks per SM
+        int device = 0, sms = 0;
+        AB_CK(cudaGetDevice(&device));
+        AB_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        partGrid_ = std::max(1, std::min(partBlocks, 16 * std::max(sms, 1)));
+    }
     s.cellSlots = cellSlots;
     s.partSlots = partSlots;
     s.numTiles = tiles;
@@ -473,7 +482,7 @@ void Arena::scan(const uint32_t* in, long long n, uint32_t* out)
 void Arena::enqueueStep()
 {
     const DevState& s = s_;
-    const int cells = s.numCellBlocks, both = s.numCellBlocks + s.numPartBlocks;
+    const int cells = s.numCellBlocks, both = s.numCellBlocks + partGrid_;
     const uint64_t before = launches_;
     AB_CK(cudaMemsetAsync(s.tileCount, 0, sizeof(uint32_t) * static_cast<size_t>(s.numTiles), stream_));
     launch(kBin, both, kBlock, s);

@@ -66,6 +66,36 @@ __device__ __forceinline__ PartCtx partCtx(const DevState& s, int pb)
     return c;
 }
 
+// The particle part of a combined launch: the grid's blocks past the cell
+// blocks stride over the particle blocks, skipping inactive worlds and the
+// blocks past a world's used slots (partBase + usedSlots(counters)), so its
+// cost follows the live particles rather than the capacity.  Everything f
+// sees is block-uniform, so f may synchronise the block; f's return ends one
+// particle block for the calling thread.
+template <class UsedSlots, class F>
+__device__ __forceinline__ void forParticleBlocks(const DevState& s, UsedSlots usedSlots, F f)
+{
+    const int stride = gridDim.x - s.numCellBlocks;
+    for (int pb = blockIdx.x - s.numCellBlocks; pb < s.numPartBlocks; pb += stride) {
+        const int w = s.partBlockWorld[pb];
+        const WorldInfo& wi = s.worlds[w];
+        const WorldCounters& wc = s.counters[w];
+        const long long end = wi.partBase + static_cast<long long>(usedSlots(wc));
+        if (!wc.active || static_cast<long long>(pb) * kBlock >= end) {
+            // on to the first block of the next world in this block's stride
+            const int next = wi.firstPartBlock + wi.numPartBlocks;
+            pb += ((next - pb + stride - 1) / stride - 1) * stride;
+            continue;
+        }
+        PartCtx c;
+        c.w = w;
+        c.q = static_cast<long long>(pb) * kBlock + threadIdx.x;
+        c.inRange = c.q < end;
+        f(c, pb);
+    }
+}
+__device__ __forceinline__ unsigned int usedParticles(const WorldCounters& wc) { return wc.numParticles; }
+
 // bonds[] holds kMaxBonds entries, unused ones -1: a fixed-trip compare
 // keeps the list in registers
 __device__ __forceinline__ bool isBondedTo(const int* bonds, int j)
@@ -161,20 +191,21 @@ __global__ void __launch_bounds__(kBlock) kBin(DevState s)
             }
         }
     } else {
-        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
-        const long long q = c.q;
-        s.pflag[q] = 0;
-        s.ptarget[q] = -1;
-        s.pslot[q] = -1;
-        s.pmerge[3 * q + 0] = 0;
-        s.pmerge[3 * q + 1] = 0;
-        s.pmerge[3 * q + 2] = 0;
-        if (!c.inRange || !s.palive[q]) return;
-        const WorldInfo& wi = s.worlds[c.w];
-        float2 pp = s.ppos[q];
-        int slot = slotX(pp.x, wi.W) + slotX(pp.y, wi.H) * wi.W;
-        s.pslot[q] = slot;
-        atomicMax(&s.pmap[wi.pmapBase + slot], static_cast<int>(q));
+        forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
+            const long long q = c.q;
+            s.pflag[q] = 0;
+            s.ptarget[q] = -1;
+            s.pslot[q] = -1;
+            s.pmerge[3 * q + 0] = 0;
+            s.pmerge[3 * q + 1] = 0;
+            s.pmerge[3 * q + 2] = 0;
+            if (!c.inRange || !s.palive[q]) return;
+            const WorldInfo& wi = s.worlds[c.w];
+            float2 pp = s.ppos[q];
+            int slot = slotX(pp.x, wi.W) + slotX(pp.y, wi.H) * wi.W;
+            s.pslot[q] = slot;
+            atomicMax(&s.pmap[wi.pmapBase + slot], static_cast<int>(q));
+        });
     }
 }
 
@@ -907,11 +938,12 @@ __global__ void __launch_bounds__(kBlock) kApplyBond1(DevState s)
         loadBondRow(s, g, s.posB, wi.W, wi.H, r);
         s.force1[g] = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 0);
     } else {
-        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
-        if (!c.inRange || !s.palive[c.q]) return;
-        const WorldInfo& wi = s.worlds[c.w];
-        const AlienPhysicsParams& p = s.params[wi.paramIndex];
-        s.ppos[c.q] = correctPosition(s.ppos[c.q] + s.pvel[c.q] * p.timestepSize, wi.W, wi.H);
+        forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
+            if (!c.inRange || !s.palive[c.q]) return;
+            const WorldInfo& wi = s.worlds[c.w];
+            const AlienPhysicsParams& p = s.params[wi.paramIndex];
+            s.ppos[c.q] = correctPosition(s.ppos[c.q] + s.pvel[c.q] * p.timestepSize, wi.W, wi.H);
+        });
     }
 }
 
@@ -944,12 +976,13 @@ __global__ void __launch_bounds__(kBlock) kVerletPos(DevState s)
         }
         s.posA[g] = correctPosition(np, wi.W, wi.H);
     } else {
-        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
-        if (!c.inRange || !s.palive[c.q]) return;
-        const WorldInfo& wi = s.worlds[c.w];
-        const float2 pp = s.ppos[c.q];
-        const int o = s.pmap[wi.pmapBase + slotX(pp.x, wi.W) + slotX(pp.y, wi.H) * wi.W];
-        if (o >= 0 && o != c.q && lensq2(pp - s.ppos[o]) < 0.5f) s.ptarget[c.q] = o;
+        forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
+            if (!c.inRange || !s.palive[c.q]) return;
+            const WorldInfo& wi = s.worlds[c.w];
+            const float2 pp = s.ppos[c.q];
+            const int o = s.pmap[wi.pmapBase + slotX(pp.x, wi.W) + slotX(pp.y, wi.H) * wi.W];
+            if (o >= 0 && o != c.q && lensq2(pp - s.ppos[o]) < 0.5f) s.ptarget[c.q] = o;
+        });
     }
 }
 
@@ -983,20 +1016,21 @@ __global__ void __launch_bounds__(kBlock) kBond2(DevState s)
         }
         s.force[g] = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 2);
     } else {
-        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
-        if (!c.inRange || !s.palive[c.q]) return;
-        const long long q = c.q;
-        const int o = s.ptarget[q];
-        if (o < 0 || s.ptarget[o] >= 0) return;
-        const float eq = s.penergy[q];
-        if (!(eq > kNearZero && s.penergy[o] > kNearZero)) return;
-        const float2 vq = s.pvel[q];
-        atomicOr(&s.pflag[o], 1u);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&s.pmerge[3LL * o + 0]), static_cast<unsigned long long>(toFix(eq)));
-        atomicAdd(reinterpret_cast<unsigned long long*>(&s.pmerge[3LL * o + 1]), static_cast<unsigned long long>(toFix(eq * vq.x)));
-        atomicAdd(reinterpret_cast<unsigned long long*>(&s.pmerge[3LL * o + 2]), static_cast<unsigned long long>(toFix(eq * vq.y)));
-        s.palive[q] = 0;
-        atomicAdd(&s.counters[c.w].deadParticles, 1u);
+        forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
+            if (!c.inRange || !s.palive[c.q]) return;
+            const long long q = c.q;
+            const int o = s.ptarget[q];
+            if (o < 0 || s.ptarget[o] >= 0) return;
+            const float eq = s.penergy[q];
+            if (!(eq > kNearZero && s.penergy[o] > kNearZero)) return;
+            const float2 vq = s.pvel[q];
+            atomicOr(&s.pflag[o], 1u);
+            atomicAdd(reinterpret_cast<unsigned long long*>(&s.pmerge[3LL * o + 0]), static_cast<unsigned long long>(toFix(eq)));
+            atomicAdd(reinterpret_cast<unsigned long long*>(&s.pmerge[3LL * o + 1]), static_cast<unsigned long long>(toFix(eq * vq.x)));
+            atomicAdd(reinterpret_cast<unsigned long long*>(&s.pmerge[3LL * o + 2]), static_cast<unsigned long long>(toFix(eq * vq.y)));
+            s.palive[q] = 0;
+            atomicAdd(&s.counters[c.w].deadParticles, 1u);
+        });
     }
 }
 
@@ -1046,51 +1080,52 @@ __global__ void __launch_bounds__(kBlock) kVerletVel(DevState s)
             if (s.livingState[g] == ALIEN_B200_LIVING_READY && s.activationTime[g] > 0) --s.activationTime[g];
         }
     } else {
-        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
-        if (!c.inRange || !s.palive[c.q]) return;
-        const long long q = c.q;
-        const WorldInfo& wi = s.worlds[c.w];
-        const AlienPhysicsParams& p = s.params[wi.paramIndex];
-        if (s.pflag[q] & 1u) {
-            const float eq = s.penergy[q];
-            const float e = eq + fromFix(s.pmerge[3 * q + 0]);
-            const float2 vq = s.pvel[q];
-            s.pvel[q] = f2((eq * vq.x + fromFix(s.pmerge[3 * q + 1])) / e, (eq * vq.y + fromFix(s.pmerge[3 * q + 2])) / e);
-            s.penergy[q] = e;
-            s.plast[q] = ~0ull;
-            return;
-        }
-        if (s.ptarget[q] >= 0) return;
-        const float2 pp = s.ppos[q], pv = s.pvel[q];
-        const int cell = slotHead(s, wi, pp + pv);
-        if (cell < 0) return;
-        if (s.barrier[cell]) {
-            const float2 vc = s.velA[cell];
-            const float2 vr = pv - vc;
-            const float2 r = correctDirection(pp - s.posB[cell], wi.W, wi.H);
-            const float dvr = dot2(vr, r);
-            if (dvr < 0.0f) {
-                const float trr = fmaxf(0.1f, lensq2(r));
-                s.pvel[q] = vr - r * 2.0f * dvr / trr + vc;
+        forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
+            if (!c.inRange || !s.palive[c.q]) return;
+            const long long q = c.q;
+            const WorldInfo& wi = s.worlds[c.w];
+            const AlienPhysicsParams& p = s.params[wi.paramIndex];
+            if (s.pflag[q] & 1u) {
+                const float eq = s.penergy[q];
+                const float e = eq + fromFix(s.pmerge[3 * q + 0]);
+                const float2 vq = s.pvel[q];
+                s.pvel[q] = f2((eq * vq.x + fromFix(s.pmerge[3 * q + 1])) / e, (eq * vq.y + fromFix(s.pmerge[3 * q + 2])) / e);
+                s.penergy[q] = e;
+                s.plast[q] = ~0ull;
+                return;
             }
-            return;
-        }
-        const unsigned long long cellId = s.id[cell];
-        if (s.plast[q] == cellId) return;
-        const float absorption = p.radiationAbsorption[s.color[cell] % ALIEN_B200_MAX_COLORS];
-        if (absorption < kNearZero) return;
-        float e = s.penergy[q];
-        float transfer = e * absorption;
-        if (e < 0.01f) transfer = e;
-        atomicAdd(reinterpret_cast<unsigned long long*>(&s.energyAcc[cell]), static_cast<unsigned long long>(toFix(transfer)));
-        e -= transfer;
-        s.penergy[q] = e;
-        if (e < kNearZero) {
-            s.palive[q] = 0;
-            atomicAdd(&s.counters[c.w].deadParticles, 1u);
-        } else {
-            s.plast[q] = cellId;
-        }
+            if (s.ptarget[q] >= 0) return;
+            const float2 pp = s.ppos[q], pv = s.pvel[q];
+            const int cell = slotHead(s, wi, pp + pv);
+            if (cell < 0) return;
+            if (s.barrier[cell]) {
+                const float2 vc = s.velA[cell];
+                const float2 vr = pv - vc;
+                const float2 r = correctDirection(pp - s.posB[cell], wi.W, wi.H);
+                const float dvr = dot2(vr, r);
+                if (dvr < 0.0f) {
+                    const float trr = fmaxf(0.1f, lensq2(r));
+                    s.pvel[q] = vr - r * 2.0f * dvr / trr + vc;
+                }
+                return;
+            }
+            const unsigned long long cellId = s.id[cell];
+            if (s.plast[q] == cellId) return;
+            const float absorption = p.radiationAbsorption[s.color[cell] % ALIEN_B200_MAX_COLORS];
+            if (absorption < kNearZero) return;
+            float e = s.penergy[q];
+            float transfer = e * absorption;
+            if (e < 0.01f) transfer = e;
+            atomicAdd(reinterpret_cast<unsigned long long*>(&s.energyAcc[cell]), static_cast<unsigned long long>(toFix(transfer)));
+            e -= transfer;
+            s.penergy[q] = e;
+            if (e < kNearZero) {
+                s.palive[q] = 0;
+                atomicAdd(&s.counters[c.w].deadParticles, 1u);
+            } else {
+                s.plast[q] = cellId;
+            }
+        });
     }
 }
 
@@ -1177,33 +1212,34 @@ __global__ void __launch_bounds__(kBlock) kTransition(DevState s)
         }
         if (f) atomicOr(&s.flags[g], f);
     } else {
-        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
-        if (!c.inRange) return;
-        const long long q = c.q;
-        const WorldInfo& wi = s.worlds[c.w];
-        if (s.pslot[q] >= 0) s.pmap[wi.pmapBase + s.pslot[q]] = -1;
-        if (!s.palive[q]) return;
-        const AlienPhysicsParams& p = s.params[wi.paramIndex];
-        const uint64_t T = s.counters[c.w].timestep;
-        const unsigned long long id = s.pid[q];
-        if (draw(id, T, kSiteSplit) >= 0.01f) return;
-        float e = s.penergy[q];
-        if (!(e > p.particleSplitEnergy[s.pcolor[q] % ALIEN_B200_MAX_COLORS])) return;
-        e *= 0.5f;
-        s.penergy[q] = e;
-        float2 vp = unitVectorOfAngle(draw(id, T, kSiteSplitAngle) * 360.0f);
-        const float2 pp = s.ppos[q];
-        const float2 otherPos = correctPosition(pp + vp / 5.0f, wi.W, wi.H);
-        s.ppos[q] = correctPosition(pp - vp / 5.0f, wi.W, wi.H);
-        vp = vp * (p.radiationVelocityPerturbation / (e + 1.0f));
-        const float2 pv = s.pvel[q];
-        s.pvel[q] = pv - vp;
-        if (e > kNearZero) {
-            s.splitPos[q] = otherPos;
-            s.splitVel[q] = pv + vp;
-            s.splitEnergy[q] = e;
-            s.pflag[q] |= 2u;
-        }
+        forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
+            if (!c.inRange) return;
+            const long long q = c.q;
+            const WorldInfo& wi = s.worlds[c.w];
+            if (s.pslot[q] >= 0) s.pmap[wi.pmapBase + s.pslot[q]] = -1;
+            if (!s.palive[q]) return;
+            const AlienPhysicsParams& p = s.params[wi.paramIndex];
+            const uint64_t T = s.counters[c.w].timestep;
+            const unsigned long long id = s.pid[q];
+            if (draw(id, T, kSiteSplit) >= 0.01f) return;
+            float e = s.penergy[q];
+            if (!(e > p.particleSplitEnergy[s.pcolor[q] % ALIEN_B200_MAX_COLORS])) return;
+            e *= 0.5f;
+            s.penergy[q] = e;
+            float2 vp = unitVectorOfAngle(draw(id, T, kSiteSplitAngle) * 360.0f);
+            const float2 pp = s.ppos[q];
+            const float2 otherPos = correctPosition(pp + vp / 5.0f, wi.W, wi.H);
+            s.ppos[q] = correctPosition(pp - vp / 5.0f, wi.W, wi.H);
+            vp = vp * (p.radiationVelocityPerturbation / (e + 1.0f));
+            const float2 pv = s.pvel[q];
+            s.pvel[q] = pv - vp;
+            if (e > kNearZero) {
+                s.splitPos[q] = otherPos;
+                s.splitVel[q] = pv + vp;
+                s.splitEnergy[q] = e;
+                s.pflag[q] |= 2u;
+            }
+        });
     }
 }
 
@@ -1413,38 +1449,51 @@ __device__ __forceinline__ bool delEvent(const DevState& s, long long g)
 __global__ void __launch_bounds__(kBlock) kEventCount(DevState s)
 {
     __shared__ uint32_t red[2][kBlock / 32];
-    uint32_t a = 0, b = 0;
+    // block sums of a and b in thread 0
+    auto blockSums = [&](uint32_t a, uint32_t b, uint32_t& ta, uint32_t& tb) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        a = __reduce_add_sync(0xffffffffu, a);
+        b = __reduce_add_sync(0xffffffffu, b);
+        __syncthreads();
+        if (lane == 0) {
+            red[0][warp] = a;
+            red[1][warp] = b;
+        }
+        __syncthreads();
+        ta = tb = 0;
+        if (threadIdx.x == 0)
+            for (int i = 0; i < kBlock / 32; ++i) {
+                ta += red[0][i];
+                tb += red[1][i];
+            }
+    };
     if (blockIdx.x < s.numCellBlocks) {
         const long long g = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
         const int w = s.cellBlockWorld[blockIdx.x];
-        if (g < s.worlds[w].cellBase + s.counters[w].numCells) {
+        WorldCounters& wc = s.counters[w];
+        uint32_t a = 0, b = 0;
+        if (g < s.worlds[w].cellBase + wc.numCells) {
             a = (s.flags[g] & kFlagRadiation) ? 1u : 0u;
             b = delEvent(s, g) ? 1u : 0u;
         }
-    } else {
-        PartCtx c = partCtx(s, blockIdx.x - s.numCellBlocks);
-        if (c.inRange) a = (s.pflag[c.q] & 2u) ? 1u : 0u;
-    }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    a = __reduce_add_sync(0xffffffffu, a);
-    b = __reduce_add_sync(0xffffffffu, b);
-    if (lane == 0) {
-        red[0][warp] = a;
-        red[1][warp] = b;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t ta = 0, tb = 0;
-        for (int i = 0; i < kBlock / 32; ++i) {
-            ta += red[0][i];
-            tb += red[1][i];
-        }
-        if (blockIdx.x < s.numCellBlocks) {
+        uint32_t ta, tb;
+        blockSums(a, b, ta, tb);
+        if (threadIdx.x == 0) {
             s.blockRad[blockIdx.x] = ta;
             s.blockDel[blockIdx.x] = tb;
-        } else {
-            s.blockSplit[blockIdx.x - s.numCellBlocks] = ta;
+            if (ta) atomicAdd(&wc.evRad, ta);
+            if (tb) atomicAdd(&wc.evDel, tb);
         }
+    } else {
+        forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int pb) {
+            const uint32_t a = c.inRange && (s.pflag[c.q] & 2u) ? 1u : 0u;
+            uint32_t ta, tb;
+            blockSums(a, 0u, ta, tb);
+            if (threadIdx.x == 0) {
+                s.blockSplit[pb] = ta;
+                if (ta) atomicAdd(&s.counters[c.w].evSplit, ta);
+            }
+        });
     }
 }
 
@@ -1468,20 +1517,29 @@ __device__ uint32_t blockScanBlocks(uint32_t* arr, int first, int count)
     return total;
 }
 
-// one block per world: block offsets, id and slot bases, timestep advance
+// one block per world: block offsets, id and slot bases, timestep advance;
+// the block scans run only for the kinds of events the step produced
 __global__ void __launch_bounds__(kBlock) kEventWorld(DevState s)
 {
     const int w = blockIdx.x;
     WorldCounters& wc = s.counters[w];
+    const uint32_t evR = wc.evRad, evD = wc.evDel, evS = wc.evSplit;
+    __syncthreads();
     if (!wc.active) {
-        if (threadIdx.x == 0) wc.numEvents = 0;
+        if (threadIdx.x == 0) {
+            wc.numEvents = 0;
+            wc.evRad = wc.evDel = wc.evSplit = 0;
+        }
         return;
     }
     const WorldInfo& wi = s.worlds[w];
-    const uint32_t R = blockScanBlocks(s.blockRad, wi.firstCellBlock, wi.numCellBlocks);
-    const uint32_t D = blockScanBlocks(s.blockDel, wi.firstCellBlock, wi.numCellBlocks);
-    const uint32_t S = blockScanBlocks(s.blockSplit, wi.firstPartBlock, wi.numPartBlocks);
+    // particle blocks holding used slots (the count before this step's appends)
+    const int usedPartBlocks = static_cast<int>((wc.numParticles + kBlock - 1) / kBlock);
+    const uint32_t R = evR ? blockScanBlocks(s.blockRad, wi.firstCellBlock, wi.numCellBlocks) : 0u;
+    const uint32_t D = evD ? blockScanBlocks(s.blockDel, wi.firstCellBlock, wi.numCellBlocks) : 0u;
+    const uint32_t S = evS ? blockScanBlocks(s.blockSplit, wi.firstPartBlock, usedPartBlocks) : 0u;
     if (threadIdx.x != 0) return;
+    wc.evRad = wc.evDel = wc.evSplit = 0;
     const unsigned long long id0 = wc.nextId;
     const uint32_t slot0 = wc.numParticles;
     wc.radIdBase = id0;
@@ -1518,6 +1576,13 @@ __device__ __forceinline__ void emitParticle(const DevState& s, const WorldInfo&
     s.pselected[q] = 0;
     s.palive[q] = 1;
     s.plast[q] = ~0ull;
+    // per-step scratch of a new slot (kBin resets the used slots at step start)
+    s.pflag[q] = 0;
+    s.ptarget[q] = -1;
+    s.pslot[q] = -1;
+    s.pmerge[3 * q + 0] = 0;
+    s.pmerge[3 * q + 1] = 0;
+    s.pmerge[3 * q + 2] = 0;
 }
 
 __global__ void __launch_bounds__(kBlock) kEventEmit(DevState s)
@@ -1538,17 +1603,19 @@ __global__ void __launch_bounds__(kBlock) kEventEmit(DevState s)
         if (rad) emitParticle(s, wi, wc.radSlotBase + rr, wc.radIdBase + rr, s.radPos[g], s.radVel[g], s.radEnergy[g], s.color[g]);
         if (del) emitParticle(s, wi, wc.delSlotBase + dr, wc.delIdBase + dr, s.posA[g], s.velA[g], s.energy[g], s.color[g]);
     } else {
-        const int pb = blockIdx.x - s.numCellBlocks;
-        const int w = s.partBlockWorld[pb];
-        const WorldCounters& wc = s.counters[w];
-        if (wc.numEvents == 0) return;
-        const WorldInfo& wi = s.worlds[w];
-        const long long q = static_cast<long long>(pb) * kBlock + threadIdx.x;
-        // particles appended by this step sit beyond the old count: their
-        // pflag is clear (reset in kBin for the whole range)
-        const uint32_t split = (s.pflag[q] & 2u) ? 1u : 0u;
-        const uint32_t sr = blockExclusiveScan(split, nullptr) + s.blockSplit[pb];
-        if (split) emitParticle(s, wi, wc.splitSlotBase + sr, wc.splitIdBase + sr, s.splitPos[q], s.splitVel[q], s.splitEnergy[q], s.pcolor[q]);
+        // splits come from the slots used before this step's appends
+        // (radSlotBase); appended particles carry no split
+        forParticleBlocks(s, [](const WorldCounters& wc) { return wc.radSlotBase; }, [&](const PartCtx& c, int pb) {
+            const WorldCounters& wc = s.counters[c.w];
+            if (wc.numEvents == 0) return;
+            const WorldInfo& wi = s.worlds[c.w];
+            const long long q = c.q;
+            const uint32_t split = c.inRange && (s.pflag[q] & 2u) ? 1u : 0u;
+            const uint32_t sr = blockExclusiveScan(split, nullptr) + s.blockSplit[pb];
+            if (split)
+                emitParticle(s, wi, wc.splitSlotBase + sr, wc.splitIdBase + sr, s.splitPos[q], s.splitVel[q], s.splitEnergy[q],
+                             s.pcolor[q]);
+        });
     }
 }
 
