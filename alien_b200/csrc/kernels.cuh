@@ -144,7 +144,7 @@ __device__ __forceinline__ void forEachWindowTile(const WorldInfo& wi, int sx, i
 // (CellProcessor::radiation, CellProcessor.cuh:725-773).
 // particles: reset, particle map (ParticleMap::set_block, Map.cuh:236-258;
 // the highest storage index wins).
-__global__ void __launch_bounds__(kBlock) kBin(DevState s)
+__global__ void __launch_bounds__(kBlock, 8) kBin(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         // per-step scratch needs no reset here: flags are cleared by
@@ -914,7 +914,7 @@ __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, cons
 // cells: checkForces + applyForces (CellProcessor.cuh:367-406), bond forces
 // #1 at the overlap-corrected positions.  particles: movement
 // (RadiationProcessor::movement, RadiationProcessor.cuh:61-70).
-__global__ void __launch_bounds__(kBlock) kApplyBond1(DevState s)
+__global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         CellCtx c = cellCtx(s);
@@ -950,7 +950,7 @@ __global__ void __launch_bounds__(kBlock) kApplyBond1(DevState s)
 // --------------------------------------------------------- kVerletPos ----
 // cells: verletPositionUpdate (CellProcessor.cuh:525-544).
 // particles: merge target (RadiationProcessor::collision, :78-80).
-__global__ void __launch_bounds__(kBlock) kVerletPos(DevState s)
+__global__ void __launch_bounds__(kBlock, 8) kVerletPos(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         CellCtx c = cellCtx(s);
@@ -990,7 +990,7 @@ __global__ void __launch_bounds__(kBlock) kVerletPos(DevState s)
 // cells: checkConnections (CellProcessor.cuh:493-523) at the new positions,
 // bond forces #2.  particles: merges into particles that do not merge
 // themselves (RadiationProcessor.cuh:82-96 under the fixed rule).
-__global__ void __launch_bounds__(kBlock) kBond2(DevState s)
+__global__ void __launch_bounds__(kBlock, 6) kBond2(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         CellCtx c = cellCtx(s);
@@ -1054,7 +1054,7 @@ __device__ __forceinline__ int slotHead(const DevState& s, const WorldInfo& wi, 
 // checkConnections, aging (CellProcessor.cuh:561-593).
 // particles: merged particles, absorption into / reflection at the cell
 // under the particle (RadiationProcessor.cuh:97-168).
-__global__ void __launch_bounds__(kBlock) kVerletVel(DevState s)
+__global__ void __launch_bounds__(kBlock, 8) kVerletVel(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         CellCtx c = cellCtx(s);
@@ -1135,7 +1135,7 @@ __global__ void __launch_bounds__(kBlock) kVerletVel(DevState s)
 // absorbed energy, inner friction (every third step: one Jacobi sweep with
 // one pair average per bond, CellProcessor.cuh:678-705), friction and decay.
 // particles: splitting (RadiationProcessor::splitting, :172-204).
-__global__ void __launch_bounds__(kBlock) kTransition(DevState s)
+__global__ void __launch_bounds__(kBlock, 8) kTransition(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         CellCtx c = cellCtx(s);
@@ -1333,7 +1333,7 @@ __device__ inline bool tryAddOneWay(const DevState& s, const WorldInfo& wi, long
 // dying / detaching resolution of decay (CellProcessor.cuh:840-850) and the
 // bond additions of mutually chosen fusion pairs (processAddOperations,
 // CellConnectionProcessor.cuh:130-143, 211-272), written to scratch.
-__global__ void __launch_bounds__(kBlock) kResolve(DevState s)
+__global__ void __launch_bounds__(kBlock, 6) kResolve(DevState s)
 {
     CellCtx c = cellCtx(s);
     if (!c.valid) return;
@@ -1376,7 +1376,7 @@ __global__ void __launch_bounds__(kBlock) kResolve(DevState s)
 // (processDeleteConnectionOperations :176-209 with deleteConnectionOneWay
 // :429-448): a bond is dropped when its partner is deleted, or when either
 // end scheduled "delete all bonds" and the bond is not this step's addition.
-__global__ void __launch_bounds__(kBlock) kCommit(DevState s)
+__global__ void __launch_bounds__(kBlock, 8) kCommit(DevState s)
 {
     CellCtx c = cellCtx(s);
     if (!c.valid) return;
