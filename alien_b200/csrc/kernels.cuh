@@ -374,6 +374,8 @@ struct FluidLaw {
     }
 
     __device__ __forceinline__ bool near(float2 pd) const { return pd.x * pd.x + pd.y * pd.y <= R2reject; }
+    // every candidate within the radius contributes (density, push)
+    __device__ __forceinline__ bool relevant(const int4*, int, float2) const { return true; }
 
     __device__ __forceinline__ void visit(int4 om, float2 vj, float2 pd)
     {
@@ -480,7 +482,7 @@ struct CollisionLaw {
     const DevState* s;
     const AlienPhysicsParams* p;
     int g;
-    float R, R2reject, minDist, fusionVelocity, maxBindingEnergy;
+    float R, R2reject, minDist, minDist2Keep, fusionVelocity, maxBindingEnergy;
     float2 pi, vi;
     bool barrierI, visibleI, fusionI;
     float densI;
@@ -497,6 +499,7 @@ struct CollisionLaw {
         R = p->cellMaxCollisionDistance;
         R2reject = R * R * 1.0001f + 1e-6f;
         minDist = p->cellMinDistance;
+        minDist2Keep = minDist * minDist * 1.0001f + 1e-6f;
         fusionVelocity = p->cellFusionVelocity;
         maxBindingEnergy = p->cellMaxBindingEnergy;
         pi = pos;
@@ -514,6 +517,18 @@ struct CollisionLaw {
     }
 
     __device__ __forceinline__ bool near(float2 raw) const { return raw.x * raw.x + raw.y * raw.y <= R2reject; }
+    // visit() changes nothing for the cell itself, and for a bonded partner
+    // it only adds the overlap push, which needs d < minDist and a cell that
+    // is not a barrier; such candidates are dropped here (the bound on q is
+    // above minDist^2 by more than the rounding of sqrtf, so no candidate
+    // with sqrtf(q) < minDist is dropped)
+    __device__ __forceinline__ bool relevant(const int4* meta, int m, float2 raw) const
+    {
+        const int j = meta[m].x;
+        if (j == g) return false;
+        if (!isBondedTo(bondsI, j)) return true;
+        return !barrierI && raw.x * raw.x + raw.y * raw.y <= minDist2Keep;
+    }
 
     __device__ __forceinline__ void visit(int4 om, float2 vj, float2 raw)
     {
@@ -774,7 +789,8 @@ __global__ void __launch_bounds__(kRegionThreads, kRegionMinBlocks) kPairsRegion
             for (int r = r0; r <= r1; ++r) {
                 const int b0 = tStart[r * LW + c0], b1 = tStart[r * LW + c1 + 1];
                 for (int m = b0; m < b1; ++m) {
-                    if (law.near(diff(m))) {
+                    const float2 dm = diff(m);
+                    if (law.near(dm) && law.relevant(sMeta, m, dm)) {
                         myHits[nh * kRegionThreads] = static_cast<uint16_t>(m);
                         if (++nh == kHitCap) flush();
                     }
@@ -914,7 +930,7 @@ __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, cons
 // cells: checkForces + applyForces (CellProcessor.cuh:367-406), bond forces
 // #1 at the overlap-corrected positions.  particles: movement
 // (RadiationProcessor::movement, RadiationProcessor.cuh:61-70).
-__global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
+__global__ void __launch_bounds__(kBlock, 8) kApplyBond1(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         CellCtx c = cellCtx(s);
@@ -990,7 +1006,7 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletPos(DevState s)
 // cells: checkConnections (CellProcessor.cuh:493-523) at the new positions,
 // bond forces #2.  particles: merges into particles that do not merge
 // themselves (RadiationProcessor.cuh:82-96 under the fixed rule).
-__global__ void __launch_bounds__(kBlock, 6) kBond2(DevState s)
+__global__ void __launch_bounds__(kBlock, 8) kBond2(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         CellCtx c = cellCtx(s);
@@ -1333,7 +1349,7 @@ __device__ inline bool tryAddOneWay(const DevState& s, const WorldInfo& wi, long
 // dying / detaching resolution of decay (CellProcessor.cuh:840-850) and the
 // bond additions of mutually chosen fusion pairs (processAddOperations,
 // CellConnectionProcessor.cuh:130-143, 211-272), written to scratch.
-__global__ void __launch_bounds__(kBlock, 6) kResolve(DevState s)
+__global__ void __launch_bounds__(kBlock, 8) kResolve(DevState s)
 {
     CellCtx c = cellCtx(s);
     if (!c.valid) return;
