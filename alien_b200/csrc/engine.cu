@@ -210,6 +210,7 @@ private:
     uint64_t launches_ = 0;
     int kernelsPerStep_ = 0;
     int partGrid_ = 1;  // blocks of the particle part of a combined launch
+    int statsGrid_ = 1;  // blocks of a statistics reduction
     cudaGraphExec_t graphExec_ = nullptr;
     uint64_t stepsSinceCheck_ = 0;
     bool hasFluid_ = false, hasCollision_ = false;
@@ -311,6 +312,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         AB_CK(cudaGetDevice(&device));
         AB_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
         partGrid_ = std::max(1, std::min(partBlocks, 16 * std::max(sms, 1)));
+        statsGrid_ = 4 * std::max(sms, 1);
     }
     s.cellSlots = cellSlots;
     s.partSlots = partSlots;
@@ -823,9 +825,13 @@ void Arena::compactParticles(int w)
 
 AlienRawStatistics Arena::statistics(int w)
 {
-    AB_CK(cudaMemsetAsync(stats_, 0, sizeof(StatsAcc) * worlds_.size(), stream_));
-    launch(kStatsCells, s_.numCellBlocks, kBlock, s_, stats_);
-    launch(kStatsParticles, s_.numPartBlocks, kBlock, s_, stats_);
+    AB_CK(cudaMemsetAsync(stats_ + w, 0, sizeof(StatsAcc), stream_));
+    {
+        const WorldInfo& wi = worlds_[w].info;
+        const long long slots = std::max(wi.cellCap, wi.partCap);
+        const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>(statsGrid_, (slots + kBlock - 1) / kBlock)));
+        launch(kStatsWorld, grid, kBlock, s_, w, stats_);
+    }
     StatsAcc a;
     AB_CK(cudaMemcpyAsync(&a, stats_ + w, sizeof(a), cudaMemcpyDeviceToHost, stream_));
     WorldCounters c;

@@ -227,53 +227,74 @@ struct StatsAcc {
     long long cellEnergyFix, particleEnergyFix;  // 2^-16 fixed point: order-independent sums
 };
 
-// one block = one world (blocks never straddle worlds): warp sums, then one
-// atomic per warp and counter
 __device__ __forceinline__ unsigned long long warpSumU64(unsigned long long v)
 {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     return v;
 }
 
-__global__ void __launch_bounds__(kBlock) kStatsCells(DevState s, StatsAcc* acc)
+// statistics of world w (getRawStatistics): a grid of a few blocks per SM
+// strides over the world's used cell and particle slots; each thread keeps
+// its partial counts in registers, each block sums them (warp shuffles, then
+// shared memory) and adds the block totals with one atomic per counter.
+// All sums are integers (energies in 2^-16 fixed point), so the result does
+// not depend on the order of the atomics.
+constexpr int kStatsFields = 4 + ALIEN_B200_MAX_COLORS + 1;  // cells, bonds, cellE, parts, colors..., partE
+__global__ void __launch_bounds__(kBlock) kStatsWorld(DevState s, int w, StatsAcc* acc)
 {
-    const int b = blockIdx.x;
-    const int w = s.cellBlockWorld[b];
+    __shared__ unsigned long long red[kStatsFields][kBlock / 32];
     const WorldInfo& wi = s.worlds[w];
-    const long long g = static_cast<long long>(b) * kBlock + threadIdx.x;
-    const bool live = g < wi.cellBase + s.counters[w].numCells && s.alive[g];
-    unsigned long long cells = live ? 1 : 0;
-    unsigned long long bonds = live ? s.numConn[g] : 0;
-    long long e = live ? __double2ll_rn(static_cast<double>(s.energy[g]) * 65536.0) : 0;
-    const int col = live ? s.color[g] % ALIEN_B200_MAX_COLORS : -1;
-    StatsAcc& a = acc[w];
-    cells = warpSumU64(cells);
-    bonds = warpSumU64(bonds);
-    e = static_cast<long long>(warpSumU64(static_cast<unsigned long long>(e)));
-    if ((threadIdx.x & 31) == 0 && cells) {
-        atomicAdd(&a.numCells, cells);
-        atomicAdd(&a.numConnections, bonds);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&a.cellEnergyFix), static_cast<unsigned long long>(e));
+    const WorldCounters& wc = s.counters[w];
+    const long long stride = static_cast<long long>(gridDim.x) * kBlock;
+    unsigned int cells = 0, bonds = 0, parts = 0;
+    unsigned int byColor[ALIEN_B200_MAX_COLORS] = {};
+    long long cellE = 0, partE = 0;
+    const long long cellEnd = wi.cellBase + wc.numCells;
+    for (long long g = wi.cellBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x; g < cellEnd; g += stride) {
+        if (!s.alive[g]) continue;
+        ++cells;
+        bonds += s.numConn[g];
+        cellE += __double2ll_rn(static_cast<double>(s.energy[g]) * 65536.0);
+        const int col = s.color[g] % ALIEN_B200_MAX_COLORS;
+#pragma unroll
+        for (int c = 0; c < ALIEN_B200_MAX_COLORS; ++c) byColor[c] += col == c ? 1u : 0u;
     }
-    for (int c = 0; c < ALIEN_B200_MAX_COLORS; ++c) {
-        const unsigned long long n = warpSumU64(col == c ? 1ull : 0ull);
-        if ((threadIdx.x & 31) == 0 && n) atomicAdd(&a.numCellsByColor[c], n);
+    const long long partEnd = wi.partBase + wc.numParticles;
+    for (long long q = wi.partBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x; q < partEnd; q += stride) {
+        if (!s.palive[q]) continue;
+        ++parts;
+        partE += __double2ll_rn(static_cast<double>(s.penergy[q]) * 65536.0);
     }
-}
-
-__global__ void __launch_bounds__(kBlock) kStatsParticles(DevState s, StatsAcc* acc)
-{
-    const int pb = blockIdx.x;
-    const int w = s.partBlockWorld[pb];
-    const WorldInfo& wi = s.worlds[w];
-    const long long q = static_cast<long long>(pb) * kBlock + threadIdx.x;
-    const bool live = q < wi.partBase + s.counters[w].numParticles && s.palive[q];
-    unsigned long long n = warpSumU64(live ? 1ull : 0ull);
-    long long e = live ? __double2ll_rn(static_cast<double>(s.penergy[q]) * 65536.0) : 0;
-    e = static_cast<long long>(warpSumU64(static_cast<unsigned long long>(e)));
-    if ((threadIdx.x & 31) == 0 && n) {
-        atomicAdd(&acc[w].numParticles, n);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&acc[w].particleEnergyFix), static_cast<unsigned long long>(e));
+    unsigned long long v[kStatsFields];
+    v[0] = cells;
+    v[1] = bonds;
+    v[2] = static_cast<unsigned long long>(cellE);
+    v[3] = parts;
+#pragma unroll
+    for (int c = 0; c < ALIEN_B200_MAX_COLORS; ++c) v[4 + c] = byColor[c];
+    v[4 + ALIEN_B200_MAX_COLORS] = static_cast<unsigned long long>(partE);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int f = 0; f < kStatsFields; ++f) {
+        const unsigned long long t = warpSumU64(v[f]);
+        if (lane == 0) red[f][warp] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < kStatsFields) {
+        unsigned long long t = 0;
+        for (int i = 0; i < kBlock / 32; ++i) t += red[threadIdx.x][i];
+        if (t) {
+            StatsAcc& a = acc[w];
+            unsigned long long* dst;
+            const int f = threadIdx.x;
+            if (f == 0) dst = &a.numCells;
+            else if (f == 1) dst = &a.numConnections;
+            else if (f == 2) dst = reinterpret_cast<unsigned long long*>(&a.cellEnergyFix);
+            else if (f == 3) dst = &a.numParticles;
+            else if (f < 4 + ALIEN_B200_MAX_COLORS) dst = &a.numCellsByColor[f - 4];
+            else dst = reinterpret_cast<unsigned long long*>(&a.particleEnergyFix);
+            atomicAdd(dst, t);
+        }
     }
 }
 
