@@ -43,15 +43,34 @@ def log(msg: str) -> None:
 # P1 hash build 24; P2 pair forces 40; P3 apply 24 + P4 bond forces 20+12b;
 # P5 Verlet x 32; P6 bond forces 20+12b; P7 Verlet v 32
 def algorithmic_bytes(kernel: str, bonds_per_cell: float) -> float:
-    b = bonds_per_cell
+    """Bytes per cell one launch must move with this data layout: each
+    array the kernel reads or writes for a cell, counted once (a partner's
+    position or stiffness is another cell's row, counted where it is owned;
+    the pair phase's halo re-reads are overhead, not algorithmic).  Angle
+    work of every third step is amortised (bond angles, 24 B / 3)."""
+    del bonds_per_cell  # bond rows are fixed-width (6 slots)
     if kernel.startswith("kPairs"):
-        return 40.0
+        # staged record (pos/vel 16 + meta 16), bond row 24; writes force 8,
+        # overlap-pushed position 8, density 4, fusion choice 4
+        return 80.0
     return {
-        "kBin": 24.0,
-        "kApplyBond1": 24.0 + 20.0 + 12.0 * b,
-        "kVerletPos": 32.0,
-        "kBond2": 20.0 + 12.0 * b,
-        "kVerletVel": 32.0,
+        # position 8, alive 1, barrier 1; tile 4 + rank 4 written, tile count
+        # atomic 8 (read + write)
+        "kBin": 26.0,
+        # alive, barrier, color, numConn 4; force 8, velocity 8, bond row 24,
+        # position 8, stiffness 4, rest lengths 24; writes velocity 8, force 8;
+        # bond angles 24 / 3
+        "kApplyBond1": 104.0,
+        # alive, barrier, color, numConn 4; bond row 24, position 8,
+        # stiffness 4, rest lengths 24; writes force 8; bond angles 24 / 3
+        "kBond2": 80.0,
+        # velocity 8, position 8, force 8, angle accumulators 16, barrier and
+        # alive 2; writes force 8, position 8
+        "kVerletPos": 58.0,
+        # velocity 8, angle accumulators 16, two forces 16, barrier, alive,
+        # living state 3, flags 4, age 4 + 4, activation time 4; writes
+        # velocity 8
+        "kVerletVel": 67.0,
     }.get(kernel, 0.0)
 
 
