@@ -17,6 +17,8 @@
 namespace ab {
 
 constexpr int kBlock = 256;           // threads per block of per-object kernels
+constexpr int kCellFunctionNeuron = 0;  // CellFunction_Neuron, CellFunctionConstants.h:8
+constexpr int kCellFunctionNone = 11;   // CellFunction_None, CellFunctionConstants.h:21
 constexpr int kMaxBonds = 6;          // MAX_CELL_BONDS, EngineConstants.h:3
 constexpr int kSlotScanLevels = 10;   // Map.cuh:117, CellProcessor.cuh:165
 constexpr float kNearZero = 1.0e-4f;  // Base/Definitions.h:27
@@ -124,6 +126,9 @@ struct DevState {
     uint32_t* activationTime;
     uint32_t* creatureId;
     uint32_t* coldIdx;
+    AlienCellTO* cold;        // ingest copies (signals and cellFunctionUsed of neuron cells change here)
+    const int* neuronRow;     // neuron table row of a neuron cell, -1 otherwise (null without neurons)
+    const float* neuronTable; // per neuron cell: weights [8 x 8] row-major, then 8 biases
     int* bond;          // [slot * 6 + k] partner slot
     float* bondDist;
     float* bondAngle;

@@ -91,6 +91,8 @@ static void validateParams(const AlienPhysicsParams& p, int W, int H)
     if (p.cellAgeLimiter || p.cellColorTransitionRules || p.advancedAbsorptionControl || p.externalEnergyControl)
         throw Error(ALIEN_B200_ERR_UNSUPPORTED, "feature flags of cell functions / energy control must be off");
     if (p.rigidity != 0.0f) throw Error(ALIEN_B200_ERR_UNSUPPORTED, "rigidity clusters (rigidity != 0) are not supported");
+    if (p.cellNumExecutionOrderNumbers < 1)
+        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "cellNumExecutionOrderNumbers must be at least 1");
     if (p.motionType != ALIEN_B200_MOTION_FLUID && p.motionType != ALIEN_B200_MOTION_COLLISION)
         throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "motionType must be 0 (fluid) or 1 (collision)");
     if (!(p.smoothingLength > 0.0f) || !(p.cellMaxCollisionDistance > 0.0f))
@@ -213,12 +215,39 @@ private:
     int statsGrid_ = 1;  // blocks of a statistics reduction
     cudaGraphExec_t graphExec_ = nullptr;
     uint64_t stepsSinceCheck_ = 0;
-    bool hasFluid_ = false, hasCollision_ = false;
+    bool hasFluid_ = false, hasCollision_ = false, hasNeurons_ = false;
+    bool signalsLive_ = false;  // some cell has a function or a nonzero signal channel
 };
 
 // ------------------------------------------------------------- build -----
+// cell functions: neurons run in this engine (kNeuron); any other function
+// would need the rest of the cell-function stage.  Checked before build()
+// changes anything.
+static void validateCells(const std::vector<WorldSetup>& setups)
+{
+    for (const WorldSetup& ws : setups)
+        for (uint64_t i = 0; i < ws.numCells; ++i) {
+            const AlienCellTO& c = ws.cells[i];
+            if (c.cellFunction == kCellFunctionNone) continue;
+            if (c.cellFunction != kCellFunctionNeuron)
+                throw Error(ALIEN_B200_ERR_UNSUPPORTED, "cell id " + std::to_string(c.id) + " has cell function "
+                                                            + std::to_string(c.cellFunction)
+                                                            + "; only neurons (0) and cells without function (11) are supported");
+            const uint64_t at = c.cellFunctionData[0];  // NeuronTO.weightsAndBiasesDataIndex
+            const uint64_t bytes = sizeof(float) * kNeuronTableStride;
+            if (at > ws.numAux || ws.numAux - at < bytes)
+                throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT,
+                            "neuron data of cell id " + std::to_string(c.id) + " lies outside the auxiliary data");
+        }
+}
+
 void Arena::build(const std::vector<WorldSetup>& setups)
 {
+    validateCells(setups);
+    for (const WorldSetup& ws : setups) {
+        if (ws.W <= 0 || ws.H <= 0) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "world size must be positive");
+        validateParams(ws.params, ws.W, ws.H);
+    }
     releaseGraph();
     AB_CK(cudaStreamSynchronize(stream_));
     mem_.freeAll();
@@ -284,6 +313,32 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         if (ws.numAux) hw.aux.assign(ws.aux, ws.aux + ws.numAux);
         worlds_.push_back(std::move(hw));
     }
+    // neuron table: weights and biases of every neuron cell
+    std::vector<float> neuronTableHost;
+    std::vector<std::pair<long long, int>> neuronCells;  // (arena slot, table row)
+    {
+        long long slotBase = 0;
+        for (int w = 0; w < n; ++w) {
+            const WorldSetup& ws = setups[w];
+            for (uint64_t i = 0; i < ws.numCells; ++i) {
+                const AlienCellTO& c = ws.cells[i];
+                if (c.cellFunction != kCellFunctionNeuron) continue;  // checked by validateCells
+                const uint64_t at = c.cellFunctionData[0];  // NeuronTO.weightsAndBiasesDataIndex
+                const uint64_t bytes = sizeof(float) * kNeuronTableStride;
+                const size_t row = neuronTableHost.size() / kNeuronTableStride;
+                neuronTableHost.resize(neuronTableHost.size() + kNeuronTableStride);
+                std::memcpy(neuronTableHost.data() + row * kNeuronTableStride, ws.aux + at, bytes);
+                neuronCells.emplace_back(slotBase + static_cast<long long>(i), static_cast<int>(row));
+            }
+            slotBase += worlds_[w].info.cellCap;
+        }
+    }
+    hasNeurons_ = !neuronCells.empty();
+    signalsLive_ = hasNeurons_;
+    for (int w = 0; w < n && !signalsLive_; ++w)
+        for (uint64_t i = 0; i < setups[w].numCells && !signalsLive_; ++i)
+            for (int ch = 0; ch < ALIEN_B200_MAX_CHANNELS; ++ch)
+                if (setups[w].cells[i].signal.channels[ch] != 0.0f) signalsLive_ = true;
     hasFluid_ = hasCollision_ = false;
     for (const HostWorld& hw : worlds_) {
         if (hw.info.motionType == ALIEN_B200_MOTION_FLUID)
@@ -401,6 +456,21 @@ void Arena::build(const std::vector<WorldSetup>& setups)
 
     stats_ = mem_.alloc<StatsAcc>(n);
     cold_ = mem_.alloc<AlienCellTO>(static_cast<size_t>(coldTotal));
+    s.cold = cold_;
+    s.neuronRow = nullptr;
+    s.neuronTable = nullptr;
+    if (hasNeurons_) {
+        int* rowDev = mem_.alloc<int>(C);
+        float* tableDev = mem_.alloc<float>(neuronTableHost.size());
+        std::vector<int> rowHost(C, -1);
+        for (const auto& nc : neuronCells) rowHost[static_cast<size_t>(nc.first)] = nc.second;
+        AB_CK(cudaMemcpyAsync(rowDev, rowHost.data(), sizeof(int) * C, cudaMemcpyHostToDevice, stream_));
+        AB_CK(cudaMemcpyAsync(tableDev, neuronTableHost.data(), sizeof(float) * neuronTableHost.size(), cudaMemcpyHostToDevice,
+                              stream_));
+        AB_CK(cudaStreamSynchronize(stream_));  // the host vectors end with this scope
+        s.neuronRow = rowDev;
+        s.neuronTable = tableDev;
+    }
     rankCells_ = mem_.alloc<int>(C);
     rankParts_ = mem_.alloc<int>(P);
     blockCount_ = mem_.alloc<uint32_t>(static_cast<size_t>(std::max(cellBlocks, partBlocks)) + 2);
@@ -500,6 +570,8 @@ void Arena::enqueueStep()
     launch(kVerletVel, both, kBlock, s);
     launch(kTransition, both, kBlock, s);
     launch(kResolve, cells, kBlock, s);
+    if (hasNeurons_) launch(kNeuron, cells, kBlock, s);
+    if (signalsLive_) launch(kSignalReset, cells, kBlock, s);
     launch(kCommit, cells, kBlock, s);
     launch(kEventCount, both, kBlock, s);
     launch(kEventWorld, s.numWorlds, kBlock, s);
@@ -963,6 +1035,7 @@ void alien_b200_default_parameters(AlienPhysicsParams* p)
     p->rigidity = 0.0f;
     p->cellFusionVelocity = 0.6f;
     p->cellMaxBindingEnergy = 3.4028234663852886e38f;
+    p->cellNumExecutionOrderNumbers = 6;
     for (int i = 0; i < ALIEN_B200_MAX_COLORS; ++i) {
         p->cellMaxBindingDistance[i] = 3.6f;
         p->radiationMinCellAge[i] = 0;

@@ -1259,6 +1259,141 @@ __global__ void __launch_bounds__(kBlock, 8) kTransition(DevState s)
     }
 }
 
+// ------------------------------------------------------------ kNeuron ----
+// The neuron cell function: CellFunctionProcessor::collectCellFunctionOperations
+// (CellFunctionProcessor.cuh:33-50) selects the cells whose execution order
+// number is timestep % cellNumExecutionOrderNumbers, that are neither under
+// construction nor activating and whose activation time is 0;
+// NeuronProcessor::processCell (NeuronProcessor.cuh:33-74) sums the signals of
+// the bonded cells of the cell's input execution order number
+// (CellFunctionProcessor::calcInputSignal, :128-164; each channel clamped to
+// [-10, 10] after every addition, in bond order), marks the function used
+// (updateInvocationState, :176-186), and writes act(W x + b).  Inputs never run
+// in the same step as the cells reading them (a different execution order
+// number), so reading and writing signals in one pass needs no snapshot.  The
+// matrix-vector sum runs in column order (the reference adds the 64 products
+// with shared-memory atomics in arbitrary order).
+constexpr int kNeuronTableStride = ALIEN_B200_MAX_CHANNELS * (ALIEN_B200_MAX_CHANNELS + 1);
+
+__device__ __forceinline__ float neuronActivation(int function, float x)
+{
+    switch (function) {
+    case 0: return 2.0f / (1.0f + expf(-x)) - 1.0f;       // sigmoid
+    case 1: return x >= kNearZero ? 1.0f : 0.0f;          // binary step
+    case 2: return fmaxf(-1.0f, fminf(1.0f, x));         // identity
+    case 3: return fminf(1.0f, fabsf(x));                 // abs
+    case 4: return expf(-2.0f * x * x);                   // gaussian
+    }
+    return 0.0f;
+}
+
+__global__ void __launch_bounds__(kBlock) kNeuron(DevState s)
+{
+    CellCtx c = cellCtx(s);
+    if (!c.valid) return;
+    const long long g = c.g;
+    const int row = s.neuronRow[g];
+    if (row < 0) return;
+    AlienCellTO& me = s.cold[s.coldIdx[g]];
+    const AlienPhysicsParams& p = s.params[c.w];
+    const uint64_t T = s.counters[c.w].timestep;
+    if (static_cast<uint64_t>(me.executionOrderNumber) != T % static_cast<uint64_t>(p.cellNumExecutionOrderNumbers)) return;
+    const int ls = s.livingState[g];
+    if (ls == ALIEN_B200_LIVING_UNDER_CONSTRUCTION || ls == ALIEN_B200_LIVING_ACTIVATING || s.activationTime[g] != 0) return;
+
+    float in[ALIEN_B200_MAX_CHANNELS];
+#pragma unroll
+    for (int ch = 0; ch < ALIEN_B200_MAX_CHANNELS; ++ch) in[ch] = 0.0f;
+    uint8_t origin = 0;
+    float tx = 0.0f, ty = 0.0f;
+    const int inputOrder = me.inputExecutionOrderNumber;
+    if (inputOrder != -1 && inputOrder != static_cast<int>(me.executionOrderNumber)) {
+        int sensors = 0;
+        const int n = s.numConn[g];
+        for (int k = 0; k < n; ++k) {
+            const int j = s.bond[g * kMaxBonds + k];
+            const AlienCellTO& o = s.cold[s.coldIdx[j]];
+            const int lsj = s.livingState[j];
+            if (o.outputBlocked || lsj == ALIEN_B200_LIVING_UNDER_CONSTRUCTION || lsj == ALIEN_B200_LIVING_ACTIVATING) continue;
+            if (static_cast<int>(o.executionOrderNumber) != inputOrder) continue;
+#pragma unroll
+            for (int ch = 0; ch < ALIEN_B200_MAX_CHANNELS; ++ch) in[ch] = fmaxf(-10.0f, fminf(10.0f, in[ch] + o.signal.channels[ch]));
+            if (o.signal.origin == 1) {  // SignalOrigin_Sensor
+                origin = 1;
+                tx += o.signal.targetX;
+                ty += o.signal.targetY;
+                ++sensors;
+            }
+        }
+        if (sensors > 0) {
+            tx /= static_cast<float>(sensors);
+            ty /= static_cast<float>(sensors);
+        }
+    }
+    if (me.cellFunctionUsed == 0) {
+        bool used = false;
+#pragma unroll
+        for (int ch = 0; ch < ALIEN_B200_MAX_CHANNELS - 1; ++ch) used |= in[ch] != 0.0f;
+        if (used) me.cellFunctionUsed = 1;
+    }
+    const float* wb = s.neuronTable + static_cast<long long>(row) * kNeuronTableStride;
+    const int32_t* act = reinterpret_cast<const int32_t*>(&me.cellFunctionData[1]);  // NeuronTO.activationFunctions
+    float out[ALIEN_B200_MAX_CHANNELS];
+#pragma unroll
+    for (int r = 0; r < ALIEN_B200_MAX_CHANNELS; ++r) {
+        float sum = wb[ALIEN_B200_MAX_CHANNELS * ALIEN_B200_MAX_CHANNELS + r];
+#pragma unroll
+        for (int col = 0; col < ALIEN_B200_MAX_CHANNELS; ++col) sum += wb[r * ALIEN_B200_MAX_CHANNELS + col] * in[col];
+        out[r] = neuronActivation(act[r], sum);
+    }
+#pragma unroll
+    for (int r = 0; r < ALIEN_B200_MAX_CHANNELS; ++r) me.signal.channels[r] = out[r];
+    me.signal.origin = origin;
+    me.signal.targetX = tx;
+    me.signal.targetY = ty;
+}
+
+// -------------------------------------------------------- kSignalReset ----
+// CellFunctionProcessor::resetFetchedSignals (CellFunctionProcessor.cuh:69-112,
+// run by the friction kernel after the cell functions, SimulationKernels.cu
+// :153-158): a cell without function loses its signal channels every step; a
+// cell with a function loses them in the step after the last of its readers
+// ran (the bonded cells whose input execution order number is this cell's
+// execution order number; without readers, the step after the cell's own).
+// Reads only execution order numbers, which no step changes.
+__global__ void __launch_bounds__(kBlock) kSignalReset(DevState s)
+{
+    CellCtx c = cellCtx(s);
+    if (!c.valid) return;
+    const long long g = c.g;
+    AlienCellTO& me = s.cold[s.coldIdx[g]];
+    bool reset = me.cellFunction == kCellFunctionNone;
+    if (!reset) {
+        const int orders = s.params[c.w].cellNumExecutionOrderNumbers;
+        const int current = static_cast<int>(s.counters[c.w].timestep % static_cast<uint64_t>(orders));
+        const int own = me.executionOrderNumber;
+        int maxOther = -1;
+        if (!me.outputBlocked) {
+            const int n = s.numConn[g];
+            for (int k = 0; k < n; ++k) {
+                const AlienCellTO& o = s.cold[s.coldIdx[s.bond[g * kMaxBonds + k]]];
+                const int other = o.executionOrderNumber;
+                if (o.inputExecutionOrderNumber != own) continue;
+                if (maxOther == -1) {
+                    maxOther = other;
+                } else if ((maxOther > own && (other > maxOther || other < own)) || (maxOther < own && other > maxOther && other < own)) {
+                    maxOther = other;
+                }
+            }
+        }
+        reset = (maxOther == -1 && current == (own + 1) % orders) || (maxOther != -1 && maxOther == current);
+    }
+    if (reset) {
+#pragma unroll
+        for (int ch = 0; ch < ALIEN_B200_MAX_CHANNELS; ++ch) me.signal.channels[ch] = 0.0f;
+    }
+}
+
 // ---------------------------------------------------- bond additions -----
 // CellConnectionProcessor::tryAddConnectionOneWay (CellConnectionProcessor.cuh
 // :274-427, angle alignment None) on a register copy of the bond list;

@@ -54,6 +54,7 @@ class PhysicsParams(ctypes.Structure):
         ("advancedAbsorptionControl", ctypes.c_uint8),
         ("externalEnergyControl", ctypes.c_uint8),
         ("reserved", ctypes.c_uint8 * 3),
+        ("cellNumExecutionOrderNumbers", ctypes.c_int32),
     ]
 
     def copy(self) -> "PhysicsParams":
@@ -100,6 +101,7 @@ def default_parameters() -> PhysicsParams:
     _fill(p.cellDeathProbability, 0.001)
     p.cellFusionVelocity = 0.6
     p.cellMaxBindingEnergy = FLT_MAX
+    p.cellNumExecutionOrderNumbers = 6
     return p
 
 

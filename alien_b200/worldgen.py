@@ -454,3 +454,42 @@ def calm_test_world(seed: int, world=(64, 64), clusters: int = 4, hex_clusters: 
     parts["vel"] = rng.uniform(-particle_speed, particle_speed, (particles, 2)).astype(np.float32)
     parts["energy"] = rng.uniform(0.5, 2.0, particles).astype(np.float32)
     return DataTO(cells, parts), world
+
+
+def add_neurons(data: DataTO, seed: int, fraction: float = 0.5, cells: np.ndarray | None = None,
+                num_orders: int = 6) -> DataTO:
+    """Turns a share of the bonded cells into neuron cells (CellFunction_Neuron)
+    with their weights and biases in the auxiliary data
+    (NeuronTO.weightsAndBiasesDataIndex, TOs.cuh:45-49): weights ~ N(0, 0.5),
+    biases ~ N(0, 0.1), random activation functions and execution order
+    numbers, and random initial signals on every cell so that inputs carry
+    something.  ``cells`` selects the candidate cells (default: all bonded)."""
+    rng = np.random.default_rng(seed)
+    c = data.cells.copy()
+    n = len(c)
+    cand = np.nonzero(c["numConnections"] > 0)[0] if cells is None else np.asarray(cells)
+    pick = cand[rng.random(len(cand)) < fraction]
+    c["executionOrderNumber"] = rng.integers(0, num_orders, n).astype(np.uint8)
+    c["inputExecutionOrderNumber"] = rng.integers(-1, num_orders, n).astype(np.int8)
+    c["outputBlocked"] = (rng.random(n) < 0.1).astype(np.uint8)
+    c["signalChannels"] = rng.normal(0.0, 1.0, (n, 8)).astype(np.float32)
+    sensor = rng.random(n) < 0.2
+    c["signalOrigin"] = sensor.astype(np.uint8)
+    c["signalTargetX"] = np.where(sensor, rng.uniform(-50, 50, n), 0).astype(np.float32)
+    c["signalTargetY"] = np.where(sensor, rng.uniform(-50, 50, n), 0).astype(np.float32)
+    c["cellFunctionUsed"] = 0
+    aux_old = data.aux
+    stride = 8 * 9 * 4
+    base = len(aux_old)
+    aux = np.zeros(base + stride * len(pick), np.uint8)
+    aux[:base] = aux_old
+    for r, i in enumerate(pick):
+        wb = np.concatenate([rng.normal(0.0, 0.5, 64), rng.normal(0.0, 0.1, 8)]).astype(np.float32)
+        aux[base + r * stride: base + (r + 1) * stride] = wb.view(np.uint8)
+        c["cellFunction"][i] = 0
+        fd = np.zeros(8, np.uint64)
+        fd[0] = base + r * stride
+        acts = rng.integers(0, 5, 8).astype(np.int32)
+        fd.view(np.uint8)[8:40] = acts.view(np.uint8)
+        c["cellFunctionData"][i] = fd
+    return DataTO(c, data.particles.copy(), aux)

@@ -230,6 +230,11 @@ typedef struct AlienPhysicsParams {
     uint8_t advancedAbsorptionControl;        /* Features.h */
     uint8_t externalEnergyControl;            /* Features.h */
     uint8_t reserved[3];
+    /* cell functions: a cell with a function runs it in the steps where
+     * timestep % cellNumExecutionOrderNumbers equals its execution order
+     * number (CellFunctionProcessor.cuh:241-244); only the neuron function is
+     * part of this engine */
+    int32_t cellNumExecutionOrderNumbers;     /* :72 */
 } AlienPhysicsParams;
 
 /* Subset of RawStatisticsData (EngineGpuKernels/SimulationStatistics.cuh)

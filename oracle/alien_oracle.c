@@ -1030,6 +1030,125 @@ static void compact(OracleWorld* w)
 }
 
 /* ---- one timestep ---- */
+/* The neuron cell function: CellFunctionProcessor::collectCellFunctionOperations
+ * (CellFunctionProcessor.cuh:33-50) picks cells whose execution order number
+ * is timestep % cellNumExecutionOrderNumbers, not under construction or
+ * activating, activation time 0; NeuronProcessor::processCell
+ * (NeuronProcessor.cuh:33-74) with calcInputSignal (CellFunctionProcessor.cuh
+ * :128-164: bonded inputs of the input execution order number, each channel
+ * clamped to [-10, 10] after every addition, in bond order) and
+ * updateInvocationState (:176-186); activations NeuronProcessor.cuh:76-90.
+ * Weights and biases are read from the auxiliary data at
+ * NeuronTO.weightsAndBiasesDataIndex (TOs.cuh:45-49).  Inputs of a running
+ * neuron never run in the same step, so signals are read and written in one
+ * pass. */
+static real neuronActivation(int function, real x)
+{
+    switch (function) {
+    case 0: return 2 / (1 + exp(-x)) - 1;
+    case 1: return x >= (real)NEAR_ZERO ? 1 : 0;
+    case 2: return x < -1 ? -1 : (x > 1 ? 1 : x);
+    case 3: return fabs(x) < 1 ? fabs(x) : 1;
+    case 4: return exp(-2 * x * x);
+    }
+    return 0;
+}
+
+static void neuronPhase(OracleWorld* w, uint64_t T)
+{
+    const int64_t N = w->nCells;
+    const uint64_t orders = (uint64_t)(w->p.cellNumExecutionOrderNumbers > 0 ? w->p.cellNumExecutionOrderNumbers : 1);
+    for (int64_t i = 0; i < N; ++i) {
+        if (!w->alive[i] || w->cellFunction[i] != 0) continue;
+        AlienCellTO* me = &w->cold[i];
+        if ((uint64_t)me->executionOrderNumber != T % orders) continue;
+        int ls = w->livingState[i];
+        if (ls == ALIEN_B200_LIVING_UNDER_CONSTRUCTION || ls == ALIEN_B200_LIVING_ACTIVATING || w->activationTime[i] != 0) continue;
+        real in[ALIEN_B200_MAX_CHANNELS] = {0};
+        uint8_t origin = 0;
+        real tx = 0, ty = 0;
+        int inputOrder = me->inputExecutionOrderNumber;
+        if (inputOrder != -1 && inputOrder != (int)me->executionOrderNumber) {
+            int sensors = 0;
+            for (int k = 0; k < w->numConn[i]; ++k) {
+                int32_t j = w->bond[i][k];
+                const AlienCellTO* o = &w->cold[j];
+                int lsj = w->livingState[j];
+                if (o->outputBlocked || lsj == ALIEN_B200_LIVING_UNDER_CONSTRUCTION || lsj == ALIEN_B200_LIVING_ACTIVATING) continue;
+                if ((int)o->executionOrderNumber != inputOrder) continue;
+                for (int c = 0; c < ALIEN_B200_MAX_CHANNELS; ++c) {
+                    real v = in[c] + (real)o->signal.channels[c];
+                    in[c] = v < -10 ? -10 : (v > 10 ? 10 : v);
+                }
+                if (o->signal.origin == 1) {
+                    origin = 1;
+                    tx += o->signal.targetX;
+                    ty += o->signal.targetY;
+                    ++sensors;
+                }
+            }
+            if (sensors > 0) {
+                tx /= sensors;
+                ty /= sensors;
+            }
+        }
+        if (me->cellFunctionUsed == 0)
+            for (int c = 0; c < ALIEN_B200_MAX_CHANNELS - 1; ++c)
+                if (in[c] != 0) {
+                    me->cellFunctionUsed = 1;
+                    break;
+                }
+        float wb[ALIEN_B200_MAX_CHANNELS * (ALIEN_B200_MAX_CHANNELS + 1)];
+        if (me->cellFunctionData[0] > w->nAux || w->nAux - me->cellFunctionData[0] < sizeof(wb)) continue;
+        memcpy(wb, w->aux + me->cellFunctionData[0], sizeof(wb));
+        int32_t act[ALIEN_B200_MAX_CHANNELS];
+        memcpy(act, (const uint8_t*)me->cellFunctionData + 8, sizeof(act));
+        real out[ALIEN_B200_MAX_CHANNELS];
+        for (int r = 0; r < ALIEN_B200_MAX_CHANNELS; ++r) {
+            real sum = wb[ALIEN_B200_MAX_CHANNELS * ALIEN_B200_MAX_CHANNELS + r];
+            for (int c = 0; c < ALIEN_B200_MAX_CHANNELS; ++c) sum += (real)wb[r * ALIEN_B200_MAX_CHANNELS + c] * in[c];
+            out[r] = neuronActivation(act[r], sum);
+        }
+        for (int r = 0; r < ALIEN_B200_MAX_CHANNELS; ++r) me->signal.channels[r] = (float)out[r];
+        me->signal.origin = origin;
+        me->signal.targetX = (float)tx;
+        me->signal.targetY = (float)ty;
+    }
+}
+
+/* CellFunctionProcessor::resetFetchedSignals (CellFunctionProcessor.cuh:69-112),
+ * called by the friction kernel after the cell functions (SimulationKernels.cu
+ * :153-158): cells without function lose their signal channels every step;
+ * cells with a function in the step after the last of their readers ran. */
+static void signalReset(OracleWorld* w, uint64_t T)
+{
+    const int64_t N = w->nCells;
+    const int orders = w->p.cellNumExecutionOrderNumbers > 0 ? w->p.cellNumExecutionOrderNumbers : 1;
+    const int current = (int)(T % (uint64_t)orders);
+    for (int64_t i = 0; i < N; ++i) {
+        if (!w->alive[i]) continue;
+        AlienCellTO* me = &w->cold[i];
+        int reset = me->cellFunction == 11; /* CellFunction_None */
+        if (!reset) {
+            int own = me->executionOrderNumber, maxOther = -1;
+            if (!me->outputBlocked) {
+                for (int k = 0; k < w->numConn[i]; ++k) {
+                    const AlienCellTO* o = &w->cold[w->bond[i][k]];
+                    int other = o->executionOrderNumber;
+                    if (o->inputExecutionOrderNumber != own) continue;
+                    if (maxOther == -1)
+                        maxOther = other;
+                    else if ((maxOther > own && (other > maxOther || other < own)) || (maxOther < own && other > maxOther && other < own))
+                        maxOther = other;
+                }
+            }
+            reset = (maxOther == -1 && current == (own + 1) % orders) || (maxOther != -1 && maxOther == current);
+        }
+        if (reset)
+            for (int c = 0; c < ALIEN_B200_MAX_CHANNELS; ++c) me->signal.channels[c] = 0;
+    }
+}
+
 static void stepOnce(OracleWorld* w)
 {
     const AlienPhysicsParams* p = &w->p;
@@ -1162,6 +1281,10 @@ static void stepOnce(OracleWorld* w)
     for (int64_t i = 0; i < N; ++i)
         if (w->alive[i]) w->livingState[i] = nextState[i];
     free(nextState);
+
+    /* cellFunction_neuron (SimulationKernelsLauncher.cu:56) */
+    neuronPhase(w, T);
+    signalReset(w, T);
 
     /* applyInnerFriction (every third step, D4), applyFriction, decay
      * (CellProcessor.cuh:678-858) */

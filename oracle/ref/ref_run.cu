@@ -48,6 +48,7 @@ SimulationParameters toReference(AlienPhysicsParams const& a)
     SimulationParameters p;
     p.timestepSize = a.timestepSize;
     p.motionType = a.motionType;
+    p.cellNumExecutionOrderNumbers = a.cellNumExecutionOrderNumbers;
     if (a.motionType == MotionType_Fluid) {
         p.motionData.fluidMotion.smoothingLength = a.smoothingLength;
         p.motionData.fluidMotion.viscosityStrength = a.viscosityStrength;

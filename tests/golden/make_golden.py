@@ -35,6 +35,19 @@ ONE_STEP = [
 ]
 
 
+NEURON_RUNS = [
+    # name, seed, motion, timestep, steps: calm worlds with neuron cells; the
+    # steps cover every execution order number (6) and chains of neurons
+    ("neuron_fluid_t0", 41, P.MOTION_FLUID, 0, 13),
+    ("neuron_collision_t4", 42, P.MOTION_COLLISION, 4, 13),
+]
+
+
+def neuron_world(seed):
+    data, world = worldgen.calm_test_world(seed)
+    return worldgen.add_neurons(data, seed, fraction=0.6), world
+
+
 def one_step_params(motion, inner_friction):
     prm = P.benchmark_parameters(motion)
     if inner_friction is not None:
@@ -92,6 +105,17 @@ def main(out_dir):
                             params=np.frombuffer(bytes(prm), np.uint8),
                             meta=np.array([seed, motion, t, world[0], world[1], ts], np.int64))
         print(name, out.num_cells, out.num_particles, ts)
+    for name, seed, motion, t, steps in NEURON_RUNS:
+        data, world = neuron_world(seed)
+        prm = P.benchmark_parameters(motion)
+        out, _, ts = refrun.run(data, world, prm, steps=steps, timestep=t)
+        np.savez_compressed(os.path.join(out_dir, f"refneuron_{name}.npz"), in_cells=data.cells,
+                            in_particles=data.particles, in_aux=data.aux, out_cells=out.cells,
+                            params=np.frombuffer(bytes(prm), np.uint8),
+                            meta=np.array([seed, motion, t, world[0], world[1], ts, steps], np.int64))
+        print(name, out.num_cells, ts)
+    if os.environ.get("NEURON_ONLY"):
+        return
     summary = {}
     for name, (builder, motion, steps) in LONG_RUNS.items():
         data, world = builder()

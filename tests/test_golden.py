@@ -11,7 +11,12 @@ B200 by tests/golden/make_golden.py.  These CPU tests pin the oracle:
   sums forces with float atomics, so it is not bit-reproducible itself;
 * long runs: aggregate observables (counts, energy, mean speed, speed
   histogram) agree statistically, since the reference's races make its
-  trajectories nondeterministic.
+  trajectories nondeterministic;
+* neuron cells over 13 steps (every execution order number, chains of
+  neurons): signals, signal origins and targets, and the function-used flag
+  of every cell within NEURON_ATOL (the reference evaluates activations with
+  the fast-math exponential and adds the 64 weight products with shared-
+  memory atomics in arbitrary order).
 """
 import glob
 import json
@@ -55,7 +60,12 @@ def test_oracle_matches_reference_one_step(path):
     assert np.array_equal(data.cells, f["in_cells"]) and np.array_equal(data.particles, f["in_particles"]), \
         "the seeded generator no longer reproduces the fixture input"
     if "params" in f:
-        prm = P.PhysicsParams.from_buffer_copy(f["params"].tobytes())
+        raw = f["params"].tobytes()
+        # fixtures written before a field was appended to the struct keep the
+        # defaults for the appended fields
+        full = bytearray(bytes(P.default_parameters()))
+        full[: len(raw)] = raw
+        prm = P.PhysicsParams.from_buffer_copy(bytes(full))
     else:
         prm = P.benchmark_parameters(motion)
     o = OracleSimulation(world, prm, t)
@@ -118,3 +128,34 @@ def test_decay_matches_reference():
     e_got = got["cell_energy"] + got["particle_energy"]
     e_ref = ref["final"]["cell_energy"] + ref["final"]["particle_energy"]
     assert abs(e_got - e_ref) / e_ref < 1e-3
+
+
+NEURON_ATOL = 1e-4
+NEURON_FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "refneuron_*.npz")))
+
+
+@pytest.mark.parametrize("path", NEURON_FIXTURES, ids=[os.path.basename(p) for p in NEURON_FIXTURES])
+def test_oracle_neurons_match_reference(path):
+    f = np.load(path)
+    seed, motion, t, wx, wy, ts, steps = (int(v) for v in f["meta"])
+    data, world = make_golden.neuron_world(seed)
+    assert world == (wx, wy)
+    assert np.array_equal(data.cells, f["in_cells"]) and np.array_equal(data.aux, f["in_aux"]), \
+        "the seeded generator no longer reproduces the fixture input"
+    prm = P.PhysicsParams.from_buffer_copy(f["params"].tobytes())
+    o = OracleSimulation(world, prm, t)
+    o.set_simulation_data(data)
+    o.calc_timesteps(steps)
+    assert o.current_timestep() == ts
+    got = o.get_simulation_data().cells
+    ref = f["out_cells"]
+    gi, ri = np.argsort(got["id"]), np.argsort(ref["id"])
+    got, ref = got[gi], ref[ri]
+    assert np.array_equal(got["id"], ref["id"])
+    assert np.array_equal(got["cellFunctionUsed"], ref["cellFunctionUsed"])
+    assert np.array_equal(got["signalOrigin"], ref["signalOrigin"])
+    np.testing.assert_allclose(got["signalChannels"], ref["signalChannels"], rtol=0, atol=NEURON_ATOL)
+    np.testing.assert_allclose(got["signalTargetX"], ref["signalTargetX"], rtol=1e-5, atol=NEURON_ATOL)
+    np.testing.assert_allclose(got["signalTargetY"], ref["signalTargetY"], rtol=1e-5, atol=NEURON_ATOL)
+    neurons = data.cells["cellFunction"][np.argsort(data.cells["id"])] == 0
+    assert np.any(np.any(got["signalChannels"][neurons] != data.cells["signalChannels"][np.argsort(data.cells["id"])][neurons], axis=1))
