@@ -87,7 +87,10 @@ struct WorldCounters {
     unsigned int pad2;
     // events counted this step (radiation, deleted cells, particle splits):
     // the event scans run only when there are any
-    unsigned int evRad, evDel, evSplit, pad3;
+    unsigned int evRad, evDel, evSplit;
+    // set at ingest: the next step clears the signals of cells without
+    // function (after that no step writes them)
+    unsigned int signalsFresh;
 };
 
 struct DevState {
@@ -127,8 +130,11 @@ struct DevState {
     uint32_t* creatureId;
     uint32_t* coldIdx;
     AlienCellTO* cold;        // ingest copies (signals and cellFunctionUsed of neuron cells change here)
-    const int* neuronRow;     // neuron table row of a neuron cell, -1 otherwise (null without neurons)
-    const float* neuronTable; // per neuron cell: weights [8 x 8] row-major, then 8 biases
+    uchar4* fnInfo;           // per cell: (function: 0 none / 1 neuron, execution order, input order as int8, output
+                              // blocked); null when no cell has a function or a signal
+    const long long* neuronList;  // arena slots of the neuron cells
+    const float* neuronTable; // per neuron (list order): weights [8 x 8] row-major, then 8 biases
+    int numNeurons;
     int* bond;          // [slot * 6 + k] partner slot
     float* bondDist;
     float* bondAngle;

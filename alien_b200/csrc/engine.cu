@@ -457,18 +457,21 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     stats_ = mem_.alloc<StatsAcc>(n);
     cold_ = mem_.alloc<AlienCellTO>(static_cast<size_t>(coldTotal));
     s.cold = cold_;
-    s.neuronRow = nullptr;
+    s.fnInfo = nullptr;
+    s.neuronList = nullptr;
     s.neuronTable = nullptr;
+    s.numNeurons = static_cast<int>(neuronCells.size());
+    if (signalsLive_) s.fnInfo = mem_.alloc<uchar4>(C);  // filled by kIngestCells
     if (hasNeurons_) {
-        int* rowDev = mem_.alloc<int>(C);
+        long long* listDev = mem_.alloc<long long>(neuronCells.size());
         float* tableDev = mem_.alloc<float>(neuronTableHost.size());
-        std::vector<int> rowHost(C, -1);
-        for (const auto& nc : neuronCells) rowHost[static_cast<size_t>(nc.first)] = nc.second;
-        AB_CK(cudaMemcpyAsync(rowDev, rowHost.data(), sizeof(int) * C, cudaMemcpyHostToDevice, stream_));
+        std::vector<long long> listHost(neuronCells.size());
+        for (const auto& nc : neuronCells) listHost[static_cast<size_t>(nc.second)] = nc.first;
+        AB_CK(cudaMemcpyAsync(listDev, listHost.data(), sizeof(long long) * listHost.size(), cudaMemcpyHostToDevice, stream_));
         AB_CK(cudaMemcpyAsync(tableDev, neuronTableHost.data(), sizeof(float) * neuronTableHost.size(), cudaMemcpyHostToDevice,
                               stream_));
         AB_CK(cudaStreamSynchronize(stream_));  // the host vectors end with this scope
-        s.neuronRow = rowDev;
+        s.neuronList = listDev;
         s.neuronTable = tableDev;
     }
     rankCells_ = mem_.alloc<int>(C);
@@ -496,6 +499,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         wc.numParticles = static_cast<unsigned int>(setups[w].numParticles);
         wc.stepsRemaining = ~0ull;
         wc.active = 1;
+        wc.signalsFresh = 1;
     }
     AB_CK(cudaMemcpyAsync(worldsDev, infos.data(), sizeof(WorldInfo) * n, cudaMemcpyHostToDevice, stream_));
     AB_CK(cudaMemcpyAsync(paramsDev, params.data(), sizeof(AlienPhysicsParams) * n, cudaMemcpyHostToDevice, stream_));
@@ -570,7 +574,7 @@ void Arena::enqueueStep()
     launch(kVerletVel, both, kBlock, s);
     launch(kTransition, both, kBlock, s);
     launch(kResolve, cells, kBlock, s);
-    if (hasNeurons_) launch(kNeuron, cells, kBlock, s);
+    if (hasNeurons_) launch(kNeuron, divUp(s.numNeurons, kBlock), kBlock, s);
     if (signalsLive_) launch(kSignalReset, cells, kBlock, s);
     launch(kCommit, cells, kBlock, s);
     launch(kEventCount, both, kBlock, s);

@@ -41,6 +41,9 @@ __global__ void __launch_bounds__(kBlock) kIngestCells(DevState s, int w, const 
     s.age[g] = c.age;
     s.activationTime[g] = c.activationTime;
     s.creatureId[g] = c.creatureId;
+    if (s.fnInfo)
+        s.fnInfo[g] = make_uchar4(c.cellFunction == kCellFunctionNeuron ? 1 : 0, c.executionOrderNumber,
+                                  static_cast<uint8_t>(c.inputExecutionOrderNumber), c.outputBlocked ? 1 : 0);
     for (int k = 0; k < kMaxBonds; ++k) {
         const bool used = k < n6;
         s.bond[g * kMaxBonds + k] = used ? static_cast<int>(wi.cellBase + c.connections[k].cellIndex) : -1;

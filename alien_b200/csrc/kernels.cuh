@@ -1289,39 +1289,41 @@ __device__ __forceinline__ float neuronActivation(int function, float x)
 
 __global__ void __launch_bounds__(kBlock) kNeuron(DevState s)
 {
-    CellCtx c = cellCtx(s);
-    if (!c.valid) return;
-    const long long g = c.g;
-    const int row = s.neuronRow[g];
-    if (row < 0) return;
-    AlienCellTO& me = s.cold[s.coldIdx[g]];
-    const AlienPhysicsParams& p = s.params[c.w];
-    const uint64_t T = s.counters[c.w].timestep;
-    if (static_cast<uint64_t>(me.executionOrderNumber) != T % static_cast<uint64_t>(p.cellNumExecutionOrderNumbers)) return;
+    const int row = blockIdx.x * kBlock + threadIdx.x;
+    if (row >= s.numNeurons) return;
+    const long long g = s.neuronList[row];
+    const int w = s.cellBlockWorld[g / kBlock];
+    const WorldCounters& wc = s.counters[w];
+    if (!wc.active || g >= s.worlds[w].cellBase + wc.numCells || !s.alive[g]) return;
+    const uchar4 fi = s.fnInfo[g];
+    const AlienPhysicsParams& p = s.params[w];
+    if (static_cast<uint64_t>(fi.y) != wc.timestep % static_cast<uint64_t>(p.cellNumExecutionOrderNumbers)) return;
     const int ls = s.livingState[g];
     if (ls == ALIEN_B200_LIVING_UNDER_CONSTRUCTION || ls == ALIEN_B200_LIVING_ACTIVATING || s.activationTime[g] != 0) return;
+    AlienCellTO& me = s.cold[s.coldIdx[g]];
 
     float in[ALIEN_B200_MAX_CHANNELS];
 #pragma unroll
     for (int ch = 0; ch < ALIEN_B200_MAX_CHANNELS; ++ch) in[ch] = 0.0f;
     uint8_t origin = 0;
     float tx = 0.0f, ty = 0.0f;
-    const int inputOrder = me.inputExecutionOrderNumber;
-    if (inputOrder != -1 && inputOrder != static_cast<int>(me.executionOrderNumber)) {
+    const int inputOrder = static_cast<int8_t>(fi.z);
+    if (inputOrder != -1 && inputOrder != static_cast<int>(fi.y)) {
         int sensors = 0;
         const int n = s.numConn[g];
         for (int k = 0; k < n; ++k) {
             const int j = s.bond[g * kMaxBonds + k];
-            const AlienCellTO& o = s.cold[s.coldIdx[j]];
+            const uchar4 fj = s.fnInfo[j];
             const int lsj = s.livingState[j];
-            if (o.outputBlocked || lsj == ALIEN_B200_LIVING_UNDER_CONSTRUCTION || lsj == ALIEN_B200_LIVING_ACTIVATING) continue;
-            if (static_cast<int>(o.executionOrderNumber) != inputOrder) continue;
+            if (fj.w || lsj == ALIEN_B200_LIVING_UNDER_CONSTRUCTION || lsj == ALIEN_B200_LIVING_ACTIVATING) continue;
+            if (static_cast<int>(fj.y) != inputOrder) continue;
+            const AlienSignalTO& sig = s.cold[s.coldIdx[j]].signal;
 #pragma unroll
-            for (int ch = 0; ch < ALIEN_B200_MAX_CHANNELS; ++ch) in[ch] = fmaxf(-10.0f, fminf(10.0f, in[ch] + o.signal.channels[ch]));
-            if (o.signal.origin == 1) {  // SignalOrigin_Sensor
+            for (int ch = 0; ch < ALIEN_B200_MAX_CHANNELS; ++ch) in[ch] = fmaxf(-10.0f, fminf(10.0f, in[ch] + sig.channels[ch]));
+            if (sig.origin == 1) {  // SignalOrigin_Sensor
                 origin = 1;
-                tx += o.signal.targetX;
-                ty += o.signal.targetY;
+                tx += sig.targetX;
+                ty += sig.targetY;
                 ++sensors;
             }
         }
@@ -1366,19 +1368,23 @@ __global__ void __launch_bounds__(kBlock) kSignalReset(DevState s)
     CellCtx c = cellCtx(s);
     if (!c.valid) return;
     const long long g = c.g;
-    AlienCellTO& me = s.cold[s.coldIdx[g]];
-    bool reset = me.cellFunction == kCellFunctionNone;
-    if (!reset) {
+    const uchar4 fi = s.fnInfo[g];
+    bool reset;
+    if (fi.x == 0) {
+        // without function: cleared every step, so only the first step after
+        // ingest finds anything to clear
+        reset = s.counters[c.w].signalsFresh != 0;
+    } else {
         const int orders = s.params[c.w].cellNumExecutionOrderNumbers;
         const int current = static_cast<int>(s.counters[c.w].timestep % static_cast<uint64_t>(orders));
-        const int own = me.executionOrderNumber;
+        const int own = fi.y;
         int maxOther = -1;
-        if (!me.outputBlocked) {
+        if (!fi.w) {
             const int n = s.numConn[g];
             for (int k = 0; k < n; ++k) {
-                const AlienCellTO& o = s.cold[s.coldIdx[s.bond[g * kMaxBonds + k]]];
-                const int other = o.executionOrderNumber;
-                if (o.inputExecutionOrderNumber != own) continue;
+                const uchar4 fo = s.fnInfo[s.bond[g * kMaxBonds + k]];
+                const int other = fo.y;
+                if (static_cast<int8_t>(fo.z) != own) continue;
                 if (maxOther == -1) {
                     maxOther = other;
                 } else if ((maxOther > own && (other > maxOther || other < own)) || (maxOther < own && other > maxOther && other < own)) {
@@ -1389,8 +1395,9 @@ __global__ void __launch_bounds__(kBlock) kSignalReset(DevState s)
         reset = (maxOther == -1 && current == (own + 1) % orders) || (maxOther != -1 && maxOther == current);
     }
     if (reset) {
+        AlienSignalTO& sig = s.cold[s.coldIdx[g]].signal;
 #pragma unroll
-        for (int ch = 0; ch < ALIEN_B200_MAX_CHANNELS; ++ch) me.signal.channels[ch] = 0.0f;
+        for (int ch = 0; ch < ALIEN_B200_MAX_CHANNELS; ++ch) sig.channels[ch] = 0.0f;
     }
 }
 
@@ -1710,6 +1717,7 @@ __global__ void __launch_bounds__(kBlock) kEventWorld(DevState s)
         wc.numParticles = static_cast<uint32_t>(want);
     }
     wc.timestep += 1;
+    wc.signalsFresh = 0;
     if (wc.stepsRemaining != ~0ull && --wc.stepsRemaining == 0) wc.active = 0;
 }
 

@@ -154,6 +154,16 @@ def build_workload(config: str, rank: int = 0):
         data, world = worldgen.hex_world(seed=seed, world=(2048, 2048), clusters=10000)
         prm = P.benchmark_parameters(P.MOTION_COLLISION)
         desc = "soft-body, profiling size: 2048x2048 torus, 1M cells in 10k hexagonal 100-cell clusters"
+    elif config == "neuron1m":
+        import numpy as np
+        data, world = worldgen.hex_world(seed=seed, world=(2048, 2048), clusters=10000)
+        rng = np.random.default_rng(seed + 1)
+        chosen = np.nonzero(rng.random(10000) < 1.0 / 3.0)[0]
+        cells = (chosen[:, None] * 100 + np.arange(100)[None, :]).ravel()
+        data = worldgen.add_neurons(data, seed + 2, fraction=1.0, cells=cells)
+        prm = P.benchmark_parameters(P.MOTION_COLLISION)
+        desc = ("soft-body with neurons: hex1m with a third of the clusters made of neuron cells "
+                "(8x8 weights ~ N(0, 0.5), biases ~ N(0, 0.1))")
     elif config == "fluid1m":
         data, world = worldgen.fluid_world(seed=seed)
         prm = P.benchmark_parameters(P.MOTION_FLUID)
@@ -378,7 +388,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="hex4m",
-                    choices=["hex4m", "hex1m", "fluid1m", "softbody", "batched256", "serving"])
+                    choices=["hex4m", "hex1m", "neuron1m", "fluid1m", "softbody", "batched256", "serving"])
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: mean requests per second")
     ap.add_argument("--pool", type=int, default=32, help="serving: distinct request worlds")
