@@ -364,7 +364,14 @@ def run_serving(args, rank):
     sizes = np.exp(rng.uniform(math.log(5_000), math.log(500_000), args.pool)).astype(int)
     pool = []
     for i, n in enumerate(sizes):
-        pool.append(worldgen.mixed_world(seed=100_000 * rank + i, num_cells=int(n)))
+        d, w = worldgen.mixed_world(seed=100_000 * rank + i, num_cells=int(n))
+        # a third of the lattice clusters (the first cells, 100 per cluster)
+        # are made of neuron cells
+        n_clusters = int(np.sum(d.cells["numConnections"] > 0) // 100)
+        chosen = np.nonzero(rng.random(n_clusters) < 1.0 / 3.0)[0]
+        d = worldgen.add_neurons(d, 100_000 * rank + i, fraction=1.0,
+                                 cells=(chosen[:, None] * 100 + np.arange(100)[None, :]).ravel())
+        pool.append((d, w))
     log(f"serving: pool of {len(pool)} worlds, {sum(d.num_cells for d, _ in pool)} cells")
     prm = P.benchmark_parameters(P.MOTION_FLUID)
 
@@ -426,7 +433,8 @@ def main():
                 "config": {"workload": "serving", "rate_per_s": args.rate, "duration_s": args.duration,
                            "hbm_budget_gb": args.hbm_budget_gb, "pool_worlds": args.pool,
                            "description": "Poisson arrivals, worlds of log-uniform 5k-500k cells (half fluid, half "
-                                          "10x10 lattices), log-uniform 100-5000 steps, continuous batching"},
+                                          "10x10 lattices, a third of the lattices neuron cells), log-uniform "
+                                          "100-5000 steps, continuous batching"},
                 "p50_step_ms": r["p50_step_ms"], "p99_step_ms": r["p99_step_ms"],
                 "requests": {"submitted": r["requests_submitted"], "finished": r["requests_finished"],
                              "waiting": r["requests_waiting"]},
