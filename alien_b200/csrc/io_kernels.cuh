@@ -15,6 +15,53 @@
 namespace ab {
 
 // ---- ingest ----
+// Checks of the transfer objects, run on the uploaded copy before the arena
+// changes: counts of cells with more than 6 bonds, bond indices outside the
+// array, cell functions other than neuron / none, neuron data outside the
+// auxiliary data, neurons and nonzero signal channels (block counts, one
+// atomic per block and counter).
+struct IngestCheck {
+    unsigned int badBondCount, badBondIndex, otherFunction, neuronOutOfAux, neurons, nonzeroSignal;
+};
+
+__global__ void __launch_bounds__(kBlock) kCheckCells(const AlienCellTO* to, long long n, unsigned long long numAux,
+                                                      IngestCheck* out)
+{
+    const long long i = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    bool badCount = false, badIndex = false, other = false, outOfAux = false, neuron = false, signal = false;
+    if (i < n) {
+        const AlienCellTO& c = to[i];
+        if (c.numConnections > kMaxBonds) {
+            badCount = true;
+        } else {
+            for (int k = 0; k < c.numConnections; ++k) {
+                const int idx = c.connections[k].cellIndex;
+                if (idx < 0 || idx >= n) badIndex = true;
+            }
+        }
+        if (c.cellFunction == kCellFunctionNeuron) {
+            neuron = true;
+            const unsigned long long at = c.cellFunctionData[0];
+            const unsigned long long bytes = sizeof(float) * ALIEN_B200_MAX_CHANNELS * (ALIEN_B200_MAX_CHANNELS + 1);
+            outOfAux = at > numAux || numAux - at < bytes;
+        } else if (c.cellFunction != kCellFunctionNone) {
+            other = true;
+        }
+#pragma unroll
+        for (int ch = 0; ch < ALIEN_B200_MAX_CHANNELS; ++ch) signal |= c.signal.channels[ch] != 0.0f;
+    }
+    const int nBadCount = __syncthreads_count(badCount), nBadIndex = __syncthreads_count(badIndex);
+    const int nOther = __syncthreads_count(other), nOutOfAux = __syncthreads_count(outOfAux);
+    const int nNeuron = __syncthreads_count(neuron), nSignal = __syncthreads_count(signal);
+    if (threadIdx.x == 0) {
+        if (nBadCount) atomicAdd(&out->badBondCount, static_cast<unsigned int>(nBadCount));
+        if (nBadIndex) atomicAdd(&out->badBondIndex, static_cast<unsigned int>(nBadIndex));
+        if (nOther) atomicAdd(&out->otherFunction, static_cast<unsigned int>(nOther));
+        if (nOutOfAux) atomicAdd(&out->neuronOutOfAux, static_cast<unsigned int>(nOutOfAux));
+        if (nNeuron) atomicAdd(&out->neurons, static_cast<unsigned int>(nNeuron));
+        if (nSignal) atomicAdd(&out->nonzeroSignal, static_cast<unsigned int>(nSignal));
+    }
+}
 __global__ void __launch_bounds__(kBlock) kIngestCells(DevState s, int w, const AlienCellTO* to, long long n, AlienCellTO* cold,
                                                        long long coldBase)
 {

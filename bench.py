@@ -517,12 +517,18 @@ def main():
         barrier()
         t0 = time.perf_counter()
         sim2.set_simulation_data(data)
+        t_set = time.perf_counter()
         for _ in range(e2e_steps):
             sim2.calc_timesteps(1)
             sim2.get_raw_statistics()
+        t_steps = time.perf_counter()
         sim2.get_simulation_data(out=out)
         barrier()
-        t_e2e = max_over_ranks(time.perf_counter() - t0)
+        t_end = time.perf_counter()
+        t_e2e = max_over_ranks(t_end - t0)
+        log(f"e2e: set_simulation_data {1e3 * (t_set - t0):.1f} ms, {e2e_steps} x (calc_timesteps(1) + "
+            f"get_raw_statistics) {1e3 * (t_steps - t_set) / e2e_steps:.3f} ms each, get_simulation_data "
+            f"{1e3 * (t_end - t_steps):.1f} ms")
         sim2.close_simulation()
         for p in pins + out_pins:
             unpin(p)
