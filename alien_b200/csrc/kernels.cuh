@@ -332,10 +332,10 @@ struct FluidLaw {
     const DevState* s;
     const AlienPhysicsParams* p;
     int g, W, H;
-    float h, R, R2reject, minDist, fusionVelocity, maxBindingEnergy;
+    float h, invH, invH2, invH3, R, R2reject, minDist, fusionVelocity, maxBindingEnergy;
     float2 pi, vi;
     bool barrierI, fusionI;
-    float densI;
+    float densI, invDensI;
     int bondsI[kMaxBonds];
     float dens;
     float2 Fp, Fv, dx;
@@ -352,6 +352,9 @@ struct FluidLaw {
         W = wi.W;
         H = wi.H;
         h = p->smoothingLength;
+        invH = 1.0f / h;
+        invH2 = invH * invH;
+        invH3 = invH2 * invH;
         R = h * 2.0f;
         R2reject = R * R * 1.0001f + 1e-6f;
         minDist = p->cellMinDistance;
@@ -362,6 +365,7 @@ struct FluidLaw {
         barrierI = me.y & kStageBarrier;
         const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
         densI = __int_as_float(me.z);
+        invDensI = __frcp_rn(densI);
         fusionI = !barrierI && nI < maxI && __int_as_float(me.w) <= maxBindingEnergy;
 #pragma unroll
         for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? st.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
@@ -390,17 +394,19 @@ struct FluidLaw {
             }
             return;
         }
-        dens += sphKernel(d / h) / (h * h);
+        const float q = d * invH;
+        dens += sphKernel(q) * invH2;
         if (j == g) return;
         if (!barrierI && d < minDist) dx = dx + pd * (minDist / 5.0f);
         if (isBondedTo(bondsI, j)) return;
         const float2 vd = vi - vj;
-        const float densJ = __int_as_float(om.z);
-        const float factor = densI / (densI * densI) + densJ / (densJ * densJ);
+        // rho_i / rho_i^2 + rho_j / rho_j^2 (CellProcessor.cuh:205) as reciprocals
+        const float invDensJ = __frcp_rn(__int_as_float(om.z));
+        const float factor = invDensI + invDensJ;
         if (fabsf(d) > kNearZero) {
-            const float kd = sphKernelD(d / h) / (h * h * h);
-            Fp = Fp + pd / (-d) * factor * kd;
-            Fv = Fv + vd / densJ * d * kd / (d * d + 0.25f);
+            const float kd = sphKernelD(q) * invH3;
+            Fp = Fp + pd * (-factor * kd * __frcp_rn(d));
+            Fv = Fv + vd * (invDensJ * d * kd * __frcp_rn(d * d + 0.25f));
         }
         if (fusionI && len2(vd) >= fusionVelocity) {
             const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
@@ -850,7 +856,8 @@ __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, cons
     const long long bb = g * kMaxBonds;
     const float si = s.stiffness[g];
     const float s2 = si * si;
-    float sj[kMaxBonds], bd[kMaxBonds];
+    float sj[kMaxBonds], bd[kMaxBonds], len[kMaxBonds];
+    float2 nrm[kMaxBonds];  // Math::normalized: unit vector, (1, 0) below NEAR_ZERO
     const float2* bdRow = reinterpret_cast<const float2*>(s.bondDist + bb);
 #pragma unroll
     for (int h = 0; h < kMaxBonds / 2; ++h) {
@@ -862,28 +869,39 @@ __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, cons
     for (int k = 0; k < kMaxBonds; ++k) sj[k] = k < n ? s.stiffness[r.j[k]] : 0.0f;
 #pragma unroll
     for (int k = 0; k < kMaxBonds; ++k) {
-        if (k < n) {
-            const float2 disp = r.disp[k];
-            const float dev = len2(disp) - bd[k];
-            F = F + normalized2(disp) * dev * (s2 + sj[k] * sj[k]) / 6.0f;
-        }
+        len[k] = len2(r.disp[k]);
+        const float inv = __frcp_rn(len[k]);
+        nrm[k] = len[k] > kNearZero ? r.disp[k] * inv : f2(1.0f, 0.0f);
     }
+    // spring forces in bond order: normalized(d) * (|d| - rest) * (s_i^2 + s_j^2) / 6
+#pragma unroll
+    for (int k = 0; k < kMaxBonds; ++k)
+        if (k < n) F = F + nrm[k] * ((len[k] - bd[k]) * (s2 + sj[k] * sj[k]) * (1.0f / 6.0f));
     if (!considerAngles || n < 2) return F;
     // angle forces: partner rows for the triangle test, then the forces in bond order
     int nj[kMaxBonds];
+    float ang[kMaxBonds];  // angle of every bond vector, once
 #pragma unroll
     for (int k = 0; k < kMaxBonds; ++k) nj[k] = k < n ? s.numConn[r.j[k]] : 0;
+#pragma unroll
+    for (int k = 0; k < kMaxBonds; ++k) {
+        const float a = 90.0f - atan2f(-r.disp[k].y, r.disp[k].x) * (180.0f / kPi);
+        ang[k] = k < n && len[k] >= kNearZero ? (a < 0.0f ? a + 360.0f : a) : 0.0f;
+    }
 #pragma unroll
     for (int k = 0; k < kMaxBonds; ++k) {
         if (k >= n || !(n > 2 || k == 0)) continue;
         const int last = k == 0 ? n - 1 : k - 1;
         int jl = r.j[0];
-        float2 prevDisp = r.disp[0];
+        float pa = ang[0], lenPrev = len[0];
+        float2 nrmPrev = nrm[0];
 #pragma unroll
         for (int m = 1; m < kMaxBonds; ++m)
             if (m == last) {
                 jl = r.j[m];
-                prevDisp = r.disp[m];
+                pa = ang[m];
+                lenPrev = len[m];
+                nrmPrev = nrm[m];
             }
         const int j = r.j[k];
         const int2* prow = reinterpret_cast<const int2*>(s.bond + static_cast<long long>(j) * kMaxBonds);
@@ -897,18 +915,13 @@ __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, cons
             }
         }
         if (tri) continue;
-        const float2 disp = r.disp[k];
-        const float a = angleOfVector(disp), pa = angleOfVector(prevDisp);
-        const float act = subtractAngle(a, pa);
+        const float act = subtractAngle(ang[k], pa);
         if (act < 0.0f) continue;
         const float ref = s.bondAngle[bb + k];
-        const float strength = fabsf(ref - act) / 2000.0f * s2;
-        float2 f1 = rotCW(normalized2(disp) / fmaxf(len2(disp), minDist) * strength);
-        float2 f2v = rotCCW(normalized2(prevDisp) / fmaxf(len2(prevDisp), minDist) * strength);
-        if (ref < act) {
-            f1 = f1 * -1.0f;
-            f2v = f2v * -1.0f;
-        }
+        const float strength = fabsf(ref - act) * (1.0f / 2000.0f) * s2;
+        const float sign = ref < act ? -1.0f : 1.0f;
+        const float2 f1 = rotCW(nrm[k] * (sign * strength * __frcp_rn(fmaxf(len[k], minDist))));
+        const float2 f2v = rotCCW(nrmPrev * (sign * strength * __frcp_rn(fmaxf(lenPrev, minDist))));
         if (!s.barrier[j]) {
             atomicAdd(reinterpret_cast<unsigned long long*>(&s.angleAcc[4LL * j + accOffset]),
                       static_cast<unsigned long long>(toFix(f1.x)));
@@ -930,7 +943,7 @@ __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, cons
 // cells: checkForces + applyForces (CellProcessor.cuh:367-406), bond forces
 // #1 at the overlap-corrected positions.  particles: movement
 // (RadiationProcessor::movement, RadiationProcessor.cuh:61-70).
-__global__ void __launch_bounds__(kBlock, 8) kApplyBond1(DevState s)
+__global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         CellCtx c = cellCtx(s);
@@ -1006,7 +1019,7 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletPos(DevState s)
 // cells: checkConnections (CellProcessor.cuh:493-523) at the new positions,
 // bond forces #2.  particles: merges into particles that do not merge
 // themselves (RadiationProcessor.cuh:82-96 under the fixed rule).
-__global__ void __launch_bounds__(kBlock, 8) kBond2(DevState s)
+__global__ void __launch_bounds__(kBlock, 6) kBond2(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         CellCtx c = cellCtx(s);
