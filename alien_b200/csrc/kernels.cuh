@@ -1173,22 +1173,52 @@ __global__ void __launch_bounds__(kBlock, 8) kTransition(DevState s)
         const WorldInfo& wi = s.worlds[c.w];
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
         const uint64_t T = s.counters[c.w].timestep;
+        const bool innerFriction = T % 3 == 0;  // SimulationKernelsLauncher.cu:32
         const int n = s.numConn[g];
         const uint32_t cr = s.creatureId[g];
         bool sameDetaching = false, otherDetaching = false, sameReviving = false, activating = false;
         float2 acc = f2(0.0f, 0.0f);
         const float2 vi = s.velB[g];
-        for (int k = 0; k < n; ++k) {
-            const int j = s.bond[g * kMaxBonds + k];
-            const int ls = s.livingState[j];
-            if (s.creatureId[j] == cr) {
+        // the bond row, then the partners' states (and velocities on inner-
+        // friction steps) with all loads of a cell in flight together
+        int jb[kMaxBonds];
+        const int2* row = reinterpret_cast<const int2*>(s.bond + g * kMaxBonds);
+#pragma unroll
+        for (int h = 0; h < kMaxBonds / 2; ++h) {
+            const int2 jj = 2 * h < n ? row[h] : make_int2(0, 0);
+            jb[2 * h] = jj.x;
+            jb[2 * h + 1] = jj.y;
+        }
+        int lsj[kMaxBonds];
+        uint32_t crj[kMaxBonds];
+#pragma unroll
+        for (int k = 0; k < kMaxBonds; ++k) {
+            lsj[k] = k < n ? s.livingState[jb[k]] : ALIEN_B200_LIVING_READY;
+            crj[k] = k < n ? s.creatureId[jb[k]] : cr;
+        }
+#pragma unroll
+        for (int k = 0; k < kMaxBonds; ++k) {
+            if (k >= n) continue;
+            const int ls = lsj[k];
+            if (crj[k] == cr) {
                 if (ls == ALIEN_B200_LIVING_DETACHING) sameDetaching = true;
                 else if (ls == ALIEN_B200_LIVING_REVIVING) sameReviving = true;
                 else if (ls == ALIEN_B200_LIVING_ACTIVATING) activating = true;
             } else if (ls == ALIEN_B200_LIVING_DETACHING) {
                 otherDetaching = true;
             }
-            if (!s.barrier[j]) acc = acc + (s.velB[j] - vi);
+        }
+        if (innerFriction) {
+            float2 vj[kMaxBonds];
+            uint8_t bj[kMaxBonds];
+#pragma unroll
+            for (int k = 0; k < kMaxBonds; ++k) {
+                bj[k] = k < n ? s.barrier[jb[k]] : 1;
+                vj[k] = k < n ? s.velB[jb[k]] : vi;
+            }
+#pragma unroll
+            for (int k = 0; k < kMaxBonds; ++k)
+                if (k < n && !bj[k]) acc = acc + (vj[k] - vi);
         }
         const int orig = s.livingState[g];
         int ls = orig;
@@ -1220,7 +1250,7 @@ __global__ void __launch_bounds__(kBlock, 8) kTransition(DevState s)
         }
         // applyInnerFriction (every third step) + applyFriction
         // (CellProcessor.cuh:678-723)
-        const float2 vf = T % 3 == 0 ? vi + acc * (p.innerFriction / 2.0f) : vi;
+        const float2 vf = innerFriction ? vi + acc * (p.innerFriction / 2.0f) : vi;
         s.velA[g] = vf * (1.0f - p.friction);
         // decay (CellProcessor.cuh:775-858) on the state after the transition
         const int col = s.color[g] % ALIEN_B200_MAX_COLORS;
@@ -1559,6 +1589,7 @@ __global__ void __launch_bounds__(kBlock, 8) kCommit(DevState s)
         return;
     }
     const int np = s.newPartner[g];
+    const bool delAllG = f & kFlagDelAll;
     BondList l;
     if (np >= 0) {
         s.newPartner[g] = -1;
@@ -1569,9 +1600,27 @@ __global__ void __launch_bounds__(kBlock, 8) kCommit(DevState s)
             l.a[k] = s.addAngle[g * kMaxBonds + k];
         }
     } else {
+        // most cells keep their bonds: look at the partners' flags first and
+        // read rest lengths and angles only when a bond goes
+        const int n = s.numConn[g];
+        int jb[kMaxBonds];
+        const int2* row = reinterpret_cast<const int2*>(s.bond + g * kMaxBonds);
+#pragma unroll
+        for (int h = 0; h < kMaxBonds / 2; ++h) {
+            const int2 jj = 2 * h < n ? row[h] : make_int2(0, 0);
+            jb[2 * h] = jj.x;
+            jb[2 * h + 1] = jj.y;
+        }
+        uint32_t fj[kMaxBonds];
+#pragma unroll
+        for (int k = 0; k < kMaxBonds; ++k) fj[k] = k < n ? s.flags[jb[k]] : 0u;
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < kMaxBonds; ++k)
+            any |= k < n && ((fj[k] & kFlagDelCell) || delAllG || (fj[k] & kFlagDelAll));
+        if (!any) return;
         loadBonds(s, g, l);
     }
-    const bool delAllG = f & kFlagDelAll;
     int drop[kMaxBonds];
     int nd = 0;
     for (int k = 0; k < l.n; ++k) {
