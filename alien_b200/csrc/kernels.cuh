@@ -994,10 +994,14 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletPos(DevState s)
         if (s.barrier[g]) {
             np = pb + v * dt;
         } else {
-            const long long ax = s.angleAcc[4 * g + 0], ay = s.angleAcc[4 * g + 1];
-            if (ax | ay) {
-                s.angleAcc[4 * g + 0] = 0;
-                s.angleAcc[4 * g + 1] = 0;
+            // angle forces are scattered only in steps with timestep % 3 == 0
+            // and consumed in the same step: other steps find zeros
+            long long ax = 0, ay = 0;
+            if (s.counters[c.w].timestep % 3 == 0) {
+                const longlong2 a = *reinterpret_cast<const longlong2*>(s.angleAcc + 4 * g);
+                ax = a.x;
+                ay = a.y;
+                if (ax | ay) *reinterpret_cast<longlong2*>(s.angleAcc + 4 * g) = make_longlong2(0, 0);
             }
             const float2 F1 = s.force1[g] + f2(fromFix(ax), fromFix(ay));
             s.force1[g] = F1;
@@ -1095,18 +1099,27 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletVel(DevState s)
         if (s.barrier[g]) {
             s.velB[g] = v;
         } else {
-            const long long ax = s.angleAcc[4 * g + 2], ay = s.angleAcc[4 * g + 3];
-            if (ax | ay) {
-                s.angleAcc[4 * g + 2] = 0;
-                s.angleAcc[4 * g + 3] = 0;
+            long long ax = 0, ay = 0;
+            if (s.counters[c.w].timestep % 3 == 0) {
+                const longlong2 a = *reinterpret_cast<const longlong2*>(s.angleAcc + 4 * g + 2);
+                ax = a.x;
+                ay = a.y;
+                if (ax | ay) *reinterpret_cast<longlong2*>(s.angleAcc + 4 * g + 2) = make_longlong2(0, 0);
             }
             const float2 F2 = s.force[g] + f2(fromFix(ax), fromFix(ay));
             s.velB[g] = v + (F2 + s.force1[g]) / 2.0f * p.timestepSize;
         }
-        if (s.flags[g] & kFlagDetach) s.livingState[g] = ALIEN_B200_LIVING_DETACHING;
+        int ls = s.livingState[g];
+        if (s.flags[g] & kFlagDetach) {
+            ls = ALIEN_B200_LIVING_DETACHING;
+            s.livingState[g] = static_cast<uint8_t>(ls);
+        }
         if (!s.barrier[g]) {
             ++s.age[g];
-            if (s.livingState[g] == ALIEN_B200_LIVING_READY && s.activationTime[g] > 0) --s.activationTime[g];
+            if (ls == ALIEN_B200_LIVING_READY) {
+                const uint32_t at = s.activationTime[g];
+                if (at > 0) s.activationTime[g] = at - 1;
+            }
         }
     } else {
         forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
