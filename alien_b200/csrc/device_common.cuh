@@ -276,7 +276,12 @@ __device__ __forceinline__ int floorInt(float v)
     if (r > v) --r;
     return r;
 }
-__device__ __forceinline__ int wrapInt(int v, int size) { return ((v % size) + size) % size; }
+__device__ __noinline__ int wrapIntOutside(int v, int size) { return ((v % size) + size) % size; }
+__device__ __forceinline__ int wrapInt(int v, int size)
+{
+    if (static_cast<unsigned>(v) < static_cast<unsigned>(size)) return v;  // the usual case: already inside
+    return wrapIntOutside(v, size);
+}
 
 // BaseMap::correctPosition(float2&), Map.cuh:20-26
 __device__ __forceinline__ float2 correctPosition(float2 p, int W, int H)

@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kBlock, 8) kBin(DevState s)
         s.tileOf[g] = tile;
         s.tileOff[g] = atomicAdd(&s.tileCount[tile], 1u);
 
-        if (s.barrier[g]) return;
+        if (s.barrier[g] || !(p.radiationProb > 0.0f)) return;  // a draw in [0, 1) never falls below 0
         const uint64_t T = s.counters[c.w].timestep;
         const uint64_t id = s.id[g];
         if (!(draw(id, T, kSiteRadiation) < p.radiationProb)) return;
@@ -1177,7 +1177,7 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletVel(DevState s)
 // absorbed energy, inner friction (every third step: one Jacobi sweep with
 // one pair average per bond, CellProcessor.cuh:678-705), friction and decay.
 // particles: splitting (RadiationProcessor::splitting, :172-204).
-__global__ void __launch_bounds__(kBlock, 8) kTransition(DevState s)
+__global__ void __launch_bounds__(kBlock, 6) kTransition(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         CellCtx c = cellCtx(s);
