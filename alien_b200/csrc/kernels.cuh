@@ -766,8 +766,8 @@ __global__ void __launch_bounds__(kRegionThreads, kRegionMinBlocks) kPairsRegion
     const int ownN = rowOwn[ownH];
     uint16_t* myHits = sHits + threadIdx.x;
     const float T = static_cast<float>(wi.T);
+    int ly = 1;  // own row of o; o only grows, so the search continues from the last row
     for (int o = threadIdx.x; o < ownN; o += kRegionThreads) {
-        int ly = 1;
         while (rowOwn[ly] <= o) ++ly;
         const int e = tStart[ly * LW + 1] + (o - rowOwn[ly - 1]);
         const float2 pi = sPos[e];
