@@ -653,6 +653,9 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         const long long nc = static_cast<long long>(ws.numCells), np = static_cast<long long>(ws.numParticles);
         const AlienCellTO* dCells = stagedCells[w];
         const AlienParticleTO* dParts = stagedParts[w];
+        if (nc)
+            AB_CK(cudaMemcpyAsync(cold_ + coldBase, dCells, sizeof(AlienCellTO) * static_cast<size_t>(nc), cudaMemcpyDeviceToDevice,
+                                  stream_));
         launch(kIngestCells, divUp(nc, kBlock), kBlock, s, w, static_cast<const AlienCellTO*>(dCells), nc, cold_, coldBase);
         launch(kIngestParticles, divUp(np, kBlock), kBlock, s, w, static_cast<const AlienParticleTO*>(dParts), np);
         launch(kMaxId, divUp(std::max(nc, np), kBlock), kBlock, s, w, static_cast<const AlienCellTO*>(dCells), nc,

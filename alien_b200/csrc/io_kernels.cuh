@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(kBlock) kIngestCells(DevState s, int w, const 
     const WorldInfo& wi = s.worlds[w];
     const long long g = wi.cellBase + i;
     const AlienCellTO& c = to[i];
-    cold[coldBase + i] = c;
+    // cold[coldBase + i] is a copy of to[i], made by one device-to-device copy
     s.coldIdx[g] = static_cast<uint32_t>(coldBase + i);
     s.id[g] = c.id;
     s.posA[g] = correctPosition(f2(c.pos.x, c.pos.y), wi.W, wi.H);
@@ -121,11 +121,22 @@ __global__ void __launch_bounds__(kBlock) kIngestParticles(DevState s, int w, co
 __global__ void __launch_bounds__(kBlock) kMaxId(DevState s, int w, const AlienCellTO* cells, long long nc,
                                                  const AlienParticleTO* parts, long long np)
 {
+    __shared__ unsigned long long warpMax[kBlock / 32];
     const long long i = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
     unsigned long long m = 0;
     if (i < nc) m = cells[i].id + 1;
     if (i < np && parts[i].id + 1 > m) m = parts[i].id + 1;
-    if (m) atomicMax(&s.counters[w].nextId, m);
+    // block maximum first: one atomic per block instead of one per object
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_down_sync(0xffffffffu, m, o);
+        m = other > m ? other : m;
+    }
+    if ((threadIdx.x & 31) == 0) warpMax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < kBlock / 32; ++k) m = warpMax[k] > m ? warpMax[k] : m;
+        if (m) atomicMax(&s.counters[w].nextId, m);
+    }
 }
 
 // ---- selection + ranks (egress and compaction) ----
