@@ -16,6 +16,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -52,59 +53,41 @@ struct Error : std::runtime_error {
 static inline long long roundUp(long long v, long long m) { return (v + m - 1) / m * m; }
 static inline int divUp(long long v, long long m) { return static_cast<int>((v + m - 1) / m); }
 
-// Device arrays of an arena.  freeAll() keeps the blocks for reuse: a rebuild
-// with the same layout (set_data on a world of the same size, a capacity
-// check that changes nothing) gets its arrays back without cudaMalloc /
-// cudaFree; trim() releases the blocks the new layout did not take.
+// Device arrays of an arena, allocated stream-ordered from the device's
+// default memory pool on the arena's stream.  The pool keeps freed blocks
+// (its release threshold is raised once per device), so a rebuild with the
+// same layout, or a new arena after a finished one (the serving loop), gets
+// its arrays back without cudaMalloc, and freeing never synchronises the
+// device.
 class DeviceMemory {
 public:
-    ~DeviceMemory()
-    {
-        freeAll();
-        trim();
-    }
+    ~DeviceMemory() { freeAll(); }
+    void setStream(cudaStream_t stream) { stream_ = stream; }
     template <class T>
     T* alloc(size_t n)
     {
         const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
         void* p = nullptr;
-        auto it = spare_.find(bytes);
-        if (it != spare_.end() && !it->second.empty()) {
-            p = it->second.back();
-            it->second.pop_back();
-        } else {
-            cudaError_t e = cudaMalloc(&p, bytes);
-            if (e != cudaSuccess) {
-                cudaGetLastError();
-                trim();  // give back what the new layout did not reuse, then retry once
-                e = cudaMalloc(&p, bytes);
-                if (e != cudaSuccess) {
-                    cudaGetLastError();
-                    throw Error(ALIEN_B200_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
-                }
-            }
+        cudaError_t e = cudaMallocAsync(&p, bytes, stream_);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(ALIEN_B200_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes failed");
         }
-        live_.emplace_back(p, bytes);
+        live_.push_back(p);
         bytes_ += bytes;
         return static_cast<T*>(p);
     }
     void freeAll()
     {
-        for (const auto& b : live_) spare_[b.second].push_back(b.first);
+        for (void* p : live_) cudaFreeAsync(p, stream_);
         live_.clear();
         bytes_ = 0;
-    }
-    void trim()
-    {
-        for (auto& kv : spare_)
-            for (void* p : kv.second) cudaFree(p);
-        spare_.clear();
     }
     size_t bytes() const { return bytes_; }
 
 private:
-    std::vector<std::pair<void*, size_t>> live_;
-    std::map<size_t, std::vector<void*>> spare_;
+    cudaStream_t stream_ = nullptr;
+    std::vector<void*> live_;
     size_t bytes_ = 0;
 };
 
@@ -193,7 +176,7 @@ struct HostWorld {
 
 class Arena {
 public:
-    explicit Arena(cudaStream_t stream) : stream_(stream) {}
+    explicit Arena(cudaStream_t stream) : stream_(stream) { mem_.setStream(stream); }
     ~Arena() { releaseGraph(); }
 
     void build(const std::vector<WorldSetup>& setups);
@@ -323,6 +306,11 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     const int nWorlds = static_cast<int>(setups.size());
     std::vector<AlienCellTO*> stagedCells(nWorlds, nullptr);
     std::vector<AlienParticleTO*> stagedParts(nWorlds, nullptr);
+    std::vector<void*> asyncStage;
+    auto freeAsyncStage = [&] {
+        for (void* p : asyncStage) cudaFreeAsync(p, stream_);
+        asyncStage.clear();
+    };
     {
         // all worlds' objects side by side in the staging buffers
         size_t totalCells = 0, totalParts = 0;
@@ -330,10 +318,21 @@ void Arena::build(const std::vector<WorldSetup>& setups)
             totalCells += ws.numCells;
             totalParts += ws.numParticles;
         }
-        AB_CK(cudaStreamSynchronize(stream_));  // earlier copies out of the staging buffers are done
-        AlienCellTO* cellBase = static_cast<AlienCellTO*>(stageCells_.ensure(sizeof(AlienCellTO) * std::max<size_t>(totalCells, 1)));
-        AlienParticleTO* partBase =
-            static_cast<AlienParticleTO*>(stageParts_.ensure(sizeof(AlienParticleTO) * std::max<size_t>(totalParts, 1)));
+        AlienCellTO* cellBase = nullptr;
+        AlienParticleTO* partBase = nullptr;
+        if (nWorlds == 1) {
+            // a single-world handle keeps its staging: set_data repeats with the same sizes
+            AB_CK(cudaStreamSynchronize(stream_));  // earlier copies out of the staging buffers are done
+            cellBase = static_cast<AlienCellTO*>(stageCells_.ensure(sizeof(AlienCellTO) * std::max<size_t>(totalCells, 1)));
+            partBase = static_cast<AlienParticleTO*>(stageParts_.ensure(sizeof(AlienParticleTO) * std::max<size_t>(totalParts, 1)));
+        } else {
+            // a batch is built once: stream-ordered staging, released without
+            // synchronising the device (other arenas keep stepping meanwhile)
+            AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&cellBase), sizeof(AlienCellTO) * std::max<size_t>(totalCells, 1), stream_));
+            AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&partBase), sizeof(AlienParticleTO) * std::max<size_t>(totalParts, 1),
+                                  stream_));
+            asyncStage = {cellBase, partBase};
+        }
         size_t c0 = 0, p0 = 0;
         for (int w = 0; w < nWorlds; ++w) {
             if (setups[w].numCells) stagedCells[w] = cellBase + c0;
@@ -377,6 +376,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
             }
         } catch (...) {
             cudaFreeAsync(dCheck, stream_);
+            freeAsyncStage();
             cudaStreamSynchronize(stream_);
             throw;
         }
@@ -662,13 +662,8 @@ void Arena::build(const std::vector<WorldSetup>& setups)
                static_cast<const AlienParticleTO*>(dParts), np);
         coldBase += nc;
     }
+    freeAsyncStage();
     sync();
-    mem_.trim();
-    if (n > 1) {
-        // a batch arena is built once: its staging is not worth keeping
-        stageCells_.release();
-        stageParts_.release();
-    }
 }
 
 // -------------------------------------------------------------- scan -----
@@ -1079,6 +1074,22 @@ static void ensureDevice()
     if (e != cudaSuccess || count == 0) {
         cudaGetLastError();
         throw Error(ALIEN_B200_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    // the default memory pool of the current device keeps freed arena
+    // blocks for reuse instead of returning them at every synchronisation
+    // (a per-process setting of this library's allocations; other users of
+    // the pool see it too)
+    static std::mutex m;
+    static bool configured[64] = {};
+    int device = 0;
+    AB_CK(cudaGetDevice(&device));
+    std::lock_guard<std::mutex> lock(m);
+    if (device >= 0 && device < 64 && !configured[device]) {
+        cudaMemPool_t pool;
+        AB_CK(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t threshold = UINT64_MAX;
+        AB_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+        configured[device] = true;
     }
 }
 

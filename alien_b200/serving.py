@@ -124,20 +124,25 @@ class ServingLoop:
             self.cohorts.append(_Cohort(wave))
 
     def tick(self, now: float) -> float:
-        """admit, then ``steps_per_tick`` timesteps of every running cohort,
-        each cohort on its own stream so that their kernels overlap; returns
-        the per-step latency in ms (wall time of the tick / steps)"""
-        self._admit(now)
-        if not self.cohorts:
-            return 0.0
+        """``steps_per_tick`` timesteps of every running cohort, each cohort
+        on its own stream so that their kernels overlap, with the admission
+        of waiting requests done while they run; returns the per-step
+        latency in ms (wall time of the tick / steps)"""
         k = self.steps_per_tick
         t0 = time.perf_counter()
-        for c in self.cohorts:
+        running = list(self.cohorts)
+        for c in running:
             c.batch.enqueue_timesteps(k)
-        for c in self.cohorts:
+        # admission (host work and the new arenas' uploads on their own
+        # streams) overlaps the steps just enqueued; new cohorts step from
+        # the next tick on
+        self._admit(now)
+        if not running:
+            return 0.0
+        for c in running:
             c.batch.synchronize()
         ms = (time.perf_counter() - t0) * 1000.0 / k
-        for c in self.cohorts:
+        for c in running:
             for r in c.requests:
                 self.cell_steps += r.cells * max(0, min(k, r.steps - c.steps_done))
             c.steps_done += k
@@ -145,7 +150,7 @@ class ServingLoop:
         done_now = time.perf_counter()
         keep = []
         for c in self.cohorts:
-            if c.done:
+            if c in running and c.done:
                 c.close(done_now, self.keep_results)
                 self.finished.extend(c.requests)
             else:

@@ -383,7 +383,7 @@ def run_serving(args, rank):
     with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
         out = serving.run_poisson(make, rate_per_s=args.rate, duration_s=args.duration,
                                   hbm_budget_bytes=int(args.hbm_budget_gb * 1e9), seed=rank, drain=False,
-                                  steps_per_tick=4)
+                                  steps_per_tick=args.steps_per_tick)
     out["clocks"] = clk.summary()
     return out
 
@@ -400,6 +400,7 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="serving: mean requests per second")
     ap.add_argument("--pool", type=int, default=32, help="serving: distinct request worlds")
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0, help="serving: admission budget")
+    ap.add_argument("--steps-per-tick", type=int, default=8, help="serving: steps of every cohort per loop tick")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -431,6 +432,7 @@ def main():
                 "warmup": 0, "ms_per_step": r["p50_step_ms"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": "serving", "rate_per_s": args.rate, "duration_s": args.duration,
+                           "steps_per_tick": args.steps_per_tick,
                            "hbm_budget_gb": args.hbm_budget_gb, "pool_worlds": args.pool,
                            "description": "Poisson arrivals, worlds of log-uniform 5k-500k cells (half fluid, half "
                                           "10x10 lattices, a third of the lattices neuron cells), log-uniform "
