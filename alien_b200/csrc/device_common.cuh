@@ -66,6 +66,7 @@ struct WorldInfo {
     // pair-phase regions: regW x regH tiles per CTA, nRX x nRY regions,
     // first CTA regionBase; regionShared = 0 for worlds too small for them
     int regW, regH, nRX, nRY, regionBase, regionShared;
+    long long auxBase;  // offset of the world's auxiliary data in DevState::aux
 };
 
 struct WorldCounters {
@@ -132,9 +133,7 @@ struct DevState {
     AlienCellTO* cold;        // ingest copies (signals and cellFunctionUsed of neuron cells change here)
     uchar4* fnInfo;           // per cell: (function: 0 none / 1 neuron, execution order, input order as int8, output
                               // blocked); null when no cell has a function or a signal
-    const long long* neuronList;  // arena slots of the neuron cells
-    const float* neuronTable; // per neuron (list order): weights [8 x 8] row-major, then 8 biases
-    int numNeurons;
+    const uint8_t* aux;       // the worlds' auxiliary data (world w at worlds[w].auxBase); null without neurons
     int* bond;          // [slot * 6 + k] partner slot
     float* bondDist;
     float* bondAngle;

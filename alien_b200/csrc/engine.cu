@@ -387,7 +387,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     mem_.freeAll();
     worlds_.clear();
     const int n = static_cast<int>(setups.size());
-    long long cellSlots = 0, partSlots = 0, tiles = 0, pmapSlots = 0, coldTotal = 0;
+    long long cellSlots = 0, partSlots = 0, tiles = 0, pmapSlots = 0, coldTotal = 0, auxTotal = 0;
     int regions = 0;
     int cellBlocks = 0, partBlocks = 0;
     maxWorldCells_ = maxWorldParts_ = 0;
@@ -445,29 +445,11 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         maxWorldCells_ = std::max(maxWorldCells_, wi.cellCap);
         maxWorldParts_ = std::max(maxWorldParts_, wi.partCap);
         if (ws.numAux) hw.aux.assign(ws.aux, ws.aux + ws.numAux);
+        hw.info.auxBase = auxTotal;
+        auxTotal += static_cast<long long>(ws.numAux);
         worlds_.push_back(std::move(hw));
     }
-    // neuron table: weights and biases of every neuron cell
-    std::vector<float> neuronTableHost;
-    std::vector<std::pair<long long, int>> neuronCells;  // (arena slot, table row)
-    if (neuronsTotal > 0) {
-        long long slotBase = 0;
-        for (int w = 0; w < n; ++w) {
-            const WorldSetup& ws = setups[w];
-            for (uint64_t i = 0; i < ws.numCells; ++i) {
-                const AlienCellTO& c = ws.cells[i];
-                if (c.cellFunction != kCellFunctionNeuron) continue;  // checked by validateCells
-                const uint64_t at = c.cellFunctionData[0];  // NeuronTO.weightsAndBiasesDataIndex
-                const uint64_t bytes = sizeof(float) * kNeuronTableStride;
-                const size_t row = neuronTableHost.size() / kNeuronTableStride;
-                neuronTableHost.resize(neuronTableHost.size() + kNeuronTableStride);
-                std::memcpy(neuronTableHost.data() + row * kNeuronTableStride, ws.aux + at, bytes);
-                neuronCells.emplace_back(slotBase + static_cast<long long>(i), static_cast<int>(row));
-            }
-            slotBase += worlds_[w].info.cellCap;
-        }
-    }
-    hasNeurons_ = !neuronCells.empty();
+    hasNeurons_ = neuronsTotal > 0;
     signalsLive_ = hasNeurons_ || signalsTotal > 0;
     hasFluid_ = hasCollision_ = false;
     for (const HostWorld& hw : worlds_) {
@@ -588,21 +570,18 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     cold_ = mem_.alloc<AlienCellTO>(static_cast<size_t>(coldTotal));
     s.cold = cold_;
     s.fnInfo = nullptr;
-    s.neuronList = nullptr;
-    s.neuronTable = nullptr;
-    s.numNeurons = static_cast<int>(neuronCells.size());
+    s.aux = nullptr;
     if (signalsLive_) s.fnInfo = mem_.alloc<uchar4>(C);  // filled by kIngestCells
     if (hasNeurons_) {
-        long long* listDev = mem_.alloc<long long>(neuronCells.size());
-        float* tableDev = mem_.alloc<float>(neuronTableHost.size());
-        std::vector<long long> listHost(neuronCells.size());
-        for (const auto& nc : neuronCells) listHost[static_cast<size_t>(nc.second)] = nc.first;
-        AB_CK(cudaMemcpyAsync(listDev, listHost.data(), sizeof(long long) * listHost.size(), cudaMemcpyHostToDevice, stream_));
-        AB_CK(cudaMemcpyAsync(tableDev, neuronTableHost.data(), sizeof(float) * neuronTableHost.size(), cudaMemcpyHostToDevice,
-                              stream_));
-        AB_CK(cudaStreamSynchronize(stream_));  // the host vectors end with this scope
-        s.neuronList = listDev;
-        s.neuronTable = tableDev;
+        // neuron weights and biases are read where they lie in the
+        // auxiliary data, uploaded once per build
+        long long auxBytes = 0;
+        for (const HostWorld& hw : worlds_) auxBytes += static_cast<long long>(hw.aux.size());
+        uint8_t* auxDev = mem_.alloc<uint8_t>(static_cast<size_t>(std::max<long long>(auxBytes, 1)));
+        for (const HostWorld& hw : worlds_)
+            if (!hw.aux.empty())
+                AB_CK(cudaMemcpyAsync(auxDev + hw.info.auxBase, hw.aux.data(), hw.aux.size(), cudaMemcpyHostToDevice, stream_));
+        s.aux = auxDev;
     }
     rankCells_ = mem_.alloc<int>(C);
     rankParts_ = mem_.alloc<int>(P);
@@ -696,7 +675,7 @@ void Arena::enqueueStep()
     launch(kVerletVel, both, kBlock, s);
     launch(kTransition, both, kBlock, s);
     launch(kResolve, cells, kBlock, s);
-    if (hasNeurons_) launch(kNeuron, divUp(s.numNeurons, kBlock), kBlock, s);
+    if (hasNeurons_) launch(kNeuron, cells, kBlock, s);
     if (signalsLive_) launch(kSignalReset, cells, kBlock, s);
     launch(kCommit, cells, kBlock, s);
     launch(kEventCount, both, kBlock, s);

@@ -1343,15 +1343,25 @@ __device__ __forceinline__ float neuronActivation(int function, float x)
     return 0.0f;
 }
 
+// a float of the auxiliary data at any byte offset (the reference's
+// converter does not promise 4-byte alignment)
+__device__ __forceinline__ float auxFloat(const uint8_t* p, bool aligned)
+{
+    if (aligned) return *reinterpret_cast<const float*>(p);
+    const uint32_t u = static_cast<uint32_t>(p[0]) | static_cast<uint32_t>(p[1]) << 8 | static_cast<uint32_t>(p[2]) << 16
+                       | static_cast<uint32_t>(p[3]) << 24;
+    return __uint_as_float(u);
+}
+
 __global__ void __launch_bounds__(kBlock) kNeuron(DevState s)
 {
-    const int row = blockIdx.x * kBlock + threadIdx.x;
-    if (row >= s.numNeurons) return;
-    const long long g = s.neuronList[row];
-    const int w = s.cellBlockWorld[g / kBlock];
-    const WorldCounters& wc = s.counters[w];
-    if (!wc.active || g >= s.worlds[w].cellBase + wc.numCells || !s.alive[g]) return;
+    CellCtx c = cellCtx(s);
+    if (!c.valid) return;
+    const long long g = c.g;
     const uchar4 fi = s.fnInfo[g];
+    if (fi.x != 1) return;
+    const int w = c.w;
+    const WorldCounters& wc = s.counters[w];
     const AlienPhysicsParams& p = s.params[w];
     if (static_cast<uint64_t>(fi.y) != wc.timestep % static_cast<uint64_t>(p.cellNumExecutionOrderNumbers)) return;
     const int ls = s.livingState[g];
@@ -1394,14 +1404,18 @@ __global__ void __launch_bounds__(kBlock) kNeuron(DevState s)
         for (int ch = 0; ch < ALIEN_B200_MAX_CHANNELS - 1; ++ch) used |= in[ch] != 0.0f;
         if (used) me.cellFunctionUsed = 1;
     }
-    const float* wb = s.neuronTable + static_cast<long long>(row) * kNeuronTableStride;
+    // NeuronFunction::NeuronState in the auxiliary data: weights [8 x 8]
+    // row-major, then 8 biases (NeuronTO.weightsAndBiasesDataIndex)
+    const uint8_t* wb = s.aux + s.worlds[w].auxBase + me.cellFunctionData[0];
+    const bool aligned = (reinterpret_cast<uintptr_t>(wb) & 3) == 0;
     const int32_t* act = reinterpret_cast<const int32_t*>(&me.cellFunctionData[1]);  // NeuronTO.activationFunctions
     float out[ALIEN_B200_MAX_CHANNELS];
 #pragma unroll
     for (int r = 0; r < ALIEN_B200_MAX_CHANNELS; ++r) {
-        float sum = wb[ALIEN_B200_MAX_CHANNELS * ALIEN_B200_MAX_CHANNELS + r];
+        float sum = auxFloat(wb + 4 * (ALIEN_B200_MAX_CHANNELS * ALIEN_B200_MAX_CHANNELS + r), aligned);
 #pragma unroll
-        for (int col = 0; col < ALIEN_B200_MAX_CHANNELS; ++col) sum += wb[r * ALIEN_B200_MAX_CHANNELS + col] * in[col];
+        for (int col = 0; col < ALIEN_B200_MAX_CHANNELS; ++col)
+            sum += auxFloat(wb + 4 * (r * ALIEN_B200_MAX_CHANNELS + col), aligned) * in[col];
         out[r] = neuronActivation(act[r], sum);
     }
 #pragma unroll

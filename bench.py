@@ -372,6 +372,8 @@ def run_serving(args, rank):
         d = worldgen.add_neurons(d, 100_000 * rank + i, fraction=1.0,
                                  cells=(chosen[:, None] * 100 + np.arange(100)[None, :]).ravel())
         pool.append((d, w))
+    # request data arrives in page-locked host buffers, as a server would keep them
+    pins = [pin(d._cells) for d, _ in pool]
     log(f"serving: pool of {len(pool)} worlds, {sum(d.num_cells for d, _ in pool)} cells")
     prm = P.benchmark_parameters(P.MOTION_FLUID)
 
@@ -385,6 +387,8 @@ def run_serving(args, rank):
                                   hbm_budget_bytes=int(args.hbm_budget_gb * 1e9), seed=rank, drain=False,
                                   steps_per_tick=args.steps_per_tick)
     out["clocks"] = clk.summary()
+    for p in pins:
+        unpin(p)
     return out
 
 
