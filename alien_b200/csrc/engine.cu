@@ -420,7 +420,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         wi.firstPartBlock = partBlocks;
         wi.numPartBlocks = static_cast<int>(wi.partCap / kBlock);
         wi.pmapBase = pmapSlots;
-        // pair-phase regions: 16 x 8 tiles with a one-tile halo that never
+        // pair-phase regions: up to 32 x 16 tiles with a one-tile halo that never
         // overlaps the region itself and lies within half a world (so that a
         // seam shift gives the minimal image)
         if (wi.nTX >= 4 && wi.nTY >= 4 && ws.W >= 4 * wi.T && ws.H >= 4 * wi.T) {
