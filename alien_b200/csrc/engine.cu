@@ -149,6 +149,15 @@ static void validateParams(const AlienPhysicsParams& p, int W, int H)
     if (W < 2 * r + 1 || H < 2 * r + 1) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "world smaller than the interaction window");
 }
 
+static int regionMaxW(int motion)
+{
+    return motion == ALIEN_B200_MOTION_FLUID ? RegionShape<ALIEN_B200_MOTION_FLUID>::W : RegionShape<ALIEN_B200_MOTION_COLLISION>::W;
+}
+static int regionMaxH(int motion)
+{
+    return motion == ALIEN_B200_MOTION_FLUID ? RegionShape<ALIEN_B200_MOTION_FLUID>::H : RegionShape<ALIEN_B200_MOTION_COLLISION>::H;
+}
+
 static int scanRadius(const AlienPhysicsParams& p)
 {
     return std::max(1, p.motionType == ALIEN_B200_MOTION_FLUID ? static_cast<int>(ceilf(p.smoothingLength * 2.0f))
@@ -420,16 +429,16 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         wi.firstPartBlock = partBlocks;
         wi.numPartBlocks = static_cast<int>(wi.partCap / kBlock);
         wi.pmapBase = pmapSlots;
-        // pair-phase regions: up to 32 x 16 tiles with a one-tile halo that never
+        // pair-phase regions (RegionShape) with a one-tile halo that never
         // overlaps the region itself and lies within half a world (so that a
         // seam shift gives the minimal image)
         if (wi.nTX >= 4 && wi.nTY >= 4 && ws.W >= 4 * wi.T && ws.H >= 4 * wi.T) {
-            wi.regW = std::min(kRegionMaxW, wi.nTX - 2);
-            wi.regH = std::min(kRegionMaxH, wi.nTY - 2);
+            wi.regW = std::min(regionMaxW(wi.motionType), wi.nTX - 2);
+            wi.regH = std::min(regionMaxH(wi.motionType), wi.nTY - 2);
             wi.regionShared = 1;
         } else {
-            wi.regW = std::min(kRegionMaxW, wi.nTX);
-            wi.regH = std::min(kRegionMaxH, wi.nTY);
+            wi.regW = std::min(regionMaxW(wi.motionType), wi.nTX);
+            wi.regH = std::min(regionMaxH(wi.motionType), wi.nTY);
             wi.regionShared = 0;
         }
         wi.nRX = divUp(wi.nTX, wi.regW);
@@ -461,12 +470,12 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     if (cellSlots >= (1ll << 31) || partSlots >= (1ll << 31) || tiles >= (1ll << 32) - 2)
         throw Error(ALIEN_B200_ERR_CAPACITY, "arena exceeds 2^31 slots");
 
-    // the pair-phase regions stage up to kRegionCap records in dynamic
+    // the pair-phase regions stage up to RegionShape<>::Cap records in dynamic
     // shared memory (above the 48 KB default)
     AB_CK(cudaFuncSetAttribute(kPairsRegion<ALIEN_B200_MOTION_FLUID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(kRegionDynSmem)));
+                               static_cast<int>(regionDynSmem<ALIEN_B200_MOTION_FLUID>())));
     AB_CK(cudaFuncSetAttribute(kPairsRegion<ALIEN_B200_MOTION_COLLISION>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(kRegionDynSmem)));
+                               static_cast<int>(regionDynSmem<ALIEN_B200_MOTION_COLLISION>())));
     DevState& s = s_;
     s = DevState{};
     s.numWorlds = n;
@@ -666,9 +675,11 @@ void Arena::enqueueStep()
     scan(s.tileCount, s.numTiles, s.tileStart);
     launch(kScatter, cells, kBlock, s);
     launch(kStage, cells, kBlock, s);
-    if (hasFluid_) launchSmem(kPairsRegion<ALIEN_B200_MOTION_FLUID>, s.numRegions, kRegionThreads, kRegionDynSmem, s);
+    if (hasFluid_)
+        launchSmem(kPairsRegion<ALIEN_B200_MOTION_FLUID>, s.numRegions, kRegionThreads, regionDynSmem<ALIEN_B200_MOTION_FLUID>(), s);
     if (hasCollision_)
-        launchSmem(kPairsRegion<ALIEN_B200_MOTION_COLLISION>, s.numRegions, kRegionThreads, kRegionDynSmem, s);
+        launchSmem(kPairsRegion<ALIEN_B200_MOTION_COLLISION>, s.numRegions, kRegionThreads,
+                   regionDynSmem<ALIEN_B200_MOTION_COLLISION>(), s);
     launch(kApplyBond1, both, kBlock, s);
     launch(kVerletPos, both, kBlock, s);
     launch(kBond2, both, kBlock, s);

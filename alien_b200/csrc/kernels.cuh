@@ -616,7 +616,8 @@ __device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
 }
 
 // ------------------------------------------------------- kPairsRegion ----
-// One CTA per region of regW x regH tiles (up to 32 x 16) of one world.  It
+// One CTA per region of regW x regH tiles (up to RegionShape<Motion>: 24 x 16
+// for collision worlds, 32 x 8 for fluid worlds) of one world.  It
 // copies the staged records of the region and of its one-tile halo from the
 // tile-sorted arrays into shared memory, all (regW+2) x (regH+2) local tiles
 // in row-major order (each tile a contiguous run in storage order), so that
@@ -640,17 +641,36 @@ __device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
 // Regions whose records exceed the shared buffer, and worlds too small for
 // regions, use pairsGlobal for their cells.
 constexpr int kRegionThreads = 256;
-constexpr int kRegionMaxW = 32, kRegionMaxH = 16;
-constexpr int kRegionMaxTiles = (kRegionMaxW + 2) * (kRegionMaxH + 2);
-constexpr int kRegionCap = 2304;  // staged records per CTA (halo included)
-constexpr int kHitCap = 24;       // hit-list entries per thread before a flush
-constexpr int kRegionMinBlocks = 2;
-constexpr size_t kRegionDynSmem = static_cast<size_t>(kRegionCap) * (sizeof(int4) + 2 * sizeof(float2))
-                                  + static_cast<size_t>(kHitCap) * kRegionThreads * sizeof(uint16_t);
+constexpr int kHitCap = 24;  // hit-list entries per thread before a flush
+// Region shape per motion type (tiles per region, shared-buffer records,
+// resident CTAs per SM), from a sweep of shapes on the B200.  Dense regions
+// are processed in bands of rows, so the buffer size bounds no world.  The
+// visiting order does not depend on the shape; the FP32 results of different
+// builds can still differ in the last bit where the compiler contracts
+// multiply-adds differently.
+template <int Motion>
+struct RegionShape;
+template <>
+struct RegionShape<ALIEN_B200_MOTION_FLUID> {
+    static constexpr int W = 32, H = 8, Cap = 1152, MinBlocks = 3;
+};
+template <>
+struct RegionShape<ALIEN_B200_MOTION_COLLISION> {
+    static constexpr int W = 24, H = 16, Cap = 1152, MinBlocks = 4;
+};
+template <int Motion>
+constexpr size_t regionDynSmem()
+{
+    return static_cast<size_t>(RegionShape<Motion>::Cap) * (sizeof(int4) + 2 * sizeof(float2))
+           + static_cast<size_t>(kHitCap) * kRegionThreads * sizeof(uint16_t);
+}
 
 template <int Motion>
-__global__ void __launch_bounds__(kRegionThreads, kRegionMinBlocks) kPairsRegion(DevState s)
+__global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks) kPairsRegion(DevState s)
 {
+    constexpr int kRegionCap = RegionShape<Motion>::Cap;
+    constexpr int kRegionMaxH = RegionShape<Motion>::H;
+    constexpr int kRegionMaxTiles = (RegionShape<Motion>::W + 2) * (RegionShape<Motion>::H + 2);
     extern __shared__ int4 dyn[];
     int4* sMeta = dyn;
     float2* sPos = reinterpret_cast<float2*>(sMeta + kRegionCap);
@@ -724,94 +744,107 @@ __global__ void __launch_bounds__(kRegionThreads, kRegionMinBlocks) kPairsRegion
         if (threadIdx.x == 0) tStart[NT] = static_cast<int>(total);
     }
     __syncthreads();
-    const int total = tStart[NT];
     if (threadIdx.x <= ownH) {
         // own records of rows 1..r (own row segments are [tStart[r*LW+1], tStart[r*LW+ownW+1]))
         int acc = 0;
         for (int r = 1; r <= static_cast<int>(threadIdx.x); ++r) acc += tStart[r * LW + ownW + 1] - tStart[r * LW + 1];
         rowOwn[threadIdx.x] = acc;
     }
-    if (total > kRegionCap) {
-        // denser than the shared buffer: the region's own cells from global memory
-        for (int ly = 1; ly <= ownH; ++ly)
+    __syncthreads();
+    uint16_t* myHits = sHits + threadIdx.x;
+    const float T = static_cast<float>(wi.T);
+    // Own rows in bands whose local rows (the band and one halo row on either
+    // side) fit the shared buffer: one band for the usual region, several for
+    // a dense one.  Every thread derives the same bands from tStart.  A single
+    // own row that does not fit even alone takes the global-memory path.
+    int band0 = 1;
+    while (band0 <= ownH) {
+        const int base = tStart[(band0 - 1) * LW];
+        if (tStart[(band0 + 2) * LW] - base > kRegionCap) {
+            const int ly = band0;
             for (int lx = 1; lx <= ownW; ++lx) {
                 const int q = ly * LW + lx;
                 const int k0 = tGlobal[q], n = tStart[q + 1] - tStart[q];
                 for (int k = k0 + threadIdx.x; k < k0 + n; k += kRegionThreads) pairsGlobal<Motion>(s, k);
             }
-        return;
-    }
-    // 2. copy: a record's local row by binary search over the row starts,
-    //    then one of the row's three global runs
-    for (int e = threadIdx.x; e < total; e += kRegionThreads) {
-        int lo = 0, hi = LH - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (tStart[mid * LW] <= e)
-                lo = mid;
-            else
-                hi = mid - 1;
+            ++band0;
+            continue;
         }
-        const int b = lo * LW;
-        const int q = e < tStart[b + 1] ? b : (e < tStart[b + LW - 1] ? b + 1 : b + LW - 1);
-        const int src = tGlobal[q] + (e - tStart[q]);
-        const float2 sh = tShift[q];
-        const float4 pv = s.stagedPV[src];
-        sPos[e] = f2(pv.x + sh.x, pv.y + sh.y);
-        sVel[e] = f2(pv.z, pv.w);
-        sMeta[e] = s.stagedMeta[src];
-    }
-    __syncthreads();
-    // 3. pair law of every own cell against the tiles its disc reaches
-    const int ownN = rowOwn[ownH];
-    uint16_t* myHits = sHits + threadIdx.x;
-    const float T = static_cast<float>(wi.T);
-    int ly = 1;  // own row of o; o only grows, so the search continues from the last row
-    for (int o = threadIdx.x; o < ownN; o += kRegionThreads) {
-        while (rowOwn[ly] <= o) ++ly;
-        const int e = tStart[ly * LW + 1] + (o - rowOwn[ly - 1]);
-        const float2 pi = sPos[e];
-        // own tile column as binned (own tiles are not shifted)
-        const int gx = slotX(pi.x, wi.W) / wi.T;
-        const int lx = min(max(gx - tx0 + 1, 1), ownW);
-        const int gy = ty0 + ly - 1;
-        auto scan = [&](auto& law, auto diff) {
-            law.begin(s, wi, sMeta[e], pi, sVel[e]);
-            // reach: R plus a margin above the rounding of positions up to the world size
-            const float reach = law.R * 1.0001f + 1e-3f + 4.0f * static_cast<float>(max(wi.W, wi.H)) * 1.2e-7f;
-            const float left = static_cast<float>(gx) * T, right = fminf(static_cast<float>(gx + 1) * T, static_cast<float>(wi.W));
-            const float bottom = static_cast<float>(gy) * T, top = fminf(static_cast<float>(gy + 1) * T, static_cast<float>(wi.H));
-            const int c0 = lx - (pi.x - reach < left ? 1 : 0), c1 = lx + (pi.x + reach >= right ? 1 : 0);
-            const int r0 = ly - (pi.y - reach < bottom ? 1 : 0), r1 = ly + (pi.y + reach >= top ? 1 : 0);
-            int nh = 0;
-            auto flush = [&]() {
-                for (int i = 0; i < nh; ++i) {
-                    const int m = myHits[i * kRegionThreads];
-                    law.visit(sMeta[m], sVel[m], diff(m));
-                }
-                nh = 0;
-            };
+        int band1 = band0;  // last own row of the band
+        while (band1 < ownH && tStart[(band1 + 3) * LW] - base <= kRegionCap) ++band1;
+        const int end = tStart[(band1 + 2) * LW];
+        // 2. copy local rows band0-1 .. band1+1: a record's local row by binary
+        //    search over the row starts, then one of the row's three global runs
+        for (int e = base + threadIdx.x; e < end; e += kRegionThreads) {
+            int lo = band0 - 1, hi = band1 + 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (tStart[mid * LW] <= e)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            const int b = lo * LW;
+            const int q = e < tStart[b + 1] ? b : (e < tStart[b + LW - 1] ? b + 1 : b + LW - 1);
+            const int src = tGlobal[q] + (e - tStart[q]);
+            const float2 sh = tShift[q];
+            const float4 pv = s.stagedPV[src];
+            sPos[e - base] = f2(pv.x + sh.x, pv.y + sh.y);
+            sVel[e - base] = f2(pv.z, pv.w);
+            sMeta[e - base] = s.stagedMeta[src];
+        }
+        __syncthreads();
+        // 3. pair law of every own cell of the band against the tiles its
+        //    disc reaches (shared-memory index = record offset - base)
+        int ly = band0;  // own row of o; o only grows, so the search continues from the last row
+        for (int o = rowOwn[band0 - 1] + threadIdx.x; o < rowOwn[band1]; o += kRegionThreads) {
+            while (rowOwn[ly] <= o) ++ly;
+            const int e = tStart[ly * LW + 1] + (o - rowOwn[ly - 1]) - base;
+            const float2 pi = sPos[e];
+            // own tile column as binned (own tiles are not shifted)
+            const int gx = slotX(pi.x, wi.W) / wi.T;
+            const int lx = min(max(gx - tx0 + 1, 1), ownW);
+            const int gy = ty0 + ly - 1;
+            auto scan = [&](auto& law, auto diff) {
+                law.begin(s, wi, sMeta[e], pi, sVel[e]);
+                // reach: R plus a margin above the rounding of positions up to the world size
+                const float reach = law.R * 1.0001f + 1e-3f + 4.0f * static_cast<float>(max(wi.W, wi.H)) * 1.2e-7f;
+                const float left = static_cast<float>(gx) * T, right = fminf(static_cast<float>(gx + 1) * T, static_cast<float>(wi.W));
+                const float bottom = static_cast<float>(gy) * T, top = fminf(static_cast<float>(gy + 1) * T, static_cast<float>(wi.H));
+                const int c0 = lx - (pi.x - reach < left ? 1 : 0), c1 = lx + (pi.x + reach >= right ? 1 : 0);
+                const int r0 = ly - (pi.y - reach < bottom ? 1 : 0), r1 = ly + (pi.y + reach >= top ? 1 : 0);
+                int nh = 0;
+                auto flush = [&]() {
+                    for (int i = 0; i < nh; ++i) {
+                        const int m = myHits[i * kRegionThreads];
+                        law.visit(sMeta[m], sVel[m], diff(m));
+                    }
+                    nh = 0;
+                };
 #pragma unroll 1
-            for (int r = r0; r <= r1; ++r) {
-                const int b0 = tStart[r * LW + c0], b1 = tStart[r * LW + c1 + 1];
-                for (int m = b0; m < b1; ++m) {
-                    const float2 dm = diff(m);
-                    if (law.near(dm) && law.relevant(sMeta, m, dm)) {
-                        myHits[nh * kRegionThreads] = static_cast<uint16_t>(m);
-                        if (++nh == kHitCap) flush();
+                for (int r = r0; r <= r1; ++r) {
+                    const int b0 = tStart[r * LW + c0] - base, b1 = tStart[r * LW + c1 + 1] - base;
+                    for (int m = b0; m < b1; ++m) {
+                        const float2 dm = diff(m);
+                        if (law.near(dm) && law.relevant(sMeta, m, dm)) {
+                            myHits[nh * kRegionThreads] = static_cast<uint16_t>(m);
+                            if (++nh == kHitCap) flush();
+                        }
                     }
                 }
+                flush();
+                law.end();
+            };
+            if (Motion == ALIEN_B200_MOTION_FLUID) {
+                FluidLaw law;
+                scan(law, [&](int m) { return pi - sPos[m]; });
+            } else {
+                CollisionLaw law;
+                scan(law, [&](int m) { return sPos[m] - pi; });
             }
-            flush();
-            law.end();
-        };
-        if (Motion == ALIEN_B200_MOTION_FLUID) {
-            FluidLaw law;
-            scan(law, [&](int m) { return pi - sPos[m]; });
-        } else {
-            CollisionLaw law;
-            scan(law, [&](int m) { return sPos[m] - pi; });
         }
+        __syncthreads();  // the next band overwrites the buffer
+        band0 = band1 + 1;
     }
 }
 
