@@ -155,6 +155,7 @@ struct DevState {
 
     // tiles
     uint32_t* tileOf;
+    uint32_t* slotOf;      // slot (x + y * W) of the cell at binning
     uint32_t* tileOff;
     uint32_t* tileCount;
     uint32_t* tileStart;   // numTiles + 1 entries (exclusive scan of tileCount)

@@ -547,6 +547,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     s.radVel = mem_.alloc<float2>(C);
     s.radEnergy = mem_.alloc<float>(C);
     s.tileOf = mem_.alloc<uint32_t>(C);
+    s.slotOf = mem_.alloc<uint32_t>(C);
     s.tileOff = mem_.alloc<uint32_t>(C);
     s.sorted = mem_.alloc<uint32_t>(C);
     s.stagedPV = mem_.alloc<float4>(C);

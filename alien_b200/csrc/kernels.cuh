@@ -73,10 +73,10 @@ __device__ __forceinline__ PartCtx partCtx(const DevState& s, int pb)
 // sees is block-uniform, so f may synchronise the block; f's return ends one
 // particle block for the calling thread.
 template <class UsedSlots, class F>
-__device__ __forceinline__ void forParticleBlocks(const DevState& s, UsedSlots usedSlots, F f)
+__device__ __forceinline__ void forParticleBlocks(const DevState& s, UsedSlots usedSlots, F f, int firstBlock)
 {
-    const int stride = gridDim.x - s.numCellBlocks;
-    for (int pb = blockIdx.x - s.numCellBlocks; pb < s.numPartBlocks; pb += stride) {
+    const int stride = gridDim.x - firstBlock;
+    for (int pb = blockIdx.x - firstBlock; pb < s.numPartBlocks; pb += stride) {
         const int w = s.partBlockWorld[pb];
         const WorldInfo& wi = s.worlds[w];
         const WorldCounters& wc = s.counters[w];
@@ -93,6 +93,11 @@ __device__ __forceinline__ void forParticleBlocks(const DevState& s, UsedSlots u
         c.inRange = c.q < end;
         f(c, pb);
     }
+}
+template <class UsedSlots, class F>
+__device__ __forceinline__ void forParticleBlocks(const DevState& s, UsedSlots usedSlots, F f)
+{
+    forParticleBlocks(s, usedSlots, f, s.numCellBlocks);
 }
 __device__ __forceinline__ unsigned int usedParticles(const WorldCounters& wc) { return wc.numParticles; }
 
@@ -159,6 +164,7 @@ __global__ void __launch_bounds__(kBlock, 8) kBin(DevState s)
         int sx = slotX(pos.x, wi.W), sy = slotX(pos.y, wi.H);
         uint32_t tile = static_cast<uint32_t>(wi.tileBase + (sx / wi.T) + static_cast<long long>(sy / wi.T) * wi.nTX);
         s.tileOf[g] = tile;
+        s.slotOf[g] = static_cast<uint32_t>(sx + sy * wi.W);
         s.tileOff[g] = atomicAdd(&s.tileCount[tile], 1u);
 
         if (s.barrier[g] || !(p.radiationProb > 0.0f)) return;  // a draw in [0, 1) never falls below 0
@@ -288,14 +294,13 @@ __global__ void __launch_bounds__(kBlock) kStage(DevState s)
     const uint32_t t = s.tileOf[g];
     const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
     const float2 pos = s.posA[g];
-    const int slot = slotX(pos.x, wi.W) + slotX(pos.y, wi.H) * wi.W;
+    const uint32_t slot = s.slotOf[g];
     int rank = 0, rankInTile = 0;
     for (uint32_t m = k0; m < k1; ++m) {
         uint32_t g2 = s.sorted[m];
         if (g2 >= g) continue;
         ++rankInTile;
-        float2 p2 = s.posA[g2];
-        rank += (slotX(p2.x, wi.W) + slotX(p2.y, wi.H) * wi.W) == slot;
+        rank += s.slotOf[g2] == slot;
     }
     // records of a tile in storage order: a fixed visiting order for the
     // pair phase, whatever order the binning atomics produced
@@ -1753,8 +1758,12 @@ __global__ void __launch_bounds__(kBlock) kEventCount(DevState s)
         WorldCounters& wc = s.counters[w];
         uint32_t a = 0, b = 0;
         if (g < s.worlds[w].cellBase + wc.numCells) {
-            a = (s.flags[g] & kFlagRadiation) ? 1u : 0u;
+            const uint32_t fl = s.flags[g];
+            a = (fl & kFlagRadiation) ? 1u : 0u;
             b = delEvent(s, g) ? 1u : 0u;
+            // the step's flags end here, except on the cells kEventEmit
+            // still reads (radiation and deletion events)
+            if (fl && !a && !b) s.flags[g] = 0;
         }
         uint32_t ta, tb;
         blockSums(a, b, ta, tb);
@@ -1872,9 +1881,10 @@ __global__ void __launch_bounds__(kBlock) kEventEmit(DevState s)
         const int w = s.cellBlockWorld[blockIdx.x];
         const WorldCounters& wc = s.counters[w];
         const long long g = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+        // without events kEventCount has cleared every flag already
+        if (wc.numEvents == 0) return;
         const uint32_t fl = s.flags[g];
         if (fl) s.flags[g] = 0;  // the step's flags end here
-        if (wc.numEvents == 0) return;
         const WorldInfo& wi = s.worlds[w];
         const bool inRange = g < wi.cellBase + wc.numCells;
         const uint32_t rad = inRange && (fl & kFlagRadiation) ? 1u : 0u;
