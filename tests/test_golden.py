@@ -17,6 +17,9 @@ B200 by tests/golden/make_golden.py.  These CPU tests pin the oracle:
   of every cell within NEURON_ATOL (the reference evaluates activations with
   the fast-math exponential and adds the 64 weight products with shared-
   memory atomics in arbitrary order).
+
+The tests marked gpu hold the CUDA engine itself to the same reference
+outputs (long-run statistics, decay, neuron signals).
 """
 import glob
 import json
@@ -159,3 +162,76 @@ def test_oracle_neurons_match_reference(path):
     np.testing.assert_allclose(got["signalTargetY"], ref["signalTargetY"], rtol=1e-5, atol=NEURON_ATOL)
     neurons = data.cells["cellFunction"][np.argsort(data.cells["id"])] == 0
     assert np.any(np.any(got["signalChannels"][neurons] != data.cells["signalChannels"][np.argsort(data.cells["id"])][neurons], axis=1))
+
+
+@needs_observables
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(make_golden.LONG_RUNS))
+def test_engine_statistics_match_reference(name):
+    """the CUDA engine over the same long runs: counts, total energy, mean
+    speed and the speed histogram agree with the reference engine's as the
+    oracle's do (the reference is not reproducible run to run)"""
+    from alien_b200.facade import SimulationFacade
+
+    ref = _obs(name)
+    builder, motion, steps = make_golden.LONG_RUNS[name]
+    data, world = builder()
+    eng = SimulationFacade()
+    eng.new_simulation(0, world, P.benchmark_parameters(motion))
+    eng.set_simulation_data(data)
+    eng.calc_timesteps(steps)
+    got = make_golden.observables(eng.get_simulation_data())
+    eng.close_simulation()
+    want = ref["final"]
+    e_got = got["cell_energy"] + got["particle_energy"]
+    e_want = want["cell_energy"] + want["particle_energy"]
+    assert abs(e_got - e_want) / e_want < 1e-3
+    assert abs(got["cells"] - want["cells"]) <= max(3, 0.02 * want["cells"])
+    assert abs(got["mean_speed"] - want["mean_speed"]) <= 0.1 * want["mean_speed"] + 1e-3
+    assert tv_distance(got["speed_hist"], want["speed_hist"]) < 0.1
+
+
+@needs_observables
+@pytest.mark.gpu
+def test_engine_decay_matches_reference():
+    """CellConnectionTests.decay on the CUDA engine: every cell decays within
+    1000 steps, energy moves to particles and is conserved"""
+    from alien_b200.facade import SimulationFacade
+
+    ref = _obs("decay")
+    data, world, prm = make_golden.decay_input()
+    eng = SimulationFacade()
+    eng.new_simulation(0, world, prm)
+    eng.set_simulation_data(data)
+    eng.calc_timesteps(ref["steps"])
+    got = make_golden.observables(eng.get_simulation_data())
+    eng.close_simulation()
+    assert got["cells"] == ref["final"]["cells"] == 0
+    e_got = got["cell_energy"] + got["particle_energy"]
+    e_ref = ref["final"]["cell_energy"] + ref["final"]["particle_energy"]
+    assert abs(e_got - e_ref) / e_ref < 1e-3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", NEURON_FIXTURES, ids=[os.path.basename(p) for p in NEURON_FIXTURES])
+def test_engine_neurons_match_reference(path):
+    """neuron signals of the CUDA engine against the reference engine's"""
+    from alien_b200.facade import SimulationFacade
+
+    f = np.load(path)
+    seed, motion, t, wx, wy, ts, steps = (int(v) for v in f["meta"])
+    data, world = make_golden.neuron_world(seed)
+    prm = P.PhysicsParams.from_buffer_copy(f["params"].tobytes())
+    eng = SimulationFacade()
+    eng.new_simulation(t, world, prm)
+    eng.set_simulation_data(data)
+    eng.calc_timesteps(steps)
+    assert eng.get_current_timestep() == ts
+    got = eng.get_simulation_data().cells
+    eng.close_simulation()
+    ref = f["out_cells"]
+    got, ref = got[np.argsort(got["id"])], ref[np.argsort(ref["id"])]
+    assert np.array_equal(got["id"], ref["id"])
+    assert np.array_equal(got["cellFunctionUsed"], ref["cellFunctionUsed"])
+    assert np.array_equal(got["signalOrigin"], ref["signalOrigin"])
+    np.testing.assert_allclose(got["signalChannels"], ref["signalChannels"], rtol=0, atol=NEURON_ATOL)
