@@ -1,6 +1,8 @@
 """Replicas across the GPUs of one node.
 
-One process per GPU (torchrun), each stepping its own worlds.  The physics
+One process per GPU (torchrun), each stepping its own worlds: either a
+replica workload per rank, or one set of worlds split across the ranks by
+cell count (``partition_worlds``).  The physics
 stage does not partition a world, and worlds never interact, so ranks share
 no data: the only cross-rank traffic is the measurement (the slowest rank's
 timed region and the sum of the work done), plus barriers around the timed
@@ -35,6 +37,11 @@ class Replicas:
         """workload seed of this rank: distinct worlds on every rank"""
         return base + 1000 * self.rank
 
+    def share(self, sizes) -> list[int]:
+        """indices of the worlds this rank steps when one set of worlds is
+        split across all ranks (``partition_worlds``)"""
+        return partition_worlds(sizes, self.world_size)[self.rank]
+
     def barrier(self) -> None:
         if self.cuda:
             self._torch.cuda.synchronize()
@@ -58,3 +65,24 @@ class Replicas:
         if self._own_group and self._dist.is_initialized():
             self._dist.destroy_process_group()
             self._own_group = False
+
+
+def partition_worlds(sizes, n_ranks: int) -> list[list[int]]:
+    """Split independent worlds across ranks, balancing the cells per rank.
+
+    Greedy longest-processing-time placement: worlds in decreasing size
+    (ties by index), each to the rank with the fewest cells so far (ties by
+    rank).  Every rank computes the same split from the same sizes, so the
+    placement needs no communication.  The largest rank load is at most
+    4/3 of the optimum (Graham's bound for this rule).  Returns the world
+    indices of each rank in ascending order.
+    """
+    if n_ranks < 1:
+        raise ValueError("n_ranks must be at least 1")
+    load = [0] * n_ranks
+    share: list[list[int]] = [[] for _ in range(n_ranks)]
+    for i in sorted(range(len(sizes)), key=lambda k: (-int(sizes[k]), k)):
+        r = min(range(n_ranks), key=lambda q: (load[q], q))
+        share[r].append(i)
+        load[r] += int(sizes[i])
+    return [sorted(s) for s in share]

@@ -311,15 +311,27 @@ def run_reference_batched(args, refrun, sample: int = 32):
 
 def run_batched(args, rank, world_size):
     """256 worlds, log-uniform 1k-200k cells: one arena stepped together vs
-    the plain engine stepping the same worlds one after another"""
+    the plain engine stepping the same worlds one after another.
+
+    ``--partition replica`` (default): every rank steps its own 256 worlds
+    (weak scaling).  ``--partition global``: the 256 worlds of rank 0 are
+    split across the ranks by cell count (strong scaling)."""
     from alien_b200 import params as P
     from alien_b200 import worldgen
     from alien_b200.facade import BatchSimulation, SimulationFacade
+    from alien_b200.replicas import partition_worlds
 
-    sizes = worldgen.batched_sizes(seed=rank, count=256)
+    if args.partition == "global":
+        sizes = worldgen.batched_sizes(seed=0, count=256)
+        mine = partition_worlds(sizes, world_size)[rank]
+        seeds = mine
+    else:
+        sizes = worldgen.batched_sizes(seed=rank, count=256)
+        mine = range(len(sizes))
+        seeds = [10_000 * rank + i for i in mine]
     worlds = []
-    for i, n in enumerate(sizes):
-        d, w = worldgen.mixed_world(seed=10_000 * rank + i, num_cells=int(n))
+    for i, sd in zip(mine, seeds):
+        d, w = worldgen.mixed_world(seed=sd, num_cells=int(sizes[i]))
         worlds.append((d, w, P.benchmark_parameters(P.MOTION_FLUID)))
     total = sum(d.num_cells for d, _, _ in worlds)
     batch = BatchSimulation(worlds)
@@ -405,6 +417,8 @@ def main():
     ap.add_argument("--pool", type=int, default=32, help="serving: distinct request worlds")
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0, help="serving: admission budget")
     ap.add_argument("--steps-per-tick", type=int, default=8, help="serving: steps of every cohort per loop tick")
+    ap.add_argument("--partition", default="replica", choices=["replica", "global"],
+                    help="batched256: each rank its own 256 worlds, or the 256 worlds split across ranks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -457,8 +471,11 @@ def main():
             line = {
                 "metric": METRIC, "value": total * args.steps / (ms / 1000.0) / 1e6, "unit": METRIC,
                 "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "batched256", "worlds": 256, "cells": r["total"],
+                "higher_is_better": True, "scaling": "strong" if args.partition == "global" else "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "batched256", "worlds": 256, "cells": total, "partition": args.partition,
+                           "parallelism": f"worlds split across {world_size} GPUs by cell count"
+                           if args.partition == "global" else f"replicas x{world_size}",
                            "description": "256 worlds, log-uniform 1k-200k cells, density 0.2, half fluid cells and half 10x10 lattices",
                            "l2": "state larger than L2, no flush"},
                 "batched_vs_plain": r["value"] / r["plain_value"],
