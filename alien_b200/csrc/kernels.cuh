@@ -349,19 +349,25 @@ struct FluidLaw {
     int best;
     unsigned long long bestId;
 
-    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float2 pos, float2 vel)
+    // the state near() and relevant() need (the scan), then the rest (the law)
+    __device__ __forceinline__ void beginScan(const DevState& st, const WorldInfo& wi, int4 me)
     {
         s = &st;
         p = &st.params[wi.paramIndex];
         g = me.x;
+        h = p->smoothingLength;
+        R = h * 2.0f;
+        R2reject = R * R * 1.0001f + 1e-6f;
+    }
+
+    __device__ __forceinline__ void beginLaw(const WorldInfo& wi, int4 me, float2 pos, float2 vel)
+    {
+        const DevState& st = *s;
         W = wi.W;
         H = wi.H;
-        h = p->smoothingLength;
         invH = 1.0f / h;
         invH2 = invH * invH;
         invH3 = invH2 * invH;
-        R = h * 2.0f;
-        R2reject = R * R * 1.0001f + 1e-6f;
         minDist = p->cellMinDistance;
         fusionVelocity = p->cellFusionVelocity;
         maxBindingEnergy = p->cellMaxBindingEnergy;
@@ -380,6 +386,12 @@ struct FluidLaw {
         bestBarrierDist = 0.0f;
         best = -1;
         bestId = ~0ull;
+    }
+
+    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float2 pos, float2 vel)
+    {
+        beginScan(st, wi, me);
+        beginLaw(wi, me, pos, vel);
     }
 
     __device__ __forceinline__ bool near(float2 pd) const { return pd.x * pd.x + pd.y * pd.y <= R2reject; }
@@ -502,7 +514,8 @@ struct CollisionLaw {
     int best;
     unsigned long long bestId;
 
-    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float2 pos, float2 vel)
+    // the state near() and relevant() need (the scan), then the rest (the law)
+    __device__ __forceinline__ void beginScan(const DevState& st, const WorldInfo& wi, int4 me)
     {
         s = &st;
         p = &st.params[wi.paramIndex];
@@ -511,20 +524,31 @@ struct CollisionLaw {
         R2reject = R * R * 1.0001f + 1e-6f;
         minDist = p->cellMinDistance;
         minDist2Keep = minDist * minDist * 1.0001f + 1e-6f;
+        barrierI = me.y & kStageBarrier;
+        const int nI = (me.y >> 4) & 0xf;
+#pragma unroll
+        for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? st.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
+    }
+
+    __device__ __forceinline__ void beginLaw(const WorldInfo&, int4 me, float2 pos, float2 vel)
+    {
         fusionVelocity = p->cellFusionVelocity;
         maxBindingEnergy = p->cellMaxBindingEnergy;
         pi = pos;
         vi = vel;
-        barrierI = me.y & kStageBarrier;
         visibleI = me.y & kStageVisible;
         const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
         densI = __int_as_float(me.z);
         fusionI = !barrierI && nI < maxI && __int_as_float(me.w) <= maxBindingEnergy;
-#pragma unroll
-        for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? st.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
         F = dx = f2(0.0f, 0.0f);
         best = -1;
         bestId = ~0ull;
+    }
+
+    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float2 pos, float2 vel)
+    {
+        beginScan(st, wi, me);
+        beginLaw(wi, me, pos, vel);
     }
 
     __device__ __forceinline__ bool near(float2 raw) const { return raw.x * raw.x + raw.y * raw.y <= R2reject; }
@@ -640,13 +664,15 @@ __device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
 // reject to a per-thread hit list in shared memory, and runs the pair law on
 // the hits afterwards: the scan loop stays convergent across the warp, and
 // the law runs once per hit instead of once per scan iteration in which any
-// lane had a hit.  Hits are visited in scan order (row by row, tile by tile,
+// lane had a hit.  The scan loop holds only the state the reject needs (the
+// law's accumulators start after it), and a cell with more than kHitCap hits
+// scans a second time, visiting on the way in the same order.  Hits are visited in scan order (row by row, tile by tile,
 // storage order), the order of the full 3x3 scan minus candidates that the
 // law ignores, so the FP32 sums do not depend on the pruning.
 // Regions whose records exceed the shared buffer, and worlds too small for
 // regions, use pairsGlobal for their cells.
 constexpr int kRegionThreads = 256;
-constexpr int kHitCap = 24;  // hit-list entries per thread before a flush
+constexpr int kHitCap = 24;  // hit-list entries per thread (more hits: the cell scans again)
 // Region shape per motion type (tiles per region, shared-buffer records,
 // resident CTAs per SM), from a sweep of shapes on the B200.  Dense regions
 // are processed in bands of rows, so the buffer size bounds no world.  The
@@ -811,33 +837,45 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
             const int lx = min(max(gx - tx0 + 1, 1), ownW);
             const int gy = ty0 + ly - 1;
             auto scan = [&](auto& law, auto diff) {
-                law.begin(s, wi, sMeta[e], pi, sVel[e]);
+                const int4 me = sMeta[e];
+                law.beginScan(s, wi, me);
                 // reach: R plus a margin above the rounding of positions up to the world size
                 const float reach = law.R * 1.0001f + 1e-3f + 4.0f * static_cast<float>(max(wi.W, wi.H)) * 1.2e-7f;
                 const float left = static_cast<float>(gx) * T, right = fminf(static_cast<float>(gx + 1) * T, static_cast<float>(wi.W));
                 const float bottom = static_cast<float>(gy) * T, top = fminf(static_cast<float>(gy + 1) * T, static_cast<float>(wi.H));
                 const int c0 = lx - (pi.x - reach < left ? 1 : 0), c1 = lx + (pi.x + reach >= right ? 1 : 0);
                 const int r0 = ly - (pi.y - reach < bottom ? 1 : 0), r1 = ly + (pi.y + reach >= top ? 1 : 0);
+                // scan: the hits in scan order (the first kHitCap kept, all counted)
                 int nh = 0;
-                auto flush = [&]() {
-                    for (int i = 0; i < nh; ++i) {
-                        const int m = myHits[i * kRegionThreads];
-                        law.visit(sMeta[m], sVel[m], diff(m));
-                    }
-                    nh = 0;
-                };
 #pragma unroll 1
                 for (int r = r0; r <= r1; ++r) {
                     const int b0 = tStart[r * LW + c0] - base, b1 = tStart[r * LW + c1 + 1] - base;
                     for (int m = b0; m < b1; ++m) {
                         const float2 dm = diff(m);
                         if (law.near(dm) && law.relevant(sMeta, m, dm)) {
-                            myHits[nh * kRegionThreads] = static_cast<uint16_t>(m);
-                            if (++nh == kHitCap) flush();
+                            if (nh < kHitCap) myHits[nh * kRegionThreads] = static_cast<uint16_t>(m);
+                            ++nh;
                         }
                     }
                 }
-                flush();
+                // law over the hits; a cell with more hits than the list holds
+                // scans again and visits on the way, in the same order
+                law.beginLaw(wi, me, pi, sVel[e]);
+                if (nh <= kHitCap) {
+                    for (int i = 0; i < nh; ++i) {
+                        const int m = myHits[i * kRegionThreads];
+                        law.visit(sMeta[m], sVel[m], diff(m));
+                    }
+                } else {
+#pragma unroll 1
+                    for (int r = r0; r <= r1; ++r) {
+                        const int b0 = tStart[r * LW + c0] - base, b1 = tStart[r * LW + c1 + 1] - base;
+                        for (int m = b0; m < b1; ++m) {
+                            const float2 dm = diff(m);
+                            if (law.near(dm) && law.relevant(sMeta, m, dm)) law.visit(sMeta[m], sVel[m], dm);
+                        }
+                    }
+                }
                 law.end();
             };
             if (Motion == ALIEN_B200_MOTION_FLUID) {
