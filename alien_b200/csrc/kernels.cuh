@@ -665,16 +665,17 @@ __device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
 // the hits afterwards: the scan loop stays convergent across the warp, and
 // the law runs once per hit instead of once per scan iteration in which any
 // lane had a hit.  The scan loop holds only the state the reject needs (the
-// law's accumulators start after it), and a cell with more than kHitCap hits
-// scans a second time, visiting on the way in the same order.  Hits are visited in scan order (row by row, tile by tile,
-// storage order), the order of the full 3x3 scan minus candidates that the
-// law ignores, so the FP32 sums do not depend on the pruning.
+// law's accumulators start after it), and a cell with more than HitCap hits
+// scans a second time, visiting on the way in the same order.  Hits are
+// visited in scan order (row by row, tile by tile, storage order), the order
+// of the full 3x3 scan minus candidates that the law ignores, so the FP32
+// sums do not depend on the pruning.
 // Regions whose records exceed the shared buffer, and worlds too small for
 // regions, use pairsGlobal for their cells.
 constexpr int kRegionThreads = 256;
-constexpr int kHitCap = 24;  // hit-list entries per thread (more hits: the cell scans again)
 // Region shape per motion type (tiles per region, shared-buffer records,
-// resident CTAs per SM), from a sweep of shapes on the B200.  Dense regions
+// hit-list entries per thread, resident CTAs per SM), from a sweep of shapes
+// on the B200.  Dense regions
 // are processed in bands of rows, so the buffer size bounds no world.  The
 // visiting order does not depend on the shape; the FP32 results of different
 // builds can still differ in the last bit where the compiler contracts
@@ -683,23 +684,24 @@ template <int Motion>
 struct RegionShape;
 template <>
 struct RegionShape<ALIEN_B200_MOTION_FLUID> {
-    static constexpr int W = 32, H = 8, Cap = 1152, MinBlocks = 3;
+    static constexpr int W = 32, H = 8, Cap = 1152, HitCap = 24, MinBlocks = 3;
 };
 template <>
 struct RegionShape<ALIEN_B200_MOTION_COLLISION> {
-    static constexpr int W = 24, H = 16, Cap = 1152, MinBlocks = 4;
+    static constexpr int W = 24, H = 16, Cap = 1152, HitCap = 24, MinBlocks = 4;
 };
 template <int Motion>
 constexpr size_t regionDynSmem()
 {
     return static_cast<size_t>(RegionShape<Motion>::Cap) * (sizeof(int4) + 2 * sizeof(float2))
-           + static_cast<size_t>(kHitCap) * kRegionThreads * sizeof(uint16_t);
+           + static_cast<size_t>(RegionShape<Motion>::HitCap) * kRegionThreads * sizeof(uint16_t);
 }
 
 template <int Motion>
 __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks) kPairsRegion(DevState s)
 {
     constexpr int kRegionCap = RegionShape<Motion>::Cap;
+    constexpr int kHitCap = RegionShape<Motion>::HitCap;
     constexpr int kRegionMaxH = RegionShape<Motion>::H;
     constexpr int kRegionMaxTiles = (RegionShape<Motion>::W + 2) * (RegionShape<Motion>::H + 2);
     extern __shared__ int4 dyn[];
@@ -775,11 +777,18 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
         if (threadIdx.x == 0) tStart[NT] = static_cast<int>(total);
     }
     __syncthreads();
-    if (threadIdx.x <= ownH) {
-        // own records of rows 1..r (own row segments are [tStart[r*LW+1], tStart[r*LW+ownW+1]))
-        int acc = 0;
-        for (int r = 1; r <= static_cast<int>(threadIdx.x); ++r) acc += tStart[r * LW + ownW + 1] - tStart[r * LW + 1];
-        rowOwn[threadIdx.x] = acc;
+    static_assert(kRegionMaxH < 32, "own rows are scanned by one warp");
+    if (threadIdx.x < 32) {
+        // own records of rows 1..r (own row segments are [tStart[r*LW+1], tStart[r*LW+ownW+1])),
+        // an inclusive scan over the rows in warp 0
+        const int r = threadIdx.x;
+        int acc = r >= 1 && r <= ownH ? tStart[r * LW + ownW + 1] - tStart[r * LW + 1] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, acc, o);
+            if (r >= o) acc += y;
+        }
+        if (r <= ownH) rowOwn[r] = acc;
     }
     __syncthreads();
     uint16_t* myHits = sHits + threadIdx.x;
