@@ -7,7 +7,11 @@ together:
 
 * admission: a waiting request is admitted when its estimated device bytes fit
   into the HBM budget next to the resident worlds; requests that arrive while
-  others run are admitted at the next tick (no queue barrier);
+  others run are admitted at the next admission wave (no queue barrier).
+  Waves are at least ``admit_interval`` seconds apart while cohorts run, so
+  that arrivals gather into fewer, larger cohorts: every cohort costs its
+  own kernel launches per step, and many one-world cohorts spend the device
+  on launches instead of cells;
 * cohorts: each admission wave becomes one batch arena (alien_b200_batch)
   whose worlds carry per-world step budgets, so a world stops exactly after
   its requested steps without host synchronisation;
@@ -86,10 +90,14 @@ class _Cohort:
 
 class ServingLoop:
     def __init__(self, hbm_budget_bytes: int, keep_results: bool = False, max_cohort_worlds: int = 256,
-                 steps_per_tick: int = 4):
+                 steps_per_tick: int = 4, admit_interval: float = 0.0):
         if not 1 <= steps_per_tick <= 64:
             raise ValueError("steps_per_tick must be in [1, 64]")
+        if admit_interval < 0:
+            raise ValueError("admit_interval must be >= 0")
         self.steps_per_tick = int(steps_per_tick)
+        self.admit_interval = float(admit_interval)
+        self.last_admit: float | None = None
         self.budget = int(hbm_budget_bytes)
         self.keep_results = keep_results
         self.max_cohort_worlds = max_cohort_worlds
@@ -97,6 +105,7 @@ class ServingLoop:
         self.cohorts: list[_Cohort] = []
         self.finished: list[Request] = []
         self.tick_ms: list[float] = []
+        self.waits: list[float] = []  # seconds from arrival to admission
         self.cell_steps = 0
 
     def resident_bytes(self) -> int:
@@ -106,6 +115,10 @@ class ServingLoop:
         self.waiting.append(req)
 
     def _admit(self, now: float) -> None:
+        if not self.waiting:
+            return
+        if self.cohorts and self.last_admit is not None and now - self.last_admit < self.admit_interval:
+            return
         free = self.budget - self.resident_bytes()
         wave, wave_bytes = [], 0
         rest = []
@@ -121,7 +134,9 @@ class ServingLoop:
             for r in wave:
                 r.admitted = now
                 r.cells = r.data.num_cells
+                self.waits.append(max(0.0, now - r.arrival))
             self.cohorts.append(_Cohort(wave))
+            self.last_admit = now
 
     def tick(self, now: float) -> float:
         """``steps_per_tick`` timesteps of every running cohort, each cohort
@@ -163,7 +178,10 @@ class ServingLoop:
 
     def report(self, wall_s: float) -> dict:
         t = np.array(self.tick_ms) if self.tick_ms else np.zeros(1)
+        wq = np.array(self.waits) if self.waits else np.zeros(1)
         return {
+            "p50_admission_wait_s": float(np.percentile(wq, 50)),
+            "p99_admission_wait_s": float(np.percentile(wq, 99)),
             "requests_finished": len(self.finished),
             "requests_waiting": len(self.waiting),
             "ticks": len(self.tick_ms),
@@ -176,11 +194,11 @@ class ServingLoop:
 
 def run_poisson(make_request: Callable[[int, np.random.Generator], Request], rate_per_s: float, duration_s: float,
                 hbm_budget_bytes: int, seed: int = 0, keep_results: bool = False, drain: bool = True,
-                steps_per_tick: int = 4) -> dict:
+                steps_per_tick: int = 4, admit_interval: float = 0.0) -> dict:
     """Poisson arrivals at ``rate_per_s`` for ``duration_s`` seconds of wall
     time; requests are built by ``make_request(rid, rng)``."""
     rng = np.random.default_rng(seed)
-    loop = ServingLoop(hbm_budget_bytes, keep_results, steps_per_tick=steps_per_tick)
+    loop = ServingLoop(hbm_budget_bytes, keep_results, steps_per_tick=steps_per_tick, admit_interval=admit_interval)
     t0 = time.perf_counter()
     next_arrival = rng.exponential(1.0 / rate_per_s)
     rid = 0

@@ -397,7 +397,7 @@ def run_serving(args, rank):
     with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
         out = serving.run_poisson(make, rate_per_s=args.rate, duration_s=args.duration,
                                   hbm_budget_bytes=int(args.hbm_budget_gb * 1e9), seed=rank, drain=False,
-                                  steps_per_tick=args.steps_per_tick)
+                                  steps_per_tick=args.steps_per_tick, admit_interval=args.admit_interval)
     out["clocks"] = clk.summary()
     for p in pins:
         unpin(p)
@@ -417,6 +417,8 @@ def main():
     ap.add_argument("--pool", type=int, default=32, help="serving: distinct request worlds")
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0, help="serving: admission budget")
     ap.add_argument("--steps-per-tick", type=int, default=8, help="serving: steps of every cohort per loop tick")
+    ap.add_argument("--admit-interval", type=float, default=0.5,
+                    help="serving: seconds between admission waves while cohorts run")
     ap.add_argument("--partition", default="replica", choices=["replica", "global"],
                     help="batched256: each rank its own 256 worlds, or the 256 worlds split across ranks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -450,12 +452,13 @@ def main():
                 "warmup": 0, "ms_per_step": r["p50_step_ms"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": "serving", "rate_per_s": args.rate, "duration_s": args.duration,
-                           "steps_per_tick": args.steps_per_tick,
+                           "steps_per_tick": args.steps_per_tick, "admit_interval_s": args.admit_interval,
                            "hbm_budget_gb": args.hbm_budget_gb, "pool_worlds": args.pool,
                            "description": "Poisson arrivals, worlds of log-uniform 5k-500k cells (half fluid, half "
                                           "10x10 lattices, a third of the lattices neuron cells), log-uniform "
                                           "100-5000 steps, continuous batching"},
                 "p50_step_ms": r["p50_step_ms"], "p99_step_ms": r["p99_step_ms"],
+                "admission_wait_s": {"p50": r["p50_admission_wait_s"], "p99": r["p99_admission_wait_s"]},
                 "requests": {"submitted": r["requests_submitted"], "finished": r["requests_finished"],
                              "waiting": r["requests_waiting"]},
                 "wall_s": r["wall_s"], "clocks": r["clocks"],
