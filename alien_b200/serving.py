@@ -8,10 +8,10 @@ together:
 * admission: a waiting request is admitted when its estimated device bytes fit
   into the HBM budget next to the resident worlds; requests that arrive while
   others run are admitted at the next admission wave (no queue barrier).
-  Waves are at least ``admit_interval`` seconds apart while cohorts run, so
-  that arrivals gather into fewer, larger cohorts: every cohort costs its
-  own kernel launches per step, and many one-world cohorts spend the device
-  on launches instead of cells;
+  Waves can be held ``admit_interval`` seconds apart while cohorts run, so
+  that arrivals gather into fewer, larger cohorts (fewer launches per step)
+  at the price of a longer wait before admission; the default admits at
+  every tick;
 * cohorts: each admission wave becomes one batch arena (alien_b200_batch)
   whose worlds carry per-world step budgets, so a world stops exactly after
   its requested steps without host synchronisation;
@@ -19,8 +19,9 @@ together:
   worlds, each cohort on its own CUDA stream so that their kernels overlap on
   the device; the tick's wall time per step is the per-step latency every
   running request sees (p50 / p99 reported);
-* a cohort whose worlds are all done is read back (results) and freed, which
-  returns its bytes to the budget.
+* a request whose steps are done is finished at once (its world no longer
+  steps; its results are read while the cohort runs on); a cohort whose
+  worlds are all done is freed, which returns its bytes to the budget.
 
 Results do not depend on what else is resident: every world evolves under the
 same deterministic step as alone (tests/test_batch_gpu.py checks alone vs in
@@ -80,11 +81,19 @@ class _Cohort:
     def done(self) -> bool:
         return self.steps_done >= self.max_steps
 
-    def close(self, now: float, keep_results: bool):
+    def finish_done(self, now: float, keep_results: bool) -> list[Request]:
+        """requests whose step budget is used up, finished now: their worlds no
+        longer step, so their results can be read while the cohort runs on"""
+        out = []
         for w, r in enumerate(self.requests):
-            r.finished = now
-            if keep_results:
-                r.result = self.batch.get_simulation_data(w)
+            if r.finished is None and r.steps <= self.steps_done:
+                r.finished = now
+                if keep_results:
+                    r.result = self.batch.get_simulation_data(w)
+                out.append(r)
+        return out
+
+    def close(self):
         self.batch.close()
 
 
@@ -163,11 +172,12 @@ class ServingLoop:
             c.steps_done += k
         self.tick_ms.append(ms)
         done_now = time.perf_counter()
+        for c in running:
+            self.finished.extend(c.finish_done(done_now, self.keep_results))
         keep = []
         for c in self.cohorts:
             if c in running and c.done:
-                c.close(done_now, self.keep_results)
-                self.finished.extend(c.requests)
+                c.close()
             else:
                 keep.append(c)
         self.cohorts = keep

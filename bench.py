@@ -417,7 +417,7 @@ def main():
     ap.add_argument("--pool", type=int, default=32, help="serving: distinct request worlds")
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0, help="serving: admission budget")
     ap.add_argument("--steps-per-tick", type=int, default=8, help="serving: steps of every cohort per loop tick")
-    ap.add_argument("--admit-interval", type=float, default=0.5,
+    ap.add_argument("--admit-interval", type=float, default=0.0,
                     help="serving: seconds between admission waves while cohorts run")
     ap.add_argument("--partition", default="replica", choices=["replica", "global"],
                     help="batched256: each rank its own 256 worlds, or the 256 worlds split across ranks")

@@ -30,9 +30,16 @@ class FakeCohort:
     def done(self):
         return self.steps_done >= self.max_steps
 
-    def close(self, now, keep_results):
+    def finish_done(self, now, keep_results):
+        out = []
         for r in self.requests:
-            r.finished = now
+            if r.finished is None and r.steps <= self.steps_done:
+                r.finished = now
+                out.append(r)
+        return out
+
+    def close(self):
+        pass
 
 
 @pytest.fixture
@@ -88,3 +95,16 @@ def test_interval_validation():
         serving.ServingLoop(1 << 30, admit_interval=-1.0)
     with pytest.raises(ValueError):
         serving.ServingLoop(1 << 30, steps_per_tick=0)
+
+
+def test_requests_finish_before_their_cohort(fake_cohorts):
+    loop = serving.ServingLoop(hbm_budget_bytes=1 << 40, steps_per_tick=4)
+    short, long_ = _request(0, 4), _request(1, 40)
+    loop.submit(short)
+    loop.submit(long_)
+    loop.tick(0.0)                      # one cohort with both
+    loop.tick(0.0)                      # 4 steps: the short one is finished
+    assert [r.rid for r in loop.finished] == [0] and len(loop.cohorts) == 1
+    while not loop.idle():
+        loop.tick(0.0)
+    assert [r.rid for r in loop.finished] == [0, 1]
