@@ -691,7 +691,7 @@ void Arena::enqueueStep()
     if (signalsLive_) launch(kSignalReset, cells, kBlock, s);
     launch(kCommit, cells, kBlock, s);
     launch(kEventCount, both, kBlock, s);
-    launch(kEventWorld, s.numWorlds, kBlock, s);
+    launch(kEventWorld, s.numWorlds, kEventWorldThreads, s);
     launch(kEventEmit, both, kBlock, s);
     kernelsPerStep_ = static_cast<int>(launches_ - before);
 }

@@ -311,20 +311,29 @@ __global__ void __launch_bounds__(kBlock) kStatsWorld(DevState s, int w, StatsAc
     unsigned int byColor[ALIEN_B200_MAX_COLORS] = {};
     long long cellE = 0, partE = 0;
     const long long cellEnd = wi.cellBase + wc.numCells;
+    // the fields of a slot are loaded together (every slot below the count
+    // is allocated), then dead slots are skipped
+#pragma unroll 4
     for (long long g = wi.cellBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x; g < cellEnd; g += stride) {
-        if (!s.alive[g]) continue;
-        ++cells;
-        bonds += s.numConn[g];
-        cellE += __double2ll_rn(static_cast<double>(s.energy[g]) * 65536.0);
+        const bool alive = s.alive[g];
+        const unsigned int nc = s.numConn[g];
+        const float e = s.energy[g];
         const int col = s.color[g] % ALIEN_B200_MAX_COLORS;
+        if (!alive) continue;
+        ++cells;
+        bonds += nc;
+        cellE += __double2ll_rn(static_cast<double>(e) * 65536.0);
 #pragma unroll
         for (int c = 0; c < ALIEN_B200_MAX_COLORS; ++c) byColor[c] += col == c ? 1u : 0u;
     }
     const long long partEnd = wi.partBase + wc.numParticles;
+#pragma unroll 4
     for (long long q = wi.partBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x; q < partEnd; q += stride) {
-        if (!s.palive[q]) continue;
+        const bool alive = s.palive[q];
+        const float e = s.penergy[q];
+        if (!alive) continue;
         ++parts;
-        partE += __double2ll_rn(static_cast<double>(s.penergy[q]) * 65536.0);
+        partE += __double2ll_rn(static_cast<double>(e) * 65536.0);
     }
     unsigned long long v[kStatsFields];
     v[0] = cells;

@@ -1833,18 +1833,19 @@ __global__ void __launch_bounds__(kBlock) kEventCount(DevState s)
     }
 }
 
-// exclusive scan of arr[first .. first+count) in place by one block: each
-// thread scans a contiguous chunk, the chunk sums are scanned across the
-// block; returns the total
+// exclusive scan of arr[first .. first+count) in place by one block of
+// Threads threads: each thread scans a contiguous chunk, the chunk sums are
+// scanned across the block; returns the total
+template <int Threads>
 __device__ uint32_t blockScanBlocks(uint32_t* arr, int first, int count)
 {
-    const int chunk = (count + kBlock - 1) / kBlock;
+    const int chunk = (count + Threads - 1) / Threads;
     const int b0 = threadIdx.x * chunk;
     const int b1 = min(b0 + chunk, count);
     uint32_t sum = 0;
     for (int k = b0; k < b1; ++k) sum += arr[first + k];
     uint32_t total;
-    uint32_t run = blockExclusiveScan(sum, &total);
+    uint32_t run = blockExclusiveScanN<Threads>(sum, &total);
     for (int k = b0; k < b1; ++k) {
         const uint32_t v = arr[first + k];
         arr[first + k] = run;
@@ -1854,8 +1855,10 @@ __device__ uint32_t blockScanBlocks(uint32_t* arr, int first, int count)
 }
 
 // one block per world: block offsets, id and slot bases, timestep advance;
-// the block scans run only for the kinds of events the step produced
-__global__ void __launch_bounds__(kBlock) kEventWorld(DevState s)
+// the block scans run only for the kinds of events the step produced (1024
+// threads ran slower than 256 on a 4M-cell world's 15,625 block counts)
+constexpr int kEventWorldThreads = kBlock;
+__global__ void __launch_bounds__(kEventWorldThreads) kEventWorld(DevState s)
 {
     const int w = blockIdx.x;
     WorldCounters& wc = s.counters[w];
@@ -1871,9 +1874,9 @@ __global__ void __launch_bounds__(kBlock) kEventWorld(DevState s)
     const WorldInfo& wi = s.worlds[w];
     // particle blocks holding used slots (the count before this step's appends)
     const int usedPartBlocks = static_cast<int>((wc.numParticles + kBlock - 1) / kBlock);
-    const uint32_t R = evR ? blockScanBlocks(s.blockRad, wi.firstCellBlock, wi.numCellBlocks) : 0u;
-    const uint32_t D = evD ? blockScanBlocks(s.blockDel, wi.firstCellBlock, wi.numCellBlocks) : 0u;
-    const uint32_t S = evS ? blockScanBlocks(s.blockSplit, wi.firstPartBlock, usedPartBlocks) : 0u;
+    const uint32_t R = evR ? blockScanBlocks<kEventWorldThreads>(s.blockRad, wi.firstCellBlock, wi.numCellBlocks) : 0u;
+    const uint32_t D = evD ? blockScanBlocks<kEventWorldThreads>(s.blockDel, wi.firstCellBlock, wi.numCellBlocks) : 0u;
+    const uint32_t S = evS ? blockScanBlocks<kEventWorldThreads>(s.blockSplit, wi.firstPartBlock, usedPartBlocks) : 0u;
     if (threadIdx.x != 0) return;
     wc.evRad = wc.evDel = wc.evSplit = 0;
     const unsigned long long id0 = wc.nextId;
@@ -1930,9 +1933,21 @@ __global__ void __launch_bounds__(kBlock) kEventEmit(DevState s)
         const long long g = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
         // without events kEventCount has cleared every flag already
         if (wc.numEvents == 0) return;
+        const WorldInfo& wi = s.worlds[w];
+        // the same for a block without events: its event count is the
+        // difference of consecutive block offsets (the world's total after
+        // its last block; offsets stay zero for a kind the step did not
+        // produce); the test is uniform across the block, ahead of its scans
+        {
+            const int b = blockIdx.x, lastBlock = wi.firstCellBlock + wi.numCellBlocks - 1;
+            const uint32_t totalRad = static_cast<uint32_t>(wc.splitIdBase - wc.radIdBase);
+            const uint32_t totalDel = static_cast<uint32_t>(wc.nextId - wc.delIdBase);
+            const uint32_t nRad = (b < lastBlock ? s.blockRad[b + 1] : totalRad) - s.blockRad[b];
+            const uint32_t nDel = (b < lastBlock ? s.blockDel[b + 1] : totalDel) - s.blockDel[b];
+            if (nRad == 0 && nDel == 0) return;
+        }
         const uint32_t fl = s.flags[g];
         if (fl) s.flags[g] = 0;  // the step's flags end here
-        const WorldInfo& wi = s.worlds[w];
         const bool inRange = g < wi.cellBase + wc.numCells;
         const uint32_t rad = inRange && (fl & kFlagRadiation) ? 1u : 0u;
         const uint32_t del = inRange && (fl & kFlagDelCell) && s.energy[g] > kNearZero ? 1u : 0u;
