@@ -14,8 +14,9 @@
 //   kScatter    cell slots grouped by tile
 //   kStage      per-slot rank (scan visibility) + sorted SoA copy
 //   kPairs*     fluid or collision pair forces (physics_calc*Forces)
-//   kApplyBond1 checkForces, applyForces, bond forces #1 | particle movement
-//   kVerletPos  verletPositionUpdate                     | particle targets
+//   kApplyBond1 checkForces, applyForces, bond forces #1, | particle movement
+//               verletPositionUpdate (steps without angle forces)
+//   kVerletPos  verletPositionUpdate (angle-force steps) | particle targets
 //   kBond2      checkConnections, bond forces #2         | particle merges
 //   kVerletVel  verletVelocityUpdate, aging              | absorption
 //   kTransition living-state transition, inner friction, | splitting,
@@ -1024,6 +1025,28 @@ __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, cons
     return F;
 }
 
+// verletPositionUpdate (CellProcessor.cuh:525-544) of cell g from its
+// overlap-corrected position, velocity v, bond force F1 and the fixed-point
+// angle forces (ax, ay); stores the total force of a non-barrier cell and
+// returns the new position
+__device__ __forceinline__ float2 verletPosition(const DevState& s, long long g, const WorldInfo& wi,
+                                                 const AlienPhysicsParams& p, bool barrierG, float2 v, float2 F1,
+                                                 long long ax, long long ay)
+{
+    const float dt = p.timestepSize;
+    const float2 pb = s.posB[g];
+    float2 np;
+    if (barrierG) {
+        s.force1[g] = F1;
+        np = pb + v * dt;
+    } else {
+        const float2 F = F1 + f2(fromFix(ax), fromFix(ay));
+        s.force1[g] = F;
+        np = pb + (v * dt + F * dt * dt / 2.0f);
+    }
+    return correctPosition(np, wi.W, wi.H);
+}
+
 // -------------------------------------------------------- kApplyBond1 ----
 // cells: checkForces + applyForces (CellProcessor.cuh:367-406), bond forces
 // #1 at the overlap-corrected positions.  particles: movement
@@ -1038,19 +1061,28 @@ __global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
         const uint64_t T = s.counters[c.w].timestep;
         if (p.motionType == ALIEN_B200_MOTION_FLUID) s.density[g] = s.densNew[g];
-        if (!s.barrier[g]) {
+        const bool barrierG = s.barrier[g];
+        float2 v = s.velA[g];
+        if (!barrierG) {
             const int col = s.color[g] % ALIEN_B200_MAX_COLORS;
             const float2 F = s.force[g];
             if (len2(F) > p.cellMaxForce[col]) {
                 if (draw(s.id[g], T, kSiteForceDecay) < p.cellMaxForceDecayProb) atomicOr(&s.flags[g], kFlagDelAll);
             }
-            float2 v = s.velA[g] + F;
+            v = v + F;
             if (len2(v) > p.cellMaxVelocity) v = normalized2(v) * p.cellMaxVelocity;
             s.velA[g] = v;
         }
         BondRow r;
         loadBondRow(s, g, s.posB, wi.W, wi.H, r);
-        s.force1[g] = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 0);
+        const float2 F1 = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 0);
+        if (T % 3 == 0) {
+            s.force1[g] = F1;  // angle forces of other cells still arrive: kVerletPos
+        } else {
+            // no angle forces this step: verletPositionUpdate here, with the
+            // arithmetic of kVerletPos for empty accumulators
+            s.posA[g] = verletPosition(s, g, wi, p, barrierG, v, F1, 0, 0);
+        }
     } else {
         forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
             if (!c.inRange || !s.palive[c.q]) return;
@@ -1062,37 +1094,29 @@ __global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
 }
 
 // --------------------------------------------------------- kVerletPos ----
-// cells: verletPositionUpdate (CellProcessor.cuh:525-544).
+// cells: verletPositionUpdate (CellProcessor.cuh:525-544) in steps with
+// timestep % 3 == 0, after the angle forces of all cells have arrived; in the
+// other steps kApplyBond1 has done it already.
 // particles: merge target (RadiationProcessor::collision, :78-80).
 __global__ void __launch_bounds__(kBlock, 8) kVerletPos(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
+        if (s.counters[s.cellBlockWorld[blockIdx.x]].timestep % 3 != 0) return;
         CellCtx c = cellCtx(s);
         if (!c.valid) return;
         const long long g = c.g;
         const WorldInfo& wi = s.worlds[c.w];
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
-        const float dt = p.timestepSize;
-        const float2 v = s.velA[g];
-        const float2 pb = s.posB[g];
-        float2 np;
-        if (s.barrier[g]) {
-            np = pb + v * dt;
-        } else {
-            // angle forces are scattered only in steps with timestep % 3 == 0
-            // and consumed in the same step: other steps find zeros
-            long long ax = 0, ay = 0;
-            if (s.counters[c.w].timestep % 3 == 0) {
-                const longlong2 a = *reinterpret_cast<const longlong2*>(s.angleAcc + 4 * g);
-                ax = a.x;
-                ay = a.y;
-                if (ax | ay) *reinterpret_cast<longlong2*>(s.angleAcc + 4 * g) = make_longlong2(0, 0);
-            }
-            const float2 F1 = s.force1[g] + f2(fromFix(ax), fromFix(ay));
-            s.force1[g] = F1;
-            np = pb + (v * dt + F1 * dt * dt / 2.0f);
+        const bool barrierG = s.barrier[g];
+        long long ax = 0, ay = 0;
+        if (!barrierG) {
+            // angle forces are scattered only in these steps and consumed here
+            const longlong2 a = *reinterpret_cast<const longlong2*>(s.angleAcc + 4 * g);
+            ax = a.x;
+            ay = a.y;
+            if (ax | ay) *reinterpret_cast<longlong2*>(s.angleAcc + 4 * g) = make_longlong2(0, 0);
         }
-        s.posA[g] = correctPosition(np, wi.W, wi.H);
+        s.posA[g] = verletPosition(s, g, wi, p, barrierG, s.velA[g], s.force1[g], ax, ay);
     } else {
         forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
             if (!c.inRange || !s.palive[c.q]) return;
