@@ -42,11 +42,15 @@ __device__ __forceinline__ CellCtx cellCtx(const DevState& s)
 {
     CellCtx c;
     int b = blockIdx.x;
-    c.w = s.cellBlockWorld[b];
     c.g = static_cast<long long>(b) * kBlock + threadIdx.x;
+    // every launched cell slot lies inside the arena (the cell blocks tile
+    // it exactly), so the alive flag is loaded together with the world
+    // lookup instead of after it
+    const bool alive = s.alive[c.g];
+    c.w = s.cellBlockWorld[b];
     const WorldInfo& wi = s.worlds[c.w];
     const WorldCounters& wc = s.counters[c.w];
-    c.valid = wc.active && c.g < wi.cellBase + wc.numCells && s.alive[c.g];
+    c.valid = wc.active && c.g < wi.cellBase + wc.numCells && alive;
     return c;
 }
 
@@ -156,19 +160,22 @@ __global__ void __launch_bounds__(kBlock, 8) kBin(DevState s)
         // per-step scratch needs no reset here: flags are cleared by
         // kEventEmit, the fixed-point accumulators and newPartner by the
         // kernels that consume them, and best is written for every live cell
+        // own fields before the world lookup (every launched cell slot lies
+        // inside the arena)
+        const float2 pos = s.posA[static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x];
+        const bool barrierG = s.barrier[static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x];
         CellCtx c = cellCtx(s);
         const long long g = c.g;
         if (!c.valid) return;
         const WorldInfo& wi = s.worlds[c.w];
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
-        float2 pos = s.posA[g];
         int sx = slotX(pos.x, wi.W), sy = slotX(pos.y, wi.H);
         uint32_t tile = static_cast<uint32_t>(wi.tileBase + (sx / wi.T) + static_cast<long long>(sy / wi.T) * wi.nTX);
         s.tileOf[g] = tile;
         s.slotOf[g] = static_cast<uint32_t>(sx + sy * wi.W);
         s.tileOff[g] = atomicAdd(&s.tileCount[tile], 1u);
 
-        if (s.barrier[g] || !(p.radiationProb > 0.0f)) return;  // a draw in [0, 1) never falls below 0
+        if (barrierG || !(p.radiationProb > 0.0f)) return;  // a draw in [0, 1) never falls below 0
         const uint64_t T = s.counters[c.w].timestep;
         const uint64_t id = s.id[g];
         if (!(draw(id, T, kSiteRadiation) < p.radiationProb)) return;
@@ -275,9 +282,11 @@ __global__ void __launch_bounds__(kBlock) kScanDown(const uint32_t* in, long lon
 // ----------------------------------------------------------- kScatter ----
 __global__ void __launch_bounds__(kBlock) kScatter(DevState s)
 {
+    const long long g0 = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    const uint32_t t = s.tileOf[g0], off = s.tileOff[g0];  // before the world lookup
     CellCtx c = cellCtx(s);
     if (!c.valid) return;
-    s.sorted[s.tileStart[s.tileOf[c.g]] + s.tileOff[c.g]] = static_cast<uint32_t>(c.g);
+    s.sorted[s.tileStart[t] + off] = static_cast<uint32_t>(c.g);
 }
 
 // ------------------------------------------------------------- kStage ----
@@ -914,10 +923,10 @@ struct BondRow {
     float2 disp[kMaxBonds];  // corrected partner - cell
 };
 
-__device__ __forceinline__ void loadBondRow(const DevState& s, long long g, const float2* __restrict__ P, int W, int H,
-                                            BondRow& r)
+__device__ __forceinline__ void loadBondRow(const DevState& s, long long g, int n, const float2* __restrict__ P, int W,
+                                            int H, BondRow& r)
 {
-    r.n = s.numConn[g];
+    r.n = n;
     const int2* row = reinterpret_cast<const int2*>(s.bond + g * kMaxBonds);
     const float2 pi = P[g];
 #pragma unroll
@@ -1054,18 +1063,22 @@ __device__ __forceinline__ float2 verletPosition(const DevState& s, long long g,
 __global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
+        // own fields before the world lookup and the first store (every
+        // launched cell slot lies inside the arena; no other cell writes
+        // them in this kernel)
+        const long long g0 = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+        const bool barrierG = s.barrier[g0];
+        const int n = s.numConn[g0];
+        const int col = s.color[g0] % ALIEN_B200_MAX_COLORS;
+        const float2 F = s.force[g0];
+        float2 v = s.velA[g0];
         CellCtx c = cellCtx(s);
         if (!c.valid) return;
         const long long g = c.g;
         const WorldInfo& wi = s.worlds[c.w];
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
         const uint64_t T = s.counters[c.w].timestep;
-        if (p.motionType == ALIEN_B200_MOTION_FLUID) s.density[g] = s.densNew[g];
-        const bool barrierG = s.barrier[g];
-        float2 v = s.velA[g];
         if (!barrierG) {
-            const int col = s.color[g] % ALIEN_B200_MAX_COLORS;
-            const float2 F = s.force[g];
             if (len2(F) > p.cellMaxForce[col]) {
                 if (draw(s.id[g], T, kSiteForceDecay) < p.cellMaxForceDecayProb) atomicOr(&s.flags[g], kFlagDelAll);
             }
@@ -1074,7 +1087,7 @@ __global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
             s.velA[g] = v;
         }
         BondRow r;
-        loadBondRow(s, g, s.posB, wi.W, wi.H, r);
+        loadBondRow(s, g, n, s.posB, wi.W, wi.H, r);
         const float2 F1 = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 0);
         if (T % 3 == 0) {
             s.force1[g] = F1;  // angle forces of other cells still arrive: kVerletPos
@@ -1083,6 +1096,7 @@ __global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
             // arithmetic of kVerletPos for empty accumulators
             s.posA[g] = verletPosition(s, g, wi, p, barrierG, v, F1, 0, 0);
         }
+        if (p.motionType == ALIEN_B200_MOTION_FLUID) s.density[g] = s.densNew[g];
     } else {
         forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
             if (!c.inRange || !s.palive[c.q]) return;
@@ -1102,21 +1116,27 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletPos(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         if (s.counters[s.cellBlockWorld[blockIdx.x]].timestep % 3 != 0) return;
+        // own fields before the world lookup (every launched cell slot lies
+        // inside the arena; no other cell writes them in this kernel)
+        const long long g0 = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+        const bool barrierG = s.barrier[g0];
+        const float2 v = s.velA[g0];
+        const float2 F1 = s.force1[g0];
+        const longlong2 a = *reinterpret_cast<const longlong2*>(s.angleAcc + 4 * g0);
         CellCtx c = cellCtx(s);
         if (!c.valid) return;
         const long long g = c.g;
         const WorldInfo& wi = s.worlds[c.w];
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
-        const bool barrierG = s.barrier[g];
         long long ax = 0, ay = 0;
         if (!barrierG) {
             // angle forces are scattered only in these steps and consumed here
-            const longlong2 a = *reinterpret_cast<const longlong2*>(s.angleAcc + 4 * g);
+            // (barrier cells receive none)
             ax = a.x;
             ay = a.y;
             if (ax | ay) *reinterpret_cast<longlong2*>(s.angleAcc + 4 * g) = make_longlong2(0, 0);
         }
-        s.posA[g] = verletPosition(s, g, wi, p, barrierG, s.velA[g], s.force1[g], ax, ay);
+        s.posA[g] = verletPosition(s, g, wi, p, barrierG, v, F1, ax, ay);
     } else {
         forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
             if (!c.inRange || !s.palive[c.q]) return;
@@ -1135,6 +1155,12 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletPos(DevState s)
 __global__ void __launch_bounds__(kBlock, 6) kBond2(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
+        // own fields before the world lookup (every launched cell slot lies
+        // inside the arena; no other cell writes them in this kernel)
+        const long long g0 = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+        const bool barrierG = s.barrier[g0];
+        const int n = s.numConn[g0];
+        const int col = s.color[g0] % ALIEN_B200_MAX_COLORS;
         CellCtx c = cellCtx(s);
         if (!c.valid) return;
         const long long g = c.g;
@@ -1142,9 +1168,9 @@ __global__ void __launch_bounds__(kBlock, 6) kBond2(DevState s)
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
         const uint64_t T = s.counters[c.w].timestep;
         BondRow r;
-        loadBondRow(s, g, s.posA, wi.W, wi.H, r);
-        if (!s.barrier[g]) {
-            const float maxDist = p.cellMaxBindingDistance[s.color[g] % ALIEN_B200_MAX_COLORS];
+        loadBondRow(s, g, n, s.posA, wi.W, wi.H, r);
+        if (!barrierG) {
+            const float maxDist = p.cellMaxBindingDistance[col];
             bool destroy = false;
 #pragma unroll
             for (int k = 0; k < kMaxBonds; ++k)
@@ -1199,13 +1225,24 @@ __device__ __forceinline__ int slotHead(const DevState& s, const WorldInfo& wi, 
 __global__ void __launch_bounds__(kBlock, 8) kVerletVel(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
+        // the cell's own fields are loaded before the world lookup and the
+        // first store (every launched cell slot lies inside the arena, and
+        // the cell part writes only the cell's own fields)
+        const long long g0 = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+        const float2 v = s.velA[g0];
+        const bool barrierG = s.barrier[g0];
+        const float2 F = s.force[g0];
+        const float2 F1 = s.force1[g0];
+        const int ls0 = s.livingState[g0];
+        const uint32_t fl = s.flags[g0];
+        const uint32_t age = s.age[g0];
+        const uint32_t at = s.activationTime[g0];
         CellCtx c = cellCtx(s);
         if (!c.valid) return;
         const long long g = c.g;
         const WorldInfo& wi = s.worlds[c.w];
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
-        const float2 v = s.velA[g];
-        if (s.barrier[g]) {
+        if (barrierG) {
             s.velB[g] = v;
         } else {
             long long ax = 0, ay = 0;
@@ -1215,20 +1252,17 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletVel(DevState s)
                 ay = a.y;
                 if (ax | ay) *reinterpret_cast<longlong2*>(s.angleAcc + 4 * g + 2) = make_longlong2(0, 0);
             }
-            const float2 F2 = s.force[g] + f2(fromFix(ax), fromFix(ay));
-            s.velB[g] = v + (F2 + s.force1[g]) / 2.0f * p.timestepSize;
+            const float2 F2 = F + f2(fromFix(ax), fromFix(ay));
+            s.velB[g] = v + (F2 + F1) / 2.0f * p.timestepSize;
         }
-        int ls = s.livingState[g];
-        if (s.flags[g] & kFlagDetach) {
+        int ls = ls0;
+        if (fl & kFlagDetach) {
             ls = ALIEN_B200_LIVING_DETACHING;
             s.livingState[g] = static_cast<uint8_t>(ls);
         }
-        if (!s.barrier[g]) {
-            ++s.age[g];
-            if (ls == ALIEN_B200_LIVING_READY) {
-                const uint32_t at = s.activationTime[g];
-                if (at > 0) s.activationTime[g] = at - 1;
-            }
+        if (!barrierG) {
+            s.age[g] = age + 1;
+            if (ls == ALIEN_B200_LIVING_READY && at > 0) s.activationTime[g] = at - 1;
         }
     } else {
         forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
@@ -1289,6 +1323,19 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletVel(DevState s)
 __global__ void __launch_bounds__(kBlock, 6) kTransition(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
+        // the cell's own fields are loaded before the world lookup and the
+        // first store (every launched cell slot lies inside the arena; the
+        // cell part reads no field that another cell writes in this kernel)
+        const long long g0 = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+        const int n = s.numConn[g0];
+        const uint32_t cr = s.creatureId[g0];
+        const float2 vi = s.velB[g0];
+        const int orig = s.livingState[g0];
+        const bool barrierG = s.barrier[g0];
+        const long long ea = s.energyAcc[g0];
+        const float e0 = s.energy[g0];
+        const int col = s.color[g0] % ALIEN_B200_MAX_COLORS;
+        const uint32_t age = s.age[g0];
         CellCtx c = cellCtx(s);
         if (!c.valid) return;
         const long long g = c.g;
@@ -1296,11 +1343,8 @@ __global__ void __launch_bounds__(kBlock, 6) kTransition(DevState s)
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
         const uint64_t T = s.counters[c.w].timestep;
         const bool innerFriction = T % 3 == 0;  // SimulationKernelsLauncher.cu:32
-        const int n = s.numConn[g];
-        const uint32_t cr = s.creatureId[g];
         bool sameDetaching = false, otherDetaching = false, sameReviving = false, activating = false;
         float2 acc = f2(0.0f, 0.0f);
-        const float2 vi = s.velB[g];
         // the bond row, then the partners' states (and velocities on inner-
         // friction steps) with all loads of a cell in flight together
         int jb[kMaxBonds];
@@ -1342,10 +1386,9 @@ __global__ void __launch_bounds__(kBlock, 6) kTransition(DevState s)
             for (int k = 0; k < kMaxBonds; ++k)
                 if (k < n && !bj[k]) acc = acc + (vj[k] - vi);
         }
-        const int orig = s.livingState[g];
         int ls = orig;
         const int dc = p.cellDeathConsequences;
-        if (s.barrier[g])
+        if (barrierG)
             ls = ALIEN_B200_LIVING_READY;
         else if (orig == ALIEN_B200_LIVING_ACTIVATING || orig == ALIEN_B200_LIVING_REVIVING)
             ls = ALIEN_B200_LIVING_READY;
@@ -1359,14 +1402,13 @@ __global__ void __launch_bounds__(kBlock, 6) kTransition(DevState s)
             if (sameDetaching && dc != ALIEN_B200_DEATH_NONE) ls = ALIEN_B200_LIVING_DETACHING;
         }
         s.nextState[g] = static_cast<uint8_t>(ls);
-        const long long ea = s.energyAcc[g];
-        float e = s.energy[g];
+        float e = e0;
         if (ea) {
             e += fromFix(ea);
             s.energy[g] = e;
             s.energyAcc[g] = 0;
         }
-        if (s.barrier[g]) {
+        if (barrierG) {
             s.velA[g] = vi;
             return;
         }
@@ -1375,7 +1417,6 @@ __global__ void __launch_bounds__(kBlock, 6) kTransition(DevState s)
         const float2 vf = innerFriction ? vi + acc * (p.innerFriction / 2.0f) : vi;
         s.velA[g] = vf * (1.0f - p.friction);
         // decay (CellProcessor.cuh:775-858) on the state after the transition
-        const int col = s.color[g] % ALIEN_B200_MAX_COLORS;
         uint32_t f = 0;
         if (e > p.cellMaxBindingEnergy) f |= kFlagDelAll;
         if (ls == ALIEN_B200_LIVING_DYING || ls == ALIEN_B200_LIVING_DETACHING) {
@@ -1383,7 +1424,7 @@ __global__ void __launch_bounds__(kBlock, 6) kTransition(DevState s)
         }
         bool destroy = e < p.cellMinEnergy[col];
         const long long maxAge = p.cellMaxAge[col];
-        if (maxAge > 0 && static_cast<long long>(s.age[g]) > maxAge) destroy = true;
+        if (maxAge > 0 && static_cast<long long>(age) > maxAge) destroy = true;
         if (destroy) {
             f |= kFlagSetDying;
             if (ls != ALIEN_B200_LIVING_DYING) {
@@ -1672,18 +1713,22 @@ __device__ inline bool tryAddOneWay(const DevState& s, const WorldInfo& wi, long
 // CellConnectionProcessor.cuh:130-143, 211-272), written to scratch.
 __global__ void __launch_bounds__(kBlock, 8) kResolve(DevState s)
 {
+    // own fields before the world lookup (every launched cell slot lies
+    // inside the arena; no other cell writes them in this kernel)
+    const long long g0 = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    const uint32_t f = s.flags[g0];
+    const int next = s.nextState[g0];
+    const int j = s.best[g0];
     CellCtx c = cellCtx(s);
     if (!c.valid) return;
     const long long g = c.g;
-    const uint32_t f = s.flags[g];
-    int ls = s.nextState[g];
+    int ls = next;
     if (f & kFlagSetDying)
         ls = ALIEN_B200_LIVING_DYING;
     else if ((f & kFlagDetachFromDying) && ls != ALIEN_B200_LIVING_DYING)
         ls = ALIEN_B200_LIVING_DETACHING;
     s.livingState[g] = static_cast<uint8_t>(ls);
 
-    const int j = s.best[g];
     if (j < 0 || j <= g || s.best[j] != g) return;
     const WorldInfo& wi = s.worlds[c.w];
     const bool gFirst = s.id[g] < s.id[j];
@@ -1715,16 +1760,20 @@ __global__ void __launch_bounds__(kBlock, 8) kResolve(DevState s)
 // end scheduled "delete all bonds" and the bond is not this step's addition.
 __global__ void __launch_bounds__(kBlock, 8) kCommit(DevState s)
 {
+    // own fields before the world lookup (every launched cell slot lies
+    // inside the arena; no other cell writes them in this kernel)
+    const long long g0 = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    const uint32_t f = s.flags[g0];
+    const int np = s.newPartner[g0];
+    const int n0 = s.numConn[g0];
     CellCtx c = cellCtx(s);
     if (!c.valid) return;
     const long long g = c.g;
-    const uint32_t f = s.flags[g];
     if (f & kFlagDelCell) {
         s.alive[g] = 0;
         atomicAdd(&s.counters[c.w].deadCells, 1u);
         return;
     }
-    const int np = s.newPartner[g];
     const bool delAllG = f & kFlagDelAll;
     BondList l;
     if (np >= 0) {
@@ -1738,7 +1787,7 @@ __global__ void __launch_bounds__(kBlock, 8) kCommit(DevState s)
     } else {
         // most cells keep their bonds: look at the partners' flags first and
         // read rest lengths and angles only when a bond goes
-        const int n = s.numConn[g];
+        const int n = n0;
         int jb[kMaxBonds];
         const int2* row = reinterpret_cast<const int2*>(s.bond + g * kMaxBonds);
 #pragma unroll
