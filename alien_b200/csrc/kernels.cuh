@@ -297,15 +297,25 @@ __global__ void __launch_bounds__(kBlock) kScatter(DevState s)
 __global__ void __launch_bounds__(kBlock) kStage(DevState s)
 {
     long long k = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
-    if (k >= s.tileStart[s.numTiles]) return;
+    // the launch covers the cell slots, so sorted[k] is inside the array
+    // whether or not k is below the number of binned cells
+    const uint32_t total = s.tileStart[s.numTiles];
     const uint32_t g = s.sorted[k];
+    if (k >= total) return;
+    // the cell's fields, all in flight together
     const int w = s.cellBlockWorld[g / kBlock];
-    const WorldInfo& wi = s.worlds[w];
     const uint32_t t = s.tileOf[g];
-    const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
-    const float2 pos = s.posA[g];
     const uint32_t slot = s.slotOf[g];
+    const float2 pos = s.posA[g];
+    const float2 vel = s.velA[g];
+    const bool barrierG = s.barrier[g];
+    const int nc = s.numConn[g];
+    const int mc = s.maxConn[g];
+    const float dens = s.density[g];
+    const float energy = s.energy[g];
+    const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
     int rank = 0, rankInTile = 0;
+#pragma unroll 4
     for (uint32_t m = k0; m < k1; ++m) {
         uint32_t g2 = s.sorted[m];
         if (g2 >= g) continue;
@@ -315,13 +325,12 @@ __global__ void __launch_bounds__(kBlock) kStage(DevState s)
     // records of a tile in storage order: a fixed visiting order for the
     // pair phase, whatever order the binning atomics produced
     k = k0 + rankInTile;
-    const float2 vel = s.velA[g];
-    int fl = (s.barrier[g] ? kStageBarrier : 0) | (rank < kSlotScanLevels ? kStageVisible : 0) | (rank == 0 ? kStageHead : 0);
-    fl |= (static_cast<int>(s.numConn[g]) & 0xf) << 4;
-    fl |= static_cast<int>(s.maxConn[g]) << 8;
+    int fl = (barrierG ? kStageBarrier : 0) | (rank < kSlotScanLevels ? kStageVisible : 0) | (rank == 0 ? kStageHead : 0);
+    fl |= (nc & 0xf) << 4;
+    fl |= mc << 8;
     fl |= w << 16;
     s.stagedPV[k] = make_float4(pos.x, pos.y, vel.x, vel.y);
-    s.stagedMeta[k] = make_int4(static_cast<int>(g), fl, __float_as_int(s.density[g]), __float_as_int(s.energy[g]));
+    s.stagedMeta[k] = make_int4(static_cast<int>(g), fl, __float_as_int(dens), __float_as_int(energy));
 }
 
 // ---------------------------------------------------------- pair laws ----
@@ -1845,11 +1854,8 @@ __global__ void __launch_bounds__(kBlock, 8) kCommit(DevState s)
 // New energy particles (RadiationProcessor::createEnergyParticle without
 // sources, :248-364, and ObjectFactory::createParticle, ObjectFactory.cuh
 // :242-256) in the order radiation (cell order), splitting (particle order),
-// deleted cells (cell order); ids continue the world's id counter.
-__device__ __forceinline__ bool delEvent(const DevState& s, long long g)
-{
-    return (s.flags[g] & kFlagDelCell) && s.energy[g] > kNearZero;
-}
+// deleted cells (cell order); ids continue the world's id counter.  A
+// deleted cell makes a particle when it has energy above NEAR_ZERO.
 
 __global__ void __launch_bounds__(kBlock) kEventCount(DevState s)
 {
@@ -1874,13 +1880,13 @@ __global__ void __launch_bounds__(kBlock) kEventCount(DevState s)
     };
     if (blockIdx.x < s.numCellBlocks) {
         const long long g = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+        const uint32_t fl = s.flags[g];  // before the world lookup: every cell slot is inside the arena
         const int w = s.cellBlockWorld[blockIdx.x];
         WorldCounters& wc = s.counters[w];
         uint32_t a = 0, b = 0;
         if (g < s.worlds[w].cellBase + wc.numCells) {
-            const uint32_t fl = s.flags[g];
             a = (fl & kFlagRadiation) ? 1u : 0u;
-            b = delEvent(s, g) ? 1u : 0u;
+            b = (fl & kFlagDelCell) && s.energy[g] > kNearZero ? 1u : 0u;
             // the step's flags end here, except on the cells kEventEmit
             // still reads (radiation and deletion events)
             if (fl && !a && !b) s.flags[g] = 0;
