@@ -656,11 +656,13 @@ void Arena::build(const std::vector<WorldSetup>& setups)
 }
 
 // -------------------------------------------------------------- scan -----
+// exclusive scan of in[0, n) into out[0, n], out[n] = total; in and out are
+// device allocations (16-byte aligned, as kScanDown's vector accesses need)
 void Arena::scan(const uint32_t* in, long long n, uint32_t* out)
 {
     const int blocks = divUp(n, kScanTile);
     launch(kScanReduce, blocks, kBlock, in, n, s_.scanPartials);
-    launch(kScanPartials, 1, kBlock, s_.scanPartials, blocks);
+    launch(kScanPartials<1024>, 1, 1024, s_.scanPartials, blocks);
     launch(kScanDown, blocks, kBlock, in, n, static_cast<const uint32_t*>(s_.scanPartials), out);
 }
 
@@ -926,12 +928,12 @@ void Arena::countData(int w, uint64_t* cells, uint64_t* particles)
 {
     const WorldInfo& wi = worlds_[w].info;
     launch(kSelectCells, wi.numCellBlocks, kBlock, s_, w, 0, 0, 0, 0, 0, rankCells_, blockCount_);
-    launch(kScanPartials, 1, kBlock, blockCount_, wi.numCellBlocks);
+    launch(kScanPartials<kBlock>, 1, kBlock, blockCount_, wi.numCellBlocks);
     uint32_t nc = 0, np = 0;
     AB_CK(cudaMemcpyAsync(&nc, blockCount_ + wi.numCellBlocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
     AB_CK(cudaStreamSynchronize(stream_));
     launch(kSelectParticles, wi.numPartBlocks, kBlock, s_, w, 0, 0, 0, 0, 0, rankParts_, blockCount_);
-    launch(kScanPartials, 1, kBlock, blockCount_, wi.numPartBlocks);
+    launch(kScanPartials<kBlock>, 1, kBlock, blockCount_, wi.numPartBlocks);
     AB_CK(cudaMemcpyAsync(&np, blockCount_ + wi.numPartBlocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
     AB_CK(cudaStreamSynchronize(stream_));
     *cells = nc;
@@ -950,14 +952,14 @@ void Arena::getData(int w, bool useRect, AlienInt2 ul, AlienInt2 lr, const Alien
     const int u = useRect ? 1 : 0;
     uint32_t nc = 0, np = 0;
     launch(kSelectCells, wi.numCellBlocks, kBlock, s_, w, u, ul.x, ul.y, lr.x, lr.y, rankCells_, blockCount_);
-    launch(kScanPartials, 1, kBlock, blockCount_, wi.numCellBlocks);
+    launch(kScanPartials<kBlock>, 1, kBlock, blockCount_, wi.numCellBlocks);
     launch(kFinishRanks, wi.numCellBlocks, kBlock, wi.cellBase, rankCells_, static_cast<const uint32_t*>(blockCount_));
     AB_CK(cudaMemcpyAsync(&nc, blockCount_ + wi.numCellBlocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
     launch(kEgressCells, wi.numCellBlocks, kBlock, s_, w, static_cast<const int*>(rankCells_), static_cast<const AlienCellTO*>(cold_),
            egressCells);
     AB_CK(cudaStreamSynchronize(stream_));
     launch(kSelectParticles, wi.numPartBlocks, kBlock, s_, w, u, ul.x, ul.y, lr.x, lr.y, rankParts_, blockCount_);
-    launch(kScanPartials, 1, kBlock, blockCount_, wi.numPartBlocks);
+    launch(kScanPartials<kBlock>, 1, kBlock, blockCount_, wi.numPartBlocks);
     launch(kFinishRanks, wi.numPartBlocks, kBlock, wi.partBase, rankParts_, static_cast<const uint32_t*>(blockCount_));
     AB_CK(cudaMemcpyAsync(&np, blockCount_ + wi.numPartBlocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
     launch(kEgressParticles, wi.numPartBlocks, kBlock, s_, w, static_cast<const int*>(rankParts_), egressParts);
@@ -981,7 +983,7 @@ void Arena::compactParticles(int w)
 {
     const WorldInfo& wi = worlds_[w].info;
     launch(kSelectParticles, wi.numPartBlocks, kBlock, s_, w, 0, 0, 0, 0, 0, rankParts_, blockCount_);
-    launch(kScanPartials, 1, kBlock, blockCount_, wi.numPartBlocks);
+    launch(kScanPartials<kBlock>, 1, kBlock, blockCount_, wi.numPartBlocks);
     launch(kFinishRanks, wi.numPartBlocks, kBlock, wi.partBase, rankParts_, static_cast<const uint32_t*>(blockCount_));
     uint32_t live = 0;
     AB_CK(cudaMemcpyAsync(&live, blockCount_ + wi.numPartBlocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));

@@ -242,40 +242,59 @@ __global__ void __launch_bounds__(kBlock) kScanReduce(const uint32_t* in, long l
     if (threadIdx.x == 0) partials[blockIdx.x] = total;
 }
 
-__global__ void __launch_bounds__(kBlock) kScanPartials(uint32_t* partials, int numPartials)
+// one block of Threads threads; sequential chunks of Threads
+template <int Threads>
+__global__ void __launch_bounds__(Threads) kScanPartials(uint32_t* partials, int numPartials)
 {
-    // one block; sequential chunks of kBlock
     uint32_t carry = 0;
-    for (int base = 0; base < numPartials; base += kBlock) {
+    for (int base = 0; base < numPartials; base += Threads) {
         int k = base + threadIdx.x;
         uint32_t v = k < numPartials ? partials[k] : 0;
         uint32_t total;
-        uint32_t ex = blockExclusiveScan(v, &total);
+        uint32_t ex = blockExclusiveScanN<Threads>(v, &total);
         if (k < numPartials) partials[k] = carry + ex;
         carry += total;
     }
     if (threadIdx.x == 0) partials[numPartials] = carry;
 }
 
+// in and out are 16-byte aligned (device allocations), so a thread's eight
+// items are two 16-byte loads and stores wherever all eight lie below n
 __global__ void __launch_bounds__(kBlock) kScanDown(const uint32_t* in, long long n, const uint32_t* partials, uint32_t* out)
 {
+    static_assert(kScanItems == 8, "two uint4 per thread");
     long long base = static_cast<long long>(blockIdx.x) * kScanTile + static_cast<long long>(threadIdx.x) * kScanItems;
+    const bool full = base + kScanItems <= n;
     uint32_t v[kScanItems];
+    if (full) {
+        const uint4 a = *reinterpret_cast<const uint4*>(in + base);
+        const uint4 b = *reinterpret_cast<const uint4*>(in + base + 4);
+        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+    } else {
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) v[i] = base + i < n ? in[base + i] : 0;
+    }
     uint32_t sum = 0;
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-        long long k = base + i;
-        v[i] = k < n ? in[k] : 0;
-        sum += v[i];
-    }
+    for (int i = 0; i < kScanItems; ++i) sum += v[i];
     uint32_t total;
     uint32_t ex = blockExclusiveScan(sum, &total) + partials[blockIdx.x];
+    uint32_t o[kScanItems];
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
-        long long k = base + i;
-        if (k < n) out[k] = ex;
+        o[i] = ex;
         ex += v[i];
-        if (k == n - 1) out[n] = ex;
+    }
+    if (full) {
+        *reinterpret_cast<uint4*>(out + base) = make_uint4(o[0], o[1], o[2], o[3]);
+        *reinterpret_cast<uint4*>(out + base + 4) = make_uint4(o[4], o[5], o[6], o[7]);
+        if (base + kScanItems == n) out[n] = ex;
+    } else {
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) {
+            if (base + i < n) out[base + i] = o[i];
+            if (base + i == n - 1) out[n] = o[i] + v[i];
+        }
     }
 }
 
