@@ -59,14 +59,16 @@ def algorithmic_bytes(kernel: str, bonds_per_cell: float) -> float:
         "kBin": 26.0,
         # alive, barrier, color, numConn 4; force 8, velocity 8, bond row 24,
         # position 8, stiffness 4, rest lengths 24; writes velocity 8, force 8;
-        # bond angles 24 / 3
-        "kApplyBond1": 104.0,
+        # bond angles 24 / 3; position 8 written in the two steps of three
+        # without angle forces (the Verlet position update done here)
+        "kApplyBond1": 104.0 + 16.0 / 3.0,
         # alive, barrier, color, numConn 4; bond row 24, position 8,
         # stiffness 4, rest lengths 24; writes force 8; bond angles 24 / 3
         "kBond2": 80.0,
         # velocity 8, position 8, force 8, angle accumulators 16, barrier and
-        # alive 2; writes force 8, position 8
-        "kVerletPos": 58.0,
+        # alive 2; writes force 8, position 8 -- in one step of three (the
+        # angle-force steps; the other steps update positions in kApplyBond1)
+        "kVerletPos": 58.0 / 3.0,
         # velocity 8, angle accumulators 16, two forces 16, barrier, alive,
         # living state 3, flags 4, age 4 + 4, activation time 4; writes
         # velocity 8
