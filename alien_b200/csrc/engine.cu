@@ -180,7 +180,11 @@ struct WorldSetup {
 struct HostWorld {
     WorldInfo info;
     AlienPhysicsParams params;
-    std::vector<uint8_t> aux;  // opaque auxiliary bytes, returned unchanged
+    // opaque auxiliary bytes, returned unchanged: on the device (at
+    // info.auxBase in the arena's aux array) when the arena holds neurons,
+    // which read their weights there, else kept here on the host
+    uint64_t auxSize = 0;
+    std::vector<uint8_t> aux;
 };
 
 class Arena {
@@ -453,7 +457,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         coldTotal += nc;
         maxWorldCells_ = std::max(maxWorldCells_, wi.cellCap);
         maxWorldParts_ = std::max(maxWorldParts_, wi.partCap);
-        if (ws.numAux) hw.aux.assign(ws.aux, ws.aux + ws.numAux);
+        hw.auxSize = ws.numAux;
         hw.info.auxBase = auxTotal;
         auxTotal += static_cast<long long>(ws.numAux);
         worlds_.push_back(std::move(hw));
@@ -584,14 +588,20 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     if (signalsLive_) s.fnInfo = mem_.alloc<uchar4>(C);  // filled by kIngestCells
     if (hasNeurons_) {
         // neuron weights and biases are read where they lie in the
-        // auxiliary data, uploaded once per build
+        // auxiliary data, uploaded once per build straight from the
+        // caller's buffers (the build synchronises before it returns); the
+        // device copy is the only one
         long long auxBytes = 0;
-        for (const HostWorld& hw : worlds_) auxBytes += static_cast<long long>(hw.aux.size());
+        for (const HostWorld& hw : worlds_) auxBytes += static_cast<long long>(hw.auxSize);
         uint8_t* auxDev = mem_.alloc<uint8_t>(static_cast<size_t>(std::max<long long>(auxBytes, 1)));
-        for (const HostWorld& hw : worlds_)
-            if (!hw.aux.empty())
-                AB_CK(cudaMemcpyAsync(auxDev + hw.info.auxBase, hw.aux.data(), hw.aux.size(), cudaMemcpyHostToDevice, stream_));
+        for (size_t w = 0; w < worlds_.size(); ++w)
+            if (worlds_[w].auxSize)
+                AB_CK(cudaMemcpyAsync(auxDev + worlds_[w].info.auxBase, setups[w].aux, worlds_[w].auxSize,
+                                      cudaMemcpyHostToDevice, stream_));
         s.aux = auxDev;
+    } else {
+        for (size_t w = 0; w < worlds_.size(); ++w)
+            if (worlds_[w].auxSize) worlds_[w].aux.assign(setups[w].aux, setups[w].aux + worlds_[w].auxSize);
     }
     rankCells_ = mem_.alloc<int>(C);
     rankParts_ = mem_.alloc<int>(P);
@@ -819,7 +829,7 @@ void Arena::ensureParticleCapacity()
     std::vector<std::vector<AlienParticleTO>> parts(numWorlds());
     std::vector<uint64_t> extra(numWorlds(), 0);
     for (int w = 0; w < numWorlds(); ++w) {
-        uint64_t nc = 0, np = 0, na = worlds_[w].aux.size();
+        uint64_t nc = 0, np = 0, na = worlds_[w].auxSize;
         countData(w, &nc, &np);
         cells[w].resize(nc);
         parts[w].resize(np);
@@ -837,6 +847,15 @@ void Arena::rebuildFromHost(const std::vector<std::vector<AlienCellTO>>& cells, 
     std::vector<WorldCounters> c = readCounters();
     std::vector<HostWorld> old = worlds_;
     std::vector<WorldSetup> setups(old.size());
+    // auxiliary bytes held only on the device come back to the host first
+    std::vector<std::vector<uint8_t>> auxHost(old.size());
+    for (size_t w = 0; w < old.size(); ++w)
+        if (old[w].auxSize && old[w].aux.empty()) {
+            auxHost[w].resize(old[w].auxSize);
+            AB_CK(cudaMemcpyAsync(auxHost[w].data(), s_.aux + old[w].info.auxBase, old[w].auxSize, cudaMemcpyDeviceToHost,
+                                  stream_));
+        }
+    AB_CK(cudaStreamSynchronize(stream_));
     for (size_t w = 0; w < old.size(); ++w) {
         WorldSetup& ws = setups[w];
         ws.W = old[w].info.W;
@@ -847,8 +866,8 @@ void Arena::rebuildFromHost(const std::vector<std::vector<AlienCellTO>>& cells, 
         ws.numCells = cells[w].size();
         ws.particles = parts[w].data();
         ws.numParticles = parts[w].size();
-        ws.aux = old[w].aux.data();
-        ws.numAux = old[w].aux.size();
+        ws.aux = old[w].aux.empty() ? auxHost[w].data() : old[w].aux.data();
+        ws.numAux = old[w].auxSize;
         ws.extraParticles = extra[w];
     }
     build(setups);
@@ -889,7 +908,7 @@ void Arena::setParams(int w, const AlienPhysicsParams& p)
         std::vector<std::vector<AlienCellTO>> cells(numWorlds());
         std::vector<std::vector<AlienParticleTO>> parts(numWorlds());
         for (int v = 0; v < numWorlds(); ++v) {
-            uint64_t nc = 0, np = 0, na = worlds_[v].aux.size();
+            uint64_t nc = 0, np = 0, na = worlds_[v].auxSize;
             countData(v, &nc, &np);
             cells[v].resize(nc);
             parts[v].resize(np);
@@ -968,15 +987,18 @@ void Arena::getData(int w, bool useRect, AlienInt2 ul, AlienInt2 lr, const Alien
     if (np && !out->particles) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "DataTO.particles is null");
     if (nc) AB_CK(cudaMemcpyAsync(out->cells, egressCells, sizeof(AlienCellTO) * nc, cudaMemcpyDeviceToHost, stream_));
     if (np) AB_CK(cudaMemcpyAsync(out->particles, egressParts, sizeof(AlienParticleTO) * np, cudaMemcpyDeviceToHost, stream_));
-    const std::vector<uint8_t>& aux = worlds_[w].aux;
-    if (!aux.empty()) {
+    const HostWorld& hw = worlds_[w];
+    if (hw.auxSize) {
         if (!out->auxiliaryData) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "DataTO.auxiliaryData is null");
-        std::memcpy(out->auxiliaryData, aux.data(), aux.size());
+        if (hw.aux.empty())
+            AB_CK(cudaMemcpyAsync(out->auxiliaryData, s_.aux + hw.info.auxBase, hw.auxSize, cudaMemcpyDeviceToHost, stream_));
+        else
+            std::memcpy(out->auxiliaryData, hw.aux.data(), hw.auxSize);
     }
     AB_CK(cudaStreamSynchronize(stream_));
     *out->numCells = nc;
     *out->numParticles = np;
-    *out->numAuxiliaryData = aux.size();
+    *out->numAuxiliaryData = hw.auxSize;
 }
 
 void Arena::compactParticles(int w)
@@ -1315,7 +1337,7 @@ int alien_b200_get_array_sizes(alien_b200_simulation* sim, AlienArraySizes* size
         const WorldInfo& wi = sim->arena->world(0).info;
         sizes->cellArraySize = static_cast<uint64_t>(wi.cellCap);
         sizes->particleArraySize = static_cast<uint64_t>(wi.partCap);
-        sizes->auxiliaryDataSize = sim->arena->world(0).aux.size();
+        sizes->auxiliaryDataSize = sim->arena->world(0).auxSize;
     });
 }
 
@@ -1332,7 +1354,7 @@ int alien_b200_resize_arrays_if_necessary(alien_b200_simulation* sim, const Alie
         if (np + additionals->particleArraySize + 4096 > static_cast<uint64_t>(wi.partCap) / 2) {
             std::vector<AlienCellTO> cells(nc);
             std::vector<AlienParticleTO> parts(np);
-            uint64_t na = sim->arena->world(0).aux.size();
+            uint64_t na = sim->arena->world(0).auxSize;
             std::vector<uint8_t> aux(std::max<uint64_t>(na, 1));
             AlienDataTO to{&nc, cells.data(), &np, parts.data(), &na, aux.data()};
             sim->arena->getData(0, false, AlienInt2{0, 0}, AlienInt2{0, 0}, &to);
@@ -1452,7 +1474,7 @@ int alien_b200_batch_get_array_sizes(alien_b200_batch* b, int world, AlienArrayS
         const WorldInfo& wi = b->arena->world(world).info;
         sizes->cellArraySize = static_cast<uint64_t>(wi.cellCap);
         sizes->particleArraySize = static_cast<uint64_t>(wi.partCap);
-        sizes->auxiliaryDataSize = b->arena->world(world).aux.size();
+        sizes->auxiliaryDataSize = b->arena->world(world).auxSize;
     });
 }
 

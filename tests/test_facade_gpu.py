@@ -39,6 +39,26 @@ def test_round_trip_exact_with_neurons_and_aux():
     f.close_simulation()
 
 
+def test_auxiliary_data_survives_rebuilds_with_neurons():
+    """neuron weights live only on the device: a parameter change that
+    re-lays out the tile grid and a resize both rebuild the arena from a
+    download, and the auxiliary bytes come back unchanged"""
+    data, world = worldgen.random_test_world(92)
+    data = worldgen.add_neurons(data, 92, fraction=0.5)
+    f = facade(world, P.benchmark_parameters(), data)
+    assert f.get_array_sizes().auxiliaryDataSize == len(data.aux)
+    f.calc_timesteps(2)
+    p2 = P.benchmark_parameters(P.MOTION_COLLISION)
+    p2.cellMaxCollisionDistance = 2.5
+    f.set_simulation_parameters(p2)
+    f.resize_arrays_if_necessary(particles=4 * f.get_array_sizes().particleArraySize)
+    f.calc_timesteps(2)
+    out = f.get_simulation_data()
+    assert np.array_equal(out.aux, data.aux)
+    assert out.num_cells == data.num_cells
+    f.close_simulation()
+
+
 def test_round_trip_exact_at_one_million_cells():
     data, world = worldgen.hex_world(seed=91, world=(2048, 2048), clusters=10000)
     f = facade(world, P.benchmark_parameters(P.MOTION_COLLISION), data)
