@@ -478,7 +478,7 @@ def main():
                 "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "strong" if args.partition == "global" else "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "batched256", "worlds": 256, "cells": total, "partition": args.partition,
+                "config": {"workload": "batched256", "worlds": 256, "cells": int(total), "partition": args.partition,
                            "parallelism": f"worlds split across {world_size} GPUs by cell count"
                            if args.partition == "global" else f"replicas x{world_size}",
                            "description": "256 worlds, log-uniform 1k-200k cells, density 0.2, half fluid cells and half 10x10 lattices",
