@@ -791,9 +791,10 @@ double Arena::timeSteps(uint64_t n)
 
 void Arena::sync()
 {
-    AB_CK(cudaStreamSynchronize(stream_));
+    // the error word is read in stream order: one wait covers the work and the read
     uint32_t flags = 0;
-    AB_CK(cudaMemcpy(&flags, s_.errorFlags, sizeof(flags), cudaMemcpyDeviceToHost));
+    AB_CK(cudaMemcpyAsync(&flags, s_.errorFlags, sizeof(flags), cudaMemcpyDeviceToHost, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
     if (flags & 1u) {
         AB_CK(cudaMemset(s_.errorFlags, 0, sizeof(uint32_t)));
         throw Error(ALIEN_B200_ERR_CAPACITY, "particle capacity exceeded: energy particles were dropped");
@@ -883,13 +884,15 @@ void Arena::rebuildFromHost(const std::vector<std::vector<AlienCellTO>>& cells, 
 
 void Arena::calcTimesteps(uint64_t n)
 {
+    // particle storage is checked (and compacted or grown) after at most 64
+    // steps, counted across calls, so that many short calls cost one wait each
     const uint64_t chunk = 64;
     while (n > 0) {
-        const uint64_t k = std::min(n, chunk);
+        const uint64_t k = std::min(n, chunk - stepsSinceCheck_);
         enqueueSteps(k);
         n -= k;
         stepsSinceCheck_ += k;
-        if (stepsSinceCheck_ >= chunk || n == 0) {
+        if (stepsSinceCheck_ >= chunk) {
             sync();
             ensureParticleCapacity();
             stepsSinceCheck_ = 0;
