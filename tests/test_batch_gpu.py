@@ -85,3 +85,26 @@ def test_serving_results_equal_alone():
         ref = alone(data, world, P.benchmark_parameters(P.MOTION_FLUID), steps)
         assert np.array_equal(r.result.cells, ref.cells), r.rid
         assert np.array_equal(r.result.particles, ref.particles), r.rid
+
+
+def test_worlds_at_different_timestep_phases_equal_alone():
+    """a world stopped by its budget and started again runs one step behind
+    the others, so the angle-force steps (timestep % 3 == 0) of the worlds
+    differ within one launch; each world still evolves as it does alone"""
+    worlds = mixed_worlds()
+    batch = BatchSimulation(worlds)
+    batch.set_step_budget(0, 1)
+    batch.set_step_budget(2, 2)
+    batch.calc_timesteps(3)            # world 0 at t = 1, world 2 at t = 2, others at t = 3
+    batch.set_step_budget(0, 10)
+    batch.set_step_budget(2, 10)
+    batch.calc_timesteps(10)
+    expect = [11, 13, 12, 13]
+    for w, (data, world, prm) in enumerate(worlds):
+        t, _, _ = batch.world_status(w)
+        assert t == expect[w], w
+        got = batch.get_simulation_data(w)
+        ref = alone(data, world, prm, expect[w])
+        assert np.array_equal(got.cells, ref.cells), w
+        assert np.array_equal(got.particles, ref.particles), w
+    batch.close()
