@@ -515,6 +515,12 @@ def main():
     value = total_cells * args.steps / (ms / 1000.0) / 1e6
 
     log(f"timed region: {ms / args.steps:.3f} ms/step")
+    # per-step distribution: each of min(K, 200) further steps between its
+    # own pair of CUDA events (a wait between steps, so not the throughput)
+    import numpy as np
+
+    step_samples = [sim.time_timesteps(1) for _ in range(min(args.steps, 200))]
+    step_p50, step_p99 = (float(np.percentile(step_samples, q)) for q in (50, 99))
     # per-kernel CUDA-event breakdown over a second stretch of the same run
     timed_steps = max(3, min(args.steps, 50))
     kernel_ms = sim.timed_timesteps(timed_steps)
@@ -585,6 +591,8 @@ def main():
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": per_launch_ms},
             "kernel_ms_per_step": {k: v / timed_steps for k, v in kernel_ms.items()},
+            "step_ms": {"p50": step_p50, "p99": step_p99, "samples": len(step_samples),
+                        "note": "single steps between CUDA events, after the timed region"},
             "clocks": clk.summary(),
             "gpu_launches": launches,
             "e2e": e2e,
