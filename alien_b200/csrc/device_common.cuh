@@ -123,6 +123,7 @@ struct DevState {
     uint8_t* numConn;
     uint8_t* barrier;
     uint8_t* alive;
+    uint8_t* triMask;         // per cell, angle-force steps: bit k = bond k's partner is bonded to the previous partner
     uint8_t* livingState;
     uint8_t* nextState;
     uint32_t* flags;

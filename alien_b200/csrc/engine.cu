@@ -527,6 +527,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     s.numConn = mem_.alloc<uint8_t>(C);
     s.barrier = mem_.alloc<uint8_t>(C);
     s.alive = mem_.alloc<uint8_t>(C);
+    s.triMask = mem_.alloc<uint8_t>(C);
     s.livingState = mem_.alloc<uint8_t>(C);
     s.nextState = mem_.alloc<uint8_t>(C);
     s.flags = mem_.alloc<uint32_t>(C);

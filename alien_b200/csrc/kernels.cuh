@@ -970,8 +970,13 @@ __device__ __forceinline__ void loadBondRow(const DevState& s, long long g, int 
     for (int k = 0; k < kMaxBonds; ++k) r.disp[k] = correctDirection(pj[k] - pi, W, H);
 }
 
+// the triangle test of the angle forces depends only on the bond rows, which
+// do not change between the two bond-force kernels of a step: the first
+// computes and stores it, the second reads it back
+enum TriMode { kTriStore, kTriLoad };
+
 __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, const BondRow& r, bool considerAngles,
-                                            float minDist, int accOffset)
+                                            float minDist, int accOffset, TriMode triMode)
 {
     float2 F = f2(0.0f, 0.0f);
     const int n = r.n;
@@ -1004,8 +1009,9 @@ __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, cons
     // angle forces: partner rows for the triangle test, then the forces in bond order
     int nj[kMaxBonds];
     float ang[kMaxBonds];  // angle of every bond vector, once
+    unsigned triBits = triMode == kTriLoad ? s.triMask[g] : 0u;
 #pragma unroll
-    for (int k = 0; k < kMaxBonds; ++k) nj[k] = k < n ? s.numConn[r.j[k]] : 0;
+    for (int k = 0; k < kMaxBonds; ++k) nj[k] = triMode == kTriStore && k < n ? s.numConn[r.j[k]] : 0;
 #pragma unroll
     for (int k = 0; k < kMaxBonds; ++k) {
         const float a = 90.0f - atan2f(-r.disp[k].y, r.disp[k].x) * (180.0f / kPi);
@@ -1027,15 +1033,21 @@ __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, cons
                 nrmPrev = nrm[m];
             }
         const int j = r.j[k];
-        const int2* prow = reinterpret_cast<const int2*>(s.bond + static_cast<long long>(j) * kMaxBonds);
-        bool tri = false;
+        bool tri;
+        if (triMode == kTriLoad) {
+            tri = (triBits >> k) & 1u;
+        } else {
+            const int2* prow = reinterpret_cast<const int2*>(s.bond + static_cast<long long>(j) * kMaxBonds);
+            tri = false;
 #pragma unroll
-        for (int h = 0; h < kMaxBonds / 2; ++h) {
-            if (2 * h < nj[k]) {
-                const int2 pp = prow[h];
-                tri |= pp.x == jl;
-                tri |= (2 * h + 1 < nj[k]) && pp.y == jl;
+            for (int h = 0; h < kMaxBonds / 2; ++h) {
+                if (2 * h < nj[k]) {
+                    const int2 pp = prow[h];
+                    tri |= pp.x == jl;
+                    tri |= (2 * h + 1 < nj[k]) && pp.y == jl;
+                }
             }
+            if (tri) triBits |= 1u << k;
         }
         if (tri) continue;
         const float act = subtractAngle(ang[k], pa);
@@ -1059,6 +1071,7 @@ __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, cons
         }
         F = F - (f1 + f2v);
     }
+    if (triMode == kTriStore) s.triMask[g] = static_cast<uint8_t>(triBits);
     return F;
 }
 
@@ -1116,7 +1129,7 @@ __global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
         }
         BondRow r;
         loadBondRow(s, g, n, s.posB, wi.W, wi.H, r);
-        const float2 F1 = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 0);
+        const float2 F1 = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 0, kTriStore);
         if (T % 3 == 0) {
             s.force1[g] = F1;  // angle forces of other cells still arrive: kVerletPos
         } else {
@@ -1210,7 +1223,7 @@ __global__ void __launch_bounds__(kBlock, 6) kBond2(DevState s)
                     if (k < r.n) atomicOr(&s.flags[r.j[k]], kFlagDetach);
             }
         }
-        s.force[g] = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 2);
+        s.force[g] = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 2, kTriLoad);
     } else {
         forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
             if (!c.inRange || !s.palive[c.q]) return;
