@@ -1,0 +1,41 @@
+"""Writes tests/golden/ref_settings_subset.json: the general settings and the
+physics-stage keys of the reference's sample settings file
+(resources/autosave.settings.json of the reference repository), in the
+file's own nested layout and string values, for the settings reader's test.
+Run in a container that holds the reference at /root/reference."""
+import json
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", ".."))
+from alien_b200 import settings  # noqa: E402
+
+SRC = "/root/reference/resources/autosave.settings.json"
+
+
+def main():
+    with open(SRC, encoding="utf-8") as f:
+        tree = json.load(f)
+    out = {"general": {k: tree["general"][k] for k in ("time step", "world size")}}
+    sp = tree["simulation parameters"]
+    keep = {}
+    for _, key, _, color in settings._FIELDS:
+        names = [f"{key}[{c}]" for c in range(7)] if color else [key]
+        for name in names:
+            parts = name.split(".")
+            node = sp
+            for p in parts[:-1]:
+                node = node.get(p, {}) if isinstance(node, dict) else {}
+            if isinstance(node, dict) and parts[-1] in node and not isinstance(node[parts[-1]], dict):
+                dst = keep
+                for p in parts[:-1]:
+                    dst = dst.setdefault(p, {})
+                dst[parts[-1]] = node[parts[-1]]
+    out["simulation parameters"] = keep
+    with open(os.path.join(HERE, "ref_settings_subset.json"), "w", encoding="utf-8") as f:
+        json.dump(out, f, indent=2)
+
+
+if __name__ == "__main__":
+    main()
