@@ -70,6 +70,7 @@ EXPORTED_SYMBOLS = [
     "alien_b200_batch_kernel_launch_count", "alien_b200_batch_kernels_per_step", "alien_b200_batch_timed_timesteps",
     "alien_b200_batch_set_step_budget", "alien_b200_batch_world_status", "alien_b200_batch_num_active",
     "alien_b200_batch_device_bytes", "alien_b200_statistics_no_alloc", "alien_b200_batch_synchronize",
+    "alien_b200_debug_cell_map",
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -128,6 +129,7 @@ def load() -> ctypes.CDLL:
     lib.alien_b200_batch_device_bytes.restype = u64
     lib.alien_b200_batch_synchronize.argtypes = [vp]
     lib.alien_b200_statistics_no_alloc.argtypes = [vp, u64, vp, u64, u64, vp, vp]
+    lib.alien_b200_debug_cell_map.argtypes = [vp, u64, vp, vp, vp, vp, P(u64)]
     lib.alien_b200_select_device.argtypes = [i32]
     lib.alien_b200_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]
     lib.alien_b200_batch_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]

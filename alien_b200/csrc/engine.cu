@@ -211,6 +211,9 @@ public:
     void setStepBudget(int w, uint64_t steps);
     void compactParticles(int w);
     void ensureParticleCapacity();
+    // the cell map of the current state, built by the step's own binning
+    // kernels and read back in tile order (alien_b200_debug_cell_map)
+    uint64_t cellMap(uint64_t capacity, uint64_t* ids, uint32_t* slots, uint32_t* tiles, uint8_t* flags);
 
     int numWorlds() const { return static_cast<int>(worlds_.size()); }
     const HostWorld& world(int w) const { return worlds_[w]; }
@@ -1042,6 +1045,39 @@ void Arena::compactParticles(int w)
     AB_CK(cudaStreamSynchronize(stream_));
 }
 
+uint64_t Arena::cellMap(uint64_t capacity, uint64_t* ids, uint32_t* slots, uint32_t* tiles, uint8_t* flags)
+{
+    const DevState& s = s_;
+    AB_CK(cudaMemsetAsync(s.tileCount, 0, sizeof(uint32_t) * static_cast<size_t>(s.numTiles), stream_));
+    launch(kBinMap, s.numCellBlocks, kBlock, s);
+    scan(s.tileCount, s.numTiles, s.tileStart);
+    launch(kScatter, s.numCellBlocks, kBlock, s);
+    launch(kStage, s.numCellBlocks, kBlock, s);
+    uint32_t total = 0;
+    AB_CK(cudaMemcpyAsync(&total, s.tileStart + s.numTiles, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+    if (total > capacity) return total;
+    const size_t n = std::max<size_t>(total, 1);
+    unsigned long long* dIds = nullptr;
+    uint32_t *dSlots = nullptr, *dTiles = nullptr;
+    uint8_t* dFlags = nullptr;
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&dIds), n * 8, stream_));
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&dSlots), n * 4, stream_));
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&dTiles), n * 4, stream_));
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&dFlags), n, stream_));
+    launch(kExportCellMap, divUp(total, kBlock), kBlock, s, dIds, dSlots, dTiles, dFlags);
+    if (total) {
+        AB_CK(cudaMemcpyAsync(ids, dIds, total * 8ull, cudaMemcpyDeviceToHost, stream_));
+        AB_CK(cudaMemcpyAsync(slots, dSlots, total * 4ull, cudaMemcpyDeviceToHost, stream_));
+        AB_CK(cudaMemcpyAsync(tiles, dTiles, total * 4ull, cudaMemcpyDeviceToHost, stream_));
+        AB_CK(cudaMemcpyAsync(flags, dFlags, total, cudaMemcpyDeviceToHost, stream_));
+    }
+    for (void* p : {static_cast<void*>(dIds), static_cast<void*>(dSlots), static_cast<void*>(dTiles), static_cast<void*>(dFlags)})
+        AB_CK(cudaFreeAsync(p, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+    return total;
+}
+
 AlienRawStatistics Arena::statistics(int w)
 {
     AB_CK(cudaMemsetAsync(stats_ + w, 0, sizeof(StatsAcc), stream_));
@@ -1400,6 +1436,19 @@ int alien_b200_get_raw_statistics(alien_b200_simulation* sim, AlienRawStatistics
     return guarded([&] {
         if (!sim || !statistics) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
         *statistics = sim->arena->statistics(0);
+    });
+}
+
+int alien_b200_debug_cell_map(alien_b200_simulation* sim, uint64_t capacity, uint64_t* ids, uint32_t* slots, uint32_t* tiles,
+                              uint8_t* flags, uint64_t* count)
+{
+    return guarded([&] {
+        if (!sim || !count || (capacity && (!ids || !slots || !tiles || !flags)))
+            throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        *count = sim->arena->cellMap(capacity, ids, slots, tiles, flags);
+        if (*count > capacity)
+            throw Error(ALIEN_B200_ERR_CAPACITY, "cell map holds " + std::to_string(*count) + " cells, capacity "
+                                                     + std::to_string(capacity));
     });
 }
 

@@ -148,6 +148,16 @@ __device__ __forceinline__ void forEachWindowTile(const WorldInfo& wi, int sx, i
     }
 }
 
+// the cell's slot and tile at binning, and its arrival rank in the tile
+__device__ __forceinline__ void binCell(const DevState& s, const WorldInfo& wi, long long g, float2 pos)
+{
+    const int sx = slotX(pos.x, wi.W), sy = slotX(pos.y, wi.H);
+    const uint32_t tile = static_cast<uint32_t>(wi.tileBase + (sx / wi.T) + static_cast<long long>(sy / wi.T) * wi.nTX);
+    s.tileOf[g] = tile;
+    s.slotOf[g] = static_cast<uint32_t>(sx + sy * wi.W);
+    s.tileOff[g] = atomicAdd(&s.tileCount[tile], 1u);
+}
+
 // ---------------------------------------------------------------- kBin ----
 // cells: reset per-step scratch, tile binning (CellMap::set_block,
 // Map.cuh:95-130, by tile instead of a pointer chain), radiation
@@ -169,11 +179,7 @@ __global__ void __launch_bounds__(kBlock, 8) kBin(DevState s)
         if (!c.valid) return;
         const WorldInfo& wi = s.worlds[c.w];
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
-        int sx = slotX(pos.x, wi.W), sy = slotX(pos.y, wi.H);
-        uint32_t tile = static_cast<uint32_t>(wi.tileBase + (sx / wi.T) + static_cast<long long>(sy / wi.T) * wi.nTX);
-        s.tileOf[g] = tile;
-        s.slotOf[g] = static_cast<uint32_t>(sx + sy * wi.W);
-        s.tileOff[g] = atomicAdd(&s.tileCount[tile], 1u);
+        binCell(s, wi, g, pos);
 
         if (barrierG || !(p.radiationProb > 0.0f)) return;  // a draw in [0, 1) never falls below 0
         const uint64_t T = s.counters[c.w].timestep;
@@ -350,6 +356,35 @@ __global__ void __launch_bounds__(kBlock) kStage(DevState s)
     fl |= w << 16;
     s.stagedPV[k] = make_float4(pos.x, pos.y, vel.x, vel.y);
     s.stagedMeta[k] = make_int4(static_cast<int>(g), fl, __float_as_int(dens), __float_as_int(energy));
+}
+
+// ------------------------------------------------- cell-map read-back ----
+// The binning of kBin alone (no radiation, no particles, no step counters):
+// with the scan, kScatter and kStage it builds the cell map of the current
+// state for alien_b200_debug_cell_map.  Everything it writes is rebuilt by
+// the next step.
+__global__ void __launch_bounds__(kBlock) kBinMap(DevState s)
+{
+    const float2 pos = s.posA[static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x];
+    CellCtx c = cellCtx(s);
+    if (!c.valid) return;
+    binCell(s, s.worlds[c.w], c.g, pos);
+}
+
+// the staged records in tile order: id, slot, tile (relative to the world's
+// first tile) and the record's map flags (barrier, visible, slot head)
+__global__ void __launch_bounds__(kBlock) kExportCellMap(DevState s, unsigned long long* ids, uint32_t* slots, uint32_t* tiles,
+                                                         uint8_t* flags)
+{
+    const long long k = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    if (k >= s.tileStart[s.numTiles]) return;
+    const int4 meta = s.stagedMeta[k];
+    const long long g = meta.x;
+    const WorldInfo& wi = s.worlds[(meta.y >> 16) & 0xffff];
+    ids[k] = s.id[g];
+    slots[k] = s.slotOf[g];
+    tiles[k] = static_cast<uint32_t>(s.tileOf[g] - wi.tileBase);
+    flags[k] = static_cast<uint8_t>(meta.y & (kStageBarrier | kStageVisible | kStageHead));
 }
 
 // ---------------------------------------------------------- pair laws ----

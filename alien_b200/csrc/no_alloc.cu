@@ -33,8 +33,10 @@ struct Partial {
     long long energyFix;  // 2^-16 fixed point, as the arena statistics
 };
 
+static_assert(sizeof(Partial) == 80, "the scratch size stated in the header assumes 80-byte partials");
+
 // Scratch: one partial per block for cells, then one per block for
-// particles (2 x 4096 x 88 B = 704 KB).  Every GPU that loads the library
+// particles (2 x 4096 x 80 B = 640 KiB).  Every GPU that loads the library
 // holds it until the process exits.  Each call overwrites the partials of
 // the blocks it launches before reading them, so nothing needs clearing; two
 // calls that overlap on the GPU share this array and race.
@@ -130,7 +132,10 @@ __global__ void __launch_bounds__(kThreads) kFinish(int cellBlocks, int particle
 }
 
 // device address of g_scratch, looked up once per device with that device
-// current (the symbol's name is only a host-side stand-in)
+// current (the symbol's name is only a host-side stand-in).  The cache lives
+// as long as the process: after a cudaDeviceReset of a device the address
+// it holds for that device is stale, so a caller that resets a device must
+// not call this entry point on it again.
 constexpr int kMaxDevices = 64;
 std::mutex g_setupMutex;
 Partial* g_scratchAddress[kMaxDevices] = {};
@@ -168,9 +173,17 @@ extern "C" int alien_b200_statistics_no_alloc(const AlienCellTO* cells, uint64_t
     {
         std::lock_guard<std::mutex> lock(g_setupMutex);
         if (!g_scratchAddress[device]) {
+            // set-up on this device: with lazy module loading (the CUDA 12
+            // default) the array and both kernels are brought onto the GPU
+            // here, which may itself need device memory; later calls need
+            // none
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_scratch);
             if (e != cudaSuccess) return fail(ALIEN_B200_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            cudaFuncAttributes attr;
+            e = cudaFuncGetAttributes(&attr, kPartials);
+            if (e == cudaSuccess) e = cudaFuncGetAttributes(&attr, kFinish);
+            if (e != cudaSuccess) return fail(ALIEN_B200_ERR_CUDA, std::string("kernel load: ") + cudaGetErrorString(e));
             g_scratchAddress[device] = static_cast<Partial*>(p);
         }
         scratch = g_scratchAddress[device];
@@ -178,6 +191,12 @@ extern "C" int alien_b200_statistics_no_alloc(const AlienCellTO* cells, uint64_t
     const int cellBlocks = static_cast<int>((numCells + kItemsPerBlock - 1) / kItemsPerBlock);
     const int particleBlocks = static_cast<int>((numParticles + kItemsPerBlock - 1) / kItemsPerBlock);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // an error left by the caller's earlier work is the caller's to read:
+    // report it without launching and without clearing it, so that the
+    // error read after the launches below can only be theirs
+    e = cudaPeekAtLastError();
+    if (e != cudaSuccess)
+        return fail(ALIEN_B200_ERR_CUDA, std::string("an earlier CUDA error is pending (not cleared): ") + cudaGetErrorString(e));
     if (cellBlocks + particleBlocks > 0)
         kPartials<<<cellBlocks + particleBlocks, kThreads, 0, s>>>(cells, numCells, particles, numParticles, cellBlocks, scratch);
     kFinish<<<1, kThreads, 0, s>>>(cellBlocks, particleBlocks, scratch, timestep, statistics);

@@ -123,6 +123,24 @@ class SimulationFacade:
         check(self._lib.alien_b200_get_raw_statistics(self._handle(), ctypes.byref(r)))
         return r
 
+    def debug_cell_map(self):
+        """The engine's cell map of the current state (alien_b200_debug_cell_map):
+        (ids, slots, tiles, flags) of every binned cell in the map's tile order."""
+        import numpy as np
+
+        count = ctypes.c_uint64()
+        code = self._lib.alien_b200_debug_cell_map(self._handle(), 0, None, None, None, None, ctypes.byref(count))
+        if code not in (0, 6):  # 6: capacity (the count is still returned)
+            check(code)
+        n = int(count.value)
+        ids = np.zeros(max(n, 1), np.uint64)
+        slots = np.zeros(max(n, 1), np.uint32)
+        tiles = np.zeros(max(n, 1), np.uint32)
+        flags = np.zeros(max(n, 1), np.uint8)
+        check(self._lib.alien_b200_debug_cell_map(self._handle(), n, ids.ctypes.data, slots.ctypes.data, tiles.ctypes.data,
+                                                  flags.ctypes.data, ctypes.byref(count)))
+        return ids[:n], slots[:n], tiles[:n], flags[:n]
+
     def stream(self) -> int:
         return int(self._lib.alien_b200_stream(self._handle()) or 0)
 

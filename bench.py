@@ -39,41 +39,46 @@ def log(msg: str) -> None:
     """progress on stderr (the JSON line is the only stdout output)"""
     print(f"[bench {time.perf_counter() - T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
-# algorithmic bytes per cell per launch of each step kernel (FP32 SoA):
-# P1 hash build 24; P2 pair forces 40; P3 apply 24 + P4 bond forces 20+12b;
-# P5 Verlet x 32; P6 bond forces 20+12b; P7 Verlet v 32
+# Algorithmic bytes per cell-step, phase by phase (compulsory FP32 SoA
+# traffic of the reference's dependency-separated phases, neighbour reads
+# counted 0 as served from shared memory / L2; b = bonds per cell):
+#   P1 hash build 24; P2 pair forces 40; P3 apply forces 24;
+#   P4 bond forces #1 20 + 12b; P5 Verlet x 32; P6 bond forces #2 20 + 12b;
+#   P7 Verlet v + friction 32  ->  B_cell = 192 + 24b.
+PHASE_BYTES = {"P1": lambda b: 24.0, "P2": lambda b: 40.0, "P3": lambda b: 24.0, "P4": lambda b: 20.0 + 12.0 * b,
+               "P5": lambda b: 32.0, "P6": lambda b: 20.0 + 12.0 * b, "P7": lambda b: 32.0}
+
+
+def step_bytes_per_cell(bonds_per_cell: float) -> float:
+    """B_cell of the whole step: 192 + 24b"""
+    return sum(f(bonds_per_cell) for f in PHASE_BYTES.values())
+
+
 def algorithmic_bytes(kernel: str, bonds_per_cell: float) -> float:
-    """Bytes per cell one launch must move with this data layout: each
-    array the kernel reads or writes for a cell, counted once (a partner's
-    position or stiffness is another cell's row, counted where it is owned;
-    the pair phase's halo re-reads are overhead, not algorithmic).  Angle
-    work of every third step is amortised (bond angles, 24 B / 3)."""
-    del bonds_per_cell  # bond rows are fixed-width (6 slots)
+    """Algorithmic bytes per cell of one launch of `kernel`: the phases it
+    carries.  The first bond-force kernel also applies the pair forces, and
+    does the Verlet position update in the two steps of three without angle
+    forces (the position kernel does it in the third)."""
+    b = bonds_per_cell
     if kernel.startswith("kPairs"):
-        # staged record (pos/vel 16 + meta 16), bond row 24; writes force 8,
-        # overlap-pushed position 8, density 4, fusion choice 4
-        return 80.0
+        return PHASE_BYTES["P2"](b)
     return {
-        # position 8, alive 1, barrier 1; tile 4 + rank 4 written, tile count
-        # atomic 8 (read + write)
-        "kBin": 26.0,
-        # alive, barrier, color, numConn 4; force 8, velocity 8, bond row 24,
-        # position 8, stiffness 4, rest lengths 24; writes velocity 8, force 8;
-        # bond angles 24 / 3; position 8 written in the two steps of three
-        # without angle forces (the Verlet position update done here)
-        "kApplyBond1": 104.0 + 16.0 / 3.0,
-        # alive, barrier, color, numConn 4; bond row 24, position 8,
-        # stiffness 4, rest lengths 24; writes force 8; bond angles 24 / 3
-        "kBond2": 80.0,
-        # velocity 8, position 8, force 8, angle accumulators 16, barrier and
-        # alive 2; writes force 8, position 8 -- in one step of three (the
-        # angle-force steps; the other steps update positions in kApplyBond1)
-        "kVerletPos": 58.0 / 3.0,
-        # velocity 8, angle accumulators 16, two forces 16, barrier, alive,
-        # living state 3, flags 4, age 4 + 4, activation time 4; writes
-        # velocity 8
-        "kVerletVel": 67.0,
+        "kApplyBond1": PHASE_BYTES["P3"](b) + PHASE_BYTES["P4"](b) + PHASE_BYTES["P5"](b) * 2.0 / 3.0,
+        "kVerletPos": PHASE_BYTES["P5"](b) / 3.0,
+        "kBond2": PHASE_BYTES["P6"](b),
+        "kVerletVel": PHASE_BYTES["P7"](b),
     }.get(kernel, 0.0)
+
+
+def layout_bytes(kernel: str) -> float:
+    """Bytes per cell one launch moves with this engine's data layout (each
+    array read or written for the cell counted once: the staged pair record
+    is 32 B, a bond row 24 B, rest lengths 24 B, ...): the traffic to expect
+    from the layout, as opposed to the algorithmic minimum above."""
+    if kernel.startswith("kPairs"):
+        return 80.0
+    return {"kApplyBond1": 104.0 + 16.0 / 3.0, "kBond2": 80.0, "kVerletPos": 58.0 / 3.0, "kVerletVel": 67.0,
+            "kBin": 26.0}.get(kernel, 0.0)
 
 
 def load_peak():
@@ -425,6 +430,8 @@ def main():
                     help="batched256: each rank its own 256 worlds, or the 256 worlds split across ranks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-same-workload", action="store_true",
+                    help="hex4m: skip timing the 1M-cell world that the reference arm runs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -529,11 +536,25 @@ def main():
     per_launch_ms = kernel_ms[dominant] / timed_steps
     alg_bytes = algorithmic_bytes(dominant, bonds) * stats1.numCells
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
+    # every force / integration kernel against the same accounting, and the
+    # whole step at B_cell = 192 + 24b
+    kernel_roofline = {}
+    for k, total_ms in kernel_ms.items():
+        ab = algorithmic_bytes(k, bonds)
+        if ab > 0:
+            gbs = ab * stats1.numCells / (total_ms / timed_steps / 1000.0) / 1e9
+            kernel_roofline[k] = {"bytes_per_cell": round(ab, 2), "ms": total_ms / timed_steps, "achieved_gbs": gbs,
+                                  "frac": gbs / peak}
+    step_gbs = step_bytes_per_cell(bonds) * stats1.numCells / (ms / args.steps / 1000.0) / 1e9
+    # DRAM bytes of one launch of the dominant kernel, from a one-kernel ncu
+    # capture of this workload (profiles/<kernel>_<workload>_traffic.json)
     traffic = None
     tpath = os.path.join(ROOT, "profiles", f"{dominant.split('<')[0]}_{args.config}_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get("bytes_per_launch")
+            tj = json.load(f)
+        if tj.get("workload") == args.config and tj.get("kernel") == dominant:
+            traffic = tj.get("bytes_per_launch")
 
     # end to end through the C ABI with host buffers: H2D of the world,
     # every step calc_timesteps(1) + a statistics read-back, D2H of the world
@@ -573,6 +594,14 @@ def main():
                "note": "set_simulation_data + per step (calc_timesteps(1) + get_raw_statistics) + get_simulation_data, pinned host buffers"}
 
     log("e2e done")
+    sim.close_simulation()
+    # the 4M-cell world does not fit the reference engine (its memory bound
+    # overflows above about 1.83M cells), so the reference arm times the
+    # 1M-cell quarter of the same workload; the same process times this
+    # engine on that world too, device-resident and end to end
+    same = None
+    if args.config == "hex4m" and not args.no_same_workload:
+        same = time_same_workload(args, rank, barrier, max_over_ranks, sum_over_ranks)
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         cpu, _, _ = cpu_baseline(data, world, prm)
@@ -589,7 +618,16 @@ def main():
                        "l2": "state larger than L2 (126 MB), no flush between steps"},
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": per_launch_ms},
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "algorithmic_bytes_per_cell": algorithmic_bytes(dominant, bonds),
+                         "layout_bytes_per_launch": layout_bytes(dominant) * stats1.numCells,
+                         "launch_ms": per_launch_ms,
+                         "note": "achieved = algorithmic bytes per launch (phase accounting, P2 = 40 B/cell) / "
+                                 "CUDA-event launch time; layout bytes = what this engine's arrays move per launch"},
+            "kernel_roofline": kernel_roofline,
+            "step_roofline": {"bytes_per_cell": step_bytes_per_cell(bonds), "achieved_gbs": step_gbs,
+                              "frac": step_gbs / peak, "note": "whole step, B_cell = 192 + 24b"},
+            "same_workload_as_reference": same,
             "kernel_ms_per_step": {k: v / timed_steps for k, v in kernel_ms.items()},
             "step_ms": {"p50": step_p50, "p99": step_p99, "samples": len(step_samples),
                         "note": "single steps between CUDA events, after the timed region"},
@@ -599,9 +637,53 @@ def main():
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))
-    sim.close_simulation()
     reps.close()
     return 0
+
+
+def time_same_workload(args, rank, barrier, max_over_ranks, sum_over_ranks):
+    """hex1m (the reference arm's world): device-resident steps and the same
+    end-to-end loop as the headline line, K steps after W warm-up steps"""
+    from alien_b200.facade import SimulationFacade
+
+    log("same-workload leg: hex1m")
+    data, world, prm, desc = build_workload("hex1m", rank)
+    sim = SimulationFacade()
+    sim.new_simulation(0, world, prm)
+    sim.set_simulation_data(data)
+    sim.calc_timesteps(args.warmup)
+    barrier()
+    ms = max_over_ranks(sim.time_timesteps(args.steps))
+    barrier()
+    sim.close_simulation()
+    n = data.num_cells
+    out = {"workload": "hex1m", "description": desc, "cells": n,
+           "value": sum_over_ranks(n) * args.steps / (ms / 1000.0) / 1e6, "unit": METRIC,
+           "ms_per_step": ms / args.steps}
+    if not args.no_e2e:
+        pins = [pin(data._cells), pin(data._particles)]
+        sim2 = SimulationFacade()
+        sim2.new_simulation(0, world, prm)
+        sim2.set_simulation_data(data)
+        res = sim2.get_simulation_data()
+        out_pins = [pin(res._cells), pin(res._particles)]
+        barrier()
+        t0 = time.perf_counter()
+        sim2.set_simulation_data(data)
+        for _ in range(args.steps):
+            sim2.calc_timesteps(1)
+            sim2.get_raw_statistics()
+        sim2.get_simulation_data(out=res)
+        barrier()
+        t_e2e = max_over_ranks(time.perf_counter() - t0)
+        sim2.close_simulation()
+        for p in pins + out_pins:
+            unpin(p)
+        out["e2e"] = {"value": sum_over_ranks(n) * args.steps / t_e2e / 1e6, "unit": METRIC,
+                      "h2d_bytes_per_step": data.nbytes() / args.steps,
+                      "d2h_bytes_per_step": (res.nbytes() + 112 * args.steps) / args.steps}
+    log(f"same-workload leg: {ms / args.steps:.3f} ms/step")
+    return out
 
 
 if __name__ == "__main__":

@@ -302,6 +302,21 @@ int alien_b200_timed_timesteps(alien_b200_simulation* sim, uint64_t timesteps, d
                                int* numKernels);
 const char* alien_b200_step_kernel_name(int index);
 
+/* The cell map of the current state as the step's own binning kernels
+ * build it (tile histogram, scan, scatter, tile-ordered staging), read back
+ * without stepping: for each binned cell in the map's tile order its id, its
+ * slot (x + y * worldSizeX, the slot of CellMap::set_block, Map.cuh:95-130),
+ * its tile (tiles of ceil(interaction radius) slots, row-major) and its map
+ * flags (bit 0 barrier, bit 1 visible to scans: among the first 10 cells of
+ * its slot in storage order, Map.cuh:117-125; bit 2 first cell of its slot,
+ * CellMap::getFirst).  Host buffers of `capacity` entries each; *count
+ * receives the number of binned cells (ALIEN_B200_ERR_CAPACITY when it
+ * exceeds capacity, nothing written).  A test and debugging hook with no
+ * counterpart in the reference (its map is a device-internal pointer grid);
+ * the state is unchanged. */
+int alien_b200_debug_cell_map(alien_b200_simulation* sim, uint64_t capacity, uint64_t* ids, uint32_t* slots, uint32_t* tiles,
+                              uint8_t* flags, uint64_t* count);
+
 /* Statistics of transfer objects that already sit in device memory,
  * computed without allocating anything on the device.  No counterpart in
  * the reference.  For callers that cannot call cudaMalloc when they need the
@@ -311,11 +326,18 @@ const char* alien_b200_step_kernel_name(int index);
  * owned by the caller (statistics: one AlienRawStatistics written on
  * `stream`, a cudaStream_t or NULL); the result equals
  * alien_b200_get_raw_statistics for the same objects.  The only scratch is a
- * fixed 704 KB array inside the library that every GPU loading it keeps
- * until exit, which bounds one call to 8,388,608 cells and as many
+ * fixed 640 KiB (655,360 B) array inside the library that every GPU loading
+ * it keeps until exit, which bounds one call to 8,388,608 cells and as many
  * particles; larger inputs return ALIEN_B200_ERR_CAPACITY.  The first call
- * on a device looks up the array's device address, so make it before any
- * stream capture.  Calls that overlap on the GPU share the array and race. */
+ * on a device is its set-up: it loads the entry point's code and array onto
+ * that device (CUDA loads modules lazily by default, and that load may need
+ * device memory) and looks up the array's device address.  So make the
+ * first call on each device before reserving the remaining device memory
+ * and before any stream capture; later calls need no device memory.  A
+ * cudaDeviceReset invalidates the looked-up address: do not call again on a
+ * device that was reset.  A CUDA error pending from earlier work is
+ * returned as ALIEN_B200_ERR_CUDA without launching and is left in place.
+ * Calls that overlap on the GPU share the array and race. */
 int alien_b200_statistics_no_alloc(const AlienCellTO* cells, uint64_t numCells, const AlienParticleTO* particles,
                                    uint64_t numParticles, uint64_t timestep, AlienRawStatistics* statistics,
                                    void* stream);

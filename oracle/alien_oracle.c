@@ -882,23 +882,37 @@ static void splittingPhase(OracleWorld* w, int64_t nOrigParts, uint64_t T)
 
 /* ---- CellConnectionProcessor::tryAddConnectionOneWay,
  *      CellConnectionProcessor.cuh:274-427 (angle alignment None), reading
- *      partner bond lists from the pre-phase snapshot (D4) */
+ *      partner bond lists as they stand before the phase (D4) */
 typedef struct {
     int n;
     int32_t b[MAX_BONDS];
     real d[MAX_BONDS], a[MAX_BONDS];
 } BondList;
 
-static int wouldOverlap(const OracleWorld* w, const BondList* snap, int64_t c1, vec2 otherPos)
+/* bond list of cell c as stored (the fusion pass reads the lists before
+ * any of its own additions, D4) */
+static BondList bondListOf(const OracleWorld* w, int64_t c)
+{
+    BondList l;
+    l.n = w->numConn[c];
+    for (int k = 0; k < MAX_BONDS; ++k) {
+        l.b[k] = w->bond[c][k];
+        l.d[k] = w->bondDist[c][k];
+        l.a[k] = w->bondAngle[c][k];
+    }
+    return l;
+}
+
+static int wouldOverlap(const OracleWorld* w, int64_t c1, vec2 otherPos)
 {
     /* CellConnectionProcessor.cuh:476-500 */
-    int n = snap[c1].n;
+    int n = w->numConn[c1];
     if (n < 2) return 0;
     for (int k = 0; k < n; ++k) {
-        int32_t cc = snap[c1].b[k], nc = snap[c1].b[(k + 1) % n];
+        int32_t cc = w->bond[c1][k], nc = w->bond[c1][(k + 1) % n];
         int both = 0;
-        for (int m = 0; m < snap[cc].n; ++m)
-            if (snap[cc].b[m] == nc) {
+        for (int m = 0; m < w->numConn[cc]; ++m)
+            if (w->bond[cc][m] == nc) {
                 both = 1;
                 break;
             }
@@ -908,11 +922,11 @@ static int wouldOverlap(const OracleWorld* w, const BondList* snap, int64_t c1, 
     return 0;
 }
 
-static int tryAddOneWay(const OracleWorld* w, const BondList* snap, int64_t c1, int64_t c2, vec2 posDelta, BondList* out)
+static int tryAddOneWay(const OracleWorld* w, int64_t c1, int64_t c2, vec2 posDelta, BondList* out)
 {
-    *out = snap[c1];
+    *out = bondListOf(w, c1);
     if (out->n == MAX_BONDS) return 0;
-    if (wouldOverlap(w, snap, c1, w->pos[c2])) return 0;
+    if (wouldOverlap(w, c1, w->pos[c2])) return 0;
     real newAngle = angleOfVector(posDelta);
     real desired = vlen(posDelta);
     if (out->n == 0) {
@@ -1335,38 +1349,46 @@ static void stepOnce(OracleWorld* w)
         }
     }
 
-    /* structuralOperations_substep2..4 (SimulationKernels.cu:167-180) */
-    BondList* snap = malloc(sizeof(BondList) * (size_t)(N > 0 ? N : 1));
-    for (int64_t i = 0; i < N; ++i) {
-        snap[i].n = w->numConn[i];
-        for (int k = 0; k < MAX_BONDS; ++k) {
-            snap[i].b[k] = w->bond[i][k];
-            snap[i].d[k] = w->bondDist[i][k];
-            snap[i].a[k] = w->bondAngle[i][k];
-        }
-    }
+    /* structuralOperations_substep2..4 (SimulationKernels.cu:167-180): every
+     * new bond list is computed from the lists as they stand before the
+     * phase, then all are applied (mutual choices pair each cell at most once) */
+    typedef struct {
+        int64_t c[2];
+        BondList l[2];
+    } Fusion;
+    int64_t nFusions = 0, capFusions = 0;
+    Fusion* fusions = NULL;
     for (int64_t i = 0; i < N; ++i) {
         int32_t j = w->best[i];
         if (!w->alive[i] || j < 0 || j <= i || w->best[j] != i) continue;
         int64_t c1 = w->id[i] < w->id[j] ? i : j, c2 = c1 == i ? j : i;
         vec2 pd = correctDirection(w, vsub(w->pos[c2], w->pos[c1]));
-        BondList l1, l2;
-        if (!tryAddOneWay(w, snap, c1, c2, pd, &l1)) continue;
-        if (!tryAddOneWay(w, snap, c2, c1, vmul(pd, -1), &l2)) continue;
-        const BondList* ls[2] = {&l1, &l2};
-        int64_t cs[2] = {c1, c2};
+        Fusion f;
+        f.c[0] = c1;
+        f.c[1] = c2;
+        if (!tryAddOneWay(w, c1, c2, pd, &f.l[0])) continue;
+        if (!tryAddOneWay(w, c2, c1, vmul(pd, -1), &f.l[1])) continue;
+        if (nFusions == capFusions) {
+            capFusions = capFusions ? 2 * capFusions : 1024;
+            fusions = realloc(fusions, sizeof(Fusion) * (size_t)capFusions);
+        }
+        fusions[nFusions++] = f;
+    }
+    for (int64_t f = 0; f < nFusions; ++f) {
         for (int s = 0; s < 2; ++s) {
-            w->numConn[cs[s]] = (uint8_t)ls[s]->n;
+            const int64_t c = fusions[f].c[s];
+            const BondList* l = &fusions[f].l[s];
+            w->numConn[c] = (uint8_t)l->n;
             for (int k = 0; k < MAX_BONDS; ++k) {
-                w->bond[cs[s]][k] = k < ls[s]->n ? ls[s]->b[k] : -1;
-                w->bondDist[cs[s]][k] = ls[s]->d[k];
-                w->bondAngle[cs[s]][k] = ls[s]->a[k];
+                w->bond[c][k] = k < l->n ? l->b[k] : -1;
+                w->bondDist[c][k] = l->d[k];
+                w->bondAngle[c][k] = l->a[k];
             }
         }
-        w->newPartner[c1] = (int32_t)c2;
-        w->newPartner[c2] = (int32_t)c1;
+        w->newPartner[fusions[f].c[0]] = (int32_t)fusions[f].c[1];
+        w->newPartner[fusions[f].c[1]] = (int32_t)fusions[f].c[0];
     }
-    free(snap);
+    free(fusions);
     for (int64_t i = 0; i < N; ++i) {
         if (!w->alive[i] || !w->delCell[i]) continue;
         createParticle(w, w->pos[i], w->vel[i], w->color[i], w->energy[i]);

@@ -62,7 +62,7 @@ _LIBS: dict[str, ctypes.CDLL] = {}
 
 
 def library(precision: str = "f64") -> ctypes.CDLL:
-    name = {"f64": "liboracle_f64.so", "f32": "liboracle_f32.so"}[precision]
+    name = {"f64": "liboracle_f64.so", "f32": "liboracle_f32.so", "f64mt": "liboracle_f64mt.so"}[precision]
     if name not in _LIBS:
         # OpenMP threads must not outnumber the CPUs: spinning waiters on an
         # oversubscribed host stall every barrier

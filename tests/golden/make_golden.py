@@ -1,6 +1,6 @@
 """Generates the golden fixtures of the reference engine (run on a GPU box).
 
-    python tests/golden/make_golden.py <out_dir>
+    python tests/golden/make_golden.py [<out_dir>]   (default: tests/golden)
 
 For each seeded input below it runs the reference's own CUDA engine
 (oracle/_ref/ref_run, built from the reference sources by oracle/ref/Makefile)
@@ -133,4 +133,4 @@ def main(out_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__)))

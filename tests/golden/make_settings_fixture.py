@@ -2,7 +2,11 @@
 physics-stage keys of the reference's sample settings file
 (resources/autosave.settings.json of the reference repository), in the
 file's own nested layout and string values, for the settings reader's test.
-Run in a container that holds the reference at /root/reference."""
+Run where the reference checkout is available:
+
+    python tests/golden/make_settings_fixture.py <reference checkout>
+
+(or with the ALIEN_REFERENCE environment variable naming the checkout)."""
 import json
 import os
 import sys
@@ -11,11 +15,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "..", ".."))
 from alien_b200 import settings  # noqa: E402
 
-SRC = "/root/reference/resources/autosave.settings.json"
+SAMPLE = os.path.join("resources", "autosave.settings.json")
 
 
 def main():
-    with open(SRC, encoding="utf-8") as f:
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ALIEN_REFERENCE", "")
+    if not ref:
+        sys.exit("usage: make_settings_fixture.py <reference checkout>")
+    with open(os.path.join(ref, SAMPLE), encoding="utf-8") as f:
         tree = json.load(f)
     out = {"general": {k: tree["general"][k] for k in ("time step", "world size")}}
     sp = tree["simulation parameters"]

@@ -1,0 +1,216 @@
+"""Parity of the CUDA engine with the FP64 oracle on the benchmark worlds
+themselves, on the engine's own cell map, and on the parts of the step that
+the default parameters leave off (radiation emission, particle splitting).
+
+* One step of each benchmark world at full size: the 512x512 soft-body world
+  (20k lattice cells, 20k energy particles, fluid motion), the 1M-cell SPH
+  fluid world (2048x2048) and the 4M-cell hexagonal soft-body world
+  (4096x4096, collision motion, bond breaking on).  These exercise the pair
+  kernel's paths that small worlds never reach (bands of dense regions, the
+  per-motion region shapes, thousands of regions per launch).  Bar: ids,
+  bond partners in order, bond counts, living states and ages identical;
+  positions, velocities, energies, bond rest lengths and angles within
+  |engine - oracle| <= 1e-5 * max(|oracle|, 1) (tests/helpers.py).  The
+  oracle is the multithreaded FP64 build (per-cell gathers; only the order
+  of its FP64 angle-force additions depends on the thread count).
+* The cell map: the engine bins the input state with its step kernels and
+  returns the map (alien_b200_debug_cell_map); per slot, the set of cell
+  ids must equal the oracle's (Map.cuh:95-130, order independent), every
+  record must lie in the tile of its slot, tiles in ascending order, and a
+  cell's "visible" flag (among the first 10 cells of its slot in storage
+  order, Map.cuh:117-125) and "head" flag (first of its slot) must match
+  the storage-order ranks exactly.
+* Radiation (CellProcessor::radiation, CellProcessor.cuh:725-773) with the
+  reference's default age strength and a high-energy factor, and particle
+  splitting (RadiationProcessor::splitting, RadiationProcessor.cuh:172-204)
+  with a finite split energy: the new particles' ids must be identical and
+  their values within the same tolerance.
+* get_raw_statistics of the engine against counts and FP64 energy sums of
+  the oracle's state after the same steps.
+"""
+import numpy as np
+import pytest
+
+from alien_b200 import params as P
+from alien_b200 import worldgen
+from alien_b200.facade import SimulationFacade
+from oracle.oracle import OracleSimulation
+from tests.helpers import compare_cells, compare_particles
+
+pytestmark = pytest.mark.gpu
+
+
+def run_both(data, world, prm, steps=1, timestep=0, precision="f64mt"):
+    eng = SimulationFacade()
+    eng.new_simulation(timestep, world, prm)
+    eng.set_simulation_data(data)
+    eng.calc_timesteps(steps)
+    got = eng.get_simulation_data()
+    stats = eng.get_raw_statistics()
+    eng.close_simulation()
+    ora = OracleSimulation(world, prm, timestep, precision=precision)
+    ora.set_simulation_data(data)
+    ora.calc_timesteps(steps)
+    ref = ora.get_simulation_data()
+    ora.close()
+    return got, ref, stats
+
+
+CONFIGS = {
+    # name: (generator, motion)
+    "softbody": (lambda: worldgen.soft_body_world(seed=0), P.MOTION_FLUID),
+    "fluid1m": (lambda: worldgen.fluid_world(seed=0), P.MOTION_FLUID),
+    "hex4m": (lambda: worldgen.hex_world(seed=0), P.MOTION_COLLISION),
+}
+_WORLDS = {}
+
+
+def config_world(name):
+    if name not in _WORLDS:
+        _WORLDS[name] = CONFIGS[name][0]()
+    return _WORLDS[name]
+
+
+@pytest.mark.parametrize("name,timestep", [("softbody", 0), ("softbody", 1), ("fluid1m", 0), ("fluid1m", 1),
+                                           ("hex4m", 0), ("hex4m", 1)])
+def test_benchmark_world_one_step(name, timestep):
+    """timestep 0: angle forces and inner friction on; timestep 1: off (the
+    position update runs inside the first bond-force kernel)"""
+    data, world = config_world(name)
+    prm = P.benchmark_parameters(CONFIGS[name][1])
+    got, ref, _ = run_both(data, world, prm, 1, timestep)
+    errs = compare_cells(got.cells, ref.cells, world)
+    errs.update(compare_particles(got.particles, ref.particles, world))
+    print(f"{name} t={timestep}: {len(got.cells)} cells, {len(got.particles)} particles, "
+          + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
+
+
+def _assert_map_matches(data, world, prm):
+    eng = SimulationFacade()
+    eng.new_simulation(0, world, prm)
+    eng.set_simulation_data(data)
+    ids, slots, tiles, flags = eng.debug_cell_map()
+    eng.close_simulation()
+    cells = data.cells
+    assert len(ids) == len(cells)
+    # the oracle's map of the same input (slot of every cell, storage order)
+    ora = OracleSimulation(world, prm, precision="f64mt")
+    ora.set_simulation_data(data)
+    oslots = ora.cell_slots().astype(np.int64)
+    ora.close()
+    W, H = world
+    # tile geometry: tiles of ceil(interaction radius) slots, row-major
+    R = prm.smoothingLength * 2 if prm.motionType == P.MOTION_FLUID else prm.cellMaxCollisionDistance
+    T = max(1, int(np.ceil(np.float32(R))))
+    nTX = -(-W // T)
+    s = slots.astype(np.int64)
+    assert np.array_equal(tiles.astype(np.int64), (s % W) // T + ((s // W) // T) * nTX), "record outside its slot's tile"
+    assert np.all(np.diff(tiles.astype(np.int64)) >= 0), "map records not grouped by tile"
+    # per-slot id sets, order independent
+    id_of = cells["id"].astype(np.uint64)
+    eng_pairs = np.stack([s, ids.astype(np.int64)], 1)
+    ora_pairs = np.stack([oslots, id_of.astype(np.int64)], 1)
+    eng_pairs = eng_pairs[np.lexsort((eng_pairs[:, 1], eng_pairs[:, 0]))]
+    ora_pairs = ora_pairs[np.lexsort((ora_pairs[:, 1], ora_pairs[:, 0]))]
+    assert np.array_equal(eng_pairs, ora_pairs), "cell-map slot sets differ from the oracle's"
+    # visibility and head flags from the storage-order rank within the slot
+    by_id = np.argsort(id_of, kind="stable")
+    order = by_id[np.searchsorted(id_of[by_id], ids)].astype(np.int64)  # storage index of each record
+    by = np.lexsort((order, s))
+    ss, so = s[by], order[by]
+    start = np.r_[0, np.nonzero(np.diff(ss))[0] + 1]
+    rank = np.arange(len(ss)) - np.repeat(start, np.diff(np.r_[start, len(ss)]))
+    want_visible = np.zeros(len(ids), bool)
+    want_head = np.zeros(len(ids), bool)
+    want_visible[by] = rank < 10
+    want_head[by] = rank == 0
+    assert np.array_equal((flags & 2) != 0, want_visible), "visible flags differ from the storage-order ranks"
+    assert np.array_equal((flags & 4) != 0, want_head), "slot-head flags differ from the storage-order ranks"
+    assert np.array_equal((flags & 1) != 0, cells["barrier"][order] != 0)
+    return int(np.max(np.bincount(s)))
+
+
+@pytest.mark.parametrize("motion", [P.MOTION_FLUID, P.MOTION_COLLISION])
+def test_engine_cell_map_matches_oracle(motion):
+    data, world = worldgen.random_test_world(9, free_cells=600, barriers=12)
+    _assert_map_matches(data, world, P.benchmark_parameters(motion))
+
+
+def test_engine_cell_map_dense_slots():
+    """more than 10 cells in some slots: only the first 10 in storage order
+    are visible to the pair scans"""
+    data, world = worldgen.random_test_world(43, world=(16, 16), clusters=0, hex_clusters=0, free_cells=900,
+                                             particles=0)
+    rng = np.random.default_rng(43)
+    c = data.cells
+    c["pos"][:120] = (np.array([3.5, 7.5]) + rng.uniform(-0.45, 0.45, (120, 2))).astype(np.float32)
+    most = _assert_map_matches(data, world, P.benchmark_parameters(P.MOTION_FLUID))
+    assert most > 10
+
+
+@pytest.mark.parametrize("name", ["fluid1m", "hex4m"])
+def test_engine_cell_map_benchmark_worlds(name):
+    data, world = config_world(name)
+    _assert_map_matches(data, world, P.benchmark_parameters(CONFIGS[name][1]))
+
+
+def _radiation_world(seed):
+    data, world = worldgen.random_test_world(seed, free_cells=400, particles=100)
+    rng = np.random.default_rng(seed)
+    data.cells["age"] = rng.integers(0, 200, len(data.cells)).astype(np.uint32)
+    return data, world
+
+
+@pytest.mark.parametrize("motion", [P.MOTION_FLUID, P.MOTION_COLLISION])
+@pytest.mark.parametrize("steps", [1, 3])
+def test_radiation_emission(motion, steps):
+    """the reference's default radiation (age strength 2e-5, probability
+    0.03) plus a high-energy factor for cells above 90 energy units"""
+    data, world = _radiation_world(31)
+    prm = P.default_parameters()
+    prm.motionType = motion
+    for c in range(P.MAX_COLORS):
+        prm.highRadiationFactor[c] = 0.002
+        prm.highRadiationMinCellEnergy[c] = 90.0
+        prm.radiationMinCellAge[c] = 50
+    got, ref, _ = run_both(data, world, prm, steps, 0, precision="f64")
+    assert len(ref.particles) > len(data.particles), "no radiation particle was emitted"
+    compare_cells(got.cells, ref.cells, world)
+    compare_particles(got.particles, ref.particles, world)
+
+
+@pytest.mark.parametrize("steps", [1, 4])
+def test_particle_splitting(steps):
+    """particles above the split energy split with probability 0.01 per step"""
+    data, world = worldgen.random_test_world(32, free_cells=100, particles=3000)
+    data.particles["energy"] = np.random.default_rng(32).uniform(0.5, 6.0, len(data.particles)).astype(np.float32)
+    prm = P.benchmark_parameters(P.MOTION_FLUID)
+    for c in range(P.MAX_COLORS):
+        prm.particleSplitEnergy[c] = 2.0
+    got, ref, _ = run_both(data, world, prm, steps, 0, precision="f64")
+    assert len(ref.particles) > len(data.particles), "no particle split"
+    compare_cells(got.cells, ref.cells, world)
+    compare_particles(got.particles, ref.particles, world)
+
+
+@pytest.mark.parametrize("motion", [P.MOTION_FLUID, P.MOTION_COLLISION])
+def test_statistics_match_oracle(motion):
+    """getRawStatistics after 5 steps (structural operations and decay on):
+    counts exact, energies within the one-step tolerance of the state"""
+    data, world = worldgen.random_test_world(33, world=(48, 48), free_cells=400, vmax=1.2, particles=200)
+    c = data.cells
+    c["energy"][::9] = 20.0
+    prm = P.default_parameters()
+    prm.motionType = motion
+    for i in range(P.MAX_COLORS):
+        prm.cellDeathProbability[i] = 0.3
+    got, ref, stats = run_both(data, world, prm, 5, 0, precision="f64")
+    cells, parts = ref.cells, ref.particles
+    assert stats.timestep == 5
+    assert stats.numCells == len(cells) and stats.numParticles == len(parts)
+    assert stats.numConnections == int(np.sum(cells["numConnections"]))
+    assert list(stats.numCellsByColor) == np.bincount(cells["color"] % 7, minlength=7).tolist()
+    ce = float(np.sum(cells["energy"], dtype=np.float64))
+    pe = float(np.sum(parts["energy"], dtype=np.float64))
+    assert abs(stats.totalCellEnergy - ce) <= 1e-5 * max(ce, 1.0)
+    assert abs(stats.totalParticleEnergy - pe) <= 1e-5 * max(pe, 1.0)

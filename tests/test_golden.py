@@ -235,3 +235,44 @@ def test_engine_neurons_match_reference(path):
     assert np.array_equal(got["cellFunctionUsed"], ref["cellFunctionUsed"])
     assert np.array_equal(got["signalOrigin"], ref["signalOrigin"])
     np.testing.assert_allclose(got["signalChannels"], ref["signalChannels"], rtol=0, atol=NEURON_ATOL)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p) for p in FIXTURES])
+def test_engine_matches_reference_one_step(path):
+    """the CUDA engine held directly to the reference engine's one-step
+    outputs, with the same tolerances as the oracle above; the maximum
+    errors of the reference and of the engine against the FP64 oracle are
+    printed beside each other (the reference is built with -use_fast_math)"""
+    from alien_b200.facade import SimulationFacade
+
+    f = np.load(path)
+    seed, motion, t, wx, wy, ts = (int(v) for v in f["meta"])
+    data, world = worldgen.calm_test_world(seed)
+    if "params" in f:
+        raw = f["params"].tobytes()
+        full = bytearray(bytes(P.default_parameters()))
+        full[: len(raw)] = raw
+        prm = P.PhysicsParams.from_buffer_copy(bytes(full))
+    else:
+        prm = P.benchmark_parameters(motion)
+    eng = SimulationFacade()
+    eng.new_simulation(t, world, prm)
+    eng.set_simulation_data(data)
+    eng.calc_timesteps(1)
+    assert eng.get_current_timestep() == ts
+    got = eng.get_simulation_data()
+    eng.close_simulation()
+    locked = t % 3 == 0 and prm.innerFriction != 0.0
+    tol = REF_RTOL_LOCKED_FRICTION if locked else REF_RTOL
+    e_ref = compare_cells(got.cells, f["out_cells"], world, rtol=tol)
+    e_ref.update(compare_particles(got.particles, f["out_particles"], world, rtol=REF_RTOL))
+    o = OracleSimulation(world, prm, t)
+    o.set_simulation_data(data)
+    o.calc_timesteps(1)
+    fp64 = o.get_simulation_data()
+    e_eng = compare_cells(got.cells, fp64.cells, world)
+    ref_vs_fp64 = compare_cells(f["out_cells"], fp64.cells, world, rtol=tol)
+    print(f"{os.path.basename(path)}: max rel err vs FP64 oracle -- engine pos {e_eng['pos']:.2e} vel {e_eng['vel']:.2e}; "
+          f"reference pos {ref_vs_fp64['pos']:.2e} vel {ref_vs_fp64['vel']:.2e}; engine vs reference pos "
+          f"{e_ref['pos']:.2e} vel {e_ref['vel']:.2e}")

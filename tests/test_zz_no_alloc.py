@@ -96,3 +96,36 @@ def test_no_alloc_statistics_empty_and_limit():
     code = lib.alien_b200_statistics_no_alloc(ctypes.c_void_p(1), MAX_OBJECTS + 1, None, 0, 0, out, None)
     assert code == 6
     assert "at most 8388608 cells" in _lib.last_error()
+
+
+def test_no_alloc_statistics_with_device_memory_reserved():
+    """A caller that reserves the device's remaining memory after the first
+    call (the set-up on this device) can still call the entry point: later
+    calls need no device memory.  The reservation leaves 64 MB free for the
+    driver's own needs and is released at the end of the test."""
+    import torch
+
+    data, world = worldgen.random_test_world(12, free_cells=200)
+    out, ref = _stepped_world(data, world, P.benchmark_parameters(P.MOTION_FLUID), 2)
+    first = _no_alloc_statistics(out.cells, out.particles, ref.timestep)  # set-up call
+    _assert_same(first, ref)
+    lib = _lib.load()
+    d_cells = _device_bytes(out.cells)
+    d_particles = _device_bytes(out.particles)
+    d_out = torch.zeros(ctypes.sizeof(_lib.RawStatistics), dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()
+    free, _ = torch.cuda.mem_get_info()
+    reserve = max(0, free - (64 << 20))
+    hold = torch.empty(reserve, dtype=torch.uint8, device="cuda") if reserve else None
+    try:
+        for _ in range(2):
+            _lib.check(lib.alien_b200_statistics_no_alloc(
+                d_cells.data_ptr(), len(out.cells), d_particles.data_ptr(), len(out.particles),
+                int(ref.timestep), d_out.data_ptr(), stream))
+            torch.cuda.synchronize()
+            got = _lib.RawStatistics.from_buffer_copy(d_out.cpu().numpy().tobytes())
+            _assert_same(got, ref)
+    finally:
+        del hold
+        torch.cuda.empty_cache()
