@@ -55,6 +55,19 @@ class RawStatistics(ctypes.Structure):
     ]
 
 
+PAIR_LANE_CHOICES = (2, 4, 8, 16)
+
+
+class LaunchConfig(ctypes.Structure):
+    """AlienLaunchConfig (include/alien_b200.h)"""
+    _fields_ = [
+        ("pairLanes", ctypes.c_int32 * 2),
+        ("pairLanesFixed", ctypes.c_int32 * 2),
+        ("tuned", ctypes.c_int32),
+        ("tunedMs", (ctypes.c_float * len(PAIR_LANE_CHOICES)) * 2),
+    ]
+
+
 # every symbol declared in include/alien_b200.h and include/alien_b200_batch.h
 EXPORTED_SYMBOLS = [
     "alien_b200_version", "alien_b200_select_device", "alien_b200_time_timesteps",
@@ -70,7 +83,8 @@ EXPORTED_SYMBOLS = [
     "alien_b200_batch_kernel_launch_count", "alien_b200_batch_kernels_per_step", "alien_b200_batch_timed_timesteps",
     "alien_b200_batch_set_step_budget", "alien_b200_batch_world_status", "alien_b200_batch_num_active",
     "alien_b200_batch_device_bytes", "alien_b200_statistics_no_alloc", "alien_b200_batch_synchronize",
-    "alien_b200_debug_cell_map",
+    "alien_b200_debug_cell_map", "alien_b200_set_launch_config", "alien_b200_get_launch_config",
+    "alien_b200_choose_pair_lanes", "alien_b200_batch_set_launch_config", "alien_b200_batch_get_launch_config",
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -130,6 +144,12 @@ def load() -> ctypes.CDLL:
     lib.alien_b200_batch_synchronize.argtypes = [vp]
     lib.alien_b200_statistics_no_alloc.argtypes = [vp, u64, vp, u64, u64, vp, vp]
     lib.alien_b200_debug_cell_map.argtypes = [vp, u64, vp, vp, vp, vp, P(u64)]
+    lib.alien_b200_set_launch_config.argtypes = [vp, P(LaunchConfig)]
+    lib.alien_b200_get_launch_config.argtypes = [vp, P(LaunchConfig)]
+    lib.alien_b200_batch_set_launch_config.argtypes = [vp, P(LaunchConfig)]
+    lib.alien_b200_batch_get_launch_config.argtypes = [vp, P(LaunchConfig)]
+    lib.alien_b200_choose_pair_lanes.argtypes = [P(ctypes.c_float), i32]
+    lib.alien_b200_choose_pair_lanes.restype = i32
     lib.alien_b200_select_device.argtypes = [i32]
     lib.alien_b200_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]
     lib.alien_b200_batch_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]

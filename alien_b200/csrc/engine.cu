@@ -214,6 +214,11 @@ public:
     // the cell map of the current state, built by the step's own binning
     // kernels and read back in tile order (alien_b200_debug_cell_map)
     uint64_t cellMap(uint64_t capacity, uint64_t* ids, uint32_t* slots, uint32_t* tiles, uint8_t* flags);
+    // launch configuration of the pair kernel: lanes per cell per motion
+    // type, fixed by the caller (nonzero) or chosen by the autotuner
+    void setPairLanes(int motion, int lanes);
+    AlienLaunchConfig launchConfig() const;
+    void autotune();
 
     int numWorlds() const { return static_cast<int>(worlds_.size()); }
     const HostWorld& world(int w) const { return worlds_[w]; }
@@ -254,6 +259,21 @@ public:
 
 private:
     void scan(const uint32_t* in, long long n, uint32_t* out);
+    // the pair kernel of one motion type with `lanes` lanes per cell
+    template <int Motion>
+    void launchPairs(int lanes)
+    {
+        const DevState& s = s_;
+        constexpr size_t smem = regionDynSmem<Motion>();
+        const char* name = Motion == ALIEN_B200_MOTION_FLUID ? "kPairsRegion<FLUID>" : "kPairsRegion<COLLISION>";
+        switch (lanes) {
+        case 2: launchNamedSmem(name, kPairsRegion<Motion, 2>, s.numRegions, kRegionThreads, smem, s); break;
+        case 4: launchNamedSmem(name, kPairsRegion<Motion, 4>, s.numRegions, kRegionThreads, smem, s); break;
+        case 8: launchNamedSmem(name, kPairsRegion<Motion, 8>, s.numRegions, kRegionThreads, smem, s); break;
+        case 16: launchNamedSmem(name, kPairsRegion<Motion, 16>, s.numRegions, kRegionThreads, smem, s); break;
+        default: throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "lanes per cell must be 2, 4, 8 or 16");
+        }
+    }
     void releaseGraph()
     {
         if (graphExec_) cudaGraphExecDestroy(graphExec_);
@@ -276,10 +296,16 @@ private:
     uint64_t launches_ = 0;
     int kernelsPerStep_ = 0;
     int partGrid_ = 1;  // blocks of the particle part of a combined launch
+    int overflowGrid_ = 1;  // blocks of kPairsOverflow (a grid-stride loop over the deferred cells)
     int statsGrid_ = 1;  // blocks of a statistics reduction
     cudaGraphExec_t graphExec_ = nullptr;
     uint64_t stepsSinceCheck_ = 0;
     bool hasFluid_ = false, hasCollision_ = false, hasNeurons_ = false;
+    int pairLanes_[2] = {kDefaultPairLanes, kDefaultPairLanes};  // lanes per cell of the pair kernel, per motion type
+    int pairLanesFixed_[2] = {0, 0};  // set by the caller: not tuned
+    bool tuned_ = false;              // the autotuner ran on this layout
+    float tunedMs_[2][kNumPairLaneChoices] = {};
+    void binCurrentState();
     bool signalsLive_ = false;  // some cell has a function or a nonzero signal channel
 };
 
@@ -402,6 +428,9 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     AB_CK(cudaStreamSynchronize(stream_));
     mem_.freeAll();
     worlds_.clear();
+    tuned_ = false;  // a new layout is tuned again at its first step
+    std::memset(tunedMs_, 0, sizeof(tunedMs_));
+    for (int m = 0; m < 2; ++m) pairLanes_[m] = pairLanesFixed_[m] ? pairLanesFixed_[m] : kDefaultPairLanes;
     const int n = static_cast<int>(setups.size());
     long long cellSlots = 0, partSlots = 0, tiles = 0, pmapSlots = 0, coldTotal = 0, auxTotal = 0;
     int regions = 0;
@@ -477,12 +506,9 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     if (cellSlots >= (1ll << 31) || partSlots >= (1ll << 31) || tiles >= (1ll << 32) - 2)
         throw Error(ALIEN_B200_ERR_CAPACITY, "arena exceeds 2^31 slots");
 
-    // the pair-phase regions stage up to RegionShape<>::Cap records in dynamic
-    // shared memory (above the 48 KB default)
-    AB_CK(cudaFuncSetAttribute(kPairsRegion<ALIEN_B200_MOTION_FLUID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(regionDynSmem<ALIEN_B200_MOTION_FLUID>())));
-    AB_CK(cudaFuncSetAttribute(kPairsRegion<ALIEN_B200_MOTION_COLLISION>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(regionDynSmem<ALIEN_B200_MOTION_COLLISION>())));
+    static_assert(regionDynSmem<ALIEN_B200_MOTION_FLUID>() <= 48 * 1024
+                      && regionDynSmem<ALIEN_B200_MOTION_COLLISION>() <= 48 * 1024,
+                  "pair regions fit the default dynamic shared-memory limit");
     DevState& s = s_;
     s = DevState{};
     s.numWorlds = n;
@@ -496,6 +522,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         AB_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
         partGrid_ = std::max(1, std::min(partBlocks, 16 * std::max(sms, 1)));
         statsGrid_ = 4 * std::max(sms, 1);
+        overflowGrid_ = std::max(1, std::min(cellBlocks, 2 * std::max(sms, 1)));
     }
     s.cellSlots = cellSlots;
     s.partSlots = partSlots;
@@ -560,7 +587,9 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     s.sorted = mem_.alloc<uint32_t>(C);
     s.stagedPV = mem_.alloc<float4>(C);
     s.stagedMeta = mem_.alloc<int4>(C);
-    s.tileCount = mem_.alloc<uint32_t>(static_cast<size_t>(tiles));
+    s.tileCount = mem_.alloc<uint32_t>(static_cast<size_t>(tiles) + 1);
+    s.pairOverflowCount = s.tileCount + tiles;
+    s.pairOverflow = mem_.alloc<uint32_t>(C);
     s.tileStart = mem_.alloc<uint32_t>(static_cast<size_t>(tiles) + 1);
     s.scanPartials = mem_.alloc<uint32_t>(static_cast<size_t>(divUp(tiles, kScanTile)) + 2);
 
@@ -687,16 +716,14 @@ void Arena::enqueueStep()
     const DevState& s = s_;
     const int cells = s.numCellBlocks, both = s.numCellBlocks + partGrid_;
     const uint64_t before = launches_;
-    AB_CK(cudaMemsetAsync(s.tileCount, 0, sizeof(uint32_t) * static_cast<size_t>(s.numTiles), stream_));
+    AB_CK(cudaMemsetAsync(s.tileCount, 0, sizeof(uint32_t) * (static_cast<size_t>(s.numTiles) + 1), stream_));
     launch(kBin, both, kBlock, s);
     scan(s.tileCount, s.numTiles, s.tileStart);
     launch(kScatter, cells, kBlock, s);
     launch(kStage, cells, kBlock, s);
-    if (hasFluid_)
-        launchSmem(kPairsRegion<ALIEN_B200_MOTION_FLUID>, s.numRegions, kRegionThreads, regionDynSmem<ALIEN_B200_MOTION_FLUID>(), s);
-    if (hasCollision_)
-        launchSmem(kPairsRegion<ALIEN_B200_MOTION_COLLISION>, s.numRegions, kRegionThreads,
-                   regionDynSmem<ALIEN_B200_MOTION_COLLISION>(), s);
+    if (hasFluid_) launchPairs<ALIEN_B200_MOTION_FLUID>(pairLanes_[ALIEN_B200_MOTION_FLUID]);
+    if (hasCollision_) launchPairs<ALIEN_B200_MOTION_COLLISION>(pairLanes_[ALIEN_B200_MOTION_COLLISION]);
+    launch(kPairsOverflow, overflowGrid_, kBlock, s);
     launch(kApplyBond1, both, kBlock, s);
     launch(kVerletPos, both, kBlock, s);
     launch(kBond2, both, kBlock, s);
@@ -715,6 +742,7 @@ void Arena::enqueueStep()
 void Arena::enqueueSteps(uint64_t n)
 {
     if (n == 0) return;
+    if (!tuned_) autotune();
     if (!graphExec_) {
         cudaGraph_t graph;
         AB_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -739,6 +767,7 @@ void Arena::enqueueSteps(uint64_t n)
 
 std::vector<double> Arena::timedSteps(uint64_t n)
 {
+    if (!tuned_) autotune();
     std::vector<double> sums;
     std::vector<cudaEvent_t> events;
     for (uint64_t i = 0; i < n; ++i) {
@@ -1045,14 +1074,100 @@ void Arena::compactParticles(int w)
     AB_CK(cudaStreamSynchronize(stream_));
 }
 
-uint64_t Arena::cellMap(uint64_t capacity, uint64_t* ids, uint32_t* slots, uint32_t* tiles, uint8_t* flags)
+// the cell map and staged records of the current state, by the step's own
+// binning kernels without the rest of the step (no radiation, no particle
+// map); everything written here is rebuilt by the next step
+void Arena::binCurrentState()
 {
     const DevState& s = s_;
-    AB_CK(cudaMemsetAsync(s.tileCount, 0, sizeof(uint32_t) * static_cast<size_t>(s.numTiles), stream_));
+    AB_CK(cudaMemsetAsync(s.tileCount, 0, sizeof(uint32_t) * (static_cast<size_t>(s.numTiles) + 1), stream_));
     launch(kBinMap, s.numCellBlocks, kBlock, s);
     scan(s.tileCount, s.numTiles, s.tileStart);
     launch(kScatter, s.numCellBlocks, kBlock, s);
     launch(kStage, s.numCellBlocks, kBlock, s);
+}
+
+void Arena::setPairLanes(int motion, int lanes)
+{
+    if (motion != ALIEN_B200_MOTION_FLUID && motion != ALIEN_B200_MOTION_COLLISION)
+        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "motion type must be 0 (fluid) or 1 (collision)");
+    if (lanes != 0 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16)
+        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "lanes per cell must be 0 (autotune), 2, 4, 8 or 16");
+    pairLanesFixed_[motion] = lanes;
+    if (lanes) pairLanes_[motion] = lanes;
+    releaseGraph();
+}
+
+AlienLaunchConfig Arena::launchConfig() const
+{
+    AlienLaunchConfig c;
+    std::memset(&c, 0, sizeof(c));
+    for (int m = 0; m < 2; ++m) {
+        c.pairLanes[m] = pairLanes_[m];
+        c.pairLanesFixed[m] = pairLanesFixed_[m];
+        for (int i = 0; i < kNumPairLaneChoices; ++i) c.tunedMs[m][i] = tunedMs_[m][i];
+    }
+    c.tuned = tuned_ ? 1 : 0;
+    return c;
+}
+
+// The autotuner: for every motion type present whose lanes per cell the
+// caller did not fix, the pair kernel of the current state is launched with
+// each lane count (one untimed launch, then three between CUDA events) and
+// the fastest is kept (alien_b200_choose_pair_lanes).  The pair kernel reads
+// only the staged records and overwrites its own outputs, which the next
+// step recomputes, and its results do not depend on the lane count (fixed-
+// point sums), so tuning changes neither the state nor any result.  Runs
+// once per arena layout, before the step graph is captured.
+void Arena::autotune()
+{
+    tuned_ = true;
+    const bool need[2] = {hasFluid_ && !pairLanesFixed_[ALIEN_B200_MOTION_FLUID],
+                          hasCollision_ && !pairLanesFixed_[ALIEN_B200_MOTION_COLLISION]};
+    if (!need[0] && !need[1]) return;
+    std::vector<WorldCounters> c = readCounters();
+    long long cells = 0;
+    for (const WorldCounters& x : c) cells += x.active ? x.numCells : 0;
+    if (cells == 0) return;
+    binCurrentState();
+    cudaEvent_t ev[4];
+    for (cudaEvent_t& e : ev) AB_CK(cudaEventCreate(&e));
+    try {
+        for (int m = 0; m < 2; ++m) {
+            if (!need[m]) continue;
+            for (int i = 0; i < kNumPairLaneChoices; ++i) {
+                const int lanes = kPairLaneChoices[i];
+                for (int rep = 0; rep < 4; ++rep) {
+                    // deferred cells are listed again by every launch
+                    AB_CK(cudaMemsetAsync(s_.pairOverflowCount, 0, sizeof(uint32_t), stream_));
+                    if (rep > 0) AB_CK(cudaEventRecord(ev[rep], stream_));
+                    if (m == ALIEN_B200_MOTION_FLUID)
+                        launchPairs<ALIEN_B200_MOTION_FLUID>(lanes);
+                    else
+                        launchPairs<ALIEN_B200_MOTION_COLLISION>(lanes);
+                    if (rep > 0) {
+                        AB_CK(cudaEventRecord(ev[0], stream_));
+                        AB_CK(cudaEventSynchronize(ev[0]));
+                        float ms = 0.0f;
+                        AB_CK(cudaEventElapsedTime(&ms, ev[rep], ev[0]));
+                        tunedMs_[m][i] += ms / 3.0f;
+                    }
+                }
+            }
+            pairLanes_[m] = alien_b200_choose_pair_lanes(tunedMs_[m], kNumPairLaneChoices);
+        }
+    } catch (...) {
+        for (cudaEvent_t& e : ev) cudaEventDestroy(e);
+        throw;
+    }
+    for (cudaEvent_t& e : ev) cudaEventDestroy(e);
+    releaseGraph();
+}
+
+uint64_t Arena::cellMap(uint64_t capacity, uint64_t* ids, uint32_t* slots, uint32_t* tiles, uint8_t* flags)
+{
+    const DevState& s = s_;
+    binCurrentState();
     uint32_t total = 0;
     AB_CK(cudaMemcpyAsync(&total, s.tileStart + s.numTiles, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
     AB_CK(cudaStreamSynchronize(stream_));
@@ -1452,7 +1567,52 @@ int alien_b200_debug_cell_map(alien_b200_simulation* sim, uint64_t capacity, uin
     });
 }
 
+int alien_b200_choose_pair_lanes(const float* milliseconds, int n)
+{
+    // the fastest lane count; a larger count must beat the best smaller one
+    // by more than 2 % (timing noise must not flip the choice between
+    // nearly equal configurations)
+    int best = -1;
+    for (int i = 0; i < n && i < kNumPairLaneChoices; ++i) {
+        if (!(milliseconds[i] > 0.0f)) continue;
+        if (best < 0 || milliseconds[i] < 0.98f * milliseconds[best]) best = i;
+    }
+    return best < 0 ? kDefaultPairLanes : kPairLaneChoices[best];
+}
+
+int alien_b200_set_launch_config(alien_b200_simulation* sim, const AlienLaunchConfig* config)
+{
+    return guarded([&] {
+        if (!sim || !config) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        for (int m = 0; m < 2; ++m) sim->arena->setPairLanes(m, config->pairLanesFixed[m]);
+    });
+}
+
+int alien_b200_get_launch_config(alien_b200_simulation* sim, AlienLaunchConfig* config)
+{
+    return guarded([&] {
+        if (!sim || !config) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        *config = sim->arena->launchConfig();
+    });
+}
+
 // ------------------------------------------------------------- batch -----
+int alien_b200_batch_set_launch_config(alien_b200_batch* b, const AlienLaunchConfig* config)
+{
+    return guarded([&] {
+        if (!b || !config) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        for (int m = 0; m < 2; ++m) b->arena->setPairLanes(m, config->pairLanesFixed[m]);
+    });
+}
+
+int alien_b200_batch_get_launch_config(alien_b200_batch* b, AlienLaunchConfig* config)
+{
+    return guarded([&] {
+        if (!b || !config) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        *config = b->arena->launchConfig();
+    });
+}
+
 int alien_b200_batch_create(int numWorlds, const AlienGeneralSettings* general, const AlienPhysicsParams* params,
                             const AlienDataTO* data, uint64_t timestep, alien_b200_batch** out)
 {

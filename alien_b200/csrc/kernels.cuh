@@ -388,20 +388,76 @@ __global__ void __launch_bounds__(kBlock) kExportCellMap(DevState s, unsigned lo
 }
 
 // ---------------------------------------------------------- pair laws ----
-// The pair phase of the two motion types as accumulators: begin() with the
-// cell's staged record, near() as a cheap reject on the squared distance,
-// visit() for the survivors, end() writes the cell's results.  Neighbours
-// are visited tile by tile (3x3 tiles around the cell, in row order) and,
-// within a tile, in storage order, so the FP32 sums are reproducible run to
-// run and identical alone or in a batch.  Two enumerations feed the laws:
-// kPairsRegion (shared-memory regions, the fast path) and pairsGlobal (tile
-// lists in global memory, for regions that do not fit).
+// The pair phase of the two motion types as accumulators: beginScan() and
+// beginLaw() with the cell's staged record, near() as a cheap reject on the
+// squared distance, relevant() for candidates whose visit can change
+// something, visit() for the survivors, reduce() across the lanes that
+// shared the cell's candidates, end() writes the cell's results.
+//
+// Every sum is a 2^-32 fixed-point integer (toFix of each FP32 term) and
+// every choice is a minimum over a total order (smallest id, nearest
+// barrier then smallest slot), so a cell's results do not depend on the
+// order in which its candidates are visited nor on how they are split
+// across lanes: the tile size, the region shape and the lanes per cell are
+// free launch parameters, and the results are bit-identical run to run,
+// between launch configurations and between a world alone and in a batch.
+// Two enumerations feed the laws: kPairsRegion (shared-memory regions, the
+// fast path) and pairsGlobal (tile lists in global memory, for regions that
+// do not fit).
 
 // sqrtf(q) <= R decided exactly (the reject bound is above R^2)
 __device__ __forceinline__ bool withinRadius(float q, float R, float& d)
 {
     d = sqrtf(q);
     return d <= R;
+}
+
+// LPC consecutive lanes of a warp that share one cell's candidates
+template <int LPC>
+struct LaneGroup {
+    static_assert(LPC >= 1 && LPC <= 32 && (LPC & (LPC - 1)) == 0, "lanes per cell: a power of two");
+    unsigned mask;
+    int lane;
+    __device__ __forceinline__ LaneGroup()
+    {
+        const int wl = threadIdx.x & 31;
+        lane = wl & (LPC - 1);
+        mask = LPC == 32 ? 0xffffffffu : (((1u << (LPC & 31)) - 1u) << (wl & ~(LPC - 1)));
+    }
+    __device__ __forceinline__ long long sum(long long v) const
+    {
+#pragma unroll
+        for (int o = LPC / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, LPC);
+        return v;
+    }
+    __device__ __forceinline__ bool any(bool p) const { return LPC == 1 ? p : __any_sync(mask, p); }
+    // (key, idx) of the lane with the smallest key, ties to the smallest idx
+    template <class K>
+    __device__ __forceinline__ void argmin(K& key, int& idx) const
+    {
+#pragma unroll
+        for (int o = LPC / 2; o > 0; o >>= 1) {
+            const K k2 = __shfl_xor_sync(mask, key, o, LPC);
+            const int i2 = __shfl_xor_sync(mask, idx, o, LPC);
+            if (k2 < key || (k2 == key && i2 < idx)) {
+                key = k2;
+                idx = i2;
+            }
+        }
+    }
+};
+
+// the cell's bond partners (slot indices, unused entries -1): three 8-byte
+// loads of the bond row
+__device__ __forceinline__ void loadBondPartners(const DevState& st, long long g, int n, int* bonds)
+{
+    const int2* row = reinterpret_cast<const int2*>(st.bond + g * kMaxBonds);
+#pragma unroll
+    for (int h = 0; h < kMaxBonds / 2; ++h) {
+        const int2 b = 2 * h < n ? row[h] : make_int2(-1, -1);
+        bonds[2 * h] = b.x;
+        bonds[2 * h + 1] = 2 * h + 1 < n ? b.y : -1;
+    }
 }
 
 // CellProcessor::calcFluidForces_reconnectCells_correctOverlap,
@@ -413,16 +469,14 @@ struct FluidLaw {
     float h, invH, invH2, invH3, R, R2reject, minDist, fusionVelocity, maxBindingEnergy;
     float2 pi, vi;
     bool barrierI, fusionI;
-    float densI, invDensI;
+    float invDensI;
     int bondsI[kMaxBonds];
-    float dens;
-    float2 Fp, Fv, dx;
-    int bestBarrier;
+    long long dens, fpx, fpy, fvx, fvy, dxx, dxy;  // fixed-point sums
+    int bestBarrier;          // nearest barrier cell (slot), -1 = none
     float bestBarrierDist;
-    int best;
+    int best;                 // fusion choice: partner with the smallest id
     unsigned long long bestId;
 
-    // the state near() and relevant() need (the scan), then the rest (the law)
     __device__ __forceinline__ void beginScan(const DevState& st, const WorldInfo& wi, int4 me)
     {
         s = &st;
@@ -448,23 +502,14 @@ struct FluidLaw {
         vi = vel;
         barrierI = me.y & kStageBarrier;
         const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
-        densI = __int_as_float(me.z);
-        invDensI = __frcp_rn(densI);
+        invDensI = __frcp_rn(__int_as_float(me.z));
         fusionI = !barrierI && nI < maxI && __int_as_float(me.w) <= maxBindingEnergy;
-#pragma unroll
-        for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? st.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
-        dens = 0.0f;
-        Fp = Fv = dx = f2(0.0f, 0.0f);
+        loadBondPartners(st, g, nI, bondsI);
+        dens = fpx = fpy = fvx = fvy = dxx = dxy = 0;
         bestBarrier = -1;
         bestBarrierDist = 0.0f;
         best = -1;
         bestId = ~0ull;
-    }
-
-    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float2 pos, float2 vel)
-    {
-        beginScan(st, wi, me);
-        beginLaw(wi, me, pos, vel);
     }
 
     __device__ __forceinline__ bool near(float2 pd) const { return pd.x * pd.x + pd.y * pd.y <= R2reject; }
@@ -485,9 +530,12 @@ struct FluidLaw {
             return;
         }
         const float q = d * invH;
-        dens += sphKernel(q) * invH2;
+        dens += toFix(sphKernel(q) * invH2);
         if (j == g) return;
-        if (!barrierI && d < minDist) dx = dx + pd * (minDist / 5.0f);
+        if (!barrierI && d < minDist) {
+            dxx += toFix(pd.x * (minDist / 5.0f));
+            dxy += toFix(pd.y * (minDist / 5.0f));
+        }
         if (isBondedTo(bondsI, j)) return;
         const float2 vd = vi - vj;
         // rho_i / rho_i^2 + rho_j / rho_j^2 (CellProcessor.cuh:205) as reciprocals
@@ -495,8 +543,12 @@ struct FluidLaw {
         const float factor = invDensI + invDensJ;
         if (fabsf(d) > kNearZero) {
             const float kd = sphKernelD(q) * invH3;
-            Fp = Fp + pd * (-factor * kd * __frcp_rn(d));
-            Fv = Fv + vd * (invDensJ * d * kd * __frcp_rn(d * d + 0.25f));
+            const float cp = -factor * kd * __frcp_rn(d);
+            const float cv = invDensJ * d * kd * __frcp_rn(d * d + 0.25f);
+            fpx += toFix(pd.x * cp);
+            fpy += toFix(pd.y * cp);
+            fvx += toFix(vd.x * cv);
+            fvy += toFix(vd.y * cv);
         }
         if (fusionI && len2(vd) >= fusionVelocity) {
             const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
@@ -507,6 +559,33 @@ struct FluidLaw {
                     best = j;
                 }
             }
+        }
+    }
+
+    template <int LPC>
+    __device__ __forceinline__ void reduce(const LaneGroup<LPC>& grp)
+    {
+        if (LPC == 1) return;
+        dens = grp.sum(dens);
+        if (grp.any((fpx | fpy | fvx | fvy | dxx | dxy) != 0)) {
+            fpx = grp.sum(fpx);
+            fpy = grp.sum(fpy);
+            fvx = grp.sum(fvx);
+            fvy = grp.sum(fvy);
+            dxx = grp.sum(dxx);
+            dxy = grp.sum(dxy);
+        }
+        if (grp.any(best >= 0)) {
+            int idx = best;
+            grp.argmin(bestId, idx);
+            best = idx;
+        }
+        if (grp.any(bestBarrier >= 0)) {
+            float key = bestBarrier >= 0 ? bestBarrierDist : __int_as_float(0x7f800000);
+            int idx = bestBarrier >= 0 ? bestBarrier : 0x7fffffff;
+            grp.argmin(key, idx);
+            bestBarrier = idx == 0x7fffffff ? -1 : idx;
+            bestBarrierDist = key;
         }
     }
 
@@ -545,10 +624,11 @@ struct FluidLaw {
                 F = rr * (-2.0f * dvr / trr) / td;
             }
         }
+        const float2 Fp = f2(fromFix(fpx), fromFix(fpy)), Fv = f2(fromFix(fvx), fromFix(fvy));
         F = F + (Fp * p->pressureStrength + Fv * p->viscosityStrength);
         st.force[g] = F;
-        st.posB[g] = pi + dx;
-        st.densNew[g] = dens;
+        st.posB[g] = pi + f2(fromFix(dxx), fromFix(dxy));
+        st.densNew[g] = fromFix(dens);
         st.best[g] = best;
     }
 };
@@ -583,7 +663,7 @@ struct CollisionLaw {
     bool barrierI, visibleI, fusionI;
     float densI;
     int bondsI[kMaxBonds];
-    float2 F, dx;
+    long long fx, fy, dxx, dxy;  // fixed-point sums
     int best;
     unsigned long long bestId;
 
@@ -598,9 +678,7 @@ struct CollisionLaw {
         minDist = p->cellMinDistance;
         minDist2Keep = minDist * minDist * 1.0001f + 1e-6f;
         barrierI = me.y & kStageBarrier;
-        const int nI = (me.y >> 4) & 0xf;
-#pragma unroll
-        for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? st.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
+        loadBondPartners(st, g, (me.y >> 4) & 0xf, bondsI);
     }
 
     __device__ __forceinline__ void beginLaw(const WorldInfo&, int4 me, float2 pos, float2 vel)
@@ -613,15 +691,9 @@ struct CollisionLaw {
         const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
         densI = __int_as_float(me.z);
         fusionI = !barrierI && nI < maxI && __int_as_float(me.w) <= maxBindingEnergy;
-        F = dx = f2(0.0f, 0.0f);
+        fx = fy = dxx = dxy = 0;
         best = -1;
         bestId = ~0ull;
-    }
-
-    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float2 pos, float2 vel)
-    {
-        beginScan(st, wi, me);
-        beginLaw(wi, me, pos, vel);
     }
 
     __device__ __forceinline__ bool near(float2 raw) const { return raw.x * raw.x + raw.y * raw.y <= R2reject; }
@@ -649,9 +721,14 @@ struct CollisionLaw {
         const float2 pd = f2(-raw.x, -raw.y);
         const bool bonded = isBondedTo(bondsI, j);
         if (visibleJ) {  // i's own scan sees j
-            if (!barrierI && d < minDist) dx = dx + pd * (minDist / 5.0f);
+            if (!barrierI && d < minDist) {
+                dxx += toFix(pd.x * (minDist / 5.0f));
+                dxy += toFix(pd.y * (minDist / 5.0f));
+            }
             if (!bonded) {
-                F = F + collisionForce(pd, d, vi, vj, barrierI, *p);
+                const float2 f = collisionForce(pd, d, vi, vj, barrierI, *p);
+                fx += toFix(f.x);
+                fy += toFix(f.y);
                 const float2 vd = vi - vj;
                 if (fusionI && len2(vd) >= fusionVelocity && dot2(pd, vd) < 0.0f) {
                     const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
@@ -665,24 +742,42 @@ struct CollisionLaw {
                 }
             }
         }
-        if (visibleI && !bonded)  // j's scan sees i and applies -f(j,i) to i
-            F = F - collisionForce(raw, d, vj, vi, om.y & kStageBarrier, *p);
+        if (visibleI && !bonded) {  // j's scan sees i and applies -f(j,i) to i
+            const float2 f = collisionForce(raw, d, vj, vi, om.y & kStageBarrier, *p);
+            fx -= toFix(f.x);
+            fy -= toFix(f.y);
+        }
+    }
+
+    template <int LPC>
+    __device__ __forceinline__ void reduce(const LaneGroup<LPC>& grp)
+    {
+        if (LPC == 1) return;
+        if (grp.any((fx | fy | dxx | dxy) != 0)) {
+            fx = grp.sum(fx);
+            fy = grp.sum(fy);
+            dxx = grp.sum(dxx);
+            dxy = grp.sum(dxy);
+        }
+        if (grp.any(best >= 0)) {
+            int idx = best;
+            grp.argmin(bestId, idx);
+            best = idx;
+        }
     }
 
     __device__ __forceinline__ void end()
     {
         const DevState& st = *s;
-        st.force[g] = F;
-        st.posB[g] = pi + dx;
+        st.force[g] = f2(fromFix(fx), fromFix(fy));
+        st.posB[g] = pi + f2(fromFix(dxx), fromFix(dxy));
         st.densNew[g] = densI;
         st.best[g] = best;
     }
 };
 
 // the pair phase of the staged cell k, neighbours from the global tile lists
-// (tiles in the same row order as the regions' 3x3 scan)
-template <int Motion>
-__device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
+__device__ __forceinline__ void pairsGlobalCell(const DevState& s, long long k, int motion)
 {
     const int4 me = s.stagedMeta[k];
     const float4 mpv = s.stagedPV[k];
@@ -690,9 +785,10 @@ __device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
     const WorldInfo& wi = s.worlds[w];
     const float2 pi = f2(mpv.x, mpv.y);
     const int sx = slotX(pi.x, wi.W), sy = slotX(pi.y, wi.H);
-    if (Motion == ALIEN_B200_MOTION_FLUID) {
+    if (motion == ALIEN_B200_MOTION_FLUID) {
         FluidLaw law;
-        law.begin(s, wi, me, pi, f2(mpv.z, mpv.w));
+        law.beginScan(s, wi, me);
+        law.beginLaw(wi, me, pi, f2(mpv.z, mpv.w));
         forEachWindowTile(wi, sx, sy, [&](long long t) {
             const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
             for (uint32_t m = k0; m < k1; ++m) {
@@ -704,7 +800,8 @@ __device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
         law.end();
     } else {
         CollisionLaw law;
-        law.begin(s, wi, me, pi, f2(mpv.z, mpv.w));
+        law.beginScan(s, wi, me);
+        law.beginLaw(wi, me, pi, f2(mpv.z, mpv.w));
         forEachWindowTile(wi, sx, sy, [&](long long t) {
             const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
             for (uint32_t m = k0; m < k1; ++m) {
@@ -716,72 +813,81 @@ __device__ __forceinline__ void pairsGlobal(const DevState& s, long long k)
         law.end();
     }
 }
+// Cells that the region kernels cannot stage (rows denser than the shared
+// buffer, worlds too small for regions) are appended to the overflow list
+// and handled by kPairsOverflow after the region kernels, one thread per
+// cell, so that the region kernels carry none of this path's registers.
+__device__ __forceinline__ void pairsDefer(const DevState& s, long long k)
+{
+    const uint32_t at = atomicAdd(s.pairOverflowCount, 1u);
+    s.pairOverflow[at] = static_cast<uint32_t>(k);  // at most one entry per staged cell
+}
+
+__global__ void __launch_bounds__(kBlock) kPairsOverflow(DevState s)
+{
+    const uint32_t n = *s.pairOverflowCount;
+    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        const long long k = s.pairOverflow[i];
+        pairsGlobalCell(s, k, s.worlds[(s.stagedMeta[k].y >> 16) & 0xffff].motionType);
+    }
+}
 
 // ------------------------------------------------------- kPairsRegion ----
-// One CTA per region of regW x regH tiles (up to RegionShape<Motion>: 24 x 16
-// for collision worlds, 32 x 8 for fluid worlds) of one world.  It
-// copies the staged records of the region and of its one-tile halo from the
-// tile-sorted arrays into shared memory, all (regW+2) x (regH+2) local tiles
-// in row-major order (each tile a contiguous run in storage order), so that
-// the tiles of one row of a cell's window are one contiguous run.  A local
-// row is at most three contiguous global runs (left halo tile, own tiles,
-// right halo tile), so the copy finds its source with a search over rows.
-// Fluid worlds shift halo tiles that lie across the torus seam by +-W / +-H,
-// so that plain differences are the minimal-image displacements; collision
-// worlds keep stored positions (the reference's distance test is on the
-// uncorrected difference, so candidates across the seam never pass).
-// Every cell scans only the tiles of its 3x3 window that the disc of radius
-// R around it reaches (a neighbour tile is skipped when the cell is farther
-// than R, plus a rounding margin, from the shared edge: such tiles hold no
-// candidate within R), appending candidates that pass the cheap distance
-// reject to a per-thread hit list in shared memory, and runs the pair law on
-// the hits afterwards: the scan loop stays convergent across the warp, and
-// the law runs once per hit instead of once per scan iteration in which any
-// lane had a hit.  The scan loop holds only the state the reject needs (the
-// law's accumulators start after it), and a cell with more than HitCap hits
-// scans a second time, visiting on the way in the same order.  Hits are
-// visited in scan order (row by row, tile by tile, storage order), the order
-// of the full 3x3 scan minus candidates that the law ignores, so the FP32
-// sums do not depend on the pruning.
-// Regions whose records exceed the shared buffer, and worlds too small for
-// regions, use pairsGlobal for their cells.
+// One CTA per region of regW x regH tiles (at most RegionShape<Motion>) of
+// one world.  It copies the staged records of the region and of its
+// one-tile halo from the tile-sorted arrays into shared memory, all
+// (regW+2) x (regH+2) local tiles in row-major order (each tile a contiguous
+// run), so that the tiles of one row of a cell's window are one contiguous
+// run.  A local row is at most three contiguous global runs (left halo tile,
+// own tiles, right halo tile), so the copy finds its source with a search
+// over rows.  Fluid worlds shift halo tiles that lie across the torus seam by
+// +-W / +-H, so that plain differences are the minimal-image displacements;
+// collision worlds keep stored positions (the reference's distance test is
+// on the uncorrected difference, so candidates across the seam never pass).
+//
+// Each own cell is handled by a group of LPC lanes: the group lists the
+// window tiles the cell's disc reaches (a neighbour tile is skipped when the
+// cell is farther than R, plus a rounding margin, from the shared edge:
+// such tiles hold no candidate within R) as at most three contiguous runs of
+// shared-memory records, the lanes take every LPC-th candidate of the
+// flattened runs, visit the candidates that pass the reject, and the group
+// reduces its fixed-point sums with shuffles; lane 0 writes the results.
+// Groups take the band's own cells round robin, so every lane of the CTA
+// has work until the last LPC-lane group finishes.
+// Regions whose records exceed the shared buffer are processed in bands of
+// own rows; rows that do not fit even alone, and worlds too small for
+// regions, defer their cells to kPairsOverflow.
 constexpr int kRegionThreads = 256;
-// Region shape per motion type (tiles per region, shared-buffer records,
-// hit-list entries per thread, resident CTAs per SM), from a sweep of shapes
-// on the B200.  Dense regions
-// are processed in bands of rows, so the buffer size bounds no world.  The
-// visiting order does not depend on the shape; the FP32 results of different
-// builds can still differ in the last bit where the compiler contracts
-// multiply-adds differently.
+constexpr int kDefaultPairLanes = 4;  // lanes per cell until the autotuner has run
+constexpr int kNumPairLaneChoices = ALIEN_B200_PAIR_LANE_CHOICES;
+constexpr int kPairLaneChoices[kNumPairLaneChoices] = {2, 4, 8, 16};
 template <int Motion>
 struct RegionShape;
 template <>
 struct RegionShape<ALIEN_B200_MOTION_FLUID> {
-    static constexpr int W = 32, H = 8, Cap = 1152, HitCap = 24, MinBlocks = 3;
+    static constexpr int W = 32, H = 8, Cap = 1152, MinBlocks = 4;
 };
 template <>
 struct RegionShape<ALIEN_B200_MOTION_COLLISION> {
-    static constexpr int W = 24, H = 16, Cap = 1152, HitCap = 24, MinBlocks = 4;
+    static constexpr int W = 24, H = 16, Cap = 1152, MinBlocks = 4;
 };
 template <int Motion>
 constexpr size_t regionDynSmem()
 {
-    return static_cast<size_t>(RegionShape<Motion>::Cap) * (sizeof(int4) + 2 * sizeof(float2))
-           + static_cast<size_t>(RegionShape<Motion>::HitCap) * kRegionThreads * sizeof(uint16_t);
+    return static_cast<size_t>(RegionShape<Motion>::Cap) * (sizeof(int4) + 2 * sizeof(float2));
 }
 
-template <int Motion>
+template <int Motion, int LPC>
 __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks) kPairsRegion(DevState s)
 {
     constexpr int kRegionCap = RegionShape<Motion>::Cap;
-    constexpr int kHitCap = RegionShape<Motion>::HitCap;
     constexpr int kRegionMaxH = RegionShape<Motion>::H;
     constexpr int kRegionMaxTiles = (RegionShape<Motion>::W + 2) * (RegionShape<Motion>::H + 2);
+    constexpr int kGroups = kRegionThreads / LPC;
     extern __shared__ int4 dyn[];
     int4* sMeta = dyn;
     float2* sPos = reinterpret_cast<float2*>(sMeta + kRegionCap);
     float2* sVel = sPos + kRegionCap;
-    uint16_t* sHits = reinterpret_cast<uint16_t*>(sVel + kRegionCap);  // [kHitCap][kRegionThreads]
     __shared__ int tStart[kRegionMaxTiles + 1];  // shared-memory offset of each local tile
     __shared__ int tGlobal[kRegionMaxTiles];     // first sorted index of the tile
     __shared__ float2 tShift[kRegionMaxTiles];
@@ -802,7 +908,7 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
             for (int lx = 0; lx < ownW; ++lx) {
                 const long long t = wi.tileBase + (tx0 + lx) + static_cast<long long>(ty0 + ly) * wi.nTX;
                 for (uint32_t k = s.tileStart[t] + threadIdx.x; k < s.tileStart[t + 1]; k += kRegionThreads)
-                    pairsGlobal<Motion>(s, k);
+                    pairsDefer(s, k);
             }
         return;
     }
@@ -864,12 +970,13 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
         if (r <= ownH) rowOwn[r] = acc;
     }
     __syncthreads();
-    uint16_t* myHits = sHits + threadIdx.x;
+    const LaneGroup<LPC> grp;
+    const int group = threadIdx.x / LPC;
     const float T = static_cast<float>(wi.T);
     // Own rows in bands whose local rows (the band and one halo row on either
     // side) fit the shared buffer: one band for the usual region, several for
     // a dense one.  Every thread derives the same bands from tStart.  A single
-    // own row that does not fit even alone takes the global-memory path.
+    // own row that does not fit even alone is deferred to kPairsOverflow.
     int band0 = 1;
     while (band0 <= ownH) {
         const int base = tStart[(band0 - 1) * LW];
@@ -878,7 +985,7 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
             for (int lx = 1; lx <= ownW; ++lx) {
                 const int q = ly * LW + lx;
                 const int k0 = tGlobal[q], n = tStart[q + 1] - tStart[q];
-                for (int k = k0 + threadIdx.x; k < k0 + n; k += kRegionThreads) pairsGlobal<Motion>(s, k);
+                for (int k = k0 + threadIdx.x; k < k0 + n; k += kRegionThreads) pairsDefer(s, k);
             }
             ++band0;
             continue;
@@ -907,19 +1014,19 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
             sMeta[e - base] = s.stagedMeta[src];
         }
         __syncthreads();
-        // 3. pair law of every own cell of the band against the tiles its
-        //    disc reaches (shared-memory index = record offset - base)
+        // 3. each own cell of the band by one group of LPC lanes, round robin
+        //    (shared-memory index = record offset - base)
         int ly = band0;  // own row of o; o only grows, so the search continues from the last row
-        for (int o = rowOwn[band0 - 1] + threadIdx.x; o < rowOwn[band1]; o += kRegionThreads) {
+        for (int o = rowOwn[band0 - 1] + group; o < rowOwn[band1]; o += kGroups) {
             while (rowOwn[ly] <= o) ++ly;
             const int e = tStart[ly * LW + 1] + (o - rowOwn[ly - 1]) - base;
             const float2 pi = sPos[e];
+            const int4 me = sMeta[e];
             // own tile column as binned (own tiles are not shifted)
             const int gx = slotX(pi.x, wi.W) / wi.T;
             const int lx = min(max(gx - tx0 + 1, 1), ownW);
             const int gy = ty0 + ly - 1;
             auto scan = [&](auto& law, auto diff) {
-                const int4 me = sMeta[e];
                 law.beginScan(s, wi, me);
                 // reach: R plus a margin above the rounding of positions up to the world size
                 const float reach = law.R * 1.0001f + 1e-3f + 4.0f * static_cast<float>(max(wi.W, wi.H)) * 1.2e-7f;
@@ -927,38 +1034,29 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
                 const float bottom = static_cast<float>(gy) * T, top = fminf(static_cast<float>(gy + 1) * T, static_cast<float>(wi.H));
                 const int c0 = lx - (pi.x - reach < left ? 1 : 0), c1 = lx + (pi.x + reach >= right ? 1 : 0);
                 const int r0 = ly - (pi.y - reach < bottom ? 1 : 0), r1 = ly + (pi.y + reach >= top ? 1 : 0);
-                // scan: the hits in scan order (the first kHitCap kept, all counted)
-                int nh = 0;
-#pragma unroll 1
-                for (int r = r0; r <= r1; ++r) {
-                    const int b0 = tStart[r * LW + c0] - base, b1 = tStart[r * LW + c1 + 1] - base;
-                    for (int m = b0; m < b1; ++m) {
-                        const float2 dm = diff(m);
-                        if (law.near(dm) && law.relevant(sMeta, m, dm)) {
-                            if (nh < kHitCap) myHits[nh * kRegionThreads] = static_cast<uint16_t>(m);
-                            ++nh;
-                        }
-                    }
-                }
-                // law over the hits; a cell with more hits than the list holds
-                // scans again and visits on the way, in the same order
-                law.beginLaw(wi, me, pi, sVel[e]);
-                if (nh <= kHitCap) {
-                    for (int i = 0; i < nh; ++i) {
-                        const int m = myHits[i * kRegionThreads];
-                        law.visit(sMeta[m], sVel[m], diff(m));
-                    }
-                } else {
-#pragma unroll 1
-                    for (int r = r0; r <= r1; ++r) {
+                // the window rows' runs, flattened: candidate k of the cell is
+                // record k + shift[r] of run r, for k in [runEnd[r-1], runEnd[r])
+                int shift[3], runEnd[3], total = 0;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const int r = r0 + i;
+                    if (r <= r1) {
                         const int b0 = tStart[r * LW + c0] - base, b1 = tStart[r * LW + c1 + 1] - base;
-                        for (int m = b0; m < b1; ++m) {
-                            const float2 dm = diff(m);
-                            if (law.near(dm) && law.relevant(sMeta, m, dm)) law.visit(sMeta[m], sVel[m], dm);
-                        }
+                        shift[i] = b0 - total;
+                        total += b1 - b0;
+                    } else {
+                        shift[i] = 0;
                     }
+                    runEnd[i] = total;
                 }
-                law.end();
+                law.beginLaw(wi, me, pi, sVel[e]);
+                for (int k = grp.lane; k < total; k += LPC) {
+                    const int m = k + (k < runEnd[0] ? shift[0] : (k < runEnd[1] ? shift[1] : shift[2]));
+                    const float2 dm = diff(m);
+                    if (law.near(dm) && law.relevant(sMeta, m, dm)) law.visit(sMeta[m], sVel[m], dm);
+                }
+                law.reduce(grp);
+                if (grp.lane == 0) law.end();
             };
             if (Motion == ALIEN_B200_MOTION_FLUID) {
                 FluidLaw law;

@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import ArraySizes, GeneralSettings, Int2, RawStatistics, check
+from ._lib import ArraySizes, GeneralSettings, Int2, LaunchConfig, RawStatistics, check
 from .params import PhysicsParams
 from .to import CELL_TO, PARTICLE_TO, DataTO
 
@@ -122,6 +122,18 @@ class SimulationFacade:
         r = RawStatistics()
         check(self._lib.alien_b200_get_raw_statistics(self._handle(), ctypes.byref(r)))
         return r
+
+    def launch_config(self) -> LaunchConfig:
+        """lanes per cell of the pair kernel in use, and the autotuner's timings"""
+        c = LaunchConfig()
+        check(self._lib.alien_b200_get_launch_config(self._handle(), ctypes.byref(c)))
+        return c
+
+    def set_pair_lanes(self, fluid: int = 0, collision: int = 0) -> None:
+        """fix the lanes per cell of the pair kernel per motion type (0 = autotune)"""
+        c = LaunchConfig()
+        c.pairLanesFixed[0], c.pairLanesFixed[1] = int(fluid), int(collision)
+        check(self._lib.alien_b200_set_launch_config(self._handle(), ctypes.byref(c)))
 
     def debug_cell_map(self):
         """The engine's cell map of the current state (alien_b200_debug_cell_map):
@@ -234,6 +246,16 @@ class BatchSimulation:
 
     def kernel_launches(self) -> int:
         return int(self._lib.alien_b200_batch_kernel_launch_count(self._h))
+
+    def launch_config(self) -> LaunchConfig:
+        c = LaunchConfig()
+        check(self._lib.alien_b200_batch_get_launch_config(self._h, ctypes.byref(c)))
+        return c
+
+    def set_pair_lanes(self, fluid: int = 0, collision: int = 0) -> None:
+        c = LaunchConfig()
+        c.pairLanesFixed[0], c.pairLanesFixed[1] = int(fluid), int(collision)
+        check(self._lib.alien_b200_batch_set_launch_config(self._h, ctypes.byref(c)))
 
     def kernels_per_step(self) -> int:
         return int(self._lib.alien_b200_batch_kernels_per_step(self._h))

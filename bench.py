@@ -60,7 +60,7 @@ def algorithmic_bytes(kernel: str, bonds_per_cell: float) -> float:
     does the Verlet position update in the two steps of three without angle
     forces (the position kernel does it in the third)."""
     b = bonds_per_cell
-    if kernel.startswith("kPairs"):
+    if kernel.startswith("kPairsRegion"):
         return PHASE_BYTES["P2"](b)
     return {
         "kApplyBond1": PHASE_BYTES["P3"](b) + PHASE_BYTES["P4"](b) + PHASE_BYTES["P5"](b) * 2.0 / 3.0,
@@ -75,7 +75,7 @@ def layout_bytes(kernel: str) -> float:
     array read or written for the cell counted once: the staged pair record
     is 32 B, a bond row 24 B, rest lengths 24 B, ...): the traffic to expect
     from the layout, as opposed to the algorithmic minimum above."""
-    if kernel.startswith("kPairs"):
+    if kernel.startswith("kPairsRegion"):
         return 80.0
     return {"kApplyBond1": 104.0 + 16.0 / 3.0, "kBond2": 80.0, "kVerletPos": 58.0 / 3.0, "kVerletVel": 67.0,
             "kBin": 26.0}.get(kernel, 0.0)
@@ -516,6 +516,11 @@ def main():
     barrier()
     launches = sim.kernel_launches() - launches0
     stats1 = sim.get_raw_statistics()
+    lc = sim.launch_config()
+    launch_cfg = {"pair_lanes_per_cell": {"fluid": lc.pairLanes[0], "collision": lc.pairLanes[1]},
+                  "autotuned": bool(lc.tuned),
+                  "tuned_ms_by_lanes": {m: {str(l): round(lc.tunedMs[i][k], 4) for k, l in enumerate((2, 4, 8, 16))}
+                                        for i, m in enumerate(("fluid", "collision"))}}
     ms = max_over_ranks(ms)
     cells_mean = 0.5 * (stats0.numCells + stats1.numCells)
     total_cells = sum_over_ranks(cells_mean)
@@ -628,6 +633,7 @@ def main():
             "step_roofline": {"bytes_per_cell": step_bytes_per_cell(bonds), "achieved_gbs": step_gbs,
                               "frac": step_gbs / peak, "note": "whole step, B_cell = 192 + 24b"},
             "same_workload_as_reference": same,
+            "launch_config": launch_cfg,
             "kernel_ms_per_step": {k: v / timed_steps for k, v in kernel_ms.items()},
             "step_ms": {"p50": step_p50, "p99": step_p99, "samples": len(step_samples),
                         "note": "single steps between CUDA events, after the timed region"},

@@ -52,6 +52,9 @@ int alien_b200_batch_time_timesteps(alien_b200_batch* batch, uint64_t timesteps,
 /* per-kernel timing as alien_b200_timed_timesteps, for all worlds */
 int alien_b200_batch_timed_timesteps(alien_b200_batch* batch, uint64_t timesteps, double* kernelMs, int maxKernels,
                                      int* numKernels);
+/* launch configuration of the batch's pair kernels (alien_b200_set_launch_config) */
+int alien_b200_batch_set_launch_config(alien_b200_batch* batch, const AlienLaunchConfig* config);
+int alien_b200_batch_get_launch_config(alien_b200_batch* batch, AlienLaunchConfig* config);
 
 #ifdef __cplusplus
 } /* extern "C" */

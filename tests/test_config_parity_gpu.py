@@ -79,8 +79,8 @@ def test_benchmark_world_one_step(name, timestep):
     data, world = config_world(name)
     prm = P.benchmark_parameters(CONFIGS[name][1])
     got, ref, _ = run_both(data, world, prm, 1, timestep)
-    errs = compare_cells(got.cells, ref.cells, world)
-    errs.update(compare_particles(got.particles, ref.particles, world))
+    errs = compare_cells(got.cells, ref.cells, world, before=data.cells)
+    errs.update(compare_particles(got.particles, ref.particles, world, before=data.particles))
     print(f"{name} t={timestep}: {len(got.cells)} cells, {len(got.particles)} particles, "
           + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
 
@@ -175,8 +175,8 @@ def test_radiation_emission(motion, steps):
         prm.radiationMinCellAge[c] = 50
     got, ref, _ = run_both(data, world, prm, steps, 0, precision="f64")
     assert len(ref.particles) > len(data.particles), "no radiation particle was emitted"
-    compare_cells(got.cells, ref.cells, world)
-    compare_particles(got.particles, ref.particles, world)
+    compare_cells(got.cells, ref.cells, world, before=data.cells)
+    compare_particles(got.particles, ref.particles, world, before=data.particles)
 
 
 @pytest.mark.parametrize("steps", [1, 4])
@@ -189,8 +189,8 @@ def test_particle_splitting(steps):
         prm.particleSplitEnergy[c] = 2.0
     got, ref, _ = run_both(data, world, prm, steps, 0, precision="f64")
     assert len(ref.particles) > len(data.particles), "no particle split"
-    compare_cells(got.cells, ref.cells, world)
-    compare_particles(got.particles, ref.particles, world)
+    compare_cells(got.cells, ref.cells, world, before=data.cells)
+    compare_particles(got.particles, ref.particles, world, before=data.particles)
 
 
 @pytest.mark.parametrize("motion", [P.MOTION_FLUID, P.MOTION_COLLISION])

@@ -41,8 +41,8 @@ def test_fluid_one_step(seed, timestep):
     data, world = worldgen.random_test_world(seed)
     prm = P.benchmark_parameters(P.MOTION_FLUID)
     got, ref = run_both(data, world, prm, 1, timestep)
-    compare_cells(got.cells, ref.cells, world)
-    compare_particles(got.particles, ref.particles, world)
+    compare_cells(got.cells, ref.cells, world, before=data.cells)
+    compare_particles(got.particles, ref.particles, world, before=data.particles)
 
 
 @pytest.mark.parametrize("seed", [4, 5, 6])
@@ -51,16 +51,16 @@ def test_collision_one_step(seed, timestep):
     data, world = worldgen.random_test_world(seed, vmax=0.9)
     prm = P.benchmark_parameters(P.MOTION_COLLISION)
     got, ref = run_both(data, world, prm, 1, timestep)
-    compare_cells(got.cells, ref.cells, world)
-    compare_particles(got.particles, ref.particles, world)
+    compare_cells(got.cells, ref.cells, world, before=data.cells)
+    compare_particles(got.particles, ref.particles, world, before=data.particles)
 
 
 def test_barriers_one_step():
     data, world = worldgen.random_test_world(7, barriers=20, free_cells=200)
     prm = P.benchmark_parameters(P.MOTION_FLUID)
     got, ref = run_both(data, world, prm, 1, 0)
-    compare_cells(got.cells, ref.cells, world)
-    compare_particles(got.particles, ref.particles, world)
+    compare_cells(got.cells, ref.cells, world, before=data.cells)
+    compare_particles(got.particles, ref.particles, world, before=data.particles)
 
 
 def test_structural_operations_one_step():
@@ -75,8 +75,8 @@ def test_structural_operations_one_step():
         prm.cellDeathProbability[i] = 0.5
         prm.cellMaxForce[i] = 0.05
     got, ref = run_both(data, world, prm, 1, 0)
-    compare_cells(got.cells, ref.cells, world)
-    compare_particles(got.particles, ref.particles, world)
+    compare_cells(got.cells, ref.cells, world, before=data.cells)
+    compare_particles(got.particles, ref.particles, world, before=data.particles)
 
 
 def test_cell_map_sets_bit_exact():
@@ -117,8 +117,8 @@ def test_world_too_small_for_regions(motion):
     data, world = worldgen.random_test_world(41, world=(7, 7), clusters=0, hex_clusters=0, free_cells=30,
                                              particles=5)
     got, ref = run_both(data, world, P.benchmark_parameters(motion), 1, 0)
-    compare_cells(got.cells, ref.cells, world)
-    compare_particles(got.particles, ref.particles, world)
+    compare_cells(got.cells, ref.cells, world, before=data.cells)
+    compare_particles(got.particles, ref.particles, world, before=data.particles)
 
 
 @pytest.mark.parametrize("motion", [P.MOTION_FLUID, P.MOTION_COLLISION])
@@ -127,5 +127,5 @@ def test_region_denser_than_shared_buffer(motion):
     data, world = worldgen.random_test_world(42, world=(16, 16), clusters=0, hex_clusters=0, free_cells=1500,
                                              particles=20, vmax=0.2)
     got, ref = run_both(data, world, P.benchmark_parameters(motion), 1, 1)
-    compare_cells(got.cells, ref.cells, world)
-    compare_particles(got.particles, ref.particles, world)
+    compare_cells(got.cells, ref.cells, world, before=data.cells)
+    compare_particles(got.particles, ref.particles, world, before=data.particles)
