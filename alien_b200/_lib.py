@@ -55,16 +55,18 @@ class RawStatistics(ctypes.Structure):
     ]
 
 
-PAIR_LANE_CHOICES = (2, 4, 8, 16)
+REGION_CHOICES = 4
 
 
 class LaunchConfig(ctypes.Structure):
     """AlienLaunchConfig (include/alien_b200.h)"""
     _fields_ = [
-        ("pairLanes", ctypes.c_int32 * 2),
-        ("pairLanesFixed", ctypes.c_int32 * 2),
+        ("regionTiles", (ctypes.c_int32 * 2) * 2),
+        ("regionChoice", ctypes.c_int32 * 2),
+        ("regionChoiceFixed", ctypes.c_int32 * 2),
         ("tuned", ctypes.c_int32),
-        ("tunedMs", (ctypes.c_float * len(PAIR_LANE_CHOICES)) * 2),
+        ("tunedMs", (ctypes.c_float * REGION_CHOICES) * 2),
+        ("candidates", ((ctypes.c_int32 * 2) * REGION_CHOICES) * 2),
     ]
 
 
@@ -84,7 +86,7 @@ EXPORTED_SYMBOLS = [
     "alien_b200_batch_set_step_budget", "alien_b200_batch_world_status", "alien_b200_batch_num_active",
     "alien_b200_batch_device_bytes", "alien_b200_statistics_no_alloc", "alien_b200_batch_synchronize",
     "alien_b200_debug_cell_map", "alien_b200_set_launch_config", "alien_b200_get_launch_config",
-    "alien_b200_choose_pair_lanes", "alien_b200_batch_set_launch_config", "alien_b200_batch_get_launch_config",
+    "alien_b200_choose_region", "alien_b200_batch_set_launch_config", "alien_b200_batch_get_launch_config",
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -148,8 +150,8 @@ def load() -> ctypes.CDLL:
     lib.alien_b200_get_launch_config.argtypes = [vp, P(LaunchConfig)]
     lib.alien_b200_batch_set_launch_config.argtypes = [vp, P(LaunchConfig)]
     lib.alien_b200_batch_get_launch_config.argtypes = [vp, P(LaunchConfig)]
-    lib.alien_b200_choose_pair_lanes.argtypes = [P(ctypes.c_float), i32]
-    lib.alien_b200_choose_pair_lanes.restype = i32
+    lib.alien_b200_choose_region.argtypes = [P(ctypes.c_float), i32]
+    lib.alien_b200_choose_region.restype = i32
     lib.alien_b200_select_device.argtypes = [i32]
     lib.alien_b200_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]
     lib.alien_b200_batch_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]

@@ -110,8 +110,10 @@ struct DevState {
 
     // cells
     unsigned long long* id;
-    float2* posA;     // position at step start / after Verlet
+    float2* posA;     // position at the start of the step (FP32 state between steps)
     float2* posB;     // position after the overlap push of the pair phase
+    float2* dpos;     // displacement since the step start: the overlap push, then plus the
+                      // Verlet increment; folded into posA by the next step's binning
     float2* velA;
     float2* velB;
     float* energy;
@@ -313,6 +315,24 @@ __device__ __forceinline__ float2 correctDirection(float2 d, int W, int H)
 }
 __device__ __forceinline__ int slotX(float x, int W) { return wrapInt(floorInt(x), W); }
 
+// b - a on a torus of the given size for coordinates in [0, size): the
+// minimal-image difference that BaseMap::correctDirection gives, computed
+// without rounding at the world's scale.  Across the seam the large
+// coordinate is brought down by the size first (x - size is exact for x in
+// [size/2, size)), so the result carries only the rounding of a small
+// difference, as for two cells away from the seam (where b - a is exact).
+__device__ __forceinline__ float seamDiff(float b, float a, float size)
+{
+    const float d = b - a;
+    if (d > 0.5f * size) return (b - size) - a;
+    if (d < -0.5f * size) return b - (a - size);
+    return d;
+}
+__device__ __forceinline__ float2 seamDiff2(float2 b, float2 a, int W, int H)
+{
+    return f2(seamDiff(b.x, a.x, static_cast<float>(W)), seamDiff(b.y, a.y, static_cast<float>(H)));
+}
+
 // counter-based draw: SplitMix64 finaliser (Steele, Lea & Flood, OOPSLA 2014)
 // of (timestep, site), xor the object id, finalised again; 24 high bits.
 __device__ __forceinline__ uint64_t splitmix64(uint64_t z)
@@ -397,5 +417,22 @@ __device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* tot
 }
 
 __device__ __forceinline__ void setError(const DevState& s, uint32_t bit) { atomicOr(s.errorFlags, bit); }
+
+// Positions within a step are the step-start position posA (exact FP32
+// state) plus the small displacement dpos accumulated by the step, so that
+// bond lengths and angles after the Verlet update are computed from exact
+// start differences and small increments instead of from positions rounded
+// at the world's scale (ulp 2.4e-4 at 4096).  The position a step produces
+// is rounded once, when the next step's binning (or an egress) folds dpos
+// into posA.
+__device__ __forceinline__ float2 stepPos(const DevState& s, long long g, int W, int H)
+{
+    return correctPosition(s.posA[g] + s.dpos[g], W, H);
+}
+// displacement from cell a to cell b at the step's current positions
+__device__ __forceinline__ float2 stepDisp(const DevState& s, long long a, long long b, int W, int H)
+{
+    return seamDiff2(s.posA[b], s.posA[a], W, H) + (s.dpos[b] - s.dpos[a]);
+}
 
 }  // namespace ab

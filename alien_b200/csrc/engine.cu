@@ -149,15 +149,6 @@ static void validateParams(const AlienPhysicsParams& p, int W, int H)
     if (W < 2 * r + 1 || H < 2 * r + 1) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "world smaller than the interaction window");
 }
 
-static int regionMaxW(int motion)
-{
-    return motion == ALIEN_B200_MOTION_FLUID ? RegionShape<ALIEN_B200_MOTION_FLUID>::W : RegionShape<ALIEN_B200_MOTION_COLLISION>::W;
-}
-static int regionMaxH(int motion)
-{
-    return motion == ALIEN_B200_MOTION_FLUID ? RegionShape<ALIEN_B200_MOTION_FLUID>::H : RegionShape<ALIEN_B200_MOTION_COLLISION>::H;
-}
-
 static int scanRadius(const AlienPhysicsParams& p)
 {
     return std::max(1, p.motionType == ALIEN_B200_MOTION_FLUID ? static_cast<int>(ceilf(p.smoothingLength * 2.0f))
@@ -214,9 +205,10 @@ public:
     // the cell map of the current state, built by the step's own binning
     // kernels and read back in tile order (alien_b200_debug_cell_map)
     uint64_t cellMap(uint64_t capacity, uint64_t* ids, uint32_t* slots, uint32_t* tiles, uint8_t* flags);
-    // launch configuration of the pair kernel: lanes per cell per motion
-    // type, fixed by the caller (nonzero) or chosen by the autotuner
-    void setPairLanes(int motion, int lanes);
+    // launch configuration of the pair kernel: region shape per motion
+    // type, fixed by the caller (candidate index + 1) or chosen by the
+    // autotuner (0)
+    void setRegionChoice(int motion, int choicePlusOne);
     AlienLaunchConfig launchConfig() const;
     void autotune();
 
@@ -259,20 +251,18 @@ public:
 
 private:
     void scan(const uint32_t* in, long long n, uint32_t* out);
-    // the pair kernel of one motion type with `lanes` lanes per cell
+    // pair-kernel region shapes: the candidates' index in use per motion type,
+    // fixed by the caller (index + 1) or chosen by the autotuner
+    int regionChoice_[2] = {0, 0};
+    int regionChoiceFixed_[2] = {0, 0};
+    const int* regionShape(int motion) const { return kRegionChoices[motion][regionChoice_[motion]]; }
+    static void assignRegions(WorldInfo& wi, const int* shape);
+    static int maxRegions(const WorldInfo& wi);
+    void applyRegionShapes();
     template <int Motion>
-    void launchPairs(int lanes)
+    void launchPairs()
     {
-        const DevState& s = s_;
-        constexpr size_t smem = regionDynSmem<Motion>();
-        const char* name = Motion == ALIEN_B200_MOTION_FLUID ? "kPairsRegion<FLUID>" : "kPairsRegion<COLLISION>";
-        switch (lanes) {
-        case 2: launchNamedSmem(name, kPairsRegion<Motion, 2>, s.numRegions, kRegionThreads, smem, s); break;
-        case 4: launchNamedSmem(name, kPairsRegion<Motion, 4>, s.numRegions, kRegionThreads, smem, s); break;
-        case 8: launchNamedSmem(name, kPairsRegion<Motion, 8>, s.numRegions, kRegionThreads, smem, s); break;
-        case 16: launchNamedSmem(name, kPairsRegion<Motion, 16>, s.numRegions, kRegionThreads, smem, s); break;
-        default: throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "lanes per cell must be 2, 4, 8 or 16");
-        }
+        launchSmem(kPairsRegion<Motion>, s_.numRegions, kRegionThreads, regionDynSmem<Motion>(), s_);
     }
     void releaseGraph()
     {
@@ -301,10 +291,8 @@ private:
     cudaGraphExec_t graphExec_ = nullptr;
     uint64_t stepsSinceCheck_ = 0;
     bool hasFluid_ = false, hasCollision_ = false, hasNeurons_ = false;
-    int pairLanes_[2] = {kDefaultPairLanes, kDefaultPairLanes};  // lanes per cell of the pair kernel, per motion type
-    int pairLanesFixed_[2] = {0, 0};  // set by the caller: not tuned
     bool tuned_ = false;              // the autotuner ran on this layout
-    float tunedMs_[2][kNumPairLaneChoices] = {};
+    float tunedMs_[2][kNumRegionChoices] = {};
     void binCurrentState();
     bool signalsLive_ = false;  // some cell has a function or a nonzero signal channel
 };
@@ -430,10 +418,10 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     worlds_.clear();
     tuned_ = false;  // a new layout is tuned again at its first step
     std::memset(tunedMs_, 0, sizeof(tunedMs_));
-    for (int m = 0; m < 2; ++m) pairLanes_[m] = pairLanesFixed_[m] ? pairLanesFixed_[m] : kDefaultPairLanes;
+    for (int m = 0; m < 2; ++m) regionChoice_[m] = regionChoiceFixed_[m] ? regionChoiceFixed_[m] - 1 : 0;
     const int n = static_cast<int>(setups.size());
     long long cellSlots = 0, partSlots = 0, tiles = 0, pmapSlots = 0, coldTotal = 0, auxTotal = 0;
-    int regions = 0;
+    int regions = 0, regionsCap = 0;  // regions of the current shapes; most regions any candidate shape gives
     int cellBlocks = 0, partBlocks = 0;
     maxWorldCells_ = maxWorldParts_ = 0;
     for (int w = 0; w < n; ++w) {
@@ -465,20 +453,8 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         wi.firstPartBlock = partBlocks;
         wi.numPartBlocks = static_cast<int>(wi.partCap / kBlock);
         wi.pmapBase = pmapSlots;
-        // pair-phase regions (RegionShape) with a one-tile halo that never
-        // overlaps the region itself and lies within half a world (so that a
-        // seam shift gives the minimal image)
-        if (wi.nTX >= 4 && wi.nTY >= 4 && ws.W >= 4 * wi.T && ws.H >= 4 * wi.T) {
-            wi.regW = std::min(regionMaxW(wi.motionType), wi.nTX - 2);
-            wi.regH = std::min(regionMaxH(wi.motionType), wi.nTY - 2);
-            wi.regionShared = 1;
-        } else {
-            wi.regW = std::min(regionMaxW(wi.motionType), wi.nTX);
-            wi.regH = std::min(regionMaxH(wi.motionType), wi.nTY);
-            wi.regionShared = 0;
-        }
-        wi.nRX = divUp(wi.nTX, wi.regW);
-        wi.nRY = divUp(wi.nTY, wi.regH);
+        assignRegions(wi, regionShape(wi.motionType));
+        regionsCap += maxRegions(wi);
         wi.regionBase = regions;
         regions += wi.nRX * wi.nRY;
         pmapSlots += static_cast<long long>(ws.W) * ws.H;
@@ -506,9 +482,12 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     if (cellSlots >= (1ll << 31) || partSlots >= (1ll << 31) || tiles >= (1ll << 32) - 2)
         throw Error(ALIEN_B200_ERR_CAPACITY, "arena exceeds 2^31 slots");
 
-    static_assert(regionDynSmem<ALIEN_B200_MOTION_FLUID>() <= 48 * 1024
-                      && regionDynSmem<ALIEN_B200_MOTION_COLLISION>() <= 48 * 1024,
-                  "pair regions fit the default dynamic shared-memory limit");
+    // the pair-phase regions stage up to RegionShape<>::Cap records in dynamic
+    // shared memory (above the 48 KB default)
+    AB_CK(cudaFuncSetAttribute(kPairsRegion<ALIEN_B200_MOTION_FLUID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(regionDynSmem<ALIEN_B200_MOTION_FLUID>())));
+    AB_CK(cudaFuncSetAttribute(kPairsRegion<ALIEN_B200_MOTION_COLLISION>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(regionDynSmem<ALIEN_B200_MOTION_COLLISION>())));
     DevState& s = s_;
     s = DevState{};
     s.numWorlds = n;
@@ -534,7 +513,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     s.counters = mem_.alloc<WorldCounters>(n);
     auto* paramsDev = mem_.alloc<AlienPhysicsParams>(n);
     s.params = paramsDev;
-    auto* rgw = mem_.alloc<int>(regions);
+    auto* rgw = mem_.alloc<int>(regionsCap);
     s.regionWorld = rgw;
     s.numRegions = regions;
     auto* cbw = mem_.alloc<int>(cellBlocks);
@@ -546,6 +525,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     s.id = mem_.alloc<unsigned long long>(C);
     s.posA = mem_.alloc<float2>(C);
     s.posB = mem_.alloc<float2>(C);
+    s.dpos = mem_.alloc<float2>(C);
     s.velA = mem_.alloc<float2>(C);
     s.velB = mem_.alloc<float2>(C);
     s.energy = mem_.alloc<float>(C);
@@ -674,6 +654,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     AB_CK(cudaMemsetAsync(s.pmap, 0xff, static_cast<size_t>(pmapSlots) * sizeof(int), stream_));
     AB_CK(cudaMemsetAsync(s.flags, 0, C * sizeof(uint32_t), stream_));
     AB_CK(cudaMemsetAsync(s.angleAcc, 0, C * 4 * sizeof(long long), stream_));
+    AB_CK(cudaMemsetAsync(s.dpos, 0, C * sizeof(float2), stream_));
     AB_CK(cudaMemsetAsync(s.energyAcc, 0, C * sizeof(long long), stream_));
     AB_CK(cudaMemsetAsync(s.newPartner, 0xff, C * sizeof(int), stream_));
     AB_CK(cudaMemsetAsync(s.best, 0xff, C * sizeof(int), stream_));
@@ -721,8 +702,8 @@ void Arena::enqueueStep()
     scan(s.tileCount, s.numTiles, s.tileStart);
     launch(kScatter, cells, kBlock, s);
     launch(kStage, cells, kBlock, s);
-    if (hasFluid_) launchPairs<ALIEN_B200_MOTION_FLUID>(pairLanes_[ALIEN_B200_MOTION_FLUID]);
-    if (hasCollision_) launchPairs<ALIEN_B200_MOTION_COLLISION>(pairLanes_[ALIEN_B200_MOTION_COLLISION]);
+    if (hasFluid_) launchPairs<ALIEN_B200_MOTION_FLUID>();
+    if (hasCollision_) launchPairs<ALIEN_B200_MOTION_COLLISION>();
     launch(kPairsOverflow, overflowGrid_, kBlock, s);
     launch(kApplyBond1, both, kBlock, s);
     launch(kVerletPos, both, kBlock, s);
@@ -1087,15 +1068,83 @@ void Arena::binCurrentState()
     launch(kStage, s.numCellBlocks, kBlock, s);
 }
 
-void Arena::setPairLanes(int motion, int lanes)
+// Region shape of a world for the pair kernel: regW x regH tiles (the
+// shape, clamped to the world) with a one-tile halo that never overlaps the
+// region itself and lies within half a world (so that a seam shift gives
+// the minimal image); worlds too small for that take the global path.
+void Arena::assignRegions(WorldInfo& wi, const int* shape)
+{
+    if (wi.nTX >= 4 && wi.nTY >= 4 && wi.W >= 4 * wi.T && wi.H >= 4 * wi.T) {
+        wi.regW = std::min(shape[0], wi.nTX - 2);
+        wi.regH = std::min(shape[1], wi.nTY - 2);
+        wi.regionShared = 1;
+    } else {
+        wi.regW = std::min(shape[0], wi.nTX);
+        wi.regH = std::min(shape[1], wi.nTY);
+        wi.regionShared = 0;
+    }
+    if (wi.regionShared && wi.motionType == ALIEN_B200_MOTION_FLUID) {
+        // the region at the right (top) seam shifts its tiles down by the
+        // world size, which is exact when its halo starts in the world's
+        // upper half: narrower regions where a world is only a few regions
+        // wide (regW = 1 always satisfies it, as nTX >= 4)
+        auto exact = [&](int reg, int nT, int size) {
+            const int last = (divUp(nT, reg) - 1) * reg;
+            return last >= 1 && 2ll * (last - 1) * wi.T >= size;
+        };
+        while (wi.regW > 1 && !exact(wi.regW, wi.nTX, wi.W)) --wi.regW;
+        while (wi.regH > 1 && !exact(wi.regH, wi.nTY, wi.H)) --wi.regH;
+    }
+    wi.nRX = divUp(wi.nTX, wi.regW);
+    wi.nRY = divUp(wi.nTY, wi.regH);
+}
+
+int Arena::maxRegions(const WorldInfo& wi)
+{
+    int most = 0;
+    for (int i = 0; i < kNumRegionChoices; ++i) {
+        WorldInfo t = wi;
+        assignRegions(t, kRegionChoices[wi.motionType][i]);
+        most = std::max(most, t.nRX * t.nRY);
+    }
+    return most;
+}
+
+// region tables of the shapes in use: every world's regions, regionBase and
+// the world of each region, uploaded on the arena's stream
+void Arena::applyRegionShapes()
+{
+    std::vector<WorldInfo> infos(worlds_.size());
+    std::vector<int> rgw;
+    for (size_t w = 0; w < worlds_.size(); ++w) {
+        WorldInfo& wi = worlds_[w].info;
+        assignRegions(wi, regionShape(wi.motionType));
+        wi.regionBase = static_cast<int>(rgw.size());
+        rgw.insert(rgw.end(), static_cast<size_t>(wi.nRX) * wi.nRY, static_cast<int>(w));
+        infos[w] = wi;
+    }
+    s_.numRegions = static_cast<int>(rgw.size());
+    if (!infos.empty())
+        AB_CK(cudaMemcpyAsync(const_cast<WorldInfo*>(s_.worlds), infos.data(), sizeof(WorldInfo) * infos.size(),
+                              cudaMemcpyHostToDevice, stream_));
+    if (!rgw.empty())
+        AB_CK(cudaMemcpyAsync(const_cast<int*>(s_.regionWorld), rgw.data(), sizeof(int) * rgw.size(), cudaMemcpyHostToDevice,
+                              stream_));
+    AB_CK(cudaStreamSynchronize(stream_));  // the host tables are temporaries
+    releaseGraph();
+}
+
+void Arena::setRegionChoice(int motion, int choicePlusOne)
 {
     if (motion != ALIEN_B200_MOTION_FLUID && motion != ALIEN_B200_MOTION_COLLISION)
         throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "motion type must be 0 (fluid) or 1 (collision)");
-    if (lanes != 0 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16)
-        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "lanes per cell must be 0 (autotune), 2, 4, 8 or 16");
-    pairLanesFixed_[motion] = lanes;
-    if (lanes) pairLanes_[motion] = lanes;
-    releaseGraph();
+    if (choicePlusOne < 0 || choicePlusOne > kNumRegionChoices)
+        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "region choice must be 0 (autotune) or 1.." + std::to_string(kNumRegionChoices));
+    regionChoiceFixed_[motion] = choicePlusOne;
+    if (choicePlusOne && regionChoice_[motion] != choicePlusOne - 1) {
+        regionChoice_[motion] = choicePlusOne - 1;
+        if (!worlds_.empty()) applyRegionShapes();
+    }
 }
 
 AlienLaunchConfig Arena::launchConfig() const
@@ -1103,27 +1152,33 @@ AlienLaunchConfig Arena::launchConfig() const
     AlienLaunchConfig c;
     std::memset(&c, 0, sizeof(c));
     for (int m = 0; m < 2; ++m) {
-        c.pairLanes[m] = pairLanes_[m];
-        c.pairLanesFixed[m] = pairLanesFixed_[m];
-        for (int i = 0; i < kNumPairLaneChoices; ++i) c.tunedMs[m][i] = tunedMs_[m][i];
+        c.regionTiles[m][0] = regionShape(m)[0];
+        c.regionTiles[m][1] = regionShape(m)[1];
+        c.regionChoice[m] = regionChoice_[m];
+        c.regionChoiceFixed[m] = regionChoiceFixed_[m];
+        for (int i = 0; i < kNumRegionChoices; ++i) {
+            c.tunedMs[m][i] = tunedMs_[m][i];
+            c.candidates[m][i][0] = kRegionChoices[m][i][0];
+            c.candidates[m][i][1] = kRegionChoices[m][i][1];
+        }
     }
     c.tuned = tuned_ ? 1 : 0;
     return c;
 }
 
-// The autotuner: for every motion type present whose lanes per cell the
+// The autotuner: for every motion type present whose region shape the
 // caller did not fix, the pair kernel of the current state is launched with
-// each lane count (one untimed launch, then three between CUDA events) and
-// the fastest is kept (alien_b200_choose_pair_lanes).  The pair kernel reads
+// each candidate shape (one untimed launch, then three between CUDA events)
+// and the fastest is kept (alien_b200_choose_region).  The pair kernel reads
 // only the staged records and overwrites its own outputs, which the next
-// step recomputes, and its results do not depend on the lane count (fixed-
-// point sums), so tuning changes neither the state nor any result.  Runs
-// once per arena layout, before the step graph is captured.
+// step recomputes, and a cell's neighbours are visited in the same order
+// whatever the region shape, so tuning changes neither the state nor any
+// result.  Runs once per arena layout, before the step graph is captured.
 void Arena::autotune()
 {
     tuned_ = true;
-    const bool need[2] = {hasFluid_ && !pairLanesFixed_[ALIEN_B200_MOTION_FLUID],
-                          hasCollision_ && !pairLanesFixed_[ALIEN_B200_MOTION_COLLISION]};
+    const bool need[2] = {hasFluid_ && !regionChoiceFixed_[ALIEN_B200_MOTION_FLUID],
+                          hasCollision_ && !regionChoiceFixed_[ALIEN_B200_MOTION_COLLISION]};
     if (!need[0] && !need[1]) return;
     std::vector<WorldCounters> c = readCounters();
     long long cells = 0;
@@ -1135,16 +1190,17 @@ void Arena::autotune()
     try {
         for (int m = 0; m < 2; ++m) {
             if (!need[m]) continue;
-            for (int i = 0; i < kNumPairLaneChoices; ++i) {
-                const int lanes = kPairLaneChoices[i];
+            for (int i = 0; i < kNumRegionChoices; ++i) {
+                regionChoice_[m] = i;
+                applyRegionShapes();
                 for (int rep = 0; rep < 4; ++rep) {
                     // deferred cells are listed again by every launch
                     AB_CK(cudaMemsetAsync(s_.pairOverflowCount, 0, sizeof(uint32_t), stream_));
                     if (rep > 0) AB_CK(cudaEventRecord(ev[rep], stream_));
                     if (m == ALIEN_B200_MOTION_FLUID)
-                        launchPairs<ALIEN_B200_MOTION_FLUID>(lanes);
+                        launchPairs<ALIEN_B200_MOTION_FLUID>();
                     else
-                        launchPairs<ALIEN_B200_MOTION_COLLISION>(lanes);
+                        launchPairs<ALIEN_B200_MOTION_COLLISION>();
                     if (rep > 0) {
                         AB_CK(cudaEventRecord(ev[0], stream_));
                         AB_CK(cudaEventSynchronize(ev[0]));
@@ -1154,14 +1210,14 @@ void Arena::autotune()
                     }
                 }
             }
-            pairLanes_[m] = alien_b200_choose_pair_lanes(tunedMs_[m], kNumPairLaneChoices);
+            regionChoice_[m] = alien_b200_choose_region(tunedMs_[m], kNumRegionChoices);
         }
     } catch (...) {
         for (cudaEvent_t& e : ev) cudaEventDestroy(e);
         throw;
     }
     for (cudaEvent_t& e : ev) cudaEventDestroy(e);
-    releaseGraph();
+    applyRegionShapes();
 }
 
 uint64_t Arena::cellMap(uint64_t capacity, uint64_t* ids, uint32_t* slots, uint32_t* tiles, uint8_t* flags)
@@ -1567,24 +1623,24 @@ int alien_b200_debug_cell_map(alien_b200_simulation* sim, uint64_t capacity, uin
     });
 }
 
-int alien_b200_choose_pair_lanes(const float* milliseconds, int n)
+int alien_b200_choose_region(const float* milliseconds, int n)
 {
-    // the fastest lane count; a larger count must beat the best smaller one
-    // by more than 2 % (timing noise must not flip the choice between
-    // nearly equal configurations)
+    // the fastest candidate; a later one must beat the best earlier one by
+    // more than 2 % (timing noise must not flip the choice between nearly
+    // equal shapes, and the first candidate is the default)
     int best = -1;
-    for (int i = 0; i < n && i < kNumPairLaneChoices; ++i) {
+    for (int i = 0; i < n && i < kNumRegionChoices; ++i) {
         if (!(milliseconds[i] > 0.0f)) continue;
         if (best < 0 || milliseconds[i] < 0.98f * milliseconds[best]) best = i;
     }
-    return best < 0 ? kDefaultPairLanes : kPairLaneChoices[best];
+    return best < 0 ? 0 : best;
 }
 
 int alien_b200_set_launch_config(alien_b200_simulation* sim, const AlienLaunchConfig* config)
 {
     return guarded([&] {
         if (!sim || !config) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
-        for (int m = 0; m < 2; ++m) sim->arena->setPairLanes(m, config->pairLanesFixed[m]);
+        for (int m = 0; m < 2; ++m) sim->arena->setRegionChoice(m, config->regionChoiceFixed[m]);
     });
 }
 
@@ -1601,7 +1657,7 @@ int alien_b200_batch_set_launch_config(alien_b200_batch* b, const AlienLaunchCon
 {
     return guarded([&] {
         if (!b || !config) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
-        for (int m = 0; m < 2; ++m) b->arena->setPairLanes(m, config->pairLanesFixed[m]);
+        for (int m = 0; m < 2; ++m) b->arena->setRegionChoice(m, config->regionChoiceFixed[m]);
     });
 }
 

@@ -74,6 +74,7 @@ __global__ void __launch_bounds__(kBlock) kIngestCells(DevState s, int w, const 
     s.coldIdx[g] = static_cast<uint32_t>(coldBase + i);
     s.id[g] = c.id;
     s.posA[g] = correctPosition(f2(c.pos.x, c.pos.y), wi.W, wi.H);
+    s.dpos[g] = f2(0.0f, 0.0f);
     s.velA[g] = f2(c.vel.x, c.vel.y);
     s.energy[g] = c.energy;
     s.stiffness[g] = c.stiffness;
@@ -153,7 +154,7 @@ __global__ void __launch_bounds__(kBlock) kSelectCells(DevState s, int w, int us
     const long long g = wi.cellBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
     uint32_t v = 0;
     if (g < wi.cellBase + s.counters[w].numCells && s.alive[g])
-        v = (!useRect || inRect(s.posA[g], ulx, uly, lrx, lry)) ? 1u : 0u;
+        v = (!useRect || inRect(stepPos(s, g, wi.W, wi.H), ulx, uly, lrx, lry)) ? 1u : 0u;
     uint32_t total;
     const uint32_t ex = blockExclusiveScan(v, &total);
     rank[g] = v ? static_cast<int>(ex) : -1;
@@ -190,7 +191,7 @@ __global__ void __launch_bounds__(kBlock) kEgressCells(DevState s, int w, const 
     if (r < 0) return;
     AlienCellTO c = cold[s.coldIdx[g]];
     c.id = s.id[g];
-    const float2 p = s.posA[g], v = s.velA[g];
+    const float2 p = stepPos(s, g, wi.W, wi.H), v = s.velA[g];
     c.pos.x = p.x;
     c.pos.y = p.y;
     c.vel.x = v.x;

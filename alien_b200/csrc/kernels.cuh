@@ -148,6 +148,18 @@ __device__ __forceinline__ void forEachWindowTile(const WorldInfo& wi, int sx, i
     }
 }
 
+// the previous step's position of the cell: its start position plus the
+// displacement the step accumulated, rounded once (the FP32 state the
+// reference keeps in Cell::pos)
+__device__ __forceinline__ float2 foldDisplacement(const DevState& s, const WorldInfo& wi, long long g, float2 pos, float2 d)
+{
+    if (d.x == 0.0f && d.y == 0.0f) return pos;
+    pos = correctPosition(pos + d, wi.W, wi.H);
+    s.posA[g] = pos;
+    s.dpos[g] = f2(0.0f, 0.0f);
+    return pos;
+}
+
 // the cell's slot and tile at binning, and its arrival rank in the tile
 __device__ __forceinline__ void binCell(const DevState& s, const WorldInfo& wi, long long g, float2 pos)
 {
@@ -172,13 +184,15 @@ __global__ void __launch_bounds__(kBlock, 8) kBin(DevState s)
         // kernels that consume them, and best is written for every live cell
         // own fields before the world lookup (every launched cell slot lies
         // inside the arena)
-        const float2 pos = s.posA[static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x];
+        float2 pos = s.posA[static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x];
+        const float2 d = s.dpos[static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x];
         const bool barrierG = s.barrier[static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x];
         CellCtx c = cellCtx(s);
         const long long g = c.g;
         if (!c.valid) return;
         const WorldInfo& wi = s.worlds[c.w];
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
+        pos = foldDisplacement(s, wi, g, pos, d);
         binCell(s, wi, g, pos);
 
         if (barrierG || !(p.radiationProb > 0.0f)) return;  // a draw in [0, 1) never falls below 0
@@ -366,9 +380,11 @@ __global__ void __launch_bounds__(kBlock) kStage(DevState s)
 __global__ void __launch_bounds__(kBlock) kBinMap(DevState s)
 {
     const float2 pos = s.posA[static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x];
+    const float2 d = s.dpos[static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x];
     CellCtx c = cellCtx(s);
     if (!c.valid) return;
-    binCell(s, s.worlds[c.w], c.g, pos);
+    const WorldInfo& wi = s.worlds[c.w];
+    binCell(s, wi, c.g, foldDisplacement(s, wi, c.g, pos, d));
 }
 
 // the staged records in tile order: id, slot, tile (relative to the world's
@@ -388,76 +404,20 @@ __global__ void __launch_bounds__(kBlock) kExportCellMap(DevState s, unsigned lo
 }
 
 // ---------------------------------------------------------- pair laws ----
-// The pair phase of the two motion types as accumulators: beginScan() and
-// beginLaw() with the cell's staged record, near() as a cheap reject on the
-// squared distance, relevant() for candidates whose visit can change
-// something, visit() for the survivors, reduce() across the lanes that
-// shared the cell's candidates, end() writes the cell's results.
-//
-// Every sum is a 2^-32 fixed-point integer (toFix of each FP32 term) and
-// every choice is a minimum over a total order (smallest id, nearest
-// barrier then smallest slot), so a cell's results do not depend on the
-// order in which its candidates are visited nor on how they are split
-// across lanes: the tile size, the region shape and the lanes per cell are
-// free launch parameters, and the results are bit-identical run to run,
-// between launch configurations and between a world alone and in a batch.
-// Two enumerations feed the laws: kPairsRegion (shared-memory regions, the
-// fast path) and pairsGlobal (tile lists in global memory, for regions that
-// do not fit).
+// The pair phase of the two motion types as accumulators: begin() with the
+// cell's staged record, near() as a cheap reject on the squared distance,
+// visit() for the survivors, end() writes the cell's results.  Neighbours
+// are visited tile by tile (3x3 tiles around the cell, in row order) and,
+// within a tile, in storage order, so the FP32 sums are reproducible run to
+// run and identical alone or in a batch.  Two enumerations feed the laws:
+// kPairsRegion (shared-memory regions, the fast path) and pairsGlobal (tile
+// lists in global memory, for regions that do not fit).
 
 // sqrtf(q) <= R decided exactly (the reject bound is above R^2)
 __device__ __forceinline__ bool withinRadius(float q, float R, float& d)
 {
     d = sqrtf(q);
     return d <= R;
-}
-
-// LPC consecutive lanes of a warp that share one cell's candidates
-template <int LPC>
-struct LaneGroup {
-    static_assert(LPC >= 1 && LPC <= 32 && (LPC & (LPC - 1)) == 0, "lanes per cell: a power of two");
-    unsigned mask;
-    int lane;
-    __device__ __forceinline__ LaneGroup()
-    {
-        const int wl = threadIdx.x & 31;
-        lane = wl & (LPC - 1);
-        mask = LPC == 32 ? 0xffffffffu : (((1u << (LPC & 31)) - 1u) << (wl & ~(LPC - 1)));
-    }
-    __device__ __forceinline__ long long sum(long long v) const
-    {
-#pragma unroll
-        for (int o = LPC / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, LPC);
-        return v;
-    }
-    __device__ __forceinline__ bool any(bool p) const { return LPC == 1 ? p : __any_sync(mask, p); }
-    // (key, idx) of the lane with the smallest key, ties to the smallest idx
-    template <class K>
-    __device__ __forceinline__ void argmin(K& key, int& idx) const
-    {
-#pragma unroll
-        for (int o = LPC / 2; o > 0; o >>= 1) {
-            const K k2 = __shfl_xor_sync(mask, key, o, LPC);
-            const int i2 = __shfl_xor_sync(mask, idx, o, LPC);
-            if (k2 < key || (k2 == key && i2 < idx)) {
-                key = k2;
-                idx = i2;
-            }
-        }
-    }
-};
-
-// the cell's bond partners (slot indices, unused entries -1): three 8-byte
-// loads of the bond row
-__device__ __forceinline__ void loadBondPartners(const DevState& st, long long g, int n, int* bonds)
-{
-    const int2* row = reinterpret_cast<const int2*>(st.bond + g * kMaxBonds);
-#pragma unroll
-    for (int h = 0; h < kMaxBonds / 2; ++h) {
-        const int2 b = 2 * h < n ? row[h] : make_int2(-1, -1);
-        bonds[2 * h] = b.x;
-        bonds[2 * h + 1] = 2 * h + 1 < n ? b.y : -1;
-    }
 }
 
 // CellProcessor::calcFluidForces_reconnectCells_correctOverlap,
@@ -469,14 +429,16 @@ struct FluidLaw {
     float h, invH, invH2, invH3, R, R2reject, minDist, fusionVelocity, maxBindingEnergy;
     float2 pi, vi;
     bool barrierI, fusionI;
-    float invDensI;
+    float densI, invDensI;
     int bondsI[kMaxBonds];
-    long long dens, fpx, fpy, fvx, fvy, dxx, dxy;  // fixed-point sums
-    int bestBarrier;          // nearest barrier cell (slot), -1 = none
+    float dens;
+    float2 Fp, Fv, dx;
+    int bestBarrier;
     float bestBarrierDist;
-    int best;                 // fusion choice: partner with the smallest id
+    int best;
     unsigned long long bestId;
 
+    // the state near() and relevant() need (the scan), then the rest (the law)
     __device__ __forceinline__ void beginScan(const DevState& st, const WorldInfo& wi, int4 me)
     {
         s = &st;
@@ -502,14 +464,23 @@ struct FluidLaw {
         vi = vel;
         barrierI = me.y & kStageBarrier;
         const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
-        invDensI = __frcp_rn(__int_as_float(me.z));
+        densI = __int_as_float(me.z);
+        invDensI = __frcp_rn(densI);
         fusionI = !barrierI && nI < maxI && __int_as_float(me.w) <= maxBindingEnergy;
-        loadBondPartners(st, g, nI, bondsI);
-        dens = fpx = fpy = fvx = fvy = dxx = dxy = 0;
+#pragma unroll
+        for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? st.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
+        dens = 0.0f;
+        Fp = Fv = dx = f2(0.0f, 0.0f);
         bestBarrier = -1;
         bestBarrierDist = 0.0f;
         best = -1;
         bestId = ~0ull;
+    }
+
+    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float2 pos, float2 vel)
+    {
+        beginScan(st, wi, me);
+        beginLaw(wi, me, pos, vel);
     }
 
     __device__ __forceinline__ bool near(float2 pd) const { return pd.x * pd.x + pd.y * pd.y <= R2reject; }
@@ -530,12 +501,9 @@ struct FluidLaw {
             return;
         }
         const float q = d * invH;
-        dens += toFix(sphKernel(q) * invH2);
+        dens += sphKernel(q) * invH2;
         if (j == g) return;
-        if (!barrierI && d < minDist) {
-            dxx += toFix(pd.x * (minDist / 5.0f));
-            dxy += toFix(pd.y * (minDist / 5.0f));
-        }
+        if (!barrierI && d < minDist) dx = dx + pd * (minDist / 5.0f);
         if (isBondedTo(bondsI, j)) return;
         const float2 vd = vi - vj;
         // rho_i / rho_i^2 + rho_j / rho_j^2 (CellProcessor.cuh:205) as reciprocals
@@ -543,12 +511,8 @@ struct FluidLaw {
         const float factor = invDensI + invDensJ;
         if (fabsf(d) > kNearZero) {
             const float kd = sphKernelD(q) * invH3;
-            const float cp = -factor * kd * __frcp_rn(d);
-            const float cv = invDensJ * d * kd * __frcp_rn(d * d + 0.25f);
-            fpx += toFix(pd.x * cp);
-            fpy += toFix(pd.y * cp);
-            fvx += toFix(vd.x * cv);
-            fvy += toFix(vd.y * cv);
+            Fp = Fp + pd * (-factor * kd * __frcp_rn(d));
+            Fv = Fv + vd * (invDensJ * d * kd * __frcp_rn(d * d + 0.25f));
         }
         if (fusionI && len2(vd) >= fusionVelocity) {
             const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
@@ -562,33 +526,6 @@ struct FluidLaw {
         }
     }
 
-    template <int LPC>
-    __device__ __forceinline__ void reduce(const LaneGroup<LPC>& grp)
-    {
-        if (LPC == 1) return;
-        dens = grp.sum(dens);
-        if (grp.any((fpx | fpy | fvx | fvy | dxx | dxy) != 0)) {
-            fpx = grp.sum(fpx);
-            fpy = grp.sum(fpy);
-            fvx = grp.sum(fvx);
-            fvy = grp.sum(fvy);
-            dxx = grp.sum(dxx);
-            dxy = grp.sum(dxy);
-        }
-        if (grp.any(best >= 0)) {
-            int idx = best;
-            grp.argmin(bestId, idx);
-            best = idx;
-        }
-        if (grp.any(bestBarrier >= 0)) {
-            float key = bestBarrier >= 0 ? bestBarrierDist : __int_as_float(0x7f800000);
-            int idx = bestBarrier >= 0 ? bestBarrier : 0x7fffffff;
-            grp.argmin(key, idx);
-            bestBarrier = idx == 0x7fffffff ? -1 : idx;
-            bestBarrierDist = key;
-        }
-    }
-
     __device__ __forceinline__ void end()
     {
         const DevState& st = *s;
@@ -599,13 +536,13 @@ struct FluidLaw {
             float2 rr = f2(0.0f, 0.0f);
             const int nb = st.numConn[b];
             if (nb <= 1) {
-                rr = correctDirection(pi - pb, W, H);
+                rr = seamDiff2(pi, pb, W, H);
             } else {
-                const float angleToCell = angleOfVector(correctDirection(pi - pb, W, H));
+                const float angleToCell = angleOfVector(seamDiff2(pi, pb, W, H));
                 for (int m = 0; m < nb; ++m) {
                     const int c1 = st.bond[b * kMaxBonds + m], c2 = st.bond[b * kMaxBonds + (m + 1) % nb];
-                    const float a1 = angleOfVector(correctDirection(st.posA[c1] - pb, W, H));
-                    const float a2 = angleOfVector(correctDirection(st.posA[c2] - pb, W, H));
+                    const float a1 = angleOfVector(seamDiff2(st.posA[c1], pb, W, H));
+                    const float a2 = angleOfVector(seamDiff2(st.posA[c2], pb, W, H));
                     if (isAngleInBetween(a1, a2, angleToCell)) {
                         rr = rotCCW(st.posA[c2] - st.posA[c1]);
                         break;
@@ -624,11 +561,11 @@ struct FluidLaw {
                 F = rr * (-2.0f * dvr / trr) / td;
             }
         }
-        const float2 Fp = f2(fromFix(fpx), fromFix(fpy)), Fv = f2(fromFix(fvx), fromFix(fvy));
         F = F + (Fp * p->pressureStrength + Fv * p->viscosityStrength);
         st.force[g] = F;
-        st.posB[g] = pi + f2(fromFix(dxx), fromFix(dxy));
-        st.densNew[g] = fromFix(dens);
+        st.posB[g] = pi + dx;
+        st.dpos[g] = dx;
+        st.densNew[g] = dens;
         st.best[g] = best;
     }
 };
@@ -663,7 +600,7 @@ struct CollisionLaw {
     bool barrierI, visibleI, fusionI;
     float densI;
     int bondsI[kMaxBonds];
-    long long fx, fy, dxx, dxy;  // fixed-point sums
+    float2 F, dx;
     int best;
     unsigned long long bestId;
 
@@ -678,7 +615,9 @@ struct CollisionLaw {
         minDist = p->cellMinDistance;
         minDist2Keep = minDist * minDist * 1.0001f + 1e-6f;
         barrierI = me.y & kStageBarrier;
-        loadBondPartners(st, g, (me.y >> 4) & 0xf, bondsI);
+        const int nI = (me.y >> 4) & 0xf;
+#pragma unroll
+        for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? st.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
     }
 
     __device__ __forceinline__ void beginLaw(const WorldInfo&, int4 me, float2 pos, float2 vel)
@@ -691,9 +630,15 @@ struct CollisionLaw {
         const int nI = (me.y >> 4) & 0xf, maxI = (me.y >> 8) & 0xff;
         densI = __int_as_float(me.z);
         fusionI = !barrierI && nI < maxI && __int_as_float(me.w) <= maxBindingEnergy;
-        fx = fy = dxx = dxy = 0;
+        F = dx = f2(0.0f, 0.0f);
         best = -1;
         bestId = ~0ull;
+    }
+
+    __device__ __forceinline__ void begin(const DevState& st, const WorldInfo& wi, int4 me, float2 pos, float2 vel)
+    {
+        beginScan(st, wi, me);
+        beginLaw(wi, me, pos, vel);
     }
 
     __device__ __forceinline__ bool near(float2 raw) const { return raw.x * raw.x + raw.y * raw.y <= R2reject; }
@@ -721,14 +666,9 @@ struct CollisionLaw {
         const float2 pd = f2(-raw.x, -raw.y);
         const bool bonded = isBondedTo(bondsI, j);
         if (visibleJ) {  // i's own scan sees j
-            if (!barrierI && d < minDist) {
-                dxx += toFix(pd.x * (minDist / 5.0f));
-                dxy += toFix(pd.y * (minDist / 5.0f));
-            }
+            if (!barrierI && d < minDist) dx = dx + pd * (minDist / 5.0f);
             if (!bonded) {
-                const float2 f = collisionForce(pd, d, vi, vj, barrierI, *p);
-                fx += toFix(f.x);
-                fy += toFix(f.y);
+                F = F + collisionForce(pd, d, vi, vj, barrierI, *p);
                 const float2 vd = vi - vj;
                 if (fusionI && len2(vd) >= fusionVelocity && dot2(pd, vd) < 0.0f) {
                     const int nJ = (om.y >> 4) & 0xf, maxJ = (om.y >> 8) & 0xff;
@@ -742,42 +682,25 @@ struct CollisionLaw {
                 }
             }
         }
-        if (visibleI && !bonded) {  // j's scan sees i and applies -f(j,i) to i
-            const float2 f = collisionForce(raw, d, vj, vi, om.y & kStageBarrier, *p);
-            fx -= toFix(f.x);
-            fy -= toFix(f.y);
-        }
-    }
-
-    template <int LPC>
-    __device__ __forceinline__ void reduce(const LaneGroup<LPC>& grp)
-    {
-        if (LPC == 1) return;
-        if (grp.any((fx | fy | dxx | dxy) != 0)) {
-            fx = grp.sum(fx);
-            fy = grp.sum(fy);
-            dxx = grp.sum(dxx);
-            dxy = grp.sum(dxy);
-        }
-        if (grp.any(best >= 0)) {
-            int idx = best;
-            grp.argmin(bestId, idx);
-            best = idx;
-        }
+        if (visibleI && !bonded)  // j's scan sees i and applies -f(j,i) to i
+            F = F - collisionForce(raw, d, vj, vi, om.y & kStageBarrier, *p);
     }
 
     __device__ __forceinline__ void end()
     {
         const DevState& st = *s;
-        st.force[g] = f2(fromFix(fx), fromFix(fy));
-        st.posB[g] = pi + f2(fromFix(dxx), fromFix(dxy));
+        st.force[g] = F;
+        st.posB[g] = pi + dx;
+        st.dpos[g] = dx;
         st.densNew[g] = densI;
         st.best[g] = best;
     }
 };
 
 // the pair phase of the staged cell k, neighbours from the global tile lists
-__device__ __forceinline__ void pairsGlobalCell(const DevState& s, long long k, int motion)
+// (tiles in the same row order as the regions' 3x3 scan)
+template <int Motion>
+__device__ __forceinline__ void pairsGlobalCell(const DevState& s, long long k)
 {
     const int4 me = s.stagedMeta[k];
     const float4 mpv = s.stagedPV[k];
@@ -785,23 +708,21 @@ __device__ __forceinline__ void pairsGlobalCell(const DevState& s, long long k, 
     const WorldInfo& wi = s.worlds[w];
     const float2 pi = f2(mpv.x, mpv.y);
     const int sx = slotX(pi.x, wi.W), sy = slotX(pi.y, wi.H);
-    if (motion == ALIEN_B200_MOTION_FLUID) {
+    if (Motion == ALIEN_B200_MOTION_FLUID) {
         FluidLaw law;
-        law.beginScan(s, wi, me);
-        law.beginLaw(wi, me, pi, f2(mpv.z, mpv.w));
+        law.begin(s, wi, me, pi, f2(mpv.z, mpv.w));
         forEachWindowTile(wi, sx, sy, [&](long long t) {
             const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
             for (uint32_t m = k0; m < k1; ++m) {
                 const float4 opv = s.stagedPV[m];
-                const float2 pd = correctDirection(pi - f2(opv.x, opv.y), wi.W, wi.H);
+                const float2 pd = seamDiff2(pi, f2(opv.x, opv.y), wi.W, wi.H);
                 if (law.near(pd)) law.visit(s.stagedMeta[m], f2(opv.z, opv.w), pd);
             }
         });
         law.end();
     } else {
         CollisionLaw law;
-        law.beginScan(s, wi, me);
-        law.beginLaw(wi, me, pi, f2(mpv.z, mpv.w));
+        law.begin(s, wi, me, pi, f2(mpv.z, mpv.w));
         forEachWindowTile(wi, sx, sy, [&](long long t) {
             const uint32_t k0 = s.tileStart[t], k1 = s.tileStart[t + 1];
             for (uint32_t m = k0; m < k1; ++m) {
@@ -813,10 +734,13 @@ __device__ __forceinline__ void pairsGlobalCell(const DevState& s, long long k, 
         law.end();
     }
 }
+
 // Cells that the region kernels cannot stage (rows denser than the shared
 // buffer, worlds too small for regions) are appended to the overflow list
 // and handled by kPairsOverflow after the region kernels, one thread per
 // cell, so that the region kernels carry none of this path's registers.
+// The visiting order is the regions' (tiles in row order, storage order
+// within a tile), so a cell's sums do not depend on the path.
 __device__ __forceinline__ void pairsDefer(const DevState& s, long long k)
 {
     const uint32_t at = atomicAdd(s.pairOverflowCount, 1u);
@@ -828,66 +752,87 @@ __global__ void __launch_bounds__(kBlock) kPairsOverflow(DevState s)
     const uint32_t n = *s.pairOverflowCount;
     for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
         const long long k = s.pairOverflow[i];
-        pairsGlobalCell(s, k, s.worlds[(s.stagedMeta[k].y >> 16) & 0xffff].motionType);
+        if (s.worlds[(s.stagedMeta[k].y >> 16) & 0xffff].motionType == ALIEN_B200_MOTION_FLUID)
+            pairsGlobalCell<ALIEN_B200_MOTION_FLUID>(s, k);
+        else
+            pairsGlobalCell<ALIEN_B200_MOTION_COLLISION>(s, k);
     }
 }
 
 // ------------------------------------------------------- kPairsRegion ----
-// One CTA per region of regW x regH tiles (at most RegionShape<Motion>) of
-// one world.  It copies the staged records of the region and of its
-// one-tile halo from the tile-sorted arrays into shared memory, all
-// (regW+2) x (regH+2) local tiles in row-major order (each tile a contiguous
-// run), so that the tiles of one row of a cell's window are one contiguous
-// run.  A local row is at most three contiguous global runs (left halo tile,
-// own tiles, right halo tile), so the copy finds its source with a search
-// over rows.  Fluid worlds shift halo tiles that lie across the torus seam by
-// +-W / +-H, so that plain differences are the minimal-image displacements;
-// collision worlds keep stored positions (the reference's distance test is
-// on the uncorrected difference, so candidates across the seam never pass).
-//
-// Each own cell is handled by a group of LPC lanes: the group lists the
-// window tiles the cell's disc reaches (a neighbour tile is skipped when the
-// cell is farther than R, plus a rounding margin, from the shared edge:
-// such tiles hold no candidate within R) as at most three contiguous runs of
-// shared-memory records, the lanes take every LPC-th candidate of the
-// flattened runs, visit the candidates that pass the reject, and the group
-// reduces its fixed-point sums with shuffles; lane 0 writes the results.
-// Groups take the band's own cells round robin, so every lane of the CTA
-// has work until the last LPC-lane group finishes.
-// Regions whose records exceed the shared buffer are processed in bands of
-// own rows; rows that do not fit even alone, and worlds too small for
-// regions, defer their cells to kPairsOverflow.
+// One CTA per region of regW x regH tiles (up to RegionShape<Motion>: 24 x 16
+// for collision worlds, 32 x 8 for fluid worlds) of one world.  It
+// copies the staged records of the region and of its one-tile halo from the
+// tile-sorted arrays into shared memory, all (regW+2) x (regH+2) local tiles
+// in row-major order (each tile a contiguous run in storage order), so that
+// the tiles of one row of a cell's window are one contiguous run.  A local
+// row is at most three contiguous global runs (left halo tile, own tiles,
+// right halo tile), so the copy finds its source with a search over rows.
+// Fluid worlds shift halo tiles that lie across the torus seam by +-W / +-H,
+// so that plain differences are the minimal-image displacements; collision
+// worlds keep stored positions (the reference's distance test is on the
+// uncorrected difference, so candidates across the seam never pass).
+// Every cell scans only the tiles of its 3x3 window that the disc of radius
+// R around it reaches (a neighbour tile is skipped when the cell is farther
+// than R, plus a rounding margin, from the shared edge: such tiles hold no
+// candidate within R), appending candidates that pass the cheap distance
+// reject to a per-thread hit list in shared memory, and runs the pair law on
+// the hits afterwards: the scan loop stays convergent across the warp, and
+// the law runs once per hit instead of once per scan iteration in which any
+// lane had a hit.  The scan loop holds only the state the reject needs (the
+// law's accumulators start after it), and a cell with more than HitCap hits
+// scans a second time, visiting on the way in the same order.  Hits are
+// visited in scan order (row by row, tile by tile, storage order), the order
+// of the full 3x3 scan minus candidates that the law ignores, so the FP32
+// sums do not depend on the pruning.
+// Rows of regions whose records exceed the shared buffer even alone, and
+// worlds too small for regions, defer their cells to kPairsOverflow.
 constexpr int kRegionThreads = 256;
-constexpr int kDefaultPairLanes = 4;  // lanes per cell until the autotuner has run
-constexpr int kNumPairLaneChoices = ALIEN_B200_PAIR_LANE_CHOICES;
-constexpr int kPairLaneChoices[kNumPairLaneChoices] = {2, 4, 8, 16};
+// Region shape per motion type (tiles per region, shared-buffer records,
+// hit-list entries per thread, resident CTAs per SM), from a sweep of shapes
+// on the B200.  Dense regions
+// are processed in bands of rows, so the buffer size bounds no world.  The
+// visiting order does not depend on the shape; the FP32 results of different
+// builds can still differ in the last bit where the compiler contracts
+// multiply-adds differently.
 template <int Motion>
 struct RegionShape;
 template <>
 struct RegionShape<ALIEN_B200_MOTION_FLUID> {
-    static constexpr int W = 32, H = 8, Cap = 1152, MinBlocks = 4;
+    static constexpr int W = 32, H = 8, Cap = 1152, HitCap = 24, MinBlocks = 3;
 };
 template <>
 struct RegionShape<ALIEN_B200_MOTION_COLLISION> {
-    static constexpr int W = 24, H = 16, Cap = 1152, MinBlocks = 4;
+    static constexpr int W = 24, H = 16, Cap = 1152, HitCap = 24, MinBlocks = 4;
+};
+// Candidate region shapes (tiles x, y) per motion type for the autotuner
+// (engine.cu, Arena::autotune), each within RegionShape<Motion>; the first
+// is the default.  A cell's neighbours are visited in the same order
+// whatever the shape, so the choice changes no result.
+constexpr int kNumRegionChoices = ALIEN_B200_REGION_CHOICES;
+constexpr int kRegionChoices[2][kNumRegionChoices][2] = {
+    {{32, 8}, {16, 8}, {32, 4}, {24, 8}},     // fluid
+    {{24, 16}, {16, 16}, {24, 8}, {12, 16}},  // collision
 };
 template <int Motion>
 constexpr size_t regionDynSmem()
 {
-    return static_cast<size_t>(RegionShape<Motion>::Cap) * (sizeof(int4) + 2 * sizeof(float2));
+    return static_cast<size_t>(RegionShape<Motion>::Cap) * (sizeof(int4) + 2 * sizeof(float2))
+           + static_cast<size_t>(RegionShape<Motion>::HitCap) * kRegionThreads * sizeof(uint16_t);
 }
 
-template <int Motion, int LPC>
+template <int Motion>
 __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks) kPairsRegion(DevState s)
 {
     constexpr int kRegionCap = RegionShape<Motion>::Cap;
+    constexpr int kHitCap = RegionShape<Motion>::HitCap;
     constexpr int kRegionMaxH = RegionShape<Motion>::H;
     constexpr int kRegionMaxTiles = (RegionShape<Motion>::W + 2) * (RegionShape<Motion>::H + 2);
-    constexpr int kGroups = kRegionThreads / LPC;
     extern __shared__ int4 dyn[];
     int4* sMeta = dyn;
     float2* sPos = reinterpret_cast<float2*>(sMeta + kRegionCap);
     float2* sVel = sPos + kRegionCap;
+    uint16_t* sHits = reinterpret_cast<uint16_t*>(sVel + kRegionCap);  // [kHitCap][kRegionThreads]
     __shared__ int tStart[kRegionMaxTiles + 1];  // shared-memory offset of each local tile
     __shared__ int tGlobal[kRegionMaxTiles];     // first sorted index of the tile
     __shared__ float2 tShift[kRegionMaxTiles];
@@ -914,6 +859,20 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
     }
 
     const int LW = ownW + 2, LH = ownH + 2, NT = LW * LH;
+    // Fluid worlds see neighbours across the torus seam as minimal images:
+    // halo tiles that wrap are shifted by -+W / -+H.  A region that touches
+    // the right (top) seam shifts all its other tiles down by W (H) instead
+    // and leaves the wrapped halo as stored, so that every shift subtracts
+    // the world size from a coordinate in its upper half, which is exact
+    // (the region is narrower than half the world, and no region touches
+    // both seams of an axis).  Differences are then the ones the global
+    // path computes with seamDiff, bit for bit, for every region shape.
+    float2 seamFlip = f2(0.0f, 0.0f);
+    if (Motion == ALIEN_B200_MOTION_FLUID) {
+        if (tx0 + ownW == wi.nTX) seamFlip.x = -static_cast<float>(wi.W);
+        if (ty0 + ownH == wi.nTY) seamFlip.y = -static_cast<float>(wi.H);
+    }
+    const float2 ownShift = seamFlip;  // shift of the region's own tiles
     // 1. local tile table (row-major over the region and its halo); every
     //    thread handles a contiguous chunk of tiles for the offsets
     {
@@ -938,6 +897,7 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
                 gy -= wi.nTY;
                 sh.y = static_cast<float>(wi.H);
             }
+            sh = sh + seamFlip;
             const long long t = wi.tileBase + gx + static_cast<long long>(gy) * wi.nTX;
             const uint32_t k0 = s.tileStart[t];
             const uint32_t n = s.tileStart[t + 1] - k0;
@@ -970,8 +930,7 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
         if (r <= ownH) rowOwn[r] = acc;
     }
     __syncthreads();
-    const LaneGroup<LPC> grp;
-    const int group = threadIdx.x / LPC;
+    uint16_t* myHits = sHits + threadIdx.x;
     const float T = static_cast<float>(wi.T);
     // Own rows in bands whose local rows (the band and one halo row on either
     // side) fit the shared buffer: one band for the usual region, several for
@@ -1014,49 +973,59 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
             sMeta[e - base] = s.stagedMeta[src];
         }
         __syncthreads();
-        // 3. each own cell of the band by one group of LPC lanes, round robin
-        //    (shared-memory index = record offset - base)
+        // 3. pair law of every own cell of the band against the tiles its
+        //    disc reaches (shared-memory index = record offset - base)
         int ly = band0;  // own row of o; o only grows, so the search continues from the last row
-        for (int o = rowOwn[band0 - 1] + group; o < rowOwn[band1]; o += kGroups) {
+        for (int o = rowOwn[band0 - 1] + threadIdx.x; o < rowOwn[band1]; o += kRegionThreads) {
             while (rowOwn[ly] <= o) ++ly;
             const int e = tStart[ly * LW + 1] + (o - rowOwn[ly - 1]) - base;
             const float2 pi = sPos[e];
-            const int4 me = sMeta[e];
+            const float2 piG = pi - ownShift;  // the stored position (exact)
             // own tile column as binned (own tiles are not shifted)
-            const int gx = slotX(pi.x, wi.W) / wi.T;
+            const int gx = slotX(piG.x, wi.W) / wi.T;
             const int lx = min(max(gx - tx0 + 1, 1), ownW);
             const int gy = ty0 + ly - 1;
             auto scan = [&](auto& law, auto diff) {
+                const int4 me = sMeta[e];
                 law.beginScan(s, wi, me);
                 // reach: R plus a margin above the rounding of positions up to the world size
                 const float reach = law.R * 1.0001f + 1e-3f + 4.0f * static_cast<float>(max(wi.W, wi.H)) * 1.2e-7f;
                 const float left = static_cast<float>(gx) * T, right = fminf(static_cast<float>(gx + 1) * T, static_cast<float>(wi.W));
                 const float bottom = static_cast<float>(gy) * T, top = fminf(static_cast<float>(gy + 1) * T, static_cast<float>(wi.H));
-                const int c0 = lx - (pi.x - reach < left ? 1 : 0), c1 = lx + (pi.x + reach >= right ? 1 : 0);
-                const int r0 = ly - (pi.y - reach < bottom ? 1 : 0), r1 = ly + (pi.y + reach >= top ? 1 : 0);
-                // the window rows' runs, flattened: candidate k of the cell is
-                // record k + shift[r] of run r, for k in [runEnd[r-1], runEnd[r])
-                int shift[3], runEnd[3], total = 0;
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    const int r = r0 + i;
-                    if (r <= r1) {
-                        const int b0 = tStart[r * LW + c0] - base, b1 = tStart[r * LW + c1 + 1] - base;
-                        shift[i] = b0 - total;
-                        total += b1 - b0;
-                    } else {
-                        shift[i] = 0;
+                const int c0 = lx - (piG.x - reach < left ? 1 : 0), c1 = lx + (piG.x + reach >= right ? 1 : 0);
+                const int r0 = ly - (piG.y - reach < bottom ? 1 : 0), r1 = ly + (piG.y + reach >= top ? 1 : 0);
+                // scan: the hits in scan order (the first kHitCap kept, all counted)
+                int nh = 0;
+#pragma unroll 1
+                for (int r = r0; r <= r1; ++r) {
+                    const int b0 = tStart[r * LW + c0] - base, b1 = tStart[r * LW + c1 + 1] - base;
+                    for (int m = b0; m < b1; ++m) {
+                        const float2 dm = diff(m);
+                        if (law.near(dm) && law.relevant(sMeta, m, dm)) {
+                            if (nh < kHitCap) myHits[nh * kRegionThreads] = static_cast<uint16_t>(m);
+                            ++nh;
+                        }
                     }
-                    runEnd[i] = total;
                 }
-                law.beginLaw(wi, me, pi, sVel[e]);
-                for (int k = grp.lane; k < total; k += LPC) {
-                    const int m = k + (k < runEnd[0] ? shift[0] : (k < runEnd[1] ? shift[1] : shift[2]));
-                    const float2 dm = diff(m);
-                    if (law.near(dm) && law.relevant(sMeta, m, dm)) law.visit(sMeta[m], sVel[m], dm);
+                // law over the hits; a cell with more hits than the list holds
+                // scans again and visits on the way, in the same order
+                law.beginLaw(wi, me, piG, sVel[e]);
+                if (nh <= kHitCap) {
+                    for (int i = 0; i < nh; ++i) {
+                        const int m = myHits[i * kRegionThreads];
+                        law.visit(sMeta[m], sVel[m], diff(m));
+                    }
+                } else {
+#pragma unroll 1
+                    for (int r = r0; r <= r1; ++r) {
+                        const int b0 = tStart[r * LW + c0] - base, b1 = tStart[r * LW + c1 + 1] - base;
+                        for (int m = b0; m < b1; ++m) {
+                            const float2 dm = diff(m);
+                            if (law.near(dm) && law.relevant(sMeta, m, dm)) law.visit(sMeta[m], sVel[m], dm);
+                        }
+                    }
                 }
-                law.reduce(grp);
-                if (grp.lane == 0) law.end();
+                law.end();
             };
             if (Motion == ALIEN_B200_MOTION_FLUID) {
                 FluidLaw law;
@@ -1084,23 +1053,28 @@ struct BondRow {
     float2 disp[kMaxBonds];  // corrected partner - cell
 };
 
-__device__ __forceinline__ void loadBondRow(const DevState& s, long long g, int n, const float2* __restrict__ P, int W,
-                                            int H, BondRow& r)
+// the bond vectors at the step's current positions: the minimal-image
+// difference of the step-start positions (exact for partners, also across
+// the seam) plus the difference of the in-step displacements
+__device__ __forceinline__ void loadBondRow(const DevState& s, long long g, int n, int W, int H, BondRow& r)
 {
     r.n = n;
     const int2* row = reinterpret_cast<const int2*>(s.bond + g * kMaxBonds);
-    const float2 pi = P[g];
+    const float2 pi = s.posA[g], di = s.dpos[g];
 #pragma unroll
     for (int h = 0; h < kMaxBonds / 2; ++h) {
         const int2 jj = 2 * h < r.n ? row[h] : make_int2(0, 0);
         r.j[2 * h] = jj.x;
         r.j[2 * h + 1] = jj.y;
     }
-    float2 pj[kMaxBonds];
+    float2 pj[kMaxBonds], dj[kMaxBonds];
 #pragma unroll
-    for (int k = 0; k < kMaxBonds; ++k) pj[k] = k < r.n ? P[r.j[k]] : pi;
+    for (int k = 0; k < kMaxBonds; ++k) {
+        pj[k] = k < r.n ? s.posA[r.j[k]] : pi;
+        dj[k] = k < r.n ? s.dpos[r.j[k]] : di;
+    }
 #pragma unroll
-    for (int k = 0; k < kMaxBonds; ++k) r.disp[k] = correctDirection(pj[k] - pi, W, H);
+    for (int k = 0; k < kMaxBonds; ++k) r.disp[k] = seamDiff2(pj[k], pi, W, H) + (dj[k] - di);
 }
 
 // the triangle test of the angle forces depends only on the bond rows, which
@@ -1208,26 +1182,24 @@ __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, cons
     return F;
 }
 
-// verletPositionUpdate (CellProcessor.cuh:525-544) of cell g from its
-// overlap-corrected position, velocity v, bond force F1 and the fixed-point
-// angle forces (ax, ay); stores the total force of a non-barrier cell and
-// returns the new position
-__device__ __forceinline__ float2 verletPosition(const DevState& s, long long g, const WorldInfo& wi,
-                                                 const AlienPhysicsParams& p, bool barrierG, float2 v, float2 F1,
-                                                 long long ax, long long ay)
+// verletPositionUpdate (CellProcessor.cuh:525-544) of cell g as an
+// increment: its displacement after the overlap push (dpos) plus
+// v * dt + F * dt^2 / 2 with the bond force F1 and the fixed-point angle
+// forces (ax, ay); stores the total force of a non-barrier cell and returns
+// the cell's displacement since the step start.  The position itself is
+// rounded once, when the next step folds the displacement in.
+__device__ __forceinline__ float2 verletIncrement(const DevState& s, long long g, const AlienPhysicsParams& p, bool barrierG,
+                                                  float2 v, float2 F1, long long ax, long long ay)
 {
     const float dt = p.timestepSize;
-    const float2 pb = s.posB[g];
-    float2 np;
+    const float2 d = s.dpos[g];
     if (barrierG) {
         s.force1[g] = F1;
-        np = pb + v * dt;
-    } else {
-        const float2 F = F1 + f2(fromFix(ax), fromFix(ay));
-        s.force1[g] = F;
-        np = pb + (v * dt + F * dt * dt / 2.0f);
+        return d + v * dt;
     }
-    return correctPosition(np, wi.W, wi.H);
+    const float2 F = F1 + f2(fromFix(ax), fromFix(ay));
+    s.force1[g] = F;
+    return d + (v * dt + F * dt * dt / 2.0f);
 }
 
 // -------------------------------------------------------- kApplyBond1 ----
@@ -1261,14 +1233,14 @@ __global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
             s.velA[g] = v;
         }
         BondRow r;
-        loadBondRow(s, g, n, s.posB, wi.W, wi.H, r);
+        loadBondRow(s, g, n, wi.W, wi.H, r);
         const float2 F1 = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 0, kTriStore);
         if (T % 3 == 0) {
             s.force1[g] = F1;  // angle forces of other cells still arrive: kVerletPos
         } else {
             // no angle forces this step: verletPositionUpdate here, with the
             // arithmetic of kVerletPos for empty accumulators
-            s.posA[g] = verletPosition(s, g, wi, p, barrierG, v, F1, 0, 0);
+            s.dpos[g] = verletIncrement(s, g, p, barrierG, v, F1, 0, 0);
         }
         if (p.motionType == ALIEN_B200_MOTION_FLUID) s.density[g] = s.densNew[g];
     } else {
@@ -1310,7 +1282,7 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletPos(DevState s)
             ay = a.y;
             if (ax | ay) *reinterpret_cast<longlong2*>(s.angleAcc + 4 * g) = make_longlong2(0, 0);
         }
-        s.posA[g] = verletPosition(s, g, wi, p, barrierG, v, F1, ax, ay);
+        s.dpos[g] = verletIncrement(s, g, p, barrierG, v, F1, ax, ay);
     } else {
         forParticleBlocks(s, usedParticles, [&](const PartCtx& c, int) {
             if (!c.inRange || !s.palive[c.q]) return;
@@ -1342,7 +1314,7 @@ __global__ void __launch_bounds__(kBlock, 6) kBond2(DevState s)
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
         const uint64_t T = s.counters[c.w].timestep;
         BondRow r;
-        loadBondRow(s, g, n, s.posA, wi.W, wi.H, r);
+        loadBondRow(s, g, n, wi.W, wi.H, r);
         if (!barrierG) {
             const float maxDist = p.cellMaxBindingDistance[col];
             bool destroy = false;
@@ -1460,7 +1432,7 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletVel(DevState s)
             if (s.barrier[cell]) {
                 const float2 vc = s.velA[cell];
                 const float2 vr = pv - vc;
-                const float2 r = correctDirection(pp - s.posB[cell], wi.W, wi.H);
+                const float2 r = seamDiff2(pp, s.posB[cell], wi.W, wi.H);
                 const float dvr = dot2(vr, r);
                 if (dvr < 0.0f) {
                     const float trr = fmaxf(0.1f, lensq2(r));
@@ -1821,15 +1793,16 @@ __device__ inline bool tryAddOneWay(const DevState& s, const WorldInfo& wi, long
     loadBonds(s, c1, out);
     const int n = out.n;
     if (n == kMaxBonds) return false;
-    const float2 p1 = s.posA[c1], p2 = s.posA[c2];
     if (n >= 2) {  // wouldResultInOverlappingConnection, CellConnectionProcessor.cuh:476-500
+        // on the positions as the reference stores them (absolute, rounded)
+        const float2 p1 = stepPos(s, c1, wi.W, wi.H), p2 = stepPos(s, c2, wi.W, wi.H);
         for (int k = 0; k < n; ++k) {
             const int cc = out.b[k], nc = out.b[(k + 1) % n];
             const int ncc = s.numConn[cc];
             bool both = false;
             for (int m = 0; m < ncc; ++m) both |= (s.bond[static_cast<long long>(cc) * kMaxBonds + m] == nc);
             if (!both) continue;
-            if (crossing(p1, p2, s.posA[cc], s.posA[nc])) return false;
+            if (crossing(p1, p2, stepPos(s, cc, wi.W, wi.H), stepPos(s, nc, wi.W, wi.H))) return false;
         }
     }
     const float newAngle = angleOfVector(posDelta);
@@ -1842,7 +1815,7 @@ __device__ inline bool tryAddOneWay(const DevState& s, const WorldInfo& wi, long
         return true;
     }
     if (n == 1) {
-        const float prevAngle = angleOfVector(correctDirection(s.posA[out.b[0]] - p1, wi.W, wi.H));
+        const float prevAngle = angleOfVector(stepDisp(s, c1, out.b[0], wi.W, wi.H));
         float diff = newAngle - prevAngle;
         if (diff < 0) diff += 360.0f;
         if (fabsf(diff) < kNearZero || fabsf(diff - 360.0f) < kNearZero || fabsf(diff + 360.0f) < kNearZero) return false;
@@ -1857,8 +1830,8 @@ __device__ inline bool tryAddOneWay(const DevState& s, const WorldInfo& wi, long
     float prevAngle = 0.0f, nextAngle = 0.0f;
     for (; index < n; ++index) {
         const int prevIndex = (index + n - 1) % n;
-        prevAngle = angleOfVector(correctDirection(s.posA[out.b[prevIndex]] - p1, wi.W, wi.H));
-        nextAngle = angleOfVector(correctDirection(s.posA[out.b[index]] - p1, wi.W, wi.H));
+        prevAngle = angleOfVector(stepDisp(s, c1, out.b[prevIndex], wi.W, wi.H));
+        nextAngle = angleOfVector(stepDisp(s, c1, out.b[index], wi.W, wi.H));
         if (isAngleInBetween(prevAngle, nextAngle, newAngle) || prevIndex == index) break;
     }
     if (index == n) return false;
@@ -1907,7 +1880,7 @@ __global__ void __launch_bounds__(kBlock, 8) kResolve(DevState s)
     const WorldInfo& wi = s.worlds[c.w];
     const bool gFirst = s.id[g] < s.id[j];
     const long long c1 = gFirst ? g : j, c2 = gFirst ? j : g;
-    const float2 pd = correctDirection(s.posA[c2] - s.posA[c1], wi.W, wi.H);
+    const float2 pd = stepDisp(s, c1, c2, wi.W, wi.H);
     BondList l1, l2;
     if (!tryAddOneWay(s, wi, c1, c2, pd, l1)) return;
     if (!tryAddOneWay(s, wi, c2, c1, pd * -1.0f, l2)) return;
@@ -2198,7 +2171,9 @@ __global__ void __launch_bounds__(kBlock) kEventEmit(DevState s)
         const uint32_t rr = blockExclusiveScan(rad, nullptr) + s.blockRad[blockIdx.x];
         const uint32_t dr = blockExclusiveScan(del, nullptr) + s.blockDel[blockIdx.x];
         if (rad) emitParticle(s, wi, wc.radSlotBase + rr, wc.radIdBase + rr, s.radPos[g], s.radVel[g], s.radEnergy[g], s.color[g]);
-        if (del) emitParticle(s, wi, wc.delSlotBase + dr, wc.delIdBase + dr, s.posA[g], s.velA[g], s.energy[g], s.color[g]);
+        if (del)
+            emitParticle(s, wi, wc.delSlotBase + dr, wc.delIdBase + dr, stepPos(s, g, wi.W, wi.H), s.velA[g], s.energy[g],
+                         s.color[g]);
     } else {
         // splits come from the slots used before this step's appends
         // (radSlotBase); appended particles carry no split

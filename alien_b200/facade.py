@@ -124,15 +124,16 @@ class SimulationFacade:
         return r
 
     def launch_config(self) -> LaunchConfig:
-        """lanes per cell of the pair kernel in use, and the autotuner's timings"""
+        """pair-kernel region shapes in use, and the autotuner's timings"""
         c = LaunchConfig()
         check(self._lib.alien_b200_get_launch_config(self._handle(), ctypes.byref(c)))
         return c
 
-    def set_pair_lanes(self, fluid: int = 0, collision: int = 0) -> None:
-        """fix the lanes per cell of the pair kernel per motion type (0 = autotune)"""
+    def set_region_choice(self, fluid: int = 0, collision: int = 0) -> None:
+        """fix the pair-kernel region shape per motion type: candidate index
+        + 1, or 0 for the autotuner"""
         c = LaunchConfig()
-        c.pairLanesFixed[0], c.pairLanesFixed[1] = int(fluid), int(collision)
+        c.regionChoiceFixed[0], c.regionChoiceFixed[1] = int(fluid), int(collision)
         check(self._lib.alien_b200_set_launch_config(self._handle(), ctypes.byref(c)))
 
     def debug_cell_map(self):
@@ -252,9 +253,9 @@ class BatchSimulation:
         check(self._lib.alien_b200_batch_get_launch_config(self._h, ctypes.byref(c)))
         return c
 
-    def set_pair_lanes(self, fluid: int = 0, collision: int = 0) -> None:
+    def set_region_choice(self, fluid: int = 0, collision: int = 0) -> None:
         c = LaunchConfig()
-        c.pairLanesFixed[0], c.pairLanesFixed[1] = int(fluid), int(collision)
+        c.regionChoiceFixed[0], c.regionChoiceFixed[1] = int(fluid), int(collision)
         check(self._lib.alien_b200_batch_set_launch_config(self._h, ctypes.byref(c)))
 
     def kernels_per_step(self) -> int:

@@ -517,10 +517,10 @@ def main():
     launches = sim.kernel_launches() - launches0
     stats1 = sim.get_raw_statistics()
     lc = sim.launch_config()
-    launch_cfg = {"pair_lanes_per_cell": {"fluid": lc.pairLanes[0], "collision": lc.pairLanes[1]},
+    launch_cfg = {"pair_region_tiles": {"fluid": list(lc.regionTiles[0]), "collision": list(lc.regionTiles[1])},
                   "autotuned": bool(lc.tuned),
-                  "tuned_ms_by_lanes": {m: {str(l): round(lc.tunedMs[i][k], 4) for k, l in enumerate((2, 4, 8, 16))}
-                                        for i, m in enumerate(("fluid", "collision"))}}
+                  "tuned_ms_by_region": {m: {f"{lc.candidates[i][k][0]}x{lc.candidates[i][k][1]}": round(lc.tunedMs[i][k], 4)
+                                             for k in range(4)} for i, m in enumerate(("fluid", "collision"))}}
     ms = max_over_ranks(ms)
     cells_mean = 0.5 * (stats0.numCells + stats1.numCells)
     total_cells = sum_over_ranks(cells_mean)

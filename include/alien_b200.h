@@ -302,32 +302,36 @@ int alien_b200_timed_timesteps(alien_b200_simulation* sim, uint64_t timesteps, d
                                int* numKernels);
 const char* alien_b200_step_kernel_name(int index);
 
-/* Launch configuration.  The pair-force kernel handles each cell with a
- * group of `lanes` lanes that split the cell's neighbour candidates (2, 4, 8
- * or 16; choices in this order in tunedMs).  Its sums are fixed-point
- * integers, so the lane count changes no result, only the speed.  Unless the
- * caller fixes it (pairLanesFixed[motion] nonzero), an autotuner chooses it
- * per motion type (0 fluid, 1 collision) at the first step of every new
- * layout (set_data, a batch): it bins the current state, times the pair
- * kernel with every lane count (three launches each after one untimed) and
- * keeps the fastest (alien_b200_choose_pair_lanes).  The state is not
- * changed.  No counterpart in the reference, whose block size per kernel is
- * fixed (KERNEL_CALL, Macros.cuh:75-83) or computed by
- * calcOptimalThreadsForFluidKernel (SimulationKernelsLauncher.cu:18-22). */
-#define ALIEN_B200_PAIR_LANE_CHOICES 4
+/* Launch configuration of the pair-force kernel.  It processes the world in
+ * regions of tiles (one CTA each, staged in shared memory); the region
+ * shape is one of ALIEN_B200_REGION_CHOICES candidates per motion type (0
+ * fluid, 1 collision; candidates[m][i] = tiles in x, y; the first is the
+ * default).  A cell's neighbours are visited in the same order whatever the
+ * shape, so the choice changes no result, only the speed.  Unless the
+ * caller fixes it (regionChoiceFixed[m] = candidate index + 1), an
+ * autotuner chooses it at the first step of every new layout (set_data, a
+ * batch): it bins the current state, times the pair kernel with every
+ * candidate (three launches each after one untimed) and keeps the fastest
+ * (alien_b200_choose_region).  The state is not changed.  No counterpart in
+ * the reference, whose launch shapes are fixed (KERNEL_CALL, Macros.cuh:75-83)
+ * or computed by calcOptimalThreadsForFluidKernel
+ * (SimulationKernelsLauncher.cu:18-22). */
+#define ALIEN_B200_REGION_CHOICES 4
 typedef struct AlienLaunchConfig {
-    int32_t pairLanes[2];       /* in use (or to be used by the next graph), per motion type */
-    int32_t pairLanesFixed[2];  /* set: fixed by the caller; 0 = autotune */
-    int32_t tuned;              /* 1 once the autotuner ran on this layout */
-    float tunedMs[2][ALIEN_B200_PAIR_LANE_CHOICES]; /* measured ms per launch (0 = not measured) */
+    int32_t regionTiles[2][2];      /* shape in use (tiles x, y), per motion type */
+    int32_t regionChoice[2];        /* its index among the candidates */
+    int32_t regionChoiceFixed[2];   /* fixed by the caller: index + 1; 0 = autotune */
+    int32_t tuned;                  /* 1 once the autotuner ran on this layout */
+    float tunedMs[2][ALIEN_B200_REGION_CHOICES];  /* measured ms per launch (0 = not measured) */
+    int32_t candidates[2][ALIEN_B200_REGION_CHOICES][2];
 } AlienLaunchConfig;
-/* Only pairLanesFixed is read: 0 returns a motion type to the autotuner. */
+/* Only regionChoiceFixed is read: 0 returns a motion type to the autotuner. */
 int alien_b200_set_launch_config(alien_b200_simulation* sim, const AlienLaunchConfig* config);
 int alien_b200_get_launch_config(alien_b200_simulation* sim, AlienLaunchConfig* config);
-/* The autotuner's rule on n measured times (ms per launch for 2, 4, 8, 16
- * lanes; entries <= 0 are skipped): the fastest, where a larger lane count
- * must beat the best smaller one by more than 2 %.  Returns the lane count. */
-int alien_b200_choose_pair_lanes(const float* milliseconds, int n);
+/* The autotuner's rule on n measured times (ms per launch of each candidate
+ * in order; entries <= 0 are skipped): the fastest, where a later candidate
+ * must beat the best earlier one by more than 2 %.  Returns the index. */
+int alien_b200_choose_region(const float* milliseconds, int n);
 
 /* The cell map of the current state as the step's own binning kernels
  * build it (tile histogram, scan, scatter, tile-ordered staging), read back

@@ -174,7 +174,8 @@ def test_radiation_emission(motion, steps):
         prm.highRadiationMinCellEnergy[c] = 90.0
         prm.radiationMinCellAge[c] = 50
     got, ref, _ = run_both(data, world, prm, steps, 0, precision="f64")
-    assert len(ref.particles) > len(data.particles), "no radiation particle was emitted"
+    new_ids = ref.particles["id"] > max(int(data.cells["id"].max()), int(data.particles["id"].max()))
+    assert np.count_nonzero(new_ids) > 0, "no radiation particle was emitted"
     compare_cells(got.cells, ref.cells, world, before=data.cells)
     compare_particles(got.particles, ref.particles, world, before=data.particles)
 
@@ -188,7 +189,8 @@ def test_particle_splitting(steps):
     for c in range(P.MAX_COLORS):
         prm.particleSplitEnergy[c] = 2.0
     got, ref, _ = run_both(data, world, prm, steps, 0, precision="f64")
-    assert len(ref.particles) > len(data.particles), "no particle split"
+    new_ids = ref.particles["id"] > max(int(data.cells["id"].max()), int(data.particles["id"].max()))
+    assert np.count_nonzero(new_ids) > 0, "no particle split"
     compare_cells(got.cells, ref.cells, world, before=data.cells)
     compare_particles(got.particles, ref.particles, world, before=data.particles)
 

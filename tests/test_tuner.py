@@ -1,10 +1,11 @@
 """The pair kernel's launch configuration and its autotuner.
 
-The pair kernel splits each cell's neighbour candidates across a group of
-2, 4, 8 or 16 lanes and sums in fixed point, so the lane count must change
-no result: worlds stepped with every fixed lane count and with the
-autotuner's choice must agree bit for bit (cells, bonds and particles).
-The autotuner's choice rule is a pure host function, checked on the CPU.
+The pair kernel works on regions of tiles, one CTA each; the region shape
+is one of four candidates per motion type.  A cell's neighbours are visited
+in the same order whatever the shape, so the shape must change no result:
+worlds stepped with every fixed shape and with the autotuner's choice must
+agree bit for bit (cells, bonds and particles).  The autotuner's choice
+rule is a pure host function, checked on the CPU.
 """
 import ctypes
 
@@ -18,28 +19,28 @@ from alien_b200 import worldgen
 
 def choose(ms):
     lib = _lib.load()
-    arr = (ctypes.c_float * len(ms))(*ms)
-    return lib.alien_b200_choose_pair_lanes(arr, len(ms))
+    arr = (ctypes.c_float * max(len(ms), 1))(*ms)
+    return lib.alien_b200_choose_region(arr, len(ms))
 
 
 def test_choice_rule():
-    assert choose([1.0, 0.9, 0.95, 1.2]) == 4
-    assert choose([1.0, 0.99, 0.985, 0.5]) == 16
-    # within 2 % of a smaller lane count: the smaller one stays
-    assert choose([1.0, 0.99, 1.0, 1.0]) == 2
-    assert choose([1.0, 0.97, 0.96, 0.955]) == 4
-    # nothing measured: the default
-    assert choose([0.0, 0.0, 0.0, 0.0]) == 4
-    assert choose([-1.0, 2.0, 0.0, 0.0]) == 4
-    assert choose([]) == 4
+    assert choose([1.0, 0.9, 0.95, 1.2]) == 1
+    assert choose([1.0, 0.99, 0.985, 0.5]) == 3
+    # within 2 % of an earlier candidate: the earlier one stays
+    assert choose([1.0, 0.99, 1.0, 1.0]) == 0
+    assert choose([1.0, 0.97, 0.96, 0.955]) == 1
+    # nothing measured: the default (first) candidate
+    assert choose([0.0, 0.0, 0.0, 0.0]) == 0
+    assert choose([-1.0, 2.0, 0.0, 0.0]) == 1
+    assert choose([]) == 0
 
 
-def _run(data, world, prm, steps, fluid_lanes=0, collision_lanes=0):
+def _run(data, world, prm, steps, fluid_choice=0, collision_choice=0):
     from alien_b200.facade import SimulationFacade
 
     eng = SimulationFacade()
     eng.new_simulation(0, world, prm)
-    eng.set_pair_lanes(fluid_lanes, collision_lanes)
+    eng.set_region_choice(fluid_choice, collision_choice)
     eng.set_simulation_data(data)
     eng.calc_timesteps(steps)
     out = eng.get_simulation_data()
@@ -50,23 +51,24 @@ def _run(data, world, prm, steps, fluid_lanes=0, collision_lanes=0):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("motion", [P.MOTION_FLUID, P.MOTION_COLLISION])
-def test_results_do_not_depend_on_lanes(motion):
-    data, world = worldgen.random_test_world(51, world=(96, 96), free_cells=800, particles=200, vmax=0.9,
+def test_results_do_not_depend_on_region_shape(motion):
+    data, world = worldgen.random_test_world(51, world=(160, 160), free_cells=2000, particles=200, vmax=0.9,
                                              barriers=6)
     prm = P.benchmark_parameters(motion)
     tuned, cfg = _run(data, world, prm, 4)
     assert cfg.tuned == 1
-    assert cfg.pairLanes[motion] in _lib.PAIR_LANE_CHOICES
-    assert all(cfg.tunedMs[motion][i] > 0 for i in range(len(_lib.PAIR_LANE_CHOICES)))
-    for lanes in _lib.PAIR_LANE_CHOICES:
-        fixed, fcfg = _run(data, world, prm, 4, lanes, lanes)
-        assert fcfg.pairLanes[motion] == lanes and fcfg.pairLanesFixed[motion] == lanes
-        assert np.array_equal(fixed.cells, tuned.cells), f"cells differ with {lanes} lanes per cell"
-        assert np.array_equal(fixed.particles, tuned.particles), f"particles differ with {lanes} lanes per cell"
+    assert 0 <= cfg.regionChoice[motion] < _lib.REGION_CHOICES
+    assert all(cfg.tunedMs[motion][i] > 0 for i in range(_lib.REGION_CHOICES))
+    for i in range(_lib.REGION_CHOICES):
+        fixed, fcfg = _run(data, world, prm, 4, i + 1, i + 1)
+        shape = tuple(fcfg.candidates[motion][i])
+        assert fcfg.regionChoice[motion] == i and tuple(fcfg.regionTiles[motion]) == shape
+        assert np.array_equal(fixed.cells, tuned.cells), f"cells differ with regions of {shape} tiles"
+        assert np.array_equal(fixed.particles, tuned.particles), f"particles differ with regions of {shape} tiles"
 
 
 @pytest.mark.gpu
-def test_dense_rows_and_small_worlds_do_not_depend_on_lanes():
+def test_dense_rows_and_small_worlds_do_not_depend_on_region_shape():
     """regions denser than the shared buffer and worlds too small for
     regions defer cells to the overflow kernel; results stay identical"""
     for world_size, cells in (((16, 16), 1500), ((7, 7), 30)):
@@ -74,6 +76,6 @@ def test_dense_rows_and_small_worlds_do_not_depend_on_lanes():
                                                  particles=10, vmax=0.2)
         for motion in (P.MOTION_FLUID, P.MOTION_COLLISION):
             prm = P.benchmark_parameters(motion)
-            ref, _ = _run(data, world, prm, 2, 2, 2)
-            got, _ = _run(data, world, prm, 2, 16, 16)
+            ref, _ = _run(data, world, prm, 2, 1, 1)
+            got, _ = _run(data, world, prm, 2, 4, 4)
             assert np.array_equal(ref.cells, got.cells) and np.array_equal(ref.particles, got.particles)
