@@ -112,8 +112,9 @@ struct DevState {
     unsigned long long* id;
     float2* posA;     // position at the start of the step (FP32 state between steps)
     float2* posB;     // position after the overlap push of the pair phase
-    float2* dpos;     // displacement since the step start: the overlap push, then plus the
-                      // Verlet increment; folded into posA by the next step's binning
+    float2* push;     // overlap push of the pair phase (displacement before the Verlet update)
+    float2* dpos;     // displacement since the step start after the Verlet update (push plus
+                      // the Verlet increment); folded into posA by the next step's binning
     float2* velA;
     float2* velB;
     float* energy;

@@ -525,6 +525,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     s.id = mem_.alloc<unsigned long long>(C);
     s.posA = mem_.alloc<float2>(C);
     s.posB = mem_.alloc<float2>(C);
+    s.push = mem_.alloc<float2>(C);
     s.dpos = mem_.alloc<float2>(C);
     s.velA = mem_.alloc<float2>(C);
     s.velB = mem_.alloc<float2>(C);
@@ -1173,7 +1174,9 @@ AlienLaunchConfig Arena::launchConfig() const
 // only the staged records and overwrites its own outputs, which the next
 // step recomputes, and a cell's neighbours are visited in the same order
 // whatever the region shape, so tuning changes neither the state nor any
-// result.  Runs once per arena layout, before the step graph is captured.
+// result.  Runs once per
+// arena layout, before its first step and before the step graph is
+// captured.
 void Arena::autotune()
 {
     tuned_ = true;

@@ -564,7 +564,7 @@ struct FluidLaw {
         F = F + (Fp * p->pressureStrength + Fv * p->viscosityStrength);
         st.force[g] = F;
         st.posB[g] = pi + dx;
-        st.dpos[g] = dx;
+        st.push[g] = dx;
         st.densNew[g] = dens;
         st.best[g] = best;
     }
@@ -691,7 +691,7 @@ struct CollisionLaw {
         const DevState& st = *s;
         st.force[g] = F;
         st.posB[g] = pi + dx;
-        st.dpos[g] = dx;
+        st.push[g] = dx;
         st.densNew[g] = densI;
         st.best[g] = best;
     }
@@ -1055,12 +1055,14 @@ struct BondRow {
 
 // the bond vectors at the step's current positions: the minimal-image
 // difference of the step-start positions (exact for partners, also across
-// the seam) plus the difference of the in-step displacements
-__device__ __forceinline__ void loadBondRow(const DevState& s, long long g, int n, int W, int H, BondRow& r)
+// the seam) plus the difference of the in-step displacements D (the overlap
+// push before the Verlet update, the total displacement after it)
+__device__ __forceinline__ void loadBondRow(const DevState& s, long long g, int n, const float2* __restrict__ D, int W, int H,
+                                            BondRow& r)
 {
     r.n = n;
     const int2* row = reinterpret_cast<const int2*>(s.bond + g * kMaxBonds);
-    const float2 pi = s.posA[g], di = s.dpos[g];
+    const float2 pi = s.posA[g], di = D[g];
 #pragma unroll
     for (int h = 0; h < kMaxBonds / 2; ++h) {
         const int2 jj = 2 * h < r.n ? row[h] : make_int2(0, 0);
@@ -1071,7 +1073,7 @@ __device__ __forceinline__ void loadBondRow(const DevState& s, long long g, int 
 #pragma unroll
     for (int k = 0; k < kMaxBonds; ++k) {
         pj[k] = k < r.n ? s.posA[r.j[k]] : pi;
-        dj[k] = k < r.n ? s.dpos[r.j[k]] : di;
+        dj[k] = k < r.n ? D[r.j[k]] : di;
     }
 #pragma unroll
     for (int k = 0; k < kMaxBonds; ++k) r.disp[k] = seamDiff2(pj[k], pi, W, H) + (dj[k] - di);
@@ -1183,7 +1185,7 @@ __device__ __forceinline__ float2 bondForce(const DevState& s, long long g, cons
 }
 
 // verletPositionUpdate (CellProcessor.cuh:525-544) of cell g as an
-// increment: its displacement after the overlap push (dpos) plus
+// increment: its overlap push plus
 // v * dt + F * dt^2 / 2 with the bond force F1 and the fixed-point angle
 // forces (ax, ay); stores the total force of a non-barrier cell and returns
 // the cell's displacement since the step start.  The position itself is
@@ -1192,7 +1194,7 @@ __device__ __forceinline__ float2 verletIncrement(const DevState& s, long long g
                                                   float2 v, float2 F1, long long ax, long long ay)
 {
     const float dt = p.timestepSize;
-    const float2 d = s.dpos[g];
+    const float2 d = s.push[g];
     if (barrierG) {
         s.force1[g] = F1;
         return d + v * dt;
@@ -1233,7 +1235,7 @@ __global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
             s.velA[g] = v;
         }
         BondRow r;
-        loadBondRow(s, g, n, wi.W, wi.H, r);
+        loadBondRow(s, g, n, s.push, wi.W, wi.H, r);
         const float2 F1 = bondForce(s, g, r, T % 3 == 0, p.cellMinDistance, 0, kTriStore);
         if (T % 3 == 0) {
             s.force1[g] = F1;  // angle forces of other cells still arrive: kVerletPos
@@ -1314,7 +1316,7 @@ __global__ void __launch_bounds__(kBlock, 6) kBond2(DevState s)
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
         const uint64_t T = s.counters[c.w].timestep;
         BondRow r;
-        loadBondRow(s, g, n, wi.W, wi.H, r);
+        loadBondRow(s, g, n, s.dpos, wi.W, wi.H, r);
         if (!barrierG) {
             const float maxDist = p.cellMaxBindingDistance[col];
             bool destroy = false;
