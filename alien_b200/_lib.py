@@ -8,7 +8,7 @@ from __future__ import annotations
 import ctypes
 import os
 
-from .params import PhysicsParams
+from .params import MAX_COLORS, PhysicsParams
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libalien_b200.so")
@@ -55,6 +55,42 @@ class RawStatistics(ctypes.Structure):
     ]
 
 
+MAX_HISTOGRAM_SLOTS = 20
+_C7 = MAX_COLORS
+
+
+class TimestepStatistics(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32 * _C7) for n in ("numCells", "numSelfReplicators", "numColonies", "numViruses",
+                                                    "numFreeCells", "numParticles")] + [
+        ("numGenomeCells", ctypes.c_uint64 * _C7),
+        ("genomeComplexity", ctypes.c_float * _C7),
+        ("maxGenomeComplexityOfColonies", ctypes.c_float * _C7),
+        ("genomeComplexityVariance", ctypes.c_double * _C7),
+        ("totalEnergy", ctypes.c_float * _C7),
+    ]
+
+
+class AccumulatedStatistics(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64 * _C7) for n in (
+        "numCreatedCells", "numCreatedReplicators", "numAttacks", "numMuscleActivities", "numDefenderActivities",
+        "numTransmitterActivities", "numInjectionActivities", "numCompletedInjections", "numNervePulses",
+        "numNeuronActivities", "numSensorActivities", "numSensorMatches", "numReconnectorCreated",
+        "numReconnectorRemoved", "numDetonations")]
+
+
+class TimelineStatistics(ctypes.Structure):
+    _fields_ = [("timestep", TimestepStatistics), ("accumulated", AccumulatedStatistics)]
+
+
+class HistogramData(ctypes.Structure):
+    _fields_ = [("maxValue", ctypes.c_int32), ("numCellsByColorBySlot", (ctypes.c_int32 * MAX_HISTOGRAM_SLOTS) * _C7)]
+
+
+class RawStatisticsData(ctypes.Structure):
+    """AlienRawStatisticsData = RawStatisticsData (EngineInterface/RawStatisticsData.h)"""
+    _fields_ = [("timeline", TimelineStatistics), ("histogram", HistogramData)]
+
+
 REGION_CHOICES = 4
 
 
@@ -87,6 +123,8 @@ EXPORTED_SYMBOLS = [
     "alien_b200_batch_device_bytes", "alien_b200_statistics_no_alloc", "alien_b200_batch_synchronize",
     "alien_b200_debug_cell_map", "alien_b200_set_launch_config", "alien_b200_get_launch_config",
     "alien_b200_choose_region", "alien_b200_batch_set_launch_config", "alien_b200_batch_get_launch_config",
+    "alien_b200_get_raw_statistics_data", "alien_b200_reset_time_interval_statistics",
+    "alien_b200_batch_get_raw_statistics_data", "alien_b200_batch_reset_time_interval_statistics",
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -152,6 +190,10 @@ def load() -> ctypes.CDLL:
     lib.alien_b200_batch_get_launch_config.argtypes = [vp, P(LaunchConfig)]
     lib.alien_b200_choose_region.argtypes = [P(ctypes.c_float), i32]
     lib.alien_b200_choose_region.restype = i32
+    lib.alien_b200_get_raw_statistics_data.argtypes = [vp, P(RawStatisticsData)]
+    lib.alien_b200_reset_time_interval_statistics.argtypes = [vp]
+    lib.alien_b200_batch_get_raw_statistics_data.argtypes = [vp, i32, P(RawStatisticsData)]
+    lib.alien_b200_batch_reset_time_interval_statistics.argtypes = [vp, i32]
     lib.alien_b200_select_device.argtypes = [i32]
     lib.alien_b200_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]
     lib.alien_b200_batch_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]

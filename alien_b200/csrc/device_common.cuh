@@ -111,7 +111,6 @@ struct DevState {
     // cells
     unsigned long long* id;
     float2* posA;     // position at the start of the step (FP32 state between steps)
-    float2* posB;     // position after the overlap push of the pair phase
     float2* push;     // overlap push of the pair phase (displacement before the Verlet update)
     float2* dpos;     // displacement since the step start after the Verlet update (push plus
                       // the Verlet increment); folded into posA by the next step's binning
@@ -186,6 +185,9 @@ struct DevState {
     float2* splitVel;
     float* splitEnergy;
     int* pmap;            // per-world dense particle maps (-1 = empty)
+
+    // accumulated statistics, per world and color: neuron cells that ran
+    unsigned long long* neuronActivity;
 
     // event scan scratch (per block)
     uint32_t* blockRad;

@@ -198,6 +198,8 @@ public:
     void getData(int w, bool useRect, AlienInt2 ul, AlienInt2 lr, const AlienDataTO* out);
     void countData(int w, uint64_t* cells, uint64_t* particles);
     AlienRawStatistics statistics(int w);
+    AlienRawStatisticsData statisticsData(int w);
+    void resetTimeIntervalStatistics(int w);
     void setTimestep(int w, uint64_t t);
     void setStepBudget(int w, uint64_t steps);
     void compactParticles(int w);
@@ -277,6 +279,7 @@ private:
     std::vector<HostWorld> worlds_;
     DevState s_{};
     StatsAcc* stats_ = nullptr;
+    TimelineAcc* timeline_ = nullptr;
     AlienCellTO* cold_ = nullptr;
     int* rankCells_ = nullptr;
     int* rankParts_ = nullptr;
@@ -524,7 +527,6 @@ void Arena::build(const std::vector<WorldSetup>& setups)
 
     s.id = mem_.alloc<unsigned long long>(C);
     s.posA = mem_.alloc<float2>(C);
-    s.posB = mem_.alloc<float2>(C);
     s.push = mem_.alloc<float2>(C);
     s.dpos = mem_.alloc<float2>(C);
     s.velA = mem_.alloc<float2>(C);
@@ -595,6 +597,8 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     s.blockSplit = mem_.alloc<uint32_t>(partBlocks);
 
     stats_ = mem_.alloc<StatsAcc>(n);
+    timeline_ = mem_.alloc<TimelineAcc>(1);
+    s.neuronActivity = mem_.alloc<unsigned long long>(static_cast<size_t>(n) * ALIEN_B200_MAX_COLORS);
     cold_ = mem_.alloc<AlienCellTO>(static_cast<size_t>(coldTotal));
     s.cold = cold_;
     s.fnInfo = nullptr;
@@ -656,6 +660,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     AB_CK(cudaMemsetAsync(s.flags, 0, C * sizeof(uint32_t), stream_));
     AB_CK(cudaMemsetAsync(s.angleAcc, 0, C * 4 * sizeof(long long), stream_));
     AB_CK(cudaMemsetAsync(s.dpos, 0, C * sizeof(float2), stream_));
+    AB_CK(cudaMemsetAsync(s.neuronActivity, 0, sizeof(unsigned long long) * n * ALIEN_B200_MAX_COLORS, stream_));
     AB_CK(cudaMemsetAsync(s.energyAcc, 0, C * sizeof(long long), stream_));
     AB_CK(cudaMemsetAsync(s.newPartner, 0xff, C * sizeof(int), stream_));
     AB_CK(cudaMemsetAsync(s.best, 0xff, C * sizeof(int), stream_));
@@ -886,7 +891,14 @@ void Arena::rebuildFromHost(const std::vector<std::vector<AlienCellTO>>& cells, 
         ws.numAux = old[w].auxSize;
         ws.extraParticles = extra[w];
     }
+    std::vector<unsigned long long> neurons(old.size() * ALIEN_B200_MAX_COLORS);
+    AB_CK(cudaMemcpyAsync(neurons.data(), s_.neuronActivity, sizeof(unsigned long long) * neurons.size(), cudaMemcpyDeviceToHost,
+                          stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
     build(setups);
+    // the accumulated statistics belong to the worlds, not to the layout
+    AB_CK(cudaMemcpyAsync(s_.neuronActivity, neurons.data(), sizeof(unsigned long long) * neurons.size(), cudaMemcpyHostToDevice,
+                          stream_));
     // ids continue where they were, not at max(id)+1 of the surviving objects
     std::vector<WorldCounters> now = readCounters();
     for (size_t w = 0; w < old.size(); ++w) {
@@ -1250,6 +1262,43 @@ uint64_t Arena::cellMap(uint64_t capacity, uint64_t* ids, uint32_t* slots, uint3
         AB_CK(cudaFreeAsync(p, stream_));
     AB_CK(cudaStreamSynchronize(stream_));
     return total;
+}
+
+AlienRawStatisticsData Arena::statisticsData(int w)
+{
+    AB_CK(cudaMemsetAsync(timeline_, 0, sizeof(TimelineAcc), stream_));
+    const WorldInfo& wi = worlds_[w].info;
+    const long long slots = std::max(wi.cellCap, wi.partCap);
+    const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>(statsGrid_, (slots + kBlock - 1) / kBlock)));
+    launch(kStatsTimeline, grid, kBlock, s_, w, timeline_);
+    launch(kStatsHistogram, grid, kBlock, s_, w, timeline_);
+    TimelineAcc a;
+    AB_CK(cudaMemcpyAsync(&a, timeline_, sizeof(a), cudaMemcpyDeviceToHost, stream_));
+    unsigned long long neurons[ALIEN_B200_MAX_COLORS];
+    AB_CK(cudaMemcpyAsync(neurons, s_.neuronActivity + static_cast<size_t>(w) * ALIEN_B200_MAX_COLORS, sizeof(neurons),
+                          cudaMemcpyDeviceToHost, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+    AlienRawStatisticsData r;
+    std::memset(&r, 0, sizeof(r));
+    AlienTimestepStatistics& t = r.timeline.timestep;
+    for (int c = 0; c < ALIEN_B200_MAX_COLORS; ++c) {
+        t.numCells[c] = static_cast<int32_t>(a.cells[c]);
+        t.numFreeCells[c] = static_cast<int32_t>(a.freeCells[c]);
+        t.numParticles[c] = static_cast<int32_t>(a.particles[c]);
+        t.totalEnergy[c] = static_cast<float>(static_cast<double>(a.energyFix[c]) / 65536.0);
+        r.timeline.accumulated.numNeuronActivities[c] = neurons[c];
+        for (int k = 0; k < ALIEN_B200_MAX_HISTOGRAM_SLOTS; ++k)
+            r.histogram.numCellsByColorBySlot[c][k] = static_cast<int32_t>(a.histogram[c][k]);
+    }
+    r.histogram.maxValue = static_cast<int32_t>(a.maxAge);
+    return r;
+}
+
+void Arena::resetTimeIntervalStatistics(int w)
+{
+    AB_CK(cudaMemsetAsync(s_.neuronActivity + static_cast<size_t>(w) * ALIEN_B200_MAX_COLORS, 0,
+                          sizeof(unsigned long long) * ALIEN_B200_MAX_COLORS, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
 }
 
 AlienRawStatistics Arena::statistics(int w)
@@ -1655,7 +1704,40 @@ int alien_b200_get_launch_config(alien_b200_simulation* sim, AlienLaunchConfig* 
     });
 }
 
+int alien_b200_get_raw_statistics_data(alien_b200_simulation* sim, AlienRawStatisticsData* statistics)
+{
+    return guarded([&] {
+        if (!sim || !statistics) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        *statistics = sim->arena->statisticsData(0);
+    });
+}
+
+int alien_b200_reset_time_interval_statistics(alien_b200_simulation* sim)
+{
+    return guarded([&] {
+        if (!sim) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
+        sim->arena->resetTimeIntervalStatistics(0);
+    });
+}
+
 // ------------------------------------------------------------- batch -----
+int alien_b200_batch_get_raw_statistics_data(alien_b200_batch* b, int world, AlienRawStatisticsData* statistics)
+{
+    return guarded([&] {
+        if (!b || !statistics || world < 0 || world >= b->arena->numWorlds())
+            throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        *statistics = b->arena->statisticsData(world);
+    });
+}
+
+int alien_b200_batch_reset_time_interval_statistics(alien_b200_batch* b, int world)
+{
+    return guarded([&] {
+        if (!b || world < 0 || world >= b->arena->numWorlds()) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        b->arena->resetTimeIntervalStatistics(world);
+    });
+}
+
 int alien_b200_batch_set_launch_config(alien_b200_batch* b, const AlienLaunchConfig* config)
 {
     return guarded([&] {

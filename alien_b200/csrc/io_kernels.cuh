@@ -283,6 +283,87 @@ __global__ void __launch_bounds__(kBlock) kCompactParticlesScatter(DevState s, i
 }
 
 // ---- statistics (subset of RawStatisticsData; StatisticsKernels.cu:5-105) ----
+// Timeline and age histogram of world w (RawStatisticsData): counts and
+// fixed-point energies per color, accumulated per block in shared memory and
+// added to `acc` with one atomic per block and field.
+struct TimelineAcc {
+    unsigned long long cells[ALIEN_B200_MAX_COLORS];
+    unsigned long long freeCells[ALIEN_B200_MAX_COLORS];
+    unsigned long long particles[ALIEN_B200_MAX_COLORS];
+    long long energyFix[ALIEN_B200_MAX_COLORS];  // 2^-16 fixed point
+    unsigned int maxAge;                          // of the cells that are not barriers
+    unsigned int pad;
+    unsigned int histogram[ALIEN_B200_MAX_COLORS][ALIEN_B200_MAX_HISTOGRAM_SLOTS];
+};
+constexpr uint32_t kMutationIdForFreeCell = 1;  // Const::MutationIdForFreeCell, CellFunctionConstants.h:176
+
+// StatisticsKernels.cu:12-46 (timestep statistics) and 73-83 (largest age)
+__global__ void __launch_bounds__(kBlock) kStatsTimeline(DevState s, int w, TimelineAcc* acc)
+{
+    __shared__ unsigned long long sh[4][ALIEN_B200_MAX_COLORS];
+    __shared__ unsigned int shMax;
+    if (threadIdx.x < 4 * ALIEN_B200_MAX_COLORS) (&sh[0][0])[threadIdx.x] = 0;
+    if (threadIdx.x == 0) shMax = 0;
+    __syncthreads();
+    const WorldInfo& wi = s.worlds[w];
+    const WorldCounters& wc = s.counters[w];
+    const long long stride = static_cast<long long>(gridDim.x) * kBlock;
+    unsigned int myMax = 0;
+    for (long long g = wi.cellBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x; g < wi.cellBase + wc.numCells;
+         g += stride) {
+        if (!s.alive[g]) continue;
+        const int col = s.color[g] % ALIEN_B200_MAX_COLORS;
+        atomicAdd(&sh[0][col], 1ull);
+        if (s.cold[s.coldIdx[g]].mutationId == kMutationIdForFreeCell) atomicAdd(&sh[1][col], 1ull);
+        atomicAdd(&sh[3][col], static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(s.energy[g]) * 65536.0)));
+        if (!s.barrier[g]) myMax = max(myMax, s.age[g]);
+    }
+    for (long long q = wi.partBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x; q < wi.partBase + wc.numParticles;
+         q += stride) {
+        if (!s.palive[q]) continue;
+        const int col = s.pcolor[q] % ALIEN_B200_MAX_COLORS;
+        atomicAdd(&sh[2][col], 1ull);
+        atomicAdd(&sh[3][col], static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(s.penergy[q]) * 65536.0)));
+    }
+    atomicMax(&shMax, myMax);
+    __syncthreads();
+    if (threadIdx.x < 4 * ALIEN_B200_MAX_COLORS) {
+        const int f = threadIdx.x / ALIEN_B200_MAX_COLORS, c = threadIdx.x % ALIEN_B200_MAX_COLORS;
+        const unsigned long long v = sh[f][c];
+        if (v) {
+            unsigned long long* dst = f == 0 ? &acc->cells[c]
+                                     : f == 1 ? &acc->freeCells[c]
+                                     : f == 2 ? &acc->particles[c]
+                                              : reinterpret_cast<unsigned long long*>(&acc->energyFix[c]);
+            atomicAdd(dst, v);
+        }
+    }
+    if (threadIdx.x == 0 && shMax) atomicMax(&acc->maxAge, shMax);
+}
+
+// StatisticsKernels.cu:90-105: age histogram with the largest age of kStatsTimeline
+__global__ void __launch_bounds__(kBlock) kStatsHistogram(DevState s, int w, TimelineAcc* acc)
+{
+    __shared__ unsigned int sh[ALIEN_B200_MAX_COLORS][ALIEN_B200_MAX_HISTOGRAM_SLOTS];
+    for (int i = threadIdx.x; i < ALIEN_B200_MAX_COLORS * ALIEN_B200_MAX_HISTOGRAM_SLOTS; i += kBlock) (&sh[0][0])[i] = 0;
+    __syncthreads();
+    const WorldInfo& wi = s.worlds[w];
+    const WorldCounters& wc = s.counters[w];
+    const unsigned long long maxAge = acc->maxAge;
+    const long long stride = static_cast<long long>(gridDim.x) * kBlock;
+    for (long long g = wi.cellBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x; g < wi.cellBase + wc.numCells;
+         g += stride) {
+        if (!s.alive[g] || s.barrier[g]) continue;
+        const int slot = static_cast<int>(static_cast<unsigned long long>(s.age[g]) * ALIEN_B200_MAX_HISTOGRAM_SLOTS / (maxAge + 1));
+        atomicAdd(&sh[s.color[g] % ALIEN_B200_MAX_COLORS][slot], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < ALIEN_B200_MAX_COLORS * ALIEN_B200_MAX_HISTOGRAM_SLOTS; i += kBlock) {
+        const unsigned int v = (&sh[0][0])[i];
+        if (v) atomicAdd(&(&acc->histogram[0][0])[i], v);
+    }
+}
+
 struct StatsAcc {
     unsigned long long numCells, numParticles, numConnections;
     unsigned long long numCellsByColor[ALIEN_B200_MAX_COLORS];

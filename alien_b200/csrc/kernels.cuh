@@ -563,7 +563,6 @@ struct FluidLaw {
         }
         F = F + (Fp * p->pressureStrength + Fv * p->viscosityStrength);
         st.force[g] = F;
-        st.posB[g] = pi + dx;
         st.push[g] = dx;
         st.densNew[g] = dens;
         st.best[g] = best;
@@ -690,7 +689,6 @@ struct CollisionLaw {
     {
         const DevState& st = *s;
         st.force[g] = F;
-        st.posB[g] = pi + dx;
         st.push[g] = dx;
         st.densNew[g] = densI;
         st.best[g] = best;
@@ -1434,7 +1432,8 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletVel(DevState s)
             if (s.barrier[cell]) {
                 const float2 vc = s.velA[cell];
                 const float2 vr = pv - vc;
-                const float2 r = seamDiff2(pp, s.posB[cell], wi.W, wi.H);
+                // the cell where the particle phase finds it: after the overlap push
+                const float2 r = seamDiff2(pp, s.posA[cell], wi.W, wi.H) - s.push[cell];
                 const float dvr = dot2(vr, r);
                 if (dvr < 0.0f) {
                     const float trr = fmaxf(0.1f, lensq2(r));
@@ -1721,6 +1720,11 @@ __global__ void __launch_bounds__(kBlock) kNeuron(DevState s)
     me.signal.origin = origin;
     me.signal.targetX = tx;
     me.signal.targetY = ty;
+    // statistics.incNumNeuronActivities (NeuronProcessor.cuh:70): one atomic
+    // per warp, world and color
+    const unsigned key = static_cast<unsigned>(w) * ALIEN_B200_MAX_COLORS + s.color[g] % ALIEN_B200_MAX_COLORS;
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&s.neuronActivity[key], static_cast<unsigned long long>(__popc(peers)));
 }
 
 // -------------------------------------------------------- kSignalReset ----

@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import ArraySizes, GeneralSettings, Int2, LaunchConfig, RawStatistics, check
+from ._lib import ArraySizes, GeneralSettings, Int2, LaunchConfig, RawStatistics, RawStatisticsData, check
 from .params import PhysicsParams
 from .to import CELL_TO, PARTICLE_TO, DataTO
 
@@ -123,6 +123,16 @@ class SimulationFacade:
         check(self._lib.alien_b200_get_raw_statistics(self._handle(), ctypes.byref(r)))
         return r
 
+    def get_raw_statistics_data(self) -> RawStatisticsData:
+        """RawStatisticsData: timeline of this timestep, accumulated counts, age histogram"""
+        r = RawStatisticsData()
+        check(self._lib.alien_b200_get_raw_statistics_data(self._handle(), ctypes.byref(r)))
+        return r
+
+    # resetTimeIntervalStatistics (SimulationFacade.h)
+    def reset_time_interval_statistics(self) -> None:
+        check(self._lib.alien_b200_reset_time_interval_statistics(self._handle()))
+
     def launch_config(self) -> LaunchConfig:
         """pair-kernel region shapes in use, and the autotuner's timings"""
         c = LaunchConfig()
@@ -216,6 +226,14 @@ class BatchSimulation:
                      particle_capacity=s.particleArraySize, aux_capacity=s.auxiliaryDataSize)
         check(self._lib.alien_b200_batch_get_data(self._h, int(world), ctypes.cast(out.c_ptr(), ctypes.c_void_p)))
         return out
+
+    def get_raw_statistics_data(self, world: int) -> RawStatisticsData:
+        r = RawStatisticsData()
+        check(self._lib.alien_b200_batch_get_raw_statistics_data(self._h, int(world), ctypes.byref(r)))
+        return r
+
+    def reset_time_interval_statistics(self, world: int) -> None:
+        check(self._lib.alien_b200_batch_reset_time_interval_statistics(self._h, int(world)))
 
     def get_raw_statistics(self, world: int) -> RawStatistics:
         r = RawStatistics()

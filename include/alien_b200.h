@@ -249,6 +249,59 @@ typedef struct AlienRawStatistics {
     double totalParticleEnergy;
 } AlienRawStatistics;
 
+/* RawStatisticsData (EngineInterface/RawStatisticsData.h:5-56), byte for
+ * byte: the timeline of the current timestep, the statistics accumulated
+ * since the last alien_b200_reset_time_interval_statistics, and the age
+ * histogram.  Fields that count cell functions outside the physics stage
+ * (self-replicators, colonies, viruses, genome sizes and complexity,
+ * constructor, attacker, muscle, ... activities) are 0: the engine accepts
+ * no cell carrying those functions. */
+#define ALIEN_B200_MAX_HISTOGRAM_SLOTS 20    /* EngineConstants.h:9 */
+typedef struct AlienTimestepStatistics {
+    int32_t numCells[ALIEN_B200_MAX_COLORS];
+    int32_t numSelfReplicators[ALIEN_B200_MAX_COLORS];
+    int32_t numColonies[ALIEN_B200_MAX_COLORS];
+    int32_t numViruses[ALIEN_B200_MAX_COLORS];
+    int32_t numFreeCells[ALIEN_B200_MAX_COLORS];     /* cells with mutationId 1 (Const::MutationIdForFreeCell) */
+    int32_t numParticles[ALIEN_B200_MAX_COLORS];
+    uint64_t numGenomeCells[ALIEN_B200_MAX_COLORS];
+    float genomeComplexity[ALIEN_B200_MAX_COLORS];
+    float maxGenomeComplexityOfColonies[ALIEN_B200_MAX_COLORS];
+    double genomeComplexityVariance[ALIEN_B200_MAX_COLORS];
+    float totalEnergy[ALIEN_B200_MAX_COLORS];        /* cells and energy particles of the color */
+} AlienTimestepStatistics;
+typedef struct AlienAccumulatedStatistics {
+    uint64_t numCreatedCells[ALIEN_B200_MAX_COLORS];
+    uint64_t numCreatedReplicators[ALIEN_B200_MAX_COLORS];
+    uint64_t numAttacks[ALIEN_B200_MAX_COLORS];
+    uint64_t numMuscleActivities[ALIEN_B200_MAX_COLORS];
+    uint64_t numDefenderActivities[ALIEN_B200_MAX_COLORS];
+    uint64_t numTransmitterActivities[ALIEN_B200_MAX_COLORS];
+    uint64_t numInjectionActivities[ALIEN_B200_MAX_COLORS];
+    uint64_t numCompletedInjections[ALIEN_B200_MAX_COLORS];
+    uint64_t numNervePulses[ALIEN_B200_MAX_COLORS];
+    uint64_t numNeuronActivities[ALIEN_B200_MAX_COLORS]; /* neuron cells that ran (NeuronProcessor.cuh:70) */
+    uint64_t numSensorActivities[ALIEN_B200_MAX_COLORS];
+    uint64_t numSensorMatches[ALIEN_B200_MAX_COLORS];
+    uint64_t numReconnectorCreated[ALIEN_B200_MAX_COLORS];
+    uint64_t numReconnectorRemoved[ALIEN_B200_MAX_COLORS];
+    uint64_t numDetonations[ALIEN_B200_MAX_COLORS];
+} AlienAccumulatedStatistics;
+typedef struct AlienTimelineStatistics {
+    AlienTimestepStatistics timestep;
+    AlienAccumulatedStatistics accumulated;
+} AlienTimelineStatistics;
+/* ages of the cells that are not barriers: maxValue = the largest age,
+ * slot = age * 20 / (maxValue + 1) (StatisticsKernels.cu:85-105) */
+typedef struct AlienHistogramData {
+    int32_t maxValue;
+    int32_t numCellsByColorBySlot[ALIEN_B200_MAX_COLORS][ALIEN_B200_MAX_HISTOGRAM_SLOTS];
+} AlienHistogramData;
+typedef struct AlienRawStatisticsData {
+    AlienTimelineStatistics timeline;
+    AlienHistogramData histogram;
+} AlienRawStatisticsData;
+
 typedef struct alien_b200_simulation alien_b200_simulation;
 
 /* library / defaults */
@@ -278,6 +331,14 @@ int alien_b200_get_current_timestep(alien_b200_simulation* sim, uint64_t* timest
 int alien_b200_set_current_timestep(alien_b200_simulation* sim, uint64_t timestep);
 int alien_b200_clear(alien_b200_simulation* sim);
 int alien_b200_get_raw_statistics(alien_b200_simulation* sim, AlienRawStatistics* statistics);
+/* _SimulationCudaFacade::getRawStatistics (SimulationCudaFacade.cu:420-440)
+ * with the reference's RawStatisticsData layout, computed at the call (the
+ * reference refreshes it at most every 30 ms of stepping and at the end of
+ * calcTimestep); energies are 2^-16 fixed-point sums, independent of order. */
+int alien_b200_get_raw_statistics_data(alien_b200_simulation* sim, AlienRawStatisticsData* statistics);
+/* resetTimeIntervalStatistics (SimulationCudaFacade.cu:452-455): clears the
+ * accumulated statistics. */
+int alien_b200_reset_time_interval_statistics(alien_b200_simulation* sim);
 
 /* Device-resident timing hook: steps `timesteps` times on the handle's
  * stream without the end-of-call synchronisation and error read-back that
@@ -416,5 +477,13 @@ ALIEN_B200_STATIC_ASSERT(offsetof(AlienParticleTO, color) == 32, "ParticleTO.col
 ALIEN_B200_STATIC_ASSERT(offsetof(AlienSignalTO, targetX) == 36, "SignalTO.targetX");
 ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellMetadataTO, nameDataIndex) == 8, "CellMetadataTO.nameDataIndex");
 ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellMetadataTO, descriptionDataIndex) == 24, "CellMetadataTO.descriptionDataIndex");
+ALIEN_B200_STATIC_ASSERT(sizeof(AlienTimestepStatistics) == 368, "TimestepStatistics is 368 bytes");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienTimestepStatistics, numGenomeCells) == 168, "TimestepStatistics.numGenomeCells");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienTimestepStatistics, genomeComplexityVariance) == 280, "TimestepStatistics.genomeComplexityVariance");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienTimestepStatistics, totalEnergy) == 336, "TimestepStatistics.totalEnergy");
+ALIEN_B200_STATIC_ASSERT(sizeof(AlienAccumulatedStatistics) == 840, "AccumulatedStatistics is 840 bytes");
+ALIEN_B200_STATIC_ASSERT(sizeof(AlienHistogramData) == 564, "HistogramData is 564 bytes");
+ALIEN_B200_STATIC_ASSERT(offsetof(AlienRawStatisticsData, histogram) == 1208, "RawStatisticsData.histogram");
+ALIEN_B200_STATIC_ASSERT(sizeof(AlienRawStatisticsData) == 1776, "RawStatisticsData is 1776 bytes");
 
 #endif /* ALIEN_B200_H */

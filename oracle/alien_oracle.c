@@ -244,6 +244,7 @@ typedef struct OracleWorld {
     int32_t* pslot;
     uint8_t* pincoming;
     real *mergeE, *mergeMx, *mergeMy;
+    uint64_t neuronActivity[ALIEN_B200_MAX_COLORS]; /* neuron cells that ran (statistics) */
 } OracleWorld;
 
 #define XALLOC(ptr, n) ((ptr) = calloc((size_t)((n) > 0 ? (n) : 1), sizeof(*(ptr))))
@@ -1127,6 +1128,7 @@ static void neuronPhase(OracleWorld* w, uint64_t T)
         me->signal.origin = origin;
         me->signal.targetX = (float)tx;
         me->signal.targetY = (float)ty;
+        ++w->neuronActivity[w->color[i] % ALIEN_B200_MAX_COLORS]; /* NeuronProcessor.cuh:70 */
     }
 }
 
@@ -1426,6 +1428,12 @@ int64_t oracle_cell_slots(OracleWorld* w, int32_t* out, int64_t cap)
             ++n;
         }
     return n;
+}
+
+/* accumulated neuron activities per color since creation */
+void oracle_neuron_activities(OracleWorld* w, uint64_t* out)
+{
+    for (int c = 0; c < ALIEN_B200_MAX_COLORS; ++c) out[c] = w->neuronActivity[c];
 }
 
 void oracle_set_threads(int n)

@@ -41,6 +41,7 @@ def _load(name: str) -> ctypes.CDLL:
     lib.oracle_cell_slots.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
     lib.oracle_num_threads.restype = ctypes.c_int
     lib.oracle_set_threads.argtypes = [ctypes.c_int]
+    lib.oracle_neuron_activities.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     return lib
 
 
@@ -115,6 +116,12 @@ class OracleSimulation:
         out = DataTO(np.zeros(0, CELL_TO), np.zeros(0, PARTICLE_TO), None, cell_capacity=c,
                      particle_capacity=p, aux_capacity=a)
         self.lib.oracle_get_data(self.h, ctypes.cast(out.c_ptr(), ctypes.c_void_p))
+        return out
+
+    def neuron_activities(self) -> np.ndarray:
+        """neuron cells that ran, per color, since creation"""
+        out = np.zeros(7, np.uint64)
+        self.lib.oracle_neuron_activities(self.h, out.ctypes.data)
         return out
 
     def cell_slots(self) -> np.ndarray:

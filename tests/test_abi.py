@@ -60,3 +60,14 @@ def test_no_device_reports_error_without_fallback():
     h = ctypes.c_void_p()
     rc = lib.alien_b200_create(ctypes.byref(g), ctypes.byref(p), 0, ctypes.byref(h))
     assert rc == 7 and not h
+
+
+def test_raw_statistics_data_layout():
+    """AlienRawStatisticsData mirrors RawStatisticsData byte for byte (ColorVector<T> = T[7],
+    EngineInterface/Colors.h; MAX_HISTOGRAM_SLOTS = 20, EngineConstants.h)"""
+    assert ctypes.sizeof(_lib.TimestepStatistics) == 368
+    assert _lib.TimestepStatistics.numGenomeCells.offset == 168
+    assert _lib.TimestepStatistics.genomeComplexityVariance.offset == 280
+    assert ctypes.sizeof(_lib.AccumulatedStatistics) == 15 * 7 * 8
+    assert _lib.RawStatisticsData.histogram.offset == 1208
+    assert ctypes.sizeof(_lib.RawStatisticsData) == 1776

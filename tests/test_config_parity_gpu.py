@@ -216,3 +216,73 @@ def test_statistics_match_oracle(motion):
     pe = float(np.sum(parts["energy"], dtype=np.float64))
     assert abs(stats.totalCellEnergy - ce) <= 1e-5 * max(ce, 1.0)
     assert abs(stats.totalParticleEnergy - pe) <= 1e-5 * max(pe, 1.0)
+
+
+def _expected_statistics(data, neuron_activities):
+    """RawStatisticsData of a state, computed from its transfer objects
+    (StatisticsKernels.cu:12-46, 73-105)"""
+    cells, parts = data.cells, data.particles
+    col = cells["color"].astype(np.int64) % 7
+    pcol = parts["color"].astype(np.int64) % 7
+    energy = np.zeros(7)
+    np.add.at(energy, col, cells["energy"].astype(np.float64))
+    np.add.at(energy, pcol, parts["energy"].astype(np.float64))
+    ages = cells["age"].astype(np.int64)
+    live = cells["barrier"] == 0
+    max_age = int(ages[live].max()) if np.any(live) else 0
+    hist = np.zeros((7, 20), np.int64)
+    np.add.at(hist, (col[live], ages[live] * 20 // (max_age + 1)), 1)
+    return {
+        "numCells": np.bincount(col, minlength=7),
+        "numFreeCells": np.bincount(col[cells["mutationId"] == 1], minlength=7),
+        "numParticles": np.bincount(pcol, minlength=7),
+        "totalEnergy": energy,
+        "maxValue": max_age,
+        "histogram": hist,
+        "numNeuronActivities": np.asarray(neuron_activities, np.int64),
+    }
+
+
+@pytest.mark.parametrize("motion", [P.MOTION_FLUID, P.MOTION_COLLISION])
+def test_raw_statistics_data_match_oracle(motion):
+    """the full RawStatisticsData after 13 steps of a world with neuron
+    cells, free cells (mutation id 1), barriers, decaying cells and energy
+    particles: counts, histogram and neuron activities exact, energies per
+    color within the one-step tolerance of the state"""
+    data, world = worldgen.calm_test_world(61)
+    data = worldgen.add_neurons(data, 61, fraction=0.5)
+    rng = np.random.default_rng(61)
+    c = data.cells
+    c["mutationId"] = np.where(rng.random(len(c)) < 0.3, 1, 7).astype(np.uint32)
+    c["age"] = rng.integers(0, 500, len(c)).astype(np.uint32)
+    c["color"] = rng.integers(0, 7, len(c)).astype(np.uint8)
+    c["energy"][::13] = 30.0
+    c["barrier"][5:8] = 1
+    prm = P.benchmark_parameters(motion)
+    for i in range(P.MAX_COLORS):
+        prm.cellDeathProbability[i] = 0.2
+    steps = 13
+    eng = SimulationFacade()
+    eng.new_simulation(0, world, prm)
+    eng.set_simulation_data(data)
+    eng.calc_timesteps(steps)
+    got = eng.get_raw_statistics_data()
+    ora = OracleSimulation(world, prm, precision="f64")
+    ora.set_simulation_data(data)
+    ora.calc_timesteps(steps)
+    want = _expected_statistics(ora.get_simulation_data(), ora.neuron_activities())
+    ts = got.timeline.timestep
+    for field in ("numCells", "numFreeCells", "numParticles"):
+        assert list(getattr(ts, field)) == want[field].tolist(), field
+    assert np.sum(want["numFreeCells"]) > 0 and np.sum(want["numParticles"]) > 0
+    e = np.array(list(ts.totalEnergy), np.float64)
+    assert np.all(np.abs(e - want["totalEnergy"]) <= 1e-5 * np.maximum(want["totalEnergy"], 1.0))
+    assert got.histogram.maxValue == want["maxValue"]
+    assert np.array_equal(np.array([list(r) for r in got.histogram.numCellsByColorBySlot]), want["histogram"])
+    acc = np.array(list(got.timeline.accumulated.numNeuronActivities), np.int64)
+    assert np.array_equal(acc, want["numNeuronActivities"]) and acc.sum() > 0
+    for field in ("numSelfReplicators", "numColonies", "numViruses"):
+        assert list(getattr(ts, field)) == [0] * 7
+    eng.reset_time_interval_statistics()
+    assert list(eng.get_raw_statistics_data().timeline.accumulated.numNeuronActivities) == [0] * 7
+    eng.close_simulation()
