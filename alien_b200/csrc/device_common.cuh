@@ -92,6 +92,14 @@ struct WorldCounters {
     // set at ingest: the next step clears the signals of cells without
     // function (after that no step writes them)
     unsigned int signalsFresh;
+    // the external energy pool and this step's backflow into it (2^-24 fixed
+    // point, added to the pool at the end of the step)
+    double externalEnergy;
+    long long backflowFix;
+    // radiation sources active in this step (bit i: source i)
+    unsigned long long activeSources;
+    // the timestep a completed step left (zones and sources move once per step)
+    unsigned long long lastStepped;
 };
 
 struct DevState {
@@ -101,7 +109,7 @@ struct DevState {
     long long numTiles;
     const WorldInfo* worlds;
     WorldCounters* counters;
-    const AlienPhysicsParams* params;
+    AlienPhysicsParams* params;  // zone and source positions move with the steps
     const int* cellBlockWorld;
     const int* partBlockWorld;
     const int* regionWorld;  // world of each pair-phase CTA

@@ -130,13 +130,27 @@ private:
 // parameters the physics stage cannot honour are rejected, not ignored
 static void validateParams(const AlienPhysicsParams& p, int W, int H)
 {
-    if (p.numZones != 0) throw Error(ALIEN_B200_ERR_UNSUPPORTED, "zones (numZones > 0) are outside the physics stage");
-    if (p.numRadiationSources != 0) throw Error(ALIEN_B200_ERR_UNSUPPORTED, "radiation sources are not supported");
+    if (p.numZones < 0 || p.numZones > ALIEN_B200_MAX_ZONES)
+        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "numZones must lie in [0, 20]");
+    if (p.numRadiationSources < 0 || p.numRadiationSources > ALIEN_B200_MAX_RADIATION_SOURCES)
+        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "numRadiationSources must lie in [0, 40]");
     if (p.particleTransformationAllowed)
         throw Error(ALIEN_B200_ERR_UNSUPPORTED, "particle-to-cell transformation is outside the physics stage");
-    if (p.cellAgeLimiter || p.cellColorTransitionRules || p.advancedAbsorptionControl || p.externalEnergyControl)
-        throw Error(ALIEN_B200_ERR_UNSUPPORTED, "feature flags of cell functions / energy control must be off");
+    if (p.cellAgeLimiter || p.cellColorTransitionRules || p.advancedAbsorptionControl)
+        throw Error(ALIEN_B200_ERR_UNSUPPORTED, "feature flags of cell functions (age limiter, color transitions, absorption control) must be off");
     if (p.rigidity != 0.0f) throw Error(ALIEN_B200_ERR_UNSUPPORTED, "rigidity clusters (rigidity != 0) are not supported");
+    for (int i = 0; i < p.numZones; ++i) {
+        const AlienZone& z = p.zones[i];
+        if (z.rigidityActivated && z.rigidity != 0.0f)
+            throw Error(ALIEN_B200_ERR_UNSUPPORTED, "rigidity clusters (a zone with rigidity != 0) are not supported");
+        if (z.shapeType != ALIEN_B200_SHAPE_CIRCULAR && z.shapeType != ALIEN_B200_SHAPE_RECTANGULAR)
+            throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "zone shape type must be 0 (circular) or 1 (rectangular)");
+        if (z.flowType < ALIEN_B200_FLOW_NONE || z.flowType > ALIEN_B200_FLOW_LINEAR)
+            throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "zone flow type must lie in [0, 3]");
+    }
+    for (int i = 0; i < p.numRadiationSources; ++i)
+        if (p.radiationSources[i].shapeType != ALIEN_B200_SHAPE_CIRCULAR && p.radiationSources[i].shapeType != ALIEN_B200_SHAPE_RECTANGULAR)
+            throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "radiation source shape type must be 0 (circular) or 1 (rectangular)");
     if (p.cellNumExecutionOrderNumbers < 1)
         throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "cellNumExecutionOrderNumbers must be at least 1");
     if (p.motionType != ALIEN_B200_MOTION_FLUID && p.motionType != ALIEN_B200_MOTION_COLLISION)
@@ -194,6 +208,10 @@ public:
     void calcTimesteps(uint64_t n);
     void sync();
     void setParams(int w, const AlienPhysicsParams& p);
+    // the parameters as the steps left them: zone and source positions,
+    // the external energy pool
+    AlienPhysicsParams params(int w);
+    void syncParamsFromDevice();
     std::vector<WorldCounters> readCounters();
     void getData(int w, bool useRect, AlienInt2 ul, AlienInt2 lr, const AlienDataTO* out);
     void countData(int w, uint64_t* cells, uint64_t* particles);
@@ -294,6 +312,11 @@ private:
     cudaGraphExec_t graphExec_ = nullptr;
     uint64_t stepsSinceCheck_ = 0;
     bool hasFluid_ = false, hasCollision_ = false, hasNeurons_ = false;
+    bool hasWorldParams_ = false;  // some world has zones, radiation sources or external energy (kWorldsEnd)
+    static bool needsWorldParams(const AlienPhysicsParams& p)
+    {
+        return p.numZones > 0 || p.numRadiationSources > 0 || p.externalEnergyControl;
+    }
     bool tuned_ = false;              // the autotuner ran on this layout
     float tunedMs_[2][kNumRegionChoices] = {};
     void binCurrentState();
@@ -475,8 +498,9 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     }
     hasNeurons_ = neuronsTotal > 0;
     signalsLive_ = hasNeurons_ || signalsTotal > 0;
-    hasFluid_ = hasCollision_ = false;
+    hasFluid_ = hasCollision_ = hasWorldParams_ = false;
     for (const HostWorld& hw : worlds_) {
+        hasWorldParams_ |= needsWorldParams(hw.params);
         if (hw.info.motionType == ALIEN_B200_MOTION_FLUID)
             hasFluid_ = true;
         else
@@ -645,6 +669,8 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         wc.stepsRemaining = ~0ull;
         wc.active = 1;
         wc.signalsFresh = 1;
+        wc.externalEnergy = setups[w].params.externalEnergy;
+        wc.lastStepped = ~0ull;
     }
     AB_CK(cudaMemcpyAsync(worldsDev, infos.data(), sizeof(WorldInfo) * n, cudaMemcpyHostToDevice, stream_));
     AB_CK(cudaMemcpyAsync(paramsDev, params.data(), sizeof(AlienPhysicsParams) * n, cudaMemcpyHostToDevice, stream_));
@@ -682,6 +708,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
         coldBase += nc;
     }
     freeAsyncStage();
+    if (hasWorldParams_) launch(kWorldsBegin, divUp(n, kBlock), kBlock, s);
     sync();
 }
 
@@ -723,6 +750,7 @@ void Arena::enqueueStep()
     launch(kEventCount, both, kBlock, s);
     launch(kEventWorld, s.numWorlds, kEventWorldThreads, s);
     launch(kEventEmit, both, kBlock, s);
+    if (hasWorldParams_) launch(kWorldsEnd, divUp(s.numWorlds, kBlock), kBlock, s);
     kernelsPerStep_ = static_cast<int>(launches_ - before);
 }
 
@@ -865,6 +893,7 @@ void Arena::ensureParticleCapacity()
 void Arena::rebuildFromHost(const std::vector<std::vector<AlienCellTO>>& cells, const std::vector<std::vector<AlienParticleTO>>& parts,
                             const std::vector<uint64_t>& extra)
 {
+    syncParamsFromDevice();  // zones, sources and the pool as the steps left them
     std::vector<WorldCounters> c = readCounters();
     std::vector<HostWorld> old = worlds_;
     std::vector<WorldSetup> setups(old.size());
@@ -951,10 +980,48 @@ void Arena::setParams(int w, const AlienPhysicsParams& p)
         return;
     }
     hw.params = p;
-    AB_CK(cudaMemcpyAsync(const_cast<AlienPhysicsParams*>(s_.params) + w, &p, sizeof(p), cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemcpyAsync(s_.params + w, &p, sizeof(p), cudaMemcpyHostToDevice, stream_));
     // prepareForSimulationParametersChanges -> cudaResetDensity (SimulationKernelsLauncher.cu:93-97)
     launch(kResetDensity, hw.info.numCellBlocks, kBlock, s_, w);
+    // the external energy pool takes the parameters' value, and the active
+    // sources follow the new zones and sources
+    std::vector<WorldCounters> c = readCounters();
+    c[w].externalEnergy = p.externalEnergy;
+    AB_CK(cudaMemcpyAsync(s_.counters + w, &c[w], sizeof(WorldCounters), cudaMemcpyHostToDevice, stream_));
+    bool any = false;
+    for (const HostWorld& x : worlds_) any |= needsWorldParams(x.params);
+    if (any != hasWorldParams_) {
+        hasWorldParams_ = any;
+        releaseGraph();  // the step gains or loses its kWorldsEnd launch
+    }
+    if (hasWorldParams_) launch(kWorldsBegin, divUp(numWorlds(), kBlock), kBlock, s_);
     sync();
+}
+
+void Arena::syncParamsFromDevice()
+{
+    if (!hasWorldParams_ || worlds_.empty()) return;
+    std::vector<AlienPhysicsParams> dev(worlds_.size());
+    AB_CK(cudaMemcpyAsync(dev.data(), s_.params, sizeof(AlienPhysicsParams) * dev.size(), cudaMemcpyDeviceToHost, stream_));
+    std::vector<WorldCounters> c = readCounters();
+    for (size_t w = 0; w < worlds_.size(); ++w) {
+        AlienPhysicsParams& h = worlds_[w].params;
+        for (int i = 0; i < ALIEN_B200_MAX_ZONES; ++i) {
+            h.zones[i].posX = dev[w].zones[i].posX;
+            h.zones[i].posY = dev[w].zones[i].posY;
+        }
+        for (int i = 0; i < ALIEN_B200_MAX_RADIATION_SOURCES; ++i) {
+            h.radiationSources[i].posX = dev[w].radiationSources[i].posX;
+            h.radiationSources[i].posY = dev[w].radiationSources[i].posY;
+        }
+        h.externalEnergy = static_cast<float>(c[w].externalEnergy);
+    }
+}
+
+AlienPhysicsParams Arena::params(int w)
+{
+    syncParamsFromDevice();
+    return worlds_[w].params;
 }
 
 void Arena::setStepBudget(int w, uint64_t steps)
@@ -1465,6 +1532,35 @@ void alien_b200_default_parameters(AlienPhysicsParams* p)
         p->cellMinEnergy[i] = 50.0f;
         p->cellDeathProbability[i] = 0.001f;
     }
+    p->externalEnergyBackflowLimit = 3.4028234663852886e38f;
+    // zones (SimulationParametersZone.h): circular, core and fade-out radius
+    // 100, radial-flow strength 0.001, the base values, nothing activated
+    for (AlienZone& z : p->zones) {
+        z.fadeoutRadius = 100.0f;
+        z.shapeType = ALIEN_B200_SHAPE_CIRCULAR;
+        z.coreRadius = 100.0f;
+        z.width = 100.0f;
+        z.height = 200.0f;
+        z.flowType = ALIEN_B200_FLOW_NONE;
+        z.flowStrength = 0.001f;
+        z.friction = p->friction;
+        z.rigidity = p->rigidity;
+        z.cellFusionVelocity = p->cellFusionVelocity;
+        z.cellMaxBindingEnergy = p->cellMaxBindingEnergy;
+        for (int c = 0; c < ALIEN_B200_MAX_COLORS; ++c) {
+            z.radiationAbsorption[c] = p->radiationAbsorption[c];
+            z.radiationCellAgeStrength[c] = p->radiationCellAgeStrength[c];
+            z.cellMaxForce[c] = p->cellMaxForce[c];
+            z.cellMinEnergy[c] = p->cellMinEnergy[c];
+            z.cellDeathProbability[c] = p->cellDeathProbability[c];
+        }
+    }
+    // radiation sources (RadiationSource.h): circular of radius 1
+    for (AlienRadiationSource& r : p->radiationSources) {
+        r.radius = 1.0f;
+        r.width = 100.0f;
+        r.height = 200.0f;
+    }
 }
 
 int alien_b200_last_error(char* buffer, size_t size)
@@ -1562,7 +1658,7 @@ int alien_b200_set_data(alien_b200_simulation* sim, const AlienDataTO* data)
         if (!sim) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
         checkDataTO(data);
         const uint64_t t = sim->arena->readCounters()[0].timestep;
-        WorldSetup ws = setupFrom(sim->general, sim->params, t, data);
+        WorldSetup ws = setupFrom(sim->general, sim->arena->params(0), t, data);
         ws.extraParticles = sim->extraParticles;
         sim->arena->build({ws});
     });
@@ -1589,7 +1685,7 @@ int alien_b200_get_parameters(alien_b200_simulation* sim, AlienPhysicsParams* pa
 {
     return guarded([&] {
         if (!sim || !params) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
-        *params = sim->params;
+        *params = sim->arena->params(0);
     });
 }
 
@@ -1622,7 +1718,7 @@ int alien_b200_resize_arrays_if_necessary(alien_b200_simulation* sim, const Alie
             AlienDataTO to{&nc, cells.data(), &np, parts.data(), &na, aux.data()};
             sim->arena->getData(0, false, AlienInt2{0, 0}, AlienInt2{0, 0}, &to);
             const uint64_t t = sim->arena->readCounters()[0].timestep;
-            WorldSetup ws = setupFrom(sim->general, sim->params, t, &to);
+            WorldSetup ws = setupFrom(sim->general, sim->arena->params(0), t, &to);
             ws.extraParticles = sim->extraParticles;
             sim->arena->build({ws});
         }
@@ -1650,7 +1746,7 @@ int alien_b200_clear(alien_b200_simulation* sim)
     return guarded([&] {
         if (!sim) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
         const uint64_t t = sim->arena->readCounters()[0].timestep;
-        sim->arena->build({setupFrom(sim->general, sim->params, t, nullptr)});
+        sim->arena->build({setupFrom(sim->general, sim->arena->params(0), t, nullptr)});
     });
 }
 

@@ -27,6 +27,7 @@
 #pragma once
 
 #include "device_common.cuh"
+#include "zones.cuh"
 
 namespace ab {
 
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(kBlock, 8) kBin(DevState s)
         float factor = 0.0f;
         if (e > p.highRadiationMinCellEnergy[col]) factor += p.highRadiationFactor[col];
         if (static_cast<long long>(s.age[g]) > static_cast<long long>(p.radiationMinCellAge[col]))
-            factor += p.radiationCellAgeStrength[col];
+            factor += zoneParam<kZRadiationCellAgeStrength>(p, wi.W, wi.H, pos, p.radiationCellAgeStrength[col], col);
         if (!(factor > 0.0f)) return;
         float loss = e * factor;
         loss = loss / p.radiationProb;
@@ -217,10 +218,17 @@ __global__ void __launch_bounds__(kBlock, 8) kBin(DevState s)
             pp = correctPosition(pp, wi.W, wi.H);
             if (loss > e - 1.0f) loss = e - 1.0f;
             s.energy[g] = e - loss;
-            if (loss > kNearZero) {  // createEnergyParticle drops energy <= NEAR_ZERO
+            // createEnergyParticle (RadiationProcessor.cuh:248-364): at an
+            // active radiation source if there is one, the external-energy
+            // backflow, and no particle for energy <= NEAR_ZERO
+            WorldCounters& wcr = s.counters[c.w];
+            placeAtSource(p, wcr.activeSources, id, T, kSiteSourceRadiation, pp, pv);
+            pp = correctPosition(pp, wi.W, wi.H);
+            const float kept = backflow(p, wcr, col, loss);
+            if (kept > kNearZero) {
                 s.radPos[g] = pp;
                 s.radVel[g] = pv;
-                s.radEnergy[g] = loss;
+                s.radEnergy[g] = kept;
                 atomicOr(&s.flags[g], kFlagRadiation);
             }
         }
@@ -458,8 +466,9 @@ struct FluidLaw {
         invH2 = invH * invH;
         invH3 = invH2 * invH;
         minDist = p->cellMinDistance;
-        fusionVelocity = p->cellFusionVelocity;
-        maxBindingEnergy = p->cellMaxBindingEnergy;
+        // zone values at the cell (CellProcessor.cuh:149-152)
+        fusionVelocity = zoneParam<kZCellFusionVelocity>(*p, W, H, pos, p->cellFusionVelocity);
+        maxBindingEnergy = zoneParam<kZCellMaxBindingEnergy>(*p, W, H, pos, p->cellMaxBindingEnergy);
         pi = pos;
         vi = vel;
         barrierI = me.y & kStageBarrier;
@@ -619,10 +628,11 @@ struct CollisionLaw {
         for (int m = 0; m < kMaxBonds; ++m) bondsI[m] = m < nI ? st.bond[static_cast<long long>(g) * kMaxBonds + m] : -1;
     }
 
-    __device__ __forceinline__ void beginLaw(const WorldInfo&, int4 me, float2 pos, float2 vel)
+    __device__ __forceinline__ void beginLaw(const WorldInfo& wi, int4 me, float2 pos, float2 vel)
     {
-        fusionVelocity = p->cellFusionVelocity;
-        maxBindingEnergy = p->cellMaxBindingEnergy;
+        // zone values at the cell (CellProcessor.cuh:344-353)
+        fusionVelocity = zoneParam<kZCellFusionVelocity>(*p, wi.W, wi.H, pos, p->cellFusionVelocity);
+        maxBindingEnergy = zoneParam<kZCellMaxBindingEnergy>(*p, wi.W, wi.H, pos, p->cellMaxBindingEnergy);
         pi = pos;
         vi = vel;
         visibleI = me.y & kStageVisible;
@@ -1216,7 +1226,7 @@ __global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
         const bool barrierG = s.barrier[g0];
         const int n = s.numConn[g0];
         const int col = s.color[g0] % ALIEN_B200_MAX_COLORS;
-        const float2 F = s.force[g0];
+        float2 F = s.force[g0];
         float2 v = s.velA[g0];
         CellCtx c = cellCtx(s);
         if (!c.valid) return;
@@ -1225,7 +1235,16 @@ __global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
         const AlienPhysicsParams& p = s.params[wi.paramIndex];
         const uint64_t T = s.counters[c.w].timestep;
         if (!barrierG) {
-            if (len2(F) > p.cellMaxForce[col]) {
+            float maxForce = p.cellMaxForce[col];
+            if (p.numZones > 0) {
+                // the cell where the reference's applyForces finds it: after
+                // the overlap push; flow fields (FlowFieldKernels.cu:48-70)
+                // add to the pair force before checkForces reads it
+                const float2 pushed = correctPosition(s.posA[g] + s.push[g], wi.W, wi.H);
+                F = F + flowAcceleration(p, pushed, wi.W, wi.H);
+                maxForce = zoneParam<kZCellMaxForce>(p, wi.W, wi.H, pushed, maxForce, col);
+            }
+            if (len2(F) > maxForce) {
                 if (draw(s.id[g], T, kSiteForceDecay) < p.cellMaxForceDecayProb) atomicOr(&s.flags[g], kFlagDelAll);
             }
             v = v + F;
@@ -1248,7 +1267,12 @@ __global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
             if (!c.inRange || !s.palive[c.q]) return;
             const WorldInfo& wi = s.worlds[c.w];
             const AlienPhysicsParams& p = s.params[wi.paramIndex];
-            s.ppos[c.q] = correctPosition(s.ppos[c.q] + s.pvel[c.q] * p.timestepSize, wi.W, wi.H);
+            float2 v = s.pvel[c.q];
+            if (p.numZones > 0) {  // flow fields (FlowFieldKernels.cu:71-87), then movement
+                v = v + flowAcceleration(p, s.ppos[c.q], wi.W, wi.H);
+                s.pvel[c.q] = v;
+            }
+            s.ppos[c.q] = correctPosition(s.ppos[c.q] + v * p.timestepSize, wi.W, wi.H);
         });
     }
 }
@@ -1443,7 +1467,11 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletVel(DevState s)
             }
             const unsigned long long cellId = s.id[cell];
             if (s.plast[q] == cellId) return;
-            const float absorption = p.radiationAbsorption[s.color[cell] % ALIEN_B200_MAX_COLORS];
+            const int cellColor = s.color[cell] % ALIEN_B200_MAX_COLORS;
+            float absorption = p.radiationAbsorption[cellColor];
+            if (p.numZones > 0)  // at the cell after the overlap push (RadiationProcessor.cuh:111-116)
+                absorption = zoneParam<kZRadiationAbsorption>(p, wi.W, wi.H, correctPosition(s.posA[cell] + s.push[cell], wi.W, wi.H),
+                                                              absorption, cellColor);
             if (absorption < kNearZero) return;
             float e = s.penergy[q];
             float transfer = e * absorption;
@@ -1559,17 +1587,27 @@ __global__ void __launch_bounds__(kBlock, 6) kTransition(DevState s)
             s.velA[g] = vi;
             return;
         }
+        // zone values at the cell's position after the Verlet update
+        float friction = p.friction, maxBindingEnergy = p.cellMaxBindingEnergy;
+        float deathProbability = p.cellDeathProbability[col], minEnergy = p.cellMinEnergy[col];
+        if (p.numZones > 0) {
+            const float2 pos = stepPos(s, g, wi.W, wi.H);
+            friction = zoneParam<kZFriction>(p, wi.W, wi.H, pos, friction);
+            maxBindingEnergy = zoneParam<kZCellMaxBindingEnergy>(p, wi.W, wi.H, pos, maxBindingEnergy);
+            deathProbability = zoneParam<kZCellDeathProbability>(p, wi.W, wi.H, pos, deathProbability, col);
+            minEnergy = zoneParam<kZCellMinEnergy>(p, wi.W, wi.H, pos, minEnergy, col);
+        }
         // applyInnerFriction (every third step) + applyFriction
         // (CellProcessor.cuh:678-723)
         const float2 vf = innerFriction ? vi + acc * (p.innerFriction / 2.0f) : vi;
-        s.velA[g] = vf * (1.0f - p.friction);
+        s.velA[g] = vf * (1.0f - friction);
         // decay (CellProcessor.cuh:775-858) on the state after the transition
         uint32_t f = 0;
-        if (e > p.cellMaxBindingEnergy) f |= kFlagDelAll;
+        if (e > maxBindingEnergy) f |= kFlagDelAll;
         if (ls == ALIEN_B200_LIVING_DYING || ls == ALIEN_B200_LIVING_DETACHING) {
-            if (draw(s.id[g], T, kSiteDeath) < p.cellDeathProbability[col]) f |= kFlagDelCell;
+            if (draw(s.id[g], T, kSiteDeath) < deathProbability) f |= kFlagDelCell;
         }
-        bool destroy = e < p.cellMinEnergy[col];
+        bool destroy = e < minEnergy;
         const long long maxAge = p.cellMaxAge[col];
         if (maxAge > 0 && static_cast<long long>(age) > maxAge) destroy = true;
         if (destroy) {
@@ -2030,7 +2068,12 @@ __global__ void __launch_bounds__(kBlock) kEventCount(DevState s)
         uint32_t a = 0, b = 0;
         if (g < s.worlds[w].cellBase + wc.numCells) {
             a = (fl & kFlagRadiation) ? 1u : 0u;
-            b = (fl & kFlagDelCell) && s.energy[g] > kNearZero ? 1u : 0u;
+            if (fl & kFlagDelCell) {
+                // the deleted cell's energy particle (createEnergyParticle):
+                // the external-energy backflow is recorded here, once
+                const AlienPhysicsParams& p = s.params[s.worlds[w].paramIndex];
+                b = backflow(p, wc, s.color[g] % ALIEN_B200_MAX_COLORS, s.energy[g]) > kNearZero ? 1u : 0u;
+            }
             // the step's flags end here, except on the cells kEventEmit
             // still reads (radiation and deletion events)
             if (fl && !a && !b) s.flags[g] = 0;
@@ -2121,8 +2164,43 @@ __global__ void __launch_bounds__(kEventWorldThreads) kEventWorld(DevState s)
         wc.numParticles = static_cast<uint32_t>(want);
     }
     wc.timestep += 1;
+    wc.lastStepped = wc.timestep;  // kWorldsEnd: this world completed a step
     wc.signalsFresh = 0;
     if (wc.stepsRemaining != ~0ull && --wc.stepsRemaining == 0) wc.active = 0;
+}
+
+// the active radiation sources of every world before its first step
+__global__ void kWorldsBegin(DevState s)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= s.numWorlds) return;
+    const WorldInfo& wi = s.worlds[w];
+    s.counters[w].activeSources = activeSources(s.params[wi.paramIndex], wi.W, wi.H);
+}
+
+// The end of a step for worlds with zones, radiation sources or external
+// energy (launched after kEventEmit, which still uses the step's sources and
+// pool): the pool takes the step's backflow, zones and sources move
+// (SimulationParametersUpdateService.cu:52-78) and the next step's active
+// sources follow their new positions.  A world that did not step (inactive)
+// has nothing to add and does not move.
+__global__ void kWorldsEnd(DevState s)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= s.numWorlds) return;
+    WorldCounters& wc = s.counters[w];
+    if (wc.backflowFix) {
+        wc.externalEnergy += static_cast<double>(wc.backflowFix) / kBackflowScale;
+        wc.backflowFix = 0;
+    }
+    if (wc.lastStepped != wc.timestep) return;
+    wc.lastStepped = ~0ull;
+    const WorldInfo& wi = s.worlds[w];
+    AlienPhysicsParams& p = s.params[wi.paramIndex];
+    if (p.numZones > 0 || p.numRadiationSources > 0) {
+        moveZonesAndSources(p, wi.W, wi.H);
+        wc.activeSources = activeSources(p, wi.W, wi.H);
+    }
 }
 
 __device__ __forceinline__ void emitParticle(const DevState& s, const WorldInfo& wi, uint32_t slotRel, unsigned long long id,
@@ -2173,13 +2251,17 @@ __global__ void __launch_bounds__(kBlock) kEventEmit(DevState s)
         if (fl) s.flags[g] = 0;  // the step's flags end here
         const bool inRange = g < wi.cellBase + wc.numCells;
         const uint32_t rad = inRange && (fl & kFlagRadiation) ? 1u : 0u;
-        const uint32_t del = inRange && (fl & kFlagDelCell) && s.energy[g] > kNearZero ? 1u : 0u;
+        const AlienPhysicsParams& p = s.params[wi.paramIndex];
+        const float kept = inRange && (fl & kFlagDelCell) ? backflowKept(p, wc, s.color[g] % ALIEN_B200_MAX_COLORS, s.energy[g]) : 0.0f;
+        const uint32_t del = kept > kNearZero ? 1u : 0u;
         const uint32_t rr = blockExclusiveScan(rad, nullptr) + s.blockRad[blockIdx.x];
         const uint32_t dr = blockExclusiveScan(del, nullptr) + s.blockDel[blockIdx.x];
         if (rad) emitParticle(s, wi, wc.radSlotBase + rr, wc.radIdBase + rr, s.radPos[g], s.radVel[g], s.radEnergy[g], s.color[g]);
-        if (del)
-            emitParticle(s, wi, wc.delSlotBase + dr, wc.delIdBase + dr, stepPos(s, g, wi.W, wi.H), s.velA[g], s.energy[g],
-                         s.color[g]);
+        if (del) {
+            float2 pos = stepPos(s, g, wi.W, wi.H), vel = s.velA[g];
+            placeAtSource(p, wc.activeSources, s.id[g], wc.timestep - 1, kSiteSourceDeletedCell, pos, vel);
+            emitParticle(s, wi, wc.delSlotBase + dr, wc.delIdBase + dr, correctPosition(pos, wi.W, wi.H), vel, kept, s.color[g]);
+        }
     } else {
         // splits come from the slots used before this step's appends
         // (radSlotBase); appended particles carry no split

@@ -14,6 +14,46 @@ MOTION_FLUID = 0
 MOTION_COLLISION = 1
 
 
+MAX_ZONES = 20
+MAX_RADIATION_SOURCES = 40
+SHAPE_CIRCULAR, SHAPE_RECTANGULAR = 0, 1
+FLOW_NONE, FLOW_RADIAL, FLOW_CENTRAL, FLOW_LINEAR = 0, 1, 2, 3
+
+_C = ctypes.c_float * MAX_COLORS
+
+
+class Zone(ctypes.Structure):
+    """AlienZone (include/alien_b200.h): SimulationParametersZone's physics-stage part"""
+    _fields_ = [
+        ("posX", ctypes.c_float), ("posY", ctypes.c_float), ("velX", ctypes.c_float), ("velY", ctypes.c_float),
+        ("fadeoutRadius", ctypes.c_float),
+        ("shapeType", ctypes.c_int32),
+        ("coreRadius", ctypes.c_float), ("width", ctypes.c_float), ("height", ctypes.c_float),
+        ("flowType", ctypes.c_int32), ("flowOrientation", ctypes.c_int32),
+        ("flowStrength", ctypes.c_float), ("flowDriftAngle", ctypes.c_float), ("flowAngle", ctypes.c_float),
+        ("friction", ctypes.c_float), ("rigidity", ctypes.c_float),
+        ("radiationAbsorption", _C), ("radiationCellAgeStrength", _C), ("cellMaxForce", _C), ("cellMinEnergy", _C),
+        ("cellDeathProbability", _C),
+        ("cellFusionVelocity", ctypes.c_float), ("cellMaxBindingEnergy", ctypes.c_float),
+        ("radiationDisableSources", ctypes.c_uint8),
+        ("frictionActivated", ctypes.c_uint8), ("rigidityActivated", ctypes.c_uint8),
+        ("radiationAbsorptionActivated", ctypes.c_uint8), ("radiationCellAgeStrengthActivated", ctypes.c_uint8),
+        ("cellMaxForceActivated", ctypes.c_uint8), ("cellMinEnergyActivated", ctypes.c_uint8),
+        ("cellDeathProbabilityActivated", ctypes.c_uint8), ("cellFusionVelocityActivated", ctypes.c_uint8),
+        ("cellMaxBindingEnergyActivated", ctypes.c_uint8), ("radiationDisableSourcesActivated", ctypes.c_uint8),
+        ("reserved", ctypes.c_uint8 * 1),
+    ]
+
+
+class RadiationSource(ctypes.Structure):
+    """AlienRadiationSource (include/alien_b200.h)"""
+    _fields_ = [
+        ("strength", ctypes.c_float), ("posX", ctypes.c_float), ("posY", ctypes.c_float), ("velX", ctypes.c_float),
+        ("velY", ctypes.c_float), ("useAngle", ctypes.c_int32), ("angle", ctypes.c_float), ("shapeType", ctypes.c_int32),
+        ("radius", ctypes.c_float), ("width", ctypes.c_float), ("height", ctypes.c_float),
+    ]
+
+
 class PhysicsParams(ctypes.Structure):
     _fields_ = [
         ("timestepSize", ctypes.c_float),
@@ -53,8 +93,14 @@ class PhysicsParams(ctypes.Structure):
         ("cellColorTransitionRules", ctypes.c_uint8),
         ("advancedAbsorptionControl", ctypes.c_uint8),
         ("externalEnergyControl", ctypes.c_uint8),
-        ("reserved", ctypes.c_uint8 * 3),
+        ("radiationDisableSources", ctypes.c_uint8),
+        ("reserved", ctypes.c_uint8 * 2),
         ("cellNumExecutionOrderNumbers", ctypes.c_int32),
+        ("externalEnergy", ctypes.c_float),
+        ("externalEnergyBackflowFactor", ctypes.c_float * MAX_COLORS),
+        ("externalEnergyBackflowLimit", ctypes.c_float),
+        ("zones", Zone * MAX_ZONES),
+        ("radiationSources", RadiationSource * MAX_RADIATION_SOURCES),
     ]
 
     def copy(self) -> "PhysicsParams":
@@ -102,7 +148,34 @@ def default_parameters() -> PhysicsParams:
     p.cellFusionVelocity = 0.6
     p.cellMaxBindingEnergy = FLT_MAX
     p.cellNumExecutionOrderNumbers = 6
+    p.externalEnergyBackflowLimit = FLT_MAX
+    for z in p.zones:
+        default_zone(z, p)
+    for r in p.radiationSources:
+        r.radius = 1.0
+        r.width, r.height = 100.0, 200.0
     return p
+
+
+def default_zone(z: Zone, base: PhysicsParams) -> Zone:
+    """the reference's zone defaults (SimulationParametersZone.h): circular,
+    core radius 100, fade-out radius 100, no flow, the base values, nothing
+    activated"""
+    z.fadeoutRadius = 100.0
+    z.shapeType = SHAPE_CIRCULAR
+    z.coreRadius = 100.0
+    z.width, z.height = 100.0, 200.0
+    z.flowType = FLOW_NONE
+    z.flowStrength = 0.001
+    z.friction, z.rigidity = base.friction, base.rigidity
+    for c in range(MAX_COLORS):
+        z.radiationAbsorption[c] = base.radiationAbsorption[c]
+        z.radiationCellAgeStrength[c] = base.radiationCellAgeStrength[c]
+        z.cellMaxForce[c] = base.cellMaxForce[c]
+        z.cellMinEnergy[c] = base.cellMinEnergy[c]
+        z.cellDeathProbability[c] = base.cellDeathProbability[c]
+    z.cellFusionVelocity, z.cellMaxBindingEnergy = base.cellFusionVelocity, base.cellMaxBindingEnergy
+    return z
 
 
 def benchmark_parameters(motion_type: int = MOTION_FLUID) -> PhysicsParams:

@@ -10,12 +10,18 @@ parameters :12-1100); color-dependent values are seven keys ``name[0]`` ..
 ``name[6]`` (ParameterParser.h:54-82).  A key that is missing takes the
 default, as in the reference's decoder.
 
-Only the fields of ``AlienPhysicsParams`` are read or written; the rest of
-the file (rendering, genome mutation, cell-function parameters, zones and
-radiation sources) belongs to other parts of the reference.  The fields whose
-non-default values the engine rejects (zones, radiation sources, rigidity,
-particle transformation, feature flags) are read so that ``read_settings``
-can name them.  ``innerFriction`` has no key in the reference's files.
+Only the fields of ``AlienPhysicsParams`` are read or written: the
+physics-stage parameters, the zones ("spots", AuxiliaryDataParserService.cpp
+:765-900) with their shapes, flow fields and physics-stage values, the
+radiation sources ("particle sources", :723-763) and the external-energy
+backflow (:271-300); the rest of the file (rendering, genome mutation,
+cell-function parameters) belongs to other parts of the reference.  A zone
+value has an ``activated`` flag: ``<key>.activated`` with ``<key>.value``, or
+with ``<key>[c]`` for color-dependent values (ParameterParser.h:155-210).  The
+fields whose non-default values the engine rejects (rigidity, in the base or
+in a zone, particle transformation, cell-function feature flags) are read so
+that ``read_settings`` can name them.  ``innerFriction`` has no key in the
+reference's files.
 """
 from __future__ import annotations
 
@@ -67,14 +73,50 @@ _FIELDS = [
     ("cellColorTransitionRules", "features.cell color transition rules", "b", False),
     ("advancedAbsorptionControl", "features.additional absorption control", "b", False),
     ("externalEnergyControl", "features.external energy", "b", False),
+    ("radiationDisableSources", "radiation.disable sources", "b", False),
+    ("externalEnergy", "cell.function.constructor.external energy", "f", False),
+    ("externalEnergyBackflowFactor", "cell.function.constructor.external energy backflow", "f", True),
+    ("externalEnergyBackflowLimit", "cell.function.constructor.external energy backflow limit", "f", False),
+]
+# zone ("spots.<i>.") fields: plain, then values with an activated flag
+_ZONE_PLAIN = [
+    ("posX", "pos.x", "f"), ("posY", "pos.y", "f"), ("velX", "vel.x", "f"), ("velY", "vel.y", "f"),
+    ("fadeoutRadius", "fadeout radius", "f"), ("shapeType", "shape.type", "i"),
+    ("coreRadius", "shape.circular.core radius", "f"), ("width", "shape.rectangular.core width", "f"),
+    ("height", "shape.rectangular.core height", "f"), ("flowType", "flow.type", "i"),
+]
+_ZONE_FLOW = {  # flow type: [(field, key, kind)]
+    P.FLOW_RADIAL: [("flowOrientation", "flow.radial.orientation", "i"), ("flowStrength", "flow.radial.strength", "f"),
+                    ("flowDriftAngle", "flow.radial.drift angle", "f")],
+    P.FLOW_CENTRAL: [("flowStrength", "flow.central.strength", "f")],
+    P.FLOW_LINEAR: [("flowAngle", "flow.linear.angle", "f"), ("flowStrength", "flow.linear.strength", "f")],
+}
+# (value field, activated flag, key, kind, color-dependent)
+_ZONE_VALUES = [
+    ("friction", "frictionActivated", "friction", "f", False),
+    ("rigidity", "rigidityActivated", "rigidity", "f", False),
+    ("radiationDisableSources", "radiationDisableSourcesActivated", "radiation.disable sources", "b", False),
+    ("radiationAbsorption", "radiationAbsorptionActivated", "radiation.absorption", "f", True),
+    ("radiationCellAgeStrength", "radiationCellAgeStrengthActivated", "radiation.factor", "f", True),
+    ("cellMaxForce", "cellMaxForceActivated", "cell.max force", "f", True),
+    ("cellMinEnergy", "cellMinEnergyActivated", "cell.min energy", "f", True),
+    ("cellDeathProbability", "cellDeathProbabilityActivated", "cell.death probability", "f", True),
+    ("cellFusionVelocity", "cellFusionVelocityActivated", "cell.fusion velocity", "f", False),
+    ("cellMaxBindingEnergy", "cellMaxBindingEnergyActivated", "cell.max binding energy", "f", False),
+]
+_SOURCE_FIELDS = [
+    ("posX", "pos.x", "f"), ("posY", "pos.y", "f"), ("velX", "vel.x", "f"), ("velY", "vel.y", "f"),
+    ("useAngle", "use angle", "b"), ("strength", "strength", "f"), ("angle", "angle", "f"),
+    ("shapeType", "shape.type", "i"), ("radius", "shape.circular.radius", "f"),
+    ("width", "shape.rectangular.width", "f"), ("height", "shape.rectangular.height", "f"),
 ]
 _MOTION_KEYS = {
     P.MOTION_FLUID: {"smoothingLength", "pressureStrength", "viscosityStrength"},
     P.MOTION_COLLISION: {"cellMaxCollisionDistance", "cellRepulsionStrength"},
 }
 # fields whose non-default values the engine rejects (ALIEN_B200_ERR_UNSUPPORTED)
-_UNSUPPORTED = ("numZones", "numRadiationSources", "rigidity", "particleTransformationAllowed", "cellAgeLimiter",
-                "cellColorTransitionRules", "advancedAbsorptionControl", "externalEnergyControl")
+_UNSUPPORTED = ("rigidity", "particleTransformationAllowed", "cellAgeLimiter", "cellColorTransitionRules",
+                "advancedAbsorptionControl")
 
 
 def _get(tree: dict, path: str) -> Any:
@@ -144,9 +186,47 @@ def decode(tree: dict) -> tuple[int, tuple[int, int], P.PhysicsParams, list[str]
             v = _get(tree, _SP + key)
             if v is not None:
                 setattr(prm, name, _parse(v, kind))
+    prm.numZones = max(0, min(prm.numZones, P.MAX_ZONES))
+    prm.numRadiationSources = max(0, min(prm.numRadiationSources, P.MAX_RADIATION_SOURCES))
+    _decode_zones(tree, prm)
+    _decode_sources(tree, prm)
     default = P.default_parameters()
     unsupported = [n for n in _UNSUPPORTED if getattr(prm, n) != getattr(default, n)]
+    unsupported += [f"zones[{i}].rigidity" for i in range(prm.numZones)
+                    if prm.zones[i].rigidityActivated and prm.zones[i].rigidity != 0.0]
     return timestep, world, prm, unsupported
+
+
+def _read(tree: dict, path: str, kind: str, fallback):
+    v = _get(tree, path)
+    return _parse(v, kind) if v is not None else fallback
+
+
+def _decode_zones(tree: dict, prm: P.PhysicsParams) -> None:
+    base_defaults = P.default_parameters()  # a missing zone key takes the struct default
+    for i in range(prm.numZones):
+        z = P.default_zone(prm.zones[i], base_defaults)
+        base = _SP + f"spots.{i}."
+        for field, key, kind in _ZONE_PLAIN:
+            setattr(z, field, _read(tree, base + key, kind, getattr(z, field)))
+        for field, key, kind in _ZONE_FLOW.get(z.flowType, []):
+            setattr(z, field, _read(tree, base + key, kind, getattr(z, field)))
+        for field, flag, key, kind, color in _ZONE_VALUES:
+            setattr(z, flag, _read(tree, base + key + ".activated", "b", 0))
+            if color:
+                arr = getattr(z, field)
+                for c in range(P.MAX_COLORS):
+                    arr[c] = _read(tree, base + f"{key}[{c}]", kind, arr[c])
+            else:
+                setattr(z, field, _read(tree, base + key + ".value", kind, getattr(z, field)))
+
+
+def _decode_sources(tree: dict, prm: P.PhysicsParams) -> None:
+    for i in range(prm.numRadiationSources):
+        r = prm.radiationSources[i]
+        base = _SP + f"particle sources.{i}."
+        for field, key, kind in _SOURCE_FIELDS:
+            setattr(r, field, _read(tree, base + key, kind, getattr(r, field)))
 
 
 def encode(timestep: int, world: tuple[int, int], prm: P.PhysicsParams) -> dict:
@@ -165,6 +245,23 @@ def encode(timestep: int, world: tuple[int, int], prm: P.PhysicsParams) -> dict:
                 _set(tree, _SP + f"{key}[{c}]", _format(arr[c], kind))
         else:
             _set(tree, _SP + key, _format(getattr(prm, name), kind))
+    for i in range(prm.numZones):
+        z = prm.zones[i]
+        base = _SP + f"spots.{i}."
+        for field, key, kind in _ZONE_PLAIN + _ZONE_FLOW.get(z.flowType, []):
+            _set(tree, base + key, _format(getattr(z, field), kind))
+        for field, flag, key, kind, color in _ZONE_VALUES:
+            _set(tree, base + key + ".activated", _format(getattr(z, flag), "b"))
+            if color:
+                arr = getattr(z, field)
+                for c in range(P.MAX_COLORS):
+                    _set(tree, base + f"{key}[{c}]", _format(arr[c], kind))
+            else:
+                _set(tree, base + key + ".value", _format(getattr(z, field), kind))
+    for i in range(prm.numRadiationSources):
+        r = prm.radiationSources[i]
+        for field, key, kind in _SOURCE_FIELDS:
+            _set(tree, _SP + f"particle sources.{i}." + key, _format(getattr(r, field), kind))
     return tree
 
 

@@ -184,6 +184,66 @@ typedef struct AlienGeneralSettings {
     int32_t worldSizeY;
 } AlienGeneralSettings;
 
+/* Zones (SimulationParametersZone, EngineInterface/SimulationParametersZone.h):
+ * regions in which parameter values blend from the base values into the
+ * zone's own (SpotCalculator.cuh:78-93, 183-232) and which may carry a flow
+ * field (FlowFieldKernels.cu:48-89).  Only the physics-stage values are
+ * carried; each has an `activated` flag as in
+ * SimulationParametersZoneActivatedValues.h.  Zones and radiation sources
+ * move by their velocity after every timestep
+ * (SimulationParametersUpdateService.cu:52-78). */
+#define ALIEN_B200_MAX_ZONES 20              /* EngineConstants.h:8 */
+#define ALIEN_B200_MAX_RADIATION_SOURCES 40  /* EngineConstants.h:7 */
+enum {
+    ALIEN_B200_SHAPE_CIRCULAR = 0,
+    ALIEN_B200_SHAPE_RECTANGULAR = 1,
+};
+enum {
+    ALIEN_B200_FLOW_NONE = 0,
+    ALIEN_B200_FLOW_RADIAL = 1,
+    ALIEN_B200_FLOW_CENTRAL = 2,
+    ALIEN_B200_FLOW_LINEAR = 3,
+};
+typedef struct AlienZone {
+    float posX, posY, velX, velY;
+    float fadeoutRadius;
+    int32_t shapeType;          /* ALIEN_B200_SHAPE_*: circular uses coreRadius, rectangular width x height */
+    float coreRadius, width, height;
+    int32_t flowType;           /* ALIEN_B200_FLOW_* */
+    int32_t flowOrientation;    /* radial: 0 clockwise, 1 counter-clockwise */
+    float flowStrength;         /* radial / central / linear */
+    float flowDriftAngle;       /* radial, degrees */
+    float flowAngle;            /* linear, degrees */
+    /* values (SimulationParametersZoneValues.h) */
+    float friction;
+    float rigidity;
+    float radiationAbsorption[ALIEN_B200_MAX_COLORS];
+    float radiationCellAgeStrength[ALIEN_B200_MAX_COLORS];
+    float cellMaxForce[ALIEN_B200_MAX_COLORS];
+    float cellMinEnergy[ALIEN_B200_MAX_COLORS];
+    float cellDeathProbability[ALIEN_B200_MAX_COLORS];
+    float cellFusionVelocity;
+    float cellMaxBindingEnergy;
+    uint8_t radiationDisableSources;
+    /* activated flags of the values above, in their order */
+    uint8_t frictionActivated, rigidityActivated, radiationAbsorptionActivated, radiationCellAgeStrengthActivated;
+    uint8_t cellMaxForceActivated, cellMinEnergyActivated, cellDeathProbabilityActivated, cellFusionVelocityActivated;
+    uint8_t cellMaxBindingEnergyActivated, radiationDisableSourcesActivated;
+    uint8_t reserved[1];
+} AlienZone;
+
+/* RadiationSource (EngineInterface/RadiationSource.h): new energy particles
+ * (radiation, deleted cells) appear at an active source, chosen in
+ * proportion to the strengths (RadiationProcessor.cuh:248-364). */
+typedef struct AlienRadiationSource {
+    float strength;
+    float posX, posY, velX, velY;
+    int32_t useAngle;
+    float angle;                /* degrees */
+    int32_t shapeType;          /* ALIEN_B200_SHAPE_*: circular uses radius, rectangular width x height */
+    float radius, width, height;
+} AlienRadiationSource;
+
 /* The physics-stage subset of SimulationParameters
  * (EngineInterface/SimulationParameters.h:18-206, base values from
  * SimulationParametersZoneValues.h:10-30, motion from Motion.h:7-36).
@@ -220,21 +280,31 @@ typedef struct AlienPhysicsParams {
     float cellDeathProbability[ALIEN_B200_MAX_COLORS];   /* :21 */
     float cellFusionVelocity;                 /* :23 */
     float cellMaxBindingEnergy;               /* :24 */
-    /* features and subsystems outside the physics stage: must be zero
-     * (checked; a nonzero value returns ALIEN_B200_ERR_UNSUPPORTED) */
-    int32_t numZones;                         /* :39 */
-    int32_t numRadiationSources;              /* :27 */
+    int32_t numZones;                         /* :39, zones[0, numZones) */
+    int32_t numRadiationSources;              /* :27, radiationSources[0, numRadiationSources) */
+    /* features outside the physics stage: must be zero (checked; a nonzero
+     * value returns ALIEN_B200_ERR_UNSUPPORTED) */
     uint8_t particleTransformationAllowed;    /* :111 */
     uint8_t cellAgeLimiter;                   /* Features.h */
     uint8_t cellColorTransitionRules;         /* Features.h */
     uint8_t advancedAbsorptionControl;        /* Features.h */
-    uint8_t externalEnergyControl;            /* Features.h */
-    uint8_t reserved[3];
+    /* external energy (Features.h, SimulationParameters.h:31-36): with it on,
+     * a new energy particle of color c sends externalEnergyBackflowFactor[c]
+     * of its energy to the external energy pool (RadiationProcessor.cuh:
+     * 345-354) */
+    uint8_t externalEnergyControl;
+    uint8_t radiationDisableSources;          /* ZoneValues.h:18, base value */
+    uint8_t reserved[2];
     /* cell functions: a cell with a function runs it in the steps where
      * timestep % cellNumExecutionOrderNumbers equals its execution order
      * number (CellFunctionProcessor.cuh:241-244); only the neuron function is
      * part of this engine */
     int32_t cellNumExecutionOrderNumbers;     /* :72 */
+    float externalEnergy;                     /* :31, the pool (updated by the steps) */
+    float externalEnergyBackflowFactor[ALIEN_B200_MAX_COLORS]; /* :34 */
+    float externalEnergyBackflowLimit;        /* :36 */
+    AlienZone zones[ALIEN_B200_MAX_ZONES];    /* :40 */
+    AlienRadiationSource radiationSources[ALIEN_B200_MAX_RADIATION_SOURCES]; /* :28 */
 } AlienPhysicsParams;
 
 /* Subset of RawStatisticsData (EngineGpuKernels/SimulationStatistics.cuh)
@@ -477,6 +547,8 @@ ALIEN_B200_STATIC_ASSERT(offsetof(AlienParticleTO, color) == 32, "ParticleTO.col
 ALIEN_B200_STATIC_ASSERT(offsetof(AlienSignalTO, targetX) == 36, "SignalTO.targetX");
 ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellMetadataTO, nameDataIndex) == 8, "CellMetadataTO.nameDataIndex");
 ALIEN_B200_STATIC_ASSERT(offsetof(AlienCellMetadataTO, descriptionDataIndex) == 24, "CellMetadataTO.descriptionDataIndex");
+ALIEN_B200_STATIC_ASSERT(sizeof(AlienZone) == 224, "AlienZone is 224 bytes");
+ALIEN_B200_STATIC_ASSERT(sizeof(AlienRadiationSource) == 44, "AlienRadiationSource is 44 bytes");
 ALIEN_B200_STATIC_ASSERT(sizeof(AlienTimestepStatistics) == 368, "TimestepStatistics is 368 bytes");
 ALIEN_B200_STATIC_ASSERT(offsetof(AlienTimestepStatistics, numGenomeCells) == 168, "TimestepStatistics.numGenomeCells");
 ALIEN_B200_STATIC_ASSERT(offsetof(AlienTimestepStatistics, genomeComplexityVariance) == 280, "TimestepStatistics.genomeComplexityVariance");

@@ -245,6 +245,9 @@ typedef struct OracleWorld {
     uint8_t* pincoming;
     real *mergeE, *mergeMx, *mergeMy;
     uint64_t neuronActivity[ALIEN_B200_MAX_COLORS]; /* neuron cells that ran (statistics) */
+    double externalEnergy;   /* the external energy pool */
+    double backflowSum;      /* this step's backflow into the pool */
+    uint64_t activeSources;  /* radiation sources active in this step (bit i: source i) */
 } OracleWorld;
 
 #define XALLOC(ptr, n) ((ptr) = calloc((size_t)((n) > 0 ? (n) : 1), sizeof(*(ptr))))
@@ -298,6 +301,7 @@ OracleWorld* oracle_create(int worldSizeX, int worldSizeY, const AlienPhysicsPar
     w->H = worldSizeY;
     w->p = *params;
     w->timestep = timestep;
+    w->externalEnergy = params->externalEnergy;
     w->nextId = 1;
     allocCells(w, 1);
     growParts(w, 16);
@@ -324,6 +328,7 @@ void oracle_destroy(OracleWorld* w)
 void oracle_set_parameters(OracleWorld* w, const AlienPhysicsParams* params)
 {
     w->p = *params;
+    w->externalEnergy = params->externalEnergy;
     /* prepareForSimulationParametersChanges -> resetDensity,
      * SimulationKernelsLauncher.cu:93-97, CellProcessor.cuh:860-870 */
     for (int64_t i = 0; i < w->nCells; ++i) w->density[i] = 1;
@@ -477,11 +482,238 @@ int oracle_get_data(OracleWorld* w, const AlienDataTO* to)
     return 0;
 }
 
-/* ---- particle creation: RadiationProcessor::createEnergyParticle without
- *      radiation sources (RadiationProcessor.cuh:248-364: the source branch
- *      needs numRadiationSources > 0; the backflow branch needs the
- *      externalEnergyControl feature) and ObjectFactory::createParticle
- *      (ObjectFactory.cuh:242-256). */
+/* ---- zones: SpotCalculator (SpotCalculator.cuh:12-251).  A parameter
+ *      blends from its base value into the values of the zones that
+ *      activate it, by each zone's weight at the position (0 in the core,
+ *      rising to 1 over the fade-out radius + 1):
+ *      base * prod(w_i) + sum_i v_i (1 - w_i) / (sum_i (1 - w_i) + prod(w_i)). */
+enum { ZF_FRICTION, ZF_RIGIDITY, ZF_RADIATION_ABSORPTION, ZF_RADIATION_CELL_AGE_STRENGTH, ZF_CELL_MAX_FORCE,
+       ZF_CELL_MIN_ENERGY, ZF_CELL_DEATH_PROBABILITY, ZF_CELL_FUSION_VELOCITY, ZF_CELL_MAX_BINDING_ENERGY,
+       ZF_RADIATION_DISABLE_SOURCES };
+
+static int zoneActivated(const AlienZone* z, int f)
+{
+    switch (f) {
+    case ZF_FRICTION: return z->frictionActivated;
+    case ZF_RIGIDITY: return z->rigidityActivated;
+    case ZF_RADIATION_ABSORPTION: return z->radiationAbsorptionActivated;
+    case ZF_RADIATION_CELL_AGE_STRENGTH: return z->radiationCellAgeStrengthActivated;
+    case ZF_CELL_MAX_FORCE: return z->cellMaxForceActivated;
+    case ZF_CELL_MIN_ENERGY: return z->cellMinEnergyActivated;
+    case ZF_CELL_DEATH_PROBABILITY: return z->cellDeathProbabilityActivated;
+    case ZF_CELL_FUSION_VELOCITY: return z->cellFusionVelocityActivated;
+    case ZF_CELL_MAX_BINDING_ENERGY: return z->cellMaxBindingEnergyActivated;
+    default: return z->radiationDisableSourcesActivated;
+    }
+}
+static real zoneValue(const AlienZone* z, int f, int color)
+{
+    switch (f) {
+    case ZF_FRICTION: return z->friction;
+    case ZF_RIGIDITY: return z->rigidity;
+    case ZF_RADIATION_ABSORPTION: return z->radiationAbsorption[color];
+    case ZF_RADIATION_CELL_AGE_STRENGTH: return z->radiationCellAgeStrength[color];
+    case ZF_CELL_MAX_FORCE: return z->cellMaxForce[color];
+    case ZF_CELL_MIN_ENERGY: return z->cellMinEnergy[color];
+    case ZF_CELL_DEATH_PROBABILITY: return z->cellDeathProbability[color];
+    case ZF_CELL_FUSION_VELOCITY: return z->cellFusionVelocity;
+    case ZF_CELL_MAX_BINDING_ENERGY: return z->cellMaxBindingEnergy;
+    default: return z->radiationDisableSources ? 1 : 0;
+    }
+}
+/* SpotCalculator::calcWeight, :183-210; delta = zone - position */
+static real zoneWeight(const AlienZone* z, vec2 delta)
+{
+    if (z->shapeType == ALIEN_B200_SHAPE_RECTANGULAR) {
+        real hw = (real)z->width / 2, hh = (real)z->height / 2;
+        if (R_ABS(delta.x) > hw || R_ABS(delta.y) > hh) {
+            vec2 d = v2(rmax(0, R_ABS(delta.x) - hw), rmax(0, R_ABS(delta.y) - hh));
+            return rmin(1, vlen(d) / ((real)z->fadeoutRadius + 1));
+        }
+        return 0;
+    }
+    real distance = vlen(delta);
+    return distance < (real)z->coreRadius ? 0 : rmin(1, (distance - (real)z->coreRadius) / ((real)z->fadeoutRadius + 1));
+}
+static real zoneWeightAt(const OracleWorld* w, const AlienZone* z, vec2 pos)
+{
+    return zoneWeight(z, correctDirection(w, vsub(v2(z->posX, z->posY), pos)));
+}
+/* SpotCalculator::calcParameter, :78-160 */
+static real zoneParam(const OracleWorld* w, int f, vec2 pos, real base, int color)
+{
+    const AlienPhysicsParams* p = &w->p;
+    if (p->numZones <= 0) return base;
+    real baseFactor = 1, sum = 0;
+    for (int i = 0; i < p->numZones; ++i) {
+        if (!zoneActivated(&p->zones[i], f)) continue;
+        real wi = zoneWeightAt(w, &p->zones[i], pos);
+        baseFactor *= wi;
+        sum += 1 - wi;
+    }
+    sum += baseFactor;
+    real result = base * baseFactor;
+    for (int i = 0; i < p->numZones; ++i) {
+        if (!zoneActivated(&p->zones[i], f)) continue;
+        real wi = zoneWeightAt(w, &p->zones[i], pos);
+        result += zoneValue(&p->zones[i], f, color) * (1 - wi) / sum;
+    }
+    return result;
+}
+/* FlowFieldKernels.cu:10-44 */
+static real flowHeight(const OracleWorld* w, const AlienZone* z, vec2 pos)
+{
+    real h = R_SQRT(vlen(correctDirection(w, vsub(pos, v2(z->posX, z->posY))))) * (real)z->flowStrength;
+    return z->flowOrientation == 0 ? h : -h;
+}
+static vec2 zoneFlow(const OracleWorld* w, const AlienZone* z, vec2 pos)
+{
+    if (z->flowType == ALIEN_B200_FLOW_RADIAL) {
+        real b = flowHeight(w, z, pos), down = flowHeight(w, z, vadd(pos, v2(0, 1))), right = flowHeight(w, z, vadd(pos, v2(1, 0)));
+        vec2 r = v2(right - b, down - b);
+        real a = ((real)90 + (real)z->flowDriftAngle) * DEG_TO_RAD; /* Math::rotateClockwise */
+        return v2(r.x * R_COS(a) - r.y * R_SIN(a), r.x * R_SIN(a) + r.y * R_COS(a));
+    }
+    if (z->flowType == ALIEN_B200_FLOW_CENTRAL) {
+        vec2 c = correctDirection(w, vsub(v2(z->posX, z->posY), pos));
+        return vmul(c, (real)z->flowStrength / (vlen2(c) + 50));
+    }
+    if (z->flowType == ALIEN_B200_FLOW_LINEAR) return vmul(unitVectorOfAngle(z->flowAngle), (real)z->flowStrength);
+    return v2(0, 0);
+}
+/* cudaApplyFlowFieldSettings with calcResultingFlowField (FlowFieldKernels.cu:48-89, SpotCalculator.cuh:58-78) */
+static vec2 flowAcceleration(const OracleWorld* w, vec2 pos)
+{
+    const AlienPhysicsParams* p = &w->p;
+    real baseFactor = 1, sum = 0;
+    int any = 0;
+    for (int i = 0; i < p->numZones; ++i) {
+        if (p->zones[i].flowType == ALIEN_B200_FLOW_NONE) continue;
+        real wi = zoneWeightAt(w, &p->zones[i], pos);
+        baseFactor *= wi;
+        sum += 1 - wi;
+        any = 1;
+    }
+    if (!any) return v2(0, 0);
+    sum += baseFactor;
+    vec2 result = v2(0, 0);
+    for (int i = 0; i < p->numZones; ++i) {
+        if (p->zones[i].flowType == ALIEN_B200_FLOW_NONE) continue;
+        real wi = zoneWeightAt(w, &p->zones[i], pos);
+        result = vadd(result, vdiv(vmul(zoneFlow(w, &p->zones[i], pos), 1 - wi), sum));
+    }
+    return result;
+}
+/* RadiationProcessor::calcActiveSources, RadiationProcessor.cuh:42-59 */
+static uint64_t calcActiveSources(const OracleWorld* w)
+{
+    const AlienPhysicsParams* p = &w->p;
+    uint64_t mask = 0;
+    for (int i = 0; i < p->numRadiationSources; ++i) {
+        const AlienRadiationSource* r = &p->radiationSources[i];
+        real disabled = zoneParam(w, ZF_RADIATION_DISABLE_SOURCES, v2(r->posX, r->posY), p->radiationDisableSources ? 1 : 0, 0);
+        if (!(disabled > (real)0.5)) mask |= 1ull << i;
+    }
+    return mask;
+}
+/* createEnergyParticle's placement at a radiation source
+ * (RadiationProcessor.cuh:252-343); draw sites as in the engine: base + 0
+ * source choice, base + 1 + 2k / base + 2 + 2k the k-th circular try,
+ * base + 21 the speed, base + 22 / 23 the rectangular offset */
+#define SITE_SOURCE_RADIATION 32
+#define SITE_SOURCE_DELETED_CELL 64
+static void placeAtSource(const OracleWorld* w, uint64_t id, uint64_t T, uint32_t site, vec2* pos, vec2* vel)
+{
+    const AlienPhysicsParams* p = &w->p;
+    uint64_t mask = w->activeSources;
+    if (!mask) return;
+    real sumRatios = 0;
+    for (int i = 0; i < p->numRadiationSources; ++i)
+        if ((mask >> i) & 1ull) sumRatios += p->radiationSources[i].strength;
+    if (!(sumRatios > 0)) return;
+    real r = draw(id, T, site);
+    sumRatios = 0;
+    int index = -1;
+    for (int i = 0; i < p->numRadiationSources; ++i) {
+        if (!((mask >> i) & 1ull)) continue;
+        sumRatios += p->radiationSources[i].strength;
+        if (r <= sumRatios) {
+            index = i;
+            break;
+        }
+    }
+    if (index < 0) return;
+    const AlienRadiationSource* src = &p->radiationSources[index];
+    *pos = v2(src->posX, src->posY);
+    real speed = (real)0.5 + (real)0.5 * draw(id, T, site + 21);
+    if (src->shapeType == ALIEN_B200_SHAPE_CIRCULAR) {
+        real radius = rmax(1, src->radius);
+        vec2 delta = v2(0, 0);
+        for (int k = 0; k < 10; ++k) {
+            delta.x = (real)draw(id, T, site + 1 + 2 * k) * radius * 2 - radius;
+            delta.y = (real)draw(id, T, site + 2 + 2 * k) * radius * 2 - radius;
+            if (vlen(delta) <= radius) break;
+        }
+        *pos = vadd(*pos, delta);
+        *vel = src->useAngle ? vmul(unitVectorOfAngle(src->angle), speed) : vmul(vnormalized(delta), speed);
+    } else {
+        real wd = src->width, ht = src->height;
+        vec2 delta = v2((real)draw(id, T, site + 22) * wd - wd / 2, (real)draw(id, T, site + 23) * ht - ht / 2);
+        *pos = vadd(*pos, delta);
+        if (src->useAngle) {
+            *vel = vmul(unitVectorOfAngle(src->angle), speed);
+        } else {
+            real round = rmin(wd, ht) / 2;
+            vec2 c1 = v2(-wd / 2, -ht / 2), c2 = v2(wd / 2, -ht / 2), c3 = v2(-wd / 2, ht / 2), c4 = v2(wd / 2, ht / 2);
+#define LMAX(v) rmax(R_ABS((v).x), R_ABS((v).y))
+            vec2 v;
+            if (LMAX(vsub(c1, delta)) <= round) {
+                v = vnormalized(vsub(delta, vadd(c1, v2(round, round))));
+            } else if (LMAX(vsub(c2, delta)) <= round) {
+                v = vnormalized(vsub(delta, vadd(c2, v2(-round, round))));
+            } else if (LMAX(vsub(c3, delta)) <= round) {
+                v = vnormalized(vsub(delta, vadd(c3, v2(round, -round))));
+            } else if (LMAX(vsub(c4, delta)) <= round) {
+                v = vnormalized(vsub(delta, vadd(c4, v2(-round, -round))));
+            } else {
+                real dx1 = wd / 2 + delta.x, dx2 = wd / 2 - delta.x, dy1 = ht / 2 + delta.y, dy2 = ht / 2 - delta.y;
+                v = v2(0, 0);
+                if (dx1 <= dy1 && dx1 <= dy2 && delta.x <= 0) v.x = -1;
+                if (dy1 <= dx1 && dy1 <= dx2 && delta.y <= 0) v.y = -1;
+                if (dx2 <= dy1 && dx2 <= dy2 && delta.x > 0) v.x = 1;
+                if (dy2 <= dx1 && dy2 <= dx2 && delta.y > 0) v.y = 1;
+            }
+#undef LMAX
+            *vel = vmul(v, speed);
+        }
+    }
+}
+/* the external-energy backflow (RadiationProcessor.cuh:345-354), accepted
+ * when the pool at the start of the step plus the amount stays within the
+ * limit; returns the particle's energy */
+static real backflow(OracleWorld* w, int color, real energy)
+{
+    const AlienPhysicsParams* p = &w->p;
+    if (!p->externalEnergyControl || !(p->externalEnergyBackflowFactor[color] > 0)) return energy;
+    real factor = p->externalEnergyBackflowFactor[color];
+    double add = (double)(energy * factor);
+    if (w->externalEnergy + add > (double)p->externalEnergyBackflowLimit) return energy;
+    w->backflowSum += add;
+    return energy * (1 - factor);
+}
+/* SimulationParametersUpdateService.cu:52-78 */
+static void moveOnTorus(const OracleWorld* w, float* x, float* y, float vx, float vy, float dt)
+{
+    real px = *x, py = *y;
+    if (R_ABS(vx) > NEAR_ZERO) px += (real)vx * dt;
+    if (R_ABS(vy) > NEAR_ZERO) py += (real)vy * dt;
+    vec2 c = correctPosition(w, v2(px, py));
+    *x = (float)c.x;
+    *y = (float)c.y;
+}
+
+/* ---- particle creation: ObjectFactory::createParticle (ObjectFactory.cuh
+ *      :242-256) for particles above NEAR_ZERO */
 static void createParticle(OracleWorld* w, vec2 pos, vec2 vel, int color, real energy)
 {
     pos = correctPosition(w, pos);
@@ -496,6 +728,17 @@ static void createParticle(OracleWorld* w, vec2 pos, vec2 vel, int color, real e
     w->pselected[k] = 0;
     w->palive[k] = 1;
     w->plastAbsorbed[k] = UINT64_MAX;
+}
+
+/* RadiationProcessor::createEnergyParticle (RadiationProcessor.cuh:248-364):
+ * at an active radiation source if there is one, then the external-energy
+ * backflow; draws keyed by the emitting cell's id */
+static void createEnergyParticle(OracleWorld* w, vec2 pos, vec2 vel, int color, real energy, uint64_t id, uint32_t site)
+{
+    placeAtSource(w, id, w->timestep, site, &pos, &vel);
+    pos = correctPosition(w, pos);
+    real kept = backflow(w, color, energy);
+    createParticle(w, pos, vel, color, kept);
 }
 
 static inline int isBonded(const OracleWorld* w, int64_t i, int64_t j)
@@ -543,7 +786,8 @@ static void radiationPhase(OracleWorld* w, uint64_t T)
         int c = w->color[i] % ALIEN_B200_MAX_COLORS;
         real factor = 0;
         if (w->energy[i] > (real)p->highRadiationMinCellEnergy[c]) factor += (real)p->highRadiationFactor[c];
-        if ((int64_t)w->age[i] > (int64_t)p->radiationMinCellAge[c]) factor += (real)p->radiationCellAgeStrength[c];
+        if ((int64_t)w->age[i] > (int64_t)p->radiationMinCellAge[c])
+            factor += zoneParam(w, ZF_RADIATION_CELL_AGE_STRENGTH, w->pos[i], p->radiationCellAgeStrength[c], c);
         if (!(factor > 0)) continue;
         real e = w->energy[i];
         real loss = e * factor;
@@ -556,7 +800,7 @@ static void radiationPhase(OracleWorld* w, uint64_t T)
             vec2 pp = vsub(vadd(w->pos[i], vmul(vnormalized(pv), (real)1.5)), pv);
             pp = correctPosition(w, pp);
             if (loss > e - 1) loss = e - 1;
-            createParticle(w, pp, pv, w->color[i], loss);
+            createEnergyParticle(w, pp, pv, w->color[i], loss, w->id[i], SITE_SOURCE_RADIATION);
             w->energy[i] -= loss;
         }
     }
@@ -574,6 +818,9 @@ static void fluidPhase(OracleWorld* w)
     for (int64_t i = 0; i < w->nCells; ++i) {
         if (!w->alive[i]) continue;
         vec2 pi = w->pos[i], vi = w->vel[i];
+        /* zone values at the cell, CellProcessor.cuh:149-152 */
+        const real fusionVelocity = zoneParam(w, ZF_CELL_FUSION_VELOCITY, pi, p->cellFusionVelocity, 0);
+        const real maxBindingEnergy = zoneParam(w, ZF_CELL_MAX_BINDING_ENERGY, pi, p->cellMaxBindingEnergy, 0);
         real dens = 0;
         vec2 Fp = v2(0, 0), Fv = v2(0, 0), dx = v2(0, 0);
         int64_t bestBarrier = -1;
@@ -607,9 +854,9 @@ static void fluidPhase(OracleWorld* w)
                                 Fp = vadd(Fp, vmul(vdiv(pd, -d), factor * kd));
                                 Fv = vadd(Fv, vmul(vdiv(vd, dj), d * kd / (d * d + (real)0.25)));
                             }
-                            if (vlen(vd) >= (real)p->cellFusionVelocity && w->numConn[i] < w->maxConn[i]
-                                && w->numConn[j] < w->maxConn[j] && w->energy[i] <= (real)p->cellMaxBindingEnergy
-                                && w->energy[j] <= (real)p->cellMaxBindingEnergy && !w->barrier[i] && !w->barrier[j]) {
+                            if (vlen(vd) >= fusionVelocity && w->numConn[i] < w->maxConn[i]
+                                && w->numConn[j] < w->maxConn[j] && w->energy[i] <= maxBindingEnergy
+                                && w->energy[j] <= maxBindingEnergy && !w->barrier[i] && !w->barrier[j]) {
                                 if (w->id[j] < bestId) {
                                     bestId = w->id[j];
                                     best = j;
@@ -684,6 +931,9 @@ static void collisionPhase(OracleWorld* w)
     for (int64_t i = 0; i < w->nCells; ++i) {
         if (!w->alive[i]) continue;
         vec2 pi = w->pos[i];
+        /* zone values at the cell, CellProcessor.cuh:344-353 */
+        const real fusionVelocity = zoneParam(w, ZF_CELL_FUSION_VELOCITY, pi, p->cellFusionVelocity, 0);
+        const real maxBindingEnergy = zoneParam(w, ZF_CELL_MAX_BINDING_ENERGY, pi, p->cellMaxBindingEnergy, 0);
         vec2 F = v2(0, 0), dx = v2(0, 0);
         int32_t best = -1;
         uint64_t bestId = UINT64_MAX;
@@ -705,8 +955,8 @@ static void collisionPhase(OracleWorld* w)
                     vec2 vd = vsub(w->vel[i], w->vel[j]);
                     int approaching = vdot(pd, vd) < 0;
                     if (w->numConn[i] < w->maxConn[i] && w->numConn[j] < w->maxConn[j]
-                        && vlen(vd) >= (real)p->cellFusionVelocity && approaching
-                        && w->energy[i] <= (real)p->cellMaxBindingEnergy && w->energy[j] <= (real)p->cellMaxBindingEnergy
+                        && vlen(vd) >= fusionVelocity && approaching
+                        && w->energy[i] <= maxBindingEnergy && w->energy[j] <= maxBindingEnergy
                         && !w->barrier[i] && !w->barrier[j]) {
                         if (w->id[j] < bestId) {
                             bestId = w->id[j];
@@ -802,6 +1052,7 @@ static void particlePhase(OracleWorld* w, int64_t nOrigParts)
     const AlienPhysicsParams* p = &w->p;
     for (int64_t q = 0; q < nOrigParts; ++q) {
         if (!w->palive[q]) continue;
+        if (p->numZones > 0) w->pvel[q] = vadd(w->pvel[q], flowAcceleration(w, w->ppos[q])); /* FlowFieldKernels.cu:71-87 */
         w->ppos[q] = correctPosition(w, vadd(w->ppos[q], vmul(w->pvel[q], (real)p->timestepSize)));
     }
     for (int64_t q = 0; q < nOrigParts; ++q) {
@@ -846,7 +1097,8 @@ static void particlePhase(OracleWorld* w, int64_t nOrigParts)
             }
         } else {
             if (w->plastAbsorbed[q] == w->id[c]) continue;
-            real absorption = (real)p->radiationAbsorption[w->color[c] % ALIEN_B200_MAX_COLORS];
+            int cc = w->color[c] % ALIEN_B200_MAX_COLORS;
+            real absorption = zoneParam(w, ZF_RADIATION_ABSORPTION, w->posPrime[c], p->radiationAbsorption[cc], cc);
             if (absorption < NEAR_ZERO) continue;
             real transfer = w->penergy[q] * absorption;
             if (w->penergy[q] < (real)0.01f) transfer = w->penergy[q];
@@ -1175,6 +1427,10 @@ static void stepOnce(OracleWorld* w)
     const int64_t nOrigParts = w->nParts; /* SimulationData::prepareForNextTimestep :46 */
     const int64_t N = w->nCells;
 
+    /* RadiationProcessor::calcActiveSources (physics_init, SimulationKernels.cu:23-27) */
+    w->activeSources = calcActiveSources(w);
+    w->backflowSum = 0;
+
     /* cudaNextTimestep_physics_init + fillMaps: SimulationKernels.cu:23-34 */
     for (int64_t i = 0; i < N; ++i) {
         w->force[i] = v2(0, 0);
@@ -1203,10 +1459,18 @@ static void stepOnce(OracleWorld* w)
         if (p->motionType == ALIEN_B200_MOTION_FLUID) w->density[i] = w->densNew[i];
         if (w->barrier[i]) continue;
         int c = w->color[i] % ALIEN_B200_MAX_COLORS;
-        if (vlen(w->force[i]) > (real)p->cellMaxForce[c]) {
+        /* flow fields (cudaApplyFlowFieldSettings, FlowFieldKernels.cu:48-70)
+         * add to the pair force at the cell after the overlap push */
+        vec2 F = w->force[i];
+        real maxForce = p->cellMaxForce[c];
+        if (p->numZones > 0) {
+            F = vadd(F, flowAcceleration(w, w->posPrime[i]));
+            maxForce = zoneParam(w, ZF_CELL_MAX_FORCE, w->posPrime[i], maxForce, c);
+        }
+        if (vlen(F) > maxForce) {
             if (draw(w->id[i], T, SITE_FORCE_DECAY) < p->cellMaxForceDecayProb) w->delAll[i] = 1;
         }
-        vec2 v = vadd(w->vel[i], w->force[i]);
+        vec2 v = vadd(w->vel[i], F);
         if (vlen(v) > (real)p->cellMaxVelocity) v = vmul(vnormalized(v), (real)p->cellMaxVelocity);
         w->vel[i] = v;
     }
@@ -1323,17 +1587,18 @@ static void stepOnce(OracleWorld* w)
     }
     for (int64_t i = 0; i < N; ++i) {
         if (!w->alive[i] || w->barrier[i]) continue;
-        w->vel[i] = vmul(w->vel[i], 1 - (real)p->friction);
+        w->vel[i] = vmul(w->vel[i], 1 - zoneParam(w, ZF_FRICTION, w->pos[i], p->friction, 0));
     }
     for (int64_t i = 0; i < N; ++i) {
         if (!w->alive[i] || w->barrier[i]) continue;
         int c = w->color[i] % ALIEN_B200_MAX_COLORS;
-        if (w->energy[i] > (real)p->cellMaxBindingEnergy) w->delAll[i] = 1;
+        if (w->energy[i] > zoneParam(w, ZF_CELL_MAX_BINDING_ENERGY, w->pos[i], p->cellMaxBindingEnergy, 0)) w->delAll[i] = 1;
         int ls = w->livingState[i];
         if (ls == ALIEN_B200_LIVING_DYING || ls == ALIEN_B200_LIVING_DETACHING) {
-            if (draw(w->id[i], T, SITE_DEATH) < p->cellDeathProbability[c]) w->delCell[i] = 1;
+            if (draw(w->id[i], T, SITE_DEATH) < zoneParam(w, ZF_CELL_DEATH_PROBABILITY, w->pos[i], p->cellDeathProbability[c], c))
+                w->delCell[i] = 1;
         }
-        int destroy = w->energy[i] < (real)p->cellMinEnergy[c];
+        int destroy = w->energy[i] < zoneParam(w, ZF_CELL_MIN_ENERGY, w->pos[i], p->cellMinEnergy[c], c);
         int64_t maxAge = p->cellMaxAge[c];
         if (maxAge > 0 && (int64_t)w->age[i] > maxAge) destroy = 1;
         if (destroy) {
@@ -1393,7 +1658,7 @@ static void stepOnce(OracleWorld* w)
     free(fusions);
     for (int64_t i = 0; i < N; ++i) {
         if (!w->alive[i] || !w->delCell[i]) continue;
-        createParticle(w, w->pos[i], w->vel[i], w->color[i], w->energy[i]);
+        createEnergyParticle(w, w->pos[i], w->vel[i], w->color[i], w->energy[i], w->id[i], SITE_SOURCE_DELETED_CELL);
         w->alive[i] = 0;
     }
     for (int64_t i = 0; i < N; ++i) {
@@ -1410,6 +1675,24 @@ static void stepOnce(OracleWorld* w)
     clearCellMap(w);
     compact(w);
     ++w->timestep;
+    /* the pool takes the step's backflow; zones and radiation sources move
+     * (SimulationParametersUpdateService.cu:52-78) */
+    w->externalEnergy += w->backflowSum;
+    for (int i = 0; i < p->numRadiationSources; ++i) {
+        AlienRadiationSource* r = &w->p.radiationSources[i];
+        moveOnTorus(w, &r->posX, &r->posY, r->velX, r->velY, p->timestepSize);
+    }
+    for (int i = 0; i < p->numZones; ++i) {
+        AlienZone* z = &w->p.zones[i];
+        moveOnTorus(w, &z->posX, &z->posY, z->velX, z->velY, p->timestepSize);
+    }
+}
+
+/* the parameters as the steps left them (zone and source positions, the pool) */
+void oracle_get_parameters(OracleWorld* w, AlienPhysicsParams* out)
+{
+    *out = w->p;
+    out->externalEnergy = (float)w->externalEnergy;
 }
 
 int oracle_step(OracleWorld* w, uint64_t n)

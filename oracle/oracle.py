@@ -42,6 +42,7 @@ def _load(name: str) -> ctypes.CDLL:
     lib.oracle_num_threads.restype = ctypes.c_int
     lib.oracle_set_threads.argtypes = [ctypes.c_int]
     lib.oracle_neuron_activities.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    lib.oracle_get_parameters.argtypes = [ctypes.c_void_p, ctypes.POINTER(PhysicsParams)]
     return lib
 
 
@@ -99,6 +100,14 @@ class OracleSimulation:
     def set_simulation_parameters(self, params: PhysicsParams):
         self._params = params.copy()
         self.lib.oracle_set_parameters(self.h, ctypes.byref(self._params))
+
+    def get_simulation_parameters(self) -> PhysicsParams:
+        """the parameters as they stand after the steps so far: zones and
+        radiation sources moved by their velocities, the external-energy
+        pool after backflow"""
+        out = PhysicsParams()
+        self.lib.oracle_get_parameters(self.h, ctypes.byref(out))
+        return out
 
     def calc_timesteps(self, n: int):
         self.lib.oracle_step(self.h, n)

@@ -81,6 +81,81 @@ SimulationParameters toReference(AlienPhysicsParams const& a)
         p.baseValues.cellMaxForce[c] = a.cellMaxForce[c];
         p.baseValues.cellMinEnergy[c] = a.cellMinEnergy[c];
         p.baseValues.cellDeathProbability[c] = a.cellDeathProbability[c];
+        p.externalEnergyBackflowFactor[c] = a.externalEnergyBackflowFactor[c];
+    }
+    p.baseValues.radiationDisableSources = a.radiationDisableSources != 0;
+    p.features.externalEnergyControl = a.externalEnergyControl != 0;
+    p.externalEnergy = a.externalEnergy;
+    p.externalEnergyBackflowLimit = a.externalEnergyBackflowLimit;
+
+    p.numZones = a.numZones;
+    for (int i = 0; i < a.numZones; ++i) {
+        AlienZone const& z = a.zones[i];
+        SimulationParametersZone& r = p.zone[i];
+        r.posX = z.posX;
+        r.posY = z.posY;
+        r.velX = z.velX;
+        r.velY = z.velY;
+        r.fadeoutRadius = z.fadeoutRadius;
+        r.shapeType = z.shapeType;
+        if (z.shapeType == SpotShapeType_Circular) {
+            r.shapeData.circularSpot.coreRadius = z.coreRadius;
+        } else {
+            r.shapeData.rectangularSpot.width = z.width;
+            r.shapeData.rectangularSpot.height = z.height;
+        }
+        r.flowType = z.flowType;
+        if (z.flowType == FlowType_Radial) {
+            r.flowData.radialFlow.orientation = z.flowOrientation;
+            r.flowData.radialFlow.strength = z.flowStrength;
+            r.flowData.radialFlow.driftAngle = z.flowDriftAngle;
+        } else if (z.flowType == FlowType_Central) {
+            r.flowData.centralFlow.strength = z.flowStrength;
+        } else if (z.flowType == FlowType_Linear) {
+            r.flowData.linearFlow.angle = z.flowAngle;
+            r.flowData.linearFlow.strength = z.flowStrength;
+        }
+        r.values.friction = z.friction;
+        r.values.rigidity = z.rigidity;
+        r.values.radiationDisableSources = z.radiationDisableSources != 0;
+        r.values.cellFusionVelocity = z.cellFusionVelocity;
+        r.values.cellMaxBindingEnergy = z.cellMaxBindingEnergy;
+        for (int c = 0; c < MAX_COLORS; ++c) {
+            r.values.radiationAbsorption[c] = z.radiationAbsorption[c];
+            r.values.radiationCellAgeStrength[c] = z.radiationCellAgeStrength[c];
+            r.values.cellMaxForce[c] = z.cellMaxForce[c];
+            r.values.cellMinEnergy[c] = z.cellMinEnergy[c];
+            r.values.cellDeathProbability[c] = z.cellDeathProbability[c];
+        }
+        r.activatedValues.friction = z.frictionActivated != 0;
+        r.activatedValues.rigidity = z.rigidityActivated != 0;
+        r.activatedValues.radiationAbsorption = z.radiationAbsorptionActivated != 0;
+        r.activatedValues.radiationCellAgeStrength = z.radiationCellAgeStrengthActivated != 0;
+        r.activatedValues.radiationDisableSources = z.radiationDisableSourcesActivated != 0;
+        r.activatedValues.cellMaxForce = z.cellMaxForceActivated != 0;
+        r.activatedValues.cellMinEnergy = z.cellMinEnergyActivated != 0;
+        r.activatedValues.cellDeathProbability = z.cellDeathProbabilityActivated != 0;
+        r.activatedValues.cellFusionVelocity = z.cellFusionVelocityActivated != 0;
+        r.activatedValues.cellMaxBindingEnergy = z.cellMaxBindingEnergyActivated != 0;
+    }
+    p.numRadiationSources = a.numRadiationSources;
+    for (int i = 0; i < a.numRadiationSources; ++i) {
+        AlienRadiationSource const& s = a.radiationSources[i];
+        RadiationSource& r = p.radiationSource[i];
+        r.strength = s.strength;
+        r.posX = s.posX;
+        r.posY = s.posY;
+        r.velX = s.velX;
+        r.velY = s.velY;
+        r.useAngle = s.useAngle != 0;
+        r.angle = s.angle;
+        r.shapeType = s.shapeType;
+        if (s.shapeType == RadiationSourceShapeType_Circular) {
+            r.shapeData.circularRadiationSource.radius = s.radius;
+        } else {
+            r.shapeData.rectangularRadiationSource.width = s.width;
+            r.shapeData.rectangularRadiationSource.height = s.height;
+        }
     }
     return p;
 }

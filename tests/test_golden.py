@@ -54,6 +54,18 @@ HAVE_OBSERVABLES = os.path.exists(os.path.join(GOLDEN, "ref_observables.json"))
 needs_observables = pytest.mark.skipif(not HAVE_OBSERVABLES, reason="reference observables not generated yet")
 
 
+def fixture_params(f, motion) -> P.PhysicsParams:
+    """the fixture's parameter block; fixtures written before fields were
+    appended to the struct (zones, sources, external energy) keep the
+    defaults for the appended fields"""
+    if "params" not in f:
+        return P.benchmark_parameters(motion)
+    raw = f["params"].tobytes()
+    full = bytearray(bytes(P.default_parameters()))
+    full[: len(raw)] = raw
+    return P.PhysicsParams.from_buffer_copy(bytes(full))
+
+
 @pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p) for p in FIXTURES])
 def test_oracle_matches_reference_one_step(path):
     f = np.load(path)
@@ -62,15 +74,7 @@ def test_oracle_matches_reference_one_step(path):
     assert world == (wx, wy)
     assert np.array_equal(data.cells, f["in_cells"]) and np.array_equal(data.particles, f["in_particles"]), \
         "the seeded generator no longer reproduces the fixture input"
-    if "params" in f:
-        raw = f["params"].tobytes()
-        # fixtures written before a field was appended to the struct keep the
-        # defaults for the appended fields
-        full = bytearray(bytes(P.default_parameters()))
-        full[: len(raw)] = raw
-        prm = P.PhysicsParams.from_buffer_copy(bytes(full))
-    else:
-        prm = P.benchmark_parameters(motion)
+    prm = fixture_params(f, motion)
     o = OracleSimulation(world, prm, t)
     o.set_simulation_data(data)
     o.calc_timesteps(1)
@@ -145,7 +149,7 @@ def test_oracle_neurons_match_reference(path):
     assert world == (wx, wy)
     assert np.array_equal(data.cells, f["in_cells"]) and np.array_equal(data.aux, f["in_aux"]), \
         "the seeded generator no longer reproduces the fixture input"
-    prm = P.PhysicsParams.from_buffer_copy(f["params"].tobytes())
+    prm = fixture_params(f, motion)
     o = OracleSimulation(world, prm, t)
     o.set_simulation_data(data)
     o.calc_timesteps(steps)
@@ -221,7 +225,7 @@ def test_engine_neurons_match_reference(path):
     f = np.load(path)
     seed, motion, t, wx, wy, ts, steps = (int(v) for v in f["meta"])
     data, world = make_golden.neuron_world(seed)
-    prm = P.PhysicsParams.from_buffer_copy(f["params"].tobytes())
+    prm = fixture_params(f, motion)
     eng = SimulationFacade()
     eng.new_simulation(t, world, prm)
     eng.set_simulation_data(data)
@@ -249,13 +253,7 @@ def test_engine_matches_reference_one_step(path):
     f = np.load(path)
     seed, motion, t, wx, wy, ts = (int(v) for v in f["meta"])
     data, world = worldgen.calm_test_world(seed)
-    if "params" in f:
-        raw = f["params"].tobytes()
-        full = bytearray(bytes(P.default_parameters()))
-        full[: len(raw)] = raw
-        prm = P.PhysicsParams.from_buffer_copy(bytes(full))
-    else:
-        prm = P.benchmark_parameters(motion)
+    prm = fixture_params(f, motion)
     eng = SimulationFacade()
     eng.new_simulation(t, world, prm)
     eng.set_simulation_data(data)

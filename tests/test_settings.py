@@ -33,9 +33,22 @@ def test_reads_the_reference_sample_file():
     assert prm.radiationAbsorption[1] == pytest.approx(0.0679)
     assert prm.highRadiationMinCellEnergy[3] == pytest.approx(1483.98205566)
     assert prm.particleSplitEnergy[0] == np.finfo(np.float32).max
-    # the sample uses zones, radiation sources and external energy control
-    assert set(unsupported) == {"numZones", "numRadiationSources", "externalEnergyControl"}
+    # the sample's zones, radiation sources and external-energy backflow
+    assert unsupported == []
     assert prm.numZones == 3 and prm.numRadiationSources == 3
+    z0, z2 = prm.zones[0], prm.zones[2]
+    assert (z0.posX, z0.posY, z0.shapeType, z0.flowType) == (500.0, 500.0, P.SHAPE_CIRCULAR, P.FLOW_RADIAL)
+    assert z0.coreRadius == pytest.approx(367.7) and z0.fadeoutRadius == pytest.approx(154.8)
+    assert z0.flowStrength == pytest.approx(0.00305) and z0.flowDriftAngle == pytest.approx(2.6)
+    assert z0.radiationCellAgeStrengthActivated == 1 and z0.frictionActivated == 0
+    assert (z2.shapeType, z2.width, z2.flowType) == (P.SHAPE_RECTANGULAR, 2000.0, P.FLOW_NONE)
+    assert z2.height == pytest.approx(54.8)
+    s0, s2 = prm.radiationSources[0], prm.radiationSources[2]
+    assert (s0.posX, s0.posY, s0.shapeType, s0.radius) == (502.0, 502.0, P.SHAPE_CIRCULAR, 82.0)
+    assert (s2.shapeType, s2.useAngle, s2.angle, s2.height) == (P.SHAPE_RECTANGULAR, 1, 90.0, 164.0)
+    assert s0.strength == pytest.approx(1 / 3)
+    assert prm.externalEnergyControl == 1 and prm.externalEnergyBackflowFactor[0] == pytest.approx(0.1436)
+    assert prm.externalEnergyBackflowFactor[1] == 0.0
 
 
 def test_write_read_round_trip(tmp_path):
@@ -56,6 +69,31 @@ def test_write_read_round_trip(tmp_path):
             assert list(a) == pytest.approx(list(b), rel=1e-7, abs=1e-8), name
         else:
             assert a == pytest.approx(b, rel=1e-7, abs=1e-8), name
+
+
+def test_zones_and_sources_round_trip(tmp_path):
+    """a reference file read and written again keeps its zones, sources and
+    backflow values; a zone with rigidity activated is named unsupported"""
+    _, _, prm, _ = settings.read_settings(GOLDEN)
+    path = tmp_path / "z.settings.json"
+    settings.write_settings(str(path), 5, (2000, 1000), prm)
+    _, _, got, unsupported = settings.read_settings(str(path))
+    assert unsupported == []
+    for i in range(prm.numZones):
+        for name, _ in P.Zone._fields_:
+            a, b = getattr(got.zones[i], name), getattr(prm.zones[i], name)
+            if hasattr(a, "__len__"):
+                assert list(a) == pytest.approx(list(b), rel=1e-7), (i, name)
+            else:
+                assert a == pytest.approx(b, rel=1e-7), (i, name)
+    for i in range(prm.numRadiationSources):
+        for name, _ in P.RadiationSource._fields_:
+            assert getattr(got.radiationSources[i], name) == pytest.approx(getattr(prm.radiationSources[i], name),
+                                                                           rel=1e-7), (i, name)
+    assert list(got.externalEnergyBackflowFactor) == pytest.approx(list(prm.externalEnergyBackflowFactor), rel=1e-7)
+    prm.zones[1].rigidityActivated, prm.zones[1].rigidity = 1, 0.5
+    settings.write_settings(str(path), 5, (2000, 1000), prm)
+    assert settings.read_settings(str(path))[3] == ["zones[1].rigidity"]
 
 
 def test_written_layout_is_the_reference_layout(tmp_path):
