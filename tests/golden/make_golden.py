@@ -34,6 +34,13 @@ ONE_STEP = [
     ("calm_collision_t3_nofric", 26, P.MOTION_COLLISION, 3, 0.0),
 ]
 
+ZONE_ONE_STEP = [
+    # name, seed, motion, timestep: calm worlds under three zones with flow
+    # fields and friction (see zone_params)
+    ("calm_zone_fluid_t1", 27, P.MOTION_FLUID, 1),
+    ("calm_zone_collision_t2", 28, P.MOTION_COLLISION, 2),
+]
+
 
 NEURON_RUNS = [
     # name, seed, motion, timestep, steps: calm worlds with neuron cells; the
@@ -52,6 +59,25 @@ def one_step_params(motion, inner_friction):
     prm = P.benchmark_parameters(motion)
     if inner_friction is not None:
         prm.innerFriction = inner_friction
+    return prm
+
+
+def zone_params(motion):
+    """three zones over the 64x64 calm world: a clockwise radial flow with
+    drift and zone friction, a rectangular central flow, a linear flow with a
+    second friction value; everything else at the benchmark values"""
+    prm = P.benchmark_parameters(motion)
+    prm.numZones = 3
+    z0, z1, z2 = (P.default_zone(prm.zones[i], prm) for i in range(3))
+    z0.posX, z0.posY, z0.coreRadius, z0.fadeoutRadius = 18.0, 20.0, 9.0, 12.0
+    z0.flowType, z0.flowStrength, z0.flowDriftAngle = P.FLOW_RADIAL, 0.004, 15.0
+    z0.frictionActivated, z0.friction = 1, 0.02
+    z1.posX, z1.posY, z1.shapeType, z1.width, z1.height, z1.fadeoutRadius = 46.0, 18.0, P.SHAPE_RECTANGULAR, 18.0, \
+        14.0, 10.0
+    z1.flowType, z1.flowStrength = P.FLOW_CENTRAL, 0.05
+    z2.posX, z2.posY, z2.coreRadius, z2.fadeoutRadius = 32.0, 48.0, 10.0, 14.0
+    z2.flowType, z2.flowAngle, z2.flowStrength = P.FLOW_LINEAR, 120.0, 0.003
+    z2.frictionActivated, z2.friction = 1, 0.0
     return prm
 
 
@@ -95,7 +121,17 @@ def decay_input():
 
 
 def main(out_dir):
+    """ZONES_ONLY=1 writes only the zone fixtures; NEURON_ONLY=1 stops after
+    the one-step and neuron fixtures"""
     os.makedirs(out_dir, exist_ok=True)
+    zone_fixtures(out_dir)
+    if os.environ.get("ZONES_ONLY"):
+        return
+    one_step_fixtures(out_dir)
+    more_fixtures(out_dir)
+
+
+def one_step_fixtures(out_dir):
     for name, seed, motion, t, fric in ONE_STEP:
         data, world = calm(seed)
         prm = one_step_params(motion, fric)
@@ -105,6 +141,21 @@ def main(out_dir):
                             params=np.frombuffer(bytes(prm), np.uint8),
                             meta=np.array([seed, motion, t, world[0], world[1], ts], np.int64))
         print(name, out.num_cells, out.num_particles, ts)
+
+
+def zone_fixtures(out_dir):
+    for name, seed, motion, t in ZONE_ONE_STEP:
+        data, world = calm(seed)
+        prm = zone_params(motion)
+        out, _, ts = refrun.run(data, world, prm, steps=1, timestep=t)
+        np.savez_compressed(os.path.join(out_dir, f"ref_{name}.npz"), in_cells=data.cells, in_particles=data.particles,
+                            out_cells=out.cells, out_particles=out.particles,
+                            params=np.frombuffer(bytes(prm), np.uint8),
+                            meta=np.array([seed, motion, t, world[0], world[1], ts], np.int64))
+        print(name, out.num_cells, out.num_particles, ts)
+
+
+def more_fixtures(out_dir):
     for name, seed, motion, t, steps in NEURON_RUNS:
         data, world = neuron_world(seed)
         prm = P.benchmark_parameters(motion)

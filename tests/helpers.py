@@ -9,7 +9,8 @@ difference, scaled by max(|b|, |position before the step|, 1) when the
 input state is given: a coordinate that crossed the seam (511.99 + 0.02 ->
 0.01 on a 512-wide torus) was computed in FP32 at its pre-wrap magnitude,
 where one unit in the last place is 6e-5, and carries that rounding after
-the wrap.  Integer and index fields (ids, bond partners, counts, living
+the wrap; an object created in the steps compared has no earlier position,
+and near the low seam its scale is the world's extent.  Integer and index fields (ids, bond partners, counts, living
 states) must match exactly.
 """
 from __future__ import annotations
@@ -17,6 +18,9 @@ from __future__ import annotations
 import numpy as np
 
 RTOL = 1e-5
+# a new object this close to the low seam may have crossed it in its first
+# steps (speeds are at most a few units per step)
+SEAM_MARGIN = 4.0
 
 
 def _wrapped_diff(a, b, size):
@@ -58,16 +62,23 @@ def rel_err(a, b, scale=1.0):
     return np.abs(a - b) / np.maximum(np.abs(b), scale)
 
 
-def position_scale(ref_sorted, before=None):
+def position_scale(ref_sorted, before=None, world=None):
     """max(|b|, |position before the step|, 1) per component, for objects
-    sorted by id; objects created in the step have no earlier position"""
+    sorted by id.  Objects created in the step have no earlier position: one
+    that lies within ``SEAM_MARGIN`` of the low seam may have been created
+    just below the high seam and crossed it, so that component is scaled by
+    the world's extent"""
     scale = np.maximum(np.abs(ref_sorted["pos"].astype(np.float64)), 1.0)
+    known = np.zeros(len(ref_sorted), bool)
     if before is not None and len(before):
         b = before[np.argsort(before["id"], kind="stable")]
         at = np.searchsorted(b["id"], ref_sorted["id"])
         at = np.minimum(at, len(b) - 1)
         known = b["id"][at] == ref_sorted["id"]
         scale[known] = np.maximum(scale[known], np.abs(b["pos"][at[known]].astype(np.float64)))
+    if before is not None and world is not None:
+        near = (~known)[:, None] & (np.abs(ref_sorted["pos"].astype(np.float64)) < SEAM_MARGIN)
+        scale = np.where(near, np.maximum(scale, np.asarray(world, np.float64)[None, :]), scale)
     return scale
 
 
@@ -83,7 +94,7 @@ def compare_cells(got, ref, world, rtol=RTOL, check_bonds=True, report=None, bef
     W, H = world
     dpos = np.stack([_wrapped_diff(g["pos"][:, 0].astype(np.float64), r["pos"][:, 0].astype(np.float64), W),
                      _wrapped_diff(g["pos"][:, 1].astype(np.float64), r["pos"][:, 1].astype(np.float64), H)], axis=1)
-    errs["pos"] = float(np.max(np.abs(dpos) / position_scale(r, before), initial=0))
+    errs["pos"] = float(np.max(np.abs(dpos) / position_scale(r, before, world), initial=0))
     errs["vel"] = float(np.max(rel_err(g["vel"], r["vel"]), initial=0))
     errs["energy"] = float(np.max(rel_err(g["energy"], r["energy"]), initial=0))
     assert np.array_equal(g["livingState"], r["livingState"]), "living states differ"
@@ -116,7 +127,7 @@ def compare_particles(got, ref, world, rtol=RTOL, before=None):
     dpos = np.stack([_wrapped_diff(g["pos"][:, 0].astype(np.float64), r["pos"][:, 0].astype(np.float64), W),
                      _wrapped_diff(g["pos"][:, 1].astype(np.float64), r["pos"][:, 1].astype(np.float64), H)], axis=1)
     errs = {
-        "ppos": float(np.max(np.abs(dpos) / position_scale(r, before), initial=0)),
+        "ppos": float(np.max(np.abs(dpos) / position_scale(r, before, world), initial=0)),
         "pvel": float(np.max(rel_err(g["vel"], r["vel"]), initial=0)),
         "penergy": float(np.max(rel_err(g["energy"], r["energy"]), initial=0)),
     }

@@ -210,15 +210,19 @@ def test_zones_match_oracle(motion, steps):
     data.cells["livingState"][::9] = 3  # detaching: zone death probability
     prm = zone_params(motion)
     got, ref, _, _ = run_both(data, world, prm, steps)
-    compare_cells(got.cells, ref.cells, world, before=data.cells)
-    compare_particles(got.particles, ref.particles, world, before=data.particles)
+    rtol = 1e-5 if steps == 1 else 5e-5  # FP32 rounding compounds over steps
+    compare_cells(got.cells, ref.cells, world, rtol=rtol, before=data.cells)
+    compare_particles(got.particles, ref.particles, world, rtol=rtol, before=data.particles)
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("motion", [P.MOTION_FLUID, P.MOTION_COLLISION])
 def test_radiation_sources_match_oracle(motion):
     """three sources, one of them switched off by a zone; emitted particles
-    start inside the active sources"""
+    start inside the active sources.  A source is drawn by comparing one
+    uniform draw in [0, 1) with the running sum of the active sources'
+    strengths (RadiationProcessor.cuh:253-270), so the strengths of the
+    active sources sum to 1 here, as the reference's editor keeps them"""
     data, world = zone_world(42)
     data.cells["age"] = np.random.default_rng(42).integers(0, 400, len(data.cells)).astype(np.uint32)
     prm = P.default_parameters()
@@ -226,8 +230,8 @@ def test_radiation_sources_match_oracle(motion):
     for c in range(P.MAX_COLORS):
         prm.radiationCellAgeStrength[c] = 0.002
     prm.numRadiationSources = 3
-    shapes = [(20.0, 20.0, 2.0, P.SHAPE_CIRCULAR, 5.0, 0, 0.0), (90.0, 60.0, 1.0, P.SHAPE_RECTANGULAR, 0.0, 1, 45.0),
-              (60.0, 110.0, 3.0, P.SHAPE_CIRCULAR, 3.0, 0, 0.0)]
+    shapes = [(20.0, 20.0, 0.4, P.SHAPE_CIRCULAR, 5.0, 0, 0.0), (90.0, 60.0, 0.6, P.SHAPE_RECTANGULAR, 0.0, 1, 45.0),
+              (60.0, 110.0, 0.5, P.SHAPE_CIRCULAR, 3.0, 0, 0.0)]
     for s, (x, y, strength, shape, radius, use_angle, angle) in zip(prm.radiationSources, shapes):
         s.posX, s.posY, s.strength, s.shapeType, s.radius, s.useAngle, s.angle = x, y, strength, shape, radius, \
             use_angle, angle
@@ -291,17 +295,25 @@ def test_zone_and_source_movement_matches_oracle():
 
 
 @pytest.mark.gpu
-def test_reference_sample_settings_match_oracle():
+@pytest.mark.parametrize("dt", [0, 1, 2])
+def test_reference_sample_settings_match_oracle(dt):
     """the reference's own sample settings (fluid motion, three zones with
     radial flows, three radiation sources, backflow on) over a random world
-    of the sample's size"""
+    of the sample's size, one step from each phase of the three-step cycle.
+    One step only: the world reaches x = 2000, where FP32 positions (the
+    transfer objects' type) resolve 1.2e-4, so two close cells' distance
+    after a stored step carries ~1e-3 relative error into the next step's
+    fluid forces."""
     t, world, prm, unsupported = settings.read_settings(SAMPLE)
     assert unsupported == []
     data, world = worldgen.random_test_world(45, world=world, clusters=60, hex_clusters=20, free_cells=6000,
                                              particles=2000)
     data.cells["age"] = np.random.default_rng(45).integers(0, 300000, len(data.cells)).astype(np.uint32)
-    got, ref, gp, rp = run_both(data, world, prm, 2, t)
+    got, ref, gp, rp = run_both(data, world, prm, 1, t + dt)
     compare_cells(got.cells, ref.cells, world, before=data.cells)
     compare_particles(got.particles, ref.particles, world, before=data.particles)
+    first_new = max(int(data.cells["id"].max()), int(data.particles["id"].max()))
+    assert np.count_nonzero(got.particles["id"] > first_new) > 50, "the sample's radiation emitted too little"
     assert gp.externalEnergy == pytest.approx(rp.externalEnergy, rel=1e-5, abs=1e-3)
-    assert not math.isnan(gp.zones[0].posX)
+    for i in range(prm.numZones):
+        assert (gp.zones[i].posX, gp.zones[i].posY) == (rp.zones[i].posX, rp.zones[i].posY)
