@@ -197,6 +197,13 @@ struct DevState {
     // accumulated statistics, per world and color: neuron cells that ran
     unsigned long long* neuronActivity;
 
+    // rigidity clusters (allocated when some world enables rigidity)
+    int* clusterLab[2];         // cluster labels, two buffers of the propagation rounds
+    uint32_t* clusterCount;     // per cluster: cells
+    long long* clusterAcc;      // [cluster * 6]: velocity, offset from the label cell, angular mass and
+                                // momentum (fixed point)
+    uint32_t* clusterChanged;   // per propagation round: some label changed
+
     // event scan scratch (per block)
     uint32_t* blockRad;
     uint32_t* blockDel;

@@ -26,6 +26,7 @@
 #include "device_common.cuh"
 #include "io_kernels.cuh"
 #include "kernels.cuh"
+#include "rigidity.cuh"
 
 namespace ab {
 
@@ -138,11 +139,8 @@ static void validateParams(const AlienPhysicsParams& p, int W, int H)
         throw Error(ALIEN_B200_ERR_UNSUPPORTED, "particle-to-cell transformation is outside the physics stage");
     if (p.cellAgeLimiter || p.cellColorTransitionRules || p.advancedAbsorptionControl)
         throw Error(ALIEN_B200_ERR_UNSUPPORTED, "feature flags of cell functions (age limiter, color transitions, absorption control) must be off");
-    if (p.rigidity != 0.0f) throw Error(ALIEN_B200_ERR_UNSUPPORTED, "rigidity clusters (rigidity != 0) are not supported");
     for (int i = 0; i < p.numZones; ++i) {
         const AlienZone& z = p.zones[i];
-        if (z.rigidityActivated && z.rigidity != 0.0f)
-            throw Error(ALIEN_B200_ERR_UNSUPPORTED, "rigidity clusters (a zone with rigidity != 0) are not supported");
         if (z.shapeType != ALIEN_B200_SHAPE_CIRCULAR && z.shapeType != ALIEN_B200_SHAPE_RECTANGULAR)
             throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "zone shape type must be 0 (circular) or 1 (rectangular)");
         if (z.flowType < ALIEN_B200_FLOW_NONE || z.flowType > ALIEN_B200_FLOW_LINEAR)
@@ -313,6 +311,7 @@ private:
     uint64_t stepsSinceCheck_ = 0;
     bool hasFluid_ = false, hasCollision_ = false, hasNeurons_ = false;
     bool hasWorldParams_ = false;  // some world has zones, radiation sources or external energy (kWorldsEnd)
+    bool hasRigidity_ = false;     // some world enables rigidity: the cluster arrays exist and the step runs the cluster pass
     static bool needsWorldParams(const AlienPhysicsParams& p)
     {
         return p.numZones > 0 || p.numRadiationSources > 0 || p.externalEnergyControl;
@@ -498,9 +497,10 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     }
     hasNeurons_ = neuronsTotal > 0;
     signalsLive_ = hasNeurons_ || signalsTotal > 0;
-    hasFluid_ = hasCollision_ = hasWorldParams_ = false;
+    hasFluid_ = hasCollision_ = hasWorldParams_ = hasRigidity_ = false;
     for (const HostWorld& hw : worlds_) {
         hasWorldParams_ |= needsWorldParams(hw.params);
+        hasRigidity_ |= rigidityEnabled(hw.params);
         if (hw.info.motionType == ALIEN_B200_MOTION_FLUID)
             hasFluid_ = true;
         else
@@ -581,6 +581,13 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     s.energyAcc = mem_.alloc<long long>(C);
     s.best = mem_.alloc<int>(C);
     s.newPartner = mem_.alloc<int>(C);
+    if (hasRigidity_) {
+        s.clusterLab[0] = mem_.alloc<int>(C);
+        s.clusterLab[1] = mem_.alloc<int>(C);
+        s.clusterCount = mem_.alloc<uint32_t>(C);
+        s.clusterAcc = mem_.alloc<long long>(C * kAccFields);
+        s.clusterChanged = mem_.alloc<uint32_t>(kClusterRounds);
+    }
     s.addNum = mem_.alloc<uint8_t>(C);
     s.addBond = mem_.alloc<int>(C * kMaxBonds);
     s.addDist = mem_.alloc<float>(C * kMaxBonds);
@@ -743,6 +750,16 @@ void Arena::enqueueStep()
     launch(kBond2, both, kBlock, s);
     launch(kVerletVel, both, kBlock, s);
     launch(kTransition, both, kBlock, s);
+    if (hasRigidity_) {
+        launch(kClusterInit, cells, kBlock, s);
+        for (int r = 0; r < kClusterRounds; ++r) {
+            launch(kClusterGather, cells, kBlock, s, r);
+            launch(kClusterScatter, cells, kBlock, s, r);
+        }
+        launch(kClusterSum1, cells, kBlock, s);
+        launch(kClusterSum2, cells, kBlock, s);
+        launch(kClusterApply, cells, kBlock, s);
+    }
     launch(kResolve, cells, kBlock, s);
     if (hasNeurons_) launch(kNeuron, cells, kBlock, s);
     if (signalsLive_) launch(kSignalReset, cells, kBlock, s);
@@ -961,9 +978,12 @@ void Arena::setParams(int w, const AlienPhysicsParams& p)
 {
     HostWorld& hw = worlds_[w];
     validateParams(p, hw.info.W, hw.info.H);
-    const bool relayout = scanRadius(p) != hw.info.radiusInt || p.motionType != hw.info.motionType;
+    // the tile grid depends on the interaction radius, and the cluster arrays
+    // exist only in arenas built with rigidity
+    const bool relayout = scanRadius(p) != hw.info.radiusInt || p.motionType != hw.info.motionType ||
+                          (rigidityEnabled(p) && !s_.clusterAcc);
     if (relayout) {
-        // the tile grid depends on the interaction radius: rebuild the arena
+        // rebuild the arena
         std::vector<std::vector<AlienCellTO>> cells(numWorlds());
         std::vector<std::vector<AlienParticleTO>> parts(numWorlds());
         for (int v = 0; v < numWorlds(); ++v) {
@@ -988,11 +1008,15 @@ void Arena::setParams(int w, const AlienPhysicsParams& p)
     std::vector<WorldCounters> c = readCounters();
     c[w].externalEnergy = p.externalEnergy;
     AB_CK(cudaMemcpyAsync(s_.counters + w, &c[w], sizeof(WorldCounters), cudaMemcpyHostToDevice, stream_));
-    bool any = false;
-    for (const HostWorld& x : worlds_) any |= needsWorldParams(x.params);
-    if (any != hasWorldParams_) {
+    bool any = false, rigid = false;
+    for (const HostWorld& x : worlds_) {
+        any |= needsWorldParams(x.params);
+        rigid |= rigidityEnabled(x.params);
+    }
+    if (any != hasWorldParams_ || rigid != hasRigidity_) {
         hasWorldParams_ = any;
-        releaseGraph();  // the step gains or loses its kWorldsEnd launch
+        hasRigidity_ = rigid;
+        releaseGraph();  // the step gains or loses its kWorldsEnd launch or its cluster pass
     }
     if (hasWorldParams_) launch(kWorldsBegin, divUp(numWorlds(), kBlock), kBlock, s_);
     sync();

@@ -18,9 +18,9 @@ backflow (:271-300); the rest of the file (rendering, genome mutation,
 cell-function parameters) belongs to other parts of the reference.  A zone
 value has an ``activated`` flag: ``<key>.activated`` with ``<key>.value``, or
 with ``<key>[c]`` for color-dependent values (ParameterParser.h:155-210).  The
-fields whose non-default values the engine rejects (rigidity, in the base or
-in a zone, particle transformation, cell-function feature flags) are read so
-that ``read_settings`` can name them.  ``innerFriction`` has no key in the
+fields whose non-default values the engine rejects (particle transformation,
+cell-function feature flags) are read so that ``read_settings`` can name
+them.  ``innerFriction`` has no key in the
 reference's files.
 """
 from __future__ import annotations
@@ -115,7 +115,7 @@ _MOTION_KEYS = {
     P.MOTION_COLLISION: {"cellMaxCollisionDistance", "cellRepulsionStrength"},
 }
 # fields whose non-default values the engine rejects (ALIEN_B200_ERR_UNSUPPORTED)
-_UNSUPPORTED = ("rigidity", "particleTransformationAllowed", "cellAgeLimiter", "cellColorTransitionRules",
+_UNSUPPORTED = ("particleTransformationAllowed", "cellAgeLimiter", "cellColorTransitionRules",
                 "advancedAbsorptionControl")
 
 
@@ -192,8 +192,6 @@ def decode(tree: dict) -> tuple[int, tuple[int, int], P.PhysicsParams, list[str]
     _decode_sources(tree, prm)
     default = P.default_parameters()
     unsupported = [n for n in _UNSUPPORTED if getattr(prm, n) != getattr(default, n)]
-    unsupported += [f"zones[{i}].rigidity" for i in range(prm.numZones)
-                    if prm.zones[i].rigidityActivated and prm.zones[i].rigidity != 0.0]
     return timestep, world, prm, unsupported
 
 

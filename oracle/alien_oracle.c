@@ -1417,6 +1417,94 @@ static void signalReset(OracleWorld* w, uint64_t T)
     }
 }
 
+/* ---- rigidity clusters (ClusterProcessor.cuh:8-168, every third step after
+ *      friction, SimulationKernelsLauncher.cu:74-83).  Clusters by the same
+ *      synchronous Shiloach-Vishkin rounds as the engine (gather: shortcut
+ *      and aggressive hooking from the previous labels; scatter: hooking of
+ *      the cell's label by minima; at most CLUSTER_ROUNDS rounds, ended by a
+ *      round that changes nothing), offsets from the label cell by minimal
+ *      image, sums in double (the reference: three lock-free label walks,
+ *      float atomics, and a world-thirds seam correction that agrees with
+ *      the minimal image for clusters smaller than a third of the world) */
+#define CLUSTER_ROUNDS 12
+static int rigidityEnabled(const AlienPhysicsParams* p) /* SimulationKernelsLauncher.cu:99-107 */
+{
+    for (int i = 0; i < p->numZones; ++i)
+        if (p->zones[i].rigidity != 0.0f) return 1;
+    return p->rigidity != 0.0f;
+}
+
+static void rigidityPhase(OracleWorld* w)
+{
+    const AlienPhysicsParams* p = &w->p;
+    const int64_t N = w->nCells;
+    if (N == 0) return;
+    int32_t* lab[2] = {malloc(sizeof(int32_t) * (size_t)N), malloc(sizeof(int32_t) * (size_t)N)};
+    for (int64_t i = 0; i < N; ++i) lab[0][i] = (int32_t)i;
+    int cur = 0;
+    for (int r = 0; r < CLUSTER_ROUNDS; ++r) {
+        const int32_t* f = lab[r & 1];
+        int32_t* g = lab[(r + 1) & 1];
+        int changed = 0;
+        for (int64_t i = 0; i < N; ++i) {
+            if (!w->alive[i]) continue;
+            int32_t m = f[f[i]] < f[i] ? f[f[i]] : f[i];
+            for (int k = 0; k < w->numConn[i]; ++k) {
+                int32_t x = f[f[w->bond[i][k]]];
+                if (x < m) m = x;
+            }
+            g[i] = m;
+            changed |= m != f[i];
+        }
+        for (int64_t i = 0; i < N; ++i) {
+            if (!w->alive[i]) continue;
+            int32_t m = f[i];
+            for (int k = 0; k < w->numConn[i]; ++k) {
+                int32_t x = f[f[w->bond[i][k]]];
+                if (x < m) m = x;
+            }
+            if (m < g[f[i]]) {
+                g[f[i]] = m;
+                changed = 1;
+            }
+        }
+        cur = (r + 1) & 1;
+        if (!changed) break;
+    }
+    const int32_t* cl = lab[cur];
+    vec2* velSum = calloc((size_t)N, sizeof(vec2));
+    vec2* relSum = calloc((size_t)N, sizeof(vec2));
+    real* mass = calloc((size_t)N, sizeof(real));
+    real* mom = calloc((size_t)N, sizeof(real));
+    int64_t* count = calloc((size_t)N, sizeof(int64_t));
+    vec2* rel = malloc(sizeof(vec2) * (size_t)N);
+    for (int64_t i = 0; i < N; ++i) {
+        if (!w->alive[i]) continue;
+        rel[i] = correctDirection(w, vsub(w->pos[i], w->pos[cl[i]]));
+        velSum[cl[i]] = vadd(velSum[cl[i]], w->vel[i]);
+        relSum[cl[i]] = vadd(relSum[cl[i]], rel[i]);
+        count[cl[i]] += 1;
+    }
+    for (int64_t i = 0; i < N; ++i) {
+        if (!w->alive[i]) continue;
+        const int32_t c = cl[i];
+        vec2 cv = vdiv(velSum[c], (real)count[c]), r = vsub(rel[i], vdiv(relSum[c], (real)count[c]));
+        vec2 dv = vsub(w->vel[i], cv);
+        mass[c] += r.x * r.x + r.y * r.y;     /* Math::lengthSquared */
+        mom[c] += r.x * dv.y - r.y * dv.x;     /* Physics::angularMomentum */
+    }
+    for (int64_t i = 0; i < N; ++i) {
+        if (!w->alive[i]) continue;
+        const int32_t c = cl[i];
+        vec2 cv = vdiv(velSum[c], (real)count[c]), r = vsub(rel[i], vdiv(relSum[c], (real)count[c]));
+        real av = R_ABS(mass[c]) < NEAR_ZERO ? 0 : mom[c] / mass[c] * RAD_TO_DEG; /* Physics.cuh:191-197 */
+        real rigidity = zoneParam(w, ZF_RIGIDITY, w->pos[i], p->rigidity, 0) * w->stiffness[i] * w->stiffness[i];
+        vec2 tangential = v2(cv.x - av * r.y * DEG_TO_RAD, cv.y + av * r.x * DEG_TO_RAD); /* Physics.cuh:181-184 */
+        w->vel[i] = vadd(vmul(w->vel[i], 1 - rigidity), vmul(tangential, rigidity));
+    }
+    free(lab[0]); free(lab[1]); free(velSum); free(relSum); free(mass); free(mom); free(count); free(rel);
+}
+
 static void stepOnce(OracleWorld* w)
 {
     const AlienPhysicsParams* p = &w->p;
@@ -1615,6 +1703,7 @@ static void stepOnce(OracleWorld* w)
             if (w->livingState[j] != ALIEN_B200_LIVING_DYING) w->livingState[j] = ALIEN_B200_LIVING_DETACHING;
         }
     }
+    if (T % 3 == 0 && rigidityEnabled(p)) rigidityPhase(w); /* SimulationKernelsLauncher.cu:33, 74-83 */
 
     /* structuralOperations_substep2..4 (SimulationKernels.cu:167-180): every
      * new bond list is computed from the lists as they stand before the

@@ -73,7 +73,7 @@ def test_write_read_round_trip(tmp_path):
 
 def test_zones_and_sources_round_trip(tmp_path):
     """a reference file read and written again keeps its zones, sources and
-    backflow values; a zone with rigidity activated is named unsupported"""
+    backflow values, zone rigidity included"""
     _, _, prm, _ = settings.read_settings(GOLDEN)
     path = tmp_path / "z.settings.json"
     settings.write_settings(str(path), 5, (2000, 1000), prm)
@@ -93,7 +93,8 @@ def test_zones_and_sources_round_trip(tmp_path):
     assert list(got.externalEnergyBackflowFactor) == pytest.approx(list(prm.externalEnergyBackflowFactor), rel=1e-7)
     prm.zones[1].rigidityActivated, prm.zones[1].rigidity = 1, 0.5
     settings.write_settings(str(path), 5, (2000, 1000), prm)
-    assert settings.read_settings(str(path))[3] == ["zones[1].rigidity"]
+    _, _, got, unsupported = settings.read_settings(str(path))
+    assert unsupported == [] and got.zones[1].rigidityActivated == 1 and got.zones[1].rigidity == 0.5
 
 
 def test_written_layout_is_the_reference_layout(tmp_path):
