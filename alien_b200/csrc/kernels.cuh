@@ -1216,7 +1216,7 @@ __device__ __forceinline__ float2 verletIncrement(const DevState& s, long long g
 // cells: checkForces + applyForces (CellProcessor.cuh:367-406), bond forces
 // #1 at the overlap-corrected positions.  particles: movement
 // (RadiationProcessor::movement, RadiationProcessor.cuh:61-70).
-__global__ void __launch_bounds__(kBlock, 6) kApplyBond1(DevState s)
+__global__ void __launch_bounds__(kBlock, 5) kApplyBond1(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         // own fields before the world lookup and the first store (every
@@ -1322,7 +1322,7 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletPos(DevState s)
 // cells: checkConnections (CellProcessor.cuh:493-523) at the new positions,
 // bond forces #2.  particles: merges into particles that do not merge
 // themselves (RadiationProcessor.cuh:82-96 under the fixed rule).
-__global__ void __launch_bounds__(kBlock, 6) kBond2(DevState s)
+__global__ void __launch_bounds__(kBlock, 5) kBond2(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         // own fields before the world lookup (every launched cell slot lies
@@ -1495,7 +1495,7 @@ __global__ void __launch_bounds__(kBlock, 8) kVerletVel(DevState s)
 // absorbed energy, inner friction (every third step: one Jacobi sweep with
 // one pair average per bond, CellProcessor.cuh:678-705), friction and decay.
 // particles: splitting (RadiationProcessor::splitting, :172-204).
-__global__ void __launch_bounds__(kBlock, 6) kTransition(DevState s)
+__global__ void __launch_bounds__(kBlock, 5) kTransition(DevState s)
 {
     if (blockIdx.x < s.numCellBlocks) {
         // the cell's own fields are loaded before the world lookup and the
