@@ -79,8 +79,82 @@ inline AlienPhysicsParams toB200(SimulationParameters const& p)
         a.cellMinEnergy[c] = p.baseValues.cellMinEnergy[c];
         a.cellDeathProbability[c] = p.baseValues.cellDeathProbability[c];
     }
-    a.numZones = p.numZones;                        // must be 0
-    a.numRadiationSources = p.numRadiationSources;  // must be 0
+    a.radiationDisableSources = p.baseValues.radiationDisableSources;
+    a.externalEnergy = p.externalEnergy;
+    a.externalEnergyBackflowLimit = p.externalEnergyBackflowLimit;
+    for (int c = 0; c < MAX_COLORS; ++c) a.externalEnergyBackflowFactor[c] = p.externalEnergyBackflowFactor[c];
+    // zones (SimulationParametersZone.h): position, velocity, shape, flow
+    // field and the physics-stage values with their activation flags
+    a.numZones = p.numZones;
+    for (int i = 0; i < p.numZones && i < ALIEN_B200_MAX_ZONES; ++i) {
+        SimulationParametersZone const& r = p.zone[i];
+        AlienZone& z = a.zones[i];
+        z.posX = r.posX;
+        z.posY = r.posY;
+        z.velX = r.velX;
+        z.velY = r.velY;
+        z.fadeoutRadius = r.fadeoutRadius;
+        z.shapeType = r.shapeType;
+        if (r.shapeType == SpotShapeType_Circular) {
+            z.coreRadius = r.shapeData.circularSpot.coreRadius;
+        } else {
+            z.width = r.shapeData.rectangularSpot.width;
+            z.height = r.shapeData.rectangularSpot.height;
+        }
+        z.flowType = r.flowType;
+        if (r.flowType == FlowType_Radial) {
+            z.flowOrientation = r.flowData.radialFlow.orientation;
+            z.flowStrength = r.flowData.radialFlow.strength;
+            z.flowDriftAngle = r.flowData.radialFlow.driftAngle;
+        } else if (r.flowType == FlowType_Central) {
+            z.flowStrength = r.flowData.centralFlow.strength;
+        } else if (r.flowType == FlowType_Linear) {
+            z.flowAngle = r.flowData.linearFlow.angle;
+            z.flowStrength = r.flowData.linearFlow.strength;
+        }
+        z.friction = r.values.friction;
+        z.rigidity = r.values.rigidity;
+        z.radiationDisableSources = r.values.radiationDisableSources;
+        z.cellFusionVelocity = r.values.cellFusionVelocity;
+        z.cellMaxBindingEnergy = r.values.cellMaxBindingEnergy;
+        for (int c = 0; c < MAX_COLORS; ++c) {
+            z.radiationAbsorption[c] = r.values.radiationAbsorption[c];
+            z.radiationCellAgeStrength[c] = r.values.radiationCellAgeStrength[c];
+            z.cellMaxForce[c] = r.values.cellMaxForce[c];
+            z.cellMinEnergy[c] = r.values.cellMinEnergy[c];
+            z.cellDeathProbability[c] = r.values.cellDeathProbability[c];
+        }
+        z.frictionActivated = r.activatedValues.friction;
+        z.rigidityActivated = r.activatedValues.rigidity;
+        z.radiationAbsorptionActivated = r.activatedValues.radiationAbsorption;
+        z.radiationCellAgeStrengthActivated = r.activatedValues.radiationCellAgeStrength;
+        z.radiationDisableSourcesActivated = r.activatedValues.radiationDisableSources;
+        z.cellMaxForceActivated = r.activatedValues.cellMaxForce;
+        z.cellMinEnergyActivated = r.activatedValues.cellMinEnergy;
+        z.cellDeathProbabilityActivated = r.activatedValues.cellDeathProbability;
+        z.cellFusionVelocityActivated = r.activatedValues.cellFusionVelocity;
+        z.cellMaxBindingEnergyActivated = r.activatedValues.cellMaxBindingEnergy;
+    }
+    // radiation sources (RadiationSource.h)
+    a.numRadiationSources = p.numRadiationSources;
+    for (int i = 0; i < p.numRadiationSources && i < ALIEN_B200_MAX_RADIATION_SOURCES; ++i) {
+        RadiationSource const& r = p.radiationSource[i];
+        AlienRadiationSource& s = a.radiationSources[i];
+        s.strength = r.strength;
+        s.posX = r.posX;
+        s.posY = r.posY;
+        s.velX = r.velX;
+        s.velY = r.velY;
+        s.useAngle = r.useAngle;
+        s.angle = r.angle;
+        s.shapeType = r.shapeType;
+        if (r.shapeType == RadiationSourceShapeType_Circular) {
+            s.radius = r.shapeData.circularRadiationSource.radius;
+        } else {
+            s.width = r.shapeData.rectangularRadiationSource.width;
+            s.height = r.shapeData.rectangularRadiationSource.height;
+        }
+    }
     a.particleTransformationAllowed = p.particleTransformationAllowed;
     a.cellAgeLimiter = p.features.cellAgeLimiter;
     a.cellColorTransitionRules = p.features.cellColorTransitionRules;
