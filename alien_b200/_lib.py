@@ -106,6 +106,18 @@ class LaunchConfig(ctypes.Structure):
     ]
 
 
+class ArenaCapacity(ctypes.Structure):
+    """AlienArenaCapacity (include/alien_b200_batch.h): what a live arena reserves"""
+    _fields_ = [
+        ("maxWorlds", ctypes.c_int32),
+        ("cellSlots", ctypes.c_uint64),
+        ("particleSlots", ctypes.c_uint64),
+        ("tiles", ctypes.c_uint64),
+        ("particleMapSlots", ctypes.c_uint64),
+        ("auxBytes", ctypes.c_uint64),
+    ]
+
+
 # every symbol declared in include/alien_b200.h and include/alien_b200_batch.h
 EXPORTED_SYMBOLS = [
     "alien_b200_version", "alien_b200_select_device", "alien_b200_time_timesteps",
@@ -125,6 +137,8 @@ EXPORTED_SYMBOLS = [
     "alien_b200_choose_region", "alien_b200_batch_set_launch_config", "alien_b200_batch_get_launch_config",
     "alien_b200_get_raw_statistics_data", "alien_b200_reset_time_interval_statistics",
     "alien_b200_batch_get_raw_statistics_data", "alien_b200_batch_reset_time_interval_statistics",
+    "alien_b200_arena_bytes", "alien_b200_arena_create", "alien_b200_world_admit", "alien_b200_world_evict",
+    "alien_b200_arena_num_resident",
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -199,6 +213,11 @@ def load() -> ctypes.CDLL:
     lib.alien_b200_batch_time_timesteps.argtypes = [vp, u64, P(ctypes.c_double)]
     lib.alien_b200_step_kernel_name.argtypes = [i32]
     lib.alien_b200_step_kernel_name.restype = ctypes.c_char_p
+    lib.alien_b200_arena_bytes.argtypes = [P(ArenaCapacity), P(u64)]
+    lib.alien_b200_arena_create.argtypes = [P(ArenaCapacity), P(vp)]
+    lib.alien_b200_world_admit.argtypes = [vp, P(GeneralSettings), P(PhysicsParams), vp, u64, u64, P(i32)]
+    lib.alien_b200_world_evict.argtypes = [vp, i32]
+    lib.alien_b200_arena_num_resident.argtypes = [vp]
     _lib = lib
     return lib
 

@@ -64,10 +64,16 @@ class DeviceMemory {
 public:
     ~DeviceMemory() { freeAll(); }
     void setStream(cudaStream_t stream) { stream_ = stream; }
+    // counting mode: allocations only add up their sizes (reserveBytes)
+    void setCountOnly(bool on) { countOnly_ = on; }
     template <class T>
     T* alloc(size_t n)
     {
         const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+        if (countOnly_) {
+            bytes_ += bytes;
+            return nullptr;
+        }
         void* p = nullptr;
         cudaError_t e = cudaMallocAsync(&p, bytes, stream_);
         if (e != cudaSuccess) {
@@ -90,6 +96,7 @@ private:
     cudaStream_t stream_ = nullptr;
     std::vector<void*> live_;
     size_t bytes_ = 0;
+    bool countOnly_ = false;
 };
 
 // A device buffer that keeps its allocation across arena rebuilds and only
@@ -188,14 +195,87 @@ struct HostWorld {
     // which read their weights there, else kept here on the host
     uint64_t auxSize = 0;
     std::vector<uint8_t> aux;
+    // live arenas: an unused world slot, and what the admission check found
+    bool vacant = false;
+    uint32_t neurons = 0, signals = 0;
+};
+
+// first-fit ranges of [0, capacity): the cell blocks, particle blocks, tiles,
+// particle-map slots and auxiliary bytes of a live arena
+class RangePool {
+public:
+    void init(long long capacity)
+    {
+        cap_ = capacity;
+        free_.clear();
+        if (capacity > 0) free_[0] = capacity;
+    }
+    // start of a free range of n units, or -1
+    long long alloc(long long n)
+    {
+        if (n <= 0) return 0;
+        for (auto it = free_.begin(); it != free_.end(); ++it)
+            if (it->second >= n) {
+                const long long start = it->first, len = it->second;
+                free_.erase(it);
+                if (len > n) free_[start + n] = len - n;
+                return start;
+            }
+        return -1;
+    }
+    void release(long long start, long long n)
+    {
+        if (n <= 0) return;
+        auto next = free_.lower_bound(start);
+        if (next != free_.end() && next->first == start + n) {
+            n += next->second;
+            next = free_.erase(next);
+        }
+        if (next != free_.begin()) {
+            auto prev = std::prev(next);
+            if (prev->first + prev->second == start) {
+                start = prev->first;
+                n += prev->second;
+                free_.erase(prev);
+            }
+        }
+        free_[start] = n;
+    }
+    // one past the last used unit (the launches cover [0, highWater))
+    long long highWater() const
+    {
+        if (free_.empty()) return cap_;
+        const auto last = std::prev(free_.end());
+        return last->first + last->second == cap_ ? last->first : cap_;
+    }
+    long long capacity() const { return cap_; }
+
+private:
+    long long cap_ = 0;
+    std::map<long long, long long> free_;
 };
 
 class Arena {
 public:
     explicit Arena(cudaStream_t stream) : stream_(stream) { mem_.setStream(stream); }
-    ~Arena() { releaseGraph(); }
+    ~Arena()
+    {
+        releaseGraph();
+        if (checkStream_) cudaStreamDestroy(checkStream_);
+    }
 
     void build(const std::vector<WorldSetup>& setups);
+    // live arenas (alien_b200_arena_create): memory for a stated capacity is
+    // reserved once; worlds are admitted into free ranges and evicted while
+    // the other worlds keep their state, all in stream order behind the
+    // steps already enqueued
+    void reserve(const AlienArenaCapacity& capacity);
+    int admit(const WorldSetup& ws, uint64_t steps, int slot = -1);
+    void evict(int w);
+    bool live() const { return live_; }
+    bool resident(int w) const { return w >= 0 && w < numWorlds() && !worlds_[w].vacant && (!live_ || w != vacant_); }
+    int residentWorlds() const;
+    static uint64_t reserveBytes(const AlienArenaCapacity& capacity);
     void enqueueStep();
     void enqueueSteps(uint64_t n);
     // n graph steps bracketed by CUDA events on the arena's stream
@@ -282,6 +362,27 @@ private:
     {
         launchSmem(kPairsRegion<Motion>, s_.numRegions, kRegionThreads, regionDynSmem<Motion>(), s_);
     }
+    void allocCellAndParticleArrays(size_t C, size_t P, long long tiles, long long pmapSlots, int cellBlocks, int partBlocks,
+                                    bool clusters);
+    // live arenas
+    bool live_ = false;
+    AlienArenaCapacity capacity_{};
+    RangePool cellPool_, partPool_, tilePool_, pmapPool_, auxPool_;  // cells and particles in blocks of kBlock
+    int regionCap_ = 0;
+    int vacant_ = -1;  // the world slot of every unused block (never active)
+    cudaStream_t checkStream_ = nullptr;
+    bool layoutDirty_ = false;  // admissions or evictions since the last layout update
+    void updateLiveLayout();
+    void refreshLayout()
+    {
+        if (layoutDirty_) {
+            layoutDirty_ = false;
+            updateLiveLayout();
+        }
+    }
+    // a resident world re-admitted (same slot) from its current state: more
+    // particle room or a new interaction radius
+    void relocate(int w, uint64_t extraParticles, const AlienPhysicsParams* newParams);
     void releaseGraph()
     {
         if (graphExec_) cudaGraphExecDestroy(graphExec_);
@@ -317,6 +418,7 @@ private:
         return p.numZones > 0 || p.numRadiationSources > 0 || p.externalEnergyControl;
     }
     bool tuned_ = false;              // the autotuner ran on this layout
+    bool motionTuned_[2] = {false, false};  // the autotuner chose the motion type's region shape
     float tunedMs_[2][kNumRegionChoices] = {};
     void binCurrentState();
     bool signalsLive_ = false;  // some cell has a function or a nonzero signal channel
@@ -348,6 +450,92 @@ static void validateCells(const std::vector<WorldSetup>& setups)
                 throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT,
                             "neuron data of cell id " + std::to_string(c.id) + " lies outside the auxiliary data");
         }
+}
+
+// the per-cell, per-particle, per-tile and per-block arrays of the arena
+// (the cluster arrays of rigidity only when asked for)
+void Arena::allocCellAndParticleArrays(size_t C, size_t P, long long tiles, long long pmapSlots, int cellBlocks, int partBlocks,
+                                       bool clusters)
+{
+    DevState& s = s_;
+    s.id = mem_.alloc<unsigned long long>(C);
+    s.posA = mem_.alloc<float2>(C);
+    s.push = mem_.alloc<float2>(C);
+    s.dpos = mem_.alloc<float2>(C);
+    s.velA = mem_.alloc<float2>(C);
+    s.velB = mem_.alloc<float2>(C);
+    s.energy = mem_.alloc<float>(C);
+    s.stiffness = mem_.alloc<float>(C);
+    s.density = mem_.alloc<float>(C);
+    s.densNew = mem_.alloc<float>(C);
+    s.color = mem_.alloc<uint8_t>(C);
+    s.maxConn = mem_.alloc<uint8_t>(C);
+    s.numConn = mem_.alloc<uint8_t>(C);
+    s.barrier = mem_.alloc<uint8_t>(C);
+    s.alive = mem_.alloc<uint8_t>(C);
+    s.triMask = mem_.alloc<uint8_t>(C);
+    s.livingState = mem_.alloc<uint8_t>(C);
+    s.nextState = mem_.alloc<uint8_t>(C);
+    s.flags = mem_.alloc<uint32_t>(C);
+    s.age = mem_.alloc<uint32_t>(C);
+    s.activationTime = mem_.alloc<uint32_t>(C);
+    s.creatureId = mem_.alloc<uint32_t>(C);
+    s.coldIdx = mem_.alloc<uint32_t>(C);
+    s.bond = mem_.alloc<int>(C * kMaxBonds);
+    s.bondDist = mem_.alloc<float>(C * kMaxBonds);
+    s.bondAngle = mem_.alloc<float>(C * kMaxBonds);
+    s.force = mem_.alloc<float2>(C);
+    s.force1 = mem_.alloc<float2>(C);
+    s.angleAcc = mem_.alloc<long long>(C * 4);
+    s.energyAcc = mem_.alloc<long long>(C);
+    s.best = mem_.alloc<int>(C);
+    s.newPartner = mem_.alloc<int>(C);
+    if (clusters) {
+        s.clusterLab[0] = mem_.alloc<int>(C);
+        s.clusterLab[1] = mem_.alloc<int>(C);
+        s.clusterCount = mem_.alloc<uint32_t>(C);
+        s.clusterAcc = mem_.alloc<long long>(C * kAccFields);
+        s.clusterChanged = mem_.alloc<uint32_t>(kClusterRounds);
+    }
+    s.addNum = mem_.alloc<uint8_t>(C);
+    s.addBond = mem_.alloc<int>(C * kMaxBonds);
+    s.addDist = mem_.alloc<float>(C * kMaxBonds);
+    s.addAngle = mem_.alloc<float>(C * kMaxBonds);
+    s.radPos = mem_.alloc<float2>(C);
+    s.radVel = mem_.alloc<float2>(C);
+    s.radEnergy = mem_.alloc<float>(C);
+    s.tileOf = mem_.alloc<uint32_t>(C);
+    s.slotOf = mem_.alloc<uint32_t>(C);
+    s.tileOff = mem_.alloc<uint32_t>(C);
+    s.sorted = mem_.alloc<uint32_t>(C);
+    s.stagedPV = mem_.alloc<float4>(C);
+    s.stagedMeta = mem_.alloc<int4>(C);
+    s.tileCount = mem_.alloc<uint32_t>(static_cast<size_t>(tiles) + 1);
+    s.pairOverflowCount = s.tileCount + tiles;
+    s.pairOverflow = mem_.alloc<uint32_t>(C);
+    s.tileStart = mem_.alloc<uint32_t>(static_cast<size_t>(tiles) + 1);
+    s.scanPartials = mem_.alloc<uint32_t>(static_cast<size_t>(divUp(tiles, kScanTile)) + 2);
+
+    s.pid = mem_.alloc<unsigned long long>(P);
+    s.ppos = mem_.alloc<float2>(P);
+    s.pvel = mem_.alloc<float2>(P);
+    s.penergy = mem_.alloc<float>(P);
+    s.pcolor = mem_.alloc<uint8_t>(P);
+    s.palive = mem_.alloc<uint8_t>(P);
+    s.pselected = mem_.alloc<uint8_t>(P);
+    s.pflag = mem_.alloc<uint32_t>(P);
+    s.plast = mem_.alloc<unsigned long long>(P);
+    s.ptarget = mem_.alloc<int>(P);
+    s.pslot = mem_.alloc<int>(P);
+    s.pmerge = mem_.alloc<long long>(P * 3);
+    s.splitPos = mem_.alloc<float2>(P);
+    s.splitVel = mem_.alloc<float2>(P);
+    s.splitEnergy = mem_.alloc<float>(P);
+    s.pmap = mem_.alloc<int>(static_cast<size_t>(pmapSlots));
+    s.blockRad = mem_.alloc<uint32_t>(cellBlocks);
+    s.blockDel = mem_.alloc<uint32_t>(cellBlocks);
+    s.blockSplit = mem_.alloc<uint32_t>(partBlocks);
+
 }
 
 void Arena::build(const std::vector<WorldSetup>& setups)
@@ -442,6 +630,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     mem_.freeAll();
     worlds_.clear();
     tuned_ = false;  // a new layout is tuned again at its first step
+    motionTuned_[0] = motionTuned_[1] = false;
     std::memset(tunedMs_, 0, sizeof(tunedMs_));
     for (int m = 0; m < 2; ++m) regionChoice_[m] = regionChoiceFixed_[m] ? regionChoiceFixed_[m] - 1 : 0;
     const int n = static_cast<int>(setups.size());
@@ -549,83 +738,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     s.partBlockWorld = pbw;
     s.errorFlags = mem_.alloc<uint32_t>(1);
 
-    s.id = mem_.alloc<unsigned long long>(C);
-    s.posA = mem_.alloc<float2>(C);
-    s.push = mem_.alloc<float2>(C);
-    s.dpos = mem_.alloc<float2>(C);
-    s.velA = mem_.alloc<float2>(C);
-    s.velB = mem_.alloc<float2>(C);
-    s.energy = mem_.alloc<float>(C);
-    s.stiffness = mem_.alloc<float>(C);
-    s.density = mem_.alloc<float>(C);
-    s.densNew = mem_.alloc<float>(C);
-    s.color = mem_.alloc<uint8_t>(C);
-    s.maxConn = mem_.alloc<uint8_t>(C);
-    s.numConn = mem_.alloc<uint8_t>(C);
-    s.barrier = mem_.alloc<uint8_t>(C);
-    s.alive = mem_.alloc<uint8_t>(C);
-    s.triMask = mem_.alloc<uint8_t>(C);
-    s.livingState = mem_.alloc<uint8_t>(C);
-    s.nextState = mem_.alloc<uint8_t>(C);
-    s.flags = mem_.alloc<uint32_t>(C);
-    s.age = mem_.alloc<uint32_t>(C);
-    s.activationTime = mem_.alloc<uint32_t>(C);
-    s.creatureId = mem_.alloc<uint32_t>(C);
-    s.coldIdx = mem_.alloc<uint32_t>(C);
-    s.bond = mem_.alloc<int>(C * kMaxBonds);
-    s.bondDist = mem_.alloc<float>(C * kMaxBonds);
-    s.bondAngle = mem_.alloc<float>(C * kMaxBonds);
-    s.force = mem_.alloc<float2>(C);
-    s.force1 = mem_.alloc<float2>(C);
-    s.angleAcc = mem_.alloc<long long>(C * 4);
-    s.energyAcc = mem_.alloc<long long>(C);
-    s.best = mem_.alloc<int>(C);
-    s.newPartner = mem_.alloc<int>(C);
-    if (hasRigidity_) {
-        s.clusterLab[0] = mem_.alloc<int>(C);
-        s.clusterLab[1] = mem_.alloc<int>(C);
-        s.clusterCount = mem_.alloc<uint32_t>(C);
-        s.clusterAcc = mem_.alloc<long long>(C * kAccFields);
-        s.clusterChanged = mem_.alloc<uint32_t>(kClusterRounds);
-    }
-    s.addNum = mem_.alloc<uint8_t>(C);
-    s.addBond = mem_.alloc<int>(C * kMaxBonds);
-    s.addDist = mem_.alloc<float>(C * kMaxBonds);
-    s.addAngle = mem_.alloc<float>(C * kMaxBonds);
-    s.radPos = mem_.alloc<float2>(C);
-    s.radVel = mem_.alloc<float2>(C);
-    s.radEnergy = mem_.alloc<float>(C);
-    s.tileOf = mem_.alloc<uint32_t>(C);
-    s.slotOf = mem_.alloc<uint32_t>(C);
-    s.tileOff = mem_.alloc<uint32_t>(C);
-    s.sorted = mem_.alloc<uint32_t>(C);
-    s.stagedPV = mem_.alloc<float4>(C);
-    s.stagedMeta = mem_.alloc<int4>(C);
-    s.tileCount = mem_.alloc<uint32_t>(static_cast<size_t>(tiles) + 1);
-    s.pairOverflowCount = s.tileCount + tiles;
-    s.pairOverflow = mem_.alloc<uint32_t>(C);
-    s.tileStart = mem_.alloc<uint32_t>(static_cast<size_t>(tiles) + 1);
-    s.scanPartials = mem_.alloc<uint32_t>(static_cast<size_t>(divUp(tiles, kScanTile)) + 2);
-
-    s.pid = mem_.alloc<unsigned long long>(P);
-    s.ppos = mem_.alloc<float2>(P);
-    s.pvel = mem_.alloc<float2>(P);
-    s.penergy = mem_.alloc<float>(P);
-    s.pcolor = mem_.alloc<uint8_t>(P);
-    s.palive = mem_.alloc<uint8_t>(P);
-    s.pselected = mem_.alloc<uint8_t>(P);
-    s.pflag = mem_.alloc<uint32_t>(P);
-    s.plast = mem_.alloc<unsigned long long>(P);
-    s.ptarget = mem_.alloc<int>(P);
-    s.pslot = mem_.alloc<int>(P);
-    s.pmerge = mem_.alloc<long long>(P * 3);
-    s.splitPos = mem_.alloc<float2>(P);
-    s.splitVel = mem_.alloc<float2>(P);
-    s.splitEnergy = mem_.alloc<float>(P);
-    s.pmap = mem_.alloc<int>(static_cast<size_t>(pmapSlots));
-    s.blockRad = mem_.alloc<uint32_t>(cellBlocks);
-    s.blockDel = mem_.alloc<uint32_t>(cellBlocks);
-    s.blockSplit = mem_.alloc<uint32_t>(partBlocks);
+    allocCellAndParticleArrays(C, P, tiles, pmapSlots, cellBlocks, partBlocks, hasRigidity_);
 
     stats_ = mem_.alloc<StatsAcc>(n);
     timeline_ = mem_.alloc<TimelineAcc>(1);
@@ -719,6 +832,430 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     sync();
 }
 
+// ------------------------------------------------------- live arenas -----
+namespace {
+constexpr int kMaxLiveWorlds = 65534;  // world indices travel in 16 bits of the staged records
+}
+
+static void validateCapacity(const AlienArenaCapacity& c)
+{
+    if (c.maxWorlds < 1 || c.maxWorlds > kMaxLiveWorlds)
+        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "maxWorlds must lie in [1, 65534]");
+    if (c.cellSlots == 0 || c.particleSlots == 0 || c.tiles == 0 || c.particleMapSlots == 0)
+        throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "capacities must be positive");
+    if (c.cellSlots >= (1ull << 31) || c.particleSlots >= (1ull << 31) || c.tiles >= (1ull << 32) - 2 ||
+        c.particleMapSlots >= (1ull << 40))
+        throw Error(ALIEN_B200_ERR_CAPACITY, "arena capacity exceeds 2^31 slots");
+}
+
+int Arena::residentWorlds() const
+{
+    int n = 0;
+    for (int w = 0; w < numWorlds(); ++w) n += resident(w) ? 1 : 0;
+    return n;
+}
+
+uint64_t Arena::reserveBytes(const AlienArenaCapacity& c)
+{
+    validateCapacity(c);
+    Arena probe(nullptr);
+    probe.mem_.setCountOnly(true);
+    const int n = c.maxWorlds + 1;
+    const long long cellBlocks = divUp(static_cast<long long>(c.cellSlots), kBlock);
+    const long long partBlocks = divUp(static_cast<long long>(c.particleSlots), kBlock);
+    const size_t C = static_cast<size_t>(cellBlocks) * kBlock, P = static_cast<size_t>(partBlocks) * kBlock;
+    const int regionCap = static_cast<int>(std::min<long long>(static_cast<long long>(c.tiles) / 16 + 4ll * n + 16, 1ll << 30));
+    probe.mem_.alloc<WorldInfo>(n);
+    probe.mem_.alloc<WorldCounters>(n);
+    probe.mem_.alloc<AlienPhysicsParams>(n);
+    probe.mem_.alloc<int>(regionCap);
+    probe.mem_.alloc<int>(cellBlocks);
+    probe.mem_.alloc<int>(partBlocks);
+    probe.mem_.alloc<uint32_t>(1);
+    probe.allocCellAndParticleArrays(C, P, static_cast<long long>(c.tiles), static_cast<long long>(c.particleMapSlots),
+                                     static_cast<int>(cellBlocks), static_cast<int>(partBlocks), true);
+    probe.mem_.alloc<StatsAcc>(n);
+    probe.mem_.alloc<TimelineAcc>(1);
+    probe.mem_.alloc<unsigned long long>(static_cast<size_t>(n) * ALIEN_B200_MAX_COLORS);
+    probe.mem_.alloc<AlienCellTO>(C);
+    probe.mem_.alloc<uchar4>(C);
+    probe.mem_.alloc<uint8_t>(std::max<uint64_t>(c.auxBytes, 1));
+    probe.mem_.alloc<int>(C);
+    probe.mem_.alloc<int>(P);
+    probe.mem_.alloc<uint32_t>(static_cast<size_t>(std::max(cellBlocks, partBlocks)) + 2);
+    return probe.mem_.bytes();
+}
+
+void Arena::reserve(const AlienArenaCapacity& c)
+{
+    validateCapacity(c);
+    releaseGraph();
+    AB_CK(cudaStreamSynchronize(stream_));
+    mem_.freeAll();
+    worlds_.clear();
+    live_ = true;
+    capacity_ = c;
+    tuned_ = false;
+    motionTuned_[0] = motionTuned_[1] = false;
+    std::memset(tunedMs_, 0, sizeof(tunedMs_));
+    for (int m = 0; m < 2; ++m) regionChoice_[m] = regionChoiceFixed_[m] ? regionChoiceFixed_[m] - 1 : 0;
+    if (!checkStream_) AB_CK(cudaStreamCreateWithFlags(&checkStream_, cudaStreamNonBlocking));
+
+    const int n = c.maxWorlds + 1;
+    vacant_ = c.maxWorlds;
+    const long long cellBlocks = divUp(static_cast<long long>(c.cellSlots), kBlock);
+    const long long partBlocks = divUp(static_cast<long long>(c.particleSlots), kBlock);
+    const size_t C = static_cast<size_t>(cellBlocks) * kBlock, P = static_cast<size_t>(partBlocks) * kBlock;
+    const long long tiles = static_cast<long long>(c.tiles), pmapSlots = static_cast<long long>(c.particleMapSlots);
+    regionCap_ = static_cast<int>(std::min<long long>(tiles / 16 + 4ll * n + 16, 1ll << 30));
+
+    DevState& s = s_;
+    s = DevState{};
+    s.numWorlds = n;
+    s.worlds = mem_.alloc<WorldInfo>(n);
+    s.counters = mem_.alloc<WorldCounters>(n);
+    s.params = mem_.alloc<AlienPhysicsParams>(n);
+    s.regionWorld = mem_.alloc<int>(regionCap_);
+    s.cellBlockWorld = mem_.alloc<int>(cellBlocks);
+    s.partBlockWorld = mem_.alloc<int>(partBlocks);
+    s.errorFlags = mem_.alloc<uint32_t>(1);
+    allocCellAndParticleArrays(C, P, tiles, pmapSlots, static_cast<int>(cellBlocks), static_cast<int>(partBlocks), true);
+    stats_ = mem_.alloc<StatsAcc>(n);
+    timeline_ = mem_.alloc<TimelineAcc>(1);
+    s.neuronActivity = mem_.alloc<unsigned long long>(static_cast<size_t>(n) * ALIEN_B200_MAX_COLORS);
+    cold_ = mem_.alloc<AlienCellTO>(C);  // a world's transfer objects at its cell slots
+    s.cold = cold_;
+    s.fnInfo = mem_.alloc<uchar4>(C);
+    s.aux = mem_.alloc<uint8_t>(std::max<uint64_t>(c.auxBytes, 1));
+    rankCells_ = mem_.alloc<int>(C);
+    rankParts_ = mem_.alloc<int>(P);
+    blockCount_ = mem_.alloc<uint32_t>(static_cast<size_t>(std::max(cellBlocks, partBlocks)) + 2);
+
+    // every slot vacant: world tables zero (inactive, no cells), default
+    // parameters, every block and region on the vacant slot
+    worlds_.assign(n, HostWorld{});
+    std::vector<AlienPhysicsParams> params(n);
+    for (int w = 0; w < n; ++w) {
+        worlds_[w].vacant = true;
+        std::memset(&worlds_[w].info, 0, sizeof(WorldInfo));
+        alien_b200_default_parameters(&params[w]);
+        worlds_[w].params = params[w];
+        worlds_[w].info.paramIndex = w;
+    }
+    std::vector<WorldInfo> infos(n);
+    for (int w = 0; w < n; ++w) infos[w] = worlds_[w].info;
+    AB_CK(cudaMemcpyAsync(const_cast<WorldInfo*>(s.worlds), infos.data(), sizeof(WorldInfo) * n, cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemcpyAsync(s.params, params.data(), sizeof(AlienPhysicsParams) * n, cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemsetAsync(s.counters, 0, sizeof(WorldCounters) * n, stream_));
+    const std::vector<int> vacantCells(cellBlocks, vacant_), vacantParts(partBlocks, vacant_), vacantRegions(regionCap_, vacant_);
+    AB_CK(cudaMemcpyAsync(const_cast<int*>(s.cellBlockWorld), vacantCells.data(), sizeof(int) * cellBlocks, cudaMemcpyHostToDevice,
+                          stream_));
+    AB_CK(cudaMemcpyAsync(const_cast<int*>(s.partBlockWorld), vacantParts.data(), sizeof(int) * partBlocks, cudaMemcpyHostToDevice,
+                          stream_));
+    AB_CK(cudaMemcpyAsync(const_cast<int*>(s.regionWorld), vacantRegions.data(), sizeof(int) * regionCap_, cudaMemcpyHostToDevice,
+                          stream_));
+    AB_CK(cudaMemsetAsync(s.errorFlags, 0, sizeof(uint32_t), stream_));
+    AB_CK(cudaMemsetAsync(s.alive, 0, C, stream_));
+    AB_CK(cudaMemsetAsync(s.palive, 0, P, stream_));
+    AB_CK(cudaMemsetAsync(s.pflag, 0, P * sizeof(uint32_t), stream_));
+    AB_CK(cudaMemsetAsync(s.pmap, 0xff, static_cast<size_t>(pmapSlots) * sizeof(int), stream_));
+    AB_CK(cudaMemsetAsync(s.flags, 0, C * sizeof(uint32_t), stream_));
+    AB_CK(cudaMemsetAsync(s.angleAcc, 0, C * 4 * sizeof(long long), stream_));
+    AB_CK(cudaMemsetAsync(s.dpos, 0, C * sizeof(float2), stream_));
+    AB_CK(cudaMemsetAsync(s.neuronActivity, 0, sizeof(unsigned long long) * n * ALIEN_B200_MAX_COLORS, stream_));
+    AB_CK(cudaMemsetAsync(s.energyAcc, 0, C * sizeof(long long), stream_));
+    AB_CK(cudaMemsetAsync(s.newPartner, 0xff, C * sizeof(int), stream_));
+    AB_CK(cudaMemsetAsync(s.best, 0xff, C * sizeof(int), stream_));
+    cellPool_.init(cellBlocks);
+    partPool_.init(partBlocks);
+    tilePool_.init(tiles);
+    pmapPool_.init(pmapSlots);
+    auxPool_.init(static_cast<long long>(c.auxBytes));
+    maxWorldCells_ = maxWorldParts_ = 0;
+    updateLiveLayout();
+    sync();
+}
+
+// launch extents (the used prefix of each range), region tables of the
+// resident worlds and the step's optional phases, after an admission or an
+// eviction; the next step captures a new graph
+void Arena::updateLiveLayout()
+{
+    DevState& s = s_;
+    s.numCellBlocks = static_cast<int>(cellPool_.highWater());
+    s.numPartBlocks = static_cast<int>(partPool_.highWater());
+    s.numTiles = tilePool_.highWater();
+    s.pairOverflowCount = s.tileCount + s.numTiles;  // cleared with the used tile counts every step
+    s.cellSlots = static_cast<long long>(s.numCellBlocks) * kBlock;
+    s.partSlots = static_cast<long long>(s.numPartBlocks) * kBlock;
+    int device = 0, sms = 0;
+    AB_CK(cudaGetDevice(&device));
+    AB_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    partGrid_ = std::max(1, std::min(s.numPartBlocks, 16 * std::max(sms, 1)));
+    statsGrid_ = 4 * std::max(sms, 1);
+    overflowGrid_ = std::max(1, std::min(s.numCellBlocks, 2 * std::max(sms, 1)));
+    hasFluid_ = hasCollision_ = hasWorldParams_ = hasRigidity_ = hasNeurons_ = signalsLive_ = false;
+    for (const HostWorld& hw : worlds_) {
+        if (hw.vacant) continue;
+        hasWorldParams_ |= needsWorldParams(hw.params);
+        hasRigidity_ |= rigidityEnabled(hw.params);
+        hasNeurons_ |= hw.neurons > 0;
+        signalsLive_ |= hw.neurons > 0 || hw.signals > 0;
+        if (hw.info.motionType == ALIEN_B200_MOTION_FLUID)
+            hasFluid_ = true;
+        else
+            hasCollision_ = true;
+        maxWorldCells_ = std::max(maxWorldCells_, hw.info.cellCap);
+        maxWorldParts_ = std::max(maxWorldParts_, hw.info.partCap);
+    }
+    // a motion type the autotuner has not seen yet is tuned at the next step
+    if ((hasFluid_ && !motionTuned_[ALIEN_B200_MOTION_FLUID]) || (hasCollision_ && !motionTuned_[ALIEN_B200_MOTION_COLLISION]))
+        tuned_ = false;
+    applyRegionShapes();
+}
+
+int Arena::admit(const WorldSetup& ws, uint64_t steps, int slot)
+{
+    if (!live_) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "not a live arena");
+    if (ws.W <= 0 || ws.H <= 0) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "world size must be positive");
+    validateParams(ws.params, ws.W, ws.H);
+    if (ws.numCells > (1ull << 30) || ws.numParticles > (1ull << 30))
+        throw Error(ALIEN_B200_ERR_CAPACITY, "more than 2^30 objects in one world");
+
+    // the world's extents, as build() lays out a world
+    HostWorld hw;
+    hw.params = ws.params;
+    WorldInfo& wi = hw.info;
+    std::memset(&wi, 0, sizeof(wi));
+    wi.W = ws.W;
+    wi.H = ws.H;
+    wi.radiusInt = scanRadius(ws.params);
+    wi.T = wi.radiusInt;
+    wi.nTX = divUp(ws.W, wi.T);
+    wi.nTY = divUp(ws.H, wi.T);
+    wi.motionType = ws.params.motionType;
+    const long long nc = static_cast<long long>(ws.numCells), np = static_cast<long long>(ws.numParticles);
+    wi.cellCap = roundUp(std::max<long long>(nc, 1), kBlock);
+    wi.partCap = roundUp(np + nc + std::max<long long>(4096, (np + nc) / 2) + static_cast<long long>(ws.extraParticles), kBlock);
+    wi.numCellBlocks = static_cast<int>(wi.cellCap / kBlock);
+    wi.numPartBlocks = static_cast<int>(wi.partCap / kBlock);
+    const long long tiles = static_cast<long long>(wi.nTX) * wi.nTY, pmapSlots = static_cast<long long>(ws.W) * ws.H;
+    int regionsAfter = maxRegions(wi);
+    for (const HostWorld& x : worlds_)
+        if (!x.vacant) regionsAfter += maxRegions(x.info);
+
+    // a free world slot and free ranges, or nothing changes
+    int w = slot;
+    if (w < 0) {
+        for (int i = 0; i < vacant_; ++i)
+            if (worlds_[i].vacant) {
+                w = i;
+                break;
+            }
+    }
+    if (w < 0 || w >= vacant_ || !worlds_[w].vacant) throw Error(ALIEN_B200_ERR_CAPACITY, "no free world slot in the arena");
+    if (regionsAfter > regionCap_) throw Error(ALIEN_B200_ERR_CAPACITY, "the arena's region table is full");
+    const long long cb = cellPool_.alloc(wi.numCellBlocks);
+    const long long pb = cb < 0 ? -1 : partPool_.alloc(wi.numPartBlocks);
+    const long long tb = pb < 0 ? -1 : tilePool_.alloc(tiles);
+    const long long mb = tb < 0 ? -1 : pmapPool_.alloc(pmapSlots);
+    const long long ab = mb < 0 ? -1 : auxPool_.alloc(static_cast<long long>(ws.numAux));
+    auto releaseRanges = [&] {
+        if (cb >= 0) cellPool_.release(cb, wi.numCellBlocks);
+        if (pb >= 0) partPool_.release(pb, wi.numPartBlocks);
+        if (tb >= 0) tilePool_.release(tb, tiles);
+        if (mb >= 0) pmapPool_.release(mb, pmapSlots);
+        if (ab >= 0) auxPool_.release(ab, static_cast<long long>(ws.numAux));
+    };
+    if (ab < 0) {
+        releaseRanges();
+        throw Error(ALIEN_B200_ERR_CAPACITY, cb < 0   ? "no free cell range in the arena"
+                                             : pb < 0 ? "no free particle range in the arena"
+                                             : tb < 0 ? "no free tile range in the arena"
+                                             : mb < 0 ? "no free particle-map range in the arena"
+                                                      : "no free auxiliary-data range in the arena");
+    }
+
+    // the transfer objects, staged and checked on the check stream while
+    // the enqueued steps run
+    AlienCellTO* dCells = nullptr;
+    AlienParticleTO* dParts = nullptr;
+    IngestCheck* dCheck = nullptr;
+    IngestCheck check{};
+    try {
+        AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&dCells), sizeof(AlienCellTO) * std::max<long long>(nc, 1), checkStream_));
+        AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&dParts), sizeof(AlienParticleTO) * std::max<long long>(np, 1), checkStream_));
+        AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&dCheck), sizeof(IngestCheck), checkStream_));
+        AB_CK(cudaMemsetAsync(dCheck, 0, sizeof(IngestCheck), checkStream_));
+        if (nc) {
+            AB_CK(cudaMemcpyAsync(dCells, ws.cells, sizeof(AlienCellTO) * nc, cudaMemcpyHostToDevice, checkStream_));
+            kCheckCells<<<divUp(nc, kBlock), kBlock, 0, checkStream_>>>(dCells, nc, static_cast<unsigned long long>(ws.numAux), dCheck);
+            AB_CK(cudaGetLastError());
+        }
+        if (np) AB_CK(cudaMemcpyAsync(dParts, ws.particles, sizeof(AlienParticleTO) * np, cudaMemcpyHostToDevice, checkStream_));
+        AB_CK(cudaMemcpyAsync(&check, dCheck, sizeof(IngestCheck), cudaMemcpyDeviceToHost, checkStream_));
+        AB_CK(cudaStreamSynchronize(checkStream_));
+        if (check.badBondCount || check.badBondIndex || check.otherFunction || check.neuronOutOfAux) {
+            validateCells({ws});  // the host scan names the first offending cell
+            throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid cell transfer objects");
+        }
+    } catch (...) {
+        if (dCells) cudaFreeAsync(dCells, checkStream_);
+        if (dParts) cudaFreeAsync(dParts, checkStream_);
+        if (dCheck) cudaFreeAsync(dCheck, checkStream_);
+        cudaStreamSynchronize(checkStream_);
+        releaseRanges();
+        throw;
+    }
+    AB_CK(cudaFreeAsync(dCheck, checkStream_));
+    cudaEvent_t staged;
+    AB_CK(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+    AB_CK(cudaEventRecord(staged, checkStream_));
+    AB_CK(cudaStreamWaitEvent(stream_, staged, 0));
+    cudaEventDestroy(staged);
+
+    wi.paramIndex = w;
+    wi.tileBase = tb;
+    wi.cellBase = cb * kBlock;
+    wi.firstCellBlock = static_cast<int>(cb);
+    wi.partBase = pb * kBlock;
+    wi.firstPartBlock = static_cast<int>(pb);
+    wi.pmapBase = mb;
+    wi.auxBase = ab;
+    hw.auxSize = ws.numAux;
+    hw.vacant = false;
+    hw.neurons = check.neurons;
+    hw.signals = check.nonzeroSignal;
+    worlds_[w] = hw;
+    maxWorldCells_ = std::max(maxWorldCells_, wi.cellCap);  // egress buffers
+    maxWorldParts_ = std::max(maxWorldParts_, wi.partCap);
+
+    // the world's tables and ranges, in stream order behind the enqueued steps
+    const DevState& s = s_;
+    WorldCounters wc;
+    std::memset(&wc, 0, sizeof(wc));
+    wc.timestep = ws.timestep;
+    wc.nextId = 1;
+    wc.numCells = static_cast<unsigned int>(nc);
+    wc.numParticles = static_cast<unsigned int>(np);
+    wc.stepsRemaining = steps == 0 ? ~0ull : steps;
+    wc.active = 1;
+    wc.signalsFresh = 1;
+    wc.externalEnergy = ws.params.externalEnergy;
+    wc.lastStepped = ~0ull;
+    AB_CK(cudaMemcpyAsync(s.counters + w, &wc, sizeof(wc), cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemcpyAsync(s.params + w, &hw.params, sizeof(AlienPhysicsParams), cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemcpyAsync(const_cast<WorldInfo*>(s.worlds) + w, &wi, sizeof(WorldInfo), cudaMemcpyHostToDevice, stream_));
+    const std::vector<int> cbw(wi.numCellBlocks, w), pbw(wi.numPartBlocks, w);
+    AB_CK(cudaMemcpyAsync(const_cast<int*>(s.cellBlockWorld) + cb, cbw.data(), sizeof(int) * cbw.size(), cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemcpyAsync(const_cast<int*>(s.partBlockWorld) + pb, pbw.data(), sizeof(int) * pbw.size(), cudaMemcpyHostToDevice, stream_));
+    const size_t c0 = static_cast<size_t>(wi.cellBase), cn = static_cast<size_t>(wi.cellCap);
+    const size_t p0 = static_cast<size_t>(wi.partBase), pn = static_cast<size_t>(wi.partCap);
+    AB_CK(cudaMemsetAsync(s.alive + c0, 0, cn, stream_));
+    AB_CK(cudaMemsetAsync(s.flags + c0, 0, cn * sizeof(uint32_t), stream_));
+    AB_CK(cudaMemsetAsync(s.angleAcc + 4 * c0, 0, cn * 4 * sizeof(long long), stream_));
+    AB_CK(cudaMemsetAsync(s.dpos + c0, 0, cn * sizeof(float2), stream_));
+    AB_CK(cudaMemsetAsync(s.energyAcc + c0, 0, cn * sizeof(long long), stream_));
+    AB_CK(cudaMemsetAsync(s.newPartner + c0, 0xff, cn * sizeof(int), stream_));
+    AB_CK(cudaMemsetAsync(s.best + c0, 0xff, cn * sizeof(int), stream_));
+    AB_CK(cudaMemsetAsync(s.palive + p0, 0, pn, stream_));
+    AB_CK(cudaMemsetAsync(s.pflag + p0, 0, pn * sizeof(uint32_t), stream_));
+    AB_CK(cudaMemsetAsync(s.pmap + mb, 0xff, static_cast<size_t>(pmapSlots) * sizeof(int), stream_));
+    AB_CK(cudaMemsetAsync(s.neuronActivity + static_cast<size_t>(w) * ALIEN_B200_MAX_COLORS, 0,
+                          sizeof(unsigned long long) * ALIEN_B200_MAX_COLORS, stream_));
+    if (ws.numAux) AB_CK(cudaMemcpyAsync(const_cast<uint8_t*>(s_.aux) + ab, ws.aux, ws.numAux, cudaMemcpyHostToDevice, stream_));
+    if (nc) AB_CK(cudaMemcpyAsync(cold_ + c0, dCells, sizeof(AlienCellTO) * nc, cudaMemcpyDeviceToDevice, stream_));
+    launch(kIngestCells, divUp(nc, kBlock), kBlock, s, w, static_cast<const AlienCellTO*>(dCells), nc, cold_,
+           static_cast<long long>(c0));
+    launch(kIngestParticles, divUp(np, kBlock), kBlock, s, w, static_cast<const AlienParticleTO*>(dParts), np);
+    launch(kMaxId, divUp(std::max(nc, np), kBlock), kBlock, s, w, static_cast<const AlienCellTO*>(dCells), nc,
+           static_cast<const AlienParticleTO*>(dParts), np);
+    AB_CK(cudaFreeAsync(dCells, stream_));
+    AB_CK(cudaFreeAsync(dParts, stream_));
+    // the launch extents and region tables follow at the next step, once for
+    // all admissions and evictions since the last one
+    layoutDirty_ = true;
+    if (needsWorldParams(hw.params)) launch(kWorldsBegin, divUp(numWorlds(), kBlock), kBlock, s_);
+    return w;
+}
+
+void Arena::evict(int w)
+{
+    if (!live_) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "not a live arena");
+    if (!resident(w)) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "world " + std::to_string(w) + " is not resident");
+    HostWorld& hw = worlds_[w];
+    const WorldInfo wi = hw.info;
+    const DevState& s = s_;
+    // the world stops being stepped and its blocks fall to the vacant slot
+    WorldCounters wc;
+    std::memset(&wc, 0, sizeof(wc));
+    AB_CK(cudaMemcpyAsync(s.counters + w, &wc, sizeof(wc), cudaMemcpyHostToDevice, stream_));
+    const std::vector<int> cbw(wi.numCellBlocks, vacant_), pbw(wi.numPartBlocks, vacant_);
+    AB_CK(cudaMemcpyAsync(const_cast<int*>(s.cellBlockWorld) + wi.firstCellBlock, cbw.data(), sizeof(int) * cbw.size(),
+                          cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemcpyAsync(const_cast<int*>(s.partBlockWorld) + wi.firstPartBlock, pbw.data(), sizeof(int) * pbw.size(),
+                          cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemsetAsync(s.alive + wi.cellBase, 0, static_cast<size_t>(wi.cellCap), stream_));
+    AB_CK(cudaMemsetAsync(s.palive + wi.partBase, 0, static_cast<size_t>(wi.partCap), stream_));
+    cellPool_.release(wi.firstCellBlock, wi.numCellBlocks);
+    partPool_.release(wi.firstPartBlock, wi.numPartBlocks);
+    tilePool_.release(wi.tileBase, static_cast<long long>(wi.nTX) * wi.nTY);
+    pmapPool_.release(wi.pmapBase, static_cast<long long>(wi.W) * wi.H);
+    auxPool_.release(wi.auxBase, static_cast<long long>(hw.auxSize));
+    HostWorld empty;
+    empty.vacant = true;
+    std::memset(&empty.info, 0, sizeof(WorldInfo));
+    empty.info.paramIndex = w;
+    empty.params = hw.params;
+    hw = empty;
+    AB_CK(cudaMemcpyAsync(const_cast<WorldInfo*>(s.worlds) + w, &hw.info, sizeof(WorldInfo), cudaMemcpyHostToDevice, stream_));
+    layoutDirty_ = true;
+}
+
+void Arena::relocate(int w, uint64_t extraParticles, const AlienPhysicsParams* newParams)
+{
+    syncParamsFromDevice();  // zones, sources and the pool as the steps left them
+    const std::vector<WorldCounters> c = readCounters();
+    const HostWorld old = worlds_[w];
+    uint64_t nc = 0, np = 0, na = old.auxSize;
+    countData(w, &nc, &np);
+    std::vector<AlienCellTO> cells(std::max<uint64_t>(nc, 1));
+    std::vector<AlienParticleTO> parts(std::max<uint64_t>(np, 1));
+    std::vector<uint8_t> aux(std::max<uint64_t>(na, 1));
+    AlienDataTO to{&nc, cells.data(), &np, parts.data(), &na, aux.data()};
+    getData(w, false, AlienInt2{0, 0}, AlienInt2{0, 0}, &to);
+    std::vector<unsigned long long> neurons(ALIEN_B200_MAX_COLORS);
+    AB_CK(cudaMemcpyAsync(neurons.data(), s_.neuronActivity + static_cast<size_t>(w) * ALIEN_B200_MAX_COLORS,
+                          sizeof(unsigned long long) * ALIEN_B200_MAX_COLORS, cudaMemcpyDeviceToHost, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+    WorldSetup ws;
+    ws.W = old.info.W;
+    ws.H = old.info.H;
+    ws.params = newParams ? *newParams : old.params;
+    if (newParams) ws.params.externalEnergy = old.params.externalEnergy;
+    ws.timestep = c[w].timestep;
+    ws.cells = cells.data();
+    ws.numCells = nc;
+    ws.particles = parts.data();
+    ws.numParticles = np;
+    ws.aux = aux.data();
+    ws.numAux = na;
+    ws.extraParticles = extraParticles;
+    evict(w);
+    admit(ws, 0, w);
+    // ids, budget and activity continue where they were
+    WorldCounters now;
+    AB_CK(cudaMemcpyAsync(&now, s_.counters + w, sizeof(now), cudaMemcpyDeviceToHost, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+    now.nextId = std::max(now.nextId, c[w].nextId);
+    now.stepsRemaining = c[w].stepsRemaining;
+    now.active = c[w].active;
+    AB_CK(cudaMemcpyAsync(s_.counters + w, &now, sizeof(now), cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemcpyAsync(s_.neuronActivity + static_cast<size_t>(w) * ALIEN_B200_MAX_COLORS, neurons.data(),
+                          sizeof(unsigned long long) * ALIEN_B200_MAX_COLORS, cudaMemcpyHostToDevice, stream_));
+    sync();
+}
+
 // -------------------------------------------------------------- scan -----
 // exclusive scan of in[0, n) into out[0, n], out[n] = total; in and out are
 // device allocations (16-byte aligned, as kScanDown's vector accesses need)
@@ -774,6 +1311,8 @@ void Arena::enqueueStep()
 void Arena::enqueueSteps(uint64_t n)
 {
     if (n == 0) return;
+    refreshLayout();
+    if (live_ && residentWorlds() == 0) return;
     if (!tuned_) autotune();
     if (!graphExec_) {
         cudaGraph_t graph;
@@ -799,6 +1338,7 @@ void Arena::enqueueSteps(uint64_t n)
 
 std::vector<double> Arena::timedSteps(uint64_t n)
 {
+    refreshLayout();
     if (!tuned_) autotune();
     std::vector<double> sums;
     std::vector<cudaEvent_t> events;
@@ -881,6 +1421,7 @@ void Arena::ensureParticleCapacity()
     std::vector<WorldCounters> c = readCounters();
     std::vector<int> grow;
     for (int w = 0; w < numWorlds(); ++w) {
+        if (!resident(w)) continue;
         const long long cap = worlds_[w].info.partCap;
         if (c[w].numParticles * 2ll <= cap) continue;
         compactParticles(w);
@@ -889,6 +1430,11 @@ void Arena::ensureParticleCapacity()
         if (static_cast<long long>(live) * 2 > cap) grow.push_back(w);
     }
     if (grow.empty()) return;
+    if (live_) {
+        // a live arena moves only the worlds that need room
+        for (int w : grow) relocate(w, 2 * static_cast<uint64_t>(worlds_[w].info.partCap), nullptr);
+        return;
+    }
     // resize (the counterpart of _SimulationCudaFacade::resizeArrays,
     // SimulationCudaFacade.cu:619-655): export, rebuild larger, re-import
     std::vector<std::vector<AlienCellTO>> cells(numWorlds());
@@ -982,6 +1528,10 @@ void Arena::setParams(int w, const AlienPhysicsParams& p)
     // exist only in arenas built with rigidity
     const bool relayout = scanRadius(p) != hw.info.radiusInt || p.motionType != hw.info.motionType ||
                           (rigidityEnabled(p) && !s_.clusterAcc);
+    if (relayout && live_) {
+        relocate(w, 0, &p);
+        return;
+    }
     if (relayout) {
         // rebuild the arena
         std::vector<std::vector<AlienCellTO>> cells(numWorlds());
@@ -1164,6 +1714,7 @@ void Arena::compactParticles(int w)
 // map); everything written here is rebuilt by the next step
 void Arena::binCurrentState()
 {
+    refreshLayout();
     const DevState& s = s_;
     AB_CK(cudaMemsetAsync(s.tileCount, 0, sizeof(uint32_t) * (static_cast<size_t>(s.numTiles) + 1), stream_));
     launch(kBinMap, s.numCellBlocks, kBlock, s);
@@ -1222,19 +1773,26 @@ void Arena::applyRegionShapes()
     std::vector<int> rgw;
     for (size_t w = 0; w < worlds_.size(); ++w) {
         WorldInfo& wi = worlds_[w].info;
-        assignRegions(wi, regionShape(wi.motionType));
+        if (worlds_[w].vacant) {
+            wi.nRX = wi.nRY = 0;  // an unused slot of a live arena has no regions
+        } else {
+            assignRegions(wi, regionShape(wi.motionType));
+        }
         wi.regionBase = static_cast<int>(rgw.size());
         rgw.insert(rgw.end(), static_cast<size_t>(wi.nRX) * wi.nRY, static_cast<int>(w));
         infos[w] = wi;
     }
     s_.numRegions = static_cast<int>(rgw.size());
+    // copies from pageable host memory are staged before the calls return,
+    // so the temporaries may go without waiting for the stream (a live
+    // arena keeps its enqueued steps running through an admission)
     if (!infos.empty())
         AB_CK(cudaMemcpyAsync(const_cast<WorldInfo*>(s_.worlds), infos.data(), sizeof(WorldInfo) * infos.size(),
                               cudaMemcpyHostToDevice, stream_));
     if (!rgw.empty())
         AB_CK(cudaMemcpyAsync(const_cast<int*>(s_.regionWorld), rgw.data(), sizeof(int) * rgw.size(), cudaMemcpyHostToDevice,
                               stream_));
-    AB_CK(cudaStreamSynchronize(stream_));  // the host tables are temporaries
+    if (!live_) AB_CK(cudaStreamSynchronize(stream_));
     releaseGraph();
 }
 
@@ -1283,8 +1841,9 @@ AlienLaunchConfig Arena::launchConfig() const
 void Arena::autotune()
 {
     tuned_ = true;
-    const bool need[2] = {hasFluid_ && !regionChoiceFixed_[ALIEN_B200_MOTION_FLUID],
-                          hasCollision_ && !regionChoiceFixed_[ALIEN_B200_MOTION_COLLISION]};
+    const bool need[2] = {hasFluid_ && !regionChoiceFixed_[ALIEN_B200_MOTION_FLUID] && !motionTuned_[ALIEN_B200_MOTION_FLUID],
+                          hasCollision_ && !regionChoiceFixed_[ALIEN_B200_MOTION_COLLISION] &&
+                              !motionTuned_[ALIEN_B200_MOTION_COLLISION]};
     if (!need[0] && !need[1]) return;
     std::vector<WorldCounters> c = readCounters();
     long long cells = 0;
@@ -1296,6 +1855,8 @@ void Arena::autotune()
     try {
         for (int m = 0; m < 2; ++m) {
             if (!need[m]) continue;
+            motionTuned_[m] = true;
+            for (int i = 0; i < kNumRegionChoices; ++i) tunedMs_[m][i] = 0.0f;
             for (int i = 0; i < kNumRegionChoices; ++i) {
                 regionChoice_[m] = i;
                 applyRegionShapes();
@@ -1844,7 +2405,7 @@ int alien_b200_reset_time_interval_statistics(alien_b200_simulation* sim)
 int alien_b200_batch_get_raw_statistics_data(alien_b200_batch* b, int world, AlienRawStatisticsData* statistics)
 {
     return guarded([&] {
-        if (!b || !statistics || world < 0 || world >= b->arena->numWorlds())
+        if (!b || !statistics || !b->arena->resident(world))
             throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
         *statistics = b->arena->statisticsData(world);
     });
@@ -1853,7 +2414,7 @@ int alien_b200_batch_get_raw_statistics_data(alien_b200_batch* b, int world, Ali
 int alien_b200_batch_reset_time_interval_statistics(alien_b200_batch* b, int world)
 {
     return guarded([&] {
-        if (!b || world < 0 || world >= b->arena->numWorlds()) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        if (!b || !b->arena->resident(world)) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
         b->arena->resetTimeIntervalStatistics(world);
     });
 }
@@ -1873,6 +2434,50 @@ int alien_b200_batch_get_launch_config(alien_b200_batch* b, AlienLaunchConfig* c
         *config = b->arena->launchConfig();
     });
 }
+
+int alien_b200_arena_bytes(const AlienArenaCapacity* capacity, uint64_t* bytes)
+{
+    return guarded([&] {
+        if (!capacity || !bytes) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        *bytes = Arena::reserveBytes(*capacity);
+    });
+}
+
+int alien_b200_arena_create(const AlienArenaCapacity* capacity, alien_b200_batch** out)
+{
+    return guarded([&] {
+        if (!capacity || !out) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        ensureDevice();
+        auto b = std::make_unique<alien_b200_batch>();
+        AB_CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        b->arena = std::make_unique<Arena>(b->stream);
+        b->arena->reserve(*capacity);
+        *out = b.release();
+    });
+}
+
+int alien_b200_world_admit(alien_b200_batch* b, const AlienGeneralSettings* general, const AlienPhysicsParams* params,
+                           const AlienDataTO* data, uint64_t timestep, uint64_t steps, int* world)
+{
+    return guarded([&] {
+        if (!b || !general || !params || !data || !world) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        if (!b->arena->live()) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "not a live arena (alien_b200_arena_create)");
+        checkDataTO(data);
+        *world = -1;
+        *world = b->arena->admit(setupFrom(*general, *params, timestep, data), steps);
+    });
+}
+
+int alien_b200_world_evict(alien_b200_batch* b, int world)
+{
+    return guarded([&] {
+        if (!b) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null handle");
+        b->arena->evict(world);
+    });
+}
+
+int alien_b200_arena_num_resident(alien_b200_batch* b) { return b && b->arena ? b->arena->residentWorlds() : -1; }
 
 int alien_b200_batch_create(int numWorlds, const AlienGeneralSettings* general, const AlienPhysicsParams* params,
                             const AlienDataTO* data, uint64_t timestep, alien_b200_batch** out)
@@ -1936,7 +2541,7 @@ int alien_b200_batch_synchronize(alien_b200_batch* b)
 int alien_b200_batch_get_data(alien_b200_batch* b, int world, const AlienDataTO* data)
 {
     return guarded([&] {
-        if (!b || world < 0 || world >= b->arena->numWorlds()) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        if (!b || !b->arena->resident(world)) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
         b->arena->getData(world, false, AlienInt2{0, 0}, AlienInt2{0, 0}, data);
     });
 }
@@ -1944,7 +2549,7 @@ int alien_b200_batch_get_data(alien_b200_batch* b, int world, const AlienDataTO*
 int alien_b200_batch_get_array_sizes(alien_b200_batch* b, int world, AlienArraySizes* sizes)
 {
     return guarded([&] {
-        if (!b || !sizes || world < 0 || world >= b->arena->numWorlds()) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        if (!b || !sizes || !b->arena->resident(world)) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
         const WorldInfo& wi = b->arena->world(world).info;
         sizes->cellArraySize = static_cast<uint64_t>(wi.cellCap);
         sizes->particleArraySize = static_cast<uint64_t>(wi.partCap);
@@ -1955,7 +2560,7 @@ int alien_b200_batch_get_array_sizes(alien_b200_batch* b, int world, AlienArrayS
 int alien_b200_batch_set_step_budget(alien_b200_batch* b, int world, uint64_t steps)
 {
     return guarded([&] {
-        if (!b || world < 0 || world >= b->arena->numWorlds()) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        if (!b || !b->arena->resident(world)) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
         b->arena->setStepBudget(world, steps);
     });
 }
@@ -1963,7 +2568,7 @@ int alien_b200_batch_set_step_budget(alien_b200_batch* b, int world, uint64_t st
 int alien_b200_batch_world_status(alien_b200_batch* b, int world, uint64_t* timestep, uint64_t* stepsRemaining, int* active)
 {
     return guarded([&] {
-        if (!b || world < 0 || world >= b->arena->numWorlds()) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        if (!b || !b->arena->resident(world)) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
         std::vector<WorldCounters> c = b->arena->readCounters();
         if (timestep) *timestep = c[world].timestep;
         if (stepsRemaining) *stepsRemaining = c[world].stepsRemaining == ~0ull ? 0 : c[world].stepsRemaining;
@@ -1989,7 +2594,7 @@ uint64_t alien_b200_batch_device_bytes(alien_b200_batch* b) { return b && b->are
 int alien_b200_batch_get_raw_statistics(alien_b200_batch* b, int world, AlienRawStatistics* statistics)
 {
     return guarded([&] {
-        if (!b || !statistics || world < 0 || world >= b->arena->numWorlds())
+        if (!b || !statistics || !b->arena->resident(world))
             throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
         *statistics = b->arena->statistics(world);
     });

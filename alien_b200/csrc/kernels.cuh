@@ -89,7 +89,8 @@ __device__ __forceinline__ void forParticleBlocks(const DevState& s, UsedSlots u
         const long long end = wi.partBase + static_cast<long long>(usedSlots(wc));
         if (!wc.active || static_cast<long long>(pb) * kBlock >= end) {
             // on to the first block of the next world in this block's stride
-            const int next = wi.firstPartBlock + wi.numPartBlocks;
+            // (an unused block of a live arena belongs to no range: the next one)
+            const int next = max(wi.firstPartBlock + wi.numPartBlocks, pb + 1);
             pb += ((next - pb + stride - 1) / stride - 1) * stride;
             continue;
         }

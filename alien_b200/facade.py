@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import ArraySizes, GeneralSettings, Int2, LaunchConfig, RawStatistics, RawStatisticsData, check
+from ._lib import ArenaCapacity, ArraySizes, GeneralSettings, Int2, LaunchConfig, RawStatistics, RawStatisticsData, check
 from .params import PhysicsParams
 from .to import CELL_TO, PARTICLE_TO, DataTO
 
@@ -240,6 +240,12 @@ class BatchSimulation:
         check(self._lib.alien_b200_batch_get_raw_statistics(self._h, int(world), ctypes.byref(r)))
         return r
 
+    def particle_slots(self, world: int) -> int:
+        """the particle slots the world holds in the arena"""
+        s = ArraySizes()
+        check(self._lib.alien_b200_batch_get_array_sizes(self._h, int(world), ctypes.byref(s)))
+        return int(s.particleArraySize)
+
     def set_step_budget(self, world: int, steps: int) -> None:
         """world steps ``steps`` more times and then stops (0 = no limit)"""
         check(self._lib.alien_b200_batch_set_step_budget(self._h, int(world), int(steps)))
@@ -281,6 +287,82 @@ class BatchSimulation:
 
     def timed_timesteps(self, timesteps: int):
         return _timed(self._lib, self._lib.alien_b200_batch_timed_timesteps, self._h, timesteps)
+
+
+class LiveArena(BatchSimulation):
+    """A batch whose worlds are admitted and evicted while the others step
+    (alien_b200_arena_create, include/alien_b200_batch.h).  Device memory for
+    ``capacity`` is reserved once; ``admit`` places a world into free ranges
+    and returns its index, which every BatchSimulation method takes."""
+
+    def __init__(self, capacity: ArenaCapacity):
+        self._lib = _lib.load()
+        self._h = ctypes.c_void_p()
+        self.capacity = capacity
+        check(self._lib.alien_b200_arena_create(ctypes.byref(capacity), ctypes.byref(self._h)))
+        self.num_worlds = int(capacity.maxWorlds)
+
+    @staticmethod
+    def bytes_for(capacity: ArenaCapacity) -> int:
+        """device bytes an arena of this capacity reserves"""
+        b = ctypes.c_uint64()
+        check(_lib.load().alien_b200_arena_bytes(ctypes.byref(capacity), ctypes.byref(b)))
+        return int(b.value)
+
+    @staticmethod
+    def capacity_for(budget_bytes: int, max_worlds: int = 1024, area_per_cell: float = 5.0, tile_side: int = 2,
+                     particles_per_cell: float = 1.6, aux_per_cell: float = 100.0) -> ArenaCapacity:
+        """the largest capacity of this mix that fits ``budget_bytes``: cell
+        slots C, particle slots particles_per_cell * C, tiles and particle-map
+        slots for worlds of area_per_cell slots per cell (density 0.2 at 5),
+        aux_per_cell bytes of neuron data per cell"""
+        def cap(cells):
+            c = ArenaCapacity()
+            c.maxWorlds = int(max_worlds)
+            c.cellSlots = int(cells)
+            c.particleSlots = int(cells * particles_per_cell) + 4096 * max_worlds // 4
+            area = cells * area_per_cell
+            c.tiles = int(area / (tile_side * tile_side) * 1.1) + 64 * max_worlds
+            c.particleMapSlots = int(area * 1.1) + 256 * max_worlds
+            c.auxBytes = int(cells * aux_per_cell)
+            return c
+        def fits(cells):
+            try:
+                return LiveArena.bytes_for(cap(cells)) <= budget_bytes
+            except _lib.AlienError:  # beyond the arena's slot limits
+                return False
+        lo, hi = 1 << 12, 1 << 30
+        if not fits(lo):
+            raise ValueError("budget too small for a live arena")
+        while not fits(hi):  # bisect the cell slots
+            mid = (lo + hi) // 2
+            if mid == lo:
+                break
+            if fits(mid):
+                lo = mid
+            else:
+                hi = mid
+        return cap(hi if fits(hi) else lo)
+
+    def admit(self, data: DataTO, world_size, params: PhysicsParams, timestep: int = 0, steps: int = 0) -> int:
+        """places the world into free ranges, behind the steps already
+        enqueued; it steps ``steps`` times (0 = no limit).  Raises AlienError
+        with ALIEN_B200_ERR_CAPACITY when it does not fit."""
+        g = GeneralSettings(int(world_size[0]), int(world_size[1]))
+        w = ctypes.c_int()
+        check(self._lib.alien_b200_world_admit(self._h, ctypes.byref(g), ctypes.byref(params),
+                                               ctypes.cast(data.c_ptr(), ctypes.c_void_p), int(timestep), int(steps),
+                                               ctypes.byref(w)))
+        return int(w.value)
+
+    def evict(self, world: int) -> None:
+        check(self._lib.alien_b200_world_evict(self._h, int(world)))
+
+    def num_resident(self) -> int:
+        n = int(self._lib.alien_b200_arena_num_resident(self._h))
+        if n < 0:
+            raise RuntimeError(_lib.last_error())
+        return n
 
 
 def _timed(lib, fn, handle, timesteps):

@@ -465,11 +465,14 @@ def main():
                            "hbm_budget_gb": args.hbm_budget_gb, "pool_worlds": args.pool,
                            "description": "Poisson arrivals, worlds of log-uniform 5k-500k cells (half fluid, half "
                                           "10x10 lattices, a third of the lattices neuron cells), log-uniform "
-                                          "100-5000 steps, continuous batching"},
+                                          "100-5000 steps, continuous batching in one live arena"},
                 "p50_step_ms": r["p50_step_ms"], "p99_step_ms": r["p99_step_ms"],
                 "admission_wait_s": {"p50": r["p50_admission_wait_s"], "p99": r["p99_admission_wait_s"]},
                 "requests": {"submitted": r["requests_submitted"], "finished": r["requests_finished"],
-                             "waiting": r["requests_waiting"]},
+                             "waiting": r["requests_waiting"], "resident": r["requests_resident"]},
+                "admission_wave_ms_p50": r["p50_admission_wave_ms"],
+                "arena": {"bytes": r["arena_bytes"], "cell_slots": r["arena_cell_slots"],
+                          "note": "one live arena: worlds admitted into and evicted from it while the others step"},
                 "wall_s": r["wall_s"], "clocks": r["clocks"],
             }
             print(json.dumps(line))

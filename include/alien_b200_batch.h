@@ -58,6 +58,46 @@ int alien_b200_batch_timed_timesteps(alien_b200_batch* batch, uint64_t timesteps
 int alien_b200_batch_set_launch_config(alien_b200_batch* batch, const AlienLaunchConfig* config);
 int alien_b200_batch_get_launch_config(alien_b200_batch* batch, AlienLaunchConfig* config);
 
+/*
+ * Live arenas: worlds admitted and evicted while the others step.
+ *
+ * No counterpart in the reference (its EngineWorker, source/EngineImpl/
+ * EngineWorker.cpp:450-476, steps one world).  A live arena reserves device
+ * memory for a stated capacity once.  alien_b200_world_admit places a world
+ * into free ranges of it and uploads and ingests the world on the arena's
+ * stream, behind the steps already enqueued, without touching the other
+ * worlds' state; alien_b200_world_evict frees a world's ranges.  Every
+ * resident world steps in the same launches (alien_b200_batch_enqueue_timesteps
+ * / calc_timesteps), and each evolves exactly as it would alone.  A live arena
+ * is an alien_b200_batch: the world index returned by the admission is what
+ * every alien_b200_batch_* call with a `world` argument takes (get_data,
+ * statistics, step budget, status); alien_b200_batch_destroy releases it.
+ * A world evicted or never admitted is an invalid index.
+ */
+typedef struct {
+    int maxWorlds;              /* resident worlds at most (1 .. 65534) */
+    uint64_t cellSlots;         /* cell slots: a world takes its cell count rounded up to 256 */
+    uint64_t particleSlots;     /* particle slots: a world takes cells + particles + max(4096, (cells + particles) / 2),
+                                   rounded up to 256 */
+    uint64_t tiles;             /* hash tiles: a world of W x H slots takes ceil(W / r) * ceil(H / r), r = its
+                                   interaction radius in whole slots (2 for the default parameters) */
+    uint64_t particleMapSlots;  /* particle-map slots: a world takes W * H */
+    uint64_t auxBytes;          /* auxiliary data (neuron weights and biases) */
+} AlienArenaCapacity;
+
+/* device bytes a live arena of this capacity reserves */
+int alien_b200_arena_bytes(const AlienArenaCapacity* capacity, uint64_t* bytes);
+int alien_b200_arena_create(const AlienArenaCapacity* capacity, alien_b200_batch** out);
+/* Admits a world that steps `steps` times (0 = no limit) from `timestep`.
+ * Returns ALIEN_B200_ERR_CAPACITY, with the arena unchanged, when a range or
+ * a world slot is not free; the objects are validated as by set_data. */
+int alien_b200_world_admit(alien_b200_batch* arena, const AlienGeneralSettings* general, const AlienPhysicsParams* params,
+                           const AlienDataTO* data, uint64_t timestep, uint64_t steps, int* world);
+/* Frees a resident world's ranges (read its results first). */
+int alien_b200_world_evict(alien_b200_batch* arena, int world);
+/* resident worlds of a live arena (-1 on error) */
+int alien_b200_arena_num_resident(alien_b200_batch* arena);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -1,13 +1,16 @@
-"""Batched multi-world arena and serving loop: every world evolves exactly as
-it does alone (bit for bit: the step is deterministic and all sums are
-order-independent), step budgets stop worlds exactly, and the serving loop's
-results equal the results of running each request alone."""
+"""Batched multi-world arena, live arena and serving loop: every world
+evolves exactly as it does alone (bit for bit: the step is deterministic and
+all sums are order-independent), also when worlds are admitted into and
+evicted from a live arena between its steps; step budgets stop worlds
+exactly, and the serving loop's results equal the results of running each
+request alone."""
 import numpy as np
 import pytest
 
 from alien_b200 import params as P
 from alien_b200 import serving, worldgen
-from alien_b200.facade import BatchSimulation, SimulationFacade
+from alien_b200._lib import AlienError, ArenaCapacity
+from alien_b200.facade import BatchSimulation, LiveArena, SimulationFacade
 
 pytestmark = pytest.mark.gpu
 
@@ -108,3 +111,99 @@ def test_worlds_at_different_timestep_phases_equal_alone():
         assert np.array_equal(got.cells, ref.cells), w
         assert np.array_equal(got.particles, ref.particles), w
     batch.close()
+
+
+def small_capacity(worlds=8, cells=40_000):
+    c = ArenaCapacity()
+    c.maxWorlds = worlds
+    c.cellSlots = cells
+    c.particleSlots = 4 * cells + 16 * 4096
+    c.tiles = 64 * cells
+    c.particleMapSlots = 64 * cells
+    c.auxBytes = 1 << 20
+    return c
+
+
+def assert_equals_alone(arena, slot, spec, steps):
+    data, world, prm = spec
+    got = arena.get_simulation_data(slot)
+    ref = alone(data, world, prm, steps)
+    assert np.array_equal(got.cells, ref.cells), slot
+    assert np.array_equal(got.particles, ref.particles), slot
+
+
+def test_live_arena_admit_evict_equals_alone():
+    """worlds admitted between steps and into ranges an evicted world freed
+    evolve as alone, and the worlds already resident are not disturbed"""
+    a, b, c, d = mixed_worlds()
+    arena = LiveArena(small_capacity())
+    assert LiveArena.bytes_for(arena.capacity) == arena.device_bytes()
+    wa = arena.admit(*a)
+    wb = arena.admit(*b)
+    arena.calc_timesteps(7)
+    wc = arena.admit(*c)                    # a third world while two have stepped
+    arena.enqueue_timesteps(5)
+    arena.synchronize()
+    assert_equals_alone(arena, wa, a, 12)
+    arena.evict(wa)
+    assert arena.num_resident() == 2
+    wd = arena.admit(*d)                    # into the freed ranges
+    assert wd == wa
+    arena.calc_timesteps(9)
+    assert_equals_alone(arena, wb, b, 21)
+    assert_equals_alone(arena, wc, c, 14)
+    assert_equals_alone(arena, wd, d, 9)
+    with pytest.raises(AlienError):
+        arena.get_simulation_data(5)        # never admitted
+    arena.close()
+
+
+def test_live_arena_full_rejects_and_keeps_its_worlds():
+    a, b = mixed_worlds()[2], mixed_worlds()[1]
+    arena = LiveArena(small_capacity(worlds=2, cells=3600))
+    wa = arena.admit(*a)
+    with pytest.raises(AlienError) as e:
+        arena.admit(*b)                     # no free cell range: the arena is unchanged
+    assert e.value.code == 6
+    arena.calc_timesteps(6)
+    assert_equals_alone(arena, wa, a, 6)
+    arena.evict(wa)
+    wb = arena.admit(*b)
+    arena.calc_timesteps(4)
+    assert_equals_alone(arena, wb, b, 4)
+    arena.close()
+
+
+def test_live_arena_budgets_and_mixed_motion_types():
+    worlds = mixed_worlds()
+    arena = LiveArena(small_capacity())
+    slots = [arena.admit(data, world, prm, 0, steps) for (data, world, prm), steps in zip(worlds, [3, 8, 5, 11])]
+    arena.calc_timesteps(12)
+    assert arena.num_active() == 0
+    for slot, spec, steps in zip(slots, worlds, [3, 8, 5, 11]):
+        assert arena.world_status(slot)[0] == steps
+        assert_equals_alone(arena, slot, spec, steps)
+    arena.close()
+
+
+def test_live_arena_grows_a_world_that_fills_its_particles():
+    """radiation without absorption fills a world's particle range: the world
+    moves to larger ranges (same index) while the other keeps stepping"""
+    data, world = worldgen.random_test_world(36, world=(384, 384), free_cells=4000, particles=0)
+    data.cells["age"] = 1000
+    prm = P.default_parameters()
+    prm.radiationProb = 0.01  # about 48 new particles per step: the range fills between two capacity checks
+    for c in range(P.MAX_COLORS):
+        prm.radiationCellAgeStrength[c] = 0.002
+        prm.radiationAbsorption[c] = 0.0
+    other = mixed_worlds()[0]
+    arena = LiveArena(small_capacity(cells=20_000))
+    wo = arena.admit(*other)
+    wg = arena.admit(data, world, prm)
+    first = arena.particle_slots(wg)
+    for _ in range(16):
+        arena.calc_timesteps(16)
+    assert arena.particle_slots(wg) > first, "the world did not outgrow its first particle range"
+    assert_equals_alone(arena, wg, (data, world, prm), 256)
+    assert_equals_alone(arena, wo, other, 256)
+    arena.close()

@@ -1,50 +1,61 @@
-"""Admission logic of the serving loop on CPU, with cohorts that stand in for
-the device arenas (the GPU tests in test_batch_gpu.py run the real ones)."""
-import numpy as np
+"""Host logic of the serving loop on CPU, with a fake live arena that stands
+in for the device arena (test_batch_gpu.py runs the real one): admission as
+ranges free up, admission intervals, exact step counting, results read and
+worlds evicted when their steps are done."""
 import pytest
 
 from alien_b200 import serving, worldgen
 from alien_b200 import params as P
+from alien_b200._lib import AlienError
 
 
-class FakeBatch:
-    def __init__(self):
+class FakeCapacity:
+    def __init__(self, cells):
+        self.cellSlots = cells
+
+
+class FakeArena:
+    """admits while the cells fit; records the steps each world received"""
+
+    def __init__(self, cells):
+        self.capacity = FakeCapacity(cells)
+        self.free = cells
+        self.worlds = {}      # slot -> [cells, budget, steps done]
+        self.next_slot = 0
         self.enqueued = 0
+        self.evicted = []
+        self.closed = False
+
+    def admit(self, data, world, params, timestep, steps):
+        n = data.num_cells
+        if n > self.free:
+            raise AlienError(serving.ERR_CAPACITY, "no free cell range in the arena")
+        self.free -= n
+        slot = self.next_slot
+        self.next_slot += 1
+        self.worlds[slot] = [n, steps, 0]
+        return slot
 
     def enqueue_timesteps(self, k):
         self.enqueued += k
+        for w in self.worlds.values():
+            w[2] = min(w[1], w[2] + k)  # the device budget stops a world exactly
 
     def synchronize(self):
         pass
 
+    def get_simulation_data(self, slot):
+        return ("result", slot, self.worlds[slot][2])
 
-class FakeCohort:
-    def __init__(self, requests):
-        self.requests = requests
-        self.batch = FakeBatch()
-        self.bytes = sum(serving.estimate_bytes(r.data, r.world) for r in requests)
-        self.max_steps = max(r.steps for r in requests)
-        self.steps_done = 0
+    def evict(self, slot):
+        self.free += self.worlds.pop(slot)[0]
+        self.evicted.append(slot)
 
-    @property
-    def done(self):
-        return self.steps_done >= self.max_steps
-
-    def finish_done(self, now, keep_results):
-        out = []
-        for r in self.requests:
-            if r.finished is None and r.steps <= self.steps_done:
-                r.finished = now
-                out.append(r)
-        return out
+    def device_bytes(self):
+        return 0
 
     def close(self):
-        pass
-
-
-@pytest.fixture
-def fake_cohorts(monkeypatch):
-    monkeypatch.setattr(serving, "_Cohort", FakeCohort)
+        self.closed = True
 
 
 def _request(rid, steps, cells=2000, arrival=0.0):
@@ -52,59 +63,76 @@ def _request(rid, steps, cells=2000, arrival=0.0):
     return serving.Request(rid, data, world, P.benchmark_parameters(P.MOTION_FLUID), steps, arrival=arrival)
 
 
-def test_admission_waves_respect_interval(fake_cohorts):
-    loop = serving.ServingLoop(hbm_budget_bytes=1 << 40, steps_per_tick=4, admit_interval=1.0)
+def _loop(cells=1 << 40, **kw):
+    return serving.ServingLoop(0, arena=FakeArena(cells), **kw)
+
+
+def test_admission_waves_respect_interval():
+    loop = _loop(steps_per_tick=4, admit_interval=1.0)
     loop.submit(_request(0, 400))
     loop.tick(0.0)                      # nothing runs: admitted at once
-    assert len(loop.cohorts) == 1
+    assert list(loop.resident) == [0]
     t = 0.1
-    for rid in range(1, 6):             # arrivals while a cohort runs, within the interval
+    for rid in range(1, 6):             # arrivals while a world runs, within the interval
         loop.submit(_request(rid, 40, arrival=t))
         loop.tick(t)
         t += 0.2
-    assert len(loop.cohorts) == 1 and len(loop.waiting) == 5
+    assert len(loop.resident) == 1 and len(loop.waiting) == 5
     loop.tick(1.05)                     # the next wave takes all five
-    assert [len(c.requests) for c in loop.cohorts] == [1, 5] and not loop.waiting
+    assert len(loop.resident) == 6 and not loop.waiting
     loop.submit(_request(6, 40, arrival=1.2))
     loop.tick(1.2)
-    assert len(loop.cohorts) == 2 and len(loop.waiting) == 1
+    assert len(loop.resident) == 6 and len(loop.waiting) == 1
     assert loop.report(1.0)["p99_admission_wait_s"] <= 1.0 + 1e-9
 
 
-def test_admission_respects_budget_and_frees_bytes(fake_cohorts):
-    r0, r1 = _request(0, 8), _request(1, 8)
-    b = serving.estimate_bytes(r0.data, r0.world)
-    loop = serving.ServingLoop(hbm_budget_bytes=int(1.5 * b), steps_per_tick=4)
-    loop.submit(r0)
-    loop.submit(r1)
-    loop.tick(0.0)
-    assert [len(c.requests) for c in loop.cohorts] == [1] and len(loop.waiting) == 1
-    loop.tick(0.0)                      # budget full: the second request waits
-    assert len(loop.waiting) == 1
-    loop.tick(0.0)                      # first cohort done and freed after 8 steps
-    loop.tick(0.0)
-    assert len(loop.waiting) == 0 and [r.rid for r in loop.finished] == [0]
+def test_admission_waits_for_free_ranges_and_counts_steps_exactly():
+    r0, r1, r2 = _request(0, 8), _request(1, 8), _request(2, 6, cells=500)
+    arena = FakeArena(int(1.5 * r0.data.num_cells))
+    loop = serving.ServingLoop(0, arena=arena, steps_per_tick=4, keep_results=True)
+    for r in (r0, r1, r2):
+        loop.submit(r)
+    loop.tick(0.0)                      # r0 fits; r1 does not; the smaller r2 behind it does
+    assert sorted(loop.resident) == [0, 1] and [r.rid for r in loop.waiting] == [1]
+    loop.tick(0.0)                      # 4 steps each
+    loop.tick(0.0)                      # r0 done at 8 steps, r2 done at 6: both evicted
+    assert sorted(r.rid for r in loop.finished) == [0, 2] and arena.evicted == [0, 1]
+    assert r0.result == ("result", 0, 8) and r2.result == ("result", 1, 6)
     while not loop.idle():
         loop.tick(0.0)
-    assert [r.rid for r in loop.finished] == [0, 1]
-    assert loop.cell_steps == 8 * (r0.data.num_cells + r1.data.num_cells)
+    assert [r.rid for r in loop.finished][-1] == 1 and r1.result[2] == 8
+    assert loop.cell_steps == 8 * (r0.data.num_cells + r1.data.num_cells) + 6 * r2.data.num_cells
+    loop.close()
+    assert arena.closed
 
 
 def test_interval_validation():
     with pytest.raises(ValueError):
-        serving.ServingLoop(1 << 30, admit_interval=-1.0)
+        serving.ServingLoop(1 << 30, admit_interval=-1.0, arena=FakeArena(1))
     with pytest.raises(ValueError):
-        serving.ServingLoop(1 << 30, steps_per_tick=0)
+        serving.ServingLoop(1 << 30, steps_per_tick=0, arena=FakeArena(1))
 
 
-def test_requests_finish_before_their_cohort(fake_cohorts):
-    loop = serving.ServingLoop(hbm_budget_bytes=1 << 40, steps_per_tick=4)
+def test_requests_finish_at_their_own_step_count():
+    loop = _loop(steps_per_tick=4)
     short, long_ = _request(0, 4), _request(1, 40)
     loop.submit(short)
     loop.submit(long_)
-    loop.tick(0.0)                      # one cohort with both
-    loop.tick(0.0)                      # 4 steps: the short one is finished
-    assert [r.rid for r in loop.finished] == [0] and len(loop.cohorts) == 1
+    loop.tick(0.0)                      # both admitted
+    loop.tick(0.0)                      # 4 steps: the short one is finished and evicted
+    assert [r.rid for r in loop.finished] == [0] and list(loop.resident) == [1]
     while not loop.idle():
         loop.tick(0.0)
     assert [r.rid for r in loop.finished] == [0, 1]
+    assert loop.report(1.0)["requests_resident"] == 0
+
+
+def test_other_admission_errors_propagate():
+    class Broken(FakeArena):
+        def admit(self, *a):
+            raise AlienError(2, "invalid cell transfer objects")
+
+    loop = serving.ServingLoop(0, arena=Broken(1 << 30))
+    loop.submit(_request(0, 4))
+    with pytest.raises(AlienError):
+        loop.tick(0.0)
