@@ -171,6 +171,8 @@ struct DevState {
     uint32_t* tileCount;
     uint32_t* tileStart;   // numTiles + 1 entries (exclusive scan of tileCount)
     uint32_t* sorted;      // cell slots grouped by tile
+    uint8_t* slotInTile;   // per cell: its slot within its tile at binning
+    uint8_t* sortedSlot;   // beside sorted: the listed cell's slot within the tile
     uint32_t* pairOverflow;       // staged indices of cells the pair regions defer to kPairsOverflow
     uint32_t* pairOverflowCount;  // = tileCount + numTiles: cleared with the tile counts every step
     float4* stagedPV;      // (pos.x, pos.y, vel.x, vel.y) in sorted order

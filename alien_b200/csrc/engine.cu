@@ -369,6 +369,7 @@ private:
     AlienArenaCapacity capacity_{};
     RangePool cellPool_, partPool_, tilePool_, pmapPool_, auxPool_;  // cells and particles in blocks of kBlock
     int regionCap_ = 0;
+    long long regionsReserved_ = 0;  // the most regions the resident worlds can take (every candidate shape)
     int vacant_ = -1;  // the world slot of every unused block (never active)
     cudaStream_t checkStream_ = nullptr;
     bool layoutDirty_ = false;  // admissions or evictions since the last layout update
@@ -452,6 +453,16 @@ static void validateCells(const std::vector<WorldSetup>& setups)
         }
 }
 
+// the pair-phase regions stage up to RegionShape<>::Cap records in dynamic
+// shared memory (above the 48 KB default): set before any arena's first step
+static void setRegionKernelAttributes()
+{
+    AB_CK(cudaFuncSetAttribute(kPairsRegion<ALIEN_B200_MOTION_FLUID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(regionDynSmem<ALIEN_B200_MOTION_FLUID>())));
+    AB_CK(cudaFuncSetAttribute(kPairsRegion<ALIEN_B200_MOTION_COLLISION>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(regionDynSmem<ALIEN_B200_MOTION_COLLISION>())));
+}
+
 // the per-cell, per-particle, per-tile and per-block arrays of the arena
 // (the cluster arrays of rigidity only when asked for)
 void Arena::allocCellAndParticleArrays(size_t C, size_t P, long long tiles, long long pmapSlots, int cellBlocks, int partBlocks,
@@ -508,6 +519,8 @@ void Arena::allocCellAndParticleArrays(size_t C, size_t P, long long tiles, long
     s.slotOf = mem_.alloc<uint32_t>(C);
     s.tileOff = mem_.alloc<uint32_t>(C);
     s.sorted = mem_.alloc<uint32_t>(C);
+    s.slotInTile = mem_.alloc<uint8_t>(C);
+    s.sortedSlot = mem_.alloc<uint8_t>(C);
     s.stagedPV = mem_.alloc<float4>(C);
     s.stagedMeta = mem_.alloc<int4>(C);
     s.tileCount = mem_.alloc<uint32_t>(static_cast<size_t>(tiles) + 1);
@@ -698,12 +711,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     if (cellSlots >= (1ll << 31) || partSlots >= (1ll << 31) || tiles >= (1ll << 32) - 2)
         throw Error(ALIEN_B200_ERR_CAPACITY, "arena exceeds 2^31 slots");
 
-    // the pair-phase regions stage up to RegionShape<>::Cap records in dynamic
-    // shared memory (above the 48 KB default)
-    AB_CK(cudaFuncSetAttribute(kPairsRegion<ALIEN_B200_MOTION_FLUID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(regionDynSmem<ALIEN_B200_MOTION_FLUID>())));
-    AB_CK(cudaFuncSetAttribute(kPairsRegion<ALIEN_B200_MOTION_COLLISION>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(regionDynSmem<ALIEN_B200_MOTION_COLLISION>())));
+    setRegionKernelAttributes();
     DevState& s = s_;
     s = DevState{};
     s.numWorlds = n;
@@ -889,6 +897,7 @@ uint64_t Arena::reserveBytes(const AlienArenaCapacity& c)
 void Arena::reserve(const AlienArenaCapacity& c)
 {
     validateCapacity(c);
+    setRegionKernelAttributes();
     releaseGraph();
     AB_CK(cudaStreamSynchronize(stream_));
     mem_.freeAll();
@@ -899,7 +908,13 @@ void Arena::reserve(const AlienArenaCapacity& c)
     motionTuned_[0] = motionTuned_[1] = false;
     std::memset(tunedMs_, 0, sizeof(tunedMs_));
     for (int m = 0; m < 2; ++m) regionChoice_[m] = regionChoiceFixed_[m] ? regionChoiceFixed_[m] - 1 : 0;
-    if (!checkStream_) AB_CK(cudaStreamCreateWithFlags(&checkStream_, cudaStreamNonBlocking));
+    if (!checkStream_) {
+        // admissions are staged and checked at the highest stream priority,
+        // so that their small kernels get SMs between the blocks of the steps
+        int least = 0, greatest = 0;
+        AB_CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        AB_CK(cudaStreamCreateWithPriority(&checkStream_, cudaStreamNonBlocking, greatest));
+    }
 
     const int n = c.maxWorlds + 1;
     vacant_ = c.maxWorlds;
@@ -966,6 +981,7 @@ void Arena::reserve(const AlienArenaCapacity& c)
     AB_CK(cudaMemsetAsync(s.energyAcc, 0, C * sizeof(long long), stream_));
     AB_CK(cudaMemsetAsync(s.newPartner, 0xff, C * sizeof(int), stream_));
     AB_CK(cudaMemsetAsync(s.best, 0xff, C * sizeof(int), stream_));
+    regionsReserved_ = 0;
     cellPool_.init(cellBlocks);
     partPool_.init(partBlocks);
     tilePool_.init(tiles);
@@ -1040,9 +1056,8 @@ int Arena::admit(const WorldSetup& ws, uint64_t steps, int slot)
     wi.numCellBlocks = static_cast<int>(wi.cellCap / kBlock);
     wi.numPartBlocks = static_cast<int>(wi.partCap / kBlock);
     const long long tiles = static_cast<long long>(wi.nTX) * wi.nTY, pmapSlots = static_cast<long long>(ws.W) * ws.H;
-    int regionsAfter = maxRegions(wi);
-    for (const HostWorld& x : worlds_)
-        if (!x.vacant) regionsAfter += maxRegions(x.info);
+    const int worldRegions = maxRegions(wi);
+    const long long regionsAfter = regionsReserved_ + worldRegions;
 
     // a free world slot and free ranges, or nothing changes
     int w = slot;
@@ -1127,6 +1142,7 @@ int Arena::admit(const WorldSetup& ws, uint64_t steps, int slot)
     hw.neurons = check.neurons;
     hw.signals = check.nonzeroSignal;
     worlds_[w] = hw;
+    regionsReserved_ += worldRegions;
     maxWorldCells_ = std::max(maxWorldCells_, wi.cellCap);  // egress buffers
     maxWorldParts_ = std::max(maxWorldParts_, wi.partCap);
 
@@ -1197,6 +1213,7 @@ void Arena::evict(int w)
                           cudaMemcpyHostToDevice, stream_));
     AB_CK(cudaMemsetAsync(s.alive + wi.cellBase, 0, static_cast<size_t>(wi.cellCap), stream_));
     AB_CK(cudaMemsetAsync(s.palive + wi.partBase, 0, static_cast<size_t>(wi.partCap), stream_));
+    regionsReserved_ -= maxRegions(wi);
     cellPool_.release(wi.firstCellBlock, wi.numCellBlocks);
     partPool_.release(wi.firstPartBlock, wi.numPartBlocks);
     tilePool_.release(wi.tileBase, static_cast<long long>(wi.nTX) * wi.nTY);

@@ -162,14 +162,32 @@ __device__ __forceinline__ float2 foldDisplacement(const DevState& s, const Worl
     return pos;
 }
 
-// the cell's slot and tile at binning, and its arrival rank in the tile
+// the cell's slot and tile at binning, its slot within the tile (T <= 15,
+// so below 225) and its arrival rank in the tile
 __device__ __forceinline__ void binCell(const DevState& s, const WorldInfo& wi, long long g, float2 pos)
 {
     const int sx = slotX(pos.x, wi.W), sy = slotX(pos.y, wi.H);
-    const uint32_t tile = static_cast<uint32_t>(wi.tileBase + (sx / wi.T) + static_cast<long long>(sy / wi.T) * wi.nTX);
+    const int tx = sx / wi.T, ty = sy / wi.T;
+    const uint32_t tile = static_cast<uint32_t>(wi.tileBase + tx + static_cast<long long>(ty) * wi.nTX);
     s.tileOf[g] = tile;
     s.slotOf[g] = static_cast<uint32_t>(sx + sy * wi.W);
+    s.slotInTile[g] = static_cast<uint8_t>((sx - tx * wi.T) + (sy - ty * wi.T) * wi.T);
     s.tileOff[g] = atomicAdd(&s.tileCount[tile], 1u);
+}
+
+// the radiation factor (CellProcessor.cuh:730-745) is a sum of the high-
+// energy factor and the age strength, the latter blended from the base and
+// the zones that activate it with nonnegative weights: with no positive term
+// among them no cell of the world can emit, whatever its draw
+__device__ __forceinline__ bool radiationPossible(const AlienPhysicsParams& p)
+{
+    bool any = false;
+#pragma unroll
+    for (int c = 0; c < ALIEN_B200_MAX_COLORS; ++c) any |= p.highRadiationFactor[c] > 0.0f || p.radiationCellAgeStrength[c] > 0.0f;
+    for (int i = 0; i < p.numZones && !any; ++i)
+        if (p.zones[i].radiationCellAgeStrengthActivated)
+            for (int c = 0; c < ALIEN_B200_MAX_COLORS; ++c) any |= p.zones[i].radiationCellAgeStrength[c] > 0.0f;
+    return any;
 }
 
 // ---------------------------------------------------------------- kBin ----
@@ -198,6 +216,7 @@ __global__ void __launch_bounds__(kBlock, 8) kBin(DevState s)
         binCell(s, wi, g, pos);
 
         if (barrierG || !(p.radiationProb > 0.0f)) return;  // a draw in [0, 1) never falls below 0
+        if (!radiationPossible(p)) return;  // the emission factor is 0 for every cell of the world
         const uint64_t T = s.counters[c.w].timestep;
         const uint64_t id = s.id[g];
         if (!(draw(id, T, kSiteRadiation) < p.radiationProb)) return;
@@ -332,9 +351,12 @@ __global__ void __launch_bounds__(kBlock) kScatter(DevState s)
 {
     const long long g0 = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
     const uint32_t t = s.tileOf[g0], off = s.tileOff[g0];  // before the world lookup
+    const uint8_t local = s.slotInTile[g0];
     CellCtx c = cellCtx(s);
     if (!c.valid) return;
-    s.sorted[s.tileStart[t] + off] = static_cast<uint32_t>(c.g);
+    const uint32_t k = s.tileStart[t] + off;
+    s.sorted[k] = static_cast<uint32_t>(c.g);
+    s.sortedSlot[k] = local;  // beside the tile's list, for the slot ranks of kStage
 }
 
 // ------------------------------------------------------------- kStage ----
@@ -346,14 +368,16 @@ __global__ void __launch_bounds__(kBlock) kStage(DevState s)
 {
     long long k = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
     // the launch covers the cell slots, so sorted[k] is inside the array
-    // whether or not k is below the number of binned cells
+    // whether or not k is below the number of binned cells (one thread per
+    // listed cell: the record writes stay contiguous, which measured faster
+    // than one thread per cell in storage order with scattered records)
     const uint32_t total = s.tileStart[s.numTiles];
     const uint32_t g = s.sorted[k];
+    const uint8_t slot = s.sortedSlot[k];  // slot within the tile
     if (k >= total) return;
     // the cell's fields, all in flight together
     const int w = s.cellBlockWorld[g / kBlock];
     const uint32_t t = s.tileOf[g];
-    const uint32_t slot = s.slotOf[g];
     const float2 pos = s.posA[g];
     const float2 vel = s.velA[g];
     const bool barrierG = s.barrier[g];
@@ -368,7 +392,7 @@ __global__ void __launch_bounds__(kBlock) kStage(DevState s)
         uint32_t g2 = s.sorted[m];
         if (g2 >= g) continue;
         ++rankInTile;
-        rank += s.slotOf[g2] == slot;
+        rank += s.sortedSlot[m] == slot;
     }
     // records of a tile in storage order: a fixed visiting order for the
     // pair phase, whatever order the binning atomics produced

@@ -56,8 +56,9 @@ class Request:
 
 class ServingLoop:
     def __init__(self, hbm_budget_bytes: int, keep_results: bool = False, steps_per_tick: int = 4,
-                 admit_interval: float = 0.0, max_worlds: int = 1024, arena=None):
-        """``arena``: a LiveArena (default: one sized for the budget)"""
+                 admit_interval: float = 0.0, max_worlds: int = 1024, arena=None, max_misses: int = 8):
+        """``arena``: a LiveArena (default: one sized for the budget);
+        ``max_misses``: requests that did not fit after which a wave ends"""
         if not 1 <= steps_per_tick <= 64:
             raise ValueError("steps_per_tick must be in [1, 64]")
         if admit_interval < 0:
@@ -66,6 +67,7 @@ class ServingLoop:
             from .facade import LiveArena
             arena = LiveArena(LiveArena.capacity_for(int(hbm_budget_bytes), max_worlds=max_worlds))
         self.arena = arena
+        self.max_misses = int(max_misses)
         self.steps_per_tick = int(steps_per_tick)
         self.admit_interval = float(admit_interval)
         self.last_admit: float | None = None
@@ -88,13 +90,18 @@ class ServingLoop:
             return
         t0 = time.perf_counter()
         rest = []
-        for r in self.waiting:
+        misses = 0
+        for i, r in enumerate(self.waiting):
+            if misses >= self.max_misses:
+                rest.extend(self.waiting[i:])  # the arena is full: the wave ends
+                break
             try:
                 slot = self.arena.admit(r.data, r.world, r.params, 0, r.steps)
             except AlienError as e:
                 if e.code != ERR_CAPACITY:
                     raise
                 rest.append(r)  # waits for ranges to free up; smaller requests behind it may fit
+                misses += 1
                 continue
             r.slot = slot
             r.admitted = now

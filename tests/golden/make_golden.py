@@ -62,6 +62,28 @@ def one_step_params(motion, inner_friction):
     return prm
 
 
+RIGID_ONE_STEP = [
+    # name, seed, motion, timestep: calm worlds with rigidity (a step with
+    # timestep % 3 == 0 runs the cluster pass); inner friction off, since it
+    # runs in the same steps under the reference's tryLock
+    ("calm_rigid_fluid_t0", 29, P.MOTION_FLUID, 0),
+    ("calm_rigid_collision_t3", 30, P.MOTION_COLLISION, 3),
+]
+
+
+def rigid_params(motion):
+    """base rigidity 0.6, and 1.0 in a circular zone around the world's
+    centre (the rigidity blend of ClusterProcessor::applyClusterData)"""
+    prm = P.benchmark_parameters(motion)
+    prm.innerFriction = 0.0
+    prm.rigidity = 0.6
+    prm.numZones = 1
+    z = P.default_zone(prm.zones[0], prm)
+    z.posX, z.posY, z.coreRadius, z.fadeoutRadius = 32.0, 32.0, 12.0, 8.0
+    z.rigidityActivated, z.rigidity = 1, 1.0
+    return prm
+
+
 def zone_params(motion):
     """three zones over the 64x64 calm world: a clockwise radial flow with
     drift and zone friction, a rectangular central flow, a linear flow with a
@@ -121,10 +143,11 @@ def decay_input():
 
 
 def main(out_dir):
-    """ZONES_ONLY=1 writes only the zone fixtures; NEURON_ONLY=1 stops after
-    the one-step and neuron fixtures"""
+    """ZONES_ONLY=1 writes only the zone and rigidity fixtures; NEURON_ONLY=1
+    stops after the one-step and neuron fixtures"""
     os.makedirs(out_dir, exist_ok=True)
     zone_fixtures(out_dir)
+    rigid_fixtures(out_dir)
     if os.environ.get("ZONES_ONLY"):
         return
     one_step_fixtures(out_dir)
@@ -147,6 +170,28 @@ def zone_fixtures(out_dir):
     for name, seed, motion, t in ZONE_ONE_STEP:
         data, world = calm(seed)
         prm = zone_params(motion)
+        out, _, ts = refrun.run(data, world, prm, steps=1, timestep=t)
+        np.savez_compressed(os.path.join(out_dir, f"ref_{name}.npz"), in_cells=data.cells, in_particles=data.particles,
+                            out_cells=out.cells, out_particles=out.particles,
+                            params=np.frombuffer(bytes(prm), np.uint8),
+                            meta=np.array([seed, motion, t, world[0], world[1], ts], np.int64))
+        print(name, out.num_cells, out.num_particles, ts)
+
+
+def rigid_world(seed):
+    """a calm world whose bonded cells carry velocity noise of 0.02, so that
+    the rigid-body blend changes their velocities noticeably"""
+    data, world = calm(seed)
+    rng = np.random.default_rng(seed)
+    bonded = data.cells["numConnections"] > 0
+    data.cells["vel"][bonded] += rng.uniform(-0.02, 0.02, (int(bonded.sum()), 2)).astype(np.float32)
+    return data, world
+
+
+def rigid_fixtures(out_dir):
+    for name, seed, motion, t in RIGID_ONE_STEP:
+        data, world = rigid_world(seed)
+        prm = rigid_params(motion)
         out, _, ts = refrun.run(data, world, prm, steps=1, timestep=t)
         np.savez_compressed(os.path.join(out_dir, f"ref_{name}.npz"), in_cells=data.cells, in_particles=data.particles,
                             out_cells=out.cells, out_particles=out.particles,

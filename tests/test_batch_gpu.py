@@ -207,3 +207,27 @@ def test_live_arena_grows_a_world_that_fills_its_particles():
     assert_equals_alone(arena, wg, (data, world, prm), 256)
     assert_equals_alone(arena, wo, other, 256)
     arena.close()
+
+
+def test_live_arena_first_in_a_fresh_process():
+    """a live arena as the process's first handle steps (its kernels' launch
+    attributes are set by the arena itself, not by an earlier handle)"""
+    import os
+    import subprocess
+    import sys
+    code = (
+        "from alien_b200 import params as P, worldgen\n"
+        "from alien_b200._lib import ArenaCapacity\n"
+        "from alien_b200.facade import LiveArena\n"
+        "c = ArenaCapacity(); c.maxWorlds = 4; c.cellSlots = 20000; c.particleSlots = 100000\n"
+        "c.tiles = 200000; c.particleMapSlots = 400000; c.auxBytes = 1024\n"
+        "a = LiveArena(c)\n"
+        "d, w = worldgen.random_test_world(7)\n"
+        "k = a.admit(d, w, P.benchmark_parameters(P.MOTION_COLLISION))\n"
+        "a.calc_timesteps(5)\n"
+        "assert a.world_status(k)[0] == 5\n"
+        "a.close()\n"
+        "print('ok')\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0 and out.stdout.strip().endswith("ok"), out.stderr[-2000:]

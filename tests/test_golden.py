@@ -54,6 +54,14 @@ HAVE_OBSERVABLES = os.path.exists(os.path.join(GOLDEN, "ref_observables.json"))
 needs_observables = pytest.mark.skipif(not HAVE_OBSERVABLES, reason="reference observables not generated yet")
 
 
+def fixture_world(path, seed):
+    """the input of a one-step fixture, regenerated from its seed: calm
+    worlds, with velocity noise on the bonded cells for the rigidity ones"""
+    if "rigid" in os.path.basename(path):
+        return make_golden.rigid_world(seed)
+    return worldgen.calm_test_world(seed)
+
+
 def fixture_params(f, motion) -> P.PhysicsParams:
     """the fixture's parameter block; fixtures written before fields were
     appended to the struct (zones, sources, external energy) keep the
@@ -70,7 +78,7 @@ def fixture_params(f, motion) -> P.PhysicsParams:
 def test_oracle_matches_reference_one_step(path):
     f = np.load(path)
     seed, motion, t, wx, wy, ts = (int(v) for v in f["meta"])
-    data, world = worldgen.calm_test_world(seed)
+    data, world = fixture_world(path, seed)
     assert world == (wx, wy)
     assert np.array_equal(data.cells, f["in_cells"]) and np.array_equal(data.particles, f["in_particles"]), \
         "the seeded generator no longer reproduces the fixture input"
@@ -252,7 +260,7 @@ def test_engine_matches_reference_one_step(path):
 
     f = np.load(path)
     seed, motion, t, wx, wy, ts = (int(v) for v in f["meta"])
-    data, world = worldgen.calm_test_world(seed)
+    data, world = fixture_world(path, seed)
     prm = fixture_params(f, motion)
     eng = SimulationFacade()
     eng.new_simulation(t, world, prm)
