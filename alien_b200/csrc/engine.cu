@@ -300,6 +300,9 @@ public:
     void setStepBudget(int w, uint64_t steps);
     void compactParticles(int w);
     void ensureParticleCapacity();
+    // more particle room for world w (the arena rebuilt, or in a live arena
+    // the world's particles moved), with no change of state
+    void growParticles(int w, uint64_t extra);
     // the cell map of the current state, built by the step's own binning
     // kernels and read back in tile order (alien_b200_debug_cell_map)
     uint64_t cellMap(uint64_t capacity, uint64_t* ids, uint32_t* slots, uint32_t* tiles, uint8_t* flags);
@@ -381,16 +384,30 @@ private:
             updateLiveLayout();
         }
     }
-    // a resident world re-admitted (same slot) from its current state: more
-    // particle room or a new interaction radius
+    // a resident world re-admitted (same slot) from its current state, for
+    // a new interaction radius
     void relocate(int w, uint64_t extraParticles, const AlienPhysicsParams* newParams);
+    // a resident world's particles (compacted) moved to a larger free range
+    // on the device; false when no range of that size is free
+    bool moveParticles(int w, long long newCap);
     void releaseGraph()
     {
         if (graphExec_) cudaGraphExecDestroy(graphExec_);
         graphExec_ = nullptr;
     }
-    void rebuildFromHost(const std::vector<std::vector<AlienCellTO>>& cells, const std::vector<std::vector<AlienParticleTO>>& parts,
-                         const std::vector<uint64_t>& extra);
+    // a world's live objects read back for a rebuild, with the state their
+    // transfer objects do not hold (kGatherCarried) on the device
+    struct Carried {
+        std::vector<AlienCellTO> cells;
+        std::vector<AlienParticleTO> parts;
+        float* density = nullptr;
+        unsigned long long* last = nullptr;
+    };
+    void exportWorld(int w, Carried& out);
+    // the arena built again from exported worlds (extra particle room per
+    // world); fluid densities continue when keepDensity, else start at 1 as
+    // after a parameter change (prepareForSimulationParametersChanges)
+    void rebuildFromHost(std::vector<Carried>& worlds, const std::vector<uint64_t>& extra, bool keepDensity);
 
     cudaStream_t stream_;
     DeviceMemory mem_;
@@ -1229,18 +1246,60 @@ void Arena::evict(int w)
     layoutDirty_ = true;
 }
 
+bool Arena::moveParticles(int w, long long newCap)
+{
+    WorldInfo& wi = worlds_[w].info;
+    const int newBlocks = static_cast<int>(divUp(newCap, kBlock));
+    const long long pb = partPool_.alloc(newBlocks);
+    if (pb < 0) return false;
+    WorldCounters c;
+    AB_CK(cudaMemcpyAsync(&c, s_.counters + w, sizeof(c), cudaMemcpyDeviceToHost, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+    const size_t n = c.numParticles;  // used slots (all live after the compaction)
+    const size_t from = static_cast<size_t>(wi.partBase), to = static_cast<size_t>(pb) * kBlock;
+    const size_t cap = static_cast<size_t>(newBlocks) * kBlock;
+    const DevState& s = s_;
+    AB_CK(cudaMemsetAsync(s.palive + to, 0, cap, stream_));
+    AB_CK(cudaMemsetAsync(s.pflag + to, 0, cap * sizeof(uint32_t), stream_));
+    if (n) {
+        // the persistent particle state; the rest is per-step scratch
+        AB_CK(cudaMemcpyAsync(s.pid + to, s.pid + from, n * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, stream_));
+        AB_CK(cudaMemcpyAsync(s.plast + to, s.plast + from, n * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, stream_));
+        AB_CK(cudaMemcpyAsync(s.ppos + to, s.ppos + from, n * sizeof(float2), cudaMemcpyDeviceToDevice, stream_));
+        AB_CK(cudaMemcpyAsync(s.pvel + to, s.pvel + from, n * sizeof(float2), cudaMemcpyDeviceToDevice, stream_));
+        AB_CK(cudaMemcpyAsync(s.penergy + to, s.penergy + from, n * sizeof(float), cudaMemcpyDeviceToDevice, stream_));
+        AB_CK(cudaMemcpyAsync(s.pcolor + to, s.pcolor + from, n, cudaMemcpyDeviceToDevice, stream_));
+        AB_CK(cudaMemcpyAsync(s.pselected + to, s.pselected + from, n, cudaMemcpyDeviceToDevice, stream_));
+        AB_CK(cudaMemcpyAsync(s.palive + to, s.palive + from, n, cudaMemcpyDeviceToDevice, stream_));
+    }
+    const std::vector<int> mine(newBlocks, w), vacant(wi.numPartBlocks, vacant_);
+    AB_CK(cudaMemcpyAsync(const_cast<int*>(s.partBlockWorld) + pb, mine.data(), sizeof(int) * mine.size(), cudaMemcpyHostToDevice,
+                          stream_));
+    AB_CK(cudaMemcpyAsync(const_cast<int*>(s.partBlockWorld) + wi.firstPartBlock, vacant.data(), sizeof(int) * vacant.size(),
+                          cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaMemsetAsync(s.palive + from, 0, static_cast<size_t>(wi.partCap), stream_));
+    partPool_.release(wi.firstPartBlock, wi.numPartBlocks);
+    wi.partBase = static_cast<long long>(to);
+    wi.firstPartBlock = static_cast<int>(pb);
+    wi.numPartBlocks = newBlocks;
+    wi.partCap = static_cast<long long>(cap);
+    AB_CK(cudaMemcpyAsync(const_cast<WorldInfo*>(s.worlds) + w, &wi, sizeof(WorldInfo), cudaMemcpyHostToDevice, stream_));
+    maxWorldParts_ = std::max(maxWorldParts_, wi.partCap);
+    layoutDirty_ = true;
+    AB_CK(cudaStreamSynchronize(stream_));
+    return true;
+}
+
 void Arena::relocate(int w, uint64_t extraParticles, const AlienPhysicsParams* newParams)
 {
     syncParamsFromDevice();  // zones, sources and the pool as the steps left them
     const std::vector<WorldCounters> c = readCounters();
     const HostWorld old = worlds_[w];
-    uint64_t nc = 0, np = 0, na = old.auxSize;
-    countData(w, &nc, &np);
-    std::vector<AlienCellTO> cells(std::max<uint64_t>(nc, 1));
-    std::vector<AlienParticleTO> parts(std::max<uint64_t>(np, 1));
-    std::vector<uint8_t> aux(std::max<uint64_t>(na, 1));
-    AlienDataTO to{&nc, cells.data(), &np, parts.data(), &na, aux.data()};
-    getData(w, false, AlienInt2{0, 0}, AlienInt2{0, 0}, &to);
+    Carried carried;
+    exportWorld(w, carried);
+    std::vector<uint8_t> aux(std::max<uint64_t>(old.auxSize, 1));
+    if (old.auxSize)
+        AB_CK(cudaMemcpyAsync(aux.data(), s_.aux + old.info.auxBase, old.auxSize, cudaMemcpyDeviceToHost, stream_));
     std::vector<unsigned long long> neurons(ALIEN_B200_MAX_COLORS);
     AB_CK(cudaMemcpyAsync(neurons.data(), s_.neuronActivity + static_cast<size_t>(w) * ALIEN_B200_MAX_COLORS,
                           sizeof(unsigned long long) * ALIEN_B200_MAX_COLORS, cudaMemcpyDeviceToHost, stream_));
@@ -1251,15 +1310,22 @@ void Arena::relocate(int w, uint64_t extraParticles, const AlienPhysicsParams* n
     ws.params = newParams ? *newParams : old.params;
     if (newParams) ws.params.externalEnergy = old.params.externalEnergy;
     ws.timestep = c[w].timestep;
-    ws.cells = cells.data();
-    ws.numCells = nc;
-    ws.particles = parts.data();
-    ws.numParticles = np;
+    ws.cells = carried.cells.data();
+    ws.numCells = carried.cells.size();
+    ws.particles = carried.parts.data();
+    ws.numParticles = carried.parts.size();
     ws.aux = aux.data();
-    ws.numAux = na;
+    ws.numAux = old.auxSize;
     ws.extraParticles = extraParticles;
     evict(w);
     admit(ws, 0, w);
+    // the absorbers continue; densities start again after a parameter change
+    const long long nc = static_cast<long long>(ws.numCells), np = static_cast<long long>(ws.numParticles);
+    launch(kRestoreCarried, static_cast<int>(divUp(std::max<long long>(std::max(nc, np), 1), kBlock)), kBlock, s_, w,
+           newParams ? nullptr : static_cast<const float*>(carried.density), nc, static_cast<const unsigned long long*>(carried.last),
+           np);
+    AB_CK(cudaFreeAsync(carried.density, stream_));
+    AB_CK(cudaFreeAsync(carried.last, stream_));
     // ids, budget and activity continue where they were
     WorldCounters now;
     AB_CK(cudaMemcpyAsync(&now, s_.counters + w, sizeof(now), cudaMemcpyDeviceToHost, stream_));
@@ -1448,30 +1514,56 @@ void Arena::ensureParticleCapacity()
     }
     if (grow.empty()) return;
     if (live_) {
-        // a live arena moves only the worlds that need room
-        for (int w : grow) relocate(w, 2 * static_cast<uint64_t>(worlds_[w].info.partCap), nullptr);
+        // a live arena moves only the particles of the worlds that need room;
+        // without a free range of three times the size a world keeps its
+        // range (an overflow is then reported by the next synchronisation)
+        for (int w : grow) moveParticles(w, 3 * worlds_[w].info.partCap);
         return;
     }
     // resize (the counterpart of _SimulationCudaFacade::resizeArrays,
-    // SimulationCudaFacade.cu:619-655): export, rebuild larger, re-import
-    std::vector<std::vector<AlienCellTO>> cells(numWorlds());
-    std::vector<std::vector<AlienParticleTO>> parts(numWorlds());
+    // SimulationCudaFacade.cu:619-655): export, rebuild larger, re-import;
+    // the growth changes no state (densities and absorbers continue)
+    std::vector<Carried> carried(numWorlds());
     std::vector<uint64_t> extra(numWorlds(), 0);
     for (int w = 0; w < numWorlds(); ++w) {
-        uint64_t nc = 0, np = 0, na = worlds_[w].auxSize;
-        countData(w, &nc, &np);
-        cells[w].resize(nc);
-        parts[w].resize(np);
-        std::vector<uint8_t> auxTmp(std::max<uint64_t>(na, 1));
-        AlienDataTO to{&nc, cells[w].data(), &np, parts[w].data(), &na, auxTmp.data()};
-        getData(w, false, AlienInt2{0, 0}, AlienInt2{0, 0}, &to);
+        exportWorld(w, carried[w]);
         extra[w] = std::find(grow.begin(), grow.end(), w) != grow.end() ? 2 * worlds_[w].info.partCap : 0;
     }
-    rebuildFromHost(cells, parts, extra);
+    rebuildFromHost(carried, extra, true);
 }
 
-void Arena::rebuildFromHost(const std::vector<std::vector<AlienCellTO>>& cells, const std::vector<std::vector<AlienParticleTO>>& parts,
-                            const std::vector<uint64_t>& extra)
+void Arena::growParticles(int w, uint64_t extra)
+{
+    if (live_) {
+        moveParticles(w, worlds_[w].info.partCap + static_cast<long long>(extra));
+        return;
+    }
+    std::vector<Carried> carried(numWorlds());
+    std::vector<uint64_t> extras(numWorlds(), 0);
+    for (int v = 0; v < numWorlds(); ++v) exportWorld(v, carried[v]);
+    extras[w] = extra;
+    rebuildFromHost(carried, extras, true);
+}
+
+void Arena::exportWorld(int w, Carried& out)
+{
+    uint64_t nc = 0, np = 0, na = worlds_[w].auxSize;
+    countData(w, &nc, &np);
+    out.cells.resize(std::max<uint64_t>(nc, 1));
+    out.parts.resize(std::max<uint64_t>(np, 1));
+    std::vector<uint8_t> auxTmp(std::max<uint64_t>(na, 1));
+    AlienDataTO to{&nc, out.cells.data(), &np, out.parts.data(), &na, auxTmp.data()};
+    getData(w, false, AlienInt2{0, 0}, AlienInt2{0, 0}, &to);  // leaves the egress ranks of world w
+    out.cells.resize(nc);
+    out.parts.resize(np);
+    const WorldInfo& wi = worlds_[w].info;
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&out.density), sizeof(float) * std::max<uint64_t>(nc, 1), stream_));
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&out.last), sizeof(unsigned long long) * std::max<uint64_t>(np, 1), stream_));
+    launch(kGatherCarried, static_cast<int>(divUp(std::max(wi.cellCap, wi.partCap), kBlock)), kBlock, s_, w,
+           static_cast<const int*>(rankCells_), static_cast<const int*>(rankParts_), out.density, out.last);
+}
+
+void Arena::rebuildFromHost(std::vector<Carried>& worlds, const std::vector<uint64_t>& extra, bool keepDensity)
 {
     syncParamsFromDevice();  // zones, sources and the pool as the steps left them
     std::vector<WorldCounters> c = readCounters();
@@ -1492,10 +1584,10 @@ void Arena::rebuildFromHost(const std::vector<std::vector<AlienCellTO>>& cells, 
         ws.H = old[w].info.H;
         ws.params = old[w].params;
         ws.timestep = c[w].timestep;
-        ws.cells = cells[w].data();
-        ws.numCells = cells[w].size();
-        ws.particles = parts[w].data();
-        ws.numParticles = parts[w].size();
+        ws.cells = worlds[w].cells.data();
+        ws.numCells = worlds[w].cells.size();
+        ws.particles = worlds[w].parts.data();
+        ws.numParticles = worlds[w].parts.size();
         ws.aux = old[w].aux.empty() ? auxHost[w].data() : old[w].aux.data();
         ws.numAux = old[w].auxSize;
         ws.extraParticles = extra[w];
@@ -1505,6 +1597,16 @@ void Arena::rebuildFromHost(const std::vector<std::vector<AlienCellTO>>& cells, 
                           stream_));
     AB_CK(cudaStreamSynchronize(stream_));
     build(setups);
+    for (size_t w = 0; w < old.size(); ++w) {
+        const long long nc = static_cast<long long>(worlds[w].cells.size()), np = static_cast<long long>(worlds[w].parts.size());
+        launch(kRestoreCarried, static_cast<int>(divUp(std::max<long long>(std::max(nc, np), 1), kBlock)), kBlock, s_,
+               static_cast<int>(w), keepDensity ? static_cast<const float*>(worlds[w].density) : nullptr, nc,
+               static_cast<const unsigned long long*>(worlds[w].last), np);
+        AB_CK(cudaFreeAsync(worlds[w].density, stream_));
+        AB_CK(cudaFreeAsync(worlds[w].last, stream_));
+        worlds[w].density = nullptr;
+        worlds[w].last = nullptr;
+    }
     // the accumulated statistics belong to the worlds, not to the layout
     AB_CK(cudaMemcpyAsync(s_.neuronActivity, neurons.data(), sizeof(unsigned long long) * neurons.size(), cudaMemcpyHostToDevice,
                           stream_));
@@ -1550,20 +1652,12 @@ void Arena::setParams(int w, const AlienPhysicsParams& p)
         return;
     }
     if (relayout) {
-        // rebuild the arena
-        std::vector<std::vector<AlienCellTO>> cells(numWorlds());
-        std::vector<std::vector<AlienParticleTO>> parts(numWorlds());
-        for (int v = 0; v < numWorlds(); ++v) {
-            uint64_t nc = 0, np = 0, na = worlds_[v].auxSize;
-            countData(v, &nc, &np);
-            cells[v].resize(nc);
-            parts[v].resize(np);
-            std::vector<uint8_t> auxTmp(std::max<uint64_t>(na, 1));
-            AlienDataTO to{&nc, cells[v].data(), &np, parts[v].data(), &na, auxTmp.data()};
-            getData(v, false, AlienInt2{0, 0}, AlienInt2{0, 0}, &to);
-        }
+        // rebuild the arena; densities start again, as after every
+        // parameter change (kResetDensity below)
+        std::vector<Carried> carried(numWorlds());
+        for (int v = 0; v < numWorlds(); ++v) exportWorld(v, carried[v]);
         hw.params = p;
-        rebuildFromHost(cells, parts, std::vector<uint64_t>(numWorlds(), 0));
+        rebuildFromHost(carried, std::vector<uint64_t>(numWorlds(), 0), false);
         return;
     }
     hw.params = p;
@@ -2312,18 +2406,8 @@ int alien_b200_resize_arrays_if_necessary(alien_b200_simulation* sim, const Alie
         const WorldInfo& wi = sim->arena->world(0).info;
         uint64_t nc = 0, np = 0;
         sim->arena->countData(0, &nc, &np);
-        if (np + additionals->particleArraySize + 4096 > static_cast<uint64_t>(wi.partCap) / 2) {
-            std::vector<AlienCellTO> cells(nc);
-            std::vector<AlienParticleTO> parts(np);
-            uint64_t na = sim->arena->world(0).auxSize;
-            std::vector<uint8_t> aux(std::max<uint64_t>(na, 1));
-            AlienDataTO to{&nc, cells.data(), &np, parts.data(), &na, aux.data()};
-            sim->arena->getData(0, false, AlienInt2{0, 0}, AlienInt2{0, 0}, &to);
-            const uint64_t t = sim->arena->readCounters()[0].timestep;
-            WorldSetup ws = setupFrom(sim->general, sim->arena->params(0), t, &to);
-            ws.extraParticles = sim->extraParticles;
-            sim->arena->build({ws});
-        }
+        if (np + additionals->particleArraySize + 4096 > static_cast<uint64_t>(wi.partCap) / 2)
+            sim->arena->growParticles(0, sim->extraParticles);
     });
 }
 

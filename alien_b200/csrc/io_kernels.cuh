@@ -458,4 +458,32 @@ __global__ void __launch_bounds__(kBlock) kResetDensity(DevState s, int w)
     if (g < wi.cellBase + wi.cellCap) s.density[g] = 1.0f;
 }
 
+// state the transfer objects do not hold, carried through an arena rebuild
+// (more particle room, a new interaction radius): the fluid density of each
+// live cell and the last absorbing cell of each live particle, in egress
+// order (rank from kSelectCells / kSelectParticles), and back after ingest
+__global__ void __launch_bounds__(kBlock) kGatherCarried(DevState s, int w, const int* cellRank, const int* partRank,
+                                                         float* density, unsigned long long* last)
+{
+    const WorldInfo& wi = s.worlds[w];
+    const long long i = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    if (i < wi.cellCap) {
+        const int r = cellRank[wi.cellBase + i];
+        if (r >= 0) density[r] = s.density[wi.cellBase + i];
+    }
+    if (i < wi.partCap) {
+        const int r = partRank[wi.partBase + i];
+        if (r >= 0) last[r] = s.plast[wi.partBase + i];
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) kRestoreCarried(DevState s, int w, const float* density, long long nc,
+                                                          const unsigned long long* last, long long np)
+{
+    const WorldInfo& wi = s.worlds[w];
+    const long long i = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    if (density && i < nc) s.density[wi.cellBase + i] = density[i];
+    if (i < np) s.plast[wi.partBase + i] = last[i];
+}
+
 }  // namespace ab

@@ -79,6 +79,7 @@ class ServingLoop:
         self.waits: list[float] = []  # seconds from arrival to admission
         self.admit_ms: list[float] = []  # host time of each admission wave
         self.cell_steps = 0
+        self.capacity_events = 0  # synchronisations that reported dropped particles
 
     def submit(self, req: Request) -> None:
         self.waiting.append(req)
@@ -128,7 +129,14 @@ class ServingLoop:
         self._admit(now)
         if not running:
             return 0.0
-        self.arena.synchronize()
+        try:
+            self.arena.synchronize()
+        except AlienError as e:
+            if e.code != ERR_CAPACITY:
+                raise
+            # a world created more particles than its range held (and no
+            # larger range was free): the excess was dropped; the loop goes on
+            self.capacity_events += 1
         ms = (time.perf_counter() - t0) * 1000.0 / k
         self.tick_ms.append(ms)
         done_now = time.perf_counter()
@@ -162,6 +170,7 @@ class ServingLoop:
             "requests_finished": len(self.finished),
             "requests_waiting": len(self.waiting),
             "requests_resident": len(self.resident),
+            "capacity_events": self.capacity_events,
             "ticks": len(self.tick_ms),
             "p50_step_ms": float(np.percentile(t, 50)),
             "p99_step_ms": float(np.percentile(t, 99)),

@@ -189,13 +189,7 @@ def test_live_arena_budgets_and_mixed_motion_types():
 def test_live_arena_grows_a_world_that_fills_its_particles():
     """radiation without absorption fills a world's particle range: the world
     moves to larger ranges (same index) while the other keeps stepping"""
-    data, world = worldgen.random_test_world(36, world=(384, 384), free_cells=4000, particles=0)
-    data.cells["age"] = 1000
-    prm = P.default_parameters()
-    prm.radiationProb = 0.01  # about 48 new particles per step: the range fills between two capacity checks
-    for c in range(P.MAX_COLORS):
-        prm.radiationCellAgeStrength[c] = 0.002
-        prm.radiationAbsorption[c] = 0.0
+    data, world, prm = growing_world()
     other = mixed_worlds()[0]
     arena = LiveArena(small_capacity(cells=20_000))
     wo = arena.admit(*other)
@@ -231,3 +225,84 @@ def test_live_arena_first_in_a_fresh_process():
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=300)
     assert out.returncode == 0 and out.stdout.strip().endswith("ok"), out.stderr[-2000:]
+
+
+def growing_world():
+    """radiation without absorption: about 48 new particles per step fill
+    the first particle range within 200 steps"""
+    data, world = worldgen.random_test_world(36, world=(384, 384), free_cells=4000, particles=0)
+    data.cells["age"] = 1000
+    prm = P.default_parameters()
+    prm.radiationProb = 0.01
+    for c in range(P.MAX_COLORS):
+        prm.radiationCellAgeStrength[c] = 0.002
+        prm.radiationAbsorption[c] = 0.0
+    return data, world, prm
+
+
+def test_growing_particle_storage_changes_no_state():
+    """a world that outgrows its particle storage (export, larger arena,
+    re-import, fluid densities and absorbers carried) ends bit for bit where
+    the same world with room reserved from the start ends"""
+    data, world, prm = growing_world()
+    grown = alone(data, world, prm, 256)
+    s = SimulationFacade()
+    s.new_simulation(0, world, prm)
+    s.set_simulation_data(data)
+    s.resize_arrays_if_necessary(particles=200_000)
+    s.calc_timesteps(256)
+    roomy = s.get_simulation_data()
+    s.close_simulation()
+    assert roomy.num_particles > 4000
+    assert np.array_equal(grown.cells, roomy.cells)
+    assert np.array_equal(grown.particles, roomy.particles)
+
+
+def feature_worlds():
+    """worlds with zones and flows, radiation sources with the backflow, and
+    rigidity, beside a plain one"""
+    import tests.test_zones_gpu as tz
+    a = tz.zone_world(71) + (tz.zone_params(P.MOTION_FLUID),)
+    data, world = tz.zone_world(72)
+    data.cells["age"] = 1000
+    prm = P.default_parameters()
+    prm.motionType = P.MOTION_COLLISION
+    for c in range(P.MAX_COLORS):
+        prm.radiationCellAgeStrength[c] = 0.002
+        prm.externalEnergyBackflowFactor[c] = 0.3
+    prm.externalEnergyControl = 1
+    prm.externalEnergy = 20.0
+    prm.numRadiationSources = 1
+    prm.radiationSources[0].posX, prm.radiationSources[0].posY = 30.0, 40.0
+    prm.radiationSources[0].strength, prm.radiationSources[0].radius = 1.0, 4.0
+    prm.radiationSources[0].velX = 0.25
+    b = (data, world, prm)
+    rp = P.benchmark_parameters(P.MOTION_FLUID)
+    rp.rigidity = 0.5
+    c = worldgen.random_test_world(73, world=(96, 96), clusters=8) + (rp,)
+    d = mixed_worlds()[1]
+    return [a, b, c, d]
+
+
+def test_batch_with_zones_sources_and_rigidity_equals_alone():
+    """zones move, sources emit, the pool takes the backflow and clusters
+    blend per world: a batch and a live arena give every world its results
+    alone, bit for bit"""
+    worlds = feature_worlds()
+    batch = BatchSimulation(worlds)
+    batch.calc_timesteps(7)
+    arena = LiveArena(small_capacity())
+    slots = [arena.admit(*spec) for spec in worlds]
+    arena.calc_timesteps(7)
+    for w, (data, world, prm) in enumerate(worlds):
+        s = SimulationFacade()
+        s.new_simulation(0, world, prm)
+        s.set_simulation_data(data)
+        s.calc_timesteps(7)
+        ref = s.get_simulation_data()
+        s.close_simulation()
+        for got in (batch.get_simulation_data(w), arena.get_simulation_data(slots[w])):
+            assert np.array_equal(got.cells, ref.cells), w
+            assert np.array_equal(got.particles, ref.particles), w
+    batch.close()
+    arena.close()
