@@ -1112,6 +1112,7 @@ int Arena::admit(const WorldSetup& ws, uint64_t steps, int slot)
     // the enqueued steps run
     AlienCellTO* dCells = nullptr;
     AlienParticleTO* dParts = nullptr;
+    uint8_t* dAux = nullptr;
     IngestCheck* dCheck = nullptr;
     IngestCheck check{};
     try {
@@ -1125,6 +1126,12 @@ int Arena::admit(const WorldSetup& ws, uint64_t steps, int slot)
             AB_CK(cudaGetLastError());
         }
         if (np) AB_CK(cudaMemcpyAsync(dParts, ws.particles, sizeof(AlienParticleTO) * np, cudaMemcpyHostToDevice, checkStream_));
+        // the auxiliary bytes too: a large copy from pageable memory on the
+        // arena's stream would wait there behind the enqueued steps
+        if (ws.numAux) {
+            AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&dAux), ws.numAux, checkStream_));
+            AB_CK(cudaMemcpyAsync(dAux, ws.aux, ws.numAux, cudaMemcpyHostToDevice, checkStream_));
+        }
         AB_CK(cudaMemcpyAsync(&check, dCheck, sizeof(IngestCheck), cudaMemcpyDeviceToHost, checkStream_));
         AB_CK(cudaStreamSynchronize(checkStream_));
         if (check.badBondCount || check.badBondIndex || check.otherFunction || check.neuronOutOfAux) {
@@ -1134,6 +1141,7 @@ int Arena::admit(const WorldSetup& ws, uint64_t steps, int slot)
     } catch (...) {
         if (dCells) cudaFreeAsync(dCells, checkStream_);
         if (dParts) cudaFreeAsync(dParts, checkStream_);
+        if (dAux) cudaFreeAsync(dAux, checkStream_);
         if (dCheck) cudaFreeAsync(dCheck, checkStream_);
         cudaStreamSynchronize(checkStream_);
         releaseRanges();
@@ -1196,7 +1204,10 @@ int Arena::admit(const WorldSetup& ws, uint64_t steps, int slot)
     AB_CK(cudaMemsetAsync(s.pmap + mb, 0xff, static_cast<size_t>(pmapSlots) * sizeof(int), stream_));
     AB_CK(cudaMemsetAsync(s.neuronActivity + static_cast<size_t>(w) * ALIEN_B200_MAX_COLORS, 0,
                           sizeof(unsigned long long) * ALIEN_B200_MAX_COLORS, stream_));
-    if (ws.numAux) AB_CK(cudaMemcpyAsync(const_cast<uint8_t*>(s_.aux) + ab, ws.aux, ws.numAux, cudaMemcpyHostToDevice, stream_));
+    if (ws.numAux) {
+        AB_CK(cudaMemcpyAsync(const_cast<uint8_t*>(s_.aux) + ab, dAux, ws.numAux, cudaMemcpyDeviceToDevice, stream_));
+        AB_CK(cudaFreeAsync(dAux, stream_));
+    }
     if (nc) AB_CK(cudaMemcpyAsync(cold_ + c0, dCells, sizeof(AlienCellTO) * nc, cudaMemcpyDeviceToDevice, stream_));
     launch(kIngestCells, divUp(nc, kBlock), kBlock, s, w, static_cast<const AlienCellTO*>(dCells), nc, cold_,
            static_cast<long long>(c0));

@@ -56,9 +56,12 @@ class Request:
 
 class ServingLoop:
     def __init__(self, hbm_budget_bytes: int, keep_results: bool = False, steps_per_tick: int = 4,
-                 admit_interval: float = 0.0, max_worlds: int = 1024, arena=None, max_misses: int = 8):
+                 admit_interval: float = 0.0, max_worlds: int = 1024, arena=None, max_misses: int = 8,
+                 max_wave_ms: float = 25.0):
         """``arena``: a LiveArena (default: one sized for the budget);
-        ``max_misses``: requests that did not fit after which a wave ends"""
+        ``max_misses``: requests that did not fit after which a wave ends;
+        ``max_wave_ms``: host time after which a wave ends (the enqueued
+        steps keep the GPU busy meanwhile; the rest waits for the next tick)"""
         if not 1 <= steps_per_tick <= 64:
             raise ValueError("steps_per_tick must be in [1, 64]")
         if admit_interval < 0:
@@ -68,6 +71,7 @@ class ServingLoop:
             arena = LiveArena(LiveArena.capacity_for(int(hbm_budget_bytes), max_worlds=max_worlds))
         self.arena = arena
         self.max_misses = int(max_misses)
+        self.max_wave_ms = float(max_wave_ms)
         self.steps_per_tick = int(steps_per_tick)
         self.admit_interval = float(admit_interval)
         self.last_admit: float | None = None
@@ -78,6 +82,9 @@ class ServingLoop:
         self.tick_ms: list[float] = []
         self.waits: list[float] = []  # seconds from arrival to admission
         self.admit_ms: list[float] = []  # host time of each admission wave
+        self.admit_call_ms: list[float] = []  # host time of each successful admission
+        self.sync_ms: list[float] = []  # host wait for the tick's steps
+        self.evict_ms: list[float] = []
         self.cell_steps = 0
         self.capacity_events = 0  # synchronisations that reported dropped particles
 
@@ -93,11 +100,13 @@ class ServingLoop:
         rest = []
         misses = 0
         for i, r in enumerate(self.waiting):
-            if misses >= self.max_misses:
-                rest.extend(self.waiting[i:])  # the arena is full: the wave ends
+            if misses >= self.max_misses or (time.perf_counter() - t0) * 1000.0 > self.max_wave_ms:
+                rest.extend(self.waiting[i:])  # the arena is full, or the wave's time is up
                 break
+            ta = time.perf_counter()
             try:
                 slot = self.arena.admit(r.data, r.world, r.params, 0, r.steps)
+                self.admit_call_ms.append((time.perf_counter() - ta) * 1000.0)
             except AlienError as e:
                 if e.code != ERR_CAPACITY:
                     raise
@@ -129,6 +138,7 @@ class ServingLoop:
         self._admit(now)
         if not running:
             return 0.0
+        ts = time.perf_counter()
         try:
             self.arena.synchronize()
         except AlienError as e:
@@ -137,6 +147,7 @@ class ServingLoop:
             # a world created more particles than its range held (and no
             # larger range was free): the excess was dropped; the loop goes on
             self.capacity_events += 1
+        self.sync_ms.append((time.perf_counter() - ts) * 1000.0)
         ms = (time.perf_counter() - t0) * 1000.0 / k
         self.tick_ms.append(ms)
         done_now = time.perf_counter()
@@ -146,9 +157,11 @@ class ServingLoop:
             r.steps_done += n
             if r.steps_done >= r.steps:
                 r.finished = done_now
+                te = time.perf_counter()
                 if self.keep_results:
                     r.result = self.arena.get_simulation_data(slot)
                 self.arena.evict(slot)
+                self.evict_ms.append((time.perf_counter() - te) * 1000.0)
                 del self.resident[slot]
                 self.finished.append(r)
         return ms
@@ -163,10 +176,17 @@ class ServingLoop:
         t = np.array(self.tick_ms) if self.tick_ms else np.zeros(1)
         wq = np.array(self.waits) if self.waits else np.zeros(1)
         am = np.array(self.admit_ms) if self.admit_ms else np.zeros(1)
+
+        def pct(xs, q):
+            return float(np.percentile(np.array(xs), q)) if xs else 0.0
         return {
             "p50_admission_wait_s": float(np.percentile(wq, 50)),
             "p99_admission_wait_s": float(np.percentile(wq, 99)),
             "p50_admission_wave_ms": float(np.percentile(am, 50)),
+            "p99_admission_wave_ms": float(np.percentile(am, 99)),
+            "admissions": len(self.admit_call_ms),
+            "p50_admit_call_ms": pct(self.admit_call_ms, 50), "p99_admit_call_ms": pct(self.admit_call_ms, 99),
+            "p50_sync_ms": pct(self.sync_ms, 50), "p50_evict_ms": pct(self.evict_ms, 50),
             "requests_finished": len(self.finished),
             "requests_waiting": len(self.waiting),
             "requests_resident": len(self.resident),

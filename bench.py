@@ -471,6 +471,9 @@ def main():
                 "requests": {"submitted": r["requests_submitted"], "finished": r["requests_finished"],
                              "waiting": r["requests_waiting"], "resident": r["requests_resident"]},
                 "admission_wave_ms_p50": r["p50_admission_wave_ms"],
+                "host_ms": {k: r[k] for k in ("p99_admission_wave_ms", "p50_admit_call_ms", "p99_admit_call_ms",
+                                              "p50_sync_ms", "p50_evict_ms")},
+                "admissions": r["admissions"], "capacity_events": r["capacity_events"],
                 "arena": {"bytes": r["arena_bytes"], "cell_slots": r["arena_cell_slots"],
                           "note": "one live arena: worlds admitted into and evicted from it while the others step"},
                 "wall_s": r["wall_s"], "clocks": r["clocks"],
