@@ -794,7 +794,7 @@ __global__ void __launch_bounds__(kBlock) kPairsOverflow(DevState s)
 
 // ------------------------------------------------------- kPairsRegion ----
 // One CTA per region of regW x regH tiles (up to RegionShape<Motion>: 24 x 16
-// for collision worlds, 32 x 8 for fluid worlds) of one world.  It
+// for collision worlds, 64 x 8 for fluid worlds) of one world.  It
 // copies the staged records of the region and of its one-tile halo from the
 // tile-sorted arrays into shared memory, all (regW+2) x (regH+2) local tiles
 // in row-major order (each tile a contiguous run in storage order), so that
@@ -832,7 +832,7 @@ template <int Motion>
 struct RegionShape;
 template <>
 struct RegionShape<ALIEN_B200_MOTION_FLUID> {
-    static constexpr int W = 32, H = 8, Cap = 1152, HitCap = 24, MinBlocks = 3;
+    static constexpr int W = 64, H = 8, Cap = 1536, HitCap = 24, MinBlocks = 3;
 };
 template <>
 struct RegionShape<ALIEN_B200_MOTION_COLLISION> {
@@ -844,7 +844,7 @@ struct RegionShape<ALIEN_B200_MOTION_COLLISION> {
 // whatever the shape, so the choice changes no result.
 constexpr int kNumRegionChoices = ALIEN_B200_REGION_CHOICES;
 constexpr int kRegionChoices[2][kNumRegionChoices][2] = {
-    {{32, 8}, {16, 8}, {32, 4}, {24, 8}},     // fluid
+    {{64, 8}, {32, 8}, {48, 8}, {40, 8}},     // fluid
     {{24, 16}, {16, 16}, {24, 8}, {12, 16}},  // collision
 };
 template <int Motion>
