@@ -77,7 +77,9 @@ struct WorldCounters {
     unsigned int deadCells;
     unsigned int deadParticles;
     unsigned int droppedParticles;  // appends refused for lack of capacity
-    unsigned int pad;
+    // 1: no larger particle range could be had; the world's steps drop what
+    // does not fit instead of halting (until the next capacity check)
+    unsigned int dropExcess;
     // event bases of the current step (ids and slots of appended particles)
     unsigned long long radIdBase, splitIdBase, delIdBase;
     unsigned int radSlotBase, splitSlotBase, delSlotBase, numEvents;
@@ -85,7 +87,10 @@ struct WorldCounters {
     // clears active (~0 = no limit)
     unsigned long long stepsRemaining;
     unsigned int active;
-    unsigned int pad2;
+    // 1 while the world waits for particle storage: its step stopped before
+    // the new particles were written (kEventWorld), nothing of the world
+    // changes until the host has grown its range and completed the step
+    unsigned int halted;
     // events counted this step (radiation, deleted cells, particle splits):
     // the event scans run only when there are any
     unsigned int evRad, evDel, evSplit;
@@ -100,7 +105,14 @@ struct WorldCounters {
     unsigned long long activeSources;
     // the timestep a completed step left (zones and sources move once per step)
     unsigned long long lastStepped;
+    // steps the world would have taken while halted (within its budget):
+    // the host runs them after it completes the halted step
+    unsigned long long missedSteps;
 };
+
+// bits of DevState::errorFlags
+constexpr unsigned int kErrDropped = 1u;  // particles dropped for lack of storage
+constexpr unsigned int kErrHalted = 8u;   // a world halted for storage (WorldCounters::halted)
 
 struct DevState {
     int numWorlds;
@@ -115,6 +127,10 @@ struct DevState {
     const int* regionWorld;  // world of each pair-phase CTA
     int numRegions;
     unsigned int* errorFlags;
+    // 1 in the launches that complete halted steps (kEventWorld, kEventEmit,
+    // kWorldsEnd): only halted worlds take part, and what does not fit is
+    // dropped instead of halting again
+    int resume;
 
     // cells
     unsigned long long* id;

@@ -80,13 +80,25 @@ public:
             cudaGetLastError();
             throw Error(ALIEN_B200_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes failed");
         }
-        live_.push_back(p);
+        live_.emplace_back(p, bytes);
         bytes_ += bytes;
         return static_cast<T*>(p);
     }
+    // one allocation returned in stream order (a replaced array)
+    void release(const void* p)
+    {
+        for (size_t i = 0; i < live_.size(); ++i) {
+            if (live_[i].first != p) continue;
+            cudaFreeAsync(live_[i].first, stream_);
+            bytes_ -= live_[i].second;
+            live_[i] = live_.back();
+            live_.pop_back();
+            return;
+        }
+    }
     void freeAll()
     {
-        for (void* p : live_) cudaFreeAsync(p, stream_);
+        for (auto& a : live_) cudaFreeAsync(a.first, stream_);
         live_.clear();
         bytes_ = 0;
     }
@@ -94,7 +106,7 @@ public:
 
 private:
     cudaStream_t stream_ = nullptr;
-    std::vector<void*> live_;
+    std::vector<std::pair<void*, size_t>> live_;
     size_t bytes_ = 0;
     bool countOnly_ = false;
 };
@@ -284,7 +296,11 @@ public:
     // summed milliseconds per launch position of the step
     std::vector<double> timedSteps(uint64_t n);
     void calcTimesteps(uint64_t n);
+    // waits for the enqueued work and completes halted worlds; throws
+    // ALIEN_B200_ERR_CAPACITY when particles were dropped
     void sync();
+    // the same without the report (entry points that read a world's state)
+    void settle();
     void setParams(int w, const AlienPhysicsParams& p);
     // the parameters as the steps left them: zone and source positions,
     // the external energy pool
@@ -367,6 +383,18 @@ private:
     }
     void allocCellAndParticleArrays(size_t C, size_t P, long long tiles, long long pmapSlots, int cellBlocks, int partBlocks,
                                     bool clusters);
+    void allocParticleArrays(size_t P, int partBlocks);
+    void allocParticleArrays(DevState& target, size_t P, int partBlocks);
+    // halted worlds (kEventWorld): their particle ranges grown, their step
+    // completed by the resume launches, then the steps they missed run with
+    // every other world parked; returns whether particles were dropped
+    bool resumeHalted();
+    // the particle arrays of an arena laid out once (batch or single world)
+    // allocated again on the device with the ranges newCap[w] (0: as it
+    // is); the used slots move with their step's split records, nothing else
+    // of the state changes
+    void growParticleArrays(const std::vector<long long>& newCap);
+    bool droppedPending_ = false;  // a resume dropped particles: the next sync() reports it
     // live arenas
     bool live_ = false;
     AlienArenaCapacity capacity_{};
@@ -387,9 +415,10 @@ private:
     // a resident world re-admitted (same slot) from its current state, for
     // a new interaction radius
     void relocate(int w, uint64_t extraParticles, const AlienPhysicsParams* newParams);
-    // a resident world's particles (compacted) moved to a larger free range
-    // on the device; false when no range of that size is free
-    bool moveParticles(int w, long long newCap);
+    // a resident world's particles moved to a larger free range on the
+    // device, with the step's split records when stepScratch (a halted
+    // world); false when no range of that size is free
+    bool moveParticles(int w, long long newCap, bool stepScratch = false);
     void releaseGraph()
     {
         if (graphExec_) cudaGraphExecDestroy(graphExec_);
@@ -546,6 +575,19 @@ void Arena::allocCellAndParticleArrays(size_t C, size_t P, long long tiles, long
     s.tileStart = mem_.alloc<uint32_t>(static_cast<size_t>(tiles) + 1);
     s.scanPartials = mem_.alloc<uint32_t>(static_cast<size_t>(divUp(tiles, kScanTile)) + 2);
 
+    allocParticleArrays(P, partBlocks);
+    s.pmap = mem_.alloc<int>(static_cast<size_t>(pmapSlots));
+    s.blockRad = mem_.alloc<uint32_t>(cellBlocks);
+    s.blockDel = mem_.alloc<uint32_t>(cellBlocks);
+}
+
+void Arena::allocParticleArrays(size_t P, int partBlocks)
+{
+    allocParticleArrays(s_, P, partBlocks);
+}
+
+void Arena::allocParticleArrays(DevState& s, size_t P, int partBlocks)
+{
     s.pid = mem_.alloc<unsigned long long>(P);
     s.ppos = mem_.alloc<float2>(P);
     s.pvel = mem_.alloc<float2>(P);
@@ -561,11 +603,7 @@ void Arena::allocCellAndParticleArrays(size_t C, size_t P, long long tiles, long
     s.splitPos = mem_.alloc<float2>(P);
     s.splitVel = mem_.alloc<float2>(P);
     s.splitEnergy = mem_.alloc<float>(P);
-    s.pmap = mem_.alloc<int>(static_cast<size_t>(pmapSlots));
-    s.blockRad = mem_.alloc<uint32_t>(cellBlocks);
-    s.blockDel = mem_.alloc<uint32_t>(cellBlocks);
     s.blockSplit = mem_.alloc<uint32_t>(partBlocks);
-
 }
 
 void Arena::build(const std::vector<WorldSetup>& setups)
@@ -1257,7 +1295,7 @@ void Arena::evict(int w)
     layoutDirty_ = true;
 }
 
-bool Arena::moveParticles(int w, long long newCap)
+bool Arena::moveParticles(int w, long long newCap, bool stepScratch)
 {
     WorldInfo& wi = worlds_[w].info;
     const int newBlocks = static_cast<int>(divUp(newCap, kBlock));
@@ -1266,7 +1304,7 @@ bool Arena::moveParticles(int w, long long newCap)
     WorldCounters c;
     AB_CK(cudaMemcpyAsync(&c, s_.counters + w, sizeof(c), cudaMemcpyDeviceToHost, stream_));
     AB_CK(cudaStreamSynchronize(stream_));
-    const size_t n = c.numParticles;  // used slots (all live after the compaction)
+    const size_t n = c.numParticles;  // used slots
     const size_t from = static_cast<size_t>(wi.partBase), to = static_cast<size_t>(pb) * kBlock;
     const size_t cap = static_cast<size_t>(newBlocks) * kBlock;
     const DevState& s = s_;
@@ -1282,6 +1320,15 @@ bool Arena::moveParticles(int w, long long newCap)
         AB_CK(cudaMemcpyAsync(s.pcolor + to, s.pcolor + from, n, cudaMemcpyDeviceToDevice, stream_));
         AB_CK(cudaMemcpyAsync(s.pselected + to, s.pselected + from, n, cudaMemcpyDeviceToDevice, stream_));
         AB_CK(cudaMemcpyAsync(s.palive + to, s.palive + from, n, cudaMemcpyDeviceToDevice, stream_));
+        if (stepScratch) {
+            // what the halted step's split emission reads (kEventEmit)
+            AB_CK(cudaMemcpyAsync(s.pflag + to, s.pflag + from, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream_));
+            AB_CK(cudaMemcpyAsync(s.splitPos + to, s.splitPos + from, n * sizeof(float2), cudaMemcpyDeviceToDevice, stream_));
+            AB_CK(cudaMemcpyAsync(s.splitVel + to, s.splitVel + from, n * sizeof(float2), cudaMemcpyDeviceToDevice, stream_));
+            AB_CK(cudaMemcpyAsync(s.splitEnergy + to, s.splitEnergy + from, n * sizeof(float), cudaMemcpyDeviceToDevice, stream_));
+            AB_CK(cudaMemcpyAsync(s.blockSplit + pb, s.blockSplit + wi.firstPartBlock, divUp(n, kBlock) * sizeof(uint32_t),
+                                  cudaMemcpyDeviceToDevice, stream_));
+        }
     }
     const std::vector<int> mine(newBlocks, w), vacant(wi.numPartBlocks, vacant_);
     AB_CK(cudaMemcpyAsync(const_cast<int*>(s.partBlockWorld) + pb, mine.data(), sizeof(int) * mine.size(), cudaMemcpyHostToDevice,
@@ -1490,14 +1537,216 @@ double Arena::timeSteps(uint64_t n)
 
 void Arena::sync()
 {
-    // the error word is read in stream order: one wait covers the work and the read
-    uint32_t flags = 0;
-    AB_CK(cudaMemcpyAsync(&flags, s_.errorFlags, sizeof(flags), cudaMemcpyDeviceToHost, stream_));
-    AB_CK(cudaStreamSynchronize(stream_));
-    if (flags & 1u) {
-        AB_CK(cudaMemset(s_.errorFlags, 0, sizeof(uint32_t)));
+    settle();
+    if (droppedPending_) {
+        droppedPending_ = false;
         throw Error(ALIEN_B200_ERR_CAPACITY, "particle capacity exceeded: energy particles were dropped");
     }
+}
+
+void Arena::settle()
+{
+    if (!s_.errorFlags) return;  // nothing built yet
+    for (;;) {
+        // the error word is read in stream order: one wait covers the work and the read
+        uint32_t flags = 0;
+        AB_CK(cudaMemcpyAsync(&flags, s_.errorFlags, sizeof(flags), cudaMemcpyDeviceToHost, stream_));
+        AB_CK(cudaStreamSynchronize(stream_));
+        if (!flags) return;
+        AB_CK(cudaMemsetAsync(s_.errorFlags, 0, sizeof(uint32_t), stream_));
+        if (flags & kErrDropped) droppedPending_ = true;
+        if (!(flags & kErrHalted)) {
+            AB_CK(cudaStreamSynchronize(stream_));
+            return;
+        }
+        if (resumeHalted()) droppedPending_ = true;
+    }
+}
+
+bool Arena::resumeHalted()
+{
+    std::vector<WorldCounters> c = readCounters();
+    std::vector<int> halted;
+    for (int w = 0; w < numWorlds(); ++w)
+        if (resident(w) && c[w].halted) halted.push_back(w);
+    if (halted.empty()) return false;
+    // room for the step's new particles with half the range free, at least
+    // three times the old range (the growth rule of ensureParticleCapacity)
+    std::vector<long long> newCap(numWorlds(), 0);
+    std::vector<int> cannotGrow;
+    for (int w : halted) {
+        const long long need = static_cast<long long>(c[w].numParticles) + c[w].evRad + c[w].evDel + c[w].evSplit;
+        const long long want = roundUp(std::max(3 * worlds_[w].info.partCap, 2 * need), kBlock);
+        if (!live_)
+            newCap[w] = want;
+        else if (!moveParticles(w, want, true))
+            cannotGrow.push_back(w);  // no free range: the resume drops the excess
+    }
+    if (!live_) {
+        try {
+            growParticleArrays(newCap);
+        } catch (const Error& e) {
+            if (e.code != ALIEN_B200_ERR_OUT_OF_MEMORY) throw;
+            cannotGrow = halted;  // the arrays are unchanged: the resume drops the excess
+        }
+    }
+    refreshLayout();
+    DevState r = s_;
+    r.resume = 1;
+    launch(kEventWorld, r.numWorlds, kEventWorldThreads, r);
+    launch(kEventEmit, r.numCellBlocks + partGrid_, kBlock, r);
+    if (hasWorldParams_) launch(kWorldsEnd, divUp(r.numWorlds, kBlock), kBlock, r);
+    std::vector<uint64_t> missed(numWorlds(), 0);
+    uint64_t most = 0;
+    for (int w : halted) {
+        missed[w] = c[w].missedSteps;
+        most = std::max(most, missed[w]);
+    }
+    // the missed steps: each world that missed some gets that many as its
+    // budget, every other world is parked; afterwards budgets and activity
+    // are what an uninterrupted run would have left
+    const std::vector<WorldCounters> saved = readCounters();
+    std::vector<WorldCounters> now = saved;
+    for (int w : cannotGrow) now[w].dropExcess = 1;
+    if (most == 0) {
+        AB_CK(cudaMemcpyAsync(s_.counters, now.data(), sizeof(WorldCounters) * now.size(), cudaMemcpyHostToDevice, stream_));
+        AB_CK(cudaStreamSynchronize(stream_));
+        return false;
+    }
+    for (int w = 0; w < numWorlds(); ++w) {
+        now[w].active = missed[w] ? 1u : 0u;
+        if (missed[w]) now[w].stepsRemaining = missed[w];
+    }
+    AB_CK(cudaMemcpyAsync(s_.counters, now.data(), sizeof(WorldCounters) * now.size(), cudaMemcpyHostToDevice, stream_));
+    enqueueSteps(most);
+    const bool before = droppedPending_;
+    droppedPending_ = false;
+    settle();  // halts within the missed steps complete here
+    const bool dropped = droppedPending_;
+    droppedPending_ = before;
+    now = readCounters();
+    for (int w = 0; w < numWorlds(); ++w) {
+        if (missed[w]) {
+            const uint64_t b = saved[w].stepsRemaining;
+            now[w].stepsRemaining = b == ~0ull ? ~0ull : b - missed[w];
+            now[w].active = now[w].stepsRemaining != 0 ? 1u : 0u;
+        } else {
+            now[w].active = saved[w].active;
+        }
+    }
+    AB_CK(cudaMemcpyAsync(s_.counters, now.data(), sizeof(WorldCounters) * now.size(), cudaMemcpyHostToDevice, stream_));
+    AB_CK(cudaStreamSynchronize(stream_));
+    return dropped;
+}
+
+void Arena::growParticleArrays(const std::vector<long long>& newCap)
+{
+    const std::vector<WorldCounters> c = readCounters();
+    const int n = numWorlds();
+    std::vector<WorldInfo> infos(n);
+    long long partSlots = 0;
+    int partBlocks = 0;
+    for (int w = 0; w < n; ++w) {
+        WorldInfo wi = worlds_[w].info;
+        if (newCap[w] > wi.partCap) wi.partCap = roundUp(newCap[w], kBlock);
+        wi.partBase = partSlots;
+        wi.firstPartBlock = partBlocks;
+        wi.numPartBlocks = static_cast<int>(wi.partCap / kBlock);
+        partSlots += wi.partCap;
+        partBlocks += wi.numPartBlocks;
+        infos[w] = wi;
+    }
+    if (partSlots >= (1ll << 31)) throw Error(ALIEN_B200_ERR_CAPACITY, "arena exceeds 2^31 particle slots");
+    const DevState old = s_;
+    const int* oldRankParts = rankParts_;
+    const uint32_t* oldBlockCount = blockCount_;
+    const size_t P = static_cast<size_t>(partSlots);
+    // the new arrays beside the old ones; a failed allocation leaves the arena as it was
+    DevState s = s_;
+    s.pid = nullptr;  // allocated so far: the non-null new pointers
+    s.ppos = s.pvel = s.splitPos = s.splitVel = nullptr;
+    s.penergy = s.splitEnergy = nullptr;
+    s.pcolor = s.palive = s.pselected = nullptr;
+    s.pflag = s.blockSplit = nullptr;
+    s.plast = nullptr;
+    s.ptarget = s.pslot = nullptr;
+    s.pmerge = nullptr;
+    int* pbw = nullptr;
+    int* rankParts = nullptr;
+    uint32_t* blockCount = nullptr;
+    try {
+        allocParticleArrays(s, P, partBlocks);
+        pbw = mem_.alloc<int>(partBlocks);
+        rankParts = mem_.alloc<int>(P);
+        blockCount = mem_.alloc<uint32_t>(static_cast<size_t>(std::max(s.numCellBlocks, partBlocks)) + 2);
+    } catch (...) {
+        for (const void* p : {static_cast<const void*>(s.pid), static_cast<const void*>(s.ppos), static_cast<const void*>(s.pvel),
+                              static_cast<const void*>(s.penergy), static_cast<const void*>(s.pcolor),
+                              static_cast<const void*>(s.palive), static_cast<const void*>(s.pselected),
+                              static_cast<const void*>(s.pflag), static_cast<const void*>(s.plast),
+                              static_cast<const void*>(s.ptarget), static_cast<const void*>(s.pslot),
+                              static_cast<const void*>(s.pmerge), static_cast<const void*>(s.splitPos),
+                              static_cast<const void*>(s.splitVel), static_cast<const void*>(s.splitEnergy),
+                              static_cast<const void*>(s.blockSplit), static_cast<const void*>(pbw),
+                              static_cast<const void*>(rankParts), static_cast<const void*>(blockCount)})
+            if (p) mem_.release(p);
+        throw;
+    }
+    AB_CK(cudaMemsetAsync(s.palive, 0, P, stream_));
+    AB_CK(cudaMemsetAsync(s.pflag, 0, P * sizeof(uint32_t), stream_));
+    std::vector<int> pbwHost(partBlocks);
+    for (int w = 0; w < n; ++w) {
+        const WorldInfo& from = worlds_[w].info;
+        const WorldInfo& to = infos[w];
+        for (int b = 0; b < to.numPartBlocks; ++b) pbwHost[to.firstPartBlock + b] = w;
+        const size_t k = c[w].numParticles, a = static_cast<size_t>(from.partBase), z = static_cast<size_t>(to.partBase);
+        if (!k) continue;
+        auto move = [&](auto* dst, const auto* src, size_t items) {
+            AB_CK(cudaMemcpyAsync(dst + z, src + a, items * sizeof(*src), cudaMemcpyDeviceToDevice, stream_));
+        };
+        move(s.pid, old.pid, k);
+        move(s.plast, old.plast, k);
+        move(s.ppos, old.ppos, k);
+        move(s.pvel, old.pvel, k);
+        move(s.penergy, old.penergy, k);
+        move(s.pcolor, old.pcolor, k);
+        move(s.pselected, old.pselected, k);
+        move(s.palive, old.palive, k);
+        move(s.pflag, old.pflag, k);
+        move(s.splitPos, old.splitPos, k);
+        move(s.splitVel, old.splitVel, k);
+        move(s.splitEnergy, old.splitEnergy, k);
+        AB_CK(cudaMemcpyAsync(s.blockSplit + to.firstPartBlock, old.blockSplit + from.firstPartBlock,
+                              divUp(k, kBlock) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream_));
+    }
+    AB_CK(cudaMemcpyAsync(pbw, pbwHost.data(), sizeof(int) * partBlocks, cudaMemcpyHostToDevice, stream_));
+    for (const void* p : {static_cast<const void*>(old.pid), static_cast<const void*>(old.ppos), static_cast<const void*>(old.pvel),
+                          static_cast<const void*>(old.penergy), static_cast<const void*>(old.pcolor),
+                          static_cast<const void*>(old.palive), static_cast<const void*>(old.pselected),
+                          static_cast<const void*>(old.pflag), static_cast<const void*>(old.plast),
+                          static_cast<const void*>(old.ptarget), static_cast<const void*>(old.pslot),
+                          static_cast<const void*>(old.pmerge), static_cast<const void*>(old.splitPos),
+                          static_cast<const void*>(old.splitVel), static_cast<const void*>(old.splitEnergy),
+                          static_cast<const void*>(old.blockSplit), static_cast<const void*>(old.partBlockWorld),
+                          static_cast<const void*>(oldRankParts), static_cast<const void*>(oldBlockCount)})
+        mem_.release(p);
+    s.partBlockWorld = pbw;
+    s.numPartBlocks = partBlocks;
+    s.partSlots = partSlots;
+    s_ = s;
+    rankParts_ = rankParts;
+    blockCount_ = blockCount;
+    int device = 0, sms = 0;
+    AB_CK(cudaGetDevice(&device));
+    AB_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    partGrid_ = std::max(1, std::min(partBlocks, 16 * std::max(sms, 1)));
+    for (int w = 0; w < n; ++w) {
+        worlds_[w].info = infos[w];
+        maxWorldParts_ = std::max(maxWorldParts_, infos[w].partCap);
+    }
+    AB_CK(cudaMemcpyAsync(const_cast<WorldInfo*>(s_.worlds), infos.data(), sizeof(WorldInfo) * n, cudaMemcpyHostToDevice, stream_));
+    releaseGraph();  // the graph holds the old arrays
+    AB_CK(cudaStreamSynchronize(stream_));
 }
 
 std::vector<WorldCounters> Arena::readCounters()
@@ -1512,7 +1761,17 @@ std::vector<WorldCounters> Arena::readCounters()
 // used slots pass 50 %, grow (rebuild) when live particles pass 50 %
 void Arena::ensureParticleCapacity()
 {
+    settle();
     std::vector<WorldCounters> c = readCounters();
+    {
+        // a world that could not grow halts again (and tries to grow) from now on
+        bool any = false;
+        for (WorldCounters& x : c) {
+            any |= x.dropExcess != 0;
+            x.dropExcess = 0;
+        }
+        if (any) AB_CK(cudaMemcpyAsync(s_.counters, c.data(), sizeof(WorldCounters) * c.size(), cudaMemcpyHostToDevice, stream_));
+    }
     std::vector<int> grow;
     for (int w = 0; w < numWorlds(); ++w) {
         if (!resident(w)) continue;
@@ -1652,6 +1911,7 @@ void Arena::calcTimesteps(uint64_t n)
 
 void Arena::setParams(int w, const AlienPhysicsParams& p)
 {
+    settle();
     HostWorld& hw = worlds_[w];
     validateParams(p, hw.info.W, hw.info.H);
     // the tile grid depends on the interaction radius, and the cluster arrays
@@ -1722,6 +1982,7 @@ AlienPhysicsParams Arena::params(int w)
 
 void Arena::setStepBudget(int w, uint64_t steps)
 {
+    settle();
     std::vector<WorldCounters> c = readCounters();
     c[w].stepsRemaining = steps == 0 ? ~0ull : steps;
     c[w].active = 1;
@@ -1730,6 +1991,7 @@ void Arena::setStepBudget(int w, uint64_t steps)
 
 void Arena::setTimestep(int w, uint64_t t)
 {
+    settle();
     std::vector<WorldCounters> c = readCounters();
     c[w].timestep = t;
     AB_CK(cudaMemcpy(s_.counters, c.data(), sizeof(WorldCounters) * c.size(), cudaMemcpyHostToDevice));
@@ -1756,6 +2018,7 @@ void Arena::getData(int w, bool useRect, AlienInt2 ul, AlienInt2 lr, const Alien
 {
     if (!out || !out->numCells || !out->numParticles || !out->numAuxiliaryData)
         throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "DataTO counters must not be null");
+    settle();  // a halted world completes its step before it is read
     const WorldInfo& wi = worlds_[w].info;
     AlienCellTO* egressCells = static_cast<AlienCellTO*>(
         egressCells_.ensure(sizeof(AlienCellTO) * static_cast<size_t>(std::max<long long>(maxWorldCells_, 1))));
@@ -2011,6 +2274,7 @@ void Arena::autotune()
 
 uint64_t Arena::cellMap(uint64_t capacity, uint64_t* ids, uint32_t* slots, uint32_t* tiles, uint8_t* flags)
 {
+    settle();
     const DevState& s = s_;
     binCurrentState();
     uint32_t total = 0;
@@ -2040,6 +2304,7 @@ uint64_t Arena::cellMap(uint64_t capacity, uint64_t* ids, uint32_t* slots, uint3
 
 AlienRawStatisticsData Arena::statisticsData(int w)
 {
+    settle();
     AB_CK(cudaMemsetAsync(timeline_, 0, sizeof(TimelineAcc), stream_));
     const WorldInfo& wi = worlds_[w].info;
     const long long slots = std::max(wi.cellCap, wi.partCap);
@@ -2077,6 +2342,7 @@ void Arena::resetTimeIntervalStatistics(int w)
 
 AlienRawStatistics Arena::statistics(int w)
 {
+    settle();
     AB_CK(cudaMemsetAsync(stats_ + w, 0, sizeof(StatsAcc), stream_));
     {
         const WorldInfo& wi = worlds_[w].info;
@@ -2681,6 +2947,7 @@ int alien_b200_batch_world_status(alien_b200_batch* b, int world, uint64_t* time
 {
     return guarded([&] {
         if (!b || !b->arena->resident(world)) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        b->arena->settle();
         std::vector<WorldCounters> c = b->arena->readCounters();
         if (timestep) *timestep = c[world].timestep;
         if (stepsRemaining) *stepsRemaining = c[world].stepsRemaining == ~0ull ? 0 : c[world].stepsRemaining;
@@ -2692,6 +2959,7 @@ int alien_b200_batch_num_active(alien_b200_batch* b)
 {
     if (!b || !b->arena) return -1;
     try {
+        b->arena->settle();
         std::vector<WorldCounters> c = b->arena->readCounters();
         int n = 0;
         for (const WorldCounters& x : c) n += x.active ? 1 : 0;

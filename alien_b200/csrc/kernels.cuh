@@ -73,12 +73,13 @@ __device__ __forceinline__ PartCtx partCtx(const DevState& s, int pb)
 }
 
 // The particle part of a combined launch: the grid's blocks past the cell
-// blocks stride over the particle blocks, skipping inactive worlds and the
-// blocks past a world's used slots (partBase + usedSlots(counters)), so its
-// cost follows the live particles rather than the capacity.  Everything f
-// sees is block-uniform, so f may synchronise the block; f's return ends one
-// particle block for the calling thread.
-template <class UsedSlots, class F>
+// blocks stride over the particle blocks, skipping inactive worlds (unless
+// SkipInactive is false) and the blocks past a world's used slots
+// (partBase + usedSlots(counters)), so its cost follows the live particles
+// rather than the capacity.  Everything f sees is block-uniform, so f may
+// synchronise the block; f's return ends one particle block for the calling
+// thread.
+template <bool SkipInactive = true, class UsedSlots, class F>
 __device__ __forceinline__ void forParticleBlocks(const DevState& s, UsedSlots usedSlots, F f, int firstBlock)
 {
     const int stride = gridDim.x - firstBlock;
@@ -87,7 +88,7 @@ __device__ __forceinline__ void forParticleBlocks(const DevState& s, UsedSlots u
         const WorldInfo& wi = s.worlds[w];
         const WorldCounters& wc = s.counters[w];
         const long long end = wi.partBase + static_cast<long long>(usedSlots(wc));
-        if (!wc.active || static_cast<long long>(pb) * kBlock >= end) {
+        if ((SkipInactive && !wc.active) || static_cast<long long>(pb) * kBlock >= end) {
             // on to the first block of the next world in this block's stride
             // (an unused block of a live arena belongs to no range: the next one)
             const int next = max(wi.firstPartBlock + wi.numPartBlocks, pb + 1);
@@ -101,10 +102,10 @@ __device__ __forceinline__ void forParticleBlocks(const DevState& s, UsedSlots u
         f(c, pb);
     }
 }
-template <class UsedSlots, class F>
+template <bool SkipInactive = true, class UsedSlots, class F>
 __device__ __forceinline__ void forParticleBlocks(const DevState& s, UsedSlots usedSlots, F f)
 {
-    forParticleBlocks(s, usedSlots, f, s.numCellBlocks);
+    forParticleBlocks<SkipInactive>(s, usedSlots, f, s.numCellBlocks);
 }
 __device__ __forceinline__ unsigned int usedParticles(const WorldCounters& wc) { return wc.numParticles; }
 
@@ -2090,6 +2091,9 @@ __global__ void __launch_bounds__(kBlock) kEventCount(DevState s)
         const uint32_t fl = s.flags[g];  // before the world lookup: every cell slot is inside the arena
         const int w = s.cellBlockWorld[blockIdx.x];
         WorldCounters& wc = s.counters[w];
+        // a halted world keeps its step's flags and block counts until the
+        // host completes that step (the test is uniform across the block)
+        if (wc.halted) return;
         uint32_t a = 0, b = 0;
         if (g < s.worlds[w].cellBase + wc.numCells) {
             a = (fl & kFlagRadiation) ? 1u : 0u;
@@ -2147,15 +2151,37 @@ __device__ uint32_t blockScanBlocks(uint32_t* arr, int first, int count)
 
 // one block per world: block offsets, id and slot bases, timestep advance;
 // the block scans run only for the kinds of events the step produced (1024
-// threads ran slower than 256 on a 4M-cell world's 15,625 block counts)
+// threads ran slower than 256 on a 4M-cell world's 15,625 block counts).
+//
+// A step whose new particles do not fit the world's particle range halts the
+// world here, before anything of the emission is written: the world turns
+// inactive with its step's flags, block counts and event scratch in place,
+// counts the steps it misses, and sets kErrHalted.  The host grows the range
+// (on the device, nothing else of the world moves) and relaunches kEventWorld,
+// kEventEmit and kWorldsEnd with DevState::resume set, which complete the
+// halted step exactly as an uninterrupted step would have; then it runs the
+// missed steps.  In the resume launches a world that still does not fit (no
+// larger range was free) drops the excess and sets kErrDropped, and so do its
+// steps until the next capacity check (WorldCounters::dropExcess).
 constexpr int kEventWorldThreads = kBlock;
 __global__ void __launch_bounds__(kEventWorldThreads) kEventWorld(DevState s)
 {
     const int w = blockIdx.x;
     WorldCounters& wc = s.counters[w];
     const uint32_t evR = wc.evRad, evD = wc.evDel, evS = wc.evSplit;
+    const bool halted = wc.halted != 0;
+    const uint32_t slot0 = wc.numParticles;  // the used slots before this step's appends
     __syncthreads();
-    if (!wc.active) {
+    if (s.resume) {
+        if (!halted) {
+            // completed worlds emit nothing in the resume launch
+            if (threadIdx.x == 0) wc.numEvents = 0;
+            return;
+        }
+    } else if (halted) {
+        if (threadIdx.x == 0 && (wc.stepsRemaining == ~0ull || wc.missedSteps + 1 < wc.stepsRemaining)) ++wc.missedSteps;
+        return;
+    } else if (!wc.active) {
         if (threadIdx.x == 0) {
             wc.numEvents = 0;
             wc.evRad = wc.evDel = wc.evSplit = 0;
@@ -2163,15 +2189,29 @@ __global__ void __launch_bounds__(kEventWorldThreads) kEventWorld(DevState s)
         return;
     }
     const WorldInfo& wi = s.worlds[w];
+    if (!s.resume && !wc.dropExcess &&
+        static_cast<unsigned long long>(slot0) + evR + evD + evS > static_cast<unsigned long long>(wi.partCap)) {
+        if (threadIdx.x == 0) {
+            wc.halted = 1;
+            wc.active = 0;
+            wc.numEvents = 0;
+            wc.missedSteps = 0;
+            atomicOr(s.errorFlags, kErrHalted);
+        }
+        return;
+    }
     // particle blocks holding used slots (the count before this step's appends)
     const int usedPartBlocks = static_cast<int>((wc.numParticles + kBlock - 1) / kBlock);
     const uint32_t R = evR ? blockScanBlocks<kEventWorldThreads>(s.blockRad, wi.firstCellBlock, wi.numCellBlocks) : 0u;
     const uint32_t D = evD ? blockScanBlocks<kEventWorldThreads>(s.blockDel, wi.firstCellBlock, wi.numCellBlocks) : 0u;
     const uint32_t S = evS ? blockScanBlocks<kEventWorldThreads>(s.blockSplit, wi.firstPartBlock, usedPartBlocks) : 0u;
     if (threadIdx.x != 0) return;
+    if (halted) {
+        wc.halted = 0;
+        wc.active = 1;
+    }
     wc.evRad = wc.evDel = wc.evSplit = 0;
     const unsigned long long id0 = wc.nextId;
-    const uint32_t slot0 = wc.numParticles;
     wc.radIdBase = id0;
     wc.splitIdBase = id0 + R;
     wc.delIdBase = id0 + R + S;
@@ -2184,7 +2224,7 @@ __global__ void __launch_bounds__(kEventWorldThreads) kEventWorld(DevState s)
     if (want > static_cast<unsigned long long>(wi.partCap)) {
         wc.droppedParticles += static_cast<uint32_t>(want - wi.partCap);
         wc.numParticles = static_cast<uint32_t>(wi.partCap);
-        atomicOr(s.errorFlags, 1u);
+        atomicOr(s.errorFlags, kErrDropped);
     } else {
         wc.numParticles = static_cast<uint32_t>(want);
     }
@@ -2214,6 +2254,8 @@ __global__ void kWorldsEnd(DevState s)
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= s.numWorlds) return;
     WorldCounters& wc = s.counters[w];
+    // a halted world's step ends when the host completes it (resume launch)
+    if (wc.halted) return;
     if (wc.backflowFix) {
         wc.externalEnergy += static_cast<double>(wc.backflowFix) / kBackflowScale;
         wc.backflowFix = 0;
@@ -2289,8 +2331,11 @@ __global__ void __launch_bounds__(kBlock) kEventEmit(DevState s)
         }
     } else {
         // splits come from the slots used before this step's appends
-        // (radSlotBase); appended particles carry no split
-        forParticleBlocks(s, [](const WorldCounters& wc) { return wc.radSlotBase; }, [&](const PartCtx& c, int pb) {
+        // (radSlotBase); appended particles carry no split.  A world whose
+        // step budget ended with this step is inactive already and still
+        // emits; worlds without events are skipped by their used slots
+        forParticleBlocks<false>(s, [](const WorldCounters& wc) { return wc.numEvents ? wc.radSlotBase : 0u; },
+                                 [&](const PartCtx& c, int pb) {
             const WorldCounters& wc = s.counters[c.w];
             if (wc.numEvents == 0) return;
             const WorldInfo& wi = s.worlds[c.w];

@@ -389,6 +389,11 @@ int alien_b200_last_error(char* buffer, size_t size);
 int alien_b200_create(const AlienGeneralSettings* general, const AlienPhysicsParams* params,
                       uint64_t timestep, alien_b200_simulation** out);
 int alien_b200_destroy(alien_b200_simulation* sim);
+/* Particle storage grows as the steps need it: every 64 steps when half of
+ * it is used, and inside a step whose new particles would not fit (the
+ * world halts before writing them; the call grows the storage on the
+ * device, completes the step and the remaining steps).  Results equal a run
+ * whose storage was large enough from the start; nothing is dropped. */
 int alien_b200_calc_timesteps(alien_b200_simulation* sim, uint64_t timesteps);
 int alien_b200_set_data(alien_b200_simulation* sim, const AlienDataTO* data);
 int alien_b200_get_data(alien_b200_simulation* sim, AlienInt2 upperLeft, AlienInt2 lowerRight,

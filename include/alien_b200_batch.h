@@ -30,7 +30,13 @@ int alien_b200_batch_calc_timesteps(alien_b200_batch* batch, uint64_t timesteps)
 int alien_b200_batch_enqueue_timesteps(alien_b200_batch* batch, uint64_t timesteps);
 /* waits for the enqueued steps, then grows particle storage where a world
  * has filled half of it (calc_timesteps does this every 64 steps); call it
- * at least every 64 enqueued steps */
+ * at least every 64 enqueued steps.  A world whose step created more
+ * particles than its range holds halted in that step; the wait grows its
+ * range, completes the step and runs the steps it missed (the other worlds
+ * parked), so every world ends as if its storage had been large enough.
+ * ALIEN_B200_ERR_CAPACITY: a live arena had no larger free range for such a
+ * world, whose steps then dropped the excess until the next capacity check
+ * (the world still completed its steps). */
 int alien_b200_batch_synchronize(alien_b200_batch* batch);
 int alien_b200_batch_get_data(alien_b200_batch* batch, int world, const AlienDataTO* data);
 int alien_b200_batch_get_array_sizes(alien_b200_batch* batch, int world, AlienArraySizes* sizes);
