@@ -848,6 +848,9 @@ constexpr int kRegionChoices[2][kNumRegionChoices][2] = {
     {{64, 8}, {32, 8}, {48, 8}, {40, 8}},     // fluid
     {{24, 16}, {16, 16}, {24, 8}, {12, 16}},  // collision
 };
+// candidates whose positions one thread loads together in the region scan
+constexpr int kScanGroup = 4;
+
 template <int Motion>
 constexpr size_t regionDynSmem()
 {
@@ -1028,16 +1031,30 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
                 const float bottom = static_cast<float>(gy) * T, top = fminf(static_cast<float>(gy + 1) * T, static_cast<float>(wi.H));
                 const int c0 = lx - (piG.x - reach < left ? 1 : 0), c1 = lx + (piG.x + reach >= right ? 1 : 0);
                 const int r0 = ly - (piG.y - reach < bottom ? 1 : 0), r1 = ly + (piG.y + reach >= top ? 1 : 0);
-                // scan: the hits in scan order (the first kHitCap kept, all counted)
+                // scan: the hits in scan order (the first kHitCap kept, all
+                // counted).  Candidates go in groups of kScanGroup: the
+                // group's positions are loaded before any of its hits is
+                // stored (the hit list shares the shared-memory buffer, so
+                // a load after a store could not be moved ahead of it), then
+                // its hits are appended in order
                 int nh = 0;
 #pragma unroll 1
                 for (int r = r0; r <= r1; ++r) {
                     const int b0 = tStart[r * LW + c0] - base, b1 = tStart[r * LW + c1 + 1] - base;
-                    for (int m = b0; m < b1; ++m) {
-                        const float2 dm = diff(m);
-                        if (law.near(dm) && law.relevant(sMeta, m, dm)) {
-                            if (nh < kHitCap) myHits[nh * kRegionThreads] = static_cast<uint16_t>(m);
-                            ++nh;
+#pragma unroll 1
+                    for (int m0 = b0; m0 < b1; m0 += kScanGroup) {
+                        float2 dm[kScanGroup];
+#pragma unroll
+                        for (int u = 0; u < kScanGroup; ++u) dm[u] = diff(min(m0 + u, b1 - 1));
+                        bool cand[kScanGroup];
+#pragma unroll
+                        for (int u = 0; u < kScanGroup; ++u) cand[u] = m0 + u < b1 && law.near(dm[u]);
+#pragma unroll
+                        for (int u = 0; u < kScanGroup; ++u) {
+                            if (cand[u] && law.relevant(sMeta, m0 + u, dm[u])) {
+                                if (nh < kHitCap) myHits[nh * kRegionThreads] = static_cast<uint16_t>(m0 + u);
+                                ++nh;
+                            }
                         }
                     }
                 }
