@@ -91,7 +91,7 @@ class RawStatisticsData(ctypes.Structure):
     _fields_ = [("timeline", TimelineStatistics), ("histogram", HistogramData)]
 
 
-REGION_CHOICES = 4
+REGION_CHOICES = 6
 
 
 class LaunchConfig(ctypes.Structure):

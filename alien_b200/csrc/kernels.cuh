@@ -844,9 +844,10 @@ struct RegionShape<ALIEN_B200_MOTION_COLLISION> {
 // is the default.  A cell's neighbours are visited in the same order
 // whatever the shape, so the choice changes no result.
 constexpr int kNumRegionChoices = ALIEN_B200_REGION_CHOICES;
+// (small shapes for small worlds, whose large regions are fewer than the SMs)
 constexpr int kRegionChoices[2][kNumRegionChoices][2] = {
-    {{64, 8}, {32, 8}, {48, 8}, {40, 8}},     // fluid
-    {{24, 16}, {16, 16}, {24, 8}, {12, 16}},  // collision
+    {{64, 8}, {32, 8}, {48, 8}, {40, 8}, {24, 8}, {16, 8}},    // fluid
+    {{24, 16}, {16, 16}, {24, 8}, {12, 16}, {16, 8}, {8, 8}},  // collision
 };
 // candidates whose positions one thread loads together in the region scan
 constexpr int kScanGroup = 4;

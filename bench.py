@@ -526,7 +526,7 @@ def main():
     launch_cfg = {"pair_region_tiles": {"fluid": list(lc.regionTiles[0]), "collision": list(lc.regionTiles[1])},
                   "autotuned": bool(lc.tuned),
                   "tuned_ms_by_region": {m: {f"{lc.candidates[i][k][0]}x{lc.candidates[i][k][1]}": round(lc.tunedMs[i][k], 4)
-                                             for k in range(4)} for i, m in enumerate(("fluid", "collision"))}}
+                                             for k in range(_lib.REGION_CHOICES)} for i, m in enumerate(("fluid", "collision"))}}
     ms = max_over_ranks(ms)
     cells_mean = 0.5 * (stats0.numCells + stats1.numCells)
     total_cells = sum_over_ranks(cells_mean)

@@ -452,7 +452,7 @@ const char* alien_b200_step_kernel_name(int index);
  * the reference, whose launch shapes are fixed (KERNEL_CALL, Macros.cuh:75-83)
  * or computed by calcOptimalThreadsForFluidKernel
  * (SimulationKernelsLauncher.cu:18-22). */
-#define ALIEN_B200_REGION_CHOICES 4
+#define ALIEN_B200_REGION_CHOICES 6
 typedef struct AlienLaunchConfig {
     int32_t regionTiles[2][2];      /* shape in use (tiles x, y), per motion type */
     int32_t regionChoice[2];        /* its index among the candidates */

@@ -1,7 +1,7 @@
 """The pair kernel's launch configuration and its autotuner.
 
 The pair kernel works on regions of tiles, one CTA each; the region shape
-is one of four candidates per motion type.  A cell's neighbours are visited
+is one of six candidates per motion type.  A cell's neighbours are visited
 in the same order whatever the shape, so the shape must change no result:
 worlds stepped with every fixed shape and with the autotuner's choice must
 agree bit for bit (cells, bonds and particles).  The autotuner's choice
