@@ -1404,8 +1404,12 @@ void Arena::scan(const uint32_t* in, long long n, uint32_t* out)
 {
     const int blocks = divUp(n, kScanTile);
     launch(kScanReduce, blocks, kBlock, in, n, s_.scanPartials);
+    if (blocks <= kScanFusedBlocks) {
+        launch(kScanDown<true>, blocks, kBlock, in, n, static_cast<const uint32_t*>(s_.scanPartials), out);
+        return;
+    }
     launch(kScanPartials<1024>, 1, 1024, s_.scanPartials, blocks);
-    launch(kScanDown, blocks, kBlock, in, n, static_cast<const uint32_t*>(s_.scanPartials), out);
+    launch(kScanDown<false>, blocks, kBlock, in, n, static_cast<const uint32_t*>(s_.scanPartials), out);
 }
 
 // -------------------------------------------------------------- step -----

@@ -392,30 +392,49 @@ __global__ void __launch_bounds__(kBlock) kStatsWorld(DevState s, int w, StatsAc
     unsigned int cells = 0, bonds = 0, parts = 0;
     unsigned int byColor[ALIEN_B200_MAX_COLORS] = {};
     long long cellE = 0, partE = 0;
-    const long long cellEnd = wi.cellBase + wc.numCells;
-    // the fields of a slot are loaded together (every slot below the count
-    // is allocated), then dead slots are skipped
-#pragma unroll 4
-    for (long long g = wi.cellBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x; g < cellEnd; g += stride) {
-        const bool alive = s.alive[g];
-        const unsigned int nc = s.numConn[g];
-        const float e = s.energy[g];
-        const int col = s.color[g] % ALIEN_B200_MAX_COLORS;
-        if (!alive) continue;
-        ++cells;
-        bonds += nc;
-        cellE += __double2ll_rn(static_cast<double>(e) * 65536.0);
+    // four slots per thread and iteration, as vector loads: ranges start at
+    // a multiple of 256 slots and their capacity is a multiple of 256, so
+    // the quads are aligned and lie inside the arrays; slots past the count
+    // and dead slots are skipped
+    const long long nCells = wc.numCells, cellQuads = (nCells + 3) / 4;
+#pragma unroll 2
+    for (long long i = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x; i < cellQuads; i += stride) {
+        const long long g = wi.cellBase + 4 * i;
+        const uchar4 al = *reinterpret_cast<const uchar4*>(s.alive + g);
+        const uchar4 nc = *reinterpret_cast<const uchar4*>(s.numConn + g);
+        const float4 e = *reinterpret_cast<const float4*>(s.energy + g);
+        const uchar4 co = *reinterpret_cast<const uchar4*>(s.color + g);
+        const long long left = nCells - 4 * i;
+        const bool a[4] = {al.x != 0, al.y != 0 && left > 1, al.z != 0 && left > 2, al.w != 0 && left > 3};
+        const unsigned int n4[4] = {nc.x, nc.y, nc.z, nc.w};
+        const float e4[4] = {e.x, e.y, e.z, e.w};
+        const int c4[4] = {co.x % ALIEN_B200_MAX_COLORS, co.y % ALIEN_B200_MAX_COLORS, co.z % ALIEN_B200_MAX_COLORS,
+                           co.w % ALIEN_B200_MAX_COLORS};
 #pragma unroll
-        for (int c = 0; c < ALIEN_B200_MAX_COLORS; ++c) byColor[c] += col == c ? 1u : 0u;
+        for (int k = 0; k < 4; ++k) {
+            if (!a[k]) continue;
+            ++cells;
+            bonds += n4[k];
+            cellE += __double2ll_rn(static_cast<double>(e4[k]) * 65536.0);
+#pragma unroll
+            for (int c = 0; c < ALIEN_B200_MAX_COLORS; ++c) byColor[c] += c4[k] == c ? 1u : 0u;
+        }
     }
-    const long long partEnd = wi.partBase + wc.numParticles;
-#pragma unroll 4
-    for (long long q = wi.partBase + static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x; q < partEnd; q += stride) {
-        const bool alive = s.palive[q];
-        const float e = s.penergy[q];
-        if (!alive) continue;
-        ++parts;
-        partE += __double2ll_rn(static_cast<double>(e) * 65536.0);
+    const long long nParts = wc.numParticles, partQuads = (nParts + 3) / 4;
+#pragma unroll 2
+    for (long long i = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x; i < partQuads; i += stride) {
+        const long long q = wi.partBase + 4 * i;
+        const uchar4 al = *reinterpret_cast<const uchar4*>(s.palive + q);
+        const float4 e = *reinterpret_cast<const float4*>(s.penergy + q);
+        const long long left = nParts - 4 * i;
+        const bool a[4] = {al.x != 0, al.y != 0 && left > 1, al.z != 0 && left > 2, al.w != 0 && left > 3};
+        const float e4[4] = {e.x, e.y, e.z, e.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (!a[k]) continue;
+            ++parts;
+            partE += __double2ll_rn(static_cast<double>(e4[k]) * 65536.0);
+        }
     }
     unsigned long long v[kStatsFields];
     v[0] = cells;

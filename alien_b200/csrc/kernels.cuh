@@ -308,7 +308,14 @@ __global__ void __launch_bounds__(Threads) kScanPartials(uint32_t* partials, int
 }
 
 // in and out are 16-byte aligned (device allocations), so a thread's eight
-// items are two 16-byte loads and stores wherever all eight lie below n
+// items are two 16-byte loads and stores wherever all eight lie below n.
+// With PrefixFromTotals the partials are kScanReduce's block totals as they
+// are, and every block sums those of the blocks before it (no kScanPartials
+// launch; for scans of at most kScanFusedBlocks blocks, where that costs at
+// most kScanFusedBlocks^2 / 2 reads from L2); otherwise they are already
+// scanned.
+constexpr int kScanFusedBlocks = 2048;
+template <bool PrefixFromTotals>
 __global__ void __launch_bounds__(kBlock) kScanDown(const uint32_t* in, long long n, const uint32_t* partials, uint32_t* out)
 {
     static_assert(kScanItems == 8, "two uint4 per thread");
@@ -323,11 +330,19 @@ __global__ void __launch_bounds__(kBlock) kScanDown(const uint32_t* in, long lon
 #pragma unroll
         for (int i = 0; i < kScanItems; ++i) v[i] = base + i < n ? in[base + i] : 0;
     }
+    uint32_t prefix;
+    if (PrefixFromTotals) {
+        uint32_t pre = 0;
+        for (int k = threadIdx.x; k < static_cast<int>(blockIdx.x); k += kBlock) pre += partials[k];
+        blockExclusiveScan(pre, &prefix);
+    } else {
+        prefix = partials[blockIdx.x];
+    }
     uint32_t sum = 0;
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) sum += v[i];
     uint32_t total;
-    uint32_t ex = blockExclusiveScan(sum, &total) + partials[blockIdx.x];
+    uint32_t ex = blockExclusiveScan(sum, &total) + prefix;
     uint32_t o[kScanItems];
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
