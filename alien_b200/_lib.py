@@ -118,6 +118,17 @@ class ArenaCapacity(ctypes.Structure):
     ]
 
 
+DENSITY_MAP_FIELDS = ("color", "otherMutant", "sameMutant1", "sameMutant2", "specificMutant", "lessComplexity1",
+                      "lessComplexity2", "moreComplexity1", "moreComplexity2")
+
+
+class DensityMap(ctypes.Structure):
+    """AlienDensityMap: sizes, and host arrays the call fills (null: skipped)"""
+    _fields_ = [("sizeX", ctypes.c_int32), ("sizeY", ctypes.c_int32)] + [
+        (name, ctypes.POINTER(ctypes.c_uint32 if name == "specificMutant" else ctypes.c_uint64))
+        for name in DENSITY_MAP_FIELDS]
+
+
 # every symbol declared in include/alien_b200.h and include/alien_b200_batch.h
 EXPORTED_SYMBOLS = [
     "alien_b200_version", "alien_b200_select_device", "alien_b200_time_timesteps",
@@ -138,7 +149,7 @@ EXPORTED_SYMBOLS = [
     "alien_b200_get_raw_statistics_data", "alien_b200_reset_time_interval_statistics",
     "alien_b200_batch_get_raw_statistics_data", "alien_b200_batch_reset_time_interval_statistics",
     "alien_b200_arena_bytes", "alien_b200_arena_create", "alien_b200_world_admit", "alien_b200_world_evict",
-    "alien_b200_arena_num_resident",
+    "alien_b200_arena_num_resident", "alien_b200_get_density_map", "alien_b200_batch_get_density_map",
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -205,6 +216,8 @@ def load() -> ctypes.CDLL:
     lib.alien_b200_choose_region.argtypes = [P(ctypes.c_float), i32]
     lib.alien_b200_choose_region.restype = i32
     lib.alien_b200_get_raw_statistics_data.argtypes = [vp, P(RawStatisticsData)]
+    lib.alien_b200_get_density_map.argtypes = [vp, P(DensityMap)]
+    lib.alien_b200_batch_get_density_map.argtypes = [vp, ctypes.c_int, P(DensityMap)]
     lib.alien_b200_reset_time_interval_statistics.argtypes = [vp]
     lib.alien_b200_batch_get_raw_statistics_data.argtypes = [vp, i32, P(RawStatisticsData)]
     lib.alien_b200_batch_reset_time_interval_statistics.argtypes = [vp, i32]

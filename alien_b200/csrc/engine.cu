@@ -210,6 +210,9 @@ struct HostWorld {
     // live arenas: an unused world slot, and what the admission check found
     bool vacant = false;
     uint32_t neurons = 0, signals = 0;
+    // the timestep the world was set with (its step counter has not moved
+    // past it when no step ran since)
+    uint64_t setTimestep = 0;
 };
 
 // first-fit ranges of [0, capacity): the cell blocks, particle blocks, tiles,
@@ -311,6 +314,8 @@ public:
     void countData(int w, uint64_t* cells, uint64_t* particles);
     AlienRawStatistics statistics(int w);
     AlienRawStatisticsData statisticsData(int w);
+    // the density map of the last step (alien_b200_get_density_map)
+    void densityMap(int w, AlienDensityMap* out);
     void resetTimeIntervalStatistics(int w);
     void setTimestep(int w, uint64_t t);
     void setStepBudget(int w, uint64_t steps);
@@ -714,6 +719,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
             throw Error(ALIEN_B200_ERR_CAPACITY, "more than 2^30 objects in one world");
         HostWorld hw;
         hw.params = ws.params;
+        hw.setTimestep = ws.timestep;
         WorldInfo& wi = hw.info;
         wi.W = ws.W;
         wi.H = ws.H;
@@ -869,6 +875,7 @@ void Arena::build(const std::vector<WorldSetup>& setups)
     AB_CK(cudaMemsetAsync(s.flags, 0, C * sizeof(uint32_t), stream_));
     AB_CK(cudaMemsetAsync(s.angleAcc, 0, C * 4 * sizeof(long long), stream_));
     AB_CK(cudaMemsetAsync(s.dpos, 0, C * sizeof(float2), stream_));
+    AB_CK(cudaMemsetAsync(s.push, 0, C * sizeof(float2), stream_));
     AB_CK(cudaMemsetAsync(s.neuronActivity, 0, sizeof(unsigned long long) * n * ALIEN_B200_MAX_COLORS, stream_));
     AB_CK(cudaMemsetAsync(s.energyAcc, 0, C * sizeof(long long), stream_));
     AB_CK(cudaMemsetAsync(s.newPartner, 0xff, C * sizeof(int), stream_));
@@ -1032,6 +1039,7 @@ void Arena::reserve(const AlienArenaCapacity& c)
     AB_CK(cudaMemsetAsync(s.flags, 0, C * sizeof(uint32_t), stream_));
     AB_CK(cudaMemsetAsync(s.angleAcc, 0, C * 4 * sizeof(long long), stream_));
     AB_CK(cudaMemsetAsync(s.dpos, 0, C * sizeof(float2), stream_));
+    AB_CK(cudaMemsetAsync(s.push, 0, C * sizeof(float2), stream_));
     AB_CK(cudaMemsetAsync(s.neuronActivity, 0, sizeof(unsigned long long) * n * ALIEN_B200_MAX_COLORS, stream_));
     AB_CK(cudaMemsetAsync(s.energyAcc, 0, C * sizeof(long long), stream_));
     AB_CK(cudaMemsetAsync(s.newPartner, 0xff, C * sizeof(int), stream_));
@@ -1096,6 +1104,7 @@ int Arena::admit(const WorldSetup& ws, uint64_t steps, int slot)
     // the world's extents, as build() lays out a world
     HostWorld hw;
     hw.params = ws.params;
+    hw.setTimestep = ws.timestep;
     WorldInfo& wi = hw.info;
     std::memset(&wi, 0, sizeof(wi));
     wi.W = ws.W;
@@ -1234,6 +1243,7 @@ int Arena::admit(const WorldSetup& ws, uint64_t steps, int slot)
     AB_CK(cudaMemsetAsync(s.flags + c0, 0, cn * sizeof(uint32_t), stream_));
     AB_CK(cudaMemsetAsync(s.angleAcc + 4 * c0, 0, cn * 4 * sizeof(long long), stream_));
     AB_CK(cudaMemsetAsync(s.dpos + c0, 0, cn * sizeof(float2), stream_));
+    AB_CK(cudaMemsetAsync(s.push + c0, 0, cn * sizeof(float2), stream_));
     AB_CK(cudaMemsetAsync(s.energyAcc + c0, 0, cn * sizeof(long long), stream_));
     AB_CK(cudaMemsetAsync(s.newPartner + c0, 0xff, cn * sizeof(int), stream_));
     AB_CK(cudaMemsetAsync(s.best + c0, 0xff, cn * sizeof(int), stream_));
@@ -1996,6 +2006,7 @@ void Arena::setStepBudget(int w, uint64_t steps)
 void Arena::setTimestep(int w, uint64_t t)
 {
     settle();
+    worlds_[w].setTimestep = t;
     std::vector<WorldCounters> c = readCounters();
     c[w].timestep = t;
     AB_CK(cudaMemcpy(s_.counters, c.data(), sizeof(WorldCounters) * c.size(), cudaMemcpyHostToDevice));
@@ -2342,6 +2353,60 @@ void Arena::resetTimeIntervalStatistics(int w)
     AB_CK(cudaMemsetAsync(s_.neuronActivity + static_cast<size_t>(w) * ALIEN_B200_MAX_COLORS, 0,
                           sizeof(unsigned long long) * ALIEN_B200_MAX_COLORS, stream_));
     AB_CK(cudaStreamSynchronize(stream_));
+}
+
+void Arena::densityMap(int w, AlienDensityMap* out)
+{
+    settle();
+    const HostWorld& hw = worlds_[w];
+    const WorldInfo& wi = hw.info;
+    out->sizeX = wi.W / kDensitySlot;
+    out->sizeY = wi.H / kDensitySlot;
+    uint64_t* host64[8] = {out->color, out->otherMutant, out->sameMutant1, out->sameMutant2, out->lessComplexity1,
+                           out->lessComplexity2, out->moreComplexity1, out->moreComplexity2};
+    bool any = out->specificMutant != nullptr;
+    for (uint64_t* p : host64) any |= p != nullptr;
+    const size_t n = static_cast<size_t>(out->sizeX) * static_cast<size_t>(out->sizeY);
+    if (!any || n == 0) return;
+    // one zeroed device block: eight u64 maps, then the u32 map
+    const size_t bytes = n * (8 * sizeof(unsigned long long) + sizeof(unsigned int));
+    unsigned long long* d = nullptr;
+    AB_CK(cudaMallocAsync(reinterpret_cast<void**>(&d), bytes, stream_));
+    try {
+        AB_CK(cudaMemsetAsync(d, 0, bytes, stream_));
+        DensityMapOut m;
+        m.color = d;
+        m.otherMutant = d + n;
+        m.sameMutant1 = d + 2 * n;
+        m.sameMutant2 = d + 3 * n;
+        m.lessComplexity1 = d + 4 * n;
+        m.lessComplexity2 = d + 5 * n;
+        m.moreComplexity1 = d + 6 * n;
+        m.moreComplexity2 = d + 7 * n;
+        m.specificMutant = reinterpret_cast<unsigned int*>(d + 8 * n);
+        m.sizeX = out->sizeX;
+        m.sizeY = out->sizeY;
+        WorldCounters c;
+        AB_CK(cudaMemcpyAsync(&c, s_.counters + w, sizeof(c), cudaMemcpyDeviceToHost, stream_));
+        AB_CK(cudaStreamSynchronize(stream_));
+        // the step that filled the map: the last one, or none since the world was set
+        m.timestep = c.timestep != hw.setTimestep && c.timestep > 0 ? c.timestep - 1 : c.timestep;
+        if (c.numCells) launch(kDensityMap, static_cast<int>(divUp(static_cast<long long>(c.numCells), kBlock)), kBlock, s_, w, m);
+        const unsigned long long* dev64[8] = {m.color, m.otherMutant, m.sameMutant1, m.sameMutant2, m.lessComplexity1,
+                                              m.lessComplexity2, m.moreComplexity1, m.moreComplexity2};
+        for (int k = 0; k < 8; ++k)
+            if (host64[k])
+                AB_CK(cudaMemcpyAsync(host64[k], dev64[k], n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_));
+        if (out->specificMutant)
+            AB_CK(cudaMemcpyAsync(out->specificMutant, m.specificMutant, n * sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                  stream_));
+        AB_CK(cudaFreeAsync(d, stream_));
+        AB_CK(cudaStreamSynchronize(stream_));
+    } catch (...) {
+        cudaFreeAsync(d, stream_);
+        cudaStreamSynchronize(stream_);
+        throw;
+    }
 }
 
 AlienRawStatistics Arena::statistics(int w)
@@ -2775,6 +2840,14 @@ int alien_b200_get_raw_statistics_data(alien_b200_simulation* sim, AlienRawStati
     });
 }
 
+int alien_b200_get_density_map(alien_b200_simulation* sim, AlienDensityMap* map)
+{
+    return guarded([&] {
+        if (!sim || !map) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "null argument");
+        sim->arena->densityMap(0, map);
+    });
+}
+
 int alien_b200_reset_time_interval_statistics(alien_b200_simulation* sim)
 {
     return guarded([&] {
@@ -2981,6 +3054,14 @@ int alien_b200_batch_get_raw_statistics(alien_b200_batch* b, int world, AlienRaw
         if (!b || !statistics || !b->arena->resident(world))
             throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
         *statistics = b->arena->statistics(world);
+    });
+}
+
+int alien_b200_batch_get_density_map(alien_b200_batch* b, int world, AlienDensityMap* map)
+{
+    return guarded([&] {
+        if (!b || !map || !b->arena->resident(world)) throw Error(ALIEN_B200_ERR_INVALID_ARGUMENT, "invalid world");
+        b->arena->densityMap(world, map);
     });
 }
 

@@ -505,4 +505,66 @@ __global__ void __launch_bounds__(kBlock) kRestoreCarried(DevState s, int w, con
     if (i < np) s.plast[wi.partBase + i] = last[i];
 }
 
+// ----------------------------------------------------------- density map --
+// DensityMap (DensityMap.cuh:8-230), the coarse map the reference fills in
+// every step (clear at SimulationKernels.cu:33, addCell for every cell in
+// the pair-force kernels :39 and :47) and that only sensor cells read.  Here
+// it is built on request, from the state the last step left: each live cell
+// at its position after that step's overlap correction (posA + push, the
+// position the reference's cell holds when its own thread adds it), on
+// slots of 8 x 8 (PreprocessedSimulationData.cuh:13), with the packed byte
+// counters of addCell (DensityMap.cuh:150-205; carries between the byte
+// lanes as in the reference's 64-bit adds).
+constexpr int kDensitySlot = 8;
+struct DensityMapOut {
+    unsigned long long *color, *otherMutant, *sameMutant1, *sameMutant2;
+    unsigned int* specificMutant;
+    unsigned long long *lessComplexity1, *lessComplexity2, *moreComplexity1, *moreComplexity2;
+    int sizeX, sizeY;
+    unsigned long long timestep;  // of the step that filled the map (other-mutant buckets)
+};
+
+__global__ void __launch_bounds__(kBlock) kDensityMap(DevState s, int w, DensityMapOut m)
+{
+    const WorldInfo& wi = s.worlds[w];
+    const long long i = static_cast<long long>(blockIdx.x) * kBlock + threadIdx.x;
+    if (i >= s.counters[w].numCells) return;
+    const long long g = wi.cellBase + i;
+    if (!s.alive[g]) return;
+    const float2 pos = s.posA[g] + s.push[g];
+    // toInt (Base.cuh:29-32) truncates; the index is checked as a whole
+    const long long index = static_cast<long long>(static_cast<int>(pos.x) / kDensitySlot) +
+                            static_cast<long long>(static_cast<int>(pos.y) / kDensitySlot) * m.sizeX;
+    if (index < 0 || index >= static_cast<long long>(m.sizeX) * m.sizeY) return;
+    const int color = s.color[g] % ALIEN_B200_MAX_COLORS;
+    atomicAdd(m.color + index, (1ull << (color * 8)) | (1ull << 56));
+    const AlienCellTO& c = s.cold[s.coldIdx[g]];
+    const uint32_t mutationId = c.mutationId;
+    if (mutationId == 0) {
+        atomicAdd(m.specificMutant + index, 1u);
+        return;
+    }
+    if (mutationId == 1) {
+        atomicAdd(m.specificMutant + index, 0x100u);
+        return;
+    }
+    const unsigned long long other = (static_cast<unsigned long long>(mutationId) + m.timestep / 23) % 8;
+    atomicAdd(m.otherMutant + index, 0x0101010101010101ull ^ (1ull << (other * 8)));
+    const unsigned long long b1 = mutationId % 3, b2 = mutationId % 5, b3 = mutationId % 7;
+    atomicAdd(m.sameMutant1 + index, (1ull << (b1 * 8)) | (1ull << ((b2 + 3) * 8)));
+    atomicAdd(m.sameMutant2 + index, 1ull << (b3 * 8));
+    // complexity bucket: the bit length of toInt(complexity * 10)
+    const int bucket = 32 - __clz(static_cast<int>(c.genomeComplexity * 10.0f));
+    const unsigned long long lanes = 0x0101010101010101ull;
+    if (bucket < 8) {
+        atomicAdd(m.lessComplexity1 + index, lanes << (bucket * 8));  // byte lanes bucket..7
+        atomicAdd(m.lessComplexity2 + index, lanes);
+        atomicAdd(m.moreComplexity1 + index, lanes >> ((7 - bucket) * 8));  // byte lanes 0..bucket
+    } else if (bucket < 16) {
+        atomicAdd(m.lessComplexity2 + index, lanes << ((bucket - 8) * 8));
+        atomicAdd(m.moreComplexity2 + index, lanes >> ((15 - bucket) * 8));
+        atomicAdd(m.moreComplexity1 + index, lanes);
+    }
+}
+
 }  // namespace ab

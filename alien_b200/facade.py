@@ -133,6 +133,11 @@ class SimulationFacade:
     def reset_time_interval_statistics(self) -> None:
         check(self._lib.alien_b200_reset_time_interval_statistics(self._handle()))
 
+    def get_density_map(self) -> dict:
+        """the density map the last step filled (DensityMap.cuh:8-230): field
+        name -> (sizeY, sizeX) array, entry [y, x] for slot x + y * sizeX"""
+        return _density_map(lambda m: self._lib.alien_b200_get_density_map(self._handle(), m))
+
     def launch_config(self) -> LaunchConfig:
         """pair-kernel region shapes in use, and the autotuner's timings"""
         c = LaunchConfig()
@@ -234,6 +239,10 @@ class BatchSimulation:
 
     def reset_time_interval_statistics(self, world: int) -> None:
         check(self._lib.alien_b200_batch_reset_time_interval_statistics(self._h, int(world)))
+
+    def get_density_map(self, world: int) -> dict:
+        """world's density map (SimulationFacade.get_density_map)"""
+        return _density_map(lambda m: self._lib.alien_b200_batch_get_density_map(self._h, int(world), m))
 
     def get_raw_statistics(self, world: int) -> RawStatistics:
         r = RawStatistics()
@@ -373,4 +382,20 @@ def _timed(lib, fn, handle, timesteps):
     for k in range(n.value):
         name = lib.alien_b200_step_kernel_name(k)
         out[name.decode() if name else f"k{k}"] = buf[k]
+    return out
+
+
+def _density_map(call) -> dict:
+    """two calls of an AlienDensityMap entry point: the sizes, then the arrays"""
+    m = _lib.DensityMap()
+    check(call(ctypes.byref(m)))
+    sx, sy = int(m.sizeX), int(m.sizeY)
+    out = {name: np.zeros((sy, sx), np.uint32 if name == "specificMutant" else np.uint64)
+           for name in _lib.DENSITY_MAP_FIELDS}
+    if sx * sy == 0:
+        return out
+    for name, arr in out.items():
+        ctype = ctypes.c_uint32 if name == "specificMutant" else ctypes.c_uint64
+        setattr(m, name, arr.ctypes.data_as(ctypes.POINTER(ctype)))
+    check(call(ctypes.byref(m)))
     return out

@@ -415,6 +415,35 @@ int alien_b200_get_raw_statistics_data(alien_b200_simulation* sim, AlienRawStati
  * accumulated statistics. */
 int alien_b200_reset_time_interval_statistics(alien_b200_simulation* sim);
 
+/* The density map (DensityMap, source/EngineGpuKernels/DensityMap.cuh:8-230)
+ * that the reference fills in every step (cleared at SimulationKernels.cu:33,
+ * DensityMap::addCell for every cell in the pair-force kernels at :39 and
+ * :47) and that only its sensor cells read.  Built on request here, with the
+ * reference's layout: slots of 8 x 8 (PreprocessedSimulationData.cuh:13),
+ * sizeX = worldSizeX / 8, sizeY = worldSizeY / 8, entry x + y * sizeX, and
+ * the packed byte counters of addCell (per color and a total byte; mutant
+ * buckets; genome-complexity buckets; carries between byte lanes as in the
+ * reference's 64-bit adds).  The map is the one the last step filled: every
+ * live cell at its position after that step's overlap correction, the
+ * other-mutant buckets at that step's timestep (the current one minus 1).
+ * Without a step since the world was set, the cells at their set positions
+ * and the current timestep.  Cells the last step removed are not in it.
+ * sizeX and sizeY are always written; each array that is not null receives
+ * sizeX * sizeY entries (call once with null arrays for the size). */
+typedef struct AlienDensityMap {
+    int32_t sizeX, sizeY;
+    uint64_t* color;            /* byte c: cells of color c; byte 7: all cells */
+    uint64_t* otherMutant;      /* mutationId >= 2: all bytes but bucket (id + timestep / 23) % 8 */
+    uint64_t* sameMutant1;      /* mutationId >= 2: byte id % 3 and byte 3 + id % 5 */
+    uint64_t* sameMutant2;      /* mutationId >= 2: byte id % 7 */
+    uint32_t* specificMutant;   /* byte 0: mutationId 0, byte 1: mutationId 1 */
+    uint64_t* lessComplexity1;  /* genome-complexity buckets (bit length of complexity * 10) */
+    uint64_t* lessComplexity2;
+    uint64_t* moreComplexity1;
+    uint64_t* moreComplexity2;
+} AlienDensityMap;
+int alien_b200_get_density_map(alien_b200_simulation* sim, AlienDensityMap* map);
+
 /* Device-resident timing hook: steps `timesteps` times on the handle's
  * stream without the end-of-call synchronisation and error read-back that
  * alien_b200_calc_timesteps performs.  For benchmarks that bracket the

@@ -42,6 +42,8 @@ int alien_b200_batch_get_data(alien_b200_batch* batch, int world, const AlienDat
 int alien_b200_batch_get_array_sizes(alien_b200_batch* batch, int world, AlienArraySizes* sizes);
 int alien_b200_batch_get_raw_statistics(alien_b200_batch* batch, int world, AlienRawStatistics* statistics);
 int alien_b200_batch_get_raw_statistics_data(alien_b200_batch* batch, int world, AlienRawStatisticsData* statistics);
+/* world's density map (alien_b200_get_density_map) */
+int alien_b200_batch_get_density_map(alien_b200_batch* batch, int world, AlienDensityMap* map);
 int alien_b200_batch_reset_time_interval_statistics(alien_b200_batch* batch, int world);
 /* World `world` steps `steps` more times and then stops (its state stays
  * resident and readable); 0 = no limit.  Worlds start active, unlimited. */

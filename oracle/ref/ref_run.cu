@@ -3,7 +3,7 @@
 // level.  TEST INFRASTRUCTURE: it is the reference arm of the benchmark and
 // the pin of the CPU oracle; the B200 engine never calls it.
 //
-//   ref_run <input> <output>
+//   ref_run <input> <output> [<density map output>]
 //
 // input : "ALRF" u32 version, i32 W, i32 H, u64 timestep, u64 warmup,
 //         u64 steps, AlienPhysicsParams, u64 numCells, u64 numParticles,
@@ -11,19 +11,54 @@
 // output: "ALRO" u32 version, u64 numCells, u64 numParticles, u64 numAux,
 //         double seconds (timed steps, wall clock around calcTimestep),
 //         u64 timestep, CellTO[], ParticleTO[], aux bytes
+// density map output (optional): "ALDM" i32 sizeX, i32 sizeY, then the
+//         reference's DensityMap arrays as the last step filled them
+//         (DensityMap.cuh:8-230), sizeX*sizeY entries each: color,
+//         otherMutant, sameMutant1, sameMutant2 (u64), specificMutant (u32),
+//         lessComplexity1, lessComplexity2, moreComplexity1,
+//         moreComplexity2 (u64)
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
+#include <type_traits>
 #include <vector>
 
 #include "EngineGpuKernels/SimulationCudaFacade.cuh"
+#include "EngineGpuKernels/SimulationData.cuh"
 #include "EngineGpuKernels/TOs.cuh"
 #include "EngineInterface/Settings.h"
 
 #include "../../include/alien_b200.h"
+
+// Read access to private members for the density-map output: an explicit
+// instantiation may name a private member, and the friend function it
+// defines hands out the member pointer (standard C++; nothing of the
+// reference's classes changes).
+template <class Tag, typename Tag::type Member>
+struct MemberAccess {
+    friend typename Tag::type memberOf(Tag) { return Member; }
+};
+#define AB_MEMBER(TAG, CLASS, TYPE, NAME)                              \
+    struct TAG {                                                       \
+        using type = TYPE CLASS::*;                                    \
+        friend type memberOf(TAG);                                     \
+    };                                                                 \
+    template struct MemberAccess<TAG, &CLASS::NAME>;
+AB_MEMBER(FacadeData, _SimulationCudaFacade, std::shared_ptr<SimulationData>, _cudaSimulationData)
+AB_MEMBER(MapSize, DensityMap, int2, _densityMapSize)
+AB_MEMBER(MapColor, DensityMap, uint64_t*, _colorDensityMap)
+AB_MEMBER(MapOther, DensityMap, uint64_t*, _otherMutantDensityMap)
+AB_MEMBER(MapSame1, DensityMap, uint64_t*, _sameMutantDensityMap1)
+AB_MEMBER(MapSame2, DensityMap, uint64_t*, _sameMutantDensityMap2)
+AB_MEMBER(MapSpecific, DensityMap, uint32_t*, _specificMutantDensityMap)
+AB_MEMBER(MapLess1, DensityMap, uint64_t*, _lessGenomeComplexityDensityMap1)
+AB_MEMBER(MapLess2, DensityMap, uint64_t*, _lessGenomeComplexityDensityMap2)
+AB_MEMBER(MapMore1, DensityMap, uint64_t*, _moreGenomeComplexityDensityMap1)
+AB_MEMBER(MapMore2, DensityMap, uint64_t*, _moreGenomeComplexityDensityMap2)
+#undef AB_MEMBER
 
 static_assert(sizeof(CellTO) == sizeof(AlienCellTO), "CellTO layout");
 static_assert(sizeof(ParticleTO) == sizeof(AlienParticleTO), "ParticleTO layout");
@@ -163,8 +198,8 @@ SimulationParameters toReference(AlienPhysicsParams const& a)
 
 int main(int argc, char** argv)
 {
-    if (argc != 3) {
-        fprintf(stderr, "usage: ref_run <input> <output>\n");
+    if (argc != 3 && argc != 4) {
+        fprintf(stderr, "usage: ref_run <input> <output> [<density map output>]\n");
         return 2;
     }
     try {
@@ -252,6 +287,32 @@ int main(int argc, char** argv)
         writeOrThrow(o, out.auxiliaryData, *out.numAuxiliaryData);
         fclose(o);
         out.destroy();
+        if (argc == 4) {
+            DensityMap const& dm = ((*facade).*memberOf(FacadeData{}))->preprocessedSimulationData.densityMap;
+            int2 const size = dm.*memberOf(MapSize{});
+            const size_t n = static_cast<size_t>(size.x) * size.y;
+            FILE* d = fopen(argv[3], "wb");
+            if (!d) throw std::runtime_error("cannot open density map output");
+            writeOrThrow(d, "ALDM", 4);
+            writeOrThrow(d, &size.x);
+            writeOrThrow(d, &size.y);
+            auto put = [&](auto* devicePtr) {
+                std::vector<std::remove_pointer_t<decltype(devicePtr)>> host(n);
+                if (cudaMemcpy(host.data(), devicePtr, n * sizeof(host[0]), cudaMemcpyDeviceToHost) != cudaSuccess)
+                    throw std::runtime_error("density map copy failed");
+                writeOrThrow(d, host.data(), n);
+            };
+            put(dm.*memberOf(MapColor{}));
+            put(dm.*memberOf(MapOther{}));
+            put(dm.*memberOf(MapSame1{}));
+            put(dm.*memberOf(MapSame2{}));
+            put(dm.*memberOf(MapSpecific{}));
+            put(dm.*memberOf(MapLess1{}));
+            put(dm.*memberOf(MapLess2{}));
+            put(dm.*memberOf(MapMore1{}));
+            put(dm.*memberOf(MapMore2{}));
+            fclose(d);
+        }
         // process exit releases the facade's device memory
         fflush(nullptr);
         std::_Exit(0);

@@ -59,17 +59,40 @@ REF_MAX_CELLS = (2**31 - 1) // 336 - 1000
 REF_MAX_CELLS = REF_MAX_CELLS // 3 - 300000
 
 
-def run(data: DataTO, world, params: PhysicsParams, steps=1, warmup=0, timestep=0, timeout=1800):
-    """returns (DataTO after warmup + steps, seconds of the timed steps, timestep)"""
+DENSITY_MAP_NAMES = ("color", "otherMutant", "sameMutant1", "sameMutant2", "specificMutant", "lessComplexity1",
+                     "lessComplexity2", "moreComplexity1", "moreComplexity2")
+
+
+def read_density_map(path):
+    """the reference's DensityMap arrays as its last step filled them
+    (DensityMap.cuh:8-230): name -> (sizeY, sizeX) array"""
+    with open(path, "rb") as f:
+        raw = f.read()
+    assert raw[:4] == b"ALDM", "bad density map file"
+    sx, sy = struct.unpack_from("<ii", raw, 4)
+    off, out = 12, {}
+    for name in DENSITY_MAP_NAMES:
+        dt = np.uint32 if name == "specificMutant" else np.uint64
+        out[name] = np.frombuffer(raw, dt, sx * sy, off).reshape(sy, sx).copy()
+        off += sx * sy * np.dtype(dt).itemsize
+    return out
+
+
+def run(data: DataTO, world, params: PhysicsParams, steps=1, warmup=0, timestep=0, timeout=1800, density_map=False):
+    """returns (DataTO after warmup + steps, seconds of the timed steps, timestep), and with density_map the
+    reference's density map of the last step as a fourth element"""
     if not available():
         raise FileNotFoundError(f"{REF_RUN} not built")
     if data.num_cells > REF_MAX_CELLS:
         raise ValueError(f"the reference engine holds at most {REF_MAX_CELLS} cells in one world "
                          f"(int overflow of its dynamic-memory bound), got {data.num_cells}")
     with tempfile.TemporaryDirectory() as d:
-        inp, out = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
+        inp, out, dm = os.path.join(d, "in.bin"), os.path.join(d, "out.bin"), os.path.join(d, "dm.bin")
         write_input(inp, data, world, params, timestep, warmup, steps)
-        r = subprocess.run([REF_RUN, inp, out], capture_output=True, text=True, timeout=timeout)
+        r = subprocess.run([REF_RUN, inp, out] + ([dm] if density_map else []), capture_output=True, text=True,
+                           timeout=timeout)
         if r.returncode != 0:
             raise RuntimeError(f"ref_run failed ({r.returncode}): {r.stderr.strip()[-500:]}")
+        if density_map:
+            return read_output(out) + (read_density_map(dm),)
         return read_output(out)

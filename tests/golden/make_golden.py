@@ -142,10 +142,49 @@ def decay_input():
     return DataTO(cells), (1000, 1000), prm
 
 
+DENSITY_ONE_STEP = [
+    # name, seed, motion, timestep
+    ("density_collision_t47", 41, P.MOTION_COLLISION, 47),
+    ("density_fluid_t70", 42, P.MOTION_FLUID, 70),
+]
+
+
+def density_world(seed):
+    """a calm world (no overlap correction moves a cell in the step, so the
+    density map holds the cells at their input positions) whose cells carry
+    colors, mutation ids (0, 1 and others) and genome complexities that reach
+    every bucket of DensityMap::addCell (DensityMap.cuh:150-205)"""
+    data, world = worldgen.calm_test_world(seed, world=(96, 96), clusters=10, hex_clusters=4, free_cells=700)
+    rng = np.random.default_rng(seed)
+    n = data.num_cells
+    c = data.cells
+    c["color"] = rng.integers(0, 7, n).astype(c["color"].dtype)
+    c["mutationId"] = rng.choice(np.array([0, 1, 2, 3, 5, 7, 11, 24, 105, 1000003], np.uint32), n)
+    c["genomeComplexity"] = np.where(rng.random(n) < 0.1, rng.uniform(7000.0, 9000.0, n),
+                                     rng.uniform(0.0, 30.0, n)).astype(np.float32)
+    return data, world
+
+
+def density_fixtures(out_dir):
+    for name, seed, motion, t in DENSITY_ONE_STEP:
+        data, world = density_world(seed)
+        prm = P.benchmark_parameters(motion)
+        out, _, ts, dm = refrun.run(data, world, prm, steps=1, timestep=t, density_map=True)
+        np.savez_compressed(os.path.join(out_dir, f"ref_{name}.npz"), in_cells=data.cells, in_particles=data.particles,
+                            out_cells=out.cells, params=np.frombuffer(bytes(prm), np.uint8),
+                            meta=np.array([seed, motion, t, world[0], world[1], ts], np.int64),
+                            **{f"map_{k}": v for k, v in dm.items()})
+        print(name, out.num_cells, ts, {k: int(np.count_nonzero(v)) for k, v in dm.items()})
+
+
 def main(out_dir):
     """ZONES_ONLY=1 writes only the zone and rigidity fixtures; NEURON_ONLY=1
-    stops after the one-step and neuron fixtures"""
+    stops after the one-step and neuron fixtures; DENSITY_ONLY=1 writes only
+    the density-map fixtures"""
     os.makedirs(out_dir, exist_ok=True)
+    density_fixtures(out_dir)
+    if os.environ.get("DENSITY_ONLY"):
+        return
     zone_fixtures(out_dir)
     rigid_fixtures(out_dir)
     if os.environ.get("ZONES_ONLY"):
