@@ -399,7 +399,11 @@ private:
     // is); the used slots move with their step's split records, nothing else
     // of the state changes
     void growParticleArrays(const std::vector<long long>& newCap);
+    // growParticleArrays, or an export and rebuild when the device has no
+    // room for both sets of arrays
+    void growOrRebuild(const std::vector<long long>& newCap);
     bool droppedPending_ = false;  // a resume dropped particles: the next sync() reports it
+    bool stepsPending_ = false;    // steps were enqueued since settle() last read the error word
     // live arenas
     bool live_ = false;
     AlienArenaCapacity capacity_{};
@@ -1485,6 +1489,7 @@ void Arena::enqueueSteps(uint64_t n)
         cudaGraphDestroy(graph);
         AB_CK(e);
     }
+    stepsPending_ = true;
     for (uint64_t i = 0; i < n; ++i) {
         AB_CK(cudaGraphLaunch(graphExec_, stream_));
         launches_ += kernelsPerStep_;
@@ -1505,6 +1510,7 @@ std::vector<double> Arena::timedSteps(uint64_t n)
         events.push_back(start);
         timingEvents_ = &events;
         timingNames_.clear();
+        stepsPending_ = true;
         try {
             enqueueStep();
         } catch (...) {
@@ -1560,7 +1566,10 @@ void Arena::sync()
 
 void Arena::settle()
 {
-    if (!s_.errorFlags) return;  // nothing built yet
+    // only the steps set the error word: without steps since the last read
+    // there is nothing to wait for or to complete
+    if (!s_.errorFlags || !stepsPending_) return;
+    stepsPending_ = false;
     for (;;) {
         // the error word is read in stream order: one wait covers the work and the read
         uint32_t flags = 0;
@@ -1805,15 +1814,12 @@ void Arena::ensureParticleCapacity()
         return;
     }
     // resize (the counterpart of _SimulationCudaFacade::resizeArrays,
-    // SimulationCudaFacade.cu:619-655): export, rebuild larger, re-import;
-    // the growth changes no state (densities and absorbers continue)
-    std::vector<Carried> carried(numWorlds());
-    std::vector<uint64_t> extra(numWorlds(), 0);
-    for (int w = 0; w < numWorlds(); ++w) {
-        exportWorld(w, carried[w]);
-        extra[w] = std::find(grow.begin(), grow.end(), w) != grow.end() ? 2 * worlds_[w].info.partCap : 0;
-    }
-    rebuildFromHost(carried, extra, true);
+    // SimulationCudaFacade.cu:619-655): the particle arrays are allocated
+    // again on the device with three times the room for these worlds; the
+    // growth changes no state
+    std::vector<long long> newCap(numWorlds(), 0);
+    for (int w : grow) newCap[w] = 3 * worlds_[w].info.partCap;
+    growOrRebuild(newCap);
 }
 
 void Arena::growParticles(int w, uint64_t extra)
@@ -1822,11 +1828,29 @@ void Arena::growParticles(int w, uint64_t extra)
         moveParticles(w, worlds_[w].info.partCap + static_cast<long long>(extra));
         return;
     }
+    std::vector<long long> newCap(numWorlds(), 0);
+    newCap[w] = worlds_[w].info.partCap + static_cast<long long>(extra);
+    growOrRebuild(newCap);
+}
+
+void Arena::growOrRebuild(const std::vector<long long>& newCap)
+{
+    try {
+        growParticleArrays(newCap);
+        return;
+    } catch (const Error& e) {
+        if (e.code != ALIEN_B200_ERR_OUT_OF_MEMORY) throw;
+    }
+    // no room for the new arrays beside the old ones: export, rebuild larger
+    // (the old arena is released first), re-import; densities and absorbers
+    // continue
     std::vector<Carried> carried(numWorlds());
-    std::vector<uint64_t> extras(numWorlds(), 0);
-    for (int v = 0; v < numWorlds(); ++v) exportWorld(v, carried[v]);
-    extras[w] = extra;
-    rebuildFromHost(carried, extras, true);
+    std::vector<uint64_t> extra(numWorlds(), 0);
+    for (int w = 0; w < numWorlds(); ++w) {
+        exportWorld(w, carried[w]);
+        extra[w] = newCap[w] > worlds_[w].info.partCap ? static_cast<uint64_t>(newCap[w] - worlds_[w].info.partCap) : 0;
+    }
+    rebuildFromHost(carried, extra, true);
 }
 
 void Arena::exportWorld(int w, Carried& out)
