@@ -1054,23 +1054,57 @@ __global__ void __launch_bounds__(kRegionThreads, RegionShape<Motion>::MinBlocks
                 // a load after a store could not be moved ahead of it), then
                 // its hits are appended in order
                 int nh = 0;
+                auto push = [&](int m) {
+                    if (nh < kHitCap) myHits[nh * kRegionThreads] = static_cast<uint16_t>(m);
+                    ++nh;
+                };
+                if (Motion == ALIEN_B200_MOTION_FLUID) {
+                    // Fluid: the window's rows are one stream of candidates,
+                    // in row order and record order within a row, grouped
+                    // across the row boundaries, so that lanes with rows of
+                    // different lengths stay together and only the stream's
+                    // last group is partly empty (fluid1m's pair kernel
+                    // 0.108 -> 0.104 ms; the collision kernel, with fewer
+                    // registers to spare, was slower this way)
+                    const int rows = r1 - r0 + 1;
+                    const int s0 = tStart[r0 * LW + c0] - base, e0 = tStart[r0 * LW + c1 + 1] - base;
+                    const int s1 = rows > 1 ? tStart[(r0 + 1) * LW + c0] - base : 0;
+                    const int e1 = rows > 1 ? tStart[(r0 + 1) * LW + c1 + 1] - base : 0;
+                    const int s2 = rows > 2 ? tStart[(r0 + 2) * LW + c0] - base : 0;
+                    const int e2 = rows > 2 ? tStart[(r0 + 2) * LW + c1 + 1] - base : 0;
+                    const int n0 = e0 - s0, n01 = n0 + (e1 - s1), total = n01 + (e2 - s2);
+                    // record of stream position i (i < total)
+                    auto record = [&](int i) { return i < n0 ? s0 + i : (i < n01 ? s1 + (i - n0) : s2 + (i - n01)); };
 #pragma unroll 1
-                for (int r = r0; r <= r1; ++r) {
-                    const int b0 = tStart[r * LW + c0] - base, b1 = tStart[r * LW + c1 + 1] - base;
-#pragma unroll 1
-                    for (int m0 = b0; m0 < b1; m0 += kScanGroup) {
+                    for (int i0 = 0; i0 < total; i0 += kScanGroup) {
+                        int mm[kScanGroup];
+#pragma unroll
+                        for (int u = 0; u < kScanGroup; ++u) mm[u] = record(min(i0 + u, total - 1));
                         float2 dm[kScanGroup];
 #pragma unroll
-                        for (int u = 0; u < kScanGroup; ++u) dm[u] = diff(min(m0 + u, b1 - 1));
+                        for (int u = 0; u < kScanGroup; ++u) dm[u] = diff(mm[u]);
                         bool cand[kScanGroup];
 #pragma unroll
-                        for (int u = 0; u < kScanGroup; ++u) cand[u] = m0 + u < b1 && law.near(dm[u]);
+                        for (int u = 0; u < kScanGroup; ++u) cand[u] = i0 + u < total && law.near(dm[u]);
 #pragma unroll
-                        for (int u = 0; u < kScanGroup; ++u) {
-                            if (cand[u] && law.relevant(sMeta, m0 + u, dm[u])) {
-                                if (nh < kHitCap) myHits[nh * kRegionThreads] = static_cast<uint16_t>(m0 + u);
-                                ++nh;
-                            }
+                        for (int u = 0; u < kScanGroup; ++u)
+                            if (cand[u] && law.relevant(sMeta, mm[u], dm[u])) push(mm[u]);
+                    }
+                } else {
+#pragma unroll 1
+                    for (int r = r0; r <= r1; ++r) {
+                        const int b0 = tStart[r * LW + c0] - base, b1 = tStart[r * LW + c1 + 1] - base;
+#pragma unroll 1
+                        for (int m0 = b0; m0 < b1; m0 += kScanGroup) {
+                            float2 dm[kScanGroup];
+#pragma unroll
+                            for (int u = 0; u < kScanGroup; ++u) dm[u] = diff(min(m0 + u, b1 - 1));
+                            bool cand[kScanGroup];
+#pragma unroll
+                            for (int u = 0; u < kScanGroup; ++u) cand[u] = m0 + u < b1 && law.near(dm[u]);
+#pragma unroll
+                            for (int u = 0; u < kScanGroup; ++u)
+                                if (cand[u] && law.relevant(sMeta, m0 + u, dm[u])) push(m0 + u);
                         }
                     }
                 }
