@@ -277,6 +277,7 @@ public:
     {
         releaseGraph();
         if (checkStream_) cudaStreamDestroy(checkStream_);
+        if (readback_) cudaFreeHost(readback_);
     }
 
     void build(const std::vector<WorldSetup>& setups);
@@ -404,6 +405,20 @@ private:
     void growOrRebuild(const std::vector<long long>& newCap);
     bool droppedPending_ = false;  // a resume dropped particles: the next sync() reports it
     bool stepsPending_ = false;    // steps were enqueued since settle() last read the error word
+    // page-locked landing place of the small per-step reads (the error word,
+    // a world's statistics and counters): a copy into pageable memory goes
+    // through a staging buffer and adds to every step's wait
+    struct Readback {
+        uint32_t flags;
+        StatsAcc stats;
+        WorldCounters counters;
+    };
+    Readback* readback_ = nullptr;
+    Readback& readback()
+    {
+        if (!readback_) AB_CK(cudaMallocHost(reinterpret_cast<void**>(&readback_), sizeof(Readback)));
+        return *readback_;
+    }
     // live arenas
     bool live_ = false;
     AlienArenaCapacity capacity_{};
@@ -1572,9 +1587,10 @@ void Arena::settle()
     stepsPending_ = false;
     for (;;) {
         // the error word is read in stream order: one wait covers the work and the read
-        uint32_t flags = 0;
-        AB_CK(cudaMemcpyAsync(&flags, s_.errorFlags, sizeof(flags), cudaMemcpyDeviceToHost, stream_));
+        uint32_t& landed = readback().flags;
+        AB_CK(cudaMemcpyAsync(&landed, s_.errorFlags, sizeof(landed), cudaMemcpyDeviceToHost, stream_));
         AB_CK(cudaStreamSynchronize(stream_));
+        const uint32_t flags = landed;
         if (!flags) return;
         AB_CK(cudaMemsetAsync(s_.errorFlags, 0, sizeof(uint32_t), stream_));
         if (flags & kErrDropped) droppedPending_ = true;
@@ -2443,11 +2459,12 @@ AlienRawStatistics Arena::statistics(int w)
         const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>(statsGrid_, (slots + kBlock - 1) / kBlock)));
         launch(kStatsWorld, grid, kBlock, s_, w, stats_);
     }
-    StatsAcc a;
-    AB_CK(cudaMemcpyAsync(&a, stats_ + w, sizeof(a), cudaMemcpyDeviceToHost, stream_));
-    WorldCounters c;
-    AB_CK(cudaMemcpyAsync(&c, s_.counters + w, sizeof(c), cudaMemcpyDeviceToHost, stream_));
+    Readback& rb = readback();
+    AB_CK(cudaMemcpyAsync(&rb.stats, stats_ + w, sizeof(StatsAcc), cudaMemcpyDeviceToHost, stream_));
+    AB_CK(cudaMemcpyAsync(&rb.counters, s_.counters + w, sizeof(WorldCounters), cudaMemcpyDeviceToHost, stream_));
     AB_CK(cudaStreamSynchronize(stream_));
+    const StatsAcc a = rb.stats;
+    const WorldCounters c = rb.counters;
     AlienRawStatistics r;
     std::memset(&r, 0, sizeof(r));
     r.timestep = c.timestep;
