@@ -1625,8 +1625,10 @@ bool Arena::resumeHalted()
         try {
             growParticleArrays(newCap);
         } catch (const Error& e) {
-            if (e.code != ALIEN_B200_ERR_OUT_OF_MEMORY) throw;
-            cannotGrow = halted;  // the arrays are unchanged: the resume drops the excess
+            // no memory, or more than 2^31 particle slots: the arrays are
+            // unchanged and the resume drops the excess
+            if (e.code != ALIEN_B200_ERR_OUT_OF_MEMORY && e.code != ALIEN_B200_ERR_CAPACITY) throw;
+            cannotGrow = halted;
         }
     }
     refreshLayout();
