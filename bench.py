@@ -516,12 +516,19 @@ def main():
     stats0 = sim.get_raw_statistics()
     log("timed region")
     launches0 = sim.kernel_launches()
+    slots0 = sim.get_array_sizes().particleArraySize
     barrier()
     with ClockSampler(local_rank) as clk:
         ms = sim.time_timesteps(args.steps)
     barrier()
     launches = sim.kernel_launches() - launches0
     stats1 = sim.get_raw_statistics()
+    # particle storage grows inside time_timesteps only when a step's new
+    # particles did not fit; the world then halted and its missed steps ran
+    # after the timed region, so a line with growth would have timed less work
+    storage_grew = sim.get_array_sizes().particleArraySize != slots0
+    if storage_grew:
+        log("WARNING: particle storage grew during the timed region (a world halted): the line is not valid")
     lc = sim.launch_config()
     launch_cfg = {"pair_region_tiles": {"fluid": list(lc.regionTiles[0]), "collision": list(lc.regionTiles[1])},
                   "autotuned": bool(lc.tuned),
@@ -645,6 +652,7 @@ def main():
                         "note": "single steps between CUDA events, after the timed region"},
             "clocks": clk.summary(),
             "gpu_launches": launches,
+            "particle_storage_grew_in_timed_region": storage_grew,
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
